@@ -1,0 +1,161 @@
+/*
+ * prandtl_b200.h — C ABI of the B200-native DGSEM right-hand side and SSP-RK
+ * stage update.
+ *
+ * This ABI stands in for Prandtl's `DGSEMOperator : mfem::TimeDependentOperator`
+ * (src/Operators/DGSEMOperator.hpp:15).  Every entry point names the reference
+ * interface it replaces.  Plain C types only: device pointers are `double*`,
+ * CUDA streams are passed as `void*` (a `cudaStream_t`), sizes are int64.
+ *
+ * State layout (identical to the reference's MFEM `Ordering::byNODES` vector,
+ * src/Simulation/Simulation.hpp:64, with DG element-contiguous numbering):
+ *
+ *     u[v * num_nodes + e * Np^dim + lex(i, j, k)],   lex = (k*Np + j)*Np + i
+ *
+ * with v = 0..dim+1 (rho, rho*u, rho*v[, rho*w], E), Np = order + 1 and
+ * num_nodes = num_elements * Np^dim.  Gradient fields (BR1 lifting output) use
+ * the same layout and hold primitive-variable gradients (rho, u, v[, w], p).
+ *
+ * Mesh: affine, axis-aligned quads/hexes of extent h[0..dim-1] with a face
+ * neighbour table nbr[e*2*dim + f], f = (-x, +x, -y, +y, -z, +z).  Element
+ * numbering is free; the face orientation rule is: the face between element a's
+ * +d face and element b's -d face has element 1 = a when a <= b (normal +d),
+ * else element 1 = b (normal -d) — MFEM gives element 1 to the lower-numbered
+ * element of a face.
+ *
+ * Errors: every call returns a pdg_status; pdg_last_error() returns text for
+ * the last failing call on a context.  Nothing aborts the process.  Kernels
+ * record non-finite or non-physical states in a device error word that
+ * pdg_check() reads and clears.
+ *
+ * Threading: one context per stream; a context is not reentrant (the reference
+ * operator's Mult mutates `mutable` members the same way,
+ * src/Integrators/DGSEMIntegrator/DGSEMIntegrator.hpp:26-58).
+ */
+#ifndef PRANDTL_B200_H
+#define PRANDTL_B200_H
+
+#include <stdint.h>
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum pdg_status {
+    PDG_OK = 0,
+    PDG_ERR_ARG = 1,          /* bad argument / size */
+    PDG_ERR_CUDA = 2,         /* CUDA runtime error */
+    PDG_ERR_NONFINITE = 3,    /* NaN/Inf met in a state (device error word) */
+    PDG_ERR_NONPHYSICAL = 4,  /* rho <= 0 or p <= 0 met (device error word) */
+    PDG_ERR_UNSUPPORTED = 5,  /* (dim, order, flags) combination not compiled */
+    PDG_ERR_NOMEM = 6         /* device allocation failed */
+} pdg_status;
+
+/* Device error-word bits (pdg_check). */
+#define PDG_FLAG_NONFINITE   1u
+#define PDG_FLAG_NONPHYSICAL 2u
+
+/* Physics + scheme options.  Mirrors the reference's compile-time macros
+ * (parse_compile_config.py:15-34) and runtime JSON keys
+ * (src/Simulation/Simulation.cpp:99-157, 477-488) as runtime fields. */
+typedef struct pdg_params {
+    int32_t parabolic;        /* PARABOLIC: Navier-Stokes with BR1 lifting */
+    int32_t blending;         /* SUBCELL_FV_BLENDING: Persson-Peraire + subcell FV */
+    int32_t compat;           /* 1: reproduce the reference's value-changing quirks
+                                 (stale viscous state, z-flux fill, 3D face
+                                 dissipation term, running max wave speed) */
+    int32_t filter;           /* entropy/positivity filter after every RK stage */
+    double gamma;             /* ratio of specific heats */
+    double Pr;                /* Prandtl number */
+    double mu;                /* constant dynamic viscosity */
+    double R_gas;             /* gas constant (only used by diagnostics) */
+    double alpha_max;         /* blending cap, reference default 0.5 */
+    double alpha_min;         /* blending snap threshold, reference default 0.001 */
+    double face_dissipation;  /* 1.0 = reference LLF term; 0.0 switches it off
+                                 (used by the discrete entropy-conservation test) */
+} pdg_params;
+
+typedef struct pdg_mesh {
+    int32_t dim;              /* 2 or 3 */
+    int32_t order;            /* polynomial order N (Np = N + 1 LGL nodes) */
+    int64_t num_elements;
+    double h[3];              /* element extents */
+    const int32_t *nbr;       /* HOST pointer, num_elements * 2*dim entries */
+} pdg_mesh;
+
+typedef struct pdg_ctx pdg_ctx;
+
+/* Fill *p with the reference defaults (gamma 1.4, Pr 0.72, mu 0, R 287,
+ * alpha_max 0.5, alpha_min 0.001, blending on, compat on). */
+void pdg_default_params(pdg_params *p);
+
+/* DGSEMOperator ctor + DGSEMIntegrator ctor + PerssonPeraireIndicator ctor
+ * (src/Operators/DGSEMOperator.cpp:5-50; src/Integrators/DGSEMIntegrator/
+ * DGSEMIntegrator.cpp:8-149; src/Simulation/Simulation.cpp:486-488).
+ * Builds LGL D / D-hat / D-hat2, subcell normals, the modal Vandermonde and
+ * uploads the neighbour table.  Allocates its scratch (alpha, eta, gradient
+ * fields, error word) on the current device. */
+int pdg_create(const pdg_mesh *mesh, const pdg_params *params, pdg_ctx **out);
+int pdg_destroy(pdg_ctx *ctx);
+
+/* TimeDependentOperator::Height (DGSEMOperator.cpp:18): number of vdofs. */
+int64_t pdg_size(const pdg_ctx *ctx);
+
+/* DGSEMOperator::Mult(u, dudt) (src/Operators/DGSEMOperator.cpp:537-591):
+ * blending coefficient, [entropy variables, BR1 lifting, primitive gradients],
+ * volume + subcell FV + face terms.  u, dudt: DEVICE pointers, byNODES. */
+int pdg_rhs(pdg_ctx *ctx, const double *u, double *dudt, void *stream);
+
+/* Same with HOST pointers (the MFEM adapter path: Mult on host Vectors).
+ * Copies in, computes, copies out, synchronises. */
+int pdg_rhs_host(pdg_ctx *ctx, const double *u_host, double *dudt_host);
+
+/* One SSP-RK3 stage with the RHS fused into the axpy (the stage bodies of
+ * MFEM's RK3SSPSolver::Step as called at src/Simulation/Simulation.cpp:1010):
+ *   stage 0: uout = us + dt*L(us)                       (us = un)
+ *   stage 1: uout = 3/4 un + 1/4 (us + dt*L(us))
+ *   stage 2: uout = 1/3 un + 2/3 (us + dt*L(us))
+ * followed by the entropy filter when params.filter is set.  DEVICE pointers;
+ * uout may alias neither un nor us. */
+int pdg_rk_stage(pdg_ctx *ctx, int stage, double dt, const double *un,
+                 const double *us, double *uout, void *stream);
+
+/* ODESolver::Step for RK3SSPSolver (Simulation.cpp:1010): advances u (DEVICE)
+ * in place by one step of size dt using context-owned stage buffers. */
+int pdg_rk3_step(pdg_ctx *ctx, double dt, double *u, void *stream);
+
+/* DGSEMOperator::GetMaxCharSpeed (DGSEMOperator.hpp:106-109).  With compat=1
+ * this is the running maximum over every RHS evaluated so far (the
+ * reference never resets it); with compat=0 it is the maximum of the last
+ * RHS.  Synchronises the stream of the last call. */
+int pdg_max_char_speed(pdg_ctx *ctx, double *out);
+
+/* dt rule of Simulation::Run (Simulation.cpp:893-907,1013-1018):
+ * dt = cfl * hmin / (max_char_speed * (N+1)^2). */
+int pdg_cfl_dt(pdg_ctx *ctx, double cfl, double *dt_out);
+
+/* Per-element Persson-Peraire indicator and blending coefficient of the last
+ * RHS (DGSEMOperator::ComputeBlendingCoefficient, DGSEMOperator.cpp:60-80),
+ * copied to HOST arrays of num_elements doubles (either may be NULL). */
+int pdg_get_blending(pdg_ctx *ctx, double *eta_host, double *alpha_host);
+
+/* Primitive-variable gradients of the last parabolic RHS (the reference's
+ * dudx/dudy/dudz grid functions after ComputeGlobalPrimitiveGradVector,
+ * DGSEMOperator.cpp:134-159), copied to a HOST array of dim*size doubles. */
+int pdg_get_gradients(pdg_ctx *ctx, double *grad_host);
+
+/* Reads and clears the device error word (PDG_FLAG_*).  Synchronises. */
+int pdg_check(pdg_ctx *ctx, uint32_t *flags);
+
+/* Text of the last error on this context ("" if none). */
+const char *pdg_last_error(const pdg_ctx *ctx);
+
+/* Number of kernels this context has launched since creation. */
+int64_t pdg_launch_count(const pdg_ctx *ctx);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* PRANDTL_B200_H */

@@ -1,0 +1,1292 @@
+// dgsem_oracle.cpp — CPU restatement of Prandtl's DGSEM right-hand side
+// (DGSEMOperator::Mult) and SSP-RK3 step, used as the parity oracle and as the
+// timed CPU baseline.
+//
+// TEST INFRASTRUCTURE ONLY.  Nothing in the product (prandtl_b200/) links or
+// calls this file; only tests/, __graft_entry__.smoke() and bench.py's CPU
+// baseline load it, always as the checker.
+//
+// Parity status: the pointwise physics (log-mean, Chandrashekar volume and
+// face fluxes, viscous flux, entropy-variable transforms) is pinned bit for
+// bit against the reference's own sources compiled here with a stand-in MFEM
+// header (oracle/ref_shim, built into oracle/_ref/).  The assembly loops are
+// restated from the reference source cited at each function; the reference
+// ships no tests, golden vectors or fixtures and cannot be linked against MFEM
+// here, so those loops are not pinned against a run of the reference.
+//
+// Mesh model: affine, axis-aligned Cartesian elements, periodic via the
+// neighbour table.  MFEM pieces the reference relies on are restated from
+// their mathematics: the Gauss-Lobatto rule on [0,1], Lagrange shape values at
+// the nodes (Kronecker delta), CalcOrtho face normals (|n| = face measure,
+// outward from element 1), ElementTransformation::Weight / AdjugateJacobian
+// of an affine map, shifted Legendre polynomials, RK3SSPSolver.
+//
+// Build: g++ -O3 -march=native -fopenmp -ffp-contract=off -shared -fPIC.
+// -ffp-contract=off keeps every product and sum rounded as written, which is
+// how the reference's pointwise functions are compiled for the pin.
+
+#include <algorithm>
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+#include <limits>
+#include <vector>
+
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+#include "../include/prandtl_b200.h"
+
+namespace orc {
+
+// ---------------------------------------------------------------------------
+// Pointwise physics
+// ---------------------------------------------------------------------------
+
+// ComputeLogMean, src/BasicOperations/BasicOperations.cpp:6-12 (eps = 1e-4,
+// BasicOperations.hpp:9).
+static inline double logmean(double x, double y)
+{
+    const double eps = 1e-4;
+    double xi = y / x;
+    double u = (xi * (xi - 2.0) + 1.0) / (xi * (xi + 2.0) + 1);
+    return (u < eps) ? (x + y) * 52.5 / (105.0 + u * (35.0 + u * (21.0 + 15.0 * u)))
+                     : (y - x) / std::log(xi);
+}
+
+// ComputeSoundSpeed with b = 0, BasicOperations.cpp:52-55.
+static inline double sound_speed(double p, double rho, double gamma)
+{
+    return std::sqrt(gamma * p / (1.0 - 0.0 * rho) / rho);
+}
+
+// ChandrashekarFlux::ComputeVolumeFlux, src/RiemannSolvers/ChandrashekarFlux.cpp:11-83.
+// metric1/metric2 are the contravariant metric rows of the two nodes; their
+// mean is used.  Returns lambda_max.
+static double volume_flux(int dim, double gamma, const double *s1, const double *s2,
+                          const double *metric1, const double *metric2, double *F)
+{
+    const int ne = dim + 2;
+    const double gammaM1 = gamma - 1.0, gammaM1Inverse = 1.0 / gammaM1;
+    double metric[3];
+    for (int d = 0; d < dim; d++) {
+        metric[d] = metric1[d];
+        metric[d] += metric2[d];
+        metric[d] *= 0.5;
+    }
+    double mom[3];
+    double rho1 = s1[0], rho2 = s2[0];
+    double rho_ln = logmean(rho1, rho2);
+    double u1 = s1[1] / rho1, u2 = s2[1] / rho2;
+    double u_mean = 0.5 * (u1 + u2);
+    double V_sq1 = u1 * u1, V_sq2 = u2 * u2;
+    double Vn = u_mean * metric[0];
+    mom[0] = rho_ln * u_mean;
+    double h_hat = -0.25 * (u1 * u1 + u2 * u2) + u_mean * u_mean;
+    if (dim > 1) {
+        double v1 = s1[2] / rho1, v2 = s2[2] / rho2;
+        double v_mean = 0.5 * (v1 + v2);
+        V_sq1 += v1 * v1;
+        V_sq2 += v2 * v2;
+        Vn += v_mean * metric[1];
+        mom[1] = rho_ln * v_mean;
+        h_hat += -0.25 * (v1 * v1 + v2 * v2) + v_mean * v_mean;
+        if (dim > 2) {
+            double w1 = s1[3] / rho1, w2 = s2[3] / rho2;
+            double w_mean = 0.5 * (w1 + w2);
+            V_sq1 += w1 * w1;
+            V_sq2 += w2 * w2;
+            Vn += w_mean * metric[2];
+            mom[2] = rho_ln * w_mean;
+            h_hat += -0.25 * (w1 * w1 + w2 * w2) + w_mean * w_mean;
+        }
+    }
+    double p1 = gammaM1 * (s1[ne - 1] - 0.5 * rho1 * V_sq1);
+    double p2 = gammaM1 * (s2[ne - 1] - 0.5 * rho2 * V_sq2);
+    double lambda_max = std::sqrt(V_sq1) + sound_speed(p1, rho1, gamma);
+    lambda_max = std::max(lambda_max, std::sqrt(V_sq2) + sound_speed(p2, rho2, gamma));
+    double beta1 = 0.5 * rho1 / p1, beta2 = 0.5 * rho2 / p2;
+    double beta_ln = logmean(beta1, beta2);
+    double p_hat = 0.5 * (rho1 + rho2) / (beta1 + beta2);
+    h_hat += 0.5 / beta_ln * gammaM1Inverse + p_hat / rho_ln;
+    F[0] = rho_ln * Vn;
+    for (int d = 0; d < dim; d++) F[1 + d] = Vn * mom[d] + p_hat * metric[d];
+    F[1 + dim] = rho_ln * Vn * h_hat;
+    return lambda_max;
+}
+
+// ChandrashekarFlux::ComputeFaceFlux, ChandrashekarFlux.cpp:85-161.
+// compat=1 keeps the 3D energy-dissipation term as the reference writes it
+// (`rho_mean * dw + w_mean`, line 131); compat=0 uses rho_mean * dw * w_mean.
+// diss_scale multiplies the local Lax-Friedrichs term (1 = reference).
+static double face_flux(int dim, double gamma, int compat, double diss_scale,
+                        const double *s1, const double *s2, const double *nor, double *flux)
+{
+    const int ne = dim + 2;
+    const double gammaM1 = gamma - 1.0, gammaM1Inverse = 1.0 / gammaM1;
+    double nn = 0.0;  // Vector::Norml2
+    for (int d = 0; d < dim; d++) nn += nor[d] * nor[d];
+    double nor_mag = std::sqrt(nn);
+    double mom[3];
+    double rho1 = s1[0], rho2 = s2[0];
+    double rho_mean = 0.5 * (rho1 + rho2);
+    double rho_ln = logmean(rho1, rho2);
+    double drho = rho2 - rho1;
+    double u1 = s1[1] / rho1, u2 = s2[1] / rho2;
+    double u_mean = 0.5 * (u1 + u2);
+    double du = u2 - u1;
+    double V_sq1 = u1 * u1, V_sq2 = u2 * u2;
+    double Vn = u_mean * nor[0];
+    mom[0] = rho_ln * u_mean;
+    double h_hat = -0.25 * (u1 * u1 + u2 * u2) + u_mean * u_mean;
+    double diss = 0.5 * drho * u1 * u2 + rho_mean * du * u_mean;
+    if (dim > 1) {
+        double v1 = s1[2] / rho1, v2 = s2[2] / rho2;
+        double v_mean = 0.5 * (v1 + v2);
+        double dv = v2 - v1;
+        V_sq1 += v1 * v1;
+        V_sq2 += v2 * v2;
+        Vn += v_mean * nor[1];
+        mom[1] = rho_ln * v_mean;
+        h_hat += -0.25 * (v1 * v1 + v2 * v2) + v_mean * v_mean;
+        diss += 0.5 * drho * v1 * v2 + rho_mean * dv * v_mean;
+        if (dim > 2) {
+            double w1 = s1[3] / rho1, w2 = s2[3] / rho2;
+            double w_mean = 0.5 * (w1 + w2);
+            double dw = w2 - w1;
+            V_sq1 += w1 * w1;
+            V_sq2 += w2 * w2;
+            Vn += w_mean * nor[2];
+            mom[2] = rho_ln * w_mean;
+            h_hat += -0.25 * (w1 * w1 + w2 * w2) + w_mean * w_mean;
+            if (compat)
+                diss += 0.5 * drho * w1 * w2 + rho_mean * dw + w_mean;
+            else
+                diss += 0.5 * drho * w1 * w2 + rho_mean * dw * w_mean;
+        }
+    }
+    double p1 = gammaM1 * (s1[ne - 1] - 0.5 * rho1 * V_sq1);
+    double p2 = gammaM1 * (s2[ne - 1] - 0.5 * rho2 * V_sq2);
+    double lambda_max = std::sqrt(V_sq1) + sound_speed(p1, rho1, gamma);
+    lambda_max = std::max(lambda_max, std::sqrt(V_sq2) + sound_speed(p2, rho2, gamma));
+    double beta1 = 0.5 * rho1 / p1, beta2 = 0.5 * rho2 / p2;
+    double beta_ln = logmean(beta1, beta2);
+    double p_hat = 0.5 * (rho1 + rho2) / (beta1 + beta2);
+    h_hat += 0.5 / beta_ln * gammaM1Inverse + p_hat / rho_ln;
+    diss += 0.5 * drho * gammaM1Inverse / beta_ln + 0.5 * rho_mean * gammaM1Inverse * (1.0 / beta2 - 1.0 / beta1);
+    const double lam = lambda_max * diss_scale;
+    flux[0] = rho_ln * Vn - 0.5 * lam * (rho2 - rho1) * nor_mag;
+    for (int d = 0; d < dim; d++)
+        flux[1 + d] = Vn * mom[d] + p_hat * nor[d] - 0.5 * lam * (s2[1 + d] - s1[1 + d]) * nor_mag;
+    flux[1 + dim] = rho_ln * Vn * h_hat - 0.5 * lam * diss * nor_mag;
+    return lambda_max;
+}
+
+// NavierStokesFlux::ComputeViscousFlux, src/Fluxes/NavierStokesFlux.cpp:12-58
+// (3D) and :60-90 (2D), constant mu, mu_bulk = 2/3 (src/Physics/Physics.hpp:34).
+// dq[d*ne + v]: primitive gradient of variable v along x_d.  Output
+// flux[v*dim + d]; row v = 0 (mass) is left at zero.
+static void viscous_flux(int dim, double gamma, double Pr, double mu, const double *state,
+                         const double *dq, double *flux)
+{
+    const int ne = dim + 2;
+    const double gammaM1 = gamma - 1.0, gammaM1Inverse = 1.0 / gammaM1, PrInverse = 1.0 / Pr;
+    const double mu_bulk = 2.0 / 3.0;
+    // Conserv2Prim, BasicOperations.cpp:225-239 (pressure via ComputePressure).
+    double prim[5];
+    prim[0] = state[0];
+    for (int d = 0; d < dim; d++) prim[1 + d] = state[1 + d] / state[0];
+    {
+        double V[3], VV = 0.0;
+        for (int d = 0; d < dim; d++) V[d] = state[1 + d] / state[0];
+        for (int d = 0; d < dim; d++) VV += V[d] * V[d];
+        prim[ne - 1] = gammaM1 * (state[ne - 1] - 0.5 * state[0] * VV);
+    }
+    for (int i = 0; i < ne * dim; i++) flux[i] = 0.0;
+    const double lambda = mu * gamma * PrInverse;
+    const double *dqdx = dq, *dqdy = dq + ne, *dqdz = dq + 2 * ne;
+    auto F = [&](int v, int d) -> double & { return flux[v * dim + d]; };
+    if (dim == 3) {
+        double dudx = dqdx[1], dvdx = dqdx[2], dwdx = dqdx[3];
+        double dudy = dqdy[1], dvdy = dqdy[2], dwdy = dqdy[3];
+        double dudz = dqdz[1], dvdz = dqdz[2], dwdz = dqdz[3];
+        double div = dudx + dvdy + dwdz;
+        double cv_dTdx = gammaM1Inverse / prim[0] * (dqdx[4] - prim[4] / prim[0] * dqdx[0]);
+        double cv_dTdy = gammaM1Inverse / prim[0] * (dqdy[4] - prim[4] / prim[0] * dqdy[0]);
+        double cv_dTdz = gammaM1Inverse / prim[0] * (dqdz[4] - prim[4] / prim[0] * dqdz[0]);
+        F(1, 0) = mu * (2.0 * dudx - mu_bulk * div);
+        F(2, 0) = mu * (dudy + dvdx);
+        F(3, 0) = mu * (dudz + dwdx);
+        F(4, 0) = prim[1] * F(1, 0) + prim[2] * F(2, 0) + prim[3] * F(3, 0) + lambda * cv_dTdx;
+        F(1, 1) = mu * (dvdx + dudy);
+        F(2, 1) = mu * (2.0 * dvdy - mu_bulk * div);
+        F(3, 1) = mu * (dvdz + dwdy);
+        F(4, 1) = prim[1] * F(1, 1) + prim[2] * F(2, 1) + prim[3] * F(3, 1) + lambda * cv_dTdy;
+        F(1, 2) = mu * (dwdx + dudz);
+        F(2, 2) = mu * (dwdy + dvdz);
+        F(3, 2) = mu * (2.0 * dwdz - mu_bulk * div);
+        F(4, 2) = prim[1] * F(1, 2) + prim[2] * F(2, 2) + prim[3] * F(3, 2) + lambda * cv_dTdz;
+    } else {
+        double dudx = dqdx[1], dvdx = dqdx[2];
+        double dudy = dqdy[1], dvdy = dqdy[2];
+        double div = dudx + dvdy;
+        double cv_dTdx = gammaM1Inverse / prim[0] * (dqdx[3] - prim[3] / prim[0] * dqdx[0]);
+        double cv_dTdy = gammaM1Inverse / prim[0] * (dqdy[3] - prim[3] / prim[0] * dqdy[0]);
+        F(1, 0) = mu * (2.0 * dudx - mu_bulk * div);
+        F(2, 0) = mu * (dudy + dvdx);
+        F(3, 0) = prim[1] * F(1, 0) + prim[2] * F(2, 0) + lambda * cv_dTdx;
+        F(1, 1) = mu * (dvdx + dudy);
+        F(2, 1) = mu * (2.0 * dvdy - mu_bulk * div);
+        F(3, 1) = prim[1] * F(1, 1) + prim[2] * F(2, 1) + lambda * cv_dTdy;
+    }
+}
+
+// Conserv2Entropy, BasicOperations.cpp:134-157 (beta = rho/p here).
+static void conserv2entropy(int dim, double gamma, const double *state, double *w)
+{
+    const int ne = dim + 2;
+    const double gammaM1 = gamma - 1.0, gammaM1Inverse = 1.0 / gammaM1;
+    double vel[3], vv = 0.0;
+    for (int d = 0; d < dim; d++) vel[d] = state[1 + d] / state[0];
+    for (int d = 0; d < dim; d++) vv += vel[d] * vel[d];
+    double v_sq = 0.5 * vv;
+    double p = gammaM1 * (state[ne - 1] - state[0] * v_sq);
+    double beta = state[0] / p;
+    double s = std::log(p * std::pow(state[0], -gamma));
+    w[0] = (gamma - s) * gammaM1Inverse - beta * v_sq;
+    for (int d = 0; d < dim; d++) w[1 + d] = beta * vel[d];
+    w[ne - 1] = -beta;
+}
+
+// EntropyGrad2PrimGrad, BasicOperations.cpp:179-223, for one node and one
+// direction: g holds the entropy-variable gradient on entry and the primitive
+// gradient on exit.  The reference divides the momenta of its row copy in
+// place (`Vector vel(state.GetData() + 1, dim); vel /= state(0);`, :190-191),
+// so the density-gradient term reads velocities where it means momenta;
+// compat=1 keeps that, compat=0 uses the momenta.
+static void entgrad2primgrad(int dim, double gamma, int compat, const double *state_in, double *g)
+{
+    double state[5];
+    for (int v = 0; v < dim + 2; v++) state[v] = state_in[v];
+    if (compat)
+        for (int d = 0; d < dim; d++) state[1 + d] = state_in[1 + d] / state_in[0];
+    const int ne = dim + 2;
+    const double gammaM1 = gamma - 1.0, gammaM1Inverse = 1.0 / gammaM1;
+    double gs[5];
+    for (int v = 0; v < ne; v++) gs[v] = g[v];
+    double vel[3], vv = 0.0;
+    for (int d = 0; d < dim; d++) vel[d] = state_in[1 + d] / state_in[0];
+    for (int d = 0; d < dim; d++) vv += vel[d] * vel[d];
+    double v_sq = 0.5 * vv;
+    double p = gammaM1 * (state[ne - 1] - state[0] * v_sq);
+    double KE = v_sq * state[0];
+    if (dim == 2) {
+        g[1] = p / state[0] * (gs[1] + vel[0] * gs[3]);
+        g[2] = p / state[0] * (gs[2] + vel[1] * gs[3]);
+        g[0] = state[0] * gs[0] - gs[3] * (KE - p * gammaM1Inverse)
+             + state[0] / p * (state[1] * g[1] + state[2] * g[2]);
+        g[3] = p / state[0] * (g[0] + p * gs[3]);
+    } else {
+        g[1] = p / state[0] * (gs[1] + vel[0] * gs[4]);
+        g[2] = p / state[0] * (gs[2] + vel[1] * gs[4]);
+        g[3] = p / state[0] * (gs[3] + vel[2] * gs[4]);
+        g[0] = state[0] * gs[0] - gs[4] * (KE - p * gammaM1Inverse)
+             + state[0] / p * (state[1] * g[1] + state[2] * g[2] + state[3] * g[3]);
+        g[4] = p / state[0] * (g[0] + p * gs[4]);
+    }
+}
+
+// ComputePressure, BasicOperations.cpp:31-37.
+static inline double pressure(int dim, double gamma, const double *s)
+{
+    double V[3], VV = 0.0;
+    for (int d = 0; d < dim; d++) V[d] = s[1 + d] / s[0];
+    for (int d = 0; d < dim; d++) VV += V[d] * V[d];
+    return (gamma - 1.0) * (s[dim + 1] - 0.5 * s[0] * VV);
+}
+
+// ComputeEntropy (Euler branch), BasicOperations.cpp:39-46.
+static inline double entropy_fn(double rho, double p, double gamma)
+{
+    return rho > 0.0 && p > 0.0 ? rho * std::log(p * std::pow(rho, -gamma))
+                                : std::numeric_limits<double>::infinity();
+}
+
+// ---------------------------------------------------------------------------
+// One-dimensional operators
+// ---------------------------------------------------------------------------
+
+// Legendre P_n and P_n' on [-1,1] by the three-term recurrence.
+static void legendre(int n, long double x, long double &P, long double &dP)
+{
+    long double p0 = 1.0L, p1 = x;
+    if (n == 0) { P = 1.0L; dP = 0.0L; return; }
+    for (int k = 1; k < n; k++) {
+        long double p2 = ((2 * k + 1) * x * p1 - k * p0) / (k + 1);
+        p0 = p1;
+        p1 = p2;
+    }
+    P = p1;
+    dP = n * (x * p1 - p0) / (x * x - 1.0L);
+}
+
+// Gauss-Lobatto rule with Np points on [0,1] (what MFEM's
+// IntegrationRules(0, GaussLobatto).Get(SEGMENT, 2Np-3) returns,
+// DGSEMIntegrator.cpp:18-22): interior nodes are the roots of P_N', found by
+// Newton in long double; weights 1/(N(N+1) P_N(x)^2) on [0,1]; the rule is
+// mirrored so x[N-i] = 1 - x[i].
+static void gll(int Np, std::vector<double> &x, std::vector<double> &w)
+{
+    const int N = Np - 1;
+    x.assign(Np, 0.0);
+    w.assign(Np, 0.0);
+    const long double pi = 3.141592653589793238462643383279502884L;
+    for (int i = 0; i <= N / 2; i++) {
+        long double t;
+        if (i == 0) {
+            t = -1.0L;
+        } else {
+            t = -std::cos(pi * i / N);
+            for (int it = 0; it < 100; it++) {
+                long double P, dP;
+                legendre(N, t, P, dP);
+                long double d2P = (2.0L * t * dP - N * (N + 1) * P) / (1.0L - t * t);
+                long double dt = dP / d2P;
+                t -= dt;
+                if (std::fabs(dt) < 1e-30L) break;
+            }
+        }
+        long double P, dP;
+        legendre(N, t, P, dP);
+        long double wt = 1.0L / (N * (N + 1) * P * P);  // [0,1] weight
+        x[i] = (double)(0.5L * (1.0L + t));
+        w[i] = (double)wt;
+        x[N - i] = 1.0 - x[i];
+        w[N - i] = w[i];
+    }
+    if (N % 2 == 0) x[N / 2] = 0.5;
+}
+
+// ---------------------------------------------------------------------------
+// Context
+// ---------------------------------------------------------------------------
+
+struct Ctx {
+    pdg_params p;
+    int dim, N, Np, ndof, nv;
+    int64_t ne, nnodes, size;
+    double h[3];
+    std::vector<int32_t> nbr;
+    std::vector<double> x, w;           // GLL rule on [0,1]
+    std::vector<double> D;              // D[i*Np + l] = l'_l(x_i)
+    std::vector<double> Dhat, Dhat2;    // D + corr, 2D + corr (rows i)
+    double J, adj[3], area[3];
+    std::vector<double> snor[3];        // subcell normal component, interfaces 0..Np
+    std::vector<double> Vinv;           // modal inverse Vandermonde, ndof x ndof
+    std::vector<int> degs;              // ndof x dim 1D degrees of mode k
+    std::vector<double> Vdm;            // modal Vandermonde
+    std::vector<int> max_order;         // max 1D degree of mode k (filter)
+    double modalThreshold;
+    std::vector<double> eta, alpha;     // per element
+    std::vector<double> grads;          // dim * size
+    std::vector<double> went;           // entropy variables, size
+    std::vector<double> facebuf;        // per (e, dir): contributions to both sides
+    std::vector<double> emin;           // filter entropy bounds per element
+    double max_char_speed;              // integrator running max
+    double last_rhs_speed;              // max of the last RHS
+    std::vector<double> k1, y1, z1;     // RK scratch
+    int64_t filtered_elements;
+};
+
+static inline int64_t idx(const Ctx &c, int v, int64_t e, int n)
+{
+    return (int64_t)v * c.nnodes + e * c.ndof + n;
+}
+
+// DGSEMIntegrator ctor: barycentric D, D-hat, D-hat2 (DGSEMIntegrator.cpp:41-82).
+// Stored untransposed: Dhat2[i*Np+m] is what the reference reads as
+// Dhat2_T(m, i) after its transpose.
+static void build_derivative_matrices(Ctx &c)
+{
+    const int Np = c.Np;
+    std::vector<double> wBary(Np, 1.0);
+    for (int i = 1; i < Np; i++)
+        for (int j = 0; j < i; j++) {
+            wBary[j] *= (c.x[j] - c.x[i]);
+            wBary[i] *= (c.x[i] - c.x[j]);
+        }
+    for (int i = 0; i < Np; i++) wBary[i] = 1.0 / wBary[i];
+    c.D.assign(Np * Np, 0.0);
+    for (int iL = 0; iL < Np; iL++)
+        for (int i = 0; i < Np; i++)
+            if (iL != i) {
+                c.D[i * Np + iL] = wBary[iL] / wBary[i] / (c.x[i] - c.x[iL]);
+                c.D[i * Np + i] -= c.D[i * Np + iL];
+            }
+    c.Dhat = c.D;
+    c.Dhat[0] += 1.0 / c.w[0];
+    c.Dhat[(Np - 1) * Np + Np - 1] -= 1.0 / c.w[Np - 1];
+    c.Dhat2.assign(Np * Np, 0.0);
+    for (int i = 0; i < Np * Np; i++) c.Dhat2[i] = c.D[i] * 2.0;
+    c.Dhat2[0] += 1.0 / c.w[0];
+    c.Dhat2[(Np - 1) * Np + Np - 1] -= 1.0 / c.w[Np - 1];
+}
+
+// ComputeSubcellMetrics on an affine element (DGSEMIntegrator.cpp:1199-1304):
+// interface i normal = adj row + sum_{l<i} w_l * sum_m D(l,m) * adj row.  Only
+// the diagonal component is non-zero.
+static void build_subcell_normals(Ctx &c)
+{
+    for (int d = 0; d < c.dim; d++) {
+        c.snor[d].assign(c.Np + 1, 0.0);
+        const double a = c.adj[d];
+        for (int i = 0; i < c.Np + 1; i++) {
+            double nor = a;
+            for (int l = 0; l < i; l++) {
+                double tmp = 0.0;
+                for (int m = 0; m < c.Np; m++) {
+                    double metric2 = a;
+                    metric2 *= c.D[l * c.Np + m];
+                    tmp += metric2;
+                }
+                tmp *= c.w[l];
+                nor += tmp;
+            }
+            c.snor[d][i] = nor;
+        }
+    }
+}
+
+// Shifted Legendre on [0,1] (what Poly_1D::CalcLegendre evaluates).
+static void legendre01(int order, double x, double *L)
+{
+    double z;
+    L[0] = 1.0;
+    if (order == 0) return;
+    L[1] = z = 2.0 * x - 1.0;
+    for (int n = 1; n < order; n++) L[n + 1] = ((2 * n + 1) * z * L[n] - n * L[n - 1]) / (n + 1);
+}
+
+// Dense inverse by Gauss-Jordan with partial pivoting.
+static bool invert(std::vector<double> &A, int n)
+{
+    std::vector<double> I(n * n, 0.0);
+    for (int i = 0; i < n; i++) I[i * n + i] = 1.0;
+    for (int col = 0; col < n; col++) {
+        int piv = col;
+        for (int r = col + 1; r < n; r++)
+            if (std::fabs(A[r * n + col]) > std::fabs(A[piv * n + col])) piv = r;
+        if (A[piv * n + col] == 0.0) return false;
+        if (piv != col)
+            for (int k = 0; k < n; k++) {
+                std::swap(A[piv * n + k], A[col * n + k]);
+                std::swap(I[piv * n + k], I[col * n + k]);
+            }
+        double inv = 1.0 / A[col * n + col];
+        for (int k = 0; k < n; k++) {
+            A[col * n + k] *= inv;
+            I[col * n + k] *= inv;
+        }
+        for (int r = 0; r < n; r++)
+            if (r != col) {
+                double f = A[r * n + col];
+                if (f != 0.0)
+                    for (int k = 0; k < n; k++) {
+                        A[r * n + k] -= f * A[col * n + k];
+                        I[r * n + k] -= f * I[col * n + k];
+                    }
+            }
+    }
+    A = I;
+    return true;
+}
+
+// ModalBasis::ComputeUBDegs / ComputeVDM (src/ModalBasis/ModalBasis.cpp:42-135):
+// mode k has degrees with the x-degree slowest; V(i,k) = prod_d L_deg(x_i,d).
+static void build_modal(Ctx &c)
+{
+    const int nd = c.ndof, Np = c.Np, dim = c.dim;
+    c.degs.assign(nd * dim, 0);
+    for (int k = 0; k < nd; k++) {
+        int r = k;
+        for (int d = dim - 1; d >= 0; d--) {
+            c.degs[k * dim + d] = r % Np;
+            r /= Np;
+        }
+    }
+    c.max_order.assign(nd, 0);
+    for (int k = 0; k < nd; k++) {
+        int m = 0;
+        for (int d = 0; d < dim; d++) m = std::max(m, c.degs[k * dim + d]);
+        c.max_order[k] = m;
+    }
+    c.Vdm.assign(nd * nd, 0.0);
+    std::vector<double> L(Np);
+    for (int i = 0; i < nd; i++) {
+        int ii[3] = {i % Np, (i / Np) % Np, i / (Np * Np)};
+        for (int d = 0; d < dim; d++) {
+            legendre01(c.N, c.x[ii[d]], L.data());
+            for (int k = 0; k < nd; k++) {
+                double v = L[c.degs[k * dim + d]];
+                c.Vdm[i * nd + k] = (d == 0) ? v : c.Vdm[i * nd + k] * v;
+            }
+        }
+    }
+    c.Vinv = c.Vdm;
+    invert(c.Vinv, nd);
+}
+
+// ---------------------------------------------------------------------------
+// Blending coefficient: PerssonPeraireIndicator::CheckSmoothness
+// (src/Indicators/PerssonPeraireIndicator.cpp:21-58) and
+// DGSEMOperator::ComputeBlendingCoefficient (DGSEMOperator.cpp:60-80).
+// ---------------------------------------------------------------------------
+static void blending_coefficient(Ctx &c, const double *u)
+{
+    const int nd = c.ndof, nv = c.nv, dim = c.dim;
+#pragma omp parallel for schedule(static)
+    for (int64_t e = 0; e < c.ne; e++) {
+        std::vector<double> q(nd), m(nd), m1(nd), m2(nd);
+        double s[5];
+        for (int i = 0; i < nd; i++) {
+            for (int v = 0; v < nv; v++) s[v] = u[idx(c, v, e, i)];
+            q[i] = s[0] * pressure(dim, c.p.gamma, s);
+        }
+        for (int r = 0; r < nd; r++) {  // DenseMatrix::Mult
+            double acc = 0.0;
+            for (int k = 0; k < nd; k++) acc += c.Vinv[r * nd + k] * q[k];
+            m[r] = acc;
+        }
+        m1 = m;
+        m2 = m;
+        for (int i = 0; i < nd; i++)
+            for (int d = 0; d < dim; d++)
+                if (c.degs[i * dim + d] > c.N - 2) {
+                    m2[i] = 0.0;
+                    if (c.degs[i * dim + d] > c.N - 1) m1[i] = 0.0;
+                }
+        double mm = 0, m1m1 = 0, m2m2 = 0;
+        for (int i = 0; i < nd; i++) {
+            mm += m[i] * m[i];
+            m1m1 += m1[i] * m1[i];
+            m2m2 += m2[i] * m2[i];
+        }
+        double eta = 1.0 - m1m1 / mm;
+        eta = std::max(eta, 1.0 - m2m2 / m1m1);
+        c.eta[e] = eta;
+        const double sharpness_fac = 9.21024, T = c.modalThreshold;
+        double a = 1.0 / (1.0 + std::exp(-sharpness_fac * (eta - T) / T));
+        if (a < c.p.alpha_min)
+            a = 0.0;
+        else if (a > (1.0 - c.p.alpha_min))
+            a = 1.0;
+        a = std::min(a, c.p.alpha_max);
+        c.alpha[e] = a;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Element-local helpers
+// ---------------------------------------------------------------------------
+
+// Node index along direction d through node (i,j,k) at position l.
+static inline int line_node(const Ctx &c, int d, int i, int j, int k, int l)
+{
+    const int Np = c.Np;
+    if (d == 0) return (k * Np + j) * Np + l;
+    if (d == 1) return (k * Np + l) * Np + i;
+    return (l * Np + j) * Np + i;
+}
+
+// ComputeFVFluxes (DGSEMIntegrator.cpp:972-1196): writes el_dudt (ndof x nv,
+// row-major node) = alpha * subcell FV update.  Returns the max wave speed.
+static double fv_fluxes(const Ctx &c, const double *el_u, double alpha_value, double *el_dudt)
+{
+    const int Np = c.Np, nv = c.nv, dim = c.dim;
+    const int Npy = dim > 1 ? Np : 1, Npz = dim > 2 ? Np : 1;
+    double lam = -1.0;
+    double dU[5], flux[5], nor[3];
+    for (int dd = 0; dd < dim; dd++) {
+        // x lines iterate (k, j), y lines (k, i), z lines (j, i)
+        int A = (dd == 2) ? Npy : Npz;  // outer count
+        int B = (dd == 0) ? Npy : Np;   // inner count
+        for (int a = 0; a < A; a++)
+            for (int b = 0; b < B; b++) {
+                int i = 0, j = 0, k = 0;
+                if (dd == 0) { k = a; j = b; }
+                else if (dd == 1) { k = a; i = b; }
+                else { j = a; i = b; }
+                for (int v = 0; v < nv; v++) dU[v] = 0.0;
+                int id1 = line_node(c, dd, i, j, k, 0);
+                for (int q = 0; q < dim; q++) nor[q] = 0.0;
+                for (int l = 0; l < Np - 1; l++) {
+                    int id2 = line_node(c, dd, i, j, k, l + 1);
+                    nor[dd] = c.snor[dd][l + 1];
+                    const double *s1 = el_u + id1 * nv, *s2 = el_u + id2 * nv;
+                    lam = std::max(lam, face_flux(dim, c.p.gamma, c.p.compat, c.p.face_dissipation, s1, s2, nor, flux));
+                    for (int v = 0; v < nv; v++) {
+                        dU[v] -= flux[v];
+                        dU[v] /= c.J * c.w[l];
+                    }
+                    for (int v = 0; v < nv; v++) {
+                        if (dd == 0) el_dudt[id1 * nv + v] = dU[v];
+                        else el_dudt[id1 * nv + v] += dU[v];
+                    }
+                    for (int v = 0; v < nv; v++) dU[v] = flux[v];
+                    id1 = id2;
+                }
+                for (int v = 0; v < nv; v++) {
+                    dU[v] /= c.J * c.w[Np - 1];
+                    if (dd == 0) el_dudt[id1 * nv + v] = dU[v];
+                    else el_dudt[id1 * nv + v] += dU[v];
+                }
+            }
+    }
+    for (int i = 0; i < c.ndof * nv; i++) el_dudt[i] *= alpha_value;
+    return lam;
+}
+
+// AssembleElementVector, Euler (DGSEMIntegrator.cpp:224-433) and NS
+// (:601-750 3D, :752-864 2D).  el_u / el_dudt are node-major (ndof x nv);
+// el_g (NS) holds the primitive gradients [d][node][v].
+static double element_vector(const Ctx &c, const double *el_u, const double *el_g,
+                             double alpha, double *el_dudt)
+{
+    const int Np = c.Np, nv = c.nv, dim = c.dim, nd = c.ndof;
+    const int Npy = dim > 1 ? Np : 1, Npz = dim > 2 ? Np : 1;
+    double lam = -1.0;
+    for (int i = 0; i < nd * nv; i++) el_dudt[i] = 0.0;
+    if (c.p.blending) lam = std::max(lam, fv_fluxes(c, el_u, alpha, el_dudt));
+
+    // Contravariant viscous fluxes per node, per direction (NS only).
+    std::vector<double> Fv;  // [d][node][v]
+    if (c.p.parabolic) {
+        Fv.assign((size_t)dim * nd * nv, 0.0);
+        double flux[15], dq[15];
+        for (int n = 0; n < nd; n++) {
+            // The reference reads the state of its member id1 here
+            // (DGSEMIntegrator.cpp:620, :770), which ComputeFVFluxes (and the
+            // previous element's loops) leave at the element's last node.
+            int sn = c.p.compat ? nd - 1 : n;
+            for (int d = 0; d < dim; d++)
+                for (int v = 0; v < nv; v++) dq[d * nv + v] = el_g[((size_t)d * nd + n) * nv + v];
+            viscous_flux(dim, c.p.gamma, c.p.Pr, c.p.mu, el_u + sn * nv, dq, flux);
+            // MultABt(adj, flux): row a = sum_b adj(a,b) flux(:,b); adj diagonal.
+            for (int a = 0; a < dim; a++)
+                for (int v = 0; v < nv; v++) {
+                    double acc = 0.0;
+                    for (int b = 0; b < dim; b++) acc += (a == b ? c.adj[a] : 0.0) * flux[v * dim + b];
+                    Fv[((size_t)a * nd + n) * nv + v] = acc;
+                }
+        }
+    }
+
+    // Two-point fluxes: Fs[d][node][m][v] with column pos(node,d) zero.
+    std::vector<double> Fs((size_t)dim * nd * Np * nv, 0.0);
+    auto FS = [&](int d, int n, int m) -> double * { return &Fs[(((size_t)d * nd + n) * Np + m) * nv]; };
+    double f[5], g[5], h[5];
+    double metric[3] = {0, 0, 0}, metric_y[3] = {0, 0, 0}, metric_z[3] = {0, 0, 0};
+    metric[0] = c.adj[0];
+    if (dim > 1) metric_y[1] = c.adj[1];
+    if (dim > 2) metric_z[2] = c.adj[2];
+    for (int k = 0; k < Npz; k++)
+        for (int j = 0; j < Npy; j++)
+            for (int i = 0; i < Np; i++) {
+                int id1 = (k * Npy + j) * Np + i;
+                const double *s1 = el_u + id1 * nv;
+                for (int v = 0; v < nv; v++) f[v] = 0.0;
+                std::memcpy(FS(0, id1, i), f, sizeof(double) * nv);
+                for (int m = i + 1; m < Np; m++) {
+                    int id2 = (k * Npy + j) * Np + m;
+                    lam = std::max(lam, volume_flux(dim, c.p.gamma, s1, el_u + id2 * nv, metric, metric, f));
+                    std::memcpy(FS(0, id1, m), f, sizeof(double) * nv);
+                    std::memcpy(FS(0, id2, i), f, sizeof(double) * nv);
+                }
+                if (dim > 1) {
+                    for (int v = 0; v < nv; v++) g[v] = 0.0;
+                    std::memcpy(FS(1, id1, j), g, sizeof(double) * nv);
+                    for (int m = j + 1; m < Npy; m++) {
+                        int id2 = (k * Npy + m) * Np + i;
+                        lam = std::max(lam, volume_flux(dim, c.p.gamma, s1, el_u + id2 * nv, metric_y, metric_y, g));
+                        std::memcpy(FS(1, id1, m), g, sizeof(double) * nv);
+                        std::memcpy(FS(1, id2, j), g, sizeof(double) * nv);
+                    }
+                    if (dim > 2) {
+                        for (int v = 0; v < nv; v++) h[v] = 0.0;
+                        std::memcpy(FS(2, id1, k), h, sizeof(double) * nv);
+                        for (int m = k + 1; m < Npz; m++) {
+                            int id2 = (m * Npy + j) * Np + i;
+                            lam = std::max(lam, volume_flux(dim, c.p.gamma, s1, el_u + id2 * nv, metric_z, metric_z, h));
+                            std::memcpy(FS(2, id1, m), h, sizeof(double) * nv);
+                            // The NS 3D path fills the partner column with the
+                            // last y-direction flux `g` (DGSEMIntegrator.cpp:702).
+                            const double *fill = (c.p.parabolic && c.p.compat) ? g : h;
+                            std::memcpy(FS(2, id2, k), fill, sizeof(double) * nv);
+                        }
+                    }
+                }
+                // Flux differencing: dU = sum_d sum_m Dhat2(pos_d, m) F_d(:, m).
+                double dU[5], dUv[5];
+                int pos[3] = {i, j, k};
+                for (int v = 0; v < nv; v++) dU[v] = 0.0;
+                for (int d = 0; d < dim; d++)
+                    for (int m = 0; m < Np; m++) {
+                        const double *col = FS(d, id1, m);
+                        double a = c.Dhat2[pos[d] * Np + m];
+                        if (d == 0 && m == 0)
+                            for (int v = 0; v < nv; v++) dU[v] = a * col[v];
+                        else
+                            for (int v = 0; v < nv; v++) dU[v] += a * col[v];
+                    }
+                for (int v = 0; v < nv; v++) dUv[v] = 0.0;
+                if (c.p.parabolic) {
+                    for (int d = 0; d < dim; d++)
+                        for (int l = 0; l < Np; l++) {
+                            int nl = line_node(c, d, i, j, k, l);
+                            double a = c.Dhat[pos[d] * Np + l];
+                            for (int v = 0; v < nv; v++) {
+                                double t = Fv[((size_t)d * nd + nl) * nv + v];
+                                t *= a;
+                                dUv[v] += t;
+                            }
+                        }
+                }
+                for (int v = 0; v < nv; v++) {
+                    double t = -dU[v];
+                    if (c.p.blending) t *= (1.0 - alpha);
+                    if (c.p.parabolic) {
+                        t = t + dUv[v];
+                    }
+                    t /= c.J;
+                    el_dudt[id1 * nv + v] += t;
+                }
+            }
+    return lam;
+}
+
+// Face node list of face (d, side) of an element: node index of face node t.
+static inline int face_node(const Ctx &c, int d, int side, int t)
+{
+    const int Np = c.Np;
+    const int l = side ? Np - 1 : 0;
+    int a = t % Np, b = t / Np;  // tangential indices (fastest first)
+    if (c.dim == 2) b = 0;
+    if (d == 0) return (b * Np + a) * Np + l;
+    if (d == 1) return (b * Np + l) * Np + a;
+    return (l * Np + b) * Np + a;
+}
+
+// AssembleFaceVector, Euler (DGSEMIntegrator.cpp:151-222) and NS
+// (:435-494 3D, :496-549 2D) for the face between element a's +d face and its
+// neighbour b's -d face.  Writes contributions for both sides into buf:
+// buf[0][t][v] for a's face nodes, buf[1][t][v] for b's.
+static double face_vector(const Ctx &c, const double *u, const double *gr, int64_t a, int d,
+                          double *buf)
+{
+    const int nv = c.nv, dim = c.dim, nfn = c.ndof / c.Np;
+    const int64_t b = c.nbr[a * 2 * dim + 2 * d + 1];
+    const bool a_is_1 = a <= b;
+    const int64_t e1 = a_is_1 ? a : b, e2 = a_is_1 ? b : a;
+    const int side1 = a_is_1 ? 1 : 0, side2 = a_is_1 ? 0 : 1;
+    double nor[3] = {0, 0, 0};
+    nor[d] = a_is_1 ? c.area[d] : -c.area[d];
+    const double scale = 1.0 / (c.w[0] * c.J);
+    double lam = -1.0;
+    double s1[5], s2[5], flux[5], dU1[5], dU2[5];
+    double dq1[15], dq2[15], fm1[15], fm2[15];
+    for (int t = 0; t < nfn; t++) {
+        int n1 = face_node(c, d, side1, t), n2 = face_node(c, d, side2, t);
+        for (int v = 0; v < nv; v++) {
+            s1[v] = u[idx(c, v, e1, n1)];
+            s2[v] = u[idx(c, v, e2, n2)];
+        }
+        if (c.p.parabolic && c.p.compat) {
+            // The NS face integrators call ComputeViscousFlux(state1, ...)
+            // before ComputeFaceFlux(state1, state2, ...); its Conserv2Prim ->
+            // ComputePressure divides the momenta of state1/state2 in place
+            // (BasicOperations.cpp:33-34), so the Riemann flux receives
+            // velocities in the momentum slots (DGSEMIntegrator.cpp:467-481).
+            double t1[5], t2[5];
+            for (int v = 0; v < nv; v++) { t1[v] = s1[v]; t2[v] = s2[v]; }
+            for (int q = 0; q < dim; q++) { t1[1 + q] = s1[1 + q] / s1[0]; t2[1 + q] = s2[1 + q] / s2[0]; }
+            lam = std::max(lam, face_flux(dim, c.p.gamma, c.p.compat, c.p.face_dissipation, t1, t2, nor, flux));
+        } else {
+            lam = std::max(lam, face_flux(dim, c.p.gamma, c.p.compat, c.p.face_dissipation, s1, s2, nor, flux));
+        }
+        for (int v = 0; v < nv; v++) {
+            dU2[v] = flux[v];
+            dU1[v] = -flux[v];
+        }
+        if (c.p.parabolic) {
+            for (int q = 0; q < dim; q++)
+                for (int v = 0; v < nv; v++) {
+                    dq1[q * nv + v] = gr[(size_t)q * c.size + idx(c, v, e1, n1)];
+                    dq2[q * nv + v] = gr[(size_t)q * c.size + idx(c, v, e2, n2)];
+                }
+            viscous_flux(dim, c.p.gamma, c.p.Pr, c.p.mu, s1, dq1, fm1);
+            viscous_flux(dim, c.p.gamma, c.p.Pr, c.p.mu, s2, dq2, fm2);
+            for (int v = 0; v < nv; v++) {
+                double fn = 0.0;
+                for (int q = 0; q < dim; q++) {
+                    double avg = fm1[v * dim + q];
+                    avg += fm2[v * dim + q];
+                    avg *= 0.5;
+                    fn += avg * nor[q];
+                }
+                dU1[v] += fn;
+                dU2[v] -= fn;
+            }
+        }
+        // AddMult_a_VWt(1/(w0 J), shape, dU): entry += (a * dU_v) * 1.
+        double *ba = buf + (size_t)(a_is_1 ? 0 : 1) * nfn * nv;
+        double *bb = buf + (size_t)(a_is_1 ? 1 : 0) * nfn * nv;
+        for (int v = 0; v < nv; v++) {
+            ba[t * nv + v] = scale * dU1[v];
+            bb[t * nv + v] = scale * dU2[v];
+        }
+    }
+    return lam;
+}
+
+// ---------------------------------------------------------------------------
+// BR1 lifting (LiftingBR1.cpp:10-115, 156-272; DGSEMNonlinearForm.cpp:213-645)
+// and ComputeGlobalPrimitiveGradVector (DGSEMOperator.cpp:96-159).
+// ---------------------------------------------------------------------------
+static void lifting(Ctx &c, const double *u)
+{
+    const int nv = c.nv, dim = c.dim, nd = c.ndof, Np = c.Np, nfn = nd / Np;
+    const int Npy = dim > 1 ? Np : 1, Npz = dim > 2 ? Np : 1;
+    // ComputeGlobalEntropyVector (DGSEMOperator.cpp:82-94).
+#pragma omp parallel for schedule(static)
+    for (int64_t e = 0; e < c.ne; e++) {
+        double s[5], w[5];
+        for (int n = 0; n < nd; n++) {
+            for (int v = 0; v < nv; v++) s[v] = u[idx(c, v, e, n)];
+            conserv2entropy(dim, c.p.gamma, s, w);
+            for (int v = 0; v < nv; v++) c.went[idx(c, v, e, n)] = w[v];
+        }
+    }
+    const double *W = c.went.data();
+    double *G = c.grads.data();
+    const double invJ = 1.0 / c.J;
+    const double scale = 1.0 / (c.w[0] * c.J);
+#pragma omp parallel for schedule(static)
+    for (int64_t e = 0; e < c.ne; e++) {
+        // Element part: strong-form derivative, * adj / J.
+        for (int k = 0; k < Npz; k++)
+            for (int j = 0; j < Npy; j++)
+                for (int i = 0; i < Np; i++) {
+                    int id = (k * Npy + j) * Np + i;
+                    int pos[3] = {i, j, k};
+                    for (int d = 0; d < dim; d++)
+                        for (int v = 0; v < nv; v++) {
+                            double acc = 0.0;
+                            for (int l = 0; l < Np; l++) {
+                                double t = W[idx(c, v, e, line_node(c, d, i, j, k, l))];
+                                t *= c.D[pos[d] * Np + l];
+                                acc += t;
+                            }
+                            // grad_mat1 * adj (diagonal), then * (1/J)
+                            double g = acc * c.adj[d];
+                            g *= invJ;
+                            G[(size_t)d * c.size + idx(c, v, e, id)] = g;
+                        }
+                }
+        // Face parts: each face adds 0.5*(w2 - w1)*n_d/(w0 J) to both sides.
+        for (int d = 0; d < dim; d++)
+            for (int side = 0; side < 2; side++) {
+                int64_t nb = c.nbr[e * 2 * dim + 2 * d + side];
+                // The face between (e, side) and nb: element 1 rule.
+                int64_t a = side ? e : nb;  // element on the -d side of the face
+                int64_t bb = side ? nb : e;
+                bool a_is_1 = a <= bb;
+                int64_t e1 = a_is_1 ? a : bb, e2 = a_is_1 ? bb : a;
+                int side1 = a_is_1 ? 1 : 0, side2 = a_is_1 ? 0 : 1;
+                double nd_ = a_is_1 ? c.area[d] : -c.area[d];
+                bool me_is_1 = (e == e1) && !(e1 == e2 && side != side1);
+                for (int t = 0; t < nfn; t++) {
+                    int n1 = face_node(c, d, side1, t), n2 = face_node(c, d, side2, t);
+                    int nme = me_is_1 ? n1 : n2;
+                    for (int v = 0; v < nv; v++) {
+                        double fval = 0.5 * (W[idx(c, v, e2, n2)] - W[idx(c, v, e1, n1)]);
+                        fval *= nd_;
+                        G[(size_t)d * c.size + idx(c, v, e, nme)] += scale * fval;
+                    }
+                }
+            }
+        // EntropyGrad2PrimGrad per node, per direction.
+        double s[5], g[5];
+        for (int n = 0; n < nd; n++) {
+            for (int v = 0; v < nv; v++) s[v] = u[idx(c, v, e, n)];
+            for (int d = 0; d < dim; d++) {
+                for (int v = 0; v < nv; v++) g[v] = G[(size_t)d * c.size + idx(c, v, e, n)];
+                entgrad2primgrad(dim, c.p.gamma, c.p.compat, s, g);
+                for (int v = 0; v < nv; v++) G[(size_t)d * c.size + idx(c, v, e, n)] = g[v];
+            }
+        }
+    }
+}
+
+// DGSEMOperator::Mult (DGSEMOperator.cpp:537-591) with the loops of
+// DGSEMNonlinearForm::Mult (DGSEMNonlinearForm.cpp:647-849, 1302-1548).
+static void rhs(Ctx &c, const double *u, double *dudt)
+{
+    const int nv = c.nv, dim = c.dim, nd = c.ndof, Np = c.Np, nfn = nd / Np;
+    if (c.p.blending) blending_coefficient(c, u);
+    else {
+        std::fill(c.alpha.begin(), c.alpha.end(), 0.0);
+        std::fill(c.eta.begin(), c.eta.end(), 0.0);
+    }
+    if (c.p.parabolic) lifting(c, u);
+    const double *G = c.grads.data();
+    double lam = -1.0;
+    // Face contributions first into a per-face buffer (both sides).
+    const size_t fstride = (size_t)2 * nfn * nv;
+#pragma omp parallel for schedule(static) reduction(max : lam)
+    for (int64_t e = 0; e < c.ne; e++)
+        for (int d = 0; d < dim; d++)
+            lam = std::max(lam, face_vector(c, u, G, e, d, &c.facebuf[((size_t)e * dim + d) * fstride]));
+#pragma omp parallel for schedule(static) reduction(max : lam)
+    for (int64_t e = 0; e < c.ne; e++) {
+        std::vector<double> el_u(nd * nv), el_d(nd * nv), el_g;
+        for (int n = 0; n < nd; n++)
+            for (int v = 0; v < nv; v++) el_u[n * nv + v] = u[idx(c, v, e, n)];
+        if (c.p.parabolic) {
+            el_g.resize((size_t)dim * nd * nv);
+            for (int d = 0; d < dim; d++)
+                for (int n = 0; n < nd; n++)
+                    for (int v = 0; v < nv; v++)
+                        el_g[((size_t)d * nd + n) * nv + v] = G[(size_t)d * c.size + idx(c, v, e, n)];
+        }
+        lam = std::max(lam, element_vector(c, el_u.data(), el_g.data(), c.alpha[e], el_d.data()));
+        // dudt = 0 + element vector + face vectors (faces in -x,+x,-y,+y,-z,+z order).
+        for (int n = 0; n < nd; n++)
+            for (int v = 0; v < nv; v++) dudt[idx(c, v, e, n)] = 0.0 + el_d[n * nv + v];
+        for (int d = 0; d < dim; d++) {
+            // -d face: stored at (nbr_minus, d); this element is its "b" side.
+            int64_t em = c.nbr[e * 2 * dim + 2 * d];
+            const double *bm = &c.facebuf[((size_t)em * dim + d) * fstride];
+            const double *mine = bm + (size_t)nfn * nv;
+            for (int t = 0; t < nfn; t++) {
+                int n = face_node(c, d, 0, t);
+                for (int v = 0; v < nv; v++) dudt[idx(c, v, e, n)] += mine[t * nv + v];
+            }
+            // +d face: stored at (e, d); this element is its "a" side.
+            const double *mine2 = &c.facebuf[((size_t)e * dim + d) * fstride];
+            for (int t = 0; t < nfn; t++) {
+                int n = face_node(c, d, 1, t);
+                for (int v = 0; v < nv; v++) dudt[idx(c, v, e, n)] += mine2[t * nv + v];
+            }
+        }
+    }
+    c.last_rhs_speed = lam;
+    c.max_char_speed = std::max(c.max_char_speed, lam);
+}
+
+// ---------------------------------------------------------------------------
+// Entropy filter, built from the intent of src/Filters/EntropyFilter.cpp
+// (GetEntropyConstraints :81-158, FilterSolution :171-242, ComputeRoot
+// :325-349): per-element bound = min of rho*log(p rho^-gamma) over the element
+// and its face neighbours at the stage input; an element with min rho < 1e-8,
+// min p < 1e-8 or min entropy < bound - 1e-4 has its modes of max degree j
+// scaled by exp(-zeta j^2), zeta found by 20 bisection steps per violating
+// node on [zeta, -ln 1e-10], visiting nodes in order.
+// ---------------------------------------------------------------------------
+static void filter_bounds(Ctx &c, const double *u)
+{
+    const int nv = c.nv, nd = c.ndof, dim = c.dim;
+    std::vector<double> own(c.ne);
+#pragma omp parallel for schedule(static)
+    for (int64_t e = 0; e < c.ne; e++) {
+        double mn = std::numeric_limits<double>::infinity(), s[5];
+        for (int n = 0; n < nd; n++) {
+            for (int v = 0; v < nv; v++) s[v] = u[idx(c, v, e, n)];
+            double rho = s[0], p = pressure(dim, c.p.gamma, s);
+            mn = std::min(mn, entropy_fn(rho, p, c.p.gamma));
+        }
+        own[e] = mn;
+    }
+#pragma omp parallel for schedule(static)
+    for (int64_t e = 0; e < c.ne; e++) {
+        double mn = own[e];
+        for (int f = 0; f < 2 * dim; f++) mn = std::min(mn, own[c.nbr[e * 2 * dim + f]]);
+        c.emin[e] = mn;
+    }
+}
+
+static void filter_apply(Ctx &c, double *x)
+{
+    const int nv = c.nv, nd = c.ndof, dim = c.dim, Np = c.Np;
+    const double rho_min = 1e-8, p_min = 1e-8, ent_tol = 1e-4, epsilon = 1e-10;
+    const int N_iter = 20;
+    int64_t nf = 0;
+#pragma omp parallel for schedule(dynamic, 16) reduction(+ : nf)
+    for (int64_t e = 0; e < c.ne; e++) {
+        double s[5];
+        double mr = std::numeric_limits<double>::infinity(), mp = mr, me = mr;
+        for (int n = 0; n < nd; n++) {
+            for (int v = 0; v < nv; v++) s[v] = x[idx(c, v, e, n)];
+            double rho = s[0], p = pressure(dim, c.p.gamma, s);
+            me = std::min(me, entropy_fn(rho, p, c.p.gamma));
+            mr = std::min(mr, rho);
+            mp = std::min(mp, p);
+        }
+        const double bound = c.emin[e];
+        if (!(mr < rho_min || mp < p_min || me < bound - ent_tol)) continue;
+        nf++;
+        std::vector<double> modes((size_t)nd * nv, 0.0), hs((size_t)Np * nv);
+        for (int v = 0; v < nv; v++)
+            for (int r = 0; r < nd; r++) {
+                double acc = 0.0;
+                for (int k = 0; k < nd; k++) acc += c.Vinv[r * nd + k] * x[idx(c, v, e, k)];
+                modes[(size_t)r * nv + v] = acc;
+            }
+        auto violates = [&](const double *st) {
+            double rho = st[0], p = pressure(dim, c.p.gamma, st);
+            double en = entropy_fn(rho, p, c.p.gamma);
+            return rho < rho_min || p < p_min || en < bound - ent_tol;
+        };
+        auto filter_modes = [&](double zeta, double *st) {  // FilterModes :160-169
+            for (int v = 0; v < nv; v++) st[v] = hs[v];
+            for (int j = 1; j < Np; j++) {
+                double fac = std::exp(-zeta * std::pow(j, 2));
+                for (int v = 0; v < nv; v++) st[v] += hs[(size_t)j * nv + v] * fac;
+            }
+        };
+        double zeta = 0.0;
+        for (int i = 0; i < nd; i++) {
+            std::fill(hs.begin(), hs.end(), 0.0);  // ComputeHierarchStates :244-260
+            for (int j = 0; j < Np; j++)
+                for (int v = 0; v < nv; v++)
+                    for (int l = 0; l < nd; l++)
+                        if (c.max_order[l] == j) hs[(size_t)j * nv + v] += c.Vdm[i * nd + l] * modes[(size_t)l * nv + v];
+            filter_modes(zeta, s);
+            if (violates(s)) {  // ComputeRoot :325-349
+                double z1 = zeta, z2 = -std::log(epsilon);
+                for (int it = 0; it < N_iter; it++) {
+                    double z3 = 0.5 * (z1 + z2);
+                    filter_modes(z3, s);
+                    if (violates(s)) z1 = z3;
+                    else z2 = z3;
+                }
+                zeta = z2;
+            }
+        }
+        std::vector<double> ffac(Np, 1.0);
+        for (int d = 1; d < Np; d++) ffac[d] = std::exp(-zeta * std::pow(d, 2));
+        for (int i = 0; i < nd; i++)
+            for (int v = 0; v < nv; v++) {
+                double tmp = 0.0;
+                for (int j = 0; j < Np; j++)
+                    for (int l = 0; l < nd; l++)
+                        if (c.max_order[l] == j) tmp += ffac[j] * c.Vdm[i * nd + l] * modes[(size_t)l * nv + v];
+                x[idx(c, v, e, i)] = tmp;
+            }
+    }
+    c.filtered_elements += nf;
+}
+
+// RK3SSPSolver::Step (Shu-Osher SSP-RK3), optionally filtering each stage.
+static void rk3_step(Ctx &c, double dt, double *x)
+{
+    const int64_t n = c.size;
+    double *k = c.k1.data(), *y = c.y1.data(), *z = c.z1.data();
+    if (c.p.filter) filter_bounds(c, x);
+    rhs(c, x, k);
+#pragma omp parallel for schedule(static)
+    for (int64_t i = 0; i < n; i++) y[i] = x[i] + dt * k[i];
+    if (c.p.filter) { filter_apply(c, y); filter_bounds(c, y); }
+    rhs(c, y, k);
+#pragma omp parallel for schedule(static)
+    for (int64_t i = 0; i < n; i++) {
+        z[i] = y[i] + dt * k[i];
+        y[i] = 3. / 4 * x[i] + 1. / 4 * z[i];
+    }
+    if (c.p.filter) { filter_apply(c, y); filter_bounds(c, y); }
+    rhs(c, y, k);
+#pragma omp parallel for schedule(static)
+    for (int64_t i = 0; i < n; i++) {
+        z[i] = y[i] + dt * k[i];
+        x[i] = 1. / 3 * x[i] + 2. / 3 * z[i];
+    }
+    if (c.p.filter) filter_apply(c, x);
+}
+
+}  // namespace orc
+
+// ---------------------------------------------------------------------------
+// C interface (used only by tests/, smoke() and bench.py's CPU baseline)
+// ---------------------------------------------------------------------------
+using orc::Ctx;
+
+extern "C" {
+
+void *orc_create(const pdg_mesh *m, const pdg_params *p)
+{
+    if (!m || !p || (m->dim != 2 && m->dim != 3) || m->order < 1 || m->num_elements < 1) return nullptr;
+    Ctx *c = new Ctx();
+    c->p = *p;
+    c->dim = m->dim;
+    c->N = m->order;
+    c->Np = m->order + 1;
+    c->ndof = 1;
+    for (int d = 0; d < c->dim; d++) c->ndof *= c->Np;
+    c->nv = c->dim + 2;
+    c->ne = m->num_elements;
+    c->nnodes = c->ne * c->ndof;
+    c->size = c->nnodes * c->nv;
+    for (int d = 0; d < 3; d++) c->h[d] = d < c->dim ? m->h[d] : 1.0;
+    c->nbr.assign(m->nbr, m->nbr + (size_t)c->ne * 2 * c->dim);
+    orc::gll(c->Np, c->x, c->w);
+    orc::build_derivative_matrices(*c);
+    if (c->dim == 2) {
+        c->J = c->h[0] * c->h[1];
+        c->adj[0] = c->h[1];
+        c->adj[1] = c->h[0];
+        c->area[0] = c->h[1];
+        c->area[1] = c->h[0];
+    } else {
+        c->J = c->h[0] * (c->h[1] * c->h[2]);
+        c->adj[0] = c->h[1] * c->h[2];
+        c->adj[1] = c->h[0] * c->h[2];
+        c->adj[2] = c->h[0] * c->h[1];
+        c->area[0] = c->h[1] * c->h[2];
+        c->area[1] = c->h[0] * c->h[2];
+        c->area[2] = c->h[0] * c->h[1];
+    }
+    orc::build_subcell_normals(*c);
+    orc::build_modal(*c);
+    c->modalThreshold = 0.5 * std::pow(10.0, -1.8 * std::pow(c->N, 0.25));
+    c->eta.assign(c->ne, 0.0);
+    c->alpha.assign(c->ne, 0.0);
+    if (c->p.parabolic) {
+        c->grads.assign((size_t)c->dim * c->size, 0.0);
+        c->went.assign(c->size, 0.0);
+    }
+    c->facebuf.assign((size_t)c->ne * c->dim * 2 * (c->ndof / c->Np) * c->nv, 0.0);
+    c->emin.assign(c->ne, std::numeric_limits<double>::infinity());
+    c->k1.assign(c->size, 0.0);
+    c->y1.assign(c->size, 0.0);
+    c->z1.assign(c->size, 0.0);
+    c->max_char_speed = -1.0;
+    c->last_rhs_speed = -1.0;
+    c->filtered_elements = 0;
+    return c;
+}
+
+void orc_destroy(void *h) { delete (Ctx *)h; }
+
+void orc_rhs(void *h, const double *u, double *dudt) { orc::rhs(*(Ctx *)h, u, dudt); }
+
+void orc_rk3_step(void *h, double dt, double *u) { orc::rk3_step(*(Ctx *)h, dt, u); }
+
+double orc_max_char_speed(void *h)
+{
+    Ctx *c = (Ctx *)h;
+    return c->p.compat ? c->max_char_speed : c->last_rhs_speed;
+}
+
+void orc_get_blending(void *h, double *eta, double *alpha)
+{
+    Ctx *c = (Ctx *)h;
+    if (eta) std::memcpy(eta, c->eta.data(), sizeof(double) * c->ne);
+    if (alpha) std::memcpy(alpha, c->alpha.data(), sizeof(double) * c->ne);
+}
+
+void orc_get_gradients(void *h, double *g)
+{
+    Ctx *c = (Ctx *)h;
+    if (c->p.parabolic) std::memcpy(g, c->grads.data(), sizeof(double) * c->grads.size());
+}
+
+int64_t orc_filtered_elements(void *h) { return ((Ctx *)h)->filtered_elements; }
+
+void orc_filter_bounds(void *h, const double *u) { orc::filter_bounds(*(Ctx *)h, u); }
+void orc_filter_apply(void *h, double *u) { orc::filter_apply(*(Ctx *)h, u); }
+
+// Stage update of pdg_rk_stage: uout = a*un + b*(us + dt*L(us)).
+void orc_rk_stage(void *h, int stage, double dt, const double *un, const double *us, double *uout)
+{
+    Ctx *c = (Ctx *)h;
+    if (c->p.filter) orc::filter_bounds(*c, us);
+    orc::rhs(*c, us, c->k1.data());
+    const double *k = c->k1.data();
+#pragma omp parallel for schedule(static)
+    for (int64_t i = 0; i < c->size; i++) {
+        double z = us[i] + dt * k[i];
+        if (stage == 0) uout[i] = z;
+        else if (stage == 1) uout[i] = 3. / 4 * un[i] + 1. / 4 * z;
+        else uout[i] = 1. / 3 * un[i] + 2. / 3 * z;
+    }
+    if (c->p.filter) orc::filter_apply(*c, uout);
+}
+
+void orc_gll(int Np, double *x, double *w)
+{
+    std::vector<double> xx, ww;
+    orc::gll(Np, xx, ww);
+    std::memcpy(x, xx.data(), sizeof(double) * Np);
+    std::memcpy(w, ww.data(), sizeof(double) * Np);
+}
+
+void orc_derivative_matrices(int Np, double *D, double *Dhat, double *Dhat2)
+{
+    Ctx c;
+    c.Np = Np;
+    orc::gll(Np, c.x, c.w);
+    orc::build_derivative_matrices(c);
+    std::memcpy(D, c.D.data(), sizeof(double) * Np * Np);
+    std::memcpy(Dhat, c.Dhat.data(), sizeof(double) * Np * Np);
+    std::memcpy(Dhat2, c.Dhat2.data(), sizeof(double) * Np * Np);
+}
+
+double orc_logmean(double x, double y) { return orc::logmean(x, y); }
+
+double orc_volume_flux(int dim, double gamma, const double *s1, const double *s2, const double *m1,
+                       const double *m2, double *F)
+{
+    return orc::volume_flux(dim, gamma, s1, s2, m1, m2, F);
+}
+
+double orc_face_flux(int dim, double gamma, int compat, const double *s1, const double *s2,
+                     const double *nor, double *F)
+{
+    return orc::face_flux(dim, gamma, compat, 1.0, s1, s2, nor, F);
+}
+
+void orc_viscous_flux(int dim, double gamma, double Pr, double mu, const double *state, const double *dq,
+                      double *flux)
+{
+    orc::viscous_flux(dim, gamma, Pr, mu, state, dq, flux);
+}
+
+void orc_conserv2entropy(int dim, double gamma, const double *state, double *w)
+{
+    orc::conserv2entropy(dim, gamma, state, w);
+}
+
+void orc_entgrad2primgrad(int dim, double gamma, int compat, const double *state, double *g)
+{
+    orc::entgrad2primgrad(dim, gamma, compat, state, g);
+}
+
+int orc_num_threads(void)
+{
+#ifdef _OPENMP
+    return omp_get_max_threads();
+#else
+    return 1;
+#endif
+}
+
+void orc_set_num_threads(int n)
+{
+#ifdef _OPENMP
+    if (n > 0) omp_set_num_threads(n);
+#else
+    (void)n;
+#endif
+}
+
+}  // extern "C"

@@ -1,0 +1,143 @@
+"""Periodic Cartesian meshes in the layout the C ABI expects.
+
+The reference builds its meshes with MFEM (src/Simulation/Simulation.cpp:271-336)
+and numbers DG nodes element by element, lexicographically inside an element
+(x fastest), with every field stored byNODES (Simulation.hpp:64).  Here a mesh
+is an axis-aligned box split into n^dim equal elements, numbered x fastest,
+with a face-neighbour table nbr[e, f], f = (-x, +x, -y, +y, -z, +z), wrapping
+periodically.
+"""
+from __future__ import annotations
+
+from dataclasses import dataclass
+
+import numpy as np
+
+
+def gll_nodes(Np: int) -> tuple[np.ndarray, np.ndarray]:
+    """Gauss-Lobatto nodes and weights on [0, 1] (Np points).
+
+    Interior nodes are roots of P_N' found by Newton's method in extended
+    precision; weights are 1/(N(N+1) P_N(x)^2); the rule is mirrored about 1/2.
+    """
+    N = Np - 1
+    x = np.zeros(Np)
+    w = np.zeros(Np)
+    for i in range(N // 2 + 1):
+        if i == 0:
+            t = np.longdouble(-1.0)
+        else:
+            t = -np.cos(np.longdouble(np.pi) * i / N)
+            for _ in range(100):
+                P, dP = _legendre(N, t)
+                d2P = (2 * t * dP - N * (N + 1) * P) / (1 - t * t)
+                dt = dP / d2P
+                t = t - dt
+                if abs(dt) < 1e-30:
+                    break
+        P, _ = _legendre(N, t)
+        x[i] = float(0.5 * (1 + t))
+        w[i] = float(1 / (N * (N + 1) * P * P))
+        x[N - i] = 1.0 - x[i]
+        w[N - i] = w[i]
+    if N % 2 == 0:
+        x[N // 2] = 0.5
+    return x, w
+
+
+def _legendre(n, t):
+    p0, p1 = np.longdouble(1), t
+    if n == 0:
+        return np.longdouble(1), np.longdouble(0)
+    for k in range(1, n):
+        p0, p1 = p1, ((2 * k + 1) * t * p1 - k * p0) / (k + 1)
+    if abs(t) == 1:
+        return p1, np.longdouble(0)  # derivative unused at the end points
+    return p1, n * (t * p1 - p0) / (t * t - 1)
+
+
+@dataclass
+class CartesianMesh:
+    dim: int
+    order: int
+    n: tuple[int, ...]          # elements per direction
+    lo: tuple[float, ...]
+    hi: tuple[float, ...]
+    nbr: np.ndarray             # (ne, 2*dim) int32
+
+    @property
+    def Np(self) -> int:
+        return self.order + 1
+
+    @property
+    def ndof(self) -> int:
+        return self.Np ** self.dim
+
+    @property
+    def num_elements(self) -> int:
+        return int(np.prod(self.n))
+
+    @property
+    def num_nodes(self) -> int:
+        return self.num_elements * self.ndof
+
+    @property
+    def nv(self) -> int:
+        return self.dim + 2
+
+    @property
+    def size(self) -> int:
+        return self.num_nodes * self.nv
+
+    @property
+    def h(self) -> tuple[float, ...]:
+        return tuple((self.hi[d] - self.lo[d]) / self.n[d] for d in range(self.dim))
+
+    def node_coords(self) -> np.ndarray:
+        """Physical coordinates, shape (dim, num_nodes), in the byNODES order."""
+        x1, _ = gll_nodes(self.Np)
+        Np, dim = self.Np, self.dim
+        ne = self.num_elements
+        e = np.arange(ne)
+        eidx = []
+        r = e.copy()
+        for d in range(dim):
+            eidx.append(r % self.n[d])
+            r //= self.n[d]
+        loc = np.arange(self.ndof)
+        lidx = []
+        r = loc.copy()
+        for d in range(dim):
+            lidx.append(r % Np)
+            r //= Np
+        h = self.h
+        out = np.empty((dim, ne * self.ndof))
+        for d in range(dim):
+            c = self.lo[d] + (eidx[d][:, None] + x1[lidx[d]][None, :]) * h[d]
+            out[d] = c.reshape(-1)
+        return out
+
+
+def periodic_box(dim: int, order: int, n, lo, hi) -> CartesianMesh:
+    """Periodic box [lo, hi] split into n[d] elements per direction."""
+    if np.isscalar(n):
+        n = (int(n),) * dim
+    n = tuple(int(v) for v in n)
+    if np.isscalar(lo):
+        lo = (float(lo),) * dim
+    if np.isscalar(hi):
+        hi = (float(hi),) * dim
+    ne = int(np.prod(n))
+    e = np.arange(ne)
+    idx = []
+    r = e.copy()
+    for d in range(dim):
+        idx.append(r % n[d])
+        r //= n[d]
+    strides = [int(np.prod(n[:d])) for d in range(dim)]
+    nbr = np.empty((ne, 2 * dim), dtype=np.int32)
+    for d in range(dim):
+        base = e - idx[d] * strides[d]
+        nbr[:, 2 * d] = base + ((idx[d] - 1) % n[d]) * strides[d]
+        nbr[:, 2 * d + 1] = base + ((idx[d] + 1) % n[d]) * strides[d]
+    return CartesianMesh(dim, order, n, tuple(lo), tuple(hi), nbr)
