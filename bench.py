@@ -1,0 +1,325 @@
+"""Benchmark: DOF-stage updates per second of the DGSEM RHS + SSP-RK3 stage.
+
+Workload (default): 3D Taylor-Green vortex, Navier-Stokes with BR1 lifting and
+subcell-FV blending, periodic [0, 2pi]^3 with 32^3 hexes, N = 3 (64 nodes per
+element, 10,485,760 vdofs), Re = 1600, Ma = 0.1, Pr = 0.71, SSP-RK3.  A "step"
+is one SSP-RK3 step (three fused stages, each a lifting kernel and an RHS +
+stage kernel).  Metric = vdofs x stages / time.  Inputs are synthetic (the
+reference's TGV initial condition and mesh are unusable) and the per-step
+working set (state, two stage buffers, three gradient fields: ~0.5 GB) is
+larger than the 126 MB L2, so no L2 flush is needed between steps.
+
+Usage:  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+For N > 1 run under torchrun; each rank advances its own replica (weak scaling).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+from prandtl_b200 import cases  # noqa: E402
+from prandtl_b200.mesh import periodic_box  # noqa: E402
+
+METRIC = "DOF-stage updates/s on 1 B200 (plain vs batched+graph); adjoint/forward cost"
+UNIT = "DOF-stage updates/s"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--n", type=int, default=32, help="elements per direction (32 = the benchmark workload)")
+    ap.add_argument("--order", type=int, default=3)
+    ap.add_argument("--e2e-steps", type=int, default=5)
+    ap.add_argument("--cpu-seconds", type=float, default=12.0)
+    ap.add_argument("--no-cpu", action="store_true")
+    return ap.parse_args()
+
+
+def workload(n, order):
+    mesh = periodic_box(3, order, n, 0.0, 2 * np.pi)
+    u = cases.taylor_green(mesh)
+    params = dict(parabolic=1, blending=1, compat=1, mu=1.0 / 1600.0, Pr=0.71, gamma=1.4)
+    return mesh, u, params
+
+
+def config_dict(mesh, n_gpus):
+    return {"workload": f"taylor_green_3d_{mesh.n[0]}^3_N{mesh.order}_navier_stokes_br1_blending_ssprk3",
+            "elements": mesh.num_elements, "order": mesh.order, "nodes_per_element": mesh.ndof,
+            "vdofs": mesh.size, "stages_per_step": 3, "compat": 1,
+            "l2": "working set per step ~0.5 GB > 126 MB L2 (no flush needed)",
+            "parallelism": f"replicas x{n_gpus}" if n_gpus > 1 else "single GPU"}
+
+
+class ClockSampler:
+    """nvidia-smi clocks/throttle reasons sampled every 200 ms while running."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index=0):
+        self.dev = device_index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        try:
+            fd, self.path = tempfile.mkstemp(suffix=".csv")
+            os.close(fd)
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.dev}", f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        rows = []
+        for line in open(self.path):
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) >= 9:
+                rows.append(parts)
+        os.unlink(self.path)
+        if not rows:
+            return None
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].lower().startswith("active")})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+def measured_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        j = json.load(open(p))
+        return float(j["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def cpu_baseline(mesh, u, params, seconds):
+    """The oracle (C++ restatement, OpenMP over elements) on the host cores."""
+    import oracle
+    cores = oracle.lib().orc_num_threads()
+    o = oracle.Oracle(mesh, **params)
+    o.rhs(u)
+    dt = 0.5 * min(mesh.h) / (o.max_char_speed() * (mesh.order + 1) ** 2)
+    x = u.copy()
+    steps = 0
+    t0 = time.perf_counter()
+    while True:
+        x = o.rk3_step(x, dt)
+        steps += 1
+        el = time.perf_counter() - t0
+        if el >= seconds or steps >= 50:
+            break
+    return {"value": mesh.size * 3 * steps / el, "unit": UNIT, "cores": cores, "kind": "port",
+            "sample": f"{steps} SSP-RK3 steps of the full workload ({el:.1f} s, OpenMP over elements)"}
+
+
+def run_ours(args):
+    import torch
+    import torch.distributed as dist
+
+    import prandtl_b200 as pb
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        torch.cuda.set_device(local)
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120))
+    dev = torch.device("cuda", local if world > 1 else 0)
+    torch.cuda.set_device(dev)
+    mesh, u0, params = workload(args.n, args.order)
+    op = pb.DGSEMOperator(mesh, **params)
+    x = torch.from_numpy(u0).to(dev)
+    tmp = torch.empty_like(x)
+    op.Mult(x, tmp)
+    dt = op.cfl_dt(0.5)
+    for _ in range(args.warmup):
+        op.rk3_step(x, dt)
+    torch.cuda.synchronize()
+    op.check()
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    sampler = ClockSampler(dev.index or 0)
+    op.profile(True)
+    op.profile_read(pb.KERNEL_LIFT)
+    op.profile_read(pb.KERNEL_NS)
+    launches0 = op.launch_count()
+    barrier()
+    torch.cuda.synchronize()
+    sampler.start()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record()
+    for _ in range(args.steps):
+        op.rk3_step(x, dt)
+    ev1.record()
+    torch.cuda.synchronize()
+    barrier()
+    clocks = sampler.stop()
+    ms = ev0.elapsed_time(ev1)
+    launches = op.launch_count() - launches0
+    ns_ms, ns_n = op.profile_read(pb.KERNEL_NS)
+    lift_ms, lift_n = op.profile_read(pb.KERNEL_LIFT)
+    op.profile(False)
+    op.check()
+    if world > 1:
+        t = torch.tensor([ms], device=dev, dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    V = mesh.size
+    value = V * 3 * args.steps * world / (ms * 1e-3)
+
+    # end to end through the host-buffer step: H2D + 3 stages + D2H per step
+    host = torch.from_numpy(x.cpu().numpy()).pin_memory().numpy()
+    op.rk3_step_host(host, dt)
+    barrier()
+    t0 = time.perf_counter()
+    for _ in range(args.e2e_steps):
+        op.rk3_step_host(host, dt)
+    e2e_s = time.perf_counter() - t0
+    if world > 1:
+        t = torch.tensor([e2e_s], device=dev, dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_s = float(t.item())
+    e2e = {"value": V * 3 * args.e2e_steps * world / e2e_s, "unit": UNIT,
+           "h2d_bytes_per_step": 8 * V, "d2h_bytes_per_step": 8 * V,
+           "path": "pdg_rk3_step_host (pinned host state in, 3 fused stages, state out)"}
+
+    peak, peak_kind = measured_peaks()
+    # algorithmic bytes of the NS RHS + stage kernel per launch: reads u (8 B),
+    # 3 gradient fields (24 B), un on stages 1-2 (8 B), writes the stage (8 B)
+    ns_bytes = V * (8 + 24 + 8) + V * 8 * (2.0 / 3.0)
+    lift_bytes = V * (8 + 24)
+    ns_avg = ns_ms / max(ns_n, 1)
+    lift_avg = lift_ms / max(lift_n, 1)
+    ns_gbs = ns_bytes / (ns_avg * 1e-3) / 1e9
+    lift_gbs = lift_bytes / (lift_avg * 1e-3) / 1e9
+    step_gbs = (3 * lift_bytes + 3 * ns_bytes) / (ms / args.steps * 1e-3) / 1e9
+    traffic = None
+    tf = os.path.join(ROOT, "profiles", "traffic.json")
+    if os.path.exists(tf):
+        traffic = json.load(open(tf)).get("ns_rhs_kernel_bytes_per_launch")
+    roofline = {"bound": "hbm", "kernel": "ns_rhs_kernel<3,3>", "achieved": ns_gbs, "peak": peak, "unit": "GB/s",
+                "frac": ns_gbs / peak, "traffic": traffic, "peak_kind": peak_kind,
+                "algorithmic_bytes_per_launch": ns_bytes, "avg_launch_ms": ns_avg,
+                "lift_kernel": {"achieved": lift_gbs, "frac": lift_gbs / peak, "avg_launch_ms": lift_avg,
+                                "algorithmic_bytes_per_launch": lift_bytes},
+                "whole_step": {"achieved": step_gbs, "frac": step_gbs / peak, "bytes_per_vdof": 232}}
+    out = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+           "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
+           "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+           "config": config_dict(mesh, world), "e2e": e2e, "gpu_launches": launches,
+           "roofline": roofline, "clocks": clocks}
+    if rank == 0 and world == 1 and not args.no_cpu:
+        out["cpu_baseline"] = cpu_baseline(mesh, u0, params, args.cpu_seconds)
+    if rank == 0:
+        print(json.dumps(out), flush=True)
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def _ref_worker(payload):
+    """One reference process: SSP-RK3 steps of its own TGV block, timed."""
+    n_el, order, steps, seconds = payload
+    sys.path.insert(0, ROOT)
+    import oracle as orc
+    mesh = periodic_box(3, order, (32, 32, n_el), 0.0, 2 * np.pi)
+    u = cases.taylor_green(mesh)
+    r = orc.Reference(mesh, parabolic=True, mu=1.0 / 1600.0, Pr=0.71)
+    k = r.rhs(u)
+    dt = 0.5 * min(mesh.h) / (r.lam * (order + 1) ** 2)
+    done = 0
+    t0 = time.perf_counter()
+    while done < steps:
+        k = r.rhs(u)
+        y = u + dt * k
+        k = r.rhs(y)
+        y = 0.75 * u + 0.25 * (y + dt * k)
+        k = r.rhs(y)
+        u = 1.0 / 3.0 * u + 2.0 / 3.0 * (y + dt * k)
+        done += 1
+        if time.perf_counter() - t0 > seconds:
+            break
+    return mesh.size * 3 * done, time.perf_counter() - t0
+
+
+def run_reference(args):
+    """The reference's own hot-path sources (oracle/_ref, built from the reference
+    tree against the stand-in MFEM header) on all host cores, one process per
+    core each advancing its own 32 x 32 x k block (MPI-style domain split)."""
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    import multiprocessing as mp
+    import oracle as orc
+    if not orc.ref_available(True):
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libref_ns.so not built (needs the reference tree)"}))
+        return
+    mesh, _, _ = workload(args.n, args.order)
+    cores = os.cpu_count() or 1
+    procs = min(cores, 32)
+    n_el = max(1, args.n // procs) if args.n >= procs else 1
+    seconds = max(5.0, args.cpu_seconds)
+    ctx = mp.get_context("spawn")
+    per_step = []
+    with ctx.Pool(procs) as pool:
+        pool.map(_ref_worker, [(n_el, args.order, 1, 1e9)] * procs)  # warm-up: one step each
+        for _ in range(max(1, min(args.steps, 3))):
+            res = pool.map(_ref_worker, [(n_el, args.order, 1, 1e9)] * procs)
+            per_step.append((sum(r[0] for r in res), max(r[1] for r in res)))
+    # all processes run concurrently: throughput = work / slowest process time
+    dofs = sum(p[0] for p in per_step)
+    wall = sum(p[1] for p in per_step)
+    value = dofs / wall
+    sample = (f"{procs} processes x {len(per_step)} timed SSP-RK3 steps, each process on its own periodic "
+              f"32x32x{n_el} N={args.order} TGV block (reference DGSEMIntegrator/ChandrashekarFlux/LiftingBR1 "
+              f"compiled from the reference tree against a stand-in MFEM header)")
+    out = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus, "steps": len(per_step),
+           "warmup": 1, "ms_per_step": wall / len(per_step) * 1e3, "higher_is_better": True, "scaling": "weak",
+           "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": config_dict(mesh, args.gpus),
+           "impl": "reference",
+           "cpu_baseline": {"value": value, "unit": UNIT, "cores": procs, "kind": "reference", "sample": sample},
+           "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(out), flush=True)
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -125,6 +125,11 @@ int pdg_rk_stage(pdg_ctx *ctx, int stage, double dt, const double *un,
  * in place by one step of size dt using context-owned stage buffers. */
 int pdg_rk3_step(pdg_ctx *ctx, double dt, double *u, void *stream);
 
+/* Same step with a HOST state (the path an MFEM adapter would take for
+ * ODESolver::Step on host Vectors): copies u in, runs the three fused stages,
+ * copies the result back and synchronises.  u_host may be pinned or pageable. */
+int pdg_rk3_step_host(pdg_ctx *ctx, double dt, double *u_host);
+
 /* DGSEMOperator::GetMaxCharSpeed (DGSEMOperator.hpp:106-109).  With compat=1
  * this is the running maximum over every RHS evaluated so far (the
  * reference never resets it); with compat=0 it is the maximum of the last
@@ -153,6 +158,17 @@ const char *pdg_last_error(const pdg_ctx *ctx);
 
 /* Number of kernels this context has launched since creation. */
 int64_t pdg_launch_count(const pdg_ctx *ctx);
+
+/* Kernel timing (no reference counterpart: the reference only times the
+ * whole run, Simulation.cpp:910-914).  When enabled, every kernel launch is
+ * bracketed by CUDA events on its own stream.  pdg_profile_read synchronises,
+ * returns the summed device time (ms) and launch count of one kernel kind
+ * (PDG_KERNEL_*) since the last read, and clears that kind's records. */
+#define PDG_KERNEL_EULER 0   /* Euler RHS / stage kernel */
+#define PDG_KERNEL_LIFT  1   /* BR1 lifting kernel */
+#define PDG_KERNEL_NS    2   /* Navier-Stokes RHS / stage kernel */
+int pdg_profile_enable(pdg_ctx *ctx, int on);
+int pdg_profile_read(pdg_ctx *ctx, int kind, double *total_ms, int64_t *launches);
 
 #ifdef __cplusplus
 }

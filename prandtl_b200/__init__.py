@@ -1,0 +1,255 @@
+"""prandtl_b200 — B200-native DGSEM right-hand side and SSP-RK stage update.
+
+Host-side mirror of the reference's operator interface for the hot path:
+
+* ``DGSEMOperator`` stands in for ``Prandtl::DGSEMOperator :
+  mfem::TimeDependentOperator`` (src/Operators/DGSEMOperator.hpp:15):
+  ``Mult(u, dudt)``, ``GetMaxCharSpeed()``, ``Height()``.
+* ``RK3SSPSolver`` stands in for MFEM's ``RK3SSPSolver`` as the reference
+  drives it (``Init(op)``, ``Step(x, t, dt)``, src/Simulation/Simulation.cpp:
+  807, 1010), with each stage's right-hand side fused into the stage axpy.
+* ``cfl_dt`` is the time-step rule of ``Simulation::Run``
+  (Simulation.cpp:893-907, 1013-1018).
+
+All compute runs in the CUDA library ``_lib/libprandtl_b200.so`` through the C
+ABI of ``include/prandtl_b200.h``; there is no CPU fallback.  State vectors use
+the reference's byNODES layout.  Device arrays are torch CUDA tensors (float64,
+contiguous); host arrays are numpy float64 arrays (``Mult`` then copies through
+the host entry point).
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+from .mesh import CartesianMesh, periodic_box  # noqa: F401
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "_lib", "libprandtl_b200.so")
+
+PDG_OK = 0
+KERNEL_EULER, KERNEL_LIFT, KERNEL_NS = 0, 1, 2
+PDG_FLAG_NONFINITE = 1
+PDG_FLAG_NONPHYSICAL = 2
+_STATUS = {1: "bad argument", 2: "CUDA error", 3: "non-finite state", 4: "non-physical state",
+           5: "unsupported configuration", 6: "out of device memory"}
+
+_dp = C.POINTER(C.c_double)
+_ip = C.POINTER(C.c_int32)
+
+
+class PdgParams(C.Structure):
+    _fields_ = [("parabolic", C.c_int32), ("blending", C.c_int32), ("compat", C.c_int32),
+                ("filter", C.c_int32), ("gamma", C.c_double), ("Pr", C.c_double),
+                ("mu", C.c_double), ("R_gas", C.c_double), ("alpha_max", C.c_double),
+                ("alpha_min", C.c_double), ("face_dissipation", C.c_double)]
+
+
+class PdgMesh(C.Structure):
+    _fields_ = [("dim", C.c_int32), ("order", C.c_int32), ("num_elements", C.c_int64),
+                ("h", C.c_double * 3), ("nbr", _ip)]
+
+
+class PdgError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"{_STATUS.get(code, 'error')} ({code}): {msg}")
+        self.code = code
+
+
+_lib = None
+
+
+def library():
+    """Loads the CUDA library; raises if it has not been built."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise RuntimeError(f"{LIB_PATH} is missing: build it with `python -m prandtl_b200.build`")
+    L = C.CDLL(LIB_PATH)
+    L.pdg_default_params.argtypes = [C.POINTER(PdgParams)]
+    L.pdg_create.argtypes = [C.POINTER(PdgMesh), C.POINTER(PdgParams), C.POINTER(C.c_void_p)]
+    L.pdg_destroy.argtypes = [C.c_void_p]
+    L.pdg_size.restype = C.c_int64
+    L.pdg_size.argtypes = [C.c_void_p]
+    L.pdg_rhs.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
+    L.pdg_rhs_host.argtypes = [C.c_void_p, _dp, _dp]
+    L.pdg_rk_stage.argtypes = [C.c_void_p, C.c_int, C.c_double, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
+    L.pdg_rk3_step.argtypes = [C.c_void_p, C.c_double, C.c_void_p, C.c_void_p]
+    L.pdg_max_char_speed.argtypes = [C.c_void_p, _dp]
+    L.pdg_cfl_dt.argtypes = [C.c_void_p, C.c_double, _dp]
+    L.pdg_get_blending.argtypes = [C.c_void_p, _dp, _dp]
+    L.pdg_get_gradients.argtypes = [C.c_void_p, _dp]
+    L.pdg_check.argtypes = [C.c_void_p, C.POINTER(C.c_uint32)]
+    L.pdg_last_error.restype = C.c_char_p
+    L.pdg_last_error.argtypes = [C.c_void_p]
+    L.pdg_launch_count.restype = C.c_int64
+    L.pdg_launch_count.argtypes = [C.c_void_p]
+    L.pdg_rk3_step_host.argtypes = [C.c_void_p, C.c_double, _dp]
+    L.pdg_profile_enable.argtypes = [C.c_void_p, C.c_int]
+    L.pdg_profile_read.argtypes = [C.c_void_p, C.c_int, _dp, C.POINTER(C.c_int64)]
+    _lib = L
+    return L
+
+
+def default_params(**overrides) -> PdgParams:
+    p = PdgParams()
+    library().pdg_default_params(C.byref(p))
+    for k, v in overrides.items():
+        setattr(p, k, v)
+    return p
+
+
+def _is_torch(x) -> bool:
+    return type(x).__module__.startswith("torch")
+
+
+def _stream_handle(stream=None) -> int:
+    import torch
+    s = stream if stream is not None else torch.cuda.current_stream()
+    return int(s.cuda_stream)
+
+
+class DGSEMOperator:
+    """DGSEMOperator::Mult on the GPU for one periodic Cartesian mesh.
+
+    Parameters mirror the reference's compile-time flags and runtime keys:
+    ``parabolic`` (PARABOLIC), ``blending`` (SUBCELL_FV_BLENDING), ``compat``
+    (reproduce the reference's value-changing quirks), ``filter`` (entropy
+    filter after each RK stage), ``gamma``, ``Pr``, ``mu``, ``alpha_max``,
+    ``alpha_min``, ``face_dissipation``.
+    """
+
+    def __init__(self, mesh: CartesianMesh, **params):
+        self.mesh = mesh
+        self.params = default_params(**params)
+        self._nbr = np.ascontiguousarray(mesh.nbr, dtype=np.int32)
+        h = list(mesh.h) + [1.0] * (3 - mesh.dim)
+        self._m = PdgMesh(mesh.dim, mesh.order, mesh.num_elements, (C.c_double * 3)(*h),
+                          self._nbr.ctypes.data_as(_ip))
+        self._ctx = C.c_void_p()
+        self._call(library().pdg_create(C.byref(self._m), C.byref(self.params), C.byref(self._ctx)), "pdg_create")
+
+    def _call(self, code: int, what: str):
+        if code != PDG_OK:
+            msg = ""
+            if self._ctx:
+                msg = library().pdg_last_error(self._ctx).decode()
+            raise PdgError(code, f"{what}: {msg}")
+
+    def close(self):
+        if getattr(self, "_ctx", None):
+            library().pdg_destroy(self._ctx)
+            self._ctx = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # --- TimeDependentOperator interface ---
+    def Height(self) -> int:
+        return int(library().pdg_size(self._ctx))
+
+    @property
+    def size(self) -> int:
+        return self.Height()
+
+    def _check_dev(self, *ts):
+        for t in ts:
+            if not (t.is_cuda and t.dtype.is_floating_point and t.element_size() == 8 and t.is_contiguous()):
+                raise ValueError("device arrays must be contiguous float64 CUDA tensors")
+            if t.numel() != self.size:
+                raise ValueError(f"array has {t.numel()} entries, operator size is {self.size}")
+
+    def Mult(self, u, dudt, stream=None):
+        """dudt = L(u).  torch CUDA tensors (device path) or numpy arrays (host path)."""
+        if _is_torch(u):
+            self._check_dev(u, dudt)
+            self._call(library().pdg_rhs(self._ctx, C.c_void_p(u.data_ptr()), C.c_void_p(dudt.data_ptr()),
+                                         C.c_void_p(_stream_handle(stream))), "pdg_rhs")
+        else:
+            if u.dtype != np.float64 or dudt.dtype != np.float64 or not u.flags.c_contiguous or not dudt.flags.c_contiguous:
+                raise ValueError("host arrays must be contiguous float64")
+            if u.size != self.size or dudt.size != self.size:
+                raise ValueError("host array size does not match the operator")
+            self._call(library().pdg_rhs_host(self._ctx, u.ctypes.data_as(_dp), dudt.ctypes.data_as(_dp)),
+                       "pdg_rhs_host")
+        return dudt
+
+    def GetMaxCharSpeed(self) -> float:
+        v = C.c_double()
+        self._call(library().pdg_max_char_speed(self._ctx, C.byref(v)), "pdg_max_char_speed")
+        return v.value
+
+    # --- fused stage update ---
+    def rk_stage(self, stage: int, dt: float, un, us, uout, stream=None):
+        self._check_dev(us, uout)
+        if un is not None:
+            self._check_dev(un)
+        self._call(library().pdg_rk_stage(self._ctx, stage, dt, C.c_void_p(un.data_ptr() if un is not None else 0),
+                                          C.c_void_p(us.data_ptr()), C.c_void_p(uout.data_ptr()),
+                                          C.c_void_p(_stream_handle(stream))), "pdg_rk_stage")
+        return uout
+
+    def rk3_step(self, u, dt: float, stream=None):
+        self._check_dev(u)
+        self._call(library().pdg_rk3_step(self._ctx, dt, C.c_void_p(u.data_ptr()), C.c_void_p(_stream_handle(stream))),
+                   "pdg_rk3_step")
+        return u
+
+    def rk3_step_host(self, u: np.ndarray, dt: float):
+        """One step on a HOST state (copy in, three fused stages, copy out)."""
+        if u.dtype != np.float64 or not u.flags.c_contiguous or u.size != self.size:
+            raise ValueError("host state must be a contiguous float64 array of the operator size")
+        self._call(library().pdg_rk3_step_host(self._ctx, dt, u.ctypes.data_as(_dp)), "pdg_rk3_step_host")
+        return u
+
+    def profile(self, on: bool = True):
+        self._call(library().pdg_profile_enable(self._ctx, int(on)), "pdg_profile_enable")
+
+    def profile_read(self, kind: int):
+        """(total device ms, launches) of one kernel kind since the last read."""
+        ms, n = C.c_double(), C.c_int64()
+        self._call(library().pdg_profile_read(self._ctx, kind, C.byref(ms), C.byref(n)), "pdg_profile_read")
+        return ms.value, n.value
+
+    def cfl_dt(self, cfl: float) -> float:
+        v = C.c_double()
+        self._call(library().pdg_cfl_dt(self._ctx, cfl, C.byref(v)), "pdg_cfl_dt")
+        return v.value
+
+    def blending(self):
+        ne = self.mesh.num_elements
+        eta, alpha = np.empty(ne), np.empty(ne)
+        self._call(library().pdg_get_blending(self._ctx, eta.ctypes.data_as(_dp), alpha.ctypes.data_as(_dp)),
+                   "pdg_get_blending")
+        return eta, alpha
+
+    def gradients(self):
+        g = np.empty(self.mesh.dim * self.size)
+        self._call(library().pdg_get_gradients(self._ctx, g.ctypes.data_as(_dp)), "pdg_get_gradients")
+        return g
+
+    def check(self) -> int:
+        """Reads and clears the device error word; raises PdgError on a flag."""
+        f = C.c_uint32()
+        self._call(library().pdg_check(self._ctx, C.byref(f)), "pdg_check")
+        return f.value
+
+    def launch_count(self) -> int:
+        return int(library().pdg_launch_count(self._ctx))
+
+
+class RK3SSPSolver:
+    """Shu-Osher SSP-RK3 with the operator's RHS fused into each stage."""
+
+    def Init(self, op: DGSEMOperator):
+        self.op = op
+
+    def Step(self, x, t: float, dt: float, stream=None) -> float:
+        self.op.rk3_step(x, dt, stream=stream)
+        return t + dt

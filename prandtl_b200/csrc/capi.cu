@@ -1,0 +1,591 @@
+// capi.cu — host side of the C ABI declared in include/prandtl_b200.h.
+//
+// A pdg_ctx plays the role of the reference's DGSEMOperator + DGSEMIntegrator
+// + PerssonPeraireIndicator objects (src/Operators/DGSEMOperator.cpp:5-50,
+// src/Integrators/DGSEMIntegrator/DGSEMIntegrator.cpp:8-149): it owns the
+// LGL operators, the subcell metrics, the modal transform, the neighbour
+// table and all scratch (blending coefficients, gradient fields, RK stage
+// buffers, the running wave-speed maximum and the error word) in device
+// memory.  Every call is asynchronous on the caller's stream unless stated.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/prandtl_b200.h"
+#include "dgsem_kernels.cuh"
+#include "kernel_table.h"
+
+using namespace pdg;
+
+struct pdg_ctx {
+    pdg_params p;
+    int dim, N, Np, ndof, nv;
+    int64_t ne, nnodes, size;
+    double h[3];
+    double hmin;
+    double modal_threshold;
+    DevConst hK;
+    // device memory
+    DevConst *K = nullptr;
+    int32_t *nbr = nullptr;
+    double *eta = nullptr, *alpha = nullptr;
+    double *grads = nullptr;
+    double *stage_a = nullptr, *stage_b = nullptr;  // RK stage buffers
+    double *io_a = nullptr, *io_b = nullptr;        // host-path staging
+    unsigned long long *lam_bits = nullptr;
+    unsigned int *err = nullptr;
+    // launch configuration per kernel kind
+    KernelInfo kinfo[3];
+    int wpb[3];
+    int grid[3];
+    size_t smem[3];
+    int64_t launches = 0;
+    bool profile = false;
+    struct TimedLaunch { int kind; cudaEvent_t a, b; };
+    std::vector<TimedLaunch> timed;
+    std::vector<cudaEvent_t> event_pool;
+    cudaStream_t last_stream = 0;
+    int device = 0;
+    std::string last_error;
+};
+
+namespace {
+
+int fail(pdg_ctx *c, int code, const char *fmt, ...)
+{
+    if (c) {
+        char buf[512];
+        va_list ap;
+        va_start(ap, fmt);
+        vsnprintf(buf, sizeof(buf), fmt, ap);
+        va_end(ap);
+        c->last_error = buf;
+    }
+    return code;
+}
+
+int cuda_fail(pdg_ctx *c, cudaError_t e, const char *what)
+{
+    return fail(c, PDG_ERR_CUDA, "%s: %s", what, cudaGetErrorString(e));
+}
+
+#define CK(call, what)                                                                                             \
+    do {                                                                                                           \
+        cudaError_t _e = (call);                                                                                   \
+        if (_e != cudaSuccess) return cuda_fail(c, _e, what);                                                      \
+    } while (0)
+
+// ---- one-dimensional operators (same mathematics as the reference's
+// DGSEMIntegrator constructor, DGSEMIntegrator.cpp:41-82) ----
+
+void legendre(int n, long double x, long double &P, long double &dP)
+{
+    long double p0 = 1.0L, p1 = x;
+    if (n == 0) { P = 1.0L; dP = 0.0L; return; }
+    for (int k = 1; k < n; k++) {
+        long double p2 = ((2 * k + 1) * x * p1 - k * p0) / (k + 1);
+        p0 = p1;
+        p1 = p2;
+    }
+    P = p1;
+    dP = (std::fabs(x) == 1.0L) ? 0.0L : n * (x * p1 - p0) / (x * x - 1.0L);
+}
+
+// Gauss-Lobatto nodes/weights on [0,1]: interior nodes are the roots of P_N'
+// (Newton's method in long double from Chebyshev-Lobatto guesses), weights
+// 1/(N(N+1) P_N^2); mirrored so x[N-i] = 1 - x[i].
+void gauss_lobatto(int Np, double *x, double *w)
+{
+    const int N = Np - 1;
+    const long double pi = 3.141592653589793238462643383279502884L;
+    for (int i = 0; i <= N / 2; i++) {
+        long double t = -1.0L;
+        if (i > 0) {
+            t = -std::cos(pi * i / N);
+            for (int it = 0; it < 100; it++) {
+                long double P, dP;
+                legendre(N, t, P, dP);
+                long double d2P = (2.0L * t * dP - N * (N + 1) * P) / (1.0L - t * t);
+                long double dt = dP / d2P;
+                t -= dt;
+                if (std::fabs(dt) < 1e-30L) break;
+            }
+        }
+        long double P, dP;
+        legendre(N, t, P, dP);
+        x[i] = (double)(0.5L * (1.0L + t));
+        w[i] = (double)(1.0L / (N * (N + 1) * P * P));
+        x[N - i] = 1.0 - x[i];
+        w[N - i] = w[i];
+    }
+    if (N % 2 == 0) x[N / 2] = 0.5;
+}
+
+void build_constants(pdg_ctx *c)
+{
+    DevConst &K = c->hK;
+    std::memset(&K, 0, sizeof(K));
+    const int Np = c->Np;
+    double x[6], w[6];
+    gauss_lobatto(Np, x, w);
+    // barycentric weights and the differentiation matrix D_il = l_l'(x_i)
+    double wb[6];
+    for (int i = 0; i < Np; i++) wb[i] = 1.0;
+    for (int i = 1; i < Np; i++)
+        for (int j = 0; j < i; j++) {
+            wb[j] *= (x[j] - x[i]);
+            wb[i] *= (x[i] - x[j]);
+        }
+    for (int i = 0; i < Np; i++) wb[i] = 1.0 / wb[i];
+    double D[36] = {0};
+    for (int l = 0; l < Np; l++)
+        for (int i = 0; i < Np; i++)
+            if (l != i) {
+                D[i * Np + l] = wb[l] / wb[i] / (x[i] - x[l]);
+                D[i * Np + i] -= D[i * Np + l];
+            }
+    for (int t = 0; t < Np * Np; t++) {
+        K.D[t] = D[t];
+        K.Dhat[t] = D[t];
+        K.Dhat2[t] = D[t] * 2.0;
+    }
+    K.Dhat[0] += 1.0 / w[0];
+    K.Dhat[Np * Np - 1] -= 1.0 / w[Np - 1];
+    K.Dhat2[0] += 1.0 / w[0];
+    K.Dhat2[Np * Np - 1] -= 1.0 / w[Np - 1];
+    for (int i = 0; i < Np; i++) K.w[i] = w[i];
+    // affine element: J = prod h, adj = diag(J / h_d), face area = J / h_d
+    const double *h = c->h;
+    if (c->dim == 2) {
+        K.J = h[0] * h[1];
+        K.adj[0] = h[1];
+        K.adj[1] = h[0];
+    } else {
+        K.J = h[0] * (h[1] * h[2]);
+        K.adj[0] = h[1] * h[2];
+        K.adj[1] = h[0] * h[2];
+        K.adj[2] = h[0] * h[1];
+    }
+    for (int d = 0; d < c->dim; d++) K.area[d] = K.adj[d];
+    K.invJ = 1.0 / K.J;
+    K.face_scale = 1.0 / (w[0] * K.J);
+    for (int i = 0; i < Np; i++) K.fv_scale[i] = 1.0 / (K.J * w[i]);
+    // subcell interface normals (ComputeSubcellMetrics, DGSEMIntegrator.cpp:
+    // 1199-1304): adj_d + sum_{l<i} w_l sum_m D(l,m) adj_d on an affine element
+    for (int d = 0; d < c->dim; d++)
+        for (int i = 0; i <= Np; i++) {
+            double nor = K.adj[d];
+            for (int l = 0; l < i; l++) {
+                double tmp = 0.0;
+                for (int m = 0; m < Np; m++) tmp += K.adj[d] * D[l * Np + m];
+                nor += tmp * w[l];
+            }
+            K.snor[d][i] = nor;
+        }
+    // 1D Legendre Vandermonde on the nodes and its inverse; the tensor-product
+    // modal transform of ModalBasis (ModalBasis.cpp:110-150) factors into it.
+    double V[36], I[36] = {0};
+    for (int i = 0; i < Np; i++) {
+        double z = 2.0 * x[i] - 1.0, L[6];
+        L[0] = 1.0;
+        if (Np > 1) L[1] = z;
+        for (int n = 1; n + 1 < Np; n++) L[n + 1] = ((2 * n + 1) * z * L[n] - n * L[n - 1]) / (n + 1);
+        for (int k = 0; k < Np; k++) V[i * Np + k] = L[k];
+    }
+    for (int i = 0; i < Np; i++) I[i * Np + i] = 1.0;
+    for (int col = 0; col < Np; col++) {  // Gauss-Jordan with partial pivoting
+        int piv = col;
+        for (int r = col + 1; r < Np; r++)
+            if (std::fabs(V[r * Np + col]) > std::fabs(V[piv * Np + col])) piv = r;
+        for (int k = 0; k < Np; k++) {
+            std::swap(V[piv * Np + k], V[col * Np + k]);
+            std::swap(I[piv * Np + k], I[col * Np + k]);
+        }
+        const double inv = 1.0 / V[col * Np + col];
+        for (int k = 0; k < Np; k++) {
+            V[col * Np + k] *= inv;
+            I[col * Np + k] *= inv;
+        }
+        for (int r = 0; r < Np; r++)
+            if (r != col) {
+                const double f = V[r * Np + col];
+                for (int k = 0; k < Np; k++) {
+                    V[r * Np + k] -= f * V[col * Np + k];
+                    I[r * Np + k] -= f * I[col * Np + k];
+                }
+            }
+    }
+    for (int t = 0; t < Np * Np; t++) K.Vinv1[t] = I[t];  // Vinv1[k*Np + i]: mode k from node i
+    c->modal_threshold = 0.5 * std::pow(10.0, -1.8 * std::pow((double)c->N, 0.25));
+}
+
+int configure_launch(pdg_ctx *c, int kind)
+{
+    KernelInfo &ki = c->kinfo[kind];
+    bool ok = c->dim == 2 ? kernel_info_2d(c->N, kind, &ki) : kernel_info_3d(c->N, kind, &ki);
+    if (!ok) return fail(c, PDG_ERR_UNSUPPORTED, "no kernel for dim=%d order=%d", c->dim, c->N);
+    int dev = c->device, max_smem = 0, sms = 0;
+    CK(cudaDeviceGetAttribute(&max_smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev), "device attribute");
+    CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev), "device attribute");
+    const size_t per_warp = (size_t)ki.epw * ki.el_doubles * sizeof(double);
+    const size_t base = (size_t)CONST_SLOTS * sizeof(double);
+    int wpb = 4;
+    while (wpb > 1 && base + wpb * per_warp > (size_t)max_smem) wpb--;
+    if (base + wpb * per_warp > (size_t)max_smem)
+        return fail(c, PDG_ERR_UNSUPPORTED, "element does not fit in shared memory (dim=%d order=%d)", c->dim, c->N);
+    const size_t smem = base + wpb * per_warp;
+    CK(cudaFuncSetAttribute(ki.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem), "smem attribute");
+    int blocks_per_sm = 0;
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks_per_sm, ki.fn, 32 * wpb, smem), "occupancy");
+    if (blocks_per_sm < 1) return fail(c, PDG_ERR_UNSUPPORTED, "kernel cannot be resident (dim=%d order=%d)", c->dim, c->N);
+    const int64_t nwt = (c->ne + ki.epw - 1) / ki.epw;
+    const int64_t need = (nwt + wpb - 1) / wpb;
+    c->wpb[kind] = wpb;
+    c->grid[kind] = (int)std::max<int64_t>(1, std::min<int64_t>(need, (int64_t)sms * blocks_per_sm));
+    c->smem[kind] = smem;
+    return PDG_OK;
+}
+
+KParams base_params(pdg_ctx *c)
+{
+    KParams P;
+    std::memset(&P, 0, sizeof(P));
+    P.nbr = c->nbr;
+    P.K = c->K;
+    P.eta_out = c->eta;
+    P.alpha_out = c->alpha;
+    P.lam_bits = c->lam_bits;
+    P.err = c->err;
+    P.ne = c->ne;
+    P.nnodes = c->nnodes;
+    P.stage = -1;
+    P.gamma = c->p.gamma;
+    P.gm1 = c->p.gamma - 1.0;
+    P.gm1inv = 1.0 / P.gm1;
+    P.mu = c->p.mu;
+    P.lambda_k = c->p.mu * c->p.gamma * (1.0 / c->p.Pr);
+    P.alpha_max = c->p.alpha_max;
+    P.alpha_min = c->p.alpha_min;
+    P.modal_threshold = c->modal_threshold;
+    P.diss_scale = c->p.face_dissipation;
+    P.blending = c->p.blending;
+    P.compat = c->p.compat;
+    return P;
+}
+
+cudaEvent_t pooled_event(pdg_ctx *c)
+{
+    if (!c->event_pool.empty()) {
+        cudaEvent_t e = c->event_pool.back();
+        c->event_pool.pop_back();
+        return e;
+    }
+    cudaEvent_t e = nullptr;
+    if (cudaEventCreate(&e) != cudaSuccess) return nullptr;
+    return e;
+}
+
+int launch(pdg_ctx *c, int kind, KParams P, cudaStream_t s)
+{
+    const KernelInfo &ki = c->kinfo[kind];
+    P.nwt = (c->ne + ki.epw - 1) / ki.epw;
+    void *args[] = {&P};
+    cudaEvent_t ea = nullptr, eb = nullptr;
+    if (c->profile) {
+        ea = pooled_event(c);
+        eb = pooled_event(c);
+        if (!ea || !eb) return fail(c, PDG_ERR_CUDA, "event creation failed");
+        CK(cudaEventRecord(ea, s), "event record");
+    }
+    CK(cudaLaunchKernel(ki.fn, dim3(c->grid[kind]), dim3(32 * c->wpb[kind]), args, c->smem[kind], s), "kernel launch");
+    if (c->profile) {
+        CK(cudaEventRecord(eb, s), "event record");
+        c->timed.push_back({kind, ea, eb});
+    }
+    c->launches++;
+    return PDG_OK;
+}
+
+// RHS (stage < 0) or fused SSP-RK3 stage of the operator on device buffers.
+int evaluate(pdg_ctx *c, int stage, double dt, const double *un, const double *us, double *out, cudaStream_t s)
+{
+    if (!c->p.compat) CK(cudaMemsetAsync(c->lam_bits, 0, sizeof(unsigned long long), s), "reset wave speed");
+    KParams P = base_params(c);
+    P.u = us;
+    P.un = un;
+    P.out = out;
+    P.stage = stage;
+    P.dt = dt;
+    c->last_stream = s;
+    if (c->p.parabolic) {
+        KParams L = P;
+        L.grads_out = c->grads;
+        int r = launch(c, KIND_LIFT, L, s);
+        if (r) return r;
+        P.grads = c->grads;
+        return launch(c, KIND_NS, P, s);
+    }
+    return launch(c, KIND_EULER, P, s);
+}
+
+}  // namespace
+
+extern "C" {
+
+void pdg_default_params(pdg_params *p)
+{
+    if (!p) return;
+    p->parabolic = 0;
+    p->blending = 1;
+    p->compat = 1;
+    p->filter = 0;
+    p->gamma = 1.4;
+    p->Pr = 0.72;
+    p->mu = 0.0;
+    p->R_gas = 287.0;
+    p->alpha_max = 0.5;
+    p->alpha_min = 0.001;
+    p->face_dissipation = 1.0;
+}
+
+int pdg_create(const pdg_mesh *mesh, const pdg_params *params, pdg_ctx **out)
+{
+    if (!out) return PDG_ERR_ARG;
+    *out = nullptr;
+    if (!mesh || !params || !mesh->nbr) return PDG_ERR_ARG;
+    if ((mesh->dim != 2 && mesh->dim != 3) || mesh->order < 1 || mesh->order > 5 || mesh->num_elements < 1)
+        return PDG_ERR_ARG;
+    if (!(params->gamma > 1.0) || (params->parabolic && !(params->Pr > 0.0))) return PDG_ERR_ARG;
+    pdg_ctx *c = new pdg_ctx();
+    c->p = *params;
+    c->dim = mesh->dim;
+    c->N = mesh->order;
+    c->Np = c->N + 1;
+    c->ndof = c->dim == 2 ? c->Np * c->Np : c->Np * c->Np * c->Np;
+    c->nv = c->dim + 2;
+    c->ne = mesh->num_elements;
+    c->nnodes = c->ne * c->ndof;
+    c->size = c->nnodes * c->nv;
+    c->hmin = 1e300;
+    for (int d = 0; d < 3; d++) {
+        c->h[d] = d < c->dim ? mesh->h[d] : 1.0;
+        if (d < c->dim) {
+            if (!(c->h[d] > 0.0)) { delete c; return PDG_ERR_ARG; }
+            c->hmin = std::min(c->hmin, c->h[d]);
+        }
+    }
+    for (int64_t i = 0; i < c->ne * 2 * c->dim; i++)
+        if (mesh->nbr[i] < 0 || mesh->nbr[i] >= c->ne) { delete c; return PDG_ERR_ARG; }
+    auto cleanup = [&](int code) {
+        pdg_destroy(c);
+        return code;
+    };
+    if (cudaGetDevice(&c->device) != cudaSuccess) return cleanup(PDG_ERR_CUDA);
+    build_constants(c);
+    const size_t fbytes = sizeof(double) * (size_t)c->size;
+    if (cudaMalloc(&c->K, sizeof(DevConst)) != cudaSuccess || cudaMalloc(&c->nbr, sizeof(int32_t) * c->ne * 2 * c->dim) ||
+        cudaMalloc(&c->eta, sizeof(double) * c->ne) || cudaMalloc(&c->alpha, sizeof(double) * c->ne) ||
+        cudaMalloc(&c->lam_bits, sizeof(unsigned long long)) || cudaMalloc(&c->err, sizeof(unsigned int)) ||
+        cudaMalloc(&c->stage_a, fbytes) || cudaMalloc(&c->stage_b, fbytes))
+        return cleanup(PDG_ERR_NOMEM);
+    if (c->p.parabolic && cudaMalloc(&c->grads, fbytes * c->dim) != cudaSuccess) return cleanup(PDG_ERR_NOMEM);
+    if (cudaMemcpy(c->K, &c->hK, sizeof(DevConst), cudaMemcpyHostToDevice) ||
+        cudaMemcpy(c->nbr, mesh->nbr, sizeof(int32_t) * c->ne * 2 * c->dim, cudaMemcpyHostToDevice) ||
+        cudaMemset(c->eta, 0, sizeof(double) * c->ne) || cudaMemset(c->alpha, 0, sizeof(double) * c->ne) ||
+        cudaMemset(c->lam_bits, 0, sizeof(unsigned long long)) || cudaMemset(c->err, 0, sizeof(unsigned int)))
+        return cleanup(PDG_ERR_CUDA);
+    for (int kind = 0; kind < 3; kind++) {
+        if (kind != KIND_EULER && !c->p.parabolic) continue;
+        if (kind == KIND_EULER && c->p.parabolic) continue;
+        int r = configure_launch(c, kind);
+        if (r) return cleanup(r);
+    }
+    *out = c;
+    return PDG_OK;
+}
+
+int pdg_destroy(pdg_ctx *c)
+{
+    if (!c) return PDG_OK;
+    cudaFree(c->K);
+    cudaFree(c->nbr);
+    cudaFree(c->eta);
+    cudaFree(c->alpha);
+    cudaFree(c->grads);
+    cudaFree(c->stage_a);
+    cudaFree(c->stage_b);
+    cudaFree(c->io_a);
+    cudaFree(c->io_b);
+    cudaFree(c->lam_bits);
+    cudaFree(c->err);
+    for (auto &t : c->timed) {
+        cudaEventDestroy(t.a);
+        cudaEventDestroy(t.b);
+    }
+    for (auto e : c->event_pool) cudaEventDestroy(e);
+    delete c;
+    return PDG_OK;
+}
+
+int64_t pdg_size(const pdg_ctx *c) { return c ? c->size : -1; }
+
+int pdg_rhs(pdg_ctx *c, const double *u, double *dudt, void *stream)
+{
+    if (!c) return PDG_ERR_ARG;
+    if (!u || !dudt || u == dudt) return fail(c, PDG_ERR_ARG, "pdg_rhs: null or aliased buffers");
+    return evaluate(c, -1, 0.0, nullptr, u, dudt, (cudaStream_t)stream);
+}
+
+int pdg_rhs_host(pdg_ctx *c, const double *u_host, double *dudt_host)
+{
+    if (!c) return PDG_ERR_ARG;
+    if (!u_host || !dudt_host) return fail(c, PDG_ERR_ARG, "pdg_rhs_host: null buffer");
+    const size_t bytes = sizeof(double) * (size_t)c->size;
+    if (!c->io_a) {
+        if (cudaMalloc(&c->io_a, bytes) != cudaSuccess || cudaMalloc(&c->io_b, bytes) != cudaSuccess)
+            return fail(c, PDG_ERR_NOMEM, "pdg_rhs_host: staging allocation failed");
+    }
+    cudaStream_t s = 0;
+    CK(cudaMemcpyAsync(c->io_a, u_host, bytes, cudaMemcpyHostToDevice, s), "copy in");
+    int r = evaluate(c, -1, 0.0, nullptr, c->io_a, c->io_b, s);
+    if (r) return r;
+    CK(cudaMemcpyAsync(dudt_host, c->io_b, bytes, cudaMemcpyDeviceToHost, s), "copy out");
+    CK(cudaStreamSynchronize(s), "synchronize");
+    return PDG_OK;
+}
+
+int pdg_rk_stage(pdg_ctx *c, int stage, double dt, const double *un, const double *us, double *uout, void *stream)
+{
+    if (!c) return PDG_ERR_ARG;
+    if (stage < 0 || stage > 2) return fail(c, PDG_ERR_ARG, "pdg_rk_stage: stage must be 0, 1 or 2");
+    if (!us || !uout || uout == us) return fail(c, PDG_ERR_ARG, "pdg_rk_stage: null or aliased buffers");
+    if (stage > 0 && !un) return fail(c, PDG_ERR_ARG, "pdg_rk_stage: stage %d needs un", stage);
+    return evaluate(c, stage, dt, stage > 0 ? un : us, us, uout, (cudaStream_t)stream);
+}
+
+int pdg_rk3_step(pdg_ctx *c, double dt, double *u, void *stream)
+{
+    if (!c) return PDG_ERR_ARG;
+    if (!u) return fail(c, PDG_ERR_ARG, "pdg_rk3_step: null state");
+    cudaStream_t s = (cudaStream_t)stream;
+    int r = evaluate(c, 0, dt, u, u, c->stage_a, s);
+    if (!r) r = evaluate(c, 1, dt, u, c->stage_a, c->stage_b, s);
+    // stage 2 reads un and writes the same entry from the same thread, so the
+    // result can overwrite u in place
+    if (!r) r = evaluate(c, 2, dt, u, c->stage_b, u, s);
+    return r;
+}
+
+int pdg_rk3_step_host(pdg_ctx *c, double dt, double *u_host)
+{
+    if (!c) return PDG_ERR_ARG;
+    if (!u_host) return fail(c, PDG_ERR_ARG, "pdg_rk3_step_host: null state");
+    const size_t bytes = sizeof(double) * (size_t)c->size;
+    if (!c->io_a) {
+        if (cudaMalloc(&c->io_a, bytes) != cudaSuccess || cudaMalloc(&c->io_b, bytes) != cudaSuccess)
+            return fail(c, PDG_ERR_NOMEM, "pdg_rk3_step_host: staging allocation failed");
+    }
+    cudaStream_t s = 0;
+    CK(cudaMemcpyAsync(c->io_a, u_host, bytes, cudaMemcpyHostToDevice, s), "copy in");
+    int r = pdg_rk3_step(c, dt, c->io_a, s);
+    if (r) return r;
+    CK(cudaMemcpyAsync(u_host, c->io_a, bytes, cudaMemcpyDeviceToHost, s), "copy out");
+    CK(cudaStreamSynchronize(s), "synchronize");
+    return PDG_OK;
+}
+
+int pdg_profile_enable(pdg_ctx *c, int on)
+{
+    if (!c) return PDG_ERR_ARG;
+    c->profile = on != 0;
+    return PDG_OK;
+}
+
+int pdg_profile_read(pdg_ctx *c, int kind, double *total_ms, int64_t *launches)
+{
+    if (!c || !total_ms || !launches) return PDG_ERR_ARG;
+    double ms = 0.0;
+    int64_t n = 0;
+    std::vector<pdg_ctx::TimedLaunch> keep;
+    for (auto &t : c->timed) {
+        if (t.kind != kind) { keep.push_back(t); continue; }
+        CK(cudaEventSynchronize(t.b), "event synchronize");
+        float dt = 0.0f;
+        CK(cudaEventElapsedTime(&dt, t.a, t.b), "event elapsed");
+        ms += dt;
+        n++;
+        c->event_pool.push_back(t.a);
+        c->event_pool.push_back(t.b);
+    }
+    c->timed.swap(keep);
+    *total_ms = ms;
+    *launches = n;
+    return PDG_OK;
+}
+
+int pdg_max_char_speed(pdg_ctx *c, double *out)
+{
+    if (!c || !out) return PDG_ERR_ARG;
+    unsigned long long bits = 0;
+    CK(cudaMemcpyAsync(&bits, c->lam_bits, sizeof(bits), cudaMemcpyDeviceToHost, c->last_stream), "read wave speed");
+    CK(cudaStreamSynchronize(c->last_stream), "synchronize");
+    double v;
+    std::memcpy(&v, &bits, sizeof(v));
+    *out = bits ? v : -1.0;
+    return PDG_OK;
+}
+
+int pdg_cfl_dt(pdg_ctx *c, double cfl, double *dt_out)
+{
+    if (!c || !dt_out) return PDG_ERR_ARG;
+    double lam;
+    int r = pdg_max_char_speed(c, &lam);
+    if (r) return r;
+    if (!(lam > 0.0)) return fail(c, PDG_ERR_ARG, "pdg_cfl_dt: no wave speed yet (evaluate a RHS first)");
+    *dt_out = cfl * c->hmin / (lam * std::pow((double)(c->N + 1), 2));
+    return PDG_OK;
+}
+
+int pdg_get_blending(pdg_ctx *c, double *eta_host, double *alpha_host)
+{
+    if (!c) return PDG_ERR_ARG;
+    CK(cudaStreamSynchronize(c->last_stream), "synchronize");
+    if (eta_host) CK(cudaMemcpy(eta_host, c->eta, sizeof(double) * c->ne, cudaMemcpyDeviceToHost), "copy eta");
+    if (alpha_host) CK(cudaMemcpy(alpha_host, c->alpha, sizeof(double) * c->ne, cudaMemcpyDeviceToHost), "copy alpha");
+    return PDG_OK;
+}
+
+int pdg_get_gradients(pdg_ctx *c, double *grad_host)
+{
+    if (!c || !grad_host) return PDG_ERR_ARG;
+    if (!c->p.parabolic) return fail(c, PDG_ERR_ARG, "pdg_get_gradients: operator is not parabolic");
+    CK(cudaStreamSynchronize(c->last_stream), "synchronize");
+    CK(cudaMemcpy(grad_host, c->grads, sizeof(double) * c->size * c->dim, cudaMemcpyDeviceToHost), "copy gradients");
+    return PDG_OK;
+}
+
+int pdg_check(pdg_ctx *c, uint32_t *flags)
+{
+    if (!c || !flags) return PDG_ERR_ARG;
+    unsigned int f = 0;
+    CK(cudaStreamSynchronize(c->last_stream), "synchronize");
+    CK(cudaMemcpy(&f, c->err, sizeof(f), cudaMemcpyDeviceToHost), "read error word");
+    CK(cudaMemset(c->err, 0, sizeof(unsigned int)), "clear error word");
+    *flags = f;
+    if (f & PDG_FLAG_NONFINITE) return fail(c, PDG_ERR_NONFINITE, "non-finite value in a state");
+    if (f & PDG_FLAG_NONPHYSICAL) return fail(c, PDG_ERR_NONPHYSICAL, "non-positive density or pressure");
+    return PDG_OK;
+}
+
+const char *pdg_last_error(const pdg_ctx *c) { return c ? c->last_error.c_str() : "null context"; }
+
+int64_t pdg_launch_count(const pdg_ctx *c) { return c ? c->launches : -1; }
+
+}  // extern "C"
