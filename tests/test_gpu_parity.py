@@ -14,6 +14,11 @@ from prandtl_b200.mesh import periodic_box
 from helpers import golden_cases, load_golden, rel_maxnorm, rough
 
 TOL = 1e-12
+# The BR1 gradient field is an intermediate, not an RHS.  Its density row is
+# rho*dw0 - dw_last*(KE - p/(g-1)) + ...: O(p/(g-1)) terms cancelling to a small
+# gradient, so for nearly constant density it carries ~1e-14 absolute noise;
+# 1e-11 relative to the field's max covers that.
+TOL_GRAD = 1e-11
 
 pytestmark = pytest.mark.gpu
 
@@ -43,7 +48,7 @@ def test_gpu_matches_reference_fixture(name, cuda_device):
     np.testing.assert_allclose(alpha, z["alpha"], rtol=0, atol=1e-10)
     assert abs(op.GetMaxCharSpeed() - float(z["lam"])) <= 1e-12 * float(z["lam"])
     if params["parabolic"]:
-        assert rel_maxnorm(op.gradients(), z["grads"]) < TOL
+        assert rel_maxnorm(op.gradients(), z["grads"]) < TOL_GRAD
     assert op.check() == 0
 
 
@@ -81,7 +86,7 @@ def test_gpu_rhs_matches_oracle(kind, dim, order, par, compat, cuda_device):
     e0, a0 = orc.blending()
     np.testing.assert_allclose(a1, a0, rtol=0, atol=1e-10)
     if par:
-        assert rel_maxnorm(op.gradients(), orc.gradients()) < TOL
+        assert rel_maxnorm(op.gradients(), orc.gradients()) < TOL_GRAD
     assert abs(op.GetMaxCharSpeed() - orc.max_char_speed()) <= 1e-12 * orc.max_char_speed()
 
 
