@@ -1,9 +1,11 @@
 // physics.cuh — FP64 pointwise physics of the DGSEM right-hand side, device side.
 //
-// Each function restates one reference function (cited) for sm_100a.  All
-// arithmetic is FP64 with CUDA's own division, sqrt, log, pow and exp; the
-// compiler may fuse multiply-adds (results then differ from the reference in
-// the last bits only).
+// Each function restates one reference function (cited) for sm_100a, with the
+// same quantities evaluated with fewer divisions: per-node reciprocals are
+// computed once, and both log-means of a two-point flux share the reciprocal
+// of the sum of their arguments.  All arithmetic is FP64 with CUDA's own
+// division, sqrt and log; results differ from the reference's formulas by
+// rounding only (the parity tests bound them at 1e-12 relative).
 #pragma once
 
 #include <cuda_runtime.h>
@@ -11,53 +13,71 @@
 
 namespace pdg {
 
-// ComputeLogMean, src/BasicOperations/BasicOperations.cpp:6-12 (eps = 1e-4).
-__device__ __forceinline__ double logmean(double x, double y)
+// Log-mean (y - x) / (ln y - ln x) of ComputeLogMean
+// (src/BasicOperations/BasicOperations.cpp:6-12): with f = (y-x)/(y+x) and
+// u = f^2 (equal to the reference's (xi-1)^2/(xi+1)^2, xi = y/x), the series
+// branch u < 1e-4 is (x+y) 52.5 / (105 + u(35 + u(21 + 15u))), otherwise
+// (y-x)/log(y/x).  Returns the mean and its reciprocal; `is` = 1/(x+y).
+__device__ __forceinline__ void logmean_inv(double x, double y, double s, double is, double &mean, double &inv)
 {
-    const double xi = y / x;
-    const double u = (xi * (xi - 2.0) + 1.0) / (xi * (xi + 2.0) + 1.0);
-    if (u < 1e-4) return (x + y) * 52.5 / (105.0 + u * (35.0 + u * (21.0 + 15.0 * u)));
-    return (y - x) / log(xi);
+    const double f = (y - x) * is;
+    const double u = f * f;
+    if (u < 1e-4) {
+        const double P = 105.0 + u * (35.0 + u * (21.0 + 15.0 * u));
+        mean = s * 52.5 / P;
+        inv = P * is * (1.0 / 52.5);
+    } else {
+        const double L = log(y / x);
+        mean = (y - x) / L;
+        inv = L / (y - x);
+    }
+}
+// Reciprocal of the log-mean only.
+__device__ __forceinline__ double logmean_recip(double x, double y, double is)
+{
+    const double f = (y - x) * is;
+    const double u = f * f;
+    if (u < 1e-4) return (105.0 + u * (35.0 + u * (21.0 + 15.0 * u))) * is * (1.0 / 52.5);
+    return log(y / x) / (y - x);
 }
 
-// Per-node primitive quantities used by the two-point fluxes.
+// Primitive quantities of one state, as the Chandrashekar flux derives them
+// (ChandrashekarFlux.cpp:17-68): v = m / rho, p = (g-1)(E - rho |v|^2 / 2),
+// beta = rho / (2p), plus 1/rho, 1/beta and the wave speed |v| + c.
 template <int DIM> struct Prim {
-    double rho, v[DIM], p, beta, vsq;
+    double rho, irho, v[DIM], p, beta, ib, lam;
 };
 
-// Primitive state as the Chandrashekar flux computes it from a conservative
-// state (ChandrashekarFlux.cpp:17-68): v = m / rho, p = (g-1)(E - rho |v|^2/2),
-// beta = rho / (2 p).
-template <int DIM> __device__ __forceinline__ Prim<DIM> make_prim(const double *s, double gm1)
+template <int DIM> __device__ __forceinline__ Prim<DIM> make_prim(const double *s, double gamma, double gm1)
 {
     Prim<DIM> q;
     q.rho = s[0];
+    q.irho = 1.0 / q.rho;
     double vsq = 0.0;
 #pragma unroll
     for (int d = 0; d < DIM; d++) {
-        q.v[d] = s[1 + d] / q.rho;
+        q.v[d] = s[1 + d] * q.irho;
         vsq += q.v[d] * q.v[d];
     }
-    q.vsq = vsq;
     q.p = gm1 * (s[DIM + 1] - 0.5 * q.rho * vsq);
     q.beta = 0.5 * q.rho / q.p;
+    q.ib = 2.0 * q.p * q.irho;
+    q.lam = sqrt(vsq) + sqrt(gamma * q.p * q.irho);
     return q;
 }
 
-// Wave speed |v| + c of one state (ChandrashekarFlux.cpp:61-65).
-template <int DIM> __device__ __forceinline__ double wave_speed(const Prim<DIM> &q, double gamma)
+// ChandrashekarFlux::ComputeVolumeFlux (ChandrashekarFlux.cpp:11-83) for a
+// contravariant metric `metric` along axis DIR.
+template <int DIM, int DIR>
+__device__ __forceinline__ void volume_flux(const Prim<DIM> &a, const Prim<DIM> &b, double metric, double gm1inv,
+                                            double *F)
 {
-    return sqrt(q.vsq) + sqrt(gamma * q.p / q.rho);
-}
-
-// ChandrashekarFlux::ComputeVolumeFlux (ChandrashekarFlux.cpp:11-83) for an
-// axis-aligned contravariant metric: the metric mean is `metric` along
-// direction DIR and zero elsewhere.
-template <int DIM>
-__device__ __forceinline__ void volume_flux(const Prim<DIM> &a, const Prim<DIM> &b, int dir, double metric,
-                                            double gm1inv, double *F)
-{
-    const double rho_ln = logmean(a.rho, b.rho);
+    const double sr = a.rho + b.rho, isr = 1.0 / sr;
+    double rho_ln, irho_ln;
+    logmean_inv(a.rho, b.rho, sr, isr, rho_ln, irho_ln);
+    const double isb = 1.0 / (a.beta + b.beta);
+    const double ibeta_ln = logmean_recip(a.beta, b.beta, isb);
+    const double p_hat = 0.5 * sr * isb;
     double vm[DIM];
     double h_hat = 0.0;
 #pragma unroll
@@ -65,122 +85,92 @@ __device__ __forceinline__ void volume_flux(const Prim<DIM> &a, const Prim<DIM> 
         vm[d] = 0.5 * (a.v[d] + b.v[d]);
         h_hat += -0.25 * (a.v[d] * a.v[d] + b.v[d] * b.v[d]) + vm[d] * vm[d];
     }
-    double vdir = vm[0];
+    h_hat += 0.5 * ibeta_ln * gm1inv + p_hat * irho_ln;
+    const double Vn = vm[DIR] * metric;
+    const double fm = rho_ln * Vn;
+    F[0] = fm;
 #pragma unroll
-    for (int d = 1; d < DIM; d++)
-        if (dir == d) vdir = vm[d];
-    const double Vn = vdir * metric;
-    const double beta_ln = logmean(a.beta, b.beta);
-    const double p_hat = 0.5 * (a.rho + b.rho) / (a.beta + b.beta);
-    h_hat += 0.5 / beta_ln * gm1inv + p_hat / rho_ln;
-    F[0] = rho_ln * Vn;
-#pragma unroll
-    for (int d = 0; d < DIM; d++) F[1 + d] = Vn * (rho_ln * vm[d]) + (d == dir ? p_hat * metric : 0.0);
-    F[1 + DIM] = rho_ln * Vn * h_hat;
+    for (int d = 0; d < DIM; d++) F[1 + d] = fm * vm[d] + (d == DIR ? p_hat * metric : 0.0);
+    F[1 + DIM] = fm * h_hat;
 }
 
 // ChandrashekarFlux::ComputeFaceFlux (ChandrashekarFlux.cpp:85-161) for a
-// normal of magnitude |nrm| along axis DIR (sign included in nrm).  compat
-// keeps the 3D energy term as the reference writes it (`rho_mean * dw +
-// w_mean`, :131).  diss scales the Lax-Friedrichs term (1 = reference).
-// s1/s2: conservative states; returns lambda_max.
-template <int DIM>
-__device__ __forceinline__ double face_flux(const double *s1, const double *s2, int dir, double nrm, double gamma,
-                                            double gm1, double gm1inv, bool compat, double diss_scale, double *F)
+// normal of magnitude |nrm| along axis DIR (sign in nrm).  ma/mb are the
+// momenta whose jump the Lax-Friedrichs term uses; compat keeps the 3D
+// energy term as the reference writes it (`rho_mean * dw + w_mean`, :131).
+template <int DIM, int DIR>
+__device__ __forceinline__ void face_flux(const Prim<DIM> &a, const Prim<DIM> &b, const double *ma, const double *mb,
+                                          double nrm, double gm1inv, bool compat, double diss_scale, double *F)
 {
-    const double nor_mag = fabs(nrm);
-    const double rho1 = s1[0], rho2 = s2[0];
-    const double rho_mean = 0.5 * (rho1 + rho2);
-    const double rho_ln = logmean(rho1, rho2);
-    const double drho = rho2 - rho1;
-    double v1[DIM], v2[DIM], vm[DIM];
-    double Vsq1 = 0.0, Vsq2 = 0.0, h_hat = 0.0, diss = 0.0;
+    const double sr = a.rho + b.rho, isr = 1.0 / sr;
+    double rho_ln, irho_ln;
+    logmean_inv(a.rho, b.rho, sr, isr, rho_ln, irho_ln);
+    const double isb = 1.0 / (a.beta + b.beta);
+    const double ibeta_ln = logmean_recip(a.beta, b.beta, isb);
+    const double p_hat = 0.5 * sr * isb;
+    const double rho_mean = 0.5 * sr, drho = b.rho - a.rho;
+    double vm[DIM];
+    double h_hat = 0.0, diss = 0.0;
 #pragma unroll
     for (int d = 0; d < DIM; d++) {
-        v1[d] = s1[1 + d] / rho1;
-        v2[d] = s2[1 + d] / rho2;
-        vm[d] = 0.5 * (v1[d] + v2[d]);
-        const double dv = v2[d] - v1[d];
-        Vsq1 += v1[d] * v1[d];
-        Vsq2 += v2[d] * v2[d];
-        h_hat += -0.25 * (v1[d] * v1[d] + v2[d] * v2[d]) + vm[d] * vm[d];
+        vm[d] = 0.5 * (a.v[d] + b.v[d]);
+        const double dv = b.v[d] - a.v[d];
+        h_hat += -0.25 * (a.v[d] * a.v[d] + b.v[d] * b.v[d]) + vm[d] * vm[d];
         if (DIM == 3 && d == 2 && compat)
-            diss += 0.5 * drho * v1[d] * v2[d] + rho_mean * dv + vm[d];
+            diss += 0.5 * drho * a.v[d] * b.v[d] + rho_mean * dv + vm[d];
         else
-            diss += 0.5 * drho * v1[d] * v2[d] + rho_mean * dv * vm[d];
+            diss += 0.5 * drho * a.v[d] * b.v[d] + rho_mean * dv * vm[d];
     }
-    double vdir = vm[0];
+    h_hat += 0.5 * ibeta_ln * gm1inv + p_hat * irho_ln;
+    diss += 0.5 * drho * gm1inv * ibeta_ln + 0.5 * rho_mean * gm1inv * (b.ib - a.ib);
+    const double lam = 0.5 * fmax(a.lam, b.lam) * diss_scale * fabs(nrm);
+    const double Vn = vm[DIR] * nrm;
+    const double fm = rho_ln * Vn;
+    F[0] = fm - lam * drho;
 #pragma unroll
-    for (int d = 1; d < DIM; d++)
-        if (dir == d) vdir = vm[d];
-    const double Vn = vdir * nrm;
-    const double p1 = gm1 * (s1[DIM + 1] - 0.5 * rho1 * Vsq1);
-    const double p2 = gm1 * (s2[DIM + 1] - 0.5 * rho2 * Vsq2);
-    const double lam1 = sqrt(Vsq1) + sqrt(gamma * p1 / rho1);
-    const double lam2 = sqrt(Vsq2) + sqrt(gamma * p2 / rho2);
-    const double lambda_max = fmax(lam1, lam2);
-    const double beta1 = 0.5 * rho1 / p1, beta2 = 0.5 * rho2 / p2;
-    const double beta_ln = logmean(beta1, beta2);
-    const double p_hat = 0.5 * (rho1 + rho2) / (beta1 + beta2);
-    h_hat += 0.5 / beta_ln * gm1inv + p_hat / rho_ln;
-    diss += 0.5 * drho * gm1inv / beta_ln + 0.5 * rho_mean * gm1inv * (1.0 / beta2 - 1.0 / beta1);
-    const double lam = 0.5 * lambda_max * diss_scale * nor_mag;
-    F[0] = rho_ln * Vn - lam * (rho2 - rho1);
-#pragma unroll
-    for (int d = 0; d < DIM; d++)
-        F[1 + d] = Vn * (rho_ln * vm[d]) + (d == dir ? p_hat * nrm : 0.0) - lam * (s2[1 + d] - s1[1 + d]);
-    F[1 + DIM] = rho_ln * Vn * h_hat - lam * diss;
-    return lambda_max;
+    for (int d = 0; d < DIM; d++) F[1 + d] = fm * vm[d] + (d == DIR ? p_hat * nrm : 0.0) - lam * (mb[d] - ma[d]);
+    F[1 + DIM] = fm * h_hat - lam * diss;
 }
 
 // NavierStokesFlux::ComputeViscousFlux (src/Fluxes/NavierStokesFlux.cpp:12-90),
-// constant mu, mu_bulk = 2/3.  dq[d][v]: primitive gradients along x_d.  Only
-// the momentum and energy rows are returned: Fv[(v-1)][d] for v = 1..DIM+1.
-template <int DIM>
-__device__ __forceinline__ void viscous_flux(const double *s, const double (*dq)[DIM + 2], double gm1, double gm1inv,
-                                             double mu, double lambda_k, double Fv[DIM + 1][DIM])
+// constant mu, mu_bulk = 2/3, column `dir` only (flux along x_dir): momentum
+// rows out[0..DIM-1] and the energy row out[DIM].  g(d, v) returns the
+// primitive gradient of variable v along x_d.
+template <int DIM, class Grad>
+__device__ __forceinline__ void viscous_col(const Prim<DIM> &q, const Grad &g, int dir, double gm1inv, double mu,
+                                            double lambda_k, double *out)
 {
-    const double rho = s[0];
-    double vel[DIM], vsq = 0.0;
-#pragma unroll
-    for (int d = 0; d < DIM; d++) {
-        vel[d] = s[1 + d] / rho;
-        vsq += vel[d] * vel[d];
-    }
-    const double p = gm1 * (s[DIM + 1] - 0.5 * rho * vsq);
     double div = 0.0;
 #pragma unroll
-    for (int d = 0; d < DIM; d++) div += dq[d][1 + d];
+    for (int d = 0; d < DIM; d++) div += g(d, 1 + d);
     const double mu_bulk = 2.0 / 3.0;
+    double e = 0.0;
 #pragma unroll
-    for (int j = 0; j < DIM; j++) {      // flux direction
-        double e = 0.0;
-#pragma unroll
-        for (int i = 0; i < DIM; i++) {  // momentum component
-            double tau = (i == j) ? mu * (2.0 * dq[j][1 + i] - mu_bulk * div) : mu * (dq[j][1 + i] + dq[i][1 + j]);
-            Fv[i][j] = tau;
-            e += vel[i] * tau;
-        }
-        const double cv_dT = gm1inv / rho * (dq[j][DIM + 1] - p / rho * dq[j][0]);
-        Fv[DIM][j] = e + lambda_k * cv_dT;
+    for (int i = 0; i < DIM; i++) {
+        const double tau = (i == dir) ? mu * (2.0 * g(dir, 1 + i) - mu_bulk * div) : mu * (g(dir, 1 + i) + g(i, 1 + dir));
+        out[i] = tau;
+        e += q.v[i] * tau;
     }
+    const double cv_dT = gm1inv * q.irho * (g(dir, DIM + 1) - q.p * q.irho * g(dir, 0));
+    out[DIM] = e + lambda_k * cv_dT;
 }
 
-// Conserv2Entropy (BasicOperations.cpp:134-157): beta = rho / p.
+// Conserv2Entropy (BasicOperations.cpp:134-157): beta = rho / p,
+// s = ln p - gamma ln rho.
 template <int DIM>
 __device__ __forceinline__ void entropy_vars(const double *s, double gamma, double gm1, double gm1inv, double *w)
 {
-    const double rho = s[0];
+    const double rho = s[0], irho = 1.0 / rho;
     double vel[DIM], vv = 0.0;
 #pragma unroll
     for (int d = 0; d < DIM; d++) {
-        vel[d] = s[1 + d] / rho;
+        vel[d] = s[1 + d] * irho;
         vv += vel[d] * vel[d];
     }
     const double v_sq = 0.5 * vv;
     const double p = gm1 * (s[DIM + 1] - rho * v_sq);
     const double beta = rho / p;
-    const double sent = log(p * pow(rho, -gamma));
+    const double sent = log(p) - gamma * log(rho);
     w[0] = (gamma - sent) * gm1inv - beta * v_sq;
 #pragma unroll
     for (int d = 0; d < DIM; d++) w[1 + d] = beta * vel[d];
@@ -194,18 +184,18 @@ __device__ __forceinline__ void entropy_vars(const double *s, double gamma, doub
 template <int DIM>
 __device__ __forceinline__ void entgrad_to_primgrad(const double *s, double gm1, double gm1inv, bool compat, double *g)
 {
-    const double rho = s[0];
+    const double rho = s[0], irho = 1.0 / rho;
     double vel[DIM], vv = 0.0;
 #pragma unroll
     for (int d = 0; d < DIM; d++) {
-        vel[d] = s[1 + d] / rho;
+        vel[d] = s[1 + d] * irho;
         vv += vel[d] * vel[d];
     }
     const double v_sq = 0.5 * vv;
     const double p = gm1 * (s[DIM + 1] - rho * v_sq);
     const double KE = v_sq * rho;
     const double gl = g[DIM + 1];
-    const double pr = p / rho;
+    const double pr = p * irho;
     double acc = 0.0;
 #pragma unroll
     for (int d = 0; d < DIM; d++) {
