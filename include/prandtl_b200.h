@@ -167,6 +167,7 @@ int64_t pdg_launch_count(const pdg_ctx *ctx);
 #define PDG_KERNEL_EULER 0   /* Euler RHS / stage kernel */
 #define PDG_KERNEL_LIFT  1   /* BR1 lifting kernel */
 #define PDG_KERNEL_NS    2   /* Navier-Stokes RHS / stage kernel */
+#define PDG_KERNEL_NSFACE 3  /* Navier-Stokes face-flux kernel */
 int pdg_profile_enable(pdg_ctx *ctx, int on);
 int pdg_profile_read(pdg_ctx *ctx, int kind, double *total_ms, int64_t *launches);
 

@@ -30,7 +30,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "_lib", "libprandtl_b200.so")
 
 PDG_OK = 0
-KERNEL_EULER, KERNEL_LIFT, KERNEL_NS = 0, 1, 2
+KERNEL_EULER, KERNEL_LIFT, KERNEL_NS, KERNEL_NSFACE = 0, 1, 2, 3
 PDG_FLAG_NONFINITE = 1
 PDG_FLAG_NONPHYSICAL = 2
 _STATUS = {1: "bad argument", 2: "CUDA error", 3: "non-finite state", 4: "non-physical state",

@@ -37,15 +37,16 @@ struct pdg_ctx {
     int32_t *nbr = nullptr;
     double *eta = nullptr, *alpha = nullptr;
     double *grads = nullptr;
+    double *fbuf = nullptr;                         // NS face contributions
     double *stage_a = nullptr, *stage_b = nullptr;  // RK stage buffers
     double *io_a = nullptr, *io_b = nullptr;        // host-path staging
     unsigned long long *lam_bits = nullptr;
     unsigned int *err = nullptr;
     // launch configuration per kernel kind
-    KernelInfo kinfo[3];
-    int wpb[3];
-    int grid[3];
-    size_t smem[3];
+    KernelInfo kinfo[KIND_COUNT];
+    int wpb[KIND_COUNT];
+    int grid[KIND_COUNT];
+    size_t smem[KIND_COUNT];
     int64_t launches = 0;
     bool profile = false;
     struct TimedLaunch { int kind; cudaEvent_t a, b; };
@@ -234,6 +235,16 @@ int configure_launch(pdg_ctx *c, int kind)
     int dev = c->device, max_smem = 0, sms = 0;
     CK(cudaDeviceGetAttribute(&max_smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev), "device attribute");
     CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev), "device attribute");
+    if (ki.el_doubles == 0) {  // thread-per-face-node kernel
+        int blocks_per_sm = 0;
+        CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks_per_sm, ki.fn, 256, 0), "occupancy");
+        const int nfn = c->dim == 2 ? c->Np : c->Np * c->Np;
+        const int64_t threads = (int64_t)c->dim * c->ne * nfn;
+        c->wpb[kind] = 8;
+        c->grid[kind] = (int)std::max<int64_t>(1, std::min<int64_t>((threads + 255) / 256, (int64_t)sms * std::max(1, blocks_per_sm)));
+        c->smem[kind] = 0;
+        return PDG_OK;
+    }
     const size_t per_warp = (size_t)ki.epw * ki.el_doubles * sizeof(double);
     const size_t base = (size_t)CONST_SLOTS * sizeof(double);
     int wpb = 4;
@@ -330,6 +341,9 @@ int evaluate(pdg_ctx *c, int stage, double dt, const double *un, const double *u
         int r = launch(c, KIND_LIFT, L, s);
         if (r) return r;
         P.grads = c->grads;
+        P.fbuf = c->fbuf;
+        r = launch(c, KIND_NSFACE, P, s);
+        if (r) return r;
         return launch(c, KIND_NS, P, s);
     }
     return launch(c, KIND_EULER, P, s);
@@ -395,13 +409,18 @@ int pdg_create(const pdg_mesh *mesh, const pdg_params *params, pdg_ctx **out)
         cudaMalloc(&c->lam_bits, sizeof(unsigned long long)) || cudaMalloc(&c->err, sizeof(unsigned int)) ||
         cudaMalloc(&c->stage_a, fbytes) || cudaMalloc(&c->stage_b, fbytes))
         return cleanup(PDG_ERR_NOMEM);
-    if (c->p.parabolic && cudaMalloc(&c->grads, fbytes * c->dim) != cudaSuccess) return cleanup(PDG_ERR_NOMEM);
+    if (c->p.parabolic) {
+        const size_t nfn = c->dim == 2 ? c->Np : c->Np * c->Np;
+        if (cudaMalloc(&c->grads, fbytes * c->dim) != cudaSuccess ||
+            cudaMalloc(&c->fbuf, sizeof(double) * c->dim * c->ne * nfn * c->nv) != cudaSuccess)
+            return cleanup(PDG_ERR_NOMEM);
+    }
     if (cudaMemcpy(c->K, &c->hK, sizeof(DevConst), cudaMemcpyHostToDevice) ||
         cudaMemcpy(c->nbr, mesh->nbr, sizeof(int32_t) * c->ne * 2 * c->dim, cudaMemcpyHostToDevice) ||
         cudaMemset(c->eta, 0, sizeof(double) * c->ne) || cudaMemset(c->alpha, 0, sizeof(double) * c->ne) ||
         cudaMemset(c->lam_bits, 0, sizeof(unsigned long long)) || cudaMemset(c->err, 0, sizeof(unsigned int)))
         return cleanup(PDG_ERR_CUDA);
-    for (int kind = 0; kind < 3; kind++) {
+    for (int kind = 0; kind < KIND_COUNT; kind++) {
         if (kind != KIND_EULER && !c->p.parabolic) continue;
         if (kind == KIND_EULER && c->p.parabolic) continue;
         int r = configure_launch(c, kind);
@@ -419,6 +438,7 @@ int pdg_destroy(pdg_ctx *c)
     cudaFree(c->eta);
     cudaFree(c->alpha);
     cudaFree(c->grads);
+    cudaFree(c->fbuf);
     cudaFree(c->stage_a);
     cudaFree(c->stage_b);
     cudaFree(c->io_a);

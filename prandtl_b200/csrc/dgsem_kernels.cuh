@@ -52,6 +52,7 @@ struct KParams {
     double *out;          // dudt (plain) or next stage state
     const double *grads;  // NS: primitive gradients [d][v][node]
     double *grads_out;    // NS lifting output
+    double *fbuf;         // NS face contributions [d][e][face node][v] of the element on the -d side
     const int32_t *nbr;   // [ne][2*dim]
     const DevConst *K;
     double *eta_out, *alpha_out;
@@ -790,6 +791,144 @@ __global__ void __launch_bounds__(128, PDG_MIN_BLOCKS) lift_kernel(const KParams
     if (lane == 0 && flags) atomicOr(P.err, flags);
 }
 
+// Primitive quantities of a state whose momentum slots hold velocities (the
+// reference's NS face states after ComputeViscousFlux divided them in place):
+// velocities v' = v / rho, pressure from E with v', and the derived terms.
+template <int DIM>
+__device__ __forceinline__ Prim<DIM> velocity_slot_prim(const Prim<DIM> &q, double E, double gamma, double gm1,
+                                                        double *mom)
+{
+    Prim<DIM> r;
+    r.rho = q.rho;
+    r.irho = q.irho;
+    double vsq = 0.0;
+#pragma unroll
+    for (int d = 0; d < DIM; d++) {
+        mom[d] = q.v[d];
+        r.v[d] = q.v[d] * q.irho;
+        vsq += r.v[d] * r.v[d];
+    }
+    r.p = gm1 * (E - 0.5 * r.rho * vsq);
+    r.beta = 0.5 * r.rho / r.p;
+    r.ib = 2.0 * r.p * r.irho;
+    r.lam = sqrt(vsq) + sqrt(gamma * r.p * r.irho);
+    return r;
+}
+
+// One Navier-Stokes face node: the face between element a's +D face and its
+// neighbour b's -D face, evaluated once with the element-1 rule (element 1 =
+// the lower-numbered element, normal out of it).  Writes a's contribution
+// C = scale * (-/+ F* +/- Fv.n) (b's contribution is -C) to P.fbuf.
+template <int DIM, int N, int D>
+__device__ __forceinline__ double ns_face_node(const KParams &P, const double *c, int64_t a, int fn)
+{
+    using S = Shape<DIM, N>;
+    constexpr int Np = S::Np, NDOF = S::NDOF, NV = S::NV, NFN = S::NFN;
+    const int64_t size = (int64_t)NV * P.nnodes, nn = P.nnodes;
+    const int64_t b = __ldg(P.nbr + a * 2 * DIM + 2 * D + 1);
+    const int na = line_node<DIM, Np, D>(fn, N), nb = line_node<DIM, Np, D>(fn, 0);
+    double sa[NV], sb[NV];
+#pragma unroll
+    for (int v = 0; v < NV; v++) {
+        sa[v] = __ldg(P.u + v * nn + a * NDOF + na);
+        sb[v] = __ldg(P.u + v * nn + b * NDOF + nb);
+    }
+    const double *ga = P.grads + a * NDOF + na, *gb = P.grads + b * NDOF + nb;
+    auto GA = [&](int d, int v) { return __ldg(ga + d * size + v * nn); };
+    auto GB = [&](int d, int v) { return __ldg(gb + d * size + v * nn); };
+    Prim<DIM> qa = make_prim<DIM>(sa, P.gamma, P.gm1), qb = make_prim<DIM>(sb, P.gamma, P.gm1);
+    double fa[DIM + 1], fb[DIM + 1];
+    viscous_col<DIM>(qa, GA, D, P.gm1inv, P.mu, P.lambda_k, fa);
+    viscous_col<DIM>(qb, GB, D, P.gm1inv, P.mu, P.lambda_k, fb);
+    double ma[DIM], mb[DIM];
+    double lam = 0.0;
+    if (P.compat) {
+        qa = velocity_slot_prim<DIM>(qa, sa[DIM + 1], P.gamma, P.gm1, ma);
+        qb = velocity_slot_prim<DIM>(qb, sb[DIM + 1], P.gamma, P.gm1, mb);
+        lam = fmax(qa.lam, qb.lam);
+    } else {
+#pragma unroll
+        for (int d = 0; d < DIM; d++) {
+            ma[d] = sa[1 + d];
+            mb[d] = sb[1 + d];
+        }
+    }
+    const bool a_is_1 = a <= b;
+    const double nrm = a_is_1 ? C_AREA(c)[D] : -C_AREA(c)[D];
+    double F[NV];
+    if (a_is_1) face_flux<DIM, D>(qa, qb, ma, mb, nrm, P.gm1inv, P.compat != 0, P.diss_scale, F);
+    else face_flux<DIM, D>(qb, qa, mb, ma, nrm, P.gm1inv, P.compat != 0, P.diss_scale, F);
+    const double sc = C_FACE(c);
+    double *dst = P.fbuf + ((D * P.ne + a) * NFN + fn) * NV;
+    dst[0] = sc * (a_is_1 ? -F[0] : F[0]);
+#pragma unroll
+    for (int i = 0; i <= DIM; i++) {
+        const double fvn = ((fa[i] + fb[i]) * 0.5) * nrm;
+        dst[1 + i] = sc * (a_is_1 ? -F[1 + i] + fvn : F[1 + i] - fvn);
+    }
+    return lam;
+}
+
+// Face kernel: one thread per (direction, element, face node), direction
+// slowest so a warp's threads share one direction.
+template <int DIM, int N>
+__global__ void __launch_bounds__(256) ns_face_kernel(const KParams P)
+{
+    using S = Shape<DIM, N>;
+    constexpr int NFN = S::NFN;
+    __shared__ double c[CONST_SLOTS];
+    load_consts(P.K, c, S::Np);
+    __syncthreads();
+    const int64_t per_dir = P.ne * NFN;
+    double lam = 0.0;
+    for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < DIM * per_dir;
+         t += (int64_t)gridDim.x * blockDim.x) {
+        const int d = (int)(t / per_dir);
+        const int64_t r = t - d * per_dir;
+        const int64_t a = r / NFN;
+        const int fn = (int)(r - a * NFN);
+        if (d == 0) lam = fmax(lam, ns_face_node<DIM, N, 0>(P, c, a, fn));
+        else if (d == 1) lam = fmax(lam, ns_face_node<DIM, N, 1>(P, c, a, fn));
+        else lam = fmax(lam, ns_face_node<DIM, N, (DIM == 3 ? 2 : 0)>(P, c, a, fn));
+    }
+    lam = group_max<32>(lam);
+    if ((threadIdx.x & 31) == 0) atomic_max_pos(P.lam_bits, lam);
+}
+
+// Adds the precomputed face contributions to the owned nodes: +C from the
+// element's +d faces (it is their "a" side), -C from its -d faces.
+template <int DIM, int N, int G>
+__device__ __forceinline__ void gather_face_buffer(const KParams &P, int64_t e, bool valid, int gl,
+                                                   double (&acc)[Shape<DIM, N>::NPL][DIM + 2])
+{
+    using S = Shape<DIM, N>;
+    constexpr int Np = S::Np, NDOF = S::NDOF, NV = S::NV, NFN = S::NFN;
+    if (!valid) return;
+#pragma unroll
+    for (int s = 0; s < S::NPL; s++) {
+        const int n = gl + s * G;
+        if (n >= NDOF) break;
+        const int idx[3] = {n % Np, (n / Np) % Np, n / (Np * Np)};
+#pragma unroll
+        for (int d = 0; d < DIM; d++) {
+            const int pos = idx[d];
+            if (pos == 0 || pos == N) {
+                const int line = d == 0 ? (DIM == 2 ? idx[1] : idx[1] + Np * idx[2])
+                                        : (d == 1 ? (DIM == 2 ? idx[0] : idx[0] + Np * idx[2]) : idx[0] + Np * idx[1]);
+                const int64_t owner = pos == N ? e : (int64_t)__ldg(P.nbr + e * 2 * DIM + 2 * d);
+                const double *F = P.fbuf + ((d * P.ne + owner) * NFN + line) * NV;
+                if (pos == N) {
+#pragma unroll
+                    for (int v = 0; v < NV; v++) acc[s][v] += __ldg(F + v);
+                } else {
+#pragma unroll
+                    for (int v = 0; v < NV; v++) acc[s][v] -= __ldg(F + v);
+                }
+            }
+        }
+    }
+}
+
 // dv[s][i] += sum_l Dhat(pos, l) fvc[D][i][line node l] for the owned nodes.
 template <int DIM, int N, int G, int D>
 __device__ __forceinline__ void viscous_divergence_dir(int gl, const double *fvc, const double *c,
@@ -888,9 +1027,7 @@ __global__ void __launch_bounds__(128, PDG_MIN_BLOCKS) ns_rhs_kernel(const KPara
                 acc[s][v] = t * invJ;
             }
         blend_fv<DIM, N, G>(P, alpha, us, pr, buf, c, gl, acc);
-        const double lf = all_faces<DIM, N, G, true>(P, e, valid, gl, us, pr, buf, c);
-        if (valid) lam = fmax(lam, lf);
-        gather_faces<DIM, N, G>(buf, gl, acc);
+        gather_face_buffer<DIM, N, G>(P, e, valid, gl, acc);
         if (valid) store_owned<DIM, N, G>(P, e, gl, us, acc);
         __syncwarp();
     }

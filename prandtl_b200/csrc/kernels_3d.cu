@@ -12,6 +12,7 @@ template <int N> static bool info_n(int kind, KernelInfo *out)
     if (kind == KIND_EULER) { out->fn = (const void *)&euler_rhs_kernel<3, N>; out->el_doubles = S::EL_EULER; }
     else if (kind == KIND_LIFT) { out->fn = (const void *)&lift_kernel<3, N>; out->el_doubles = S::EL_LIFT; }
     else if (kind == KIND_NS) { out->fn = (const void *)&ns_rhs_kernel<3, N>; out->el_doubles = S::EL_NS; }
+    else if (kind == KIND_NSFACE) { out->fn = (const void *)&ns_face_kernel<3, N>; out->el_doubles = 0; }
     else return false;
     return true;
 }
