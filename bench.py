@@ -171,7 +171,7 @@ def run_ours(args):
 
     sampler = ClockSampler(dev.index or 0)
     op.profile(True)
-    for k in (pb.KERNEL_LIFT, pb.KERNEL_NS, pb.KERNEL_NSFACE):
+    for k in (pb.KERNEL_LIFT, pb.KERNEL_NS, pb.KERNEL_FACE_NS, pb.KERNEL_LIFT_FACE):
         op.profile_read(k)
     launches0 = op.launch_count()
     barrier()
@@ -189,7 +189,8 @@ def run_ours(args):
     launches = op.launch_count() - launches0
     ns_ms, ns_n = op.profile_read(pb.KERNEL_NS)
     lift_ms, lift_n = op.profile_read(pb.KERNEL_LIFT)
-    face_ms, face_n = op.profile_read(pb.KERNEL_NSFACE)
+    face_ms, face_n = op.profile_read(pb.KERNEL_FACE_NS)
+    lface_ms, lface_n = op.profile_read(pb.KERNEL_LIFT_FACE)
     op.profile(False)
     op.check()
     if world > 1:
@@ -234,6 +235,7 @@ def run_ours(args):
                 "algorithmic_bytes_per_launch": ns_bytes, "avg_launch_ms": ns_avg,
                 "lift_kernel": {"achieved": lift_gbs, "frac": lift_gbs / peak, "avg_launch_ms": lift_avg,
                                 "algorithmic_bytes_per_launch": lift_bytes},
+                "lift_face_kernel": {"avg_launch_ms": lface_ms / max(lface_n, 1)},
                 "face_kernel": {"avg_launch_ms": face_ms / max(face_n, 1),
                                 "algorithmic_bytes_per_launch": 0,
                                 "note": "face fluxes of the state + gradients the other two kernels stream; "

@@ -145,10 +145,13 @@ int pdg_cfl_dt(pdg_ctx *ctx, double cfl, double *dt_out);
  * copied to HOST arrays of num_elements doubles (either may be NULL). */
 int pdg_get_blending(pdg_ctx *ctx, double *eta_host, double *alpha_host);
 
-/* Primitive-variable gradients of the last parabolic RHS (the reference's
- * dudx/dudy/dudz grid functions after ComputeGlobalPrimitiveGradVector,
- * DGSEMOperator.cpp:134-159), copied to a HOST array of dim*size doubles. */
-int pdg_get_gradients(pdg_ctx *ctx, double *grad_host);
+/* BR1 primitive-variable gradients of a DEVICE state u (the reference's
+ * MultLifting + ComputeGlobalPrimitiveGradVector, DGSEMNonlinearForm.cpp:
+ * 424-645 and DGSEMOperator.cpp:134-159): grads (DEVICE, dim*size doubles)
+ * receives d/dx_d of (rho, u, v[, w], p) in the byNODES layout, direction d
+ * slowest.  The right-hand side computes the same gradients internally and
+ * only keeps the viscous fluxes derived from them. */
+int pdg_gradients(pdg_ctx *ctx, const double *u, double *grads, void *stream);
 
 /* Reads and clears the device error word (PDG_FLAG_*).  Synchronises. */
 int pdg_check(pdg_ctx *ctx, uint32_t *flags);
@@ -164,10 +167,12 @@ int64_t pdg_launch_count(const pdg_ctx *ctx);
  * bracketed by CUDA events on its own stream.  pdg_profile_read synchronises,
  * returns the summed device time (ms) and launch count of one kernel kind
  * (PDG_KERNEL_*) since the last read, and clears that kind's records. */
-#define PDG_KERNEL_EULER 0   /* Euler RHS / stage kernel */
-#define PDG_KERNEL_LIFT  1   /* BR1 lifting kernel */
-#define PDG_KERNEL_NS    2   /* Navier-Stokes RHS / stage kernel */
-#define PDG_KERNEL_NSFACE 3  /* Navier-Stokes face-flux kernel */
+#define PDG_KERNEL_EULER      0  /* Euler volume / stage kernel */
+#define PDG_KERNEL_LIFT       1  /* BR1 lifting + viscous flux kernel */
+#define PDG_KERNEL_NS         2  /* Navier-Stokes volume / stage kernel */
+#define PDG_KERNEL_FACE_NS    3  /* Navier-Stokes face-flux kernel */
+#define PDG_KERNEL_FACE_EULER 4  /* Euler face-flux kernel */
+#define PDG_KERNEL_LIFT_FACE  5  /* BR1 lifting face-jump kernel */
 int pdg_profile_enable(pdg_ctx *ctx, int on);
 int pdg_profile_read(pdg_ctx *ctx, int kind, double *total_ms, int64_t *launches);
 

@@ -30,7 +30,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "_lib", "libprandtl_b200.so")
 
 PDG_OK = 0
-KERNEL_EULER, KERNEL_LIFT, KERNEL_NS, KERNEL_NSFACE = 0, 1, 2, 3
+KERNEL_EULER, KERNEL_LIFT, KERNEL_NS, KERNEL_FACE_NS, KERNEL_FACE_EULER, KERNEL_LIFT_FACE = 0, 1, 2, 3, 4, 5
 PDG_FLAG_NONFINITE = 1
 PDG_FLAG_NONPHYSICAL = 2
 _STATUS = {1: "bad argument", 2: "CUDA error", 3: "non-finite state", 4: "non-physical state",
@@ -81,7 +81,7 @@ def library():
     L.pdg_max_char_speed.argtypes = [C.c_void_p, _dp]
     L.pdg_cfl_dt.argtypes = [C.c_void_p, C.c_double, _dp]
     L.pdg_get_blending.argtypes = [C.c_void_p, _dp, _dp]
-    L.pdg_get_gradients.argtypes = [C.c_void_p, _dp]
+    L.pdg_gradients.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
     L.pdg_check.argtypes = [C.c_void_p, C.POINTER(C.c_uint32)]
     L.pdg_last_error.restype = C.c_char_p
     L.pdg_last_error.argtypes = [C.c_void_p]
@@ -229,9 +229,13 @@ class DGSEMOperator:
                    "pdg_get_blending")
         return eta, alpha
 
-    def gradients(self):
-        g = np.empty(self.mesh.dim * self.size)
-        self._call(library().pdg_get_gradients(self._ctx, g.ctypes.data_as(_dp)), "pdg_get_gradients")
+    def gradients(self, u, stream=None):
+        """BR1 primitive gradients of a device state u: tensor of dim*size doubles."""
+        import torch
+        self._check_dev(u)
+        g = torch.empty(self.mesh.dim * self.size, dtype=u.dtype, device=u.device)
+        self._call(library().pdg_gradients(self._ctx, C.c_void_p(u.data_ptr()), C.c_void_p(g.data_ptr()),
+                                           C.c_void_p(_stream_handle(stream))), "pdg_gradients")
         return g
 
     def check(self) -> int:

@@ -19,7 +19,7 @@
 #include <vector>
 
 #include "../../include/prandtl_b200.h"
-#include "dgsem_kernels.cuh"
+#include "line_kernels.cuh"
 #include "kernel_table.h"
 
 using namespace pdg;
@@ -36,8 +36,10 @@ struct pdg_ctx {
     DevConst *K = nullptr;
     int32_t *nbr = nullptr;
     double *eta = nullptr, *alpha = nullptr;
-    double *grads = nullptr;
-    double *fbuf = nullptr;                         // NS face contributions
+    double *fbuf = nullptr;                         // face contributions [d][e][fn][v]
+    double *lbuf = nullptr;                         // BR1 lifting jumps [d][e][fn][v]
+    double *fvb = nullptr;                          // contravariant viscous fluxes [d][i][node]
+    double *fcol = nullptr;                         // viscous normal columns at faces
     double *stage_a = nullptr, *stage_b = nullptr;  // RK stage buffers
     double *io_a = nullptr, *io_b = nullptr;        // host-path staging
     unsigned long long *lam_bits = nullptr;
@@ -269,6 +271,10 @@ KParams base_params(pdg_ctx *c)
     KParams P;
     std::memset(&P, 0, sizeof(P));
     P.nbr = c->nbr;
+    P.fbuf = c->fbuf;
+    P.lbuf = c->lbuf;
+    P.fv = c->fvb;
+    P.fcol = c->fcol;
     P.K = c->K;
     P.eta_out = c->eta;
     P.alpha_out = c->alpha;
@@ -324,6 +330,18 @@ int launch(pdg_ctx *c, int kind, KParams P, cudaStream_t s)
     return PDG_OK;
 }
 
+// BR1 lifting of state u: face jumps, then gradients and viscous fluxes
+// (gradients also written to grads_out when it is not null).
+int lift(pdg_ctx *c, const double *u, double *grads_out, cudaStream_t s)
+{
+    KParams P = base_params(c);
+    P.u = u;
+    P.grads_out = grads_out;
+    int r = launch(c, KIND_LIFT_FACE, P, s);
+    if (r) return r;
+    return launch(c, KIND_LIFT, P, s);
+}
+
 // RHS (stage < 0) or fused SSP-RK3 stage of the operator on device buffers.
 int evaluate(pdg_ctx *c, int stage, double dt, const double *un, const double *us, double *out, cudaStream_t s)
 {
@@ -335,17 +353,13 @@ int evaluate(pdg_ctx *c, int stage, double dt, const double *un, const double *u
     P.stage = stage;
     P.dt = dt;
     c->last_stream = s;
+    int r;
     if (c->p.parabolic) {
-        KParams L = P;
-        L.grads_out = c->grads;
-        int r = launch(c, KIND_LIFT, L, s);
-        if (r) return r;
-        P.grads = c->grads;
-        P.fbuf = c->fbuf;
-        r = launch(c, KIND_NSFACE, P, s);
-        if (r) return r;
+        if ((r = lift(c, us, nullptr, s))) return r;
+        if ((r = launch(c, KIND_FACE_NS, P, s))) return r;
         return launch(c, KIND_NS, P, s);
     }
+    if ((r = launch(c, KIND_FACE_EULER, P, s))) return r;
     return launch(c, KIND_EULER, P, s);
 }
 
@@ -409,10 +423,14 @@ int pdg_create(const pdg_mesh *mesh, const pdg_params *params, pdg_ctx **out)
         cudaMalloc(&c->lam_bits, sizeof(unsigned long long)) || cudaMalloc(&c->err, sizeof(unsigned int)) ||
         cudaMalloc(&c->stage_a, fbytes) || cudaMalloc(&c->stage_b, fbytes))
         return cleanup(PDG_ERR_NOMEM);
-    if (c->p.parabolic) {
+    {
         const size_t nfn = c->dim == 2 ? c->Np : c->Np * c->Np;
-        if (cudaMalloc(&c->grads, fbytes * c->dim) != cudaSuccess ||
-            cudaMalloc(&c->fbuf, sizeof(double) * c->dim * c->ne * nfn * c->nv) != cudaSuccess)
+        const size_t fdoubles = (size_t)c->dim * c->ne * nfn * c->nv;
+        if (cudaMalloc(&c->fbuf, sizeof(double) * fdoubles) != cudaSuccess) return cleanup(PDG_ERR_NOMEM);
+        if (c->p.parabolic &&
+            (cudaMalloc(&c->lbuf, sizeof(double) * fdoubles) != cudaSuccess ||
+             cudaMalloc(&c->fvb, sizeof(double) * c->dim * (c->nv - 1) * c->nnodes) != cudaSuccess ||
+             cudaMalloc(&c->fcol, sizeof(double) * 2 * c->dim * c->ne * nfn * (c->nv - 1)) != cudaSuccess))
             return cleanup(PDG_ERR_NOMEM);
     }
     if (cudaMemcpy(c->K, &c->hK, sizeof(DevConst), cudaMemcpyHostToDevice) ||
@@ -420,10 +438,12 @@ int pdg_create(const pdg_mesh *mesh, const pdg_params *params, pdg_ctx **out)
         cudaMemset(c->eta, 0, sizeof(double) * c->ne) || cudaMemset(c->alpha, 0, sizeof(double) * c->ne) ||
         cudaMemset(c->lam_bits, 0, sizeof(unsigned long long)) || cudaMemset(c->err, 0, sizeof(unsigned int)))
         return cleanup(PDG_ERR_CUDA);
-    for (int kind = 0; kind < KIND_COUNT; kind++) {
-        if (kind != KIND_EULER && !c->p.parabolic) continue;
-        if (kind == KIND_EULER && c->p.parabolic) continue;
-        int r = configure_launch(c, kind);
+    const int kinds_euler[] = {KIND_FACE_EULER, KIND_EULER};
+    const int kinds_ns[] = {KIND_LIFT_FACE, KIND_LIFT, KIND_FACE_NS, KIND_NS};
+    const int *kinds = c->p.parabolic ? kinds_ns : kinds_euler;
+    const int nk = c->p.parabolic ? 4 : 2;
+    for (int i = 0; i < nk; i++) {
+        int r = configure_launch(c, kinds[i]);
         if (r) return cleanup(r);
     }
     *out = c;
@@ -437,8 +457,10 @@ int pdg_destroy(pdg_ctx *c)
     cudaFree(c->nbr);
     cudaFree(c->eta);
     cudaFree(c->alpha);
-    cudaFree(c->grads);
     cudaFree(c->fbuf);
+    cudaFree(c->lbuf);
+    cudaFree(c->fvb);
+    cudaFree(c->fcol);
     cudaFree(c->stage_a);
     cudaFree(c->stage_b);
     cudaFree(c->io_a);
@@ -582,13 +604,13 @@ int pdg_get_blending(pdg_ctx *c, double *eta_host, double *alpha_host)
     return PDG_OK;
 }
 
-int pdg_get_gradients(pdg_ctx *c, double *grad_host)
+int pdg_gradients(pdg_ctx *c, const double *u, double *grads, void *stream)
 {
-    if (!c || !grad_host) return PDG_ERR_ARG;
-    if (!c->p.parabolic) return fail(c, PDG_ERR_ARG, "pdg_get_gradients: operator is not parabolic");
-    CK(cudaStreamSynchronize(c->last_stream), "synchronize");
-    CK(cudaMemcpy(grad_host, c->grads, sizeof(double) * c->size * c->dim, cudaMemcpyDeviceToHost), "copy gradients");
-    return PDG_OK;
+    if (!c) return PDG_ERR_ARG;
+    if (!c->p.parabolic) return fail(c, PDG_ERR_ARG, "pdg_gradients: operator is not parabolic");
+    if (!u || !grads) return fail(c, PDG_ERR_ARG, "pdg_gradients: null buffer");
+    c->last_stream = (cudaStream_t)stream;
+    return lift(c, u, grads, (cudaStream_t)stream);
 }
 
 int pdg_check(pdg_ctx *c, uint32_t *flags)

@@ -1,7 +1,7 @@
-// kernels_3d.cu — instantiations of the 3D element kernels for N = 1..5
-// and the table the host dispatches through.
-#include "dgsem_kernels.cuh"
+// kernels_3d.cu — instantiations of the 3D kernels for N = 1..5 and the
+// table the host dispatches through.
 #include "kernel_table.h"
+#include "line_kernels.cuh"
 
 namespace pdg {
 
@@ -9,11 +9,16 @@ template <int N> static bool info_n(int kind, KernelInfo *out)
 {
     using S = Shape<3, N>;
     out->epw = S::EPW;
-    if (kind == KIND_EULER) { out->fn = (const void *)&euler_rhs_kernel<3, N>; out->el_doubles = S::EL_EULER; }
-    else if (kind == KIND_LIFT) { out->fn = (const void *)&lift_kernel<3, N>; out->el_doubles = S::EL_LIFT; }
-    else if (kind == KIND_NS) { out->fn = (const void *)&ns_rhs_kernel<3, N>; out->el_doubles = S::EL_NS; }
-    else if (kind == KIND_NSFACE) { out->fn = (const void *)&ns_face_kernel<3, N>; out->el_doubles = 0; }
-    else return false;
+    out->el_doubles = 0;
+    switch (kind) {
+    case KIND_EULER: out->fn = (const void *)&rhs_kernel<3, N, false>; out->el_doubles = S::EL_RHS; break;
+    case KIND_NS: out->fn = (const void *)&rhs_kernel<3, N, true>; out->el_doubles = S::EL_RHS; break;
+    case KIND_LIFT: out->fn = (const void *)&lift_kernel<3, N>; out->el_doubles = S::EL_LIFT; break;
+    case KIND_FACE_NS: out->fn = (const void *)&face_kernel<3, N, true>; break;
+    case KIND_FACE_EULER: out->fn = (const void *)&face_kernel<3, N, false>; break;
+    case KIND_LIFT_FACE: out->fn = (const void *)&lift_face_kernel<3, N>; break;
+    default: return false;
+    }
     return true;
 }
 

@@ -1,0 +1,868 @@
+// line_kernels.cuh — sm_100a FP64 kernels of the DGSEM right-hand side,
+// organised by LGL lines.
+//
+// Work decomposition.  A group of L lanes (L = lines per direction rounded up
+// to a power of two, at most 32) owns one element; a warp holds 32/L
+// elements and synchronises only with __syncwarp.  Volume work is done by
+// line tasks: for each direction the lane that owns a line loads its Np nodes
+// and evaluates every two-point flux of that line (Np(Np-1)/2 independent
+// evaluations, which the scheduler overlaps), sums the line's contributions
+// in registers and adds them to a per-node accumulator in shared memory.
+// Element faces are evaluated once per face node by separate face kernels
+// (one thread per face node) that write the contribution of the element on
+// the -d side, C; the element on the +d side receives -C for the inviscid and
+// viscous fluxes and +C' for the BR1 lifting jump.  Both sides therefore see
+// bit-identical face fluxes.
+//
+// Kernels per right-hand side:
+//   Euler:          face_kernel<false>  ->  rhs_kernel<false>
+//   Navier-Stokes:  lift_face_kernel -> lift_kernel -> face_kernel<true> -> rhs_kernel<true>
+// lift_kernel turns the state into BR1 primitive gradients and from them the
+// viscous fluxes the other kernels need (volume: contravariant, every node;
+// faces: the normal column at every face node), so the gradients themselves
+// never travel through HBM.
+//
+// Reference mapping (paths relative to the reference tree):
+//   indicator + blending   src/Indicators/PerssonPeraireIndicator.cpp:21-58,
+//                          src/Operators/DGSEMOperator.cpp:60-80
+//   subcell FV             src/Integrators/DGSEMIntegrator/DGSEMIntegrator.cpp:972-1196
+//   flux differencing      DGSEMIntegrator.cpp:224-433 (Euler), 601-864 (NS)
+//   faces                  DGSEMIntegrator.cpp:151-222 (Euler), 435-549 (NS)
+//   BR1 lifting            src/Integrators/Lifting/LiftingBR1/LiftingBR1.cpp:10-272
+//   primitive gradients    src/Operators/DGSEMOperator.cpp:82-159
+//   RK stage               RK3SSPSolver::Step as called at src/Simulation/Simulation.cpp:1010
+#pragma once
+
+#include "physics.cuh"
+
+namespace pdg {
+
+constexpr unsigned int PDG_FLAG_NONFINITE_DEV = 1u;
+constexpr unsigned int PDG_FLAG_NONPHYSICAL_DEV = 2u;
+
+// Per-context constants (device memory, copied to shared memory per CTA).
+struct DevConst {
+    double D[36];       // D[i*Np+l] = l'_l(x_i)
+    double Dhat[36];    // D + boundary corrections (viscous volume term)
+    double Dhat2[36];   // 2D + boundary corrections (flux differencing)
+    double Vinv1[36];   // 1D inverse Legendre Vandermonde (modal transform)
+    double w[6];        // GLL weights on [0,1]
+    double snor[3][7];  // subcell interface normals per direction
+    double fv_scale[6]; // 1 / (J w_i)
+    double J, invJ, face_scale;
+    double adj[3], area[3];
+};
+
+// Kernel parameters shared by all kernels.
+struct KParams {
+    const double *u;      // stage input (us)
+    const double *un;     // RK base state (stages 1, 2)
+    double *out;          // dudt (plain) or next stage state
+    double *fbuf;         // face contributions [d][e][face node][v] of the element on the -d side
+    double *lbuf;         // BR1 lifting jumps [d][e][face node][v]
+    double *fv;           // contravariant viscous fluxes [d][i][node], i = momentum rows, energy
+    double *fcol;         // viscous flux normal columns at faces [d][side][e][face node][i]
+    double *grads_out;    // optional: primitive gradients [d][v][node] (diagnostics)
+    const int32_t *nbr;   // [ne][2*dim]
+    const DevConst *K;
+    double *eta_out, *alpha_out;
+    unsigned long long *lam_bits;  // running max wave speed (as ordered bits)
+    unsigned int *err;
+    int64_t ne, nnodes;
+    int64_t nwt;          // number of warp tiles
+    int stage;            // -1: plain RHS; 0, 1, 2: SSP-RK3 stage
+    double dt;
+    double gamma, gm1, gm1inv;
+    double mu, lambda_k;  // NS: mu and mu*gamma/Pr
+    double alpha_max, alpha_min, modal_threshold;
+    double diss_scale;
+    int blending, compat;
+};
+
+constexpr int pow2_at_least(int x) { return x <= 1 ? 1 : x <= 2 ? 2 : x <= 4 ? 4 : x <= 8 ? 8 : x <= 16 ? 16 : 32; }
+
+template <int DIM, int N> struct Shape {
+    static constexpr int Np = N + 1;
+    static constexpr int NDOF = DIM == 2 ? Np * Np : Np * Np * Np;
+    static constexpr int NV = DIM + 2;
+    static constexpr int NFN = DIM == 2 ? Np : Np * Np;  // face nodes = lines per direction
+    static constexpr int L = pow2_at_least(NFN);        // lanes per element
+    static constexpr int EPW = 32 / L;                  // elements per warp
+    static constexpr int NPL = (NDOF + L - 1) / L;      // nodes per lane
+    static constexpr int LPL = (NFN + L - 1) / L;       // lines per lane per direction
+    static constexpr int NPRIM = DIM + 4;               // rho, v[DIM], beta, 1/beta, speed
+    // rhs element slot: primitives, accumulator, scratch (modal transform /
+    // the compat z-fill buffer)
+    static constexpr int SCRATCH = (2 * NDOF > NFN * N * NV) ? 2 * NDOF : NFN * N * NV;
+    static constexpr int EL_RHS = NPRIM * NDOF + NV * NDOF + SCRATCH;
+    // lift element slot: entropy variables, gradients along each direction
+    static constexpr int EL_LIFT = NV * NDOF + DIM * NV * NDOF;
+};
+
+enum { P_RHO = 0, P_V = 1 };
+template <int DIM> struct PSlot {
+    static constexpr int BETA = P_V + DIM, IB = P_V + DIM + 1, LAM = P_V + DIM + 2;
+};
+
+// Node index of position `pos` on line `line` of direction D (x fastest).
+template <int DIM, int Np, int D> __device__ __forceinline__ int line_node(int line, int pos)
+{
+    if (DIM == 2) return D == 0 ? line * Np + pos : pos * Np + line;
+    if (D == 0) return line * Np + pos;
+    if (D == 1) return (line / Np) * Np * Np + pos * Np + (line % Np);
+    return pos * Np * Np + line;
+}
+
+__device__ __forceinline__ void atomic_max_pos(unsigned long long *addr, double v)
+{
+    if (v > 0.0) atomicMax(addr, (unsigned long long)__double_as_longlong(v));
+}
+template <int G> __device__ __forceinline__ double group_sum(double x)
+{
+#pragma unroll
+    for (int o = G / 2; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
+    return x;
+}
+template <int G> __device__ __forceinline__ double group_max(double x)
+{
+#pragma unroll
+    for (int o = G / 2; o > 0; o >>= 1) x = fmax(x, __shfl_xor_sync(0xffffffffu, x, o));
+    return x;
+}
+
+// ---- constants in shared memory ----
+#define C_D(c) (c)
+#define C_DHAT(c) ((c) + 36)
+#define C_DHAT2(c) ((c) + 72)
+#define C_VINV(c) ((c) + 108)
+#define C_W(c) ((c) + 144)
+#define C_SNOR(c, d) ((c) + 150 + 7 * (d))
+#define C_FVS(c) ((c) + 171)
+#define C_ADJ(c) ((c) + 177)
+#define C_AREA(c) ((c) + 180)
+#define C_J(c) ((c)[183])
+#define C_INVJ(c) ((c)[184])
+#define C_FACE(c) ((c)[185])
+constexpr int CONST_SLOTS = 192;
+
+__device__ __forceinline__ void load_consts(const DevConst *K, double *c, int Np)
+{
+    for (int t = threadIdx.x; t < Np * Np; t += blockDim.x) {
+        c[t] = K->D[t];
+        c[36 + t] = K->Dhat[t];
+        c[72 + t] = K->Dhat2[t];
+        c[108 + t] = K->Vinv1[t];
+    }
+    for (int t = threadIdx.x; t < Np; t += blockDim.x) {
+        c[144 + t] = K->w[t];
+        c[171 + t] = K->fv_scale[t];
+    }
+    for (int t = threadIdx.x; t < 3 * 7; t += blockDim.x) c[150 + t] = (&K->snor[0][0])[t];
+    if (threadIdx.x < 3) {
+        c[177 + threadIdx.x] = K->adj[threadIdx.x];
+        c[180 + threadIdx.x] = K->area[threadIdx.x];
+    }
+    if (threadIdx.x == 0) {
+        c[183] = K->J;
+        c[184] = K->invJ;
+        c[185] = K->face_scale;
+    }
+}
+
+// Primitive quantities of a node from the shared slot (p and 1/rho are not
+// kept: the two-point fluxes only need rho, v, beta, 1/beta and the speed).
+template <int DIM> __device__ __forceinline__ Prim<DIM> slot_prim(const double *pr, int n, int NDOF)
+{
+    using PS = PSlot<DIM>;
+    Prim<DIM> q;
+    q.rho = pr[P_RHO * NDOF + n];
+#pragma unroll
+    for (int d = 0; d < DIM; d++) q.v[d] = pr[(P_V + d) * NDOF + n];
+    q.beta = pr[PS::BETA * NDOF + n];
+    q.ib = pr[PS::IB * NDOF + n];
+    q.lam = pr[PS::LAM * NDOF + n];
+    q.p = 0.0;
+    q.irho = 0.0;
+    return q;
+}
+
+__device__ __forceinline__ double blending_alpha(double eta, const KParams &P)
+{
+    const double T = P.modal_threshold;
+    double a = 1.0 / (1.0 + exp(-9.21024 * (eta - T) / T));
+    if (a < P.alpha_min) a = 0.0;
+    else if (a > (1.0 - P.alpha_min)) a = 1.0;
+    return fmin(a, P.alpha_max);
+}
+
+// One 1D pass of the modal transform: dst[line, k] = sum_l Vinv(k,l) src[line, l].
+template <int DIM, int N, int D>
+__device__ __forceinline__ void modal_pass(const double *src, double *dst, int gl, const double *Vinv)
+{
+    using S = Shape<DIM, N>;
+    constexpr int Np = S::Np;
+#pragma unroll
+    for (int r = 0; r < S::LPL; r++) {
+        const int line = gl + r * S::L;
+        if (line < S::NFN) {
+            double x[Np];
+#pragma unroll
+            for (int l = 0; l < Np; l++) x[l] = src[line_node<DIM, Np, D>(line, l)];
+#pragma unroll
+            for (int k = 0; k < Np; k++) {
+                double s = 0.0;
+#pragma unroll
+                for (int l = 0; l < Np; l++) s += Vinv[k * Np + l] * x[l];
+                dst[line_node<DIM, Np, D>(line, k)] = s;
+            }
+        }
+    }
+    __syncwarp();
+}
+
+// Persson-Peraire indicator from q = rho p at the nodes (buf[0..NDOF)):
+// modes = (V1^-1 x ... x V1^-1) q, eta = max(1 - |m1|^2/|m|^2,
+// 1 - |m2|^2/|m1|^2), m1 without modes of 1D degree N, m2 without degree >= N-1.
+template <int DIM, int N>
+__device__ __forceinline__ double indicator_eta(double *buf, int gl, const double *Vinv)
+{
+    using S = Shape<DIM, N>;
+    constexpr int Np = S::Np, NDOF = S::NDOF;
+    double *a = buf, *b = buf + NDOF;
+    modal_pass<DIM, N, 0>(a, b, gl, Vinv);
+    modal_pass<DIM, N, 1>(b, a, gl, Vinv);
+    if (DIM == 3) modal_pass<DIM, N, (DIM == 3 ? 2 : 0)>(a, b, gl, Vinv);
+    const double *m = (DIM == 3) ? b : a;
+    double mm = 0.0, m1 = 0.0, m2 = 0.0;
+#pragma unroll
+    for (int s = 0; s < S::NPL; s++) {
+        const int t = gl + s * S::L;
+        if (t < NDOF) {
+            const int i = t % Np, j = (t / Np) % Np, k = DIM == 3 ? t / (Np * Np) : 0;
+            int mx = i > j ? i : j;
+            if (DIM == 3) mx = mx > k ? mx : k;
+            const double v = m[t] * m[t];
+            mm += v;
+            if (mx <= N - 1) m1 += v;
+            if (mx <= N - 2) m2 += v;
+        }
+    }
+    mm = group_sum<S::L>(mm);
+    m1 = group_sum<S::L>(m1);
+    m2 = group_sum<S::L>(m2);
+    const double eta = 1.0 - m1 / mm;
+    return fmax(eta, 1.0 - m2 / m1);
+}
+
+// Loads the element's nodes, writes their primitives to the shared slot and
+// rho*p to the scratch (indicator input).  Returns this lane's max speed.
+template <int DIM, int N>
+__device__ __forceinline__ double stage_nodes(const KParams &P, int64_t e, bool valid, int gl, double *pr,
+                                              double *scratch, unsigned int &flags)
+{
+    using S = Shape<DIM, N>;
+    using PS = PSlot<DIM>;
+    constexpr int NDOF = S::NDOF, NV = S::NV;
+    double lam = 0.0;
+#pragma unroll
+    for (int k = 0; k < S::NPL; k++) {
+        const int n = gl + k * S::L;
+        if (n < NDOF) {
+            double s[NV];
+#pragma unroll
+            for (int v = 0; v < NV; v++)
+                s[v] = valid ? __ldg(P.u + (int64_t)v * P.nnodes + e * NDOF + n) : (v == 0 ? 1.0 : (v == NV - 1 ? P.gm1inv : 0.0));
+            const Prim<DIM> q = make_prim<DIM>(s, P.gamma, P.gm1);
+            pr[P_RHO * NDOF + n] = q.rho;
+#pragma unroll
+            for (int d = 0; d < DIM; d++) pr[(P_V + d) * NDOF + n] = q.v[d];
+            pr[PS::BETA * NDOF + n] = q.beta;
+            pr[PS::IB * NDOF + n] = q.ib;
+            pr[PS::LAM * NDOF + n] = q.lam;
+            scratch[n] = q.rho * q.p;
+            lam = fmax(lam, q.lam);
+            bool finite = true;
+#pragma unroll
+            for (int v = 0; v < NV; v++) finite = finite && isfinite(s[v]);
+            if (!finite) flags |= PDG_FLAG_NONFINITE_DEV;
+            else if (!(q.rho > 0.0) || !(q.p > 0.0)) flags |= PDG_FLAG_NONPHYSICAL_DEV;
+        }
+    }
+    __syncwarp();
+    return lam;
+}
+
+// Flux-differencing line tasks along direction D: every pair (a < b) of the
+// line is evaluated once and contributes Dhat2(a,b) F to node a and
+// Dhat2(b,a) F to node b; the line sums, scaled by `scale`, are stored
+// (FIRST) or added to acc.  Node a receives its terms in ascending partner
+// order, as the reference's row sum does.
+// Compat NS 3D keeps the reference's z-direction fill (DGSEMIntegrator.cpp:
+// 702): during the y pass (ZFILL_SAVE) the flux of pair (j, N) of y line
+// (i, m) is saved to zf[(i + Np m) * N + j]; during the z pass (ZFILL_USE)
+// node (i, j, k) takes Dhat2(k, m) * zf[(i + Np m) * N + j] (0 when j = N)
+// for its partners m < k instead of the z flux.
+template <int DIM, int N, int D, bool FIRST, bool ZFILL_SAVE, bool ZFILL_USE>
+__device__ __forceinline__ void ec_lines(const KParams &P, const double *pr, double *acc, double *zf,
+                                         const double *c, int gl, double scale)
+{
+    using S = Shape<DIM, N>;
+    constexpr int Np = S::Np, NDOF = S::NDOF, NV = S::NV;
+    const double metric = C_ADJ(c)[D];
+    const double *D2 = C_DHAT2(c);
+#pragma unroll
+    for (int r = 0; r < S::LPL; r++) {
+        const int line = gl + r * S::L;
+        if (line < S::NFN) {
+            Prim<DIM> q[Np];
+#pragma unroll
+            for (int l = 0; l < Np; l++) q[l] = slot_prim<DIM>(pr, line_node<DIM, Np, D>(line, l), NDOF);
+            double la[Np][NV];
+#pragma unroll
+            for (int l = 0; l < Np; l++)
+#pragma unroll
+                for (int v = 0; v < NV; v++) la[l][v] = 0.0;
+#pragma unroll
+            for (int a = 0; a < Np; a++)
+#pragma unroll
+                for (int b = a + 1; b < Np; b++) {
+                    double F[NV];
+                    volume_flux<DIM, D>(q[a], q[b], metric, P.gm1inv, F);
+                    const double cab = D2[a * Np + b], cba = D2[b * Np + a];
+                    if (ZFILL_SAVE && b == N) {
+#pragma unroll
+                        for (int v = 0; v < NV; v++) zf[(line * N + a) * NV + v] = F[v];
+                    }
+#pragma unroll
+                    for (int v = 0; v < NV; v++) {
+                        la[a][v] += cab * F[v];
+                        if (!ZFILL_USE) la[b][v] += cba * F[v];
+                    }
+                }
+            if (ZFILL_USE) {
+                // z line (i, j): node (i, j, k) gets Dhat2(k, m) zf[(i + Np m), j] for m < k
+                const int i = line % Np, j = line / Np;
+                if (j < N) {
+#pragma unroll
+                    for (int k = 1; k < Np; k++)
+#pragma unroll
+                        for (int m = 0; m < k; m++) {
+                            const double ckm = D2[k * Np + m];
+                            const double *F = zf + ((i + Np * m) * N + j) * NV;
+#pragma unroll
+                            for (int v = 0; v < NV; v++) la[k][v] += ckm * F[v];
+                        }
+                }
+            }
+#pragma unroll
+            for (int l = 0; l < Np; l++) {
+                const int n = line_node<DIM, Np, D>(line, l);
+#pragma unroll
+                for (int v = 0; v < NV; v++) {
+                    const double x = scale * la[l][v];
+                    if (FIRST) acc[v * NDOF + n] = x;
+                    else acc[v * NDOF + n] += x;
+                }
+            }
+        }
+    }
+    __syncwarp();
+}
+
+// Subcell finite-volume line tasks along D (ComputeFVFluxes): node l of the
+// line gets alpha (f_{l-1/2} - f_{l+1/2}) / (J w_l), interface fluxes being
+// Chandrashekar face fluxes with the subcell normals.
+template <int DIM, int N, int D>
+__device__ __forceinline__ void fv_lines(const KParams &P, const double *pr, double *acc, const double *c, int gl,
+                                         double alpha)
+{
+    using S = Shape<DIM, N>;
+    constexpr int Np = S::Np, NDOF = S::NDOF, NV = S::NV;
+    const double *sn = C_SNOR(c, D), *fvs = C_FVS(c);
+#pragma unroll
+    for (int r = 0; r < S::LPL; r++) {
+        const int line = gl + r * S::L;
+        if (line < S::NFN) {
+            double prev[NV];
+#pragma unroll
+            for (int v = 0; v < NV; v++) prev[v] = 0.0;
+            Prim<DIM> qa = slot_prim<DIM>(pr, line_node<DIM, Np, D>(line, 0), NDOF);
+#pragma unroll
+            for (int l = 0; l < Np; l++) {
+                const int n = line_node<DIM, Np, D>(line, l);
+                double F[NV];
+                Prim<DIM> qb;
+                if (l < N) {
+                    qb = slot_prim<DIM>(pr, line_node<DIM, Np, D>(line, l + 1), NDOF);
+                    double ma[DIM], mb[DIM];
+#pragma unroll
+                    for (int d = 0; d < DIM; d++) {
+                        ma[d] = qa.rho * qa.v[d];
+                        mb[d] = qb.rho * qb.v[d];
+                    }
+                    face_flux<DIM, D>(qa, qb, ma, mb, sn[l + 1], P.gm1inv, P.compat != 0, P.diss_scale, F);
+                } else {
+#pragma unroll
+                    for (int v = 0; v < NV; v++) F[v] = 0.0;
+                }
+#pragma unroll
+                for (int v = 0; v < NV; v++) {
+                    acc[v * NDOF + n] += alpha * ((prev[v] - F[v]) * fvs[l]);
+                    prev[v] = F[v];
+                }
+                if (l < N) qa = qb;
+            }
+        }
+    }
+    __syncwarp();
+}
+
+// Viscous volume line tasks along D: node l gets
+// invJ * sum_m Dhat(l, m) Fv_D[m] for the momentum and energy rows, with
+// Fv_D the contravariant viscous flux written by lift_kernel.
+template <int DIM, int N, int D>
+__device__ __forceinline__ void viscous_lines(const KParams &P, int64_t e, bool valid, double *acc, const double *c,
+                                              int gl)
+{
+    using S = Shape<DIM, N>;
+    constexpr int Np = S::Np, NDOF = S::NDOF, NV = S::NV;
+    const double *Dh = C_DHAT(c);
+    const double invJ = C_INVJ(c);
+#pragma unroll
+    for (int r = 0; r < S::LPL; r++) {
+        const int line = gl + r * S::L;
+        if (line < S::NFN && valid) {
+            double f[Np][NV - 1];
+#pragma unroll
+            for (int l = 0; l < Np; l++) {
+                const int n = line_node<DIM, Np, D>(line, l);
+#pragma unroll
+                for (int i = 0; i < NV - 1; i++) f[l][i] = __ldg(P.fv + (int64_t)(D * (NV - 1) + i) * P.nnodes + e * NDOF + n);
+            }
+#pragma unroll
+            for (int l = 0; l < Np; l++) {
+                const int n = line_node<DIM, Np, D>(line, l);
+#pragma unroll
+                for (int i = 0; i < NV - 1; i++) {
+                    double s = 0.0;
+#pragma unroll
+                    for (int m = 0; m < Np; m++) s += Dh[l * Np + m] * f[m][i];
+                    acc[(1 + i) * NDOF + n] += invJ * s;
+                }
+            }
+        }
+    }
+    __syncwarp();
+}
+
+// Right-hand side element kernel (Euler or Navier-Stokes volume terms, face
+// buffer gather, optional SSP-RK3 stage).
+template <int DIM, int N, bool NS>
+__global__ void __launch_bounds__(128) rhs_kernel(const KParams P)
+{
+    using S = Shape<DIM, N>;
+    constexpr int Np = S::Np, NDOF = S::NDOF, NV = S::NV, NFN = S::NFN, L = S::L, EPW = S::EPW;
+    extern __shared__ double smem[];
+    double *c = smem;
+    load_consts(P.K, c, Np);
+    __syncthreads();
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int grp = lane / L, gl = lane % L;
+    const int wpb = blockDim.x >> 5;
+    const bool lane_used = grp < EPW;
+    double *pr = smem + CONST_SLOTS + (size_t)(warp * EPW + (lane_used ? grp : 0)) * S::EL_RHS;
+    double *acc = pr + S::NPRIM * NDOF, *scratch = acc + NV * NDOF;
+    const bool compat = P.compat != 0;
+    unsigned int flags = 0;
+    double lam = 0.0;
+    for (int64_t wt = (int64_t)blockIdx.x * wpb + warp; wt < P.nwt; wt += (int64_t)gridDim.x * wpb) {
+        const int64_t e0 = wt * EPW + grp;
+        const bool valid = lane_used && e0 < P.ne;
+        const int64_t e = valid ? e0 : 0;
+        if (lane_used) {
+            const double ls = stage_nodes<DIM, N>(P, e, valid, gl, pr, scratch, flags);
+            if (valid) lam = fmax(lam, ls);
+        }
+        __syncwarp();
+        double alpha = 0.0;
+        if (P.blending) {
+            const double eta = indicator_eta<DIM, N>(scratch, gl, C_VINV(c));
+            alpha = blending_alpha(eta, P);
+            if (valid && gl == 0) {
+                P.eta_out[e] = eta;
+                P.alpha_out[e] = alpha;
+            }
+        }
+        const double sc = -(1.0 - alpha) * C_INVJ(c);
+        if (lane_used) {
+            ec_lines<DIM, N, 0, true, false, false>(P, pr, acc, scratch, c, gl, sc);
+            if (DIM == 3 && NS && compat) {
+                ec_lines<DIM, N, 1, false, true, false>(P, pr, acc, scratch, c, gl, sc);
+                ec_lines<DIM, N, (DIM == 3 ? 2 : 0), false, false, true>(P, pr, acc, scratch, c, gl, sc);
+            } else {
+                ec_lines<DIM, N, 1, false, false, false>(P, pr, acc, scratch, c, gl, sc);
+                if (DIM == 3) ec_lines<DIM, N, (DIM == 3 ? 2 : 0), false, false, false>(P, pr, acc, scratch, c, gl, sc);
+            }
+            if (NS) {
+                viscous_lines<DIM, N, 0>(P, e, valid, acc, c, gl);
+                viscous_lines<DIM, N, 1>(P, e, valid, acc, c, gl);
+                if (DIM == 3) viscous_lines<DIM, N, (DIM == 3 ? 2 : 0)>(P, e, valid, acc, c, gl);
+            }
+        }
+        if (P.blending && __any_sync(0xffffffffu, alpha > 0.0)) {
+            if (lane_used) {
+                fv_lines<DIM, N, 0>(P, pr, acc, c, gl, alpha);
+                fv_lines<DIM, N, 1>(P, pr, acc, c, gl, alpha);
+                if (DIM == 3) fv_lines<DIM, N, (DIM == 3 ? 2 : 0)>(P, pr, acc, c, gl, alpha);
+            }
+        }
+        // faces and store: +C from the element's +d faces, -C from its -d faces
+        if (valid) {
+#pragma unroll
+            for (int k = 0; k < S::NPL; k++) {
+                const int n = gl + k * L;
+                if (n < NDOF) {
+                    double r[NV];
+#pragma unroll
+                    for (int v = 0; v < NV; v++) r[v] = acc[v * NDOF + n];
+                    const int idx[3] = {n % Np, (n / Np) % Np, n / (Np * Np)};
+#pragma unroll
+                    for (int d = 0; d < DIM; d++) {
+                        const int pos = idx[d];
+                        if (pos == 0 || pos == N) {
+                            const int line = d == 0 ? (DIM == 2 ? idx[1] : idx[1] + Np * idx[2])
+                                                    : (d == 1 ? (DIM == 2 ? idx[0] : idx[0] + Np * idx[2]) : idx[0] + Np * idx[1]);
+                            const int64_t owner = pos == N ? e : (int64_t)__ldg(P.nbr + e * 2 * DIM + 2 * d);
+                            const double *F = P.fbuf + ((d * P.ne + owner) * NFN + line) * NV;
+#pragma unroll
+                            for (int v = 0; v < NV; v++) r[v] = pos == N ? r[v] + __ldg(F + v) : r[v] - __ldg(F + v);
+                        }
+                    }
+#pragma unroll
+                    for (int v = 0; v < NV; v++) {
+                        const int64_t gi = (int64_t)v * P.nnodes + e * NDOF + n;
+                        double x = r[v];
+                        if (P.stage >= 0) {
+                            const double z = __ldg(P.u + gi) + P.dt * x;
+                            if (P.stage == 0) x = z;
+                            else if (P.stage == 1) x = 3. / 4 * __ldg(P.un + gi) + 1. / 4 * z;
+                            else x = 1. / 3 * __ldg(P.un + gi) + 2. / 3 * z;
+                        }
+                        P.out[gi] = x;
+                    }
+                }
+            }
+        }
+        __syncwarp();
+    }
+    lam = group_max<32>(lam);
+    if (lane == 0) atomic_max_pos(P.lam_bits, lam);
+    flags = __reduce_or_sync(0xffffffffu, flags);
+    if (lane == 0 && flags) atomicOr(P.err, flags);
+}
+
+// Primitive quantities of a state whose momentum slots hold velocities (the
+// reference's NS face states after ComputeViscousFlux divided them in place):
+// velocities v' = v / rho, pressure from E with v', and the derived terms.
+template <int DIM>
+__device__ __forceinline__ Prim<DIM> velocity_slot_prim(const Prim<DIM> &q, double E, double gamma, double gm1,
+                                                        double *mom)
+{
+    Prim<DIM> r;
+    r.rho = q.rho;
+    r.irho = q.irho;
+    double vsq = 0.0;
+#pragma unroll
+    for (int d = 0; d < DIM; d++) {
+        mom[d] = q.v[d];
+        r.v[d] = q.v[d] * q.irho;
+        vsq += r.v[d] * r.v[d];
+    }
+    r.p = gm1 * (E - 0.5 * r.rho * vsq);
+    r.beta = 0.5 * r.rho / r.p;
+    r.ib = 2.0 * r.p * r.irho;
+    r.lam = sqrt(vsq) + sqrt(gamma * r.p * r.irho);
+    return r;
+}
+
+// One face node: the face between element a's +D face and its neighbour b's
+// -D face, evaluated once with the element-1 rule (element 1 = the
+// lower-numbered element, normal out of it).  Writes a's contribution
+// C = scale * (-/+ F* [+/- Fv.n]) to P.fbuf; b receives -C.  NS adds the
+// central (BR1) viscous flux from the normal columns lift_kernel wrote, and in
+// compat mode evaluates the inviscid flux with velocities in the momentum
+// slots, as the reference does (its ComputeViscousFlux divides the face
+// states' momenta in place before ComputeFaceFlux reads them,
+// BasicOperations.cpp:33-34, DGSEMIntegrator.cpp:467-481).
+template <int DIM, int N, int D, bool NS>
+__device__ __forceinline__ double face_node(const KParams &P, const double *c, int64_t a, int fn)
+{
+    using S = Shape<DIM, N>;
+    constexpr int Np = S::Np, NDOF = S::NDOF, NV = S::NV, NFN = S::NFN;
+    const int64_t nn = P.nnodes;
+    const int64_t b = __ldg(P.nbr + a * 2 * DIM + 2 * D + 1);
+    const int na = line_node<DIM, Np, D>(fn, N), nb = line_node<DIM, Np, D>(fn, 0);
+    double sa[NV], sb[NV];
+#pragma unroll
+    for (int v = 0; v < NV; v++) {
+        sa[v] = __ldg(P.u + v * nn + a * NDOF + na);
+        sb[v] = __ldg(P.u + v * nn + b * NDOF + nb);
+    }
+    Prim<DIM> qa = make_prim<DIM>(sa, P.gamma, P.gm1), qb = make_prim<DIM>(sb, P.gamma, P.gm1);
+    double ma[DIM], mb[DIM];
+    double lam = 0.0;
+    const bool compat = P.compat != 0;
+    if (NS && compat) {
+        qa = velocity_slot_prim<DIM>(qa, sa[DIM + 1], P.gamma, P.gm1, ma);
+        qb = velocity_slot_prim<DIM>(qb, sb[DIM + 1], P.gamma, P.gm1, mb);
+        lam = fmax(qa.lam, qb.lam);
+    } else {
+#pragma unroll
+        for (int d = 0; d < DIM; d++) {
+            ma[d] = sa[1 + d];
+            mb[d] = sb[1 + d];
+        }
+    }
+    const bool a_is_1 = a <= b;
+    const double nrm = a_is_1 ? C_AREA(c)[D] : -C_AREA(c)[D];
+    double F[NV];
+    if (a_is_1) face_flux<DIM, D>(qa, qb, ma, mb, nrm, P.gm1inv, compat, P.diss_scale, F);
+    else face_flux<DIM, D>(qb, qa, mb, ma, nrm, P.gm1inv, compat, P.diss_scale, F);
+    const double sc = C_FACE(c);
+    double *dst = P.fbuf + ((D * P.ne + a) * NFN + fn) * NV;
+    dst[0] = sc * (a_is_1 ? -F[0] : F[0]);
+#pragma unroll
+    for (int i = 0; i <= DIM; i++) {
+        double du = a_is_1 ? -F[1 + i] : F[1 + i];
+        if (NS) {
+            const double fa = __ldg(P.fcol + (((D * 2 + 1) * P.ne + a) * NFN + fn) * (NV - 1) + i);
+            const double fb = __ldg(P.fcol + (((D * 2 + 0) * P.ne + b) * NFN + fn) * (NV - 1) + i);
+            const double fvn = ((fa + fb) * 0.5) * nrm;
+            du = a_is_1 ? du + fvn : du - fvn;
+        }
+        dst[1 + i] = sc * du;
+    }
+    return lam;
+}
+
+// Face kernel: one thread per (direction, element, face node), direction
+// slowest so a warp's threads share one direction.
+template <int DIM, int N, bool NS>
+__global__ void __launch_bounds__(256) face_kernel(const KParams P)
+{
+    using S = Shape<DIM, N>;
+    constexpr int NFN = S::NFN;
+    __shared__ double c[CONST_SLOTS];
+    load_consts(P.K, c, S::Np);
+    __syncthreads();
+    const int64_t per_dir = P.ne * NFN;
+    double lam = 0.0;
+    for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < DIM * per_dir;
+         t += (int64_t)gridDim.x * blockDim.x) {
+        const int d = (int)(t / per_dir);
+        const int64_t r = t - d * per_dir;
+        const int64_t a = r / NFN;
+        const int fn = (int)(r - a * NFN);
+        if (d == 0) lam = fmax(lam, face_node<DIM, N, 0, NS>(P, c, a, fn));
+        else if (d == 1) lam = fmax(lam, face_node<DIM, N, 1, NS>(P, c, a, fn));
+        else lam = fmax(lam, face_node<DIM, N, (DIM == 3 ? 2 : 0), NS>(P, c, a, fn));
+    }
+    lam = group_max<32>(lam);
+    if ((threadIdx.x & 31) == 0) atomic_max_pos(P.lam_bits, lam);
+}
+
+// BR1 lifting face node: 0.5 (w2 - w1) n1_D / (w0 J), the same value for both
+// sides (LiftingBR1.cpp:10-115).  Written to P.lbuf for the -D-side element a.
+template <int DIM, int N, int D>
+__device__ __forceinline__ void lift_face_node(const KParams &P, const double *c, int64_t a, int fn)
+{
+    using S = Shape<DIM, N>;
+    constexpr int Np = S::Np, NDOF = S::NDOF, NV = S::NV, NFN = S::NFN;
+    const int64_t nn = P.nnodes;
+    const int64_t b = __ldg(P.nbr + a * 2 * DIM + 2 * D + 1);
+    const int na = line_node<DIM, Np, D>(fn, N), nb = line_node<DIM, Np, D>(fn, 0);
+    double sa[NV], sb[NV], wa[NV], wb[NV];
+#pragma unroll
+    for (int v = 0; v < NV; v++) {
+        sa[v] = __ldg(P.u + v * nn + a * NDOF + na);
+        sb[v] = __ldg(P.u + v * nn + b * NDOF + nb);
+    }
+    entropy_vars<DIM>(sa, P.gamma, P.gm1, P.gm1inv, wa);
+    entropy_vars<DIM>(sb, P.gamma, P.gm1, P.gm1inv, wb);
+    const bool a_is_1 = a <= b;
+    const double nrm = a_is_1 ? C_AREA(c)[D] : -C_AREA(c)[D];
+    const double sc = C_FACE(c);
+    double *dst = P.lbuf + ((D * P.ne + a) * NFN + fn) * NV;
+#pragma unroll
+    for (int v = 0; v < NV; v++) {
+        const double w1 = a_is_1 ? wa[v] : wb[v], w2 = a_is_1 ? wb[v] : wa[v];
+        dst[v] = sc * ((0.5 * (w2 - w1)) * nrm);
+    }
+}
+
+template <int DIM, int N>
+__global__ void __launch_bounds__(256) lift_face_kernel(const KParams P)
+{
+    using S = Shape<DIM, N>;
+    constexpr int NFN = S::NFN;
+    __shared__ double c[CONST_SLOTS];
+    load_consts(P.K, c, S::Np);
+    __syncthreads();
+    const int64_t per_dir = P.ne * NFN;
+    for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < DIM * per_dir;
+         t += (int64_t)gridDim.x * blockDim.x) {
+        const int d = (int)(t / per_dir);
+        const int64_t r = t - d * per_dir;
+        const int64_t a = r / NFN;
+        const int fn = (int)(r - a * NFN);
+        if (d == 0) lift_face_node<DIM, N, 0>(P, c, a, fn);
+        else if (d == 1) lift_face_node<DIM, N, 1>(P, c, a, fn);
+        else lift_face_node<DIM, N, (DIM == 3 ? 2 : 0)>(P, c, a, fn);
+    }
+}
+
+// Strong-form entropy-variable gradient along D by line tasks:
+// g_D[v][n] = (sum_l D(pos,l) w_l) adj_D / J.
+template <int DIM, int N, int D>
+__device__ __forceinline__ void grad_lines(const double *wv, double *g, const double *c, int gl)
+{
+    using S = Shape<DIM, N>;
+    constexpr int Np = S::Np, NDOF = S::NDOF, NV = S::NV;
+    const double *Dm = C_D(c);
+    const double sc = C_ADJ(c)[D], invJ = C_INVJ(c);
+#pragma unroll
+    for (int r = 0; r < S::LPL; r++) {
+        const int line = gl + r * S::L;
+        if (line < S::NFN) {
+#pragma unroll
+            for (int v = 0; v < NV; v++) {
+                double x[Np];
+#pragma unroll
+                for (int l = 0; l < Np; l++) x[l] = wv[v * NDOF + line_node<DIM, Np, D>(line, l)];
+#pragma unroll
+                for (int p = 0; p < Np; p++) {
+                    double a = 0.0;
+#pragma unroll
+                    for (int l = 0; l < Np; l++) a += Dm[p * Np + l] * x[l];
+                    g[(D * NV + v) * NDOF + line_node<DIM, Np, D>(line, p)] = (a * sc) * invJ;
+                }
+            }
+        }
+    }
+}
+
+// BR1 lifting element kernel: entropy variables, strong-form gradients, face
+// jumps from lbuf, conversion to primitive gradients, then the viscous fluxes:
+// contravariant volume fluxes at every node (with the state of the element's
+// last node in compat mode, as the reference's member id1 gives,
+// DGSEMIntegrator.cpp:620, :770) and the normal column at every face node
+// (with the node's own state, DGSEMIntegrator.cpp:467-477).
+template <int DIM, int N>
+__global__ void __launch_bounds__(128) lift_kernel(const KParams P)
+{
+    using S = Shape<DIM, N>;
+    constexpr int Np = S::Np, NDOF = S::NDOF, NV = S::NV, NFN = S::NFN, L = S::L, EPW = S::EPW;
+    extern __shared__ double smem[];
+    double *c = smem;
+    load_consts(P.K, c, Np);
+    __syncthreads();
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int grp = lane / L, gl = lane % L;
+    const int wpb = blockDim.x >> 5;
+    const bool lane_used = grp < EPW;
+    double *wv = smem + CONST_SLOTS + (size_t)(warp * EPW + (lane_used ? grp : 0)) * S::EL_LIFT;
+    double *g = wv + NV * NDOF;
+    const int64_t nn = P.nnodes;
+    const bool compat = P.compat != 0;
+    unsigned int flags = 0;
+    for (int64_t wt = (int64_t)blockIdx.x * wpb + warp; wt < P.nwt; wt += (int64_t)gridDim.x * wpb) {
+        const int64_t e0 = wt * EPW + grp;
+        const bool valid = lane_used && e0 < P.ne;
+        const int64_t e = valid ? e0 : 0;
+        if (lane_used) {
+#pragma unroll
+            for (int k = 0; k < S::NPL; k++) {
+                const int n = gl + k * L;
+                if (n < NDOF) {
+                    double s[NV], w[NV];
+#pragma unroll
+                    for (int v = 0; v < NV; v++)
+                        s[v] = valid ? __ldg(P.u + v * nn + e * NDOF + n) : (v == 0 ? 1.0 : (v == NV - 1 ? P.gm1inv : 0.0));
+                    entropy_vars<DIM>(s, P.gamma, P.gm1, P.gm1inv, w);
+#pragma unroll
+                    for (int v = 0; v < NV; v++) wv[v * NDOF + n] = w[v];
+                }
+            }
+        }
+        __syncwarp();
+        if (lane_used) {
+            grad_lines<DIM, N, 0>(wv, g, c, gl);
+            grad_lines<DIM, N, 1>(wv, g, c, gl);
+            if (DIM == 3) grad_lines<DIM, N, (DIM == 3 ? 2 : 0)>(wv, g, c, gl);
+        }
+        __syncwarp();
+        if (valid) {
+            // state of the element's last node (compat volume viscous flux)
+            double sl[NV];
+#pragma unroll
+            for (int v = 0; v < NV; v++) sl[v] = __ldg(P.u + v * nn + e * NDOF + NDOF - 1);
+            const Prim<DIM> ql = make_prim<DIM>(sl, P.gamma, P.gm1);
+#pragma unroll 1
+            for (int k = 0; k < S::NPL; k++) {
+                const int n = gl + k * L;
+                if (n >= NDOF) break;
+                double s[NV];
+#pragma unroll
+                for (int v = 0; v < NV; v++) s[v] = __ldg(P.u + v * nn + e * NDOF + n);
+                const int idx[3] = {n % Np, (n / Np) % Np, n / (Np * Np)};
+                double dq[DIM][NV];
+#pragma unroll
+                for (int d = 0; d < DIM; d++) {
+#pragma unroll
+                    for (int v = 0; v < NV; v++) dq[d][v] = g[(d * NV + v) * NDOF + n];
+                    const int pos = idx[d];
+                    if (pos == 0 || pos == N) {
+                        const int line = d == 0 ? (DIM == 2 ? idx[1] : idx[1] + Np * idx[2])
+                                                : (d == 1 ? (DIM == 2 ? idx[0] : idx[0] + Np * idx[2]) : idx[0] + Np * idx[1]);
+                        const int64_t owner = pos == N ? e : (int64_t)__ldg(P.nbr + e * 2 * DIM + 2 * d);
+                        const double *F = P.lbuf + ((d * P.ne + owner) * NFN + line) * NV;
+#pragma unroll
+                        for (int v = 0; v < NV; v++) dq[d][v] += __ldg(F + v);
+                    }
+                    entgrad_to_primgrad<DIM>(s, P.gm1, P.gm1inv, compat, dq[d]);
+#pragma unroll
+                    for (int v = 0; v < NV; v++) {
+                        if (!isfinite(dq[d][v])) flags |= PDG_FLAG_NONFINITE_DEV;
+                        if (P.grads_out) P.grads_out[(int64_t)d * NV * nn + v * nn + e * NDOF + n] = dq[d][v];
+                    }
+                }
+                auto GQ = [&](int d, int v) { return dq[d][v]; };
+                const Prim<DIM> qn = make_prim<DIM>(s, P.gamma, P.gm1);
+                const Prim<DIM> &qv = compat ? ql : qn;
+#pragma unroll
+                for (int d = 0; d < DIM; d++) {
+                    double col[DIM + 1];
+                    viscous_col<DIM>(qv, GQ, d, P.gm1inv, P.mu, P.lambda_k, col);
+                    const double a = C_ADJ(c)[d];
+#pragma unroll
+                    for (int i = 0; i <= DIM; i++) P.fv[(int64_t)(d * (NV - 1) + i) * nn + e * NDOF + n] = a * col[i];
+                    const int pos = idx[d];
+                    if (pos == 0 || pos == N) {
+                        if (compat) viscous_col<DIM>(qn, GQ, d, P.gm1inv, P.mu, P.lambda_k, col);
+                        const int line = d == 0 ? (DIM == 2 ? idx[1] : idx[1] + Np * idx[2])
+                                                : (d == 1 ? (DIM == 2 ? idx[0] : idx[0] + Np * idx[2]) : idx[0] + Np * idx[1]);
+                        const int side = pos == N ? 1 : 0;
+                        double *dst = P.fcol + (((d * 2 + side) * P.ne + e) * NFN + line) * (NV - 1);
+#pragma unroll
+                        for (int i = 0; i <= DIM; i++) dst[i] = col[i];
+                    }
+                }
+            }
+        }
+        __syncwarp();
+    }
+    flags = __reduce_or_sync(0xffffffffu, flags);
+    if (lane == 0 && flags) atomicOr(P.err, flags);
+}
+
+}  // namespace pdg
