@@ -38,7 +38,7 @@ struct pdg_ctx {
     double *eta = nullptr, *alpha = nullptr;
     double *fbuf = nullptr;                         // face contributions [d][e][fn][v]
     double *lbuf = nullptr;                         // BR1 lifting jumps [d][e][fn][v]
-    double *fvb = nullptr;                          // contravariant viscous fluxes [d][i][node]
+    double *fvb = nullptr;                          // viscous volume term [row][node]
     double *fcol = nullptr;                         // viscous normal columns at faces
     double *stage_a = nullptr, *stage_b = nullptr;  // RK stage buffers
     double *io_a = nullptr, *io_b = nullptr;        // host-path staging
@@ -429,7 +429,7 @@ int pdg_create(const pdg_mesh *mesh, const pdg_params *params, pdg_ctx **out)
         if (cudaMalloc(&c->fbuf, sizeof(double) * fdoubles) != cudaSuccess) return cleanup(PDG_ERR_NOMEM);
         if (c->p.parabolic &&
             (cudaMalloc(&c->lbuf, sizeof(double) * fdoubles) != cudaSuccess ||
-             cudaMalloc(&c->fvb, sizeof(double) * c->dim * (c->nv - 1) * c->nnodes) != cudaSuccess ||
+             cudaMalloc(&c->fvb, sizeof(double) * (c->nv - 1) * c->nnodes) != cudaSuccess ||
              cudaMalloc(&c->fcol, sizeof(double) * 2 * c->dim * c->ne * nfn * (c->nv - 1)) != cudaSuccess))
             return cleanup(PDG_ERR_NOMEM);
     }

@@ -18,9 +18,9 @@
 //   Euler:          face_kernel<false>  ->  rhs_kernel<false>
 //   Navier-Stokes:  lift_face_kernel -> lift_kernel -> face_kernel<true> -> rhs_kernel<true>
 // lift_kernel turns the state into BR1 primitive gradients and from them the
-// viscous fluxes the other kernels need (volume: contravariant, every node;
-// faces: the normal column at every face node), so the gradients themselves
-// never travel through HBM.
+// viscous terms the other kernels need (the volume divergence of the viscous
+// flux at every node and its normal column at every face node), so neither
+// the gradients nor the volume viscous fluxes travel through HBM.
 //
 // Reference mapping (paths relative to the reference tree):
 //   indicator + blending   src/Indicators/PerssonPeraireIndicator.cpp:21-58,
@@ -60,7 +60,7 @@ struct KParams {
     double *out;          // dudt (plain) or next stage state
     double *fbuf;         // face contributions [d][e][face node][v] of the element on the -d side
     double *lbuf;         // BR1 lifting jumps [d][e][face node][v]
-    double *fv;           // contravariant viscous fluxes [d][i][node], i = momentum rows, energy
+    double *fv;           // viscous volume term [row][node], rows = momentum, energy (already / J)
     double *fcol;         // viscous flux normal columns at faces [d][side][e][face node][i]
     double *grads_out;    // optional: primitive gradients [d][v][node] (diagnostics)
     const int32_t *nbr;   // [ne][2*dim]
@@ -91,13 +91,28 @@ template <int DIM, int N> struct Shape {
     static constexpr int NPL = (NDOF + L - 1) / L;      // nodes per lane
     static constexpr int LPL = (NFN + L - 1) / L;       // lines per lane per direction
     static constexpr int NPRIM = DIM + 4;               // rho, v[DIM], beta, 1/beta, speed
+    static constexpr int NS_ = NDOF + NDOF / Np;        // padded per-variable stride in shared memory
     // rhs element slot: primitives, accumulator, scratch (modal transform /
     // the compat z-fill buffer)
-    static constexpr int SCRATCH = (2 * NDOF > NFN * N * NV) ? 2 * NDOF : NFN * N * NV;
-    static constexpr int EL_RHS = NPRIM * NDOF + NV * NDOF + SCRATCH;
-    // lift element slot: entropy variables, gradients along each direction
-    static constexpr int EL_LIFT = NV * NDOF + DIM * NV * NDOF;
+    static constexpr int SCRATCH = (2 * NS_ > NFN * N * NV) ? 2 * NS_ : NFN * N * NV;
+    static constexpr int EL_RHS = NPRIM * NS_ + NV * NS_ + SCRATCH;
+    // lift element slot: entropy variables (later the viscous RHS), gradients
+    // along each direction (later the contravariant viscous fluxes)
+    static constexpr int EL_LIFT = NV * NS_ + DIM * NV * NS_;
 };
+
+// Shared-memory position of node n: one padding slot per x line, so that
+// line tasks of every direction read (nearly) distinct banks.
+template <int Np> __device__ __forceinline__ constexpr int sp(int n) { return n + n / Np; }
+
+// Prefetch a byte range into L2 (TMA bulk prefetch); the range is shrunk to
+// whole 16-byte blocks inside it.
+__device__ __forceinline__ void prefetch_l2(const void *p, size_t bytes)
+{
+    const uintptr_t a = (uintptr_t)p;
+    const uintptr_t s = (a + 15) & ~(uintptr_t)15, e = (a + bytes) & ~(uintptr_t)15;
+    if (e > s) asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(s), "r"((unsigned)(e - s)) : "memory");
+}
 
 enum { P_RHO = 0, P_V = 1 };
 template <int DIM> struct PSlot {
@@ -171,16 +186,16 @@ __device__ __forceinline__ void load_consts(const DevConst *K, double *c, int Np
 
 // Primitive quantities of a node from the shared slot (p and 1/rho are not
 // kept: the two-point fluxes only need rho, v, beta, 1/beta and the speed).
-template <int DIM> __device__ __forceinline__ Prim<DIM> slot_prim(const double *pr, int n, int NDOF)
+template <int DIM> __device__ __forceinline__ Prim<DIM> slot_prim(const double *pr, int sn, int ST)
 {
     using PS = PSlot<DIM>;
     Prim<DIM> q;
-    q.rho = pr[P_RHO * NDOF + n];
+    q.rho = pr[P_RHO * ST + sn];
 #pragma unroll
-    for (int d = 0; d < DIM; d++) q.v[d] = pr[(P_V + d) * NDOF + n];
-    q.beta = pr[PS::BETA * NDOF + n];
-    q.ib = pr[PS::IB * NDOF + n];
-    q.lam = pr[PS::LAM * NDOF + n];
+    for (int d = 0; d < DIM; d++) q.v[d] = pr[(P_V + d) * ST + sn];
+    q.beta = pr[PS::BETA * ST + sn];
+    q.ib = pr[PS::IB * ST + sn];
+    q.lam = pr[PS::LAM * ST + sn];
     q.p = 0.0;
     q.irho = 0.0;
     return q;
@@ -207,13 +222,13 @@ __device__ __forceinline__ void modal_pass(const double *src, double *dst, int g
         if (line < S::NFN) {
             double x[Np];
 #pragma unroll
-            for (int l = 0; l < Np; l++) x[l] = src[line_node<DIM, Np, D>(line, l)];
+            for (int l = 0; l < Np; l++) x[l] = src[sp<Np>(line_node<DIM, Np, D>(line, l))];
 #pragma unroll
             for (int k = 0; k < Np; k++) {
                 double s = 0.0;
 #pragma unroll
                 for (int l = 0; l < Np; l++) s += Vinv[k * Np + l] * x[l];
-                dst[line_node<DIM, Np, D>(line, k)] = s;
+                dst[sp<Np>(line_node<DIM, Np, D>(line, k))] = s;
             }
         }
     }
@@ -228,7 +243,7 @@ __device__ __forceinline__ double indicator_eta(double *buf, int gl, const doubl
 {
     using S = Shape<DIM, N>;
     constexpr int Np = S::Np, NDOF = S::NDOF;
-    double *a = buf, *b = buf + NDOF;
+    double *a = buf, *b = buf + S::NS_;
     modal_pass<DIM, N, 0>(a, b, gl, Vinv);
     modal_pass<DIM, N, 1>(b, a, gl, Vinv);
     if (DIM == 3) modal_pass<DIM, N, (DIM == 3 ? 2 : 0)>(a, b, gl, Vinv);
@@ -241,7 +256,7 @@ __device__ __forceinline__ double indicator_eta(double *buf, int gl, const doubl
             const int i = t % Np, j = (t / Np) % Np, k = DIM == 3 ? t / (Np * Np) : 0;
             int mx = i > j ? i : j;
             if (DIM == 3) mx = mx > k ? mx : k;
-            const double v = m[t] * m[t];
+            const double v = m[sp<Np>(t)] * m[sp<Np>(t)];
             mm += v;
             if (mx <= N - 1) m1 += v;
             if (mx <= N - 2) m2 += v;
@@ -273,13 +288,15 @@ __device__ __forceinline__ double stage_nodes(const KParams &P, int64_t e, bool 
             for (int v = 0; v < NV; v++)
                 s[v] = valid ? __ldg(P.u + (int64_t)v * P.nnodes + e * NDOF + n) : (v == 0 ? 1.0 : (v == NV - 1 ? P.gm1inv : 0.0));
             const Prim<DIM> q = make_prim<DIM>(s, P.gamma, P.gm1);
-            pr[P_RHO * NDOF + n] = q.rho;
+            constexpr int ST = S::NS_;
+            const int m = sp<S::Np>(n);
+            pr[P_RHO * ST + m] = q.rho;
 #pragma unroll
-            for (int d = 0; d < DIM; d++) pr[(P_V + d) * NDOF + n] = q.v[d];
-            pr[PS::BETA * NDOF + n] = q.beta;
-            pr[PS::IB * NDOF + n] = q.ib;
-            pr[PS::LAM * NDOF + n] = q.lam;
-            scratch[n] = q.rho * q.p;
+            for (int d = 0; d < DIM; d++) pr[(P_V + d) * ST + m] = q.v[d];
+            pr[PS::BETA * ST + m] = q.beta;
+            pr[PS::IB * ST + m] = q.ib;
+            pr[PS::LAM * ST + m] = q.lam;
+            scratch[m] = q.rho * q.p;
             lam = fmax(lam, q.lam);
             bool finite = true;
 #pragma unroll
@@ -316,7 +333,7 @@ __device__ __forceinline__ void ec_lines(const KParams &P, const double *pr, dou
         if (line < S::NFN) {
             Prim<DIM> q[Np];
 #pragma unroll
-            for (int l = 0; l < Np; l++) q[l] = slot_prim<DIM>(pr, line_node<DIM, Np, D>(line, l), NDOF);
+            for (int l = 0; l < Np; l++) q[l] = slot_prim<DIM>(pr, sp<Np>(line_node<DIM, Np, D>(line, l)), S::NS_);
             double la[Np][NV];
 #pragma unroll
             for (int l = 0; l < Np; l++)
@@ -356,12 +373,12 @@ __device__ __forceinline__ void ec_lines(const KParams &P, const double *pr, dou
             }
 #pragma unroll
             for (int l = 0; l < Np; l++) {
-                const int n = line_node<DIM, Np, D>(line, l);
+                const int n = sp<Np>(line_node<DIM, Np, D>(line, l));
 #pragma unroll
                 for (int v = 0; v < NV; v++) {
                     const double x = scale * la[l][v];
-                    if (FIRST) acc[v * NDOF + n] = x;
-                    else acc[v * NDOF + n] += x;
+                    if (FIRST) acc[v * S::NS_ + n] = x;
+                    else acc[v * S::NS_ + n] += x;
                 }
             }
         }
@@ -386,14 +403,14 @@ __device__ __forceinline__ void fv_lines(const KParams &P, const double *pr, dou
             double prev[NV];
 #pragma unroll
             for (int v = 0; v < NV; v++) prev[v] = 0.0;
-            Prim<DIM> qa = slot_prim<DIM>(pr, line_node<DIM, Np, D>(line, 0), NDOF);
+            Prim<DIM> qa = slot_prim<DIM>(pr, sp<Np>(line_node<DIM, Np, D>(line, 0)), S::NS_);
 #pragma unroll
             for (int l = 0; l < Np; l++) {
-                const int n = line_node<DIM, Np, D>(line, l);
+                const int n = sp<Np>(line_node<DIM, Np, D>(line, l));
                 double F[NV];
                 Prim<DIM> qb;
                 if (l < N) {
-                    qb = slot_prim<DIM>(pr, line_node<DIM, Np, D>(line, l + 1), NDOF);
+                    qb = slot_prim<DIM>(pr, sp<Np>(line_node<DIM, Np, D>(line, l + 1)), S::NS_);
                     double ma[DIM], mb[DIM];
 #pragma unroll
                     for (int d = 0; d < DIM; d++) {
@@ -407,48 +424,10 @@ __device__ __forceinline__ void fv_lines(const KParams &P, const double *pr, dou
                 }
 #pragma unroll
                 for (int v = 0; v < NV; v++) {
-                    acc[v * NDOF + n] += alpha * ((prev[v] - F[v]) * fvs[l]);
+                    acc[v * S::NS_ + n] += alpha * ((prev[v] - F[v]) * fvs[l]);
                     prev[v] = F[v];
                 }
                 if (l < N) qa = qb;
-            }
-        }
-    }
-    __syncwarp();
-}
-
-// Viscous volume line tasks along D: node l gets
-// invJ * sum_m Dhat(l, m) Fv_D[m] for the momentum and energy rows, with
-// Fv_D the contravariant viscous flux written by lift_kernel.
-template <int DIM, int N, int D>
-__device__ __forceinline__ void viscous_lines(const KParams &P, int64_t e, bool valid, double *acc, const double *c,
-                                              int gl)
-{
-    using S = Shape<DIM, N>;
-    constexpr int Np = S::Np, NDOF = S::NDOF, NV = S::NV;
-    const double *Dh = C_DHAT(c);
-    const double invJ = C_INVJ(c);
-#pragma unroll
-    for (int r = 0; r < S::LPL; r++) {
-        const int line = gl + r * S::L;
-        if (line < S::NFN && valid) {
-            double f[Np][NV - 1];
-#pragma unroll
-            for (int l = 0; l < Np; l++) {
-                const int n = line_node<DIM, Np, D>(line, l);
-#pragma unroll
-                for (int i = 0; i < NV - 1; i++) f[l][i] = __ldg(P.fv + (int64_t)(D * (NV - 1) + i) * P.nnodes + e * NDOF + n);
-            }
-#pragma unroll
-            for (int l = 0; l < Np; l++) {
-                const int n = line_node<DIM, Np, D>(line, l);
-#pragma unroll
-                for (int i = 0; i < NV - 1; i++) {
-                    double s = 0.0;
-#pragma unroll
-                    for (int m = 0; m < Np; m++) s += Dh[l * Np + m] * f[m][i];
-                    acc[(1 + i) * NDOF + n] += invJ * s;
-                }
             }
         }
     }
@@ -470,15 +449,30 @@ __global__ void __launch_bounds__(128) rhs_kernel(const KParams P)
     const int grp = lane / L, gl = lane % L;
     const int wpb = blockDim.x >> 5;
     const bool lane_used = grp < EPW;
+    constexpr int ST = S::NS_;
     double *pr = smem + CONST_SLOTS + (size_t)(warp * EPW + (lane_used ? grp : 0)) * S::EL_RHS;
-    double *acc = pr + S::NPRIM * NDOF, *scratch = acc + NV * NDOF;
+    double *acc = pr + S::NPRIM * ST, *scratch = acc + NV * ST;
+    const int64_t wstride = (int64_t)gridDim.x * wpb;
     const bool compat = P.compat != 0;
     unsigned int flags = 0;
     double lam = 0.0;
-    for (int64_t wt = (int64_t)blockIdx.x * wpb + warp; wt < P.nwt; wt += (int64_t)gridDim.x * wpb) {
+    for (int64_t wt = (int64_t)blockIdx.x * wpb + warp; wt < P.nwt; wt += wstride) {
         const int64_t e0 = wt * EPW + grp;
         const bool valid = lane_used && e0 < P.ne;
         const int64_t e = valid ? e0 : 0;
+        {
+            // L2 prefetch of the next element this group will process
+            const int64_t en = (wt + wstride) * EPW + grp;
+            if (lane_used && en < P.ne && gl < NV) {
+                const size_t cb = sizeof(double) * NDOF;
+                prefetch_l2(P.u + (int64_t)gl * P.nnodes + en * NDOF, cb);
+                if (P.stage > 0) prefetch_l2(P.un + (int64_t)gl * P.nnodes + en * NDOF, cb);
+                if (NS && gl < NV - 1) prefetch_l2(P.fv + (int64_t)gl * P.nnodes + en * NDOF, cb);
+            } else if (lane_used && en < P.ne && gl >= NV && gl < NV + DIM) {
+                const int d = gl - NV;
+                prefetch_l2(P.fbuf + ((d * P.ne + en) * NFN) * NV, sizeof(double) * NFN * NV);
+            }
+        }
         if (lane_used) {
             const double ls = stage_nodes<DIM, N>(P, e, valid, gl, pr, scratch, flags);
             if (valid) lam = fmax(lam, ls);
@@ -503,11 +497,6 @@ __global__ void __launch_bounds__(128) rhs_kernel(const KParams P)
                 ec_lines<DIM, N, 1, false, false, false>(P, pr, acc, scratch, c, gl, sc);
                 if (DIM == 3) ec_lines<DIM, N, (DIM == 3 ? 2 : 0), false, false, false>(P, pr, acc, scratch, c, gl, sc);
             }
-            if (NS) {
-                viscous_lines<DIM, N, 0>(P, e, valid, acc, c, gl);
-                viscous_lines<DIM, N, 1>(P, e, valid, acc, c, gl);
-                if (DIM == 3) viscous_lines<DIM, N, (DIM == 3 ? 2 : 0)>(P, e, valid, acc, c, gl);
-            }
         }
         if (P.blending && __any_sync(0xffffffffu, alpha > 0.0)) {
             if (lane_used) {
@@ -524,7 +513,12 @@ __global__ void __launch_bounds__(128) rhs_kernel(const KParams P)
                 if (n < NDOF) {
                     double r[NV];
 #pragma unroll
-                    for (int v = 0; v < NV; v++) r[v] = acc[v * NDOF + n];
+                    for (int v = 0; v < NV; v++) r[v] = acc[v * ST + sp<Np>(n)];
+                    if (NS) {
+                        // viscous volume term (lift_kernel, already divided by J)
+#pragma unroll
+                        for (int i = 0; i < NV - 1; i++) r[1 + i] += __ldg(P.fv + (int64_t)i * P.nnodes + e * NDOF + n);
+                    }
                     const int idx[3] = {n % Np, (n / Np) % Np, n / (Np * Np)};
 #pragma unroll
                     for (int d = 0; d < DIM; d++) {
@@ -727,7 +721,7 @@ template <int DIM, int N, int D>
 __device__ __forceinline__ void grad_lines(const double *wv, double *g, const double *c, int gl)
 {
     using S = Shape<DIM, N>;
-    constexpr int Np = S::Np, NDOF = S::NDOF, NV = S::NV;
+    constexpr int Np = S::Np, NV = S::NV, ST = S::NS_;
     const double *Dm = C_D(c);
     const double sc = C_ADJ(c)[D], invJ = C_INVJ(c);
 #pragma unroll
@@ -738,30 +732,65 @@ __device__ __forceinline__ void grad_lines(const double *wv, double *g, const do
             for (int v = 0; v < NV; v++) {
                 double x[Np];
 #pragma unroll
-                for (int l = 0; l < Np; l++) x[l] = wv[v * NDOF + line_node<DIM, Np, D>(line, l)];
+                for (int l = 0; l < Np; l++) x[l] = wv[v * ST + sp<Np>(line_node<DIM, Np, D>(line, l))];
 #pragma unroll
                 for (int p = 0; p < Np; p++) {
                     double a = 0.0;
 #pragma unroll
                     for (int l = 0; l < Np; l++) a += Dm[p * Np + l] * x[l];
-                    g[(D * NV + v) * NDOF + line_node<DIM, Np, D>(line, p)] = (a * sc) * invJ;
+                    g[(D * NV + v) * ST + sp<Np>(line_node<DIM, Np, D>(line, p))] = (a * sc) * invJ;
                 }
             }
         }
     }
 }
 
+// Viscous volume divergence along D by line tasks: node p of the line gets
+// (1/J) sum_l Dhat(p, l) Fv_D[l] (momentum and energy rows), Fv_D being the
+// contravariant fluxes stored in the gradient slots (slot D*(NV-1)+i).
+template <int DIM, int N, int D, bool FIRST>
+__device__ __forceinline__ void divergence_lines(const double *fvs, double *dv, const double *c, int gl)
+{
+    using S = Shape<DIM, N>;
+    constexpr int Np = S::Np, NV = S::NV, ST = S::NS_;
+    const double *Dh = C_DHAT(c);
+    const double invJ = C_INVJ(c);
+#pragma unroll
+    for (int r = 0; r < S::LPL; r++) {
+        const int line = gl + r * S::L;
+        if (line < S::NFN) {
+#pragma unroll
+            for (int i = 0; i < NV - 1; i++) {
+                double x[Np];
+#pragma unroll
+                for (int l = 0; l < Np; l++) x[l] = fvs[(D * (NV - 1) + i) * ST + sp<Np>(line_node<DIM, Np, D>(line, l))];
+#pragma unroll
+                for (int p = 0; p < Np; p++) {
+                    double a = 0.0;
+#pragma unroll
+                    for (int l = 0; l < Np; l++) a += Dh[p * Np + l] * x[l];
+                    const int m = i * ST + sp<Np>(line_node<DIM, Np, D>(line, p));
+                    if (FIRST) dv[m] = invJ * a;
+                    else dv[m] += invJ * a;
+                }
+            }
+        }
+    }
+    __syncwarp();
+}
+
 // BR1 lifting element kernel: entropy variables, strong-form gradients, face
 // jumps from lbuf, conversion to primitive gradients, then the viscous fluxes:
 // contravariant volume fluxes at every node (with the state of the element's
 // last node in compat mode, as the reference's member id1 gives,
-// DGSEMIntegrator.cpp:620, :770) and the normal column at every face node
-// (with the node's own state, DGSEMIntegrator.cpp:467-477).
+// DGSEMIntegrator.cpp:620, :770), their divergence (the viscous volume term,
+// written to P.fv as [row][node]) and the normal column at every face node
+// (with the node's own state, DGSEMIntegrator.cpp:467-477, written to P.fcol).
 template <int DIM, int N>
 __global__ void __launch_bounds__(128) lift_kernel(const KParams P)
 {
     using S = Shape<DIM, N>;
-    constexpr int Np = S::Np, NDOF = S::NDOF, NV = S::NV, NFN = S::NFN, L = S::L, EPW = S::EPW;
+    constexpr int Np = S::Np, NDOF = S::NDOF, NV = S::NV, NFN = S::NFN, L = S::L, EPW = S::EPW, ST = S::NS_;
     extern __shared__ double smem[];
     double *c = smem;
     load_consts(P.K, c, Np);
@@ -771,14 +800,19 @@ __global__ void __launch_bounds__(128) lift_kernel(const KParams P)
     const int wpb = blockDim.x >> 5;
     const bool lane_used = grp < EPW;
     double *wv = smem + CONST_SLOTS + (size_t)(warp * EPW + (lane_used ? grp : 0)) * S::EL_LIFT;
-    double *g = wv + NV * NDOF;
+    double *g = wv + NV * ST;
     const int64_t nn = P.nnodes;
     const bool compat = P.compat != 0;
+    const int64_t wstride = (int64_t)gridDim.x * wpb;
     unsigned int flags = 0;
-    for (int64_t wt = (int64_t)blockIdx.x * wpb + warp; wt < P.nwt; wt += (int64_t)gridDim.x * wpb) {
+    for (int64_t wt = (int64_t)blockIdx.x * wpb + warp; wt < P.nwt; wt += wstride) {
         const int64_t e0 = wt * EPW + grp;
         const bool valid = lane_used && e0 < P.ne;
         const int64_t e = valid ? e0 : 0;
+        {
+            const int64_t en = (wt + wstride) * EPW + grp;
+            if (lane_used && en < P.ne && gl < NV) prefetch_l2(P.u + (int64_t)gl * nn + en * NDOF, sizeof(double) * NDOF);
+        }
         if (lane_used) {
 #pragma unroll
             for (int k = 0; k < S::NPL; k++) {
@@ -790,7 +824,7 @@ __global__ void __launch_bounds__(128) lift_kernel(const KParams P)
                         s[v] = valid ? __ldg(P.u + v * nn + e * NDOF + n) : (v == 0 ? 1.0 : (v == NV - 1 ? P.gm1inv : 0.0));
                     entropy_vars<DIM>(s, P.gamma, P.gm1, P.gm1inv, w);
 #pragma unroll
-                    for (int v = 0; v < NV; v++) wv[v * NDOF + n] = w[v];
+                    for (int v = 0; v < NV; v++) wv[v * ST + sp<Np>(n)] = w[v];
                 }
             }
         }
@@ -801,27 +835,28 @@ __global__ void __launch_bounds__(128) lift_kernel(const KParams P)
             if (DIM == 3) grad_lines<DIM, N, (DIM == 3 ? 2 : 0)>(wv, g, c, gl);
         }
         __syncwarp();
-        if (valid) {
+        if (lane_used) {
             // state of the element's last node (compat volume viscous flux)
             double sl[NV];
 #pragma unroll
-            for (int v = 0; v < NV; v++) sl[v] = __ldg(P.u + v * nn + e * NDOF + NDOF - 1);
+            for (int v = 0; v < NV; v++) sl[v] = valid ? __ldg(P.u + v * nn + e * NDOF + NDOF - 1) : (v == 0 ? 1.0 : (v == NV - 1 ? P.gm1inv : 0.0));
             const Prim<DIM> ql = make_prim<DIM>(sl, P.gamma, P.gm1);
 #pragma unroll 1
             for (int k = 0; k < S::NPL; k++) {
                 const int n = gl + k * L;
                 if (n >= NDOF) break;
+                const int m = sp<Np>(n);
                 double s[NV];
 #pragma unroll
-                for (int v = 0; v < NV; v++) s[v] = __ldg(P.u + v * nn + e * NDOF + n);
+                for (int v = 0; v < NV; v++) s[v] = valid ? __ldg(P.u + v * nn + e * NDOF + n) : (v == 0 ? 1.0 : (v == NV - 1 ? P.gm1inv : 0.0));
                 const int idx[3] = {n % Np, (n / Np) % Np, n / (Np * Np)};
                 double dq[DIM][NV];
 #pragma unroll
                 for (int d = 0; d < DIM; d++) {
 #pragma unroll
-                    for (int v = 0; v < NV; v++) dq[d][v] = g[(d * NV + v) * NDOF + n];
+                    for (int v = 0; v < NV; v++) dq[d][v] = g[(d * NV + v) * ST + m];
                     const int pos = idx[d];
-                    if (pos == 0 || pos == N) {
+                    if (valid && (pos == 0 || pos == N)) {
                         const int line = d == 0 ? (DIM == 2 ? idx[1] : idx[1] + Np * idx[2])
                                                 : (d == 1 ? (DIM == 2 ? idx[0] : idx[0] + Np * idx[2]) : idx[0] + Np * idx[1]);
                         const int64_t owner = pos == N ? e : (int64_t)__ldg(P.nbr + e * 2 * DIM + 2 * d);
@@ -830,10 +865,12 @@ __global__ void __launch_bounds__(128) lift_kernel(const KParams P)
                         for (int v = 0; v < NV; v++) dq[d][v] += __ldg(F + v);
                     }
                     entgrad_to_primgrad<DIM>(s, P.gm1, P.gm1inv, compat, dq[d]);
+                    if (valid) {
 #pragma unroll
-                    for (int v = 0; v < NV; v++) {
-                        if (!isfinite(dq[d][v])) flags |= PDG_FLAG_NONFINITE_DEV;
-                        if (P.grads_out) P.grads_out[(int64_t)d * NV * nn + v * nn + e * NDOF + n] = dq[d][v];
+                        for (int v = 0; v < NV; v++) {
+                            if (!isfinite(dq[d][v])) flags |= PDG_FLAG_NONFINITE_DEV;
+                            if (P.grads_out) P.grads_out[(int64_t)d * NV * nn + v * nn + e * NDOF + n] = dq[d][v];
+                        }
                     }
                 }
                 auto GQ = [&](int d, int v) { return dq[d][v]; };
@@ -844,10 +881,11 @@ __global__ void __launch_bounds__(128) lift_kernel(const KParams P)
                     double col[DIM + 1];
                     viscous_col<DIM>(qv, GQ, d, P.gm1inv, P.mu, P.lambda_k, col);
                     const double a = C_ADJ(c)[d];
+                    // contravariant flux into the (now consumed) gradient slots of node n
 #pragma unroll
-                    for (int i = 0; i <= DIM; i++) P.fv[(int64_t)(d * (NV - 1) + i) * nn + e * NDOF + n] = a * col[i];
+                    for (int i = 0; i <= DIM; i++) g[(d * (NV - 1) + i) * ST + m] = a * col[i];
                     const int pos = idx[d];
-                    if (pos == 0 || pos == N) {
+                    if (valid && (pos == 0 || pos == N)) {
                         if (compat) viscous_col<DIM>(qn, GQ, d, P.gm1inv, P.mu, P.lambda_k, col);
                         const int line = d == 0 ? (DIM == 2 ? idx[1] : idx[1] + Np * idx[2])
                                                 : (d == 1 ? (DIM == 2 ? idx[0] : idx[0] + Np * idx[2]) : idx[0] + Np * idx[1]);
@@ -856,6 +894,26 @@ __global__ void __launch_bounds__(128) lift_kernel(const KParams P)
 #pragma unroll
                         for (int i = 0; i <= DIM; i++) dst[i] = col[i];
                     }
+                }
+            }
+        }
+        __syncwarp();
+        if (lane_used) {
+            divergence_lines<DIM, N, 0, true>(g, wv, c, gl);
+            divergence_lines<DIM, N, 1, false>(g, wv, c, gl);
+            if (DIM == 3) divergence_lines<DIM, N, (DIM == 3 ? 2 : 0), false>(g, wv, c, gl);
+        } else {
+            __syncwarp();
+            __syncwarp();
+            if (DIM == 3) __syncwarp();
+        }
+        if (valid) {
+#pragma unroll
+            for (int k = 0; k < S::NPL; k++) {
+                const int n = gl + k * L;
+                if (n < NDOF) {
+#pragma unroll
+                    for (int i = 0; i < NV - 1; i++) P.fv[(int64_t)i * nn + e * NDOF + n] = wv[i * ST + sp<Np>(n)];
                 }
             }
         }
