@@ -13,6 +13,7 @@
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <mutex>
 #include <string>
@@ -50,6 +51,7 @@ struct pdg_ctx {
     int grid[KIND_COUNT];
     size_t smem[KIND_COUNT];
     int64_t launches = 0;
+    int prefetch = 1;  // PDG_PREFETCH=0 in the environment turns the L2 prefetch off
     bool profile = false;
     struct TimedLaunch { int kind; cudaEvent_t a, b; };
     std::vector<TimedLaunch> timed;
@@ -294,6 +296,7 @@ KParams base_params(pdg_ctx *c)
     P.diss_scale = c->p.face_dissipation;
     P.blending = c->p.blending;
     P.compat = c->p.compat;
+    P.prefetch = c->prefetch;
     return P;
 }
 
@@ -416,6 +419,7 @@ int pdg_create(const pdg_mesh *mesh, const pdg_params *params, pdg_ctx **out)
         return code;
     };
     if (cudaGetDevice(&c->device) != cudaSuccess) return cleanup(PDG_ERR_CUDA);
+    if (const char *pf = std::getenv("PDG_PREFETCH")) c->prefetch = std::atoi(pf) != 0;
     build_constants(c);
     const size_t fbytes = sizeof(double) * (size_t)c->size;
     if (cudaMalloc(&c->K, sizeof(DevConst)) != cudaSuccess || cudaMalloc(&c->nbr, sizeof(int32_t) * c->ne * 2 * c->dim) ||

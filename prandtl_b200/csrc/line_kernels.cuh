@@ -77,6 +77,7 @@ struct KParams {
     double alpha_max, alpha_min, modal_threshold;
     double diss_scale;
     int blending, compat;
+    int prefetch;         // L2-prefetch the next element's inputs
 };
 
 constexpr int pow2_at_least(int x) { return x <= 1 ? 1 : x <= 2 ? 2 : x <= 4 ? 4 : x <= 8 ? 8 : x <= 16 ? 16 : 32; }
@@ -90,12 +91,13 @@ template <int DIM, int N> struct Shape {
     static constexpr int EPW = 32 / L;                  // elements per warp
     static constexpr int NPL = (NDOF + L - 1) / L;      // nodes per lane
     static constexpr int LPL = (NFN + L - 1) / L;       // lines per lane per direction
-    static constexpr int NPRIM = DIM + 4;               // rho, v[DIM], beta, 1/beta, speed
+    static constexpr int NPRIM = DIM + 2;               // rho, v[DIM], beta
     static constexpr int NS_ = NDOF + NDOF / Np;        // padded per-variable stride in shared memory
-    // rhs element slot: primitives, accumulator, scratch (modal transform /
-    // the compat z-fill buffer)
-    static constexpr int SCRATCH = (2 * NS_ > NFN * N * NV) ? 2 * NS_ : NFN * N * NV;
-    static constexpr int EL_RHS = NPRIM * NS_ + NV * NS_ + SCRATCH;
+    // rhs element slot: primitives, accumulator (which also holds the modal
+    // transform of the indicator before the first flux pass), and the compat
+    // z-fill buffer
+    static constexpr int ZFILL = NFN * N * NV;
+    static constexpr int EL_RHS = NPRIM * NS_ + NV * NS_ + ZFILL;
     // lift element slot: entropy variables (later the viscous RHS), gradients
     // along each direction (later the contravariant viscous fluxes)
     static constexpr int EL_LIFT = NV * NS_ + DIM * NV * NS_;
@@ -116,7 +118,7 @@ __device__ __forceinline__ void prefetch_l2(const void *p, size_t bytes)
 
 enum { P_RHO = 0, P_V = 1 };
 template <int DIM> struct PSlot {
-    static constexpr int BETA = P_V + DIM, IB = P_V + DIM + 1, LAM = P_V + DIM + 2;
+    static constexpr int BETA = P_V + DIM;
 };
 
 // Node index of position `pos` on line `line` of direction D (x fastest).
@@ -194,11 +196,20 @@ template <int DIM> __device__ __forceinline__ Prim<DIM> slot_prim(const double *
 #pragma unroll
     for (int d = 0; d < DIM; d++) q.v[d] = pr[(P_V + d) * ST + sn];
     q.beta = pr[PS::BETA * ST + sn];
-    q.ib = pr[PS::IB * ST + sn];
-    q.lam = pr[PS::LAM * ST + sn];
+    q.ib = 0.0;
+    q.lam = 0.0;
     q.p = 0.0;
     q.irho = 0.0;
     return q;
+}
+// Adds 1/beta and the wave speed |v| + sqrt(gamma p / rho) = |v| + sqrt(gamma / (2 beta)).
+template <int DIM> __device__ __forceinline__ void complete_prim(Prim<DIM> &q, double gamma)
+{
+    double vsq = 0.0;
+#pragma unroll
+    for (int d = 0; d < DIM; d++) vsq += q.v[d] * q.v[d];
+    q.ib = 1.0 / q.beta;
+    q.lam = sqrt(vsq) + sqrt(0.5 * gamma * q.ib);
 }
 
 __device__ __forceinline__ double blending_alpha(double eta, const KParams &P)
@@ -294,8 +305,6 @@ __device__ __forceinline__ double stage_nodes(const KParams &P, int64_t e, bool 
 #pragma unroll
             for (int d = 0; d < DIM; d++) pr[(P_V + d) * ST + m] = q.v[d];
             pr[PS::BETA * ST + m] = q.beta;
-            pr[PS::IB * ST + m] = q.ib;
-            pr[PS::LAM * ST + m] = q.lam;
             scratch[m] = q.rho * q.p;
             lam = fmax(lam, q.lam);
             bool finite = true;
@@ -404,6 +413,7 @@ __device__ __forceinline__ void fv_lines(const KParams &P, const double *pr, dou
 #pragma unroll
             for (int v = 0; v < NV; v++) prev[v] = 0.0;
             Prim<DIM> qa = slot_prim<DIM>(pr, sp<Np>(line_node<DIM, Np, D>(line, 0)), S::NS_);
+            complete_prim<DIM>(qa, P.gamma);
 #pragma unroll
             for (int l = 0; l < Np; l++) {
                 const int n = sp<Np>(line_node<DIM, Np, D>(line, l));
@@ -411,6 +421,7 @@ __device__ __forceinline__ void fv_lines(const KParams &P, const double *pr, dou
                 Prim<DIM> qb;
                 if (l < N) {
                     qb = slot_prim<DIM>(pr, sp<Np>(line_node<DIM, Np, D>(line, l + 1)), S::NS_);
+                    complete_prim<DIM>(qb, P.gamma);
                     double ma[DIM], mb[DIM];
 #pragma unroll
                     for (int d = 0; d < DIM; d++) {
@@ -451,7 +462,7 @@ __global__ void __launch_bounds__(128) rhs_kernel(const KParams P)
     const bool lane_used = grp < EPW;
     constexpr int ST = S::NS_;
     double *pr = smem + CONST_SLOTS + (size_t)(warp * EPW + (lane_used ? grp : 0)) * S::EL_RHS;
-    double *acc = pr + S::NPRIM * ST, *scratch = acc + NV * ST;
+    double *acc = pr + S::NPRIM * ST, *scratch = acc, *zf = acc + NV * ST;
     const int64_t wstride = (int64_t)gridDim.x * wpb;
     const bool compat = P.compat != 0;
     unsigned int flags = 0;
@@ -463,7 +474,8 @@ __global__ void __launch_bounds__(128) rhs_kernel(const KParams P)
         {
             // L2 prefetch of the next element this group will process
             const int64_t en = (wt + wstride) * EPW + grp;
-            if (lane_used && en < P.ne && gl < NV) {
+            if (!P.prefetch) {
+            } else if (lane_used && en < P.ne && gl < NV) {
                 const size_t cb = sizeof(double) * NDOF;
                 prefetch_l2(P.u + (int64_t)gl * P.nnodes + en * NDOF, cb);
                 if (P.stage > 0) prefetch_l2(P.un + (int64_t)gl * P.nnodes + en * NDOF, cb);
@@ -489,13 +501,13 @@ __global__ void __launch_bounds__(128) rhs_kernel(const KParams P)
         }
         const double sc = -(1.0 - alpha) * C_INVJ(c);
         if (lane_used) {
-            ec_lines<DIM, N, 0, true, false, false>(P, pr, acc, scratch, c, gl, sc);
+            ec_lines<DIM, N, 0, true, false, false>(P, pr, acc, zf, c, gl, sc);
             if (DIM == 3 && NS && compat) {
-                ec_lines<DIM, N, 1, false, true, false>(P, pr, acc, scratch, c, gl, sc);
-                ec_lines<DIM, N, (DIM == 3 ? 2 : 0), false, false, true>(P, pr, acc, scratch, c, gl, sc);
+                ec_lines<DIM, N, 1, false, true, false>(P, pr, acc, zf, c, gl, sc);
+                ec_lines<DIM, N, (DIM == 3 ? 2 : 0), false, false, true>(P, pr, acc, zf, c, gl, sc);
             } else {
-                ec_lines<DIM, N, 1, false, false, false>(P, pr, acc, scratch, c, gl, sc);
-                if (DIM == 3) ec_lines<DIM, N, (DIM == 3 ? 2 : 0), false, false, false>(P, pr, acc, scratch, c, gl, sc);
+                ec_lines<DIM, N, 1, false, false, false>(P, pr, acc, zf, c, gl, sc);
+                if (DIM == 3) ec_lines<DIM, N, (DIM == 3 ? 2 : 0), false, false, false>(P, pr, acc, zf, c, gl, sc);
             }
         }
         if (P.blending && __any_sync(0xffffffffu, alpha > 0.0)) {
@@ -811,7 +823,7 @@ __global__ void __launch_bounds__(128) lift_kernel(const KParams P)
         const int64_t e = valid ? e0 : 0;
         {
             const int64_t en = (wt + wstride) * EPW + grp;
-            if (lane_used && en < P.ne && gl < NV) prefetch_l2(P.u + (int64_t)gl * nn + en * NDOF, sizeof(double) * NDOF);
+            if (P.prefetch && lane_used && en < P.ne && gl < NV) prefetch_l2(P.u + (int64_t)gl * nn + en * NDOF, sizeof(double) * NDOF);
         }
         if (lane_used) {
 #pragma unroll
