@@ -171,7 +171,7 @@ def run_ours(args):
 
     sampler = ClockSampler(dev.index or 0)
     op.profile(True)
-    for k in (pb.KERNEL_LIFT, pb.KERNEL_NS, pb.KERNEL_FACE_NS, pb.KERNEL_LIFT_FACE):
+    for k in (pb.KERNEL_LIFT, pb.KERNEL_NS, pb.KERNEL_LIFT_FACE) + pb.KERNEL_FACE_NS:
         op.profile_read(k)
     launches0 = op.launch_count()
     barrier()
@@ -189,7 +189,10 @@ def run_ours(args):
     launches = op.launch_count() - launches0
     ns_ms, ns_n = op.profile_read(pb.KERNEL_NS)
     lift_ms, lift_n = op.profile_read(pb.KERNEL_LIFT)
-    face_ms, face_n = op.profile_read(pb.KERNEL_FACE_NS)
+    face_ms, face_n = 0.0, 0
+    for k in pb.KERNEL_FACE_NS:
+        fm, fnn = op.profile_read(k)
+        face_ms, face_n = face_ms + fm, max(face_n, fnn)
     lface_ms, lface_n = op.profile_read(pb.KERNEL_LIFT_FACE)
     op.profile(False)
     op.check()
@@ -236,10 +239,8 @@ def run_ours(args):
                 "lift_kernel": {"achieved": lift_gbs, "frac": lift_gbs / peak, "avg_launch_ms": lift_avg,
                                 "algorithmic_bytes_per_launch": lift_bytes},
                 "lift_face_kernel": {"avg_launch_ms": lface_ms / max(lface_n, 1)},
-                "face_kernel": {"avg_launch_ms": face_ms / max(face_n, 1),
-                                "algorithmic_bytes_per_launch": 0,
-                                "note": "face fluxes of the state + gradients the other two kernels stream; "
-                                        "its re-reads are counted as traffic, not algorithmic bytes"},
+                "face_kernels": {"avg_ms_per_stage": face_ms / max(face_n, 1),
+                                 "note": "x, y, z face passes adding the face fluxes to the stage output"},
                 "whole_step": {"achieved": step_gbs, "frac": step_gbs / peak, "bytes_per_vdof": 232}}
     out = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
            "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,

@@ -167,12 +167,12 @@ int64_t pdg_launch_count(const pdg_ctx *ctx);
  * bracketed by CUDA events on its own stream.  pdg_profile_read synchronises,
  * returns the summed device time (ms) and launch count of one kernel kind
  * (PDG_KERNEL_*) since the last read, and clears that kind's records. */
-#define PDG_KERNEL_EULER      0  /* Euler volume / stage kernel */
-#define PDG_KERNEL_LIFT       1  /* BR1 lifting + viscous flux kernel */
-#define PDG_KERNEL_NS         2  /* Navier-Stokes volume / stage kernel */
-#define PDG_KERNEL_FACE_NS    3  /* Navier-Stokes face-flux kernel */
-#define PDG_KERNEL_FACE_EULER 4  /* Euler face-flux kernel */
-#define PDG_KERNEL_LIFT_FACE  5  /* BR1 lifting face-jump kernel */
+#define PDG_KERNEL_EULER     0  /* Euler volume (+ stage) kernel */
+#define PDG_KERNEL_LIFT      1  /* BR1 lifting + viscous volume term kernel */
+#define PDG_KERNEL_NS        2  /* Navier-Stokes inviscid volume (+ stage) kernel */
+#define PDG_KERNEL_LIFT_FACE 3  /* BR1 lifting face-jump kernel */
+#define PDG_KERNEL_FACE_E0   4  /* Euler face kernels, x / y / z */
+#define PDG_KERNEL_FACE_NS0  7  /* Navier-Stokes face kernels, x / y / z (7, 8, 9) */
 int pdg_profile_enable(pdg_ctx *ctx, int on);
 int pdg_profile_read(pdg_ctx *ctx, int kind, double *total_ms, int64_t *launches);
 

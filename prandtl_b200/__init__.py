@@ -30,7 +30,9 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "_lib", "libprandtl_b200.so")
 
 PDG_OK = 0
-KERNEL_EULER, KERNEL_LIFT, KERNEL_NS, KERNEL_FACE_NS, KERNEL_FACE_EULER, KERNEL_LIFT_FACE = 0, 1, 2, 3, 4, 5
+KERNEL_EULER, KERNEL_LIFT, KERNEL_NS, KERNEL_LIFT_FACE = 0, 1, 2, 3
+KERNEL_FACE_EULER = (4, 5, 6)
+KERNEL_FACE_NS = (7, 8, 9)
 PDG_FLAG_NONFINITE = 1
 PDG_FLAG_NONPHYSICAL = 2
 _STATUS = {1: "bad argument", 2: "CUDA error", 3: "non-finite state", 4: "non-physical state",

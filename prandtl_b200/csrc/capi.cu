@@ -37,9 +37,7 @@ struct pdg_ctx {
     DevConst *K = nullptr;
     int32_t *nbr = nullptr;
     double *eta = nullptr, *alpha = nullptr;
-    double *fbuf = nullptr;                         // face contributions [d][e][fn][v]
     double *lbuf = nullptr;                         // BR1 lifting jumps [d][e][fn][v]
-    double *fvb = nullptr;                          // viscous volume term [row][node]
     double *fcol = nullptr;                         // viscous normal columns at faces
     double *stage_a = nullptr, *stage_b = nullptr;  // RK stage buffers
     double *io_a = nullptr, *io_b = nullptr;        // host-path staging
@@ -243,7 +241,7 @@ int configure_launch(pdg_ctx *c, int kind)
         int blocks_per_sm = 0;
         CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks_per_sm, ki.fn, 256, 0), "occupancy");
         const int nfn = c->dim == 2 ? c->Np : c->Np * c->Np;
-        const int64_t threads = (int64_t)c->dim * c->ne * nfn;
+        const int64_t threads = (kind == KIND_LIFT_FACE ? (int64_t)c->dim : 1) * c->ne * nfn;
         c->wpb[kind] = 8;
         c->grid[kind] = (int)std::max<int64_t>(1, std::min<int64_t>((threads + 255) / 256, (int64_t)sms * std::max(1, blocks_per_sm)));
         c->smem[kind] = 0;
@@ -273,9 +271,7 @@ KParams base_params(pdg_ctx *c)
     KParams P;
     std::memset(&P, 0, sizeof(P));
     P.nbr = c->nbr;
-    P.fbuf = c->fbuf;
     P.lbuf = c->lbuf;
-    P.fv = c->fvb;
     P.fcol = c->fcol;
     P.K = c->K;
     P.eta_out = c->eta;
@@ -333,11 +329,11 @@ int launch(pdg_ctx *c, int kind, KParams P, cudaStream_t s)
     return PDG_OK;
 }
 
-// BR1 lifting of state u: face jumps, then gradients and viscous fluxes
-// (gradients also written to grads_out when it is not null).
-int lift(pdg_ctx *c, const double *u, double *grads_out, cudaStream_t s)
+// BR1 lifting of state u: face jumps, then gradients (to grads_out when it
+// is not null) and, with P.out set, the viscous volume term added to the
+// output and the face columns of the viscous flux.
+int lift(pdg_ctx *c, KParams P, const double *u, double *grads_out, cudaStream_t s)
 {
-    KParams P = base_params(c);
     P.u = u;
     P.grads_out = grads_out;
     int r = launch(c, KIND_LIFT_FACE, P, s);
@@ -345,7 +341,9 @@ int lift(pdg_ctx *c, const double *u, double *grads_out, cudaStream_t s)
     return launch(c, KIND_LIFT, P, s);
 }
 
-// RHS (stage < 0) or fused SSP-RK3 stage of the operator on device buffers.
+// RHS (stage < 0) or fused SSP-RK3 stage of the operator on device buffers:
+// the volume kernel writes the output, the lifting kernel (NS) and the face
+// kernels of each direction add their terms.
 int evaluate(pdg_ctx *c, int stage, double dt, const double *un, const double *us, double *out, cudaStream_t s)
 {
     if (!c->p.compat) CK(cudaMemsetAsync(c->lam_bits, 0, sizeof(unsigned long long), s), "reset wave speed");
@@ -358,12 +356,18 @@ int evaluate(pdg_ctx *c, int stage, double dt, const double *un, const double *u
     c->last_stream = s;
     int r;
     if (c->p.parabolic) {
-        if ((r = lift(c, us, nullptr, s))) return r;
-        if ((r = launch(c, KIND_FACE_NS, P, s))) return r;
-        return launch(c, KIND_NS, P, s);
+        KParams Lf = P;
+        if ((r = launch(c, KIND_LIFT_FACE, Lf, s))) return r;
+        if ((r = launch(c, KIND_NS, P, s))) return r;
+        if ((r = launch(c, KIND_LIFT, P, s))) return r;
+        for (int d = 0; d < c->dim; d++)
+            if ((r = launch(c, KIND_FACE_NS0 + d, P, s))) return r;
+        return PDG_OK;
     }
-    if ((r = launch(c, KIND_FACE_EULER, P, s))) return r;
-    return launch(c, KIND_EULER, P, s);
+    if ((r = launch(c, KIND_EULER, P, s))) return r;
+    for (int d = 0; d < c->dim; d++)
+        if ((r = launch(c, KIND_FACE_E0 + d, P, s))) return r;
+    return PDG_OK;
 }
 
 }  // namespace
@@ -427,14 +431,10 @@ int pdg_create(const pdg_mesh *mesh, const pdg_params *params, pdg_ctx **out)
         cudaMalloc(&c->lam_bits, sizeof(unsigned long long)) || cudaMalloc(&c->err, sizeof(unsigned int)) ||
         cudaMalloc(&c->stage_a, fbytes) || cudaMalloc(&c->stage_b, fbytes))
         return cleanup(PDG_ERR_NOMEM);
-    {
+    if (c->p.parabolic) {
         const size_t nfn = c->dim == 2 ? c->Np : c->Np * c->Np;
-        const size_t fdoubles = (size_t)c->dim * c->ne * nfn * c->nv;
-        if (cudaMalloc(&c->fbuf, sizeof(double) * fdoubles) != cudaSuccess) return cleanup(PDG_ERR_NOMEM);
-        if (c->p.parabolic &&
-            (cudaMalloc(&c->lbuf, sizeof(double) * fdoubles) != cudaSuccess ||
-             cudaMalloc(&c->fvb, sizeof(double) * (c->nv - 1) * c->nnodes) != cudaSuccess ||
-             cudaMalloc(&c->fcol, sizeof(double) * 2 * c->dim * c->ne * nfn * (c->nv - 1)) != cudaSuccess))
+        if (cudaMalloc(&c->lbuf, sizeof(double) * c->dim * c->ne * nfn * c->nv) != cudaSuccess ||
+            cudaMalloc(&c->fcol, sizeof(double) * 2 * c->dim * c->ne * nfn * (c->nv - 1)) != cudaSuccess)
             return cleanup(PDG_ERR_NOMEM);
     }
     if (cudaMemcpy(c->K, &c->hK, sizeof(DevConst), cudaMemcpyHostToDevice) ||
@@ -442,12 +442,12 @@ int pdg_create(const pdg_mesh *mesh, const pdg_params *params, pdg_ctx **out)
         cudaMemset(c->eta, 0, sizeof(double) * c->ne) || cudaMemset(c->alpha, 0, sizeof(double) * c->ne) ||
         cudaMemset(c->lam_bits, 0, sizeof(unsigned long long)) || cudaMemset(c->err, 0, sizeof(unsigned int)))
         return cleanup(PDG_ERR_CUDA);
-    const int kinds_euler[] = {KIND_FACE_EULER, KIND_EULER};
-    const int kinds_ns[] = {KIND_LIFT_FACE, KIND_LIFT, KIND_FACE_NS, KIND_NS};
-    const int *kinds = c->p.parabolic ? kinds_ns : kinds_euler;
-    const int nk = c->p.parabolic ? 4 : 2;
-    for (int i = 0; i < nk; i++) {
-        int r = configure_launch(c, kinds[i]);
+    for (int kind = 0; kind < KIND_COUNT; kind++) {
+        const bool ns_kind = kind == KIND_NS || kind == KIND_LIFT || kind == KIND_LIFT_FACE ||
+                             (kind >= KIND_FACE_NS0 && kind <= KIND_FACE_NS2);
+        if (ns_kind != (c->p.parabolic != 0)) continue;
+        if ((kind == KIND_FACE_E2 || kind == KIND_FACE_NS2) && c->dim < 3) continue;
+        int r = configure_launch(c, kind);
         if (r) return cleanup(r);
     }
     *out = c;
@@ -461,9 +461,7 @@ int pdg_destroy(pdg_ctx *c)
     cudaFree(c->nbr);
     cudaFree(c->eta);
     cudaFree(c->alpha);
-    cudaFree(c->fbuf);
     cudaFree(c->lbuf);
-    cudaFree(c->fvb);
     cudaFree(c->fcol);
     cudaFree(c->stage_a);
     cudaFree(c->stage_b);
@@ -614,7 +612,9 @@ int pdg_gradients(pdg_ctx *c, const double *u, double *grads, void *stream)
     if (!c->p.parabolic) return fail(c, PDG_ERR_ARG, "pdg_gradients: operator is not parabolic");
     if (!u || !grads) return fail(c, PDG_ERR_ARG, "pdg_gradients: null buffer");
     c->last_stream = (cudaStream_t)stream;
-    return lift(c, u, grads, (cudaStream_t)stream);
+    KParams P = base_params(c);
+    P.out = nullptr;
+    return lift(c, P, u, grads, (cudaStream_t)stream);
 }
 
 int pdg_check(pdg_ctx *c, uint32_t *flags)

@@ -4,13 +4,17 @@
 namespace pdg {
 
 enum KernelKind {
-    KIND_EULER = 0,     // rhs_kernel<dim, N, false>
-    KIND_LIFT = 1,      // lift_kernel<dim, N>
-    KIND_NS = 2,        // rhs_kernel<dim, N, true>
-    KIND_FACE_NS = 3,   // face_kernel<dim, N, true>
-    KIND_FACE_EULER = 4,// face_kernel<dim, N, false>
-    KIND_LIFT_FACE = 5, // lift_face_kernel<dim, N>
-    KIND_COUNT = 6
+    KIND_EULER = 0,      // rhs_kernel<dim, N, false>: Euler volume terms (+ stage)
+    KIND_LIFT = 1,       // lift_kernel<dim, N>: BR1 gradients, viscous volume term, face columns
+    KIND_NS = 2,         // rhs_kernel<dim, N, true>: NS inviscid volume terms (+ stage)
+    KIND_LIFT_FACE = 3,  // lift_face_kernel<dim, N>
+    KIND_FACE_E0 = 4,    // face_kernel<dim, N, d, false>, d = 0, 1, 2
+    KIND_FACE_E1 = 5,
+    KIND_FACE_E2 = 6,
+    KIND_FACE_NS0 = 7,   // face_kernel<dim, N, d, true>, d = 0, 1, 2
+    KIND_FACE_NS1 = 8,
+    KIND_FACE_NS2 = 9,
+    KIND_COUNT = 10
 };
 
 struct KernelInfo {

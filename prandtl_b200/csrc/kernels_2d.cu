@@ -14,9 +14,13 @@ template <int N> static bool info_n(int kind, KernelInfo *out)
     case KIND_EULER: out->fn = (const void *)&rhs_kernel<2, N, false>; out->el_doubles = S::EL_RHS; break;
     case KIND_NS: out->fn = (const void *)&rhs_kernel<2, N, true>; out->el_doubles = S::EL_RHS; break;
     case KIND_LIFT: out->fn = (const void *)&lift_kernel<2, N>; out->el_doubles = S::EL_LIFT; break;
-    case KIND_FACE_NS: out->fn = (const void *)&face_kernel<2, N, true>; break;
-    case KIND_FACE_EULER: out->fn = (const void *)&face_kernel<2, N, false>; break;
     case KIND_LIFT_FACE: out->fn = (const void *)&lift_face_kernel<2, N>; break;
+    case KIND_FACE_E0: out->fn = (const void *)&face_kernel<2, N, 0, false>; break;
+    case KIND_FACE_E1: out->fn = (const void *)&face_kernel<2, N, 1, false>; break;
+    
+    case KIND_FACE_NS0: out->fn = (const void *)&face_kernel<2, N, 0, true>; break;
+    case KIND_FACE_NS1: out->fn = (const void *)&face_kernel<2, N, 1, true>; break;
+    
     default: return false;
     }
     return true;

@@ -9,14 +9,15 @@
 // evaluations, which the scheduler overlaps), sums the line's contributions
 // in registers and adds them to a per-node accumulator in shared memory.
 // Element faces are evaluated once per face node by separate face kernels
-// (one thread per face node) that write the contribution of the element on
-// the -d side, C; the element on the +d side receives -C for the inviscid and
-// viscous fluxes and +C' for the BR1 lifting jump.  Both sides therefore see
-// bit-identical face fluxes.
+// (one thread per face node): the element on the -d side receives C and the
+// one on the +d side -C for the inviscid and viscous fluxes; both receive the
+// same BR1 lifting jump.  Both sides therefore see bit-identical face fluxes.
+// The volume kernel writes the output (RHS or SSP-RK3 stage) and the other
+// kernels add their terms to it, scaled by the stage factor.
 //
 // Kernels per right-hand side:
-//   Euler:          face_kernel<false>  ->  rhs_kernel<false>
-//   Navier-Stokes:  lift_face_kernel -> lift_kernel -> face_kernel<true> -> rhs_kernel<true>
+//   Euler:          rhs_kernel<false> -> face_kernel<x>, <y>[, <z>]
+//   Navier-Stokes:  lift_face_kernel -> rhs_kernel<true> -> lift_kernel -> face_kernel<x>, <y>[, <z>]
 // lift_kernel turns the state into BR1 primitive gradients and from them the
 // viscous terms the other kernels need (the volume divergence of the viscous
 // flux at every node and its normal column at every face node), so neither
@@ -58,9 +59,7 @@ struct KParams {
     const double *u;      // stage input (us)
     const double *un;     // RK base state (stages 1, 2)
     double *out;          // dudt (plain) or next stage state
-    double *fbuf;         // face contributions [d][e][face node][v] of the element on the -d side
     double *lbuf;         // BR1 lifting jumps [d][e][face node][v]
-    double *fv;           // viscous volume term [row][node], rows = momentum, energy (already / J)
     double *fcol;         // viscous flux normal columns at faces [d][side][e][face node][i]
     double *grads_out;    // optional: primitive gradients [d][v][node] (diagnostics)
     const int32_t *nbr;   // [ne][2*dim]
@@ -445,6 +444,26 @@ __device__ __forceinline__ void fv_lines(const KParams &P, const double *pr, dou
     __syncwarp();
 }
 
+// Output of a volume kernel for node value gi with right-hand side x:
+// plain RHS: x; SSP-RK3 stage: z = us + dt x and stage 0: z, 1: 3/4 un + 1/4 z,
+// 2: 1/3 un + 2/3 z (RK3SSPSolver::Step).
+__device__ __forceinline__ double stage_combine(const KParams &P, int64_t gi, double x)
+{
+    if (P.stage < 0) return x;
+    const double z = __ldg(P.u + gi) + P.dt * x;
+    if (P.stage == 0) return z;
+    if (P.stage == 1) return 3. / 4 * __ldg(P.un + gi) + 1. / 4 * z;
+    return 1. / 3 * __ldg(P.un + gi) + 2. / 3 * z;
+}
+// Factor with which a further right-hand-side term enters the output.
+__device__ __forceinline__ double stage_coef(const KParams &P)
+{
+    if (P.stage < 0) return 1.0;
+    if (P.stage == 0) return P.dt;
+    if (P.stage == 1) return 1. / 4 * P.dt;
+    return 2. / 3 * P.dt;
+}
+
 // Right-hand side element kernel (Euler or Navier-Stokes volume terms, face
 // buffer gather, optional SSP-RK3 stage).
 template <int DIM, int N, bool NS>
@@ -471,20 +490,6 @@ __global__ void __launch_bounds__(128) rhs_kernel(const KParams P)
         const int64_t e0 = wt * EPW + grp;
         const bool valid = lane_used && e0 < P.ne;
         const int64_t e = valid ? e0 : 0;
-        {
-            // L2 prefetch of the next element this group will process
-            const int64_t en = (wt + wstride) * EPW + grp;
-            if (!P.prefetch) {
-            } else if (lane_used && en < P.ne && gl < NV) {
-                const size_t cb = sizeof(double) * NDOF;
-                prefetch_l2(P.u + (int64_t)gl * P.nnodes + en * NDOF, cb);
-                if (P.stage > 0) prefetch_l2(P.un + (int64_t)gl * P.nnodes + en * NDOF, cb);
-                if (NS && gl < NV - 1) prefetch_l2(P.fv + (int64_t)gl * P.nnodes + en * NDOF, cb);
-            } else if (lane_used && en < P.ne && gl >= NV && gl < NV + DIM) {
-                const int d = gl - NV;
-                prefetch_l2(P.fbuf + ((d * P.ne + en) * NFN) * NV, sizeof(double) * NFN * NV);
-            }
-        }
         if (lane_used) {
             const double ls = stage_nodes<DIM, N>(P, e, valid, gl, pr, scratch, flags);
             if (valid) lam = fmax(lam, ls);
@@ -517,44 +522,17 @@ __global__ void __launch_bounds__(128) rhs_kernel(const KParams P)
                 if (DIM == 3) fv_lines<DIM, N, (DIM == 3 ? 2 : 0)>(P, pr, acc, c, gl, alpha);
             }
         }
-        // faces and store: +C from the element's +d faces, -C from its -d faces
+        // store: out = a un + b (us + dt V); the viscous volume term and the
+        // face terms are added afterwards by lift_kernel and face_kernel
         if (valid) {
 #pragma unroll
             for (int k = 0; k < S::NPL; k++) {
                 const int n = gl + k * L;
                 if (n < NDOF) {
-                    double r[NV];
-#pragma unroll
-                    for (int v = 0; v < NV; v++) r[v] = acc[v * ST + sp<Np>(n)];
-                    if (NS) {
-                        // viscous volume term (lift_kernel, already divided by J)
-#pragma unroll
-                        for (int i = 0; i < NV - 1; i++) r[1 + i] += __ldg(P.fv + (int64_t)i * P.nnodes + e * NDOF + n);
-                    }
-                    const int idx[3] = {n % Np, (n / Np) % Np, n / (Np * Np)};
-#pragma unroll
-                    for (int d = 0; d < DIM; d++) {
-                        const int pos = idx[d];
-                        if (pos == 0 || pos == N) {
-                            const int line = d == 0 ? (DIM == 2 ? idx[1] : idx[1] + Np * idx[2])
-                                                    : (d == 1 ? (DIM == 2 ? idx[0] : idx[0] + Np * idx[2]) : idx[0] + Np * idx[1]);
-                            const int64_t owner = pos == N ? e : (int64_t)__ldg(P.nbr + e * 2 * DIM + 2 * d);
-                            const double *F = P.fbuf + ((d * P.ne + owner) * NFN + line) * NV;
-#pragma unroll
-                            for (int v = 0; v < NV; v++) r[v] = pos == N ? r[v] + __ldg(F + v) : r[v] - __ldg(F + v);
-                        }
-                    }
 #pragma unroll
                     for (int v = 0; v < NV; v++) {
                         const int64_t gi = (int64_t)v * P.nnodes + e * NDOF + n;
-                        double x = r[v];
-                        if (P.stage >= 0) {
-                            const double z = __ldg(P.u + gi) + P.dt * x;
-                            if (P.stage == 0) x = z;
-                            else if (P.stage == 1) x = 3. / 4 * __ldg(P.un + gi) + 1. / 4 * z;
-                            else x = 1. / 3 * __ldg(P.un + gi) + 2. / 3 * z;
-                        }
-                        P.out[gi] = x;
+                        P.out[gi] = stage_combine(P, gi, acc[v * ST + sp<Np>(n)]);
                     }
                 }
             }
@@ -593,15 +571,16 @@ __device__ __forceinline__ Prim<DIM> velocity_slot_prim(const Prim<DIM> &q, doub
 
 // One face node: the face between element a's +D face and its neighbour b's
 // -D face, evaluated once with the element-1 rule (element 1 = the
-// lower-numbered element, normal out of it).  Writes a's contribution
-// C = scale * (-/+ F* [+/- Fv.n]) to P.fbuf; b receives -C.  NS adds the
-// central (BR1) viscous flux from the normal columns lift_kernel wrote, and in
-// compat mode evaluates the inviscid flux with velocities in the momentum
-// slots, as the reference does (its ComputeViscousFlux divides the face
-// states' momenta in place before ComputeFaceFlux reads them,
+// lower-numbered element, normal out of it).  Element a's contribution is
+// C = scale * (-/+ F* [+/- Fv.n]); b's is -C.  Both are added (times the
+// stage factor) to the output, which the volume kernel has already written.
+// NS adds the central (BR1) viscous flux from the normal columns lift_kernel
+// wrote, and in compat mode evaluates the inviscid flux with velocities in
+// the momentum slots, as the reference does (its ComputeViscousFlux divides
+// the face states' momenta in place before ComputeFaceFlux reads them,
 // BasicOperations.cpp:33-34, DGSEMIntegrator.cpp:467-481).
 template <int DIM, int N, int D, bool NS>
-__device__ __forceinline__ double face_node(const KParams &P, const double *c, int64_t a, int fn)
+__device__ __forceinline__ double face_node(const KParams &P, const double *c, int64_t a, int fn, double coef)
 {
     using S = Shape<DIM, N>;
     constexpr int Np = S::Np, NDOF = S::NDOF, NV = S::NV, NFN = S::NFN;
@@ -613,6 +592,14 @@ __device__ __forceinline__ double face_node(const KParams &P, const double *c, i
     for (int v = 0; v < NV; v++) {
         sa[v] = __ldg(P.u + v * nn + a * NDOF + na);
         sb[v] = __ldg(P.u + v * nn + b * NDOF + nb);
+    }
+    double fa[DIM + 1], fb[DIM + 1];
+    if (NS) {
+#pragma unroll
+        for (int i = 0; i <= DIM; i++) {
+            fa[i] = __ldg(P.fcol + (((D * 2 + 1) * P.ne + a) * NFN + fn) * (NV - 1) + i);
+            fb[i] = __ldg(P.fcol + (((D * 2 + 0) * P.ne + b) * NFN + fn) * (NV - 1) + i);
+        }
     }
     Prim<DIM> qa = make_prim<DIM>(sa, P.gamma, P.gm1), qb = make_prim<DIM>(sb, P.gamma, P.gm1);
     double ma[DIM], mb[DIM];
@@ -634,26 +621,30 @@ __device__ __forceinline__ double face_node(const KParams &P, const double *c, i
     double F[NV];
     if (a_is_1) face_flux<DIM, D>(qa, qb, ma, mb, nrm, P.gm1inv, compat, P.diss_scale, F);
     else face_flux<DIM, D>(qb, qa, mb, ma, nrm, P.gm1inv, compat, P.diss_scale, F);
-    const double sc = C_FACE(c);
-    double *dst = P.fbuf + ((D * P.ne + a) * NFN + fn) * NV;
-    dst[0] = sc * (a_is_1 ? -F[0] : F[0]);
+    const double sc = C_FACE(c) * coef;
+    double C[NV];
+    C[0] = sc * (a_is_1 ? -F[0] : F[0]);
 #pragma unroll
     for (int i = 0; i <= DIM; i++) {
         double du = a_is_1 ? -F[1 + i] : F[1 + i];
         if (NS) {
-            const double fa = __ldg(P.fcol + (((D * 2 + 1) * P.ne + a) * NFN + fn) * (NV - 1) + i);
-            const double fb = __ldg(P.fcol + (((D * 2 + 0) * P.ne + b) * NFN + fn) * (NV - 1) + i);
-            const double fvn = ((fa + fb) * 0.5) * nrm;
+            const double fvn = ((fa[i] + fb[i]) * 0.5) * nrm;
             du = a_is_1 ? du + fvn : du - fvn;
         }
-        dst[1 + i] = sc * du;
+        C[1 + i] = sc * du;
+    }
+#pragma unroll
+    for (int v = 0; v < NV; v++) {
+        P.out[v * nn + a * NDOF + na] += C[v];
+        P.out[v * nn + b * NDOF + nb] -= C[v];
     }
     return lam;
 }
 
-// Face kernel: one thread per (direction, element, face node), direction
-// slowest so a warp's threads share one direction.
-template <int DIM, int N, bool NS>
+// Face kernel of direction D: one thread per (element, face node).  Within one
+// direction every output entry belongs to exactly one face, so the
+// read-modify-write updates need no atomics.
+template <int DIM, int N, int D, bool NS>
 __global__ void __launch_bounds__(256) face_kernel(const KParams P)
 {
     using S = Shape<DIM, N>;
@@ -661,17 +652,13 @@ __global__ void __launch_bounds__(256) face_kernel(const KParams P)
     __shared__ double c[CONST_SLOTS];
     load_consts(P.K, c, S::Np);
     __syncthreads();
-    const int64_t per_dir = P.ne * NFN;
+    const double coef = stage_coef(P);
     double lam = 0.0;
-    for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < DIM * per_dir;
+    for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < P.ne * NFN;
          t += (int64_t)gridDim.x * blockDim.x) {
-        const int d = (int)(t / per_dir);
-        const int64_t r = t - d * per_dir;
-        const int64_t a = r / NFN;
-        const int fn = (int)(r - a * NFN);
-        if (d == 0) lam = fmax(lam, face_node<DIM, N, 0, NS>(P, c, a, fn));
-        else if (d == 1) lam = fmax(lam, face_node<DIM, N, 1, NS>(P, c, a, fn));
-        else lam = fmax(lam, face_node<DIM, N, (DIM == 3 ? 2 : 0), NS>(P, c, a, fn));
+        const int64_t a = t / NFN;
+        const int fn = (int)(t - a * NFN);
+        lam = fmax(lam, face_node<DIM, N, D, NS>(P, c, a, fn, coef));
     }
     lam = group_max<32>(lam);
     if ((threadIdx.x & 31) == 0) atomic_max_pos(P.lam_bits, lam);
@@ -796,8 +783,9 @@ __device__ __forceinline__ void divergence_lines(const double *fvs, double *dv, 
 // contravariant volume fluxes at every node (with the state of the element's
 // last node in compat mode, as the reference's member id1 gives,
 // DGSEMIntegrator.cpp:620, :770), their divergence (the viscous volume term,
-// written to P.fv as [row][node]) and the normal column at every face node
-// (with the node's own state, DGSEMIntegrator.cpp:467-477, written to P.fcol).
+// added to the output the volume kernel wrote, times the stage factor) and the
+// normal column at every face node (with the node's own state,
+// DGSEMIntegrator.cpp:467-477, written to P.fcol).
 template <int DIM, int N>
 __global__ void __launch_bounds__(128) lift_kernel(const KParams P)
 {
@@ -919,13 +907,14 @@ __global__ void __launch_bounds__(128) lift_kernel(const KParams P)
             __syncwarp();
             if (DIM == 3) __syncwarp();
         }
-        if (valid) {
+        if (valid && P.out) {
+            const double coef = stage_coef(P);
 #pragma unroll
             for (int k = 0; k < S::NPL; k++) {
                 const int n = gl + k * L;
                 if (n < NDOF) {
 #pragma unroll
-                    for (int i = 0; i < NV - 1; i++) P.fv[(int64_t)i * nn + e * NDOF + n] = wv[i * ST + sp<Np>(n)];
+                    for (int i = 0; i < NV - 1; i++) P.out[(int64_t)(1 + i) * nn + e * NDOF + n] += coef * wv[i * ST + sp<Np>(n)];
                 }
             }
         }
