@@ -120,6 +120,15 @@ template <int DIM> struct PSlot {
     static constexpr int BETA = P_V + DIM;
 };
 
+// Node index of position `pos` on line `line` of a runtime direction d.
+template <int DIM, int Np> __device__ __forceinline__ int line_node_rt(int d, int line, int pos)
+{
+    if (DIM == 2) return d == 0 ? line * Np + pos : pos * Np + line;
+    if (d == 0) return line * Np + pos;
+    if (d == 1) return (line / Np) * Np * Np + pos * Np + (line % Np);
+    return pos * Np * Np + line;
+}
+
 // Node index of position `pos` on line `line` of direction D (x fastest).
 template <int DIM, int Np, int D> __device__ __forceinline__ int line_node(int line, int pos)
 {
@@ -317,23 +326,24 @@ __device__ __forceinline__ double stage_nodes(const KParams &P, int64_t e, bool 
     return lam;
 }
 
-// Flux-differencing line tasks along direction D: every pair (a < b) of the
-// line is evaluated once and contributes Dhat2(a,b) F to node a and
-// Dhat2(b,a) F to node b; the line sums, scaled by `scale`, are stored
-// (FIRST) or added to acc.  Node a receives its terms in ascending partner
-// order, as the reference's row sum does.
+// Flux-differencing line tasks along direction d (a runtime value, so the
+// two-point flux code exists once per kernel): every pair (a < b) of the line
+// is evaluated once and contributes Dhat2(a,b) F to node a and Dhat2(b,a) F
+// to node b; the line sums, scaled by `scale`, are stored (d == 0) or added
+// to acc.  Node a receives its terms in ascending partner order, as the
+// reference's row sum does.
 // Compat NS 3D keeps the reference's z-direction fill (DGSEMIntegrator.cpp:
-// 702): during the y pass (ZFILL_SAVE) the flux of pair (j, N) of y line
-// (i, m) is saved to zf[(i + Np m) * N + j]; during the z pass (ZFILL_USE)
-// node (i, j, k) takes Dhat2(k, m) * zf[(i + Np m) * N + j] (0 when j = N)
-// for its partners m < k instead of the z flux.
-template <int DIM, int N, int D, bool FIRST, bool ZFILL_SAVE, bool ZFILL_USE>
-__device__ __forceinline__ void ec_lines(const KParams &P, const double *pr, double *acc, double *zf,
-                                         const double *c, int gl, double scale)
+// 702): during the y pass (zsave) the flux of pair (j, N) of y line (i, m) is
+// saved to zf[(i + Np m) * N + j]; during the z pass (zuse) node (i, j, k)
+// takes Dhat2(k, m) * zf[(i + Np m) * N + j] (0 when j = N) for its partners
+// m < k instead of the z flux.
+template <int DIM, int N>
+__device__ __forceinline__ void ec_lines_rt(const KParams &P, int d, const double *pr, double *acc, double *zf,
+                                            const double *c, int gl, double scale, bool zsave, bool zuse)
 {
     using S = Shape<DIM, N>;
-    constexpr int Np = S::Np, NDOF = S::NDOF, NV = S::NV;
-    const double metric = C_ADJ(c)[D];
+    constexpr int Np = S::Np, NV = S::NV;
+    const double metric = C_ADJ(c)[d];
     const double *D2 = C_DHAT2(c);
 #pragma unroll
     for (int r = 0; r < S::LPL; r++) {
@@ -341,7 +351,7 @@ __device__ __forceinline__ void ec_lines(const KParams &P, const double *pr, dou
         if (line < S::NFN) {
             Prim<DIM> q[Np];
 #pragma unroll
-            for (int l = 0; l < Np; l++) q[l] = slot_prim<DIM>(pr, sp<Np>(line_node<DIM, Np, D>(line, l)), S::NS_);
+            for (int l = 0; l < Np; l++) q[l] = slot_prim<DIM>(pr, sp<Np>(line_node_rt<DIM, Np>(d, line, l)), S::NS_);
             double la[Np][NV];
 #pragma unroll
             for (int l = 0; l < Np; l++)
@@ -352,20 +362,19 @@ __device__ __forceinline__ void ec_lines(const KParams &P, const double *pr, dou
 #pragma unroll
                 for (int b = a + 1; b < Np; b++) {
                     double F[NV];
-                    volume_flux<DIM, D>(q[a], q[b], metric, P.gm1inv, F);
+                    volume_flux_rt<DIM>(q[a], q[b], d, metric, P.gm1inv, F);
                     const double cab = D2[a * Np + b], cba = D2[b * Np + a];
-                    if (ZFILL_SAVE && b == N) {
+                    if (zsave && b == N) {
 #pragma unroll
                         for (int v = 0; v < NV; v++) zf[(line * N + a) * NV + v] = F[v];
                     }
 #pragma unroll
                     for (int v = 0; v < NV; v++) {
                         la[a][v] += cab * F[v];
-                        if (!ZFILL_USE) la[b][v] += cba * F[v];
+                        if (!zuse) la[b][v] += cba * F[v];
                     }
                 }
-            if (ZFILL_USE) {
-                // z line (i, j): node (i, j, k) gets Dhat2(k, m) zf[(i + Np m), j] for m < k
+            if (zuse) {
                 const int i = line % Np, j = line / Np;
                 if (j < N) {
 #pragma unroll
@@ -381,11 +390,11 @@ __device__ __forceinline__ void ec_lines(const KParams &P, const double *pr, dou
             }
 #pragma unroll
             for (int l = 0; l < Np; l++) {
-                const int n = sp<Np>(line_node<DIM, Np, D>(line, l));
+                const int n = sp<Np>(line_node_rt<DIM, Np>(d, line, l));
 #pragma unroll
                 for (int v = 0; v < NV; v++) {
                     const double x = scale * la[l][v];
-                    if (FIRST) acc[v * S::NS_ + n] = x;
+                    if (d == 0) acc[v * S::NS_ + n] = x;
                     else acc[v * S::NS_ + n] += x;
                 }
             }
@@ -506,14 +515,10 @@ __global__ void __launch_bounds__(128) rhs_kernel(const KParams P)
         }
         const double sc = -(1.0 - alpha) * C_INVJ(c);
         if (lane_used) {
-            ec_lines<DIM, N, 0, true, false, false>(P, pr, acc, zf, c, gl, sc);
-            if (DIM == 3 && NS && compat) {
-                ec_lines<DIM, N, 1, false, true, false>(P, pr, acc, zf, c, gl, sc);
-                ec_lines<DIM, N, (DIM == 3 ? 2 : 0), false, false, true>(P, pr, acc, zf, c, gl, sc);
-            } else {
-                ec_lines<DIM, N, 1, false, false, false>(P, pr, acc, zf, c, gl, sc);
-                if (DIM == 3) ec_lines<DIM, N, (DIM == 3 ? 2 : 0), false, false, false>(P, pr, acc, zf, c, gl, sc);
-            }
+            const bool zfill = DIM == 3 && NS && compat;
+#pragma unroll 1
+            for (int d = 0; d < DIM; d++)
+                ec_lines_rt<DIM, N>(P, d, pr, acc, zf, c, gl, sc, zfill && d == 1, zfill && d == 2);
         }
         if (P.blending && __any_sync(0xffffffffu, alpha > 0.0)) {
             if (lane_used) {

@@ -94,6 +94,36 @@ __device__ __forceinline__ void volume_flux(const Prim<DIM> &a, const Prim<DIM> 
     F[1 + DIM] = fm * h_hat;
 }
 
+// Same flux for a runtime direction d.
+template <int DIM>
+__device__ __forceinline__ void volume_flux_rt(const Prim<DIM> &a, const Prim<DIM> &b, int dir, double metric,
+                                               double gm1inv, double *F)
+{
+    const double sr = a.rho + b.rho, isr = 1.0 / sr;
+    double rho_ln, irho_ln;
+    logmean_inv(a.rho, b.rho, sr, isr, rho_ln, irho_ln);
+    const double isb = 1.0 / (a.beta + b.beta);
+    const double ibeta_ln = logmean_recip(a.beta, b.beta, isb);
+    const double p_hat = 0.5 * sr * isb;
+    double vm[DIM];
+    double h_hat = 0.0;
+#pragma unroll
+    for (int d = 0; d < DIM; d++) {
+        vm[d] = 0.5 * (a.v[d] + b.v[d]);
+        h_hat += -0.25 * (a.v[d] * a.v[d] + b.v[d] * b.v[d]) + vm[d] * vm[d];
+    }
+    h_hat += 0.5 * ibeta_ln * gm1inv + p_hat * irho_ln;
+    double vd = vm[0];
+#pragma unroll
+    for (int d = 1; d < DIM; d++) vd = dir == d ? vm[d] : vd;
+    const double Vn = vd * metric;
+    const double fm = rho_ln * Vn;
+    F[0] = fm;
+#pragma unroll
+    for (int d = 0; d < DIM; d++) F[1 + d] = fm * vm[d] + (d == dir ? p_hat * metric : 0.0);
+    F[1 + DIM] = fm * h_hat;
+}
+
 // ChandrashekarFlux::ComputeFaceFlux (ChandrashekarFlux.cpp:85-161) for a
 // normal of magnitude |nrm| along axis DIR (sign in nrm).  ma/mb are the
 // momenta whose jump the Lax-Friedrichs term uses; compat keeps the 3D
