@@ -49,7 +49,8 @@ typedef enum pdg_status {
     PDG_ERR_NONFINITE = 3,    /* NaN/Inf met in a state (device error word) */
     PDG_ERR_NONPHYSICAL = 4,  /* rho <= 0 or p <= 0 met (device error word) */
     PDG_ERR_UNSUPPORTED = 5,  /* (dim, order, flags) combination not compiled */
-    PDG_ERR_NOMEM = 6         /* device allocation failed */
+    PDG_ERR_NOMEM = 6,        /* device allocation failed */
+    PDG_ERR_CAPACITY = 7      /* mesh too large for pdg_rhs_noalloc's fixed scratch */
 } pdg_status;
 
 /* Device error-word bits (pdg_check). */
@@ -106,6 +107,31 @@ int64_t pdg_size(const pdg_ctx *ctx);
  * blending coefficient, [entropy variables, BR1 lifting, primitive gradients],
  * volume + subcell FV + face terms.  u, dudt: DEVICE pointers, byNODES. */
 int pdg_rhs(pdg_ctx *ctx, const double *u, double *dudt, void *stream);
+
+/* Allocation-free right-hand side.  No counterpart in the reference: it is
+ * for callers that cannot allocate device memory when they need the operator
+ * — code running where another allocator owns the device's memory, or an
+ * integrator that must keep its footprint fixed — so it takes no context and
+ * calls no cudaMalloc, cudaFree or allocating library routine.  It computes
+ * the same dudt = L(u) as pdg_rhs for the given mesh and parameters, except
+ * that the wave-speed maximum starts from zero on every call.  u, dudt:
+ * DEVICE pointers, byNODES, not aliased.
+ *
+ * All device scratch (constants, neighbour table, blending outputs, the
+ * Navier-Stokes lifting jumps and face columns) lives in one file-scope
+ * device array of PDG_NOALLOC_SCRATCH_DOUBLES doubles (24 MiB) that every GPU
+ * loading this library holds until the process exits.  A mesh that needs
+ * more returns PDG_ERR_CAPACITY: at order 3 that is above about 5,000
+ * elements for Navier-Stokes in 3D and above about 600,000 for Euler.
+ * The first call on a device looks up the array's device address on that
+ * device (the current device); make that first call before any stream
+ * capture.  Every call on a device shares the array and leaves its contents
+ * behind: calls that overlap on the GPU race.  The constants and the
+ * neighbour table are copied from host memory on `stream` in every call.
+ * The device error word is cleared on entry and not reported. */
+#define PDG_NOALLOC_SCRATCH_DOUBLES (3 * 1024 * 1024)
+int pdg_rhs_noalloc(const pdg_mesh *mesh, const pdg_params *params, const double *u, double *dudt,
+                    void *stream);
 
 /* Same with HOST pointers (the MFEM adapter path: Mult on host Vectors).
  * Copies in, computes, copies out, synchronises. */

@@ -36,7 +36,8 @@ KERNEL_FACE_NS = (7, 8, 9)
 PDG_FLAG_NONFINITE = 1
 PDG_FLAG_NONPHYSICAL = 2
 _STATUS = {1: "bad argument", 2: "CUDA error", 3: "non-finite state", 4: "non-physical state",
-           5: "unsupported configuration", 6: "out of device memory"}
+           5: "unsupported configuration", 6: "out of device memory",
+           7: "mesh exceeds the allocation-free scratch"}
 
 _dp = C.POINTER(C.c_double)
 _ip = C.POINTER(C.c_int32)
@@ -92,6 +93,7 @@ def library():
     L.pdg_rk3_step_host.argtypes = [C.c_void_p, C.c_double, _dp]
     L.pdg_profile_enable.argtypes = [C.c_void_p, C.c_int]
     L.pdg_profile_read.argtypes = [C.c_void_p, C.c_int, _dp, C.POINTER(C.c_int64)]
+    L.pdg_rhs_noalloc.argtypes = [C.POINTER(PdgMesh), C.POINTER(PdgParams), C.c_void_p, C.c_void_p, C.c_void_p]
     _lib = L
     return L
 

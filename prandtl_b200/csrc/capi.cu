@@ -21,6 +21,7 @@
 
 #include "../../include/prandtl_b200.h"
 #include "line_kernels.cuh"
+#include "host_common.h"
 #include "kernel_table.h"
 
 using namespace pdg;
@@ -131,11 +132,14 @@ void gauss_lobatto(int Np, double *x, double *w)
     if (N % 2 == 0) x[N / 2] = 0.5;
 }
 
-void build_constants(pdg_ctx *c)
+}  // namespace
+
+namespace pdg_host {
+
+void fill_constants(int dim, int N, const double *h, DevConst &K, double &modal_threshold)
 {
-    DevConst &K = c->hK;
     std::memset(&K, 0, sizeof(K));
-    const int Np = c->Np;
+    const int Np = N + 1;
     double x[6], w[6];
     gauss_lobatto(Np, x, w);
     // barycentric weights and the differentiation matrix D_il = l_l'(x_i)
@@ -165,8 +169,7 @@ void build_constants(pdg_ctx *c)
     K.Dhat2[Np * Np - 1] -= 1.0 / w[Np - 1];
     for (int i = 0; i < Np; i++) K.w[i] = w[i];
     // affine element: J = prod h, adj = diag(J / h_d), face area = J / h_d
-    const double *h = c->h;
-    if (c->dim == 2) {
+    if (dim == 2) {
         K.J = h[0] * h[1];
         K.adj[0] = h[1];
         K.adj[1] = h[0];
@@ -176,13 +179,13 @@ void build_constants(pdg_ctx *c)
         K.adj[1] = h[0] * h[2];
         K.adj[2] = h[0] * h[1];
     }
-    for (int d = 0; d < c->dim; d++) K.area[d] = K.adj[d];
+    for (int d = 0; d < dim; d++) K.area[d] = K.adj[d];
     K.invJ = 1.0 / K.J;
     K.face_scale = 1.0 / (w[0] * K.J);
     for (int i = 0; i < Np; i++) K.fv_scale[i] = 1.0 / (K.J * w[i]);
     // subcell interface normals (ComputeSubcellMetrics, DGSEMIntegrator.cpp:
     // 1199-1304): adj_d + sum_{l<i} w_l sum_m D(l,m) adj_d on an affine element
-    for (int d = 0; d < c->dim; d++)
+    for (int d = 0; d < dim; d++)
         for (int i = 0; i <= Np; i++) {
             double nor = K.adj[d];
             for (int l = 0; l < i; l++) {
@@ -226,43 +229,95 @@ void build_constants(pdg_ctx *c)
             }
     }
     for (int t = 0; t < Np * Np; t++) K.Vinv1[t] = I[t];  // Vinv1[k*Np + i]: mode k from node i
-    c->modal_threshold = 0.5 * std::pow(10.0, -1.8 * std::pow((double)c->N, 0.25));
+    modal_threshold = 0.5 * std::pow(10.0, -1.8 * std::pow((double)N, 0.25));
 }
 
-int configure_launch(pdg_ctx *c, int kind)
+int kernel_config(int dim, int N, int kind, int64_t ne, int device, LaunchCfg *cfg, const char **why)
 {
-    KernelInfo &ki = c->kinfo[kind];
-    bool ok = c->dim == 2 ? kernel_info_2d(c->N, kind, &ki) : kernel_info_3d(c->N, kind, &ki);
-    if (!ok) return fail(c, PDG_ERR_UNSUPPORTED, "no kernel for dim=%d order=%d", c->dim, c->N);
-    int dev = c->device, max_smem = 0, sms = 0;
-    CK(cudaDeviceGetAttribute(&max_smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev), "device attribute");
-    CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev), "device attribute");
+    KernelInfo &ki = cfg->ki;
+    const bool ok = dim == 2 ? kernel_info_2d(N, kind, &ki) : kernel_info_3d(N, kind, &ki);
+    if (!ok) { *why = "no kernel for this dimension and order"; return PDG_ERR_UNSUPPORTED; }
+    int max_smem = 0, sms = 0;
+    if (cudaDeviceGetAttribute(&max_smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, device) != cudaSuccess ||
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device) != cudaSuccess) {
+        *why = "device attribute query failed";
+        return PDG_ERR_CUDA;
+    }
+    const int Np = N + 1, nfn = dim == 2 ? Np : Np * Np;
     if (ki.el_doubles == 0) {  // thread-per-face-node kernel
         int blocks_per_sm = 0;
-        CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks_per_sm, ki.fn, 256, 0), "occupancy");
-        const int nfn = c->dim == 2 ? c->Np : c->Np * c->Np;
-        const int64_t threads = (kind == KIND_LIFT_FACE ? (int64_t)c->dim : 1) * c->ne * nfn;
-        c->wpb[kind] = 8;
-        c->grid[kind] = (int)std::max<int64_t>(1, std::min<int64_t>((threads + 255) / 256, (int64_t)sms * std::max(1, blocks_per_sm)));
-        c->smem[kind] = 0;
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks_per_sm, ki.fn, 256, 0) != cudaSuccess) {
+            *why = "occupancy query failed";
+            return PDG_ERR_CUDA;
+        }
+        const int64_t threads = (kind == KIND_LIFT_FACE ? (int64_t)dim : 1) * ne * nfn;
+        cfg->wpb = 8;
+        cfg->grid = (int)std::max<int64_t>(1, std::min<int64_t>((threads + 255) / 256, (int64_t)sms * std::max(1, blocks_per_sm)));
+        cfg->smem = 0;
         return PDG_OK;
     }
     const size_t per_warp = (size_t)ki.epw * ki.el_doubles * sizeof(double);
     const size_t base = (size_t)CONST_SLOTS * sizeof(double);
     int wpb = 4;
     while (wpb > 1 && base + wpb * per_warp > (size_t)max_smem) wpb--;
-    if (base + wpb * per_warp > (size_t)max_smem)
-        return fail(c, PDG_ERR_UNSUPPORTED, "element does not fit in shared memory (dim=%d order=%d)", c->dim, c->N);
+    if (base + wpb * per_warp > (size_t)max_smem) { *why = "element does not fit in shared memory"; return PDG_ERR_UNSUPPORTED; }
     const size_t smem = base + wpb * per_warp;
-    CK(cudaFuncSetAttribute(ki.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem), "smem attribute");
+    if (cudaFuncSetAttribute(ki.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) {
+        *why = "shared-memory attribute failed";
+        return PDG_ERR_CUDA;
+    }
     int blocks_per_sm = 0;
-    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks_per_sm, ki.fn, 32 * wpb, smem), "occupancy");
-    if (blocks_per_sm < 1) return fail(c, PDG_ERR_UNSUPPORTED, "kernel cannot be resident (dim=%d order=%d)", c->dim, c->N);
-    const int64_t nwt = (c->ne + ki.epw - 1) / ki.epw;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks_per_sm, ki.fn, 32 * wpb, smem) != cudaSuccess) {
+        *why = "occupancy query failed";
+        return PDG_ERR_CUDA;
+    }
+    if (blocks_per_sm < 1) { *why = "kernel cannot be resident"; return PDG_ERR_UNSUPPORTED; }
+    const int64_t nwt = (ne + ki.epw - 1) / ki.epw;
     const int64_t need = (nwt + wpb - 1) / wpb;
-    c->wpb[kind] = wpb;
-    c->grid[kind] = (int)std::max<int64_t>(1, std::min<int64_t>(need, (int64_t)sms * blocks_per_sm));
-    c->smem[kind] = smem;
+    cfg->wpb = wpb;
+    cfg->grid = (int)std::max<int64_t>(1, std::min<int64_t>(need, (int64_t)sms * blocks_per_sm));
+    cfg->smem = smem;
+    return PDG_OK;
+}
+
+bool kind_used(int kind, int dim, bool parabolic)
+{
+    const bool ns_kind = kind == KIND_NS || kind == KIND_LIFT || kind == KIND_LIFT_FACE ||
+                         (kind >= KIND_FACE_NS0 && kind <= KIND_FACE_NS2);
+    if (ns_kind != parabolic) return false;
+    if ((kind == KIND_FACE_E2 || kind == KIND_FACE_NS2) && dim < 3) return false;
+    return true;
+}
+
+int launch_kernel(const LaunchCfg &cfg, KParams P, int64_t ne, cudaStream_t s)
+{
+    P.nwt = (ne + cfg.ki.epw - 1) / cfg.ki.epw;
+    void *args[] = {&P};
+    return cudaLaunchKernel(cfg.ki.fn, dim3(cfg.grid), dim3(32 * cfg.wpb), args, cfg.smem, s) == cudaSuccess
+               ? PDG_OK
+               : PDG_ERR_CUDA;
+}
+
+}  // namespace pdg_host
+
+namespace {
+using namespace pdg_host;
+
+void build_constants(pdg_ctx *c)
+{
+    fill_constants(c->dim, c->N, c->h, c->hK, c->modal_threshold);
+}
+
+int configure_launch(pdg_ctx *c, int kind)
+{
+    LaunchCfg cfg;
+    const char *why = "";
+    const int r = kernel_config(c->dim, c->N, kind, c->ne, c->device, &cfg, &why);
+    if (r) return fail(c, r, "%s (dim=%d order=%d kernel %d)", why, c->dim, c->N, kind);
+    c->kinfo[kind] = cfg.ki;
+    c->wpb[kind] = cfg.wpb;
+    c->grid[kind] = cfg.grid;
+    c->smem[kind] = cfg.smem;
     return PDG_OK;
 }
 
@@ -443,10 +498,7 @@ int pdg_create(const pdg_mesh *mesh, const pdg_params *params, pdg_ctx **out)
         cudaMemset(c->lam_bits, 0, sizeof(unsigned long long)) || cudaMemset(c->err, 0, sizeof(unsigned int)))
         return cleanup(PDG_ERR_CUDA);
     for (int kind = 0; kind < KIND_COUNT; kind++) {
-        const bool ns_kind = kind == KIND_NS || kind == KIND_LIFT || kind == KIND_LIFT_FACE ||
-                             (kind >= KIND_FACE_NS0 && kind <= KIND_FACE_NS2);
-        if (ns_kind != (c->p.parabolic != 0)) continue;
-        if ((kind == KIND_FACE_E2 || kind == KIND_FACE_NS2) && c->dim < 3) continue;
+        if (!kind_used(kind, c->dim, c->p.parabolic != 0)) continue;
         int r = configure_launch(c, kind);
         if (r) return cleanup(r);
     }
