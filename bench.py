@@ -33,6 +33,9 @@ from prandtl_b200.mesh import periodic_box  # noqa: E402
 
 METRIC = "DOF-stage updates/s on 1 B200 (plain vs batched+graph); adjoint/forward cost"
 UNIT = "DOF-stage updates/s"
+# kernels of one Navier-Stokes stage, in launch order, with their PDG_KERNEL_* kinds
+KERNELS = [("lift_face_kernel", (3,)), ("rhs_kernel<NS>", (2,)), ("lift_kernel", (1,)),
+           ("face_kernel<NS>", (7, 8, 9))]
 
 
 def parse():
@@ -171,8 +174,9 @@ def run_ours(args):
 
     sampler = ClockSampler(dev.index or 0)
     op.profile(True)
-    for k in (pb.KERNEL_LIFT, pb.KERNEL_NS, pb.KERNEL_LIFT_FACE) + pb.KERNEL_FACE_NS:
-        op.profile_read(k)
+    for _, kinds in KERNELS:
+        for k in kinds:
+            op.profile_read(k)
     launches0 = op.launch_count()
     barrier()
     torch.cuda.synchronize()
@@ -187,13 +191,13 @@ def run_ours(args):
     clocks = sampler.stop()
     ms = ev0.elapsed_time(ev1)
     launches = op.launch_count() - launches0
-    ns_ms, ns_n = op.profile_read(pb.KERNEL_NS)
-    lift_ms, lift_n = op.profile_read(pb.KERNEL_LIFT)
-    face_ms, face_n = 0.0, 0
-    for k in pb.KERNEL_FACE_NS:
-        fm, fnn = op.profile_read(k)
-        face_ms, face_n = face_ms + fm, max(face_n, fnn)
-    lface_ms, lface_n = op.profile_read(pb.KERNEL_LIFT_FACE)
+    kernel_ms = {}
+    for name, kinds in KERNELS:
+        tot, n = 0.0, 0
+        for k in kinds:
+            km, kn = op.profile_read(k)
+            tot, n = tot + km, n + kn
+        kernel_ms[name] = (tot, n)
     op.profile(False)
     op.check()
     if world > 1:
@@ -220,28 +224,28 @@ def run_ours(args):
            "path": "pdg_rk3_step_host (pinned host state in, 3 fused stages, state out)"}
 
     peak, peak_kind = measured_peaks()
-    # algorithmic bytes of the NS RHS + stage kernel per launch: reads u (8 B),
-    # 3 gradient fields (24 B), un on stages 1-2 (8 B), writes the stage (8 B)
-    ns_bytes = V * (8 + 24 + 8) + V * 8 * (2.0 / 3.0)
-    lift_bytes = V * (8 + 24)
-    ns_avg = ns_ms / max(ns_n, 1)
-    lift_avg = lift_ms / max(lift_n, 1)
-    ns_gbs = ns_bytes / (ns_avg * 1e-3) / 1e9
-    lift_gbs = lift_bytes / (lift_avg * 1e-3) / 1e9
-    step_gbs = (3 * lift_bytes + 3 * ns_bytes) / (ms / args.steps * 1e-3) / 1e9
-    traffic = None
+    stages = 3 * args.steps
+    stage_ms = ms / stages
+    # algorithmic bytes of one NS stage (two-pass BR1 with the stage axpy
+    # fused): 72 B/vdof for stage 0, 80 B/vdof for stages 1 and 2
+    stage_bytes = V * (72 + 80 + 80) / 3.0
+    achieved = stage_bytes / (stage_ms * 1e-3) / 1e9
+    total_kernel_ms = sum(t for t, _ in kernel_ms.values())
+    traffic, traffic_src = None, None
     tf = os.path.join(ROOT, "profiles", "traffic.json")
     if os.path.exists(tf):
-        traffic = json.load(open(tf)).get("ns_rhs_kernel_bytes_per_launch")
-    roofline = {"bound": "hbm", "kernel": "ns_rhs_kernel<3,3>", "achieved": ns_gbs, "peak": peak, "unit": "GB/s",
-                "frac": ns_gbs / peak, "traffic": traffic, "peak_kind": peak_kind,
-                "algorithmic_bytes_per_launch": ns_bytes, "avg_launch_ms": ns_avg,
-                "lift_kernel": {"achieved": lift_gbs, "frac": lift_gbs / peak, "avg_launch_ms": lift_avg,
-                                "algorithmic_bytes_per_launch": lift_bytes},
-                "lift_face_kernel": {"avg_launch_ms": lface_ms / max(lface_n, 1)},
-                "face_kernels": {"avg_ms_per_stage": face_ms / max(face_n, 1),
-                                 "note": "x, y, z face passes adding the face fluxes to the stage output"},
-                "whole_step": {"achieved": step_gbs, "frac": step_gbs / peak, "bytes_per_vdof": 232}}
+        tj = json.load(open(tf))
+        if tj.get("workload") == config_dict(mesh, 1)["workload"]:
+            traffic = tj.get("dram_bytes_per_stage")
+            traffic_src = tj.get("source")
+    roofline = {"bound": "hbm", "kernel": "one NS RK stage: " + ", ".join(n for n, _ in KERNELS),
+                "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                "traffic": traffic, "traffic_source": traffic_src, "peak_kind": peak_kind,
+                "algorithmic_bytes_per_launch": stage_bytes, "bytes_per_vdof": (72 + 80 + 80) / 3.0,
+                "avg_launch_ms": stage_ms,
+                "kernels": {n: {"avg_launch_ms": t / c if c else 0.0, "ms_per_stage": t / stages,
+                                "launches": c, "share": t / total_kernel_ms if total_kernel_ms else None}
+                            for n, (t, c) in kernel_ms.items()}}
     out = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
            "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
