@@ -49,6 +49,8 @@ def parse():
     ap.add_argument("--e2e-steps", type=int, default=5)
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--sweep-steps", type=int, default=100,
+                    help="SSP-RK3 steps of the 256-case vortex sweep (0 skips it)")
     return ap.parse_args()
 
 
@@ -251,6 +253,8 @@ def run_ours(args):
            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
            "config": config_dict(mesh, world), "e2e": e2e, "gpu_launches": launches,
            "roofline": roofline, "clocks": clocks}
+    if args.sweep_steps > 0:
+        out["sweep"] = run_sweep(args, dev)
     if rank == 0 and world == 1 and not args.no_cpu:
         out["cpu_baseline"] = cpu_baseline(mesh, u0, params, args.cpu_seconds)
     if rank == 0:
@@ -258,6 +262,68 @@ def run_ours(args):
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()
+
+
+def run_sweep(args, dev):
+    """256-case isentropic-vortex sweep: the batched form (one persistent
+    launch per stage, graph-replayed, autotuned) against per-case plain
+    launches, same per-case dt, same steps."""
+    import torch
+
+    import prandtl_b200 as pb
+    specs = cases.sweep_cases(256, seed=3)
+    meshes = [periodic_box(2, N, n, -5.0, 5.0) for n, N, _ in specs]
+    states = [cases.isentropic_vortex(m, strength=e) for m, (_, _, e) in zip(meshes, specs)]
+    batch = pb.DGSEMBatch(meshes)
+    u0 = np.concatenate(states)
+    assert u0.size == batch.size
+    u = torch.from_numpy(u0).to(dev)
+    tmp = torch.empty_like(u)
+    batch.Mult(u, tmp)
+    dt = batch.cfl_dt(0.5)
+    batch.set_dt(dt)
+    tuned_ms = batch.tune(u)
+    cfg = batch.config()
+    V = batch.size
+    K = args.sweep_steps
+
+    def timed(fn):
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        fn()
+        e1.record()
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1)
+
+    res = {"workload": "isentropic_vortex_sweep_256_cases_n8-64_N2-5_euler_blending_ssprk3",
+           "cases": 256, "vdofs": V, "steps": K, "warmup": args.warmup}
+    for graph in (True, False):
+        x = torch.from_numpy(u0).to(dev)
+        batch.rk3_step(x, args.warmup, graph=graph)
+        l0 = batch.launch_count()
+        ms = timed(lambda: batch.rk3_step(x, K, graph=graph))
+        res["batched_graph" if graph else "batched_launches"] = {
+            "value": V * 3 * K / (ms * 1e-3), "ms_per_step": ms / K, "gpu_launches": batch.launch_count() - l0}
+    batch.check()
+    ops = [pb.DGSEMOperator(m) for m in meshes]
+    xs = [torch.from_numpy(s).to(dev) for s in states]
+    for _ in range(args.warmup):
+        for op, x, d in zip(ops, xs, dt):
+            op.rk3_step(x, float(d))
+    l0 = sum(op.launch_count() for op in ops)
+
+    def plain():
+        for _ in range(K):
+            for op, x, d in zip(ops, xs, dt):
+                op.rk3_step(x, float(d))
+    ms = timed(plain)
+    res["per_case_launches"] = {"value": V * 3 * K / (ms * 1e-3), "ms_per_step": ms / K,
+                                "gpu_launches": sum(op.launch_count() for op in ops) - l0}
+    res["batched_vs_per_case"] = res["batched_graph"]["value"] / res["per_case_launches"]["value"]
+    res["autotuner"] = dict(cfg, best_rhs_launch_ms=tuned_ms)
+    res["unit"] = UNIT
+    return res
 
 
 def _ref_worker(payload):

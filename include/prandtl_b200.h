@@ -179,6 +179,14 @@ int pdg_get_blending(pdg_ctx *ctx, double *eta_host, double *alpha_host);
  * only keeps the viscous fluxes derived from them. */
 int pdg_gradients(pdg_ctx *ctx, const double *u, double *grads, void *stream);
 
+/* Entropy filter (params.filter = 1): EntropyFilter::FilterSolution
+ * (src/Filters/EntropyFilter.cpp:171-242) after every RK stage, with the
+ * element bounds of GetEntropyConstraints (:81-158) taken at the stage input.
+ * Applies to pdg_rk_stage / pdg_rk3_step*; pdg_rhs is never filtered.
+ * pdg_filter_count returns the number of element filterings since creation
+ * (synchronises). */
+int pdg_filter_count(pdg_ctx *ctx, int64_t *filtered);
+
 /* Reads and clears the device error word (PDG_FLAG_*).  Synchronises. */
 int pdg_check(pdg_ctx *ctx, uint32_t *flags);
 
@@ -199,8 +207,46 @@ int64_t pdg_launch_count(const pdg_ctx *ctx);
 #define PDG_KERNEL_LIFT_FACE 3  /* BR1 lifting face-jump kernel */
 #define PDG_KERNEL_FACE_E0   4  /* Euler face kernels, x / y / z */
 #define PDG_KERNEL_FACE_NS0  7  /* Navier-Stokes face kernels, x / y / z (7, 8, 9) */
+#define PDG_KERNEL_FILTER_BOUNDS 10  /* entropy filter: per-element entropy minimum */
+#define PDG_KERNEL_FILTER    11  /* entropy filter of a stage output */
 int pdg_profile_enable(pdg_ctx *ctx, int on);
 int pdg_profile_read(pdg_ctx *ctx, int kind, double *total_ms, int64_t *launches);
+
+/* ---- Batched sweep: many independent cases in one launch per RK stage ----
+ *
+ * No single reference counterpart: the reference runs one case per process
+ * (Simulation::Run, src/Simulation/Simulation.cpp:800-1020) and a sweep is a
+ * loop over runs.  A batch holds periodic 2D Euler cases (params.parabolic =
+ * params.filter = 0) of any size and order 1..5 that share pdg_params; their
+ * states are concatenated, case c occupying pdg_batch_offset(c) ..
+ * pdg_batch_offset(c + 1) - 1 in the usual byNODES layout of its own mesh.
+ * Every case has its own time step (pdg_batch_set_dt) and running wave-speed
+ * maximum.  Results per case equal the per-case context's pdg_rhs /
+ * pdg_rk3_step to rounding. */
+typedef struct pdg_batch pdg_batch;
+int pdg_batch_create(int ncases, const pdg_mesh *meshes, const pdg_params *params, pdg_batch **out);
+int pdg_batch_destroy(pdg_batch *batch);
+/* Offset (in doubles) of case c's state; c = ncases gives the total size. */
+int64_t pdg_batch_offset(const pdg_batch *batch, int case_index);
+/* Per-case time steps (host array of ncases doubles). */
+int pdg_batch_set_dt(pdg_batch *batch, const double *dt);
+/* DGSEMOperator::Mult of every case in one launch.  DEVICE pointers. */
+int pdg_batch_rhs(pdg_batch *batch, const double *u, double *dudt, void *stream);
+/* nsteps SSP-RK3 steps of every case in place (RK3SSPSolver::Step,
+ * Simulation.cpp:1010), three launches per step; with use_graph the step is
+ * captured once in a CUDA graph and replayed. */
+int pdg_batch_rk3_step(pdg_batch *batch, double *u, int nsteps, int use_graph, void *stream);
+/* Autotuner: times the batch kernel on u for each warps-per-block x
+ * tiles-per-fetch x tile-order candidate and keeps the fastest (synchronises).
+ * best_ms (may be null) receives the fastest launch time. */
+int pdg_batch_tune(pdg_batch *batch, const double *u, void *stream, float *best_ms);
+int pdg_batch_config(const pdg_batch *batch, int *warps_per_block, int *blocks, int *tiles_per_fetch,
+                     int *tile_order);
+/* Per-case running maximum wave speed (host array of ncases; synchronises). */
+int pdg_batch_max_char_speed(pdg_batch *batch, double *lam);
+int pdg_batch_check(pdg_batch *batch, uint32_t *flags);
+int64_t pdg_batch_launch_count(const pdg_batch *batch);
+const char *pdg_batch_last_error(const pdg_batch *batch);
 
 #ifdef __cplusplus
 }

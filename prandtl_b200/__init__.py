@@ -33,6 +33,7 @@ PDG_OK = 0
 KERNEL_EULER, KERNEL_LIFT, KERNEL_NS, KERNEL_LIFT_FACE = 0, 1, 2, 3
 KERNEL_FACE_EULER = (4, 5, 6)
 KERNEL_FACE_NS = (7, 8, 9)
+KERNEL_FILTER_BOUNDS, KERNEL_FILTER = 10, 11
 PDG_FLAG_NONFINITE = 1
 PDG_FLAG_NONPHYSICAL = 2
 _STATUS = {1: "bad argument", 2: "CUDA error", 3: "non-finite state", 4: "non-physical state",
@@ -93,6 +94,23 @@ def library():
     L.pdg_rk3_step_host.argtypes = [C.c_void_p, C.c_double, _dp]
     L.pdg_profile_enable.argtypes = [C.c_void_p, C.c_int]
     L.pdg_profile_read.argtypes = [C.c_void_p, C.c_int, _dp, C.POINTER(C.c_int64)]
+    vp = C.c_void_p
+    L.pdg_batch_create.argtypes = [C.c_int, C.POINTER(PdgMesh), C.POINTER(PdgParams), C.POINTER(vp)]
+    L.pdg_batch_destroy.argtypes = [vp]
+    L.pdg_batch_offset.restype = C.c_int64
+    L.pdg_batch_offset.argtypes = [vp, C.c_int]
+    L.pdg_batch_set_dt.argtypes = [vp, _dp]
+    L.pdg_batch_rhs.argtypes = [vp, vp, vp, vp]
+    L.pdg_batch_rk3_step.argtypes = [vp, vp, C.c_int, C.c_int, vp]
+    L.pdg_batch_tune.argtypes = [vp, vp, vp, C.POINTER(C.c_float)]
+    L.pdg_batch_config.argtypes = [vp] + [C.POINTER(C.c_int)] * 4
+    L.pdg_batch_max_char_speed.argtypes = [vp, _dp]
+    L.pdg_batch_check.argtypes = [vp, C.POINTER(C.c_uint32)]
+    L.pdg_batch_launch_count.restype = C.c_int64
+    L.pdg_batch_launch_count.argtypes = [vp]
+    L.pdg_batch_last_error.restype = C.c_char_p
+    L.pdg_batch_last_error.argtypes = [vp]
+    L.pdg_filter_count.argtypes = [C.c_void_p, C.POINTER(C.c_int64)]
     L.pdg_rhs_noalloc.argtypes = [C.POINTER(PdgMesh), C.POINTER(PdgParams), C.c_void_p, C.c_void_p, C.c_void_p]
     _lib = L
     return L
@@ -248,8 +266,112 @@ class DGSEMOperator:
         self._call(library().pdg_check(self._ctx, C.byref(f)), "pdg_check")
         return f.value
 
+    def filter_count(self) -> int:
+        """Element filterings by the entropy filter since creation (synchronises)."""
+        n = C.c_int64()
+        self._call(library().pdg_filter_count(self._ctx, C.byref(n)), "pdg_filter_count")
+        return n.value
+
     def launch_count(self) -> int:
         return int(library().pdg_launch_count(self._ctx))
+
+
+class DGSEMBatch:
+    """Many independent periodic 2D Euler cases advanced together: one
+    persistent launch per SSP-RK3 stage over all cases, replayed from a CUDA
+    graph.  The state is one device tensor; case c is
+    ``u[offsets[c]:offsets[c + 1]]`` in its own mesh's byNODES layout."""
+
+    def __init__(self, meshes, **params):
+        self.meshes = list(meshes)
+        self.params = default_params(**params)
+        self._nbrs = [np.ascontiguousarray(m.nbr, dtype=np.int32) for m in self.meshes]
+        arr = (PdgMesh * len(self.meshes))()
+        for i, (m, nb) in enumerate(zip(self.meshes, self._nbrs)):
+            h = list(m.h) + [1.0] * (3 - m.dim)
+            arr[i] = PdgMesh(m.dim, m.order, m.num_elements, (C.c_double * 3)(*h), nb.ctypes.data_as(_ip))
+        self._arr = arr
+        self._b = C.c_void_p()
+        code = library().pdg_batch_create(len(self.meshes), arr, C.byref(self.params), C.byref(self._b))
+        if code != PDG_OK:
+            raise PdgError(code, "pdg_batch_create")
+        L = library()
+        self.offsets = np.array([L.pdg_batch_offset(self._b, c) for c in range(len(self.meshes) + 1)],
+                                dtype=np.int64)
+
+    def _call(self, code, what):
+        if code != PDG_OK:
+            raise PdgError(code, f"{what}: {library().pdg_batch_last_error(self._b).decode()}")
+
+    def close(self):
+        if getattr(self, "_b", None):
+            library().pdg_batch_destroy(self._b)
+            self._b = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def size(self) -> int:
+        return int(self.offsets[-1])
+
+    def _check_dev(self, *ts):
+        for t in ts:
+            if not (t.is_cuda and t.element_size() == 8 and t.dtype.is_floating_point and t.is_contiguous()):
+                raise ValueError("device arrays must be contiguous float64 CUDA tensors")
+            if t.numel() != self.size:
+                raise ValueError(f"array has {t.numel()} entries, batch size is {self.size}")
+
+    def set_dt(self, dt):
+        dt = np.ascontiguousarray(dt, dtype=np.float64)
+        if dt.size != len(self.meshes):
+            raise ValueError("one dt per case")
+        self._call(library().pdg_batch_set_dt(self._b, dt.ctypes.data_as(_dp)), "pdg_batch_set_dt")
+
+    def Mult(self, u, dudt, stream=None):
+        self._check_dev(u, dudt)
+        self._call(library().pdg_batch_rhs(self._b, C.c_void_p(u.data_ptr()), C.c_void_p(dudt.data_ptr()),
+                                           C.c_void_p(_stream_handle(stream))), "pdg_batch_rhs")
+        return dudt
+
+    def rk3_step(self, u, nsteps: int = 1, graph: bool = True, stream=None):
+        self._check_dev(u)
+        self._call(library().pdg_batch_rk3_step(self._b, C.c_void_p(u.data_ptr()), int(nsteps), int(bool(graph)),
+                                                C.c_void_p(_stream_handle(stream))), "pdg_batch_rk3_step")
+        return u
+
+    def tune(self, u, stream=None) -> float:
+        self._check_dev(u)
+        ms = C.c_float()
+        self._call(library().pdg_batch_tune(self._b, C.c_void_p(u.data_ptr()), C.c_void_p(_stream_handle(stream)),
+                                            C.byref(ms)), "pdg_batch_tune")
+        return ms.value
+
+    def config(self) -> dict:
+        v = [C.c_int() for _ in range(4)]
+        self._call(library().pdg_batch_config(self._b, *[C.byref(x) for x in v]), "pdg_batch_config")
+        return dict(zip(("warps_per_block", "blocks", "tiles_per_fetch", "tile_order"), (x.value for x in v)))
+
+    def max_char_speed(self) -> np.ndarray:
+        lam = np.empty(len(self.meshes))
+        self._call(library().pdg_batch_max_char_speed(self._b, lam.ctypes.data_as(_dp)), "pdg_batch_max_char_speed")
+        return lam
+
+    def cfl_dt(self, cfl: float) -> np.ndarray:
+        """Per-case dt = cfl h_min / (lambda_max (N+1)^2) from the running maxima."""
+        lam = self.max_char_speed()
+        return np.array([cfl * min(m.h) / (l * (m.order + 1) ** 2) for m, l in zip(self.meshes, lam)])
+
+    def check(self) -> int:
+        f = C.c_uint32()
+        self._call(library().pdg_batch_check(self._b, C.byref(f)), "pdg_batch_check")
+        return f.value
+
+    def launch_count(self) -> int:
+        return int(library().pdg_batch_launch_count(self._b))
 
 
 class RK3SSPSolver:

@@ -44,6 +44,8 @@ struct pdg_ctx {
     double *io_a = nullptr, *io_b = nullptr;        // host-path staging
     unsigned long long *lam_bits = nullptr;
     unsigned int *err = nullptr;
+    double *ent_own = nullptr;                // filter: per-element entropy minimum at the stage input
+    unsigned long long *filter_count = nullptr;
     // launch configuration per kernel kind
     KernelInfo kinfo[KIND_COUNT];
     int wpb[KIND_COUNT];
@@ -205,6 +207,7 @@ void fill_constants(int dim, int N, const double *h, DevConst &K, double &modal_
         for (int n = 1; n + 1 < Np; n++) L[n + 1] = ((2 * n + 1) * z * L[n] - n * L[n - 1]) / (n + 1);
         for (int k = 0; k < Np; k++) V[i * Np + k] = L[k];
     }
+    for (int t = 0; t < Np * Np; t++) K.V1[t] = V[t];
     for (int i = 0; i < Np; i++) I[i * Np + i] = 1.0;
     for (int col = 0; col < Np; col++) {  // Gauss-Jordan with partial pivoting
         int piv = col;
@@ -250,7 +253,7 @@ int kernel_config(int dim, int N, int kind, int64_t ne, int device, LaunchCfg *c
             *why = "occupancy query failed";
             return PDG_ERR_CUDA;
         }
-        const int64_t threads = (kind == KIND_LIFT_FACE ? (int64_t)dim : 1) * ne * nfn;
+        const int64_t threads = kind == KIND_FILTER_BOUNDS ? 32 * ne : (kind == KIND_LIFT_FACE ? (int64_t)dim : 1) * ne * nfn;
         cfg->wpb = 8;
         cfg->grid = (int)std::max<int64_t>(1, std::min<int64_t>((threads + 255) / 256, (int64_t)sms * std::max(1, blocks_per_sm)));
         cfg->smem = 0;
@@ -280,8 +283,9 @@ int kernel_config(int dim, int N, int kind, int64_t ne, int device, LaunchCfg *c
     return PDG_OK;
 }
 
-bool kind_used(int kind, int dim, bool parabolic)
+bool kind_used(int kind, int dim, bool parabolic, bool filter)
 {
+    if (kind == KIND_FILTER_BOUNDS || kind == KIND_FILTER) return filter;
     const bool ns_kind = kind == KIND_NS || kind == KIND_LIFT || kind == KIND_LIFT_FACE ||
                          (kind >= KIND_FACE_NS0 && kind <= KIND_FACE_NS2);
     if (ns_kind != parabolic) return false;
@@ -333,6 +337,8 @@ KParams base_params(pdg_ctx *c)
     P.alpha_out = c->alpha;
     P.lam_bits = c->lam_bits;
     P.err = c->err;
+    P.ent_own = c->ent_own;
+    P.filter_count = c->filter_count;
     P.ne = c->ne;
     P.nnodes = c->nnodes;
     P.stage = -1;
@@ -412,16 +418,20 @@ int evaluate(pdg_ctx *c, int stage, double dt, const double *un, const double *u
     int r;
     if (c->p.parabolic) {
         KParams Lf = P;
+        if (c->p.filter && stage >= 0 && (r = launch(c, KIND_FILTER_BOUNDS, P, s))) return r;
         if ((r = launch(c, KIND_LIFT_FACE, Lf, s))) return r;
         if ((r = launch(c, KIND_NS, P, s))) return r;
         if ((r = launch(c, KIND_LIFT, P, s))) return r;
         for (int d = 0; d < c->dim; d++)
             if ((r = launch(c, KIND_FACE_NS0 + d, P, s))) return r;
-        return PDG_OK;
+    } else {
+        if (c->p.filter && stage >= 0 && (r = launch(c, KIND_FILTER_BOUNDS, P, s))) return r;
+        if ((r = launch(c, KIND_EULER, P, s))) return r;
+        for (int d = 0; d < c->dim; d++)
+            if ((r = launch(c, KIND_FACE_E0 + d, P, s))) return r;
     }
-    if ((r = launch(c, KIND_EULER, P, s))) return r;
-    for (int d = 0; d < c->dim; d++)
-        if ((r = launch(c, KIND_FACE_E0 + d, P, s))) return r;
+    // entropy filter of the stage output (EntropyFilter::FilterSolution)
+    if (c->p.filter && stage >= 0 && (r = launch(c, KIND_FILTER, P, s))) return r;
     return PDG_OK;
 }
 
@@ -486,6 +496,12 @@ int pdg_create(const pdg_mesh *mesh, const pdg_params *params, pdg_ctx **out)
         cudaMalloc(&c->lam_bits, sizeof(unsigned long long)) || cudaMalloc(&c->err, sizeof(unsigned int)) ||
         cudaMalloc(&c->stage_a, fbytes) || cudaMalloc(&c->stage_b, fbytes))
         return cleanup(PDG_ERR_NOMEM);
+    if (c->p.filter) {
+        if (cudaMalloc(&c->ent_own, sizeof(double) * c->ne) != cudaSuccess ||
+            cudaMalloc(&c->filter_count, sizeof(unsigned long long)) != cudaSuccess ||
+            cudaMemset(c->filter_count, 0, sizeof(unsigned long long)) != cudaSuccess)
+            return cleanup(PDG_ERR_NOMEM);
+    }
     if (c->p.parabolic) {
         const size_t nfn = c->dim == 2 ? c->Np : c->Np * c->Np;
         if (cudaMalloc(&c->lbuf, sizeof(double) * c->dim * c->ne * nfn * c->nv) != cudaSuccess ||
@@ -498,7 +514,7 @@ int pdg_create(const pdg_mesh *mesh, const pdg_params *params, pdg_ctx **out)
         cudaMemset(c->lam_bits, 0, sizeof(unsigned long long)) || cudaMemset(c->err, 0, sizeof(unsigned int)))
         return cleanup(PDG_ERR_CUDA);
     for (int kind = 0; kind < KIND_COUNT; kind++) {
-        if (!kind_used(kind, c->dim, c->p.parabolic != 0)) continue;
+        if (!kind_used(kind, c->dim, c->p.parabolic != 0, c->p.filter != 0)) continue;
         int r = configure_launch(c, kind);
         if (r) return cleanup(r);
     }
@@ -521,6 +537,8 @@ int pdg_destroy(pdg_ctx *c)
     cudaFree(c->io_b);
     cudaFree(c->lam_bits);
     cudaFree(c->err);
+    cudaFree(c->ent_own);
+    cudaFree(c->filter_count);
     for (auto &t : c->timed) {
         cudaEventDestroy(t.a);
         cudaEventDestroy(t.b);
@@ -685,5 +703,19 @@ int pdg_check(pdg_ctx *c, uint32_t *flags)
 const char *pdg_last_error(const pdg_ctx *c) { return c ? c->last_error.c_str() : "null context"; }
 
 int64_t pdg_launch_count(const pdg_ctx *c) { return c ? c->launches : -1; }
+
+int pdg_filter_count(pdg_ctx *c, int64_t *filtered)
+{
+    if (!c || !filtered) return PDG_ERR_ARG;
+    if (!c->p.filter) {
+        *filtered = 0;
+        return PDG_OK;
+    }
+    unsigned long long n = 0;
+    CK(cudaStreamSynchronize(c->last_stream), "synchronize");
+    CK(cudaMemcpy(&n, c->filter_count, sizeof(n), cudaMemcpyDeviceToHost), "read filter count");
+    *filtered = (int64_t)n;
+    return PDG_OK;
+}
 
 }  // extern "C"

@@ -29,8 +29,8 @@ void fill_constants(int dim, int N, const double *h, DevConst &K, double &modal_
 // dynamic shared-memory limit).  No allocation.
 int kernel_config(int dim, int N, int kind, int64_t ne, int device, LaunchCfg *cfg, const char **why);
 
-// Whether a kernel kind takes part in the (dim, parabolic) right-hand side.
-bool kind_used(int kind, int dim, bool parabolic);
+// Whether a kernel kind takes part in the (dim, parabolic, filter) operator.
+bool kind_used(int kind, int dim, bool parabolic, bool filter);
 
 int launch_kernel(const LaunchCfg &cfg, KParams P, int64_t ne, cudaStream_t s);
 

@@ -14,7 +14,9 @@ enum KernelKind {
     KIND_FACE_NS0 = 7,   // face_kernel<dim, N, d, true>, d = 0, 1, 2
     KIND_FACE_NS1 = 8,
     KIND_FACE_NS2 = 9,
-    KIND_COUNT = 10
+    KIND_FILTER_BOUNDS = 10,  // filter_bounds_kernel<dim, N>: per-element entropy minimum
+    KIND_FILTER = 11,         // filter_kernel<dim, N>: entropy/positivity filter of the stage output
+    KIND_COUNT = 12
 };
 
 struct KernelInfo {

@@ -47,6 +47,7 @@ struct DevConst {
     double Dhat[36];    // D + boundary corrections (viscous volume term)
     double Dhat2[36];   // 2D + boundary corrections (flux differencing)
     double Vinv1[36];   // 1D inverse Legendre Vandermonde (modal transform)
+    double V1[36];      // 1D Legendre Vandermonde V1[i*Np + k] = L_k(x_i) (filter)
     double w[6];        // GLL weights on [0,1]
     double snor[3][7];  // subcell interface normals per direction
     double fv_scale[6]; // 1 / (J w_i)
@@ -67,6 +68,8 @@ struct KParams {
     double *eta_out, *alpha_out;
     unsigned long long *lam_bits;  // running max wave speed (as ordered bits)
     unsigned int *err;
+    double *ent_own;                    // filter: per-element entropy minimum at the stage input
+    unsigned long long *filter_count;   // filter: elements filtered so far
     int64_t ne, nnodes;
     int64_t nwt;          // number of warp tiles
     int stage;            // -1: plain RHS; 0, 1, 2: SSP-RK3 stage
@@ -170,28 +173,32 @@ template <int G> __device__ __forceinline__ double group_max(double x)
 #define C_FACE(c) ((c)[185])
 constexpr int CONST_SLOTS = 192;
 
-__device__ __forceinline__ void load_consts(const DevConst *K, double *c, int Np)
+__device__ __forceinline__ void load_consts(const DevConst *K, double *c, int Np, int tid, int nth)
 {
-    for (int t = threadIdx.x; t < Np * Np; t += blockDim.x) {
+    for (int t = tid; t < Np * Np; t += nth) {
         c[t] = K->D[t];
         c[36 + t] = K->Dhat[t];
         c[72 + t] = K->Dhat2[t];
         c[108 + t] = K->Vinv1[t];
     }
-    for (int t = threadIdx.x; t < Np; t += blockDim.x) {
+    for (int t = tid; t < Np; t += nth) {
         c[144 + t] = K->w[t];
         c[171 + t] = K->fv_scale[t];
     }
-    for (int t = threadIdx.x; t < 3 * 7; t += blockDim.x) c[150 + t] = (&K->snor[0][0])[t];
-    if (threadIdx.x < 3) {
-        c[177 + threadIdx.x] = K->adj[threadIdx.x];
-        c[180 + threadIdx.x] = K->area[threadIdx.x];
+    for (int t = tid; t < 3 * 7; t += nth) c[150 + t] = (&K->snor[0][0])[t];
+    for (int t = tid; t < 3; t += nth) {
+        c[177 + t] = K->adj[t];
+        c[180 + t] = K->area[t];
     }
-    if (threadIdx.x == 0) {
+    if (tid == 0) {
         c[183] = K->J;
         c[184] = K->invJ;
         c[185] = K->face_scale;
     }
+}
+__device__ __forceinline__ void load_consts(const DevConst *K, double *c, int Np)
+{
+    load_consts(K, c, Np, threadIdx.x, blockDim.x);
 }
 
 // Primitive quantities of a node from the shared slot (p and 1/rho are not
@@ -473,60 +480,58 @@ __device__ __forceinline__ double stage_coef(const KParams &P)
     return 2. / 3 * P.dt;
 }
 
-// Right-hand side element kernel (Euler or Navier-Stokes volume terms, face
-// buffer gather, optional SSP-RK3 stage).
-template <int DIM, int N, bool NS>
-__global__ void __launch_bounds__(128) rhs_kernel(const KParams P)
+template <int DIM, int N, int D>
+__device__ __forceinline__ void face_contrib(const KParams &P, const double *c, int64_t a, int fn, double coef,
+                                             double *C);
+
+// One warp tile of the right-hand side element kernel: EPW elements from
+// e_base, one lane group each.  Volume terms (flux differencing, subcell FV
+// blending) into acc, then either the stage output is stored and the face
+// terms are left to the face kernels (FACES = false), or (FACES = true, Euler)
+// every element also adds the face terms of its own face nodes, evaluated
+// with the same element-1 rule and in the same order (x faces, then y [, z])
+// as the face kernels use, and stores the finished stage.
+template <int DIM, int N, bool NS, bool FACES>
+__device__ __forceinline__ void rhs_tile(const KParams &P, const double *c, double *pr, int64_t e_base, int grp,
+                                         int gl, bool lane_used, unsigned int &flags, double &lam)
 {
     using S = Shape<DIM, N>;
-    constexpr int Np = S::Np, NDOF = S::NDOF, NV = S::NV, NFN = S::NFN, L = S::L, EPW = S::EPW;
-    extern __shared__ double smem[];
-    double *c = smem;
-    load_consts(P.K, c, Np);
-    __syncthreads();
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int grp = lane / L, gl = lane % L;
-    const int wpb = blockDim.x >> 5;
-    const bool lane_used = grp < EPW;
+    constexpr int Np = S::Np, NDOF = S::NDOF, NV = S::NV, NFN = S::NFN, L = S::L;
     constexpr int ST = S::NS_;
-    double *pr = smem + CONST_SLOTS + (size_t)(warp * EPW + (lane_used ? grp : 0)) * S::EL_RHS;
     double *acc = pr + S::NPRIM * ST, *scratch = acc, *zf = acc + NV * ST;
-    const int64_t wstride = (int64_t)gridDim.x * wpb;
     const bool compat = P.compat != 0;
-    unsigned int flags = 0;
-    double lam = 0.0;
-    for (int64_t wt = (int64_t)blockIdx.x * wpb + warp; wt < P.nwt; wt += wstride) {
-        const int64_t e0 = wt * EPW + grp;
-        const bool valid = lane_used && e0 < P.ne;
-        const int64_t e = valid ? e0 : 0;
-        if (lane_used) {
-            const double ls = stage_nodes<DIM, N>(P, e, valid, gl, pr, scratch, flags);
-            if (valid) lam = fmax(lam, ls);
+    const int64_t e0 = e_base + grp;
+    const bool valid = lane_used && e0 < P.ne;
+    const int64_t e = valid ? e0 : 0;
+    if (lane_used) {
+        const double ls = stage_nodes<DIM, N>(P, e, valid, gl, pr, scratch, flags);
+        if (valid) lam = fmax(lam, ls);
+    }
+    __syncwarp();
+    double alpha = 0.0;
+    if (P.blending) {
+        const double eta = indicator_eta<DIM, N>(scratch, gl, C_VINV(c));
+        alpha = blending_alpha(eta, P);
+        if (valid && gl == 0) {
+            P.eta_out[e] = eta;
+            P.alpha_out[e] = alpha;
         }
-        __syncwarp();
-        double alpha = 0.0;
-        if (P.blending) {
-            const double eta = indicator_eta<DIM, N>(scratch, gl, C_VINV(c));
-            alpha = blending_alpha(eta, P);
-            if (valid && gl == 0) {
-                P.eta_out[e] = eta;
-                P.alpha_out[e] = alpha;
-            }
-        }
-        const double sc = -(1.0 - alpha) * C_INVJ(c);
-        if (lane_used) {
-            const bool zfill = DIM == 3 && NS && compat;
+    }
+    const double sc = -(1.0 - alpha) * C_INVJ(c);
+    if (lane_used) {
+        const bool zfill = DIM == 3 && NS && compat;
 #pragma unroll 1
-            for (int d = 0; d < DIM; d++)
-                ec_lines_rt<DIM, N>(P, d, pr, acc, zf, c, gl, sc, zfill && d == 1, zfill && d == 2);
+        for (int d = 0; d < DIM; d++)
+            ec_lines_rt<DIM, N>(P, d, pr, acc, zf, c, gl, sc, zfill && d == 1, zfill && d == 2);
+    }
+    if (P.blending && __any_sync(0xffffffffu, alpha > 0.0)) {
+        if (lane_used) {
+            fv_lines<DIM, N, 0>(P, pr, acc, c, gl, alpha);
+            fv_lines<DIM, N, 1>(P, pr, acc, c, gl, alpha);
+            if (DIM == 3) fv_lines<DIM, N, (DIM == 3 ? 2 : 0)>(P, pr, acc, c, gl, alpha);
         }
-        if (P.blending && __any_sync(0xffffffffu, alpha > 0.0)) {
-            if (lane_used) {
-                fv_lines<DIM, N, 0>(P, pr, acc, c, gl, alpha);
-                fv_lines<DIM, N, 1>(P, pr, acc, c, gl, alpha);
-                if (DIM == 3) fv_lines<DIM, N, (DIM == 3 ? 2 : 0)>(P, pr, acc, c, gl, alpha);
-            }
-        }
+    }
+    if (!FACES) {
         // store: out = a un + b (us + dt V); the viscous volume term and the
         // face terms are added afterwards by lift_kernel and face_kernel
         if (valid) {
@@ -543,7 +548,81 @@ __global__ void __launch_bounds__(128) rhs_kernel(const KParams P)
             }
         }
         __syncwarp();
+        return;
     }
+    // element-centric faces: combine first, then add each direction's face
+    // terms in turn, then store
+    if (valid) {
+#pragma unroll
+        for (int k = 0; k < S::NPL; k++) {
+            const int n = gl + k * L;
+            if (n < NDOF) {
+#pragma unroll
+                for (int v = 0; v < NV; v++) {
+                    const int64_t gi = (int64_t)v * P.nnodes + e * NDOF + n;
+                    acc[v * ST + sp<Np>(n)] = stage_combine(P, gi, acc[v * ST + sp<Np>(n)]);
+                }
+            }
+        }
+    }
+    __syncwarp();
+    const double coef = stage_coef(P);
+#pragma unroll 1
+    for (int d = 0; d < DIM; d++) {
+        if (valid) {
+            for (int t = gl; t < 2 * NFN; t += L) {
+                const int side = t >= NFN, fn = side ? t - NFN : t;
+                // side 1: this element's +d face (it is element a); side 0:
+                // its -d face, whose element a is the -d neighbour
+                const int64_t a = side ? e : (int64_t)__ldg(P.nbr + e * 2 * DIM + 2 * d);
+                double C[NV];
+                if (d == 0) face_contrib<DIM, N, 0>(P, c, a, fn, coef, C);
+                else if (d == 1) face_contrib<DIM, N, 1>(P, c, a, fn, coef, C);
+                else face_contrib<DIM, N, (DIM == 3 ? 2 : 0)>(P, c, a, fn, coef, C);
+                const int n = sp<Np>(line_node_rt<DIM, Np>(d, fn, side ? N : 0));
+#pragma unroll
+                for (int v = 0; v < NV; v++) {
+                    if (side) acc[v * ST + n] += C[v];
+                    else acc[v * ST + n] -= C[v];
+                }
+            }
+        }
+        __syncwarp();
+    }
+    if (valid) {
+#pragma unroll
+        for (int k = 0; k < S::NPL; k++) {
+            const int n = gl + k * L;
+            if (n < NDOF) {
+#pragma unroll
+                for (int v = 0; v < NV; v++) P.out[(int64_t)v * P.nnodes + e * NDOF + n] = acc[v * ST + sp<Np>(n)];
+            }
+        }
+    }
+    __syncwarp();
+}
+
+// Right-hand side element kernel (Euler or Navier-Stokes volume terms,
+// optional SSP-RK3 stage).
+template <int DIM, int N, bool NS>
+__global__ void __launch_bounds__(128) rhs_kernel(const KParams P)
+{
+    using S = Shape<DIM, N>;
+    constexpr int Np = S::Np, L = S::L, EPW = S::EPW;
+    extern __shared__ double smem[];
+    double *c = smem;
+    load_consts(P.K, c, Np);
+    __syncthreads();
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int grp = lane / L, gl = lane % L;
+    const int wpb = blockDim.x >> 5;
+    const bool lane_used = grp < EPW;
+    double *pr = smem + CONST_SLOTS + (size_t)(warp * EPW + (lane_used ? grp : 0)) * S::EL_RHS;
+    const int64_t wstride = (int64_t)gridDim.x * wpb;
+    unsigned int flags = 0;
+    double lam = 0.0;
+    for (int64_t wt = (int64_t)blockIdx.x * wpb + warp; wt < P.nwt; wt += wstride)
+        rhs_tile<DIM, N, NS, false>(P, c, pr, wt * EPW, grp, gl, lane_used, flags, lam);
     lam = group_max<32>(lam);
     if (lane == 0) atomic_max_pos(P.lam_bits, lam);
     flags = __reduce_or_sync(0xffffffffu, flags);
@@ -585,12 +664,12 @@ __device__ __forceinline__ Prim<DIM> velocity_slot_prim(const Prim<DIM> &q, doub
 // the face states' momenta in place before ComputeFaceFlux reads them,
 // BasicOperations.cpp:33-34, DGSEMIntegrator.cpp:467-481).
 template <int DIM, int N, int D, bool NS>
-__device__ __forceinline__ double face_node(const KParams &P, const double *c, int64_t a, int fn, double coef)
+__device__ __forceinline__ double face_node_terms(const KParams &P, const double *c, int64_t a, int64_t b, int fn,
+                                                  double coef, double *C)
 {
     using S = Shape<DIM, N>;
     constexpr int Np = S::Np, NDOF = S::NDOF, NV = S::NV, NFN = S::NFN;
     const int64_t nn = P.nnodes;
-    const int64_t b = __ldg(P.nbr + a * 2 * DIM + 2 * D + 1);
     const int na = line_node<DIM, Np, D>(fn, N), nb = line_node<DIM, Np, D>(fn, 0);
     double sa[NV], sb[NV];
 #pragma unroll
@@ -627,7 +706,6 @@ __device__ __forceinline__ double face_node(const KParams &P, const double *c, i
     if (a_is_1) face_flux<DIM, D>(qa, qb, ma, mb, nrm, P.gm1inv, compat, P.diss_scale, F);
     else face_flux<DIM, D>(qb, qa, mb, ma, nrm, P.gm1inv, compat, P.diss_scale, F);
     const double sc = C_FACE(c) * coef;
-    double C[NV];
     C[0] = sc * (a_is_1 ? -F[0] : F[0]);
 #pragma unroll
     for (int i = 0; i <= DIM; i++) {
@@ -638,12 +716,35 @@ __device__ __forceinline__ double face_node(const KParams &P, const double *c, i
         }
         C[1 + i] = sc * du;
     }
+    return lam;
+}
+
+template <int DIM, int N, int D, bool NS>
+__device__ __forceinline__ double face_node(const KParams &P, const double *c, int64_t a, int fn, double coef)
+{
+    using S = Shape<DIM, N>;
+    constexpr int Np = S::Np, NDOF = S::NDOF, NV = S::NV;
+    const int64_t nn = P.nnodes;
+    const int64_t b = __ldg(P.nbr + a * 2 * DIM + 2 * D + 1);
+    double C[NV];
+    const double lam = face_node_terms<DIM, N, D, NS>(P, c, a, b, fn, coef, C);
+    const int na = line_node<DIM, Np, D>(fn, N), nb = line_node<DIM, Np, D>(fn, 0);
 #pragma unroll
     for (int v = 0; v < NV; v++) {
         P.out[v * nn + a * NDOF + na] += C[v];
         P.out[v * nn + b * NDOF + nb] -= C[v];
     }
     return lam;
+}
+
+// Euler face terms C of the face node (a's +D face, node fn) for the
+// element-centric face pass of rhs_tile.
+template <int DIM, int N, int D>
+__device__ __forceinline__ void face_contrib(const KParams &P, const double *c, int64_t a, int fn, double coef,
+                                             double *C)
+{
+    const int64_t b = __ldg(P.nbr + a * 2 * DIM + 2 * D + 1);
+    face_node_terms<DIM, N, D, false>(P, c, a, b, fn, coef, C);
 }
 
 // Face kernel of direction D: one thread per (element, face node).  Within one
