@@ -11,6 +11,10 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+// Pointwise functions compile for host and device, so that host-side checks
+// can run them on the CPU.
+#define PDG_FN __host__ __device__ __forceinline__
+
 namespace pdg {
 
 // Log-mean (y - x) / (ln y - ln x) of ComputeLogMean
@@ -18,7 +22,7 @@ namespace pdg {
 // u = f^2 (equal to the reference's (xi-1)^2/(xi+1)^2, xi = y/x), the series
 // branch u < 1e-4 is (x+y) 52.5 / (105 + u(35 + u(21 + 15u))), otherwise
 // (y-x)/log(y/x).  Returns the mean and its reciprocal; `is` = 1/(x+y).
-__device__ __forceinline__ void logmean_inv(double x, double y, double s, double is, double &mean, double &inv)
+PDG_FN void logmean_inv(double x, double y, double s, double is, double &mean, double &inv)
 {
     const double f = (y - x) * is;
     const double u = f * f;
@@ -33,7 +37,7 @@ __device__ __forceinline__ void logmean_inv(double x, double y, double s, double
     }
 }
 // Reciprocal of the log-mean only.
-__device__ __forceinline__ double logmean_recip(double x, double y, double is)
+PDG_FN double logmean_recip(double x, double y, double is)
 {
     const double f = (y - x) * is;
     const double u = f * f;
@@ -48,7 +52,7 @@ template <int DIM> struct Prim {
     double rho, irho, v[DIM], p, beta, ib, lam;
 };
 
-template <int DIM> __device__ __forceinline__ Prim<DIM> make_prim(const double *s, double gamma, double gm1)
+template <int DIM> PDG_FN Prim<DIM> make_prim(const double *s, double gamma, double gm1)
 {
     Prim<DIM> q;
     q.rho = s[0];
@@ -69,7 +73,7 @@ template <int DIM> __device__ __forceinline__ Prim<DIM> make_prim(const double *
 // ChandrashekarFlux::ComputeVolumeFlux (ChandrashekarFlux.cpp:11-83) for a
 // contravariant metric `metric` along axis DIR.
 template <int DIM, int DIR>
-__device__ __forceinline__ void volume_flux(const Prim<DIM> &a, const Prim<DIM> &b, double metric, double gm1inv,
+PDG_FN void volume_flux(const Prim<DIM> &a, const Prim<DIM> &b, double metric, double gm1inv,
                                             double *F)
 {
     const double sr = a.rho + b.rho, isr = 1.0 / sr;
@@ -96,7 +100,7 @@ __device__ __forceinline__ void volume_flux(const Prim<DIM> &a, const Prim<DIM> 
 
 // Same flux for a runtime direction d.
 template <int DIM>
-__device__ __forceinline__ void volume_flux_rt(const Prim<DIM> &a, const Prim<DIM> &b, int dir, double metric,
+PDG_FN void volume_flux_rt(const Prim<DIM> &a, const Prim<DIM> &b, int dir, double metric,
                                                double gm1inv, double *F)
 {
     const double sr = a.rho + b.rho, isr = 1.0 / sr;
@@ -129,7 +133,7 @@ __device__ __forceinline__ void volume_flux_rt(const Prim<DIM> &a, const Prim<DI
 // momenta whose jump the Lax-Friedrichs term uses; compat keeps the 3D
 // energy term as the reference writes it (`rho_mean * dw + w_mean`, :131).
 template <int DIM, int DIR>
-__device__ __forceinline__ void face_flux(const Prim<DIM> &a, const Prim<DIM> &b, const double *ma, const double *mb,
+PDG_FN void face_flux(const Prim<DIM> &a, const Prim<DIM> &b, const double *ma, const double *mb,
                                           double nrm, double gm1inv, bool compat, double diss_scale, double *F)
 {
     const double sr = a.rho + b.rho, isr = 1.0 / sr;
@@ -167,7 +171,7 @@ __device__ __forceinline__ void face_flux(const Prim<DIM> &a, const Prim<DIM> &b
 // rows out[0..DIM-1] and the energy row out[DIM].  g(d, v) returns the
 // primitive gradient of variable v along x_d.
 template <int DIM, class Grad>
-__device__ __forceinline__ void viscous_col(const Prim<DIM> &q, const Grad &g, int dir, double gm1inv, double mu,
+PDG_FN void viscous_col(const Prim<DIM> &q, const Grad &g, int dir, double gm1inv, double mu,
                                             double lambda_k, double *out)
 {
     double div = 0.0;
@@ -188,7 +192,7 @@ __device__ __forceinline__ void viscous_col(const Prim<DIM> &q, const Grad &g, i
 // Conserv2Entropy (BasicOperations.cpp:134-157): beta = rho / p,
 // s = ln p - gamma ln rho.
 template <int DIM>
-__device__ __forceinline__ void entropy_vars(const double *s, double gamma, double gm1, double gm1inv, double *w)
+PDG_FN void entropy_vars(const double *s, double gamma, double gm1, double gm1inv, double *w)
 {
     const double rho = s[0], irho = 1.0 / rho;
     double vel[DIM], vv = 0.0;
@@ -212,7 +216,7 @@ __device__ __forceinline__ void entropy_vars(const double *s, double gamma, doub
 // exit.  compat keeps the reference's density term, which reads velocities
 // where the formula means momenta (its row copy is divided in place, :190-191).
 template <int DIM>
-__device__ __forceinline__ void entgrad_to_primgrad(const double *s, double gm1, double gm1inv, bool compat, double *g)
+PDG_FN void entgrad_to_primgrad(const double *s, double gm1, double gm1inv, bool compat, double *g)
 {
     const double rho = s[0], irho = 1.0 / rho;
     double vel[DIM], vv = 0.0;
