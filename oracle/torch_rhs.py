@@ -82,6 +82,12 @@ def logmean(x, y):
     return torch.where(small, series, direct)
 
 
+def _norm(vsq):
+    """sqrt(vsq) with a zero (not NaN) derivative at vsq = 0."""
+    pos = vsq > 0
+    return torch.where(pos, torch.sqrt(torch.where(pos, vsq, torch.ones_like(vsq))), torch.zeros_like(vsq))
+
+
 class TorchDGSEM:
     """RHS of the fixed DGSEM operator on a periodic Cartesian mesh."""
 
@@ -166,8 +172,8 @@ class TorchDGSEM:
         h = h + 0.5 / (beta_ln * self.gm1) + p_hat / rho_ln
         diss = sum(0.5 * drho * va[k] * vb[k] + rho_mean * (vb[k] - va[k]) * vm[k] for k in range(self.dim))
         diss = diss + 0.5 * drho / (self.gm1 * beta_ln) + 0.5 * rho_mean / self.gm1 * (1.0 / bb - 1.0 / ba)
-        la = torch.sqrt(sum(v * v for v in va)) + torch.sqrt(self.gamma * pa / ra)
-        lb = torch.sqrt(sum(v * v for v in vb)) + torch.sqrt(self.gamma * pb / rb)
+        la = _norm(sum(v * v for v in va)) + torch.sqrt(self.gamma * pa / ra)
+        lb = _norm(sum(v * v for v in vb)) + torch.sqrt(self.gamma * pb / rb)
         lam = 0.5 * torch.maximum(la, lb) * self.diss * abs(nrm)
         fm = rho_ln * vm[d] * nrm
         F = [fm - lam * drho]
@@ -243,7 +249,7 @@ class TorchDGSEM:
     # ---- operator ----
     def alpha(self, s):
         if not self.blending:
-            return torch.zeros(self.ne, dtype=s.dtype)
+            return torch.zeros(self.ne, dtype=s[0].dtype)
         rho, vel, p = self.prims(s)
         q = rho * p  # [ne, ...]
         m = q
