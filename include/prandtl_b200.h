@@ -179,6 +179,16 @@ int pdg_get_blending(pdg_ctx *ctx, double *eta_host, double *alpha_host);
  * only keeps the viscous fluxes derived from them. */
 int pdg_gradients(pdg_ctx *ctx, const double *u, double *grads, void *stream);
 
+/* Adjoint (vector-Jacobian product) of the right-hand side: ubar =
+ * (dL/du)^T cot, with L = DGSEMOperator::Mult (DGSEMOperator.cpp:537-591) in
+ * its fixed form; the reference has no adjoint.  Requires params.compat = 0
+ * (PDG_ERR_UNSUPPORTED otherwise).  The blending coefficient is
+ * differentiated where its sigmoid is active and is constant where it is
+ * snapped or capped.  u, cot, ubar: DEVICE pointers, byNODES; ubar is
+ * overwritten and aliases neither input.  The first call allocates the
+ * Navier-Stokes adjoint scratch. */
+int pdg_rhs_vjp(pdg_ctx *ctx, const double *u, const double *cot, double *ubar, void *stream);
+
 /* Entropy filter (params.filter = 1): EntropyFilter::FilterSolution
  * (src/Filters/EntropyFilter.cpp:171-242) after every RK stage, with the
  * element bounds of GetEntropyConstraints (:81-158) taken at the stage input.
@@ -209,6 +219,10 @@ int64_t pdg_launch_count(const pdg_ctx *ctx);
 #define PDG_KERNEL_FACE_NS0  7  /* Navier-Stokes face kernels, x / y / z (7, 8, 9) */
 #define PDG_KERNEL_FILTER_BOUNDS 10  /* entropy filter: per-element entropy minimum */
 #define PDG_KERNEL_FILTER    11  /* entropy filter of a stage output */
+#define PDG_KERNEL_ADJ_RHS   12  /* adjoint: inviscid volume terms and blending */
+#define PDG_KERNEL_ADJ_LIFT  13  /* adjoint: viscous terms */
+#define PDG_KERNEL_ADJ_FACE_E0  14  /* adjoint Euler face kernels, x / y / z (14, 15, 16) */
+#define PDG_KERNEL_ADJ_FACE_NS0 17  /* adjoint Navier-Stokes face kernels (17, 18, 19) */
 int pdg_profile_enable(pdg_ctx *ctx, int on);
 int pdg_profile_read(pdg_ctx *ctx, int kind, double *total_ms, int64_t *launches);
 

@@ -34,6 +34,9 @@ KERNEL_EULER, KERNEL_LIFT, KERNEL_NS, KERNEL_LIFT_FACE = 0, 1, 2, 3
 KERNEL_FACE_EULER = (4, 5, 6)
 KERNEL_FACE_NS = (7, 8, 9)
 KERNEL_FILTER_BOUNDS, KERNEL_FILTER = 10, 11
+KERNEL_ADJ_RHS, KERNEL_ADJ_LIFT = 12, 13
+KERNEL_ADJ_FACE_EULER = (14, 15, 16)
+KERNEL_ADJ_FACE_NS = (17, 18, 19)
 PDG_FLAG_NONFINITE = 1
 PDG_FLAG_NONPHYSICAL = 2
 _STATUS = {1: "bad argument", 2: "CUDA error", 3: "non-finite state", 4: "non-physical state",
@@ -111,6 +114,7 @@ def library():
     L.pdg_batch_last_error.restype = C.c_char_p
     L.pdg_batch_last_error.argtypes = [vp]
     L.pdg_filter_count.argtypes = [C.c_void_p, C.POINTER(C.c_int64)]
+    L.pdg_rhs_vjp.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
     L.pdg_rhs_noalloc.argtypes = [C.POINTER(PdgMesh), C.POINTER(PdgParams), C.c_void_p, C.c_void_p, C.c_void_p]
     _lib = L
     return L
@@ -265,6 +269,17 @@ class DGSEMOperator:
         f = C.c_uint32()
         self._call(library().pdg_check(self._ctx, C.byref(f)), "pdg_check")
         return f.value
+
+    def vjp(self, u, cot, out=None, stream=None):
+        """(dL/du)^T cot for device tensors u, cot (fixed operator, compat=0)."""
+        import torch
+        self._check_dev(u, cot)
+        ubar = out if out is not None else torch.empty_like(u)
+        self._check_dev(ubar)
+        self._call(library().pdg_rhs_vjp(self._ctx, C.c_void_p(u.data_ptr()), C.c_void_p(cot.data_ptr()),
+                                         C.c_void_p(ubar.data_ptr()), C.c_void_p(_stream_handle(stream))),
+                   "pdg_rhs_vjp")
+        return ubar
 
     def filter_count(self) -> int:
         """Element filterings by the entropy filter since creation (synchronises)."""

@@ -14,7 +14,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB_DIR = os.path.join(HERE, "_lib")
 LIB = os.path.join(LIB_DIR, "libprandtl_b200.so")
-SOURCES = ["capi.cu", "kernels_2d.cu", "kernels_3d.cu", "noalloc.cu", "batch.cu"]
+SOURCES = ["capi.cu", "kernels_2d.cu", "kernels_3d.cu", "noalloc.cu", "batch.cu", "adjoint_2d.cu", "adjoint_3d.cu"]
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-O3", "-lineinfo", "-std=c++17",
          "-Xcompiler", "-fPIC", "-Xcompiler", "-O3"]

@@ -1,0 +1,634 @@
+// adjoint_kernels.cuh — vector-Jacobian product of the fixed (compat = 0)
+// right-hand side: given a cotangent lam of dudt, ubar = (dL/du)^T lam.
+//
+// The kernels mirror the forward ones in reverse:
+//   adj_rhs_kernel   flux-differencing volume terms, subcell FV blending and
+//                    the blending coefficient (indicator) — stores ubar;
+//   adj_lift_kernel  (Navier-Stokes) viscous volume divergence, face viscous
+//                    columns, viscous fluxes, primitive-gradient conversion
+//                    and the BR1 volume lifting — adds to ubar and leaves the
+//                    cotangents of the face-normal entropy gradients in gcol;
+//   adj_face_kernel  per direction: Riemann fluxes and (Navier-Stokes) the
+//                    BR1 face jumps — adds to ubar at face nodes.
+// The reference has no adjoint; each reversed step names the forward
+// function it reverses.
+#pragma once
+
+#include "adjoint_physics.cuh"
+#include "line_kernels.cuh"
+
+namespace pdg {
+
+template <int DIM, int N> struct AdjShape {
+    using S = Shape<DIM, N>;
+    // slot: primitives (rho, v, beta), cotangent lam, primitive cotangents,
+    // scratch (indicator input / modal buffers / forward volume sums)
+    static constexpr int EL = 4 * S::NV * S::NS_;
+};
+
+// Line index (within direction d) and position of node n = (i, j, k).
+template <int DIM, int Np> __device__ __forceinline__ int line_of(int d, const int *idx)
+{
+    return d == 0 ? (DIM == 2 ? idx[1] : idx[1] + Np * idx[2])
+                  : (d == 1 ? (DIM == 2 ? idx[0] : idx[0] + Np * idx[2]) : idx[0] + Np * idx[1]);
+}
+
+// Transposed 1D modal pass: dst[line, l] = sum_k Vinv(k, l) src[line, k].
+template <int DIM, int N, int D>
+__device__ __forceinline__ void modal_pass_t(const double *src, double *dst, int gl, const double *Vinv)
+{
+    using S = Shape<DIM, N>;
+    constexpr int Np = S::Np;
+#pragma unroll
+    for (int r = 0; r < S::LPL; r++) {
+        const int line = gl + r * S::L;
+        if (line < S::NFN) {
+            double x[Np];
+#pragma unroll
+            for (int k = 0; k < Np; k++) x[k] = src[sp<Np>(line_node<DIM, Np, D>(line, k))];
+#pragma unroll
+            for (int l = 0; l < Np; l++) {
+                double s = 0.0;
+#pragma unroll
+                for (int k = 0; k < Np; k++) s += Vinv[k * Np + l] * x[k];
+                dst[sp<Np>(line_node<DIM, Np, D>(line, l))] = s;
+            }
+        }
+    }
+    __syncwarp();
+}
+
+// Reverse of the flux-differencing line tasks (ec_lines_rt) along d: pair
+// (a, b) contributes scale (Dhat2(a,b) lam_a + Dhat2(b,a) lam_b) as the
+// cotangent of its two-point flux.
+template <int DIM, int N>
+__device__ __forceinline__ void ec_lines_vjp(const KParams &P, int d, const double *pr, const double *lm, double *pb,
+                                             const double *c, int gl, double scale)
+{
+    using S = Shape<DIM, N>;
+    constexpr int Np = S::Np, NV = S::NV, ST = S::NS_;
+    using PS = PSlot<DIM>;
+    const double metric = C_ADJ(c)[d];
+    const double *D2 = C_DHAT2(c);
+#pragma unroll 1
+    for (int r = 0; r < S::LPL; r++) {
+        const int line = gl + r * S::L;
+        if (line < S::NFN) {
+            Prim<DIM> q[Np];
+            PBar<DIM> qb[Np];
+#pragma unroll
+            for (int l = 0; l < Np; l++) {
+                q[l] = slot_prim<DIM>(pr, sp<Np>(line_node_rt<DIM, Np>(d, line, l)), ST);
+                pbar_zero(qb[l]);
+            }
+#pragma unroll
+            for (int a = 0; a < Np; a++)
+#pragma unroll
+                for (int b = a + 1; b < Np; b++) {
+                    const int na = sp<Np>(line_node_rt<DIM, Np>(d, line, a));
+                    const int nb = sp<Np>(line_node_rt<DIM, Np>(d, line, b));
+                    const double cab = scale * D2[a * Np + b], cba = scale * D2[b * Np + a];
+                    double Fb[NV];
+#pragma unroll
+                    for (int v = 0; v < NV; v++) Fb[v] = cab * lm[v * ST + na] + cba * lm[v * ST + nb];
+                    volume_flux_vjp<DIM>(q[a], q[b], d, metric, P.gm1inv, Fb, qb[a], qb[b]);
+                }
+#pragma unroll
+            for (int l = 0; l < Np; l++) {
+                const int n = sp<Np>(line_node_rt<DIM, Np>(d, line, l));
+                pb[P_RHO * ST + n] += qb[l].rho;
+#pragma unroll
+                for (int k = 0; k < DIM; k++) pb[(P_V + k) * ST + n] += qb[l].v[k];
+                pb[PS::BETA * ST + n] += qb[l].beta;
+            }
+        }
+    }
+    __syncwarp();
+}
+
+// Reverse of the subcell finite-volume line tasks (fv_lines) along D:
+// interface flux F_{l+1/2} enters node l with -alpha fvs_l and node l+1 with
+// +alpha fvs_{l+1}; its momenta are rho v of the slot primitives.
+template <int DIM, int N, int D>
+__device__ __forceinline__ void fv_lines_vjp(const KParams &P, const double *pr, const double *lm, double *pb,
+                                             const double *c, int gl, double alpha)
+{
+    using S = Shape<DIM, N>;
+    constexpr int Np = S::Np, NV = S::NV, ST = S::NS_;
+    using PS = PSlot<DIM>;
+    const double *sn = C_SNOR(c, D), *fvs = C_FVS(c);
+#pragma unroll
+    for (int r = 0; r < S::LPL; r++) {
+        const int line = gl + r * S::L;
+        if (line < S::NFN) {
+#pragma unroll 1
+            for (int l = 0; l < N; l++) {
+                const int na = sp<Np>(line_node<DIM, Np, D>(line, l)), nb = sp<Np>(line_node<DIM, Np, D>(line, l + 1));
+                Prim<DIM> qa = slot_prim<DIM>(pr, na, ST), qb = slot_prim<DIM>(pr, nb, ST);
+                complete_prim<DIM>(qa, P.gamma);
+                complete_prim<DIM>(qb, P.gamma);
+                double ma[DIM], mb[DIM], mab[DIM], mbb[DIM];
+#pragma unroll
+                for (int k = 0; k < DIM; k++) {
+                    ma[k] = qa.rho * qa.v[k];
+                    mb[k] = qb.rho * qb.v[k];
+                    mab[k] = mbb[k] = 0.0;
+                }
+                double Fb[NV];
+#pragma unroll
+                for (int v = 0; v < NV; v++) Fb[v] = alpha * (fvs[l + 1] * lm[v * ST + nb] - fvs[l] * lm[v * ST + na]);
+                PBar<DIM> ab, bb;
+                pbar_zero(ab);
+                pbar_zero(bb);
+                face_flux_vjp<DIM>(qa, qb, ma, mb, D, sn[l + 1], P.gamma, P.gm1inv, P.diss_scale, Fb, ab, bb, mab, mbb);
+#pragma unroll
+                for (int k = 0; k < DIM; k++) {
+                    ab.rho += mab[k] * qa.v[k];
+                    ab.v[k] += mab[k] * qa.rho;
+                    bb.rho += mbb[k] * qb.v[k];
+                    bb.v[k] += mbb[k] * qb.rho;
+                }
+                pb[P_RHO * ST + na] += ab.rho;
+                pb[P_RHO * ST + nb] += bb.rho;
+#pragma unroll
+                for (int k = 0; k < DIM; k++) {
+                    pb[(P_V + k) * ST + na] += ab.v[k];
+                    pb[(P_V + k) * ST + nb] += bb.v[k];
+                }
+                pb[PS::BETA * ST + na] += ab.beta;
+                pb[PS::BETA * ST + nb] += bb.beta;
+            }
+        }
+    }
+    __syncwarp();
+}
+
+// Reverse of the blending coefficient for one lane group (an element):
+// etab is the cotangent of eta; adds the primitive cotangents of q = rho p to
+// pb.  scr holds two modal buffers of the slot's scratch region.
+template <int DIM, int N>
+__device__ __forceinline__ void indicator_vjp(const double *pr, double *pb, double *scr, const double *c, int gl,
+                                              double etab)
+{
+    using S = Shape<DIM, N>;
+    using PS = PSlot<DIM>;
+    constexpr int Np = S::Np, NDOF = S::NDOF, L = S::L, ST = S::NS_;
+#pragma unroll
+    for (int k = 0; k < S::NPL; k++) {
+        const int n = gl + k * L;
+        if (n < NDOF) {
+            const int m = sp<Np>(n);
+            const double rho = pr[P_RHO * ST + m], beta = pr[PS::BETA * ST + m];
+            scr[m] = rho * (0.5 * rho / beta);
+        }
+    }
+    __syncwarp();
+    double *qa = scr, *qb = scr + ST;
+    modal_pass<DIM, N, 0>(qa, qb, gl, C_VINV(c));
+    modal_pass<DIM, N, 1>(qb, qa, gl, C_VINV(c));
+    if (DIM == 3) modal_pass<DIM, N, (DIM == 3 ? 2 : 0)>(qa, qb, gl, C_VINV(c));
+    double *mo = (DIM == 3) ? qb : qa, *other = (DIM == 3) ? qa : qb;
+    double mm = 0.0, m1 = 0.0, m2 = 0.0;
+#pragma unroll
+    for (int k = 0; k < S::NPL; k++) {
+        const int t = gl + k * L;
+        if (t < NDOF) {
+            const int i = t % Np, j = (t / Np) % Np, kk = DIM == 3 ? t / (Np * Np) : 0;
+            int mx = i > j ? i : j;
+            if (DIM == 3) mx = mx > kk ? mx : kk;
+            const double v = mo[sp<Np>(t)] * mo[sp<Np>(t)];
+            mm += v;
+            if (mx <= N - 1) m1 += v;
+            if (mx <= N - 2) m2 += v;
+        }
+    }
+    mm = group_sum<L>(mm);
+    m1 = group_sum<L>(m1);
+    m2 = group_sum<L>(m2);
+    // eta = max(1 - m1/mm, 1 - m2/m1)
+    double mmb = 0.0, m1b = 0.0, m2b = 0.0;
+    if (1.0 - m1 / mm >= 1.0 - m2 / m1) {
+        mmb = etab * m1 / (mm * mm);
+        m1b = -etab / mm;
+    } else {
+        m1b = etab * m2 / (m1 * m1);
+        m2b = -etab / m1;
+    }
+    __syncwarp();
+#pragma unroll
+    for (int k = 0; k < S::NPL; k++) {
+        const int t = gl + k * L;
+        if (t < NDOF) {
+            const int i = t % Np, j = (t / Np) % Np, kk = DIM == 3 ? t / (Np * Np) : 0;
+            int mx = i > j ? i : j;
+            if (DIM == 3) mx = mx > kk ? mx : kk;
+            const double w = mmb + (mx <= N - 1 ? m1b : 0.0) + (mx <= N - 2 ? m2b : 0.0);
+            mo[sp<Np>(t)] = 2.0 * mo[sp<Np>(t)] * w;
+        }
+    }
+    __syncwarp();
+    if (DIM == 3) {
+        modal_pass_t<DIM, N, (DIM == 3 ? 2 : 0)>(mo, other, gl, C_VINV(c));
+        modal_pass_t<DIM, N, 1>(other, mo, gl, C_VINV(c));
+        modal_pass_t<DIM, N, 0>(mo, other, gl, C_VINV(c));
+    } else {
+        modal_pass_t<DIM, N, 1>(mo, other, gl, C_VINV(c));
+        modal_pass_t<DIM, N, 0>(other, mo, gl, C_VINV(c));
+    }
+    const double *qbar = (DIM == 3) ? other : mo;
+    // q = rho p with p = rho / (2 beta)
+#pragma unroll
+    for (int k = 0; k < S::NPL; k++) {
+        const int n = gl + k * L;
+        if (n < NDOF) {
+            const int m = sp<Np>(n);
+            const double rho = pr[P_RHO * ST + m], beta = pr[PS::BETA * ST + m];
+            const double p = 0.5 * rho / beta, g = qbar[m];
+            const double pbar = g * rho;
+            pb[P_RHO * ST + m] += g * p + pbar * 0.5 / beta;
+            pb[PS::BETA * ST + m] -= pbar * 0.5 * rho / (beta * beta);
+        }
+    }
+    __syncwarp();
+}
+
+// Adjoint of the inviscid volume terms and the blending coefficient; stores
+// ubar = cotangent of u through those terms.
+template <int DIM, int N>
+__global__ void __launch_bounds__(128) adj_rhs_kernel(const KParams P, const double *__restrict__ cot,
+                                                      double *__restrict__ ubar)
+{
+    using S = Shape<DIM, N>;
+    using PS = PSlot<DIM>;
+    constexpr int Np = S::Np, NDOF = S::NDOF, NV = S::NV, L = S::L, EPW = S::EPW, ST = S::NS_;
+    extern __shared__ double smem[];
+    double *c = smem;
+    load_consts(P.K, c, Np);
+    __syncthreads();
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int grp = lane / L, gl = lane % L;
+    const int wpb = blockDim.x >> 5;
+    // EPW * L = 32: every lane belongs to an element slot
+    double *pr = smem + CONST_SLOTS + (size_t)(warp * EPW + grp) * AdjShape<DIM, N>::EL;
+    double *lm = pr + NV * ST, *pb = lm + NV * ST, *scr = pb + NV * ST;
+    const int64_t nn = P.nnodes;
+    const int64_t wstride = (int64_t)gridDim.x * wpb;
+    for (int64_t wt = (int64_t)blockIdx.x * wpb + warp; wt < P.nwt; wt += wstride) {
+        const int64_t e0 = wt * EPW + grp;
+        const bool valid = e0 < P.ne;
+        const int64_t e = valid ? e0 : 0;
+#pragma unroll
+        for (int k = 0; k < S::NPL; k++) {
+            const int n = gl + k * L;
+            if (n < NDOF) {
+                double s[NV];
+#pragma unroll
+                for (int v = 0; v < NV; v++)
+                    s[v] = valid ? __ldg(P.u + v * nn + e * NDOF + n) : (v == 0 ? 1.0 : (v == NV - 1 ? P.gm1inv : 0.0));
+                const Prim<DIM> q = make_prim<DIM>(s, P.gamma, P.gm1);
+                const int m = sp<Np>(n);
+                pr[P_RHO * ST + m] = q.rho;
+#pragma unroll
+                for (int d = 0; d < DIM; d++) pr[(P_V + d) * ST + m] = q.v[d];
+                pr[PS::BETA * ST + m] = q.beta;
+                scr[m] = q.rho * q.p;
+#pragma unroll
+                for (int v = 0; v < NV; v++) {
+                    lm[v * ST + m] = valid ? __ldg(cot + v * nn + e * NDOF + n) : 0.0;
+                    pb[v * ST + m] = 0.0;
+                }
+            }
+        }
+        __syncwarp();
+        double alpha = 0.0, dalpha = 0.0;
+        if (P.blending) {
+            const double eta = indicator_eta<DIM, N>(scr, gl, C_VINV(c));
+            alpha = blending_alpha(eta, P);
+            const double T = P.modal_threshold;
+            const double a = 1.0 / (1.0 + exp(-9.21024 * (eta - T) / T));
+            if (a >= P.alpha_min && a <= 1.0 - P.alpha_min && a < P.alpha_max) dalpha = a * (1.0 - a) * 9.21024 / T;
+        }
+        // blending coefficient: d(acc)/d(alpha) = invJ EC + FV; alpha <- eta <- rho p
+        if (__any_sync(0xffffffffu, dalpha != 0.0)) {
+#pragma unroll 1
+            for (int d = 0; d < DIM; d++) ec_lines_rt<DIM, N>(P, d, pr, scr, nullptr, c, gl, C_INVJ(c), false, false);
+            fv_lines<DIM, N, 0>(P, pr, scr, c, gl, 1.0);
+            fv_lines<DIM, N, 1>(P, pr, scr, c, gl, 1.0);
+            if (DIM == 3) fv_lines<DIM, N, (DIM == 3 ? 2 : 0)>(P, pr, scr, c, gl, 1.0);
+            double abar = 0.0;
+#pragma unroll
+            for (int k = 0; k < S::NPL; k++) {
+                const int n = gl + k * L;
+                if (n < NDOF)
+#pragma unroll
+                    for (int v = 0; v < NV; v++) abar += lm[v * ST + sp<Np>(n)] * scr[v * ST + sp<Np>(n)];
+            }
+            abar = group_sum<L>(abar);
+            __syncwarp();
+            indicator_vjp<DIM, N>(pr, pb, scr, c, gl, valid ? abar * dalpha : 0.0);
+        }
+        const double sc = -(1.0 - alpha) * C_INVJ(c);
+#pragma unroll 1
+        for (int d = 0; d < DIM; d++) ec_lines_vjp<DIM, N>(P, d, pr, lm, pb, c, gl, sc);
+        if (P.blending && __any_sync(0xffffffffu, alpha > 0.0)) {
+            fv_lines_vjp<DIM, N, 0>(P, pr, lm, pb, c, gl, alpha);
+            fv_lines_vjp<DIM, N, 1>(P, pr, lm, pb, c, gl, alpha);
+            if (DIM == 3) fv_lines_vjp<DIM, N, (DIM == 3 ? 2 : 0)>(P, pr, lm, pb, c, gl, alpha);
+        }
+        if (valid) {
+#pragma unroll
+            for (int k = 0; k < S::NPL; k++) {
+                const int n = gl + k * L;
+                if (n < NDOF) {
+                    const int m = sp<Np>(n);
+                    double s[NV], sb[NV];
+#pragma unroll
+                    for (int v = 0; v < NV; v++) {
+                        s[v] = __ldg(P.u + v * nn + e * NDOF + n);
+                        sb[v] = 0.0;
+                    }
+                    PBar<DIM> b;
+                    pbar_zero(b);
+                    b.rho = pb[P_RHO * ST + m];
+#pragma unroll
+                    for (int d = 0; d < DIM; d++) b.v[d] = pb[(P_V + d) * ST + m];
+                    b.beta = pb[PS::BETA * ST + m];
+                    pbar_to_cons<DIM>(s, b, nullptr, P.gm1, sb);
+#pragma unroll
+                    for (int v = 0; v < NV; v++) ubar[v * nn + e * NDOF + n] = sb[v];
+                }
+            }
+        }
+        __syncwarp();
+    }
+}
+
+// Adjoint of the viscous terms (lift_kernel in reverse).  cot: cotangent of
+// dudt; P.lbuf holds the forward BR1 face jumps (lift_face_kernel of u);
+// gcol receives, at every face node, the cotangent of the face-normal
+// entropy-variable gradient ([d][side][e][face node][v]).
+template <int DIM, int N>
+__global__ void __launch_bounds__(128) adj_lift_kernel(const KParams P, const double *__restrict__ cot,
+                                                       double *__restrict__ ubar, double *__restrict__ gcol)
+{
+    using S = Shape<DIM, N>;
+    constexpr int Np = S::Np, NDOF = S::NDOF, NV = S::NV, NFN = S::NFN, L = S::L, EPW = S::EPW, ST = S::NS_;
+    extern __shared__ double smem[];
+    double *c = smem;
+    load_consts(P.K, c, Np);
+    __syncthreads();
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int grp = lane / L, gl = lane % L;
+    const int wpb = blockDim.x >> 5;
+    double *wv = smem + CONST_SLOTS + (size_t)(warp * EPW + grp) * S::EL_LIFT;
+    double *g = wv + NV * ST;
+    const int64_t nn = P.nnodes;
+    const int64_t wstride = (int64_t)gridDim.x * wpb;
+    const double invJ = C_INVJ(c), fsc = C_FACE(c);
+    const double *Dh = C_DHAT(c), *Dm = C_D(c);
+    for (int64_t wt = (int64_t)blockIdx.x * wpb + warp; wt < P.nwt; wt += wstride) {
+        const int64_t e0 = wt * EPW + grp;
+        const bool valid = e0 < P.ne;
+        const int64_t e = valid ? e0 : 0;
+        // (i) entropy variables and their strong-form gradients
+#pragma unroll
+        for (int k = 0; k < S::NPL; k++) {
+            const int n = gl + k * L;
+            if (n < NDOF) {
+                double s[NV], w[NV];
+#pragma unroll
+                for (int v = 0; v < NV; v++)
+                    s[v] = valid ? __ldg(P.u + v * nn + e * NDOF + n) : (v == 0 ? 1.0 : (v == NV - 1 ? P.gm1inv : 0.0));
+                entropy_vars<DIM>(s, P.gamma, P.gm1, P.gm1inv, w);
+#pragma unroll
+                for (int v = 0; v < NV; v++) wv[v * ST + sp<Np>(n)] = w[v];
+            }
+        }
+        __syncwarp();
+        grad_lines<DIM, N, 0>(wv, g, c, gl);
+        grad_lines<DIM, N, 1>(wv, g, c, gl);
+        if (DIM == 3) grad_lines<DIM, N, (DIM == 3 ? 2 : 0)>(wv, g, c, gl);
+        __syncwarp();
+        // (ii) the cotangent replaces the entropy variables in the slot
+#pragma unroll
+        for (int k = 0; k < S::NPL; k++) {
+            const int n = gl + k * L;
+            if (n < NDOF) {
+#pragma unroll
+                for (int v = 0; v < NV; v++) wv[v * ST + sp<Np>(n)] = valid ? __ldg(cot + v * nn + e * NDOF + n) : 0.0;
+            }
+        }
+        __syncwarp();
+        // (iii) per node: viscous fluxes and gradient conversion in reverse
+        double sacc[S::NPL][NV];
+#pragma unroll
+        for (int k = 0; k < S::NPL; k++)
+#pragma unroll
+            for (int v = 0; v < NV; v++) sacc[k][v] = 0.0;
+#pragma unroll 1
+        for (int k = 0; k < S::NPL; k++) {
+            const int n = gl + k * L;
+            if (n >= NDOF) break;
+            const int m = sp<Np>(n);
+            double s[NV];
+#pragma unroll
+            for (int v = 0; v < NV; v++) s[v] = valid ? __ldg(P.u + v * nn + e * NDOF + n) : (v == 0 ? 1.0 : (v == NV - 1 ? P.gm1inv : 0.0));
+            const int idx[3] = {n % Np, (n / Np) % Np, n / (Np * Np)};
+            double gin[DIM][NV], dq[DIM][NV];
+#pragma unroll
+            for (int d = 0; d < DIM; d++) {
+#pragma unroll
+                for (int v = 0; v < NV; v++) gin[d][v] = g[(d * NV + v) * ST + m];
+                const int pos = idx[d];
+                if (valid && (pos == 0 || pos == N)) {
+                    const int line = line_of<DIM, Np>(d, idx);
+                    const int64_t owner = pos == N ? e : (int64_t)__ldg(P.nbr + e * 2 * DIM + 2 * d);
+                    const double *F = P.lbuf + ((d * P.ne + owner) * NFN + line) * NV;
+#pragma unroll
+                    for (int v = 0; v < NV; v++) gin[d][v] += __ldg(F + v);
+                }
+#pragma unroll
+                for (int v = 0; v < NV; v++) dq[d][v] = gin[d][v];
+                entgrad_to_primgrad<DIM>(s, P.gm1, P.gm1inv, false, dq[d]);
+            }
+            // cotangent of each viscous column: volume divergence (Dhat
+            // transposed along the line through n) and the face terms
+            double cb[DIM][DIM + 1];
+#pragma unroll
+            for (int d = 0; d < DIM; d++) {
+                const int pos = idx[d];
+                const double a = C_ADJ(c)[d] * invJ;
+                const int line = line_of<DIM, Np>(d, idx);
+#pragma unroll
+                for (int i = 0; i <= DIM; i++) {
+                    double acc = 0.0;
+#pragma unroll
+                    for (int p = 0; p < Np; p++)
+                        acc += Dh[p * Np + pos] * wv[(1 + i) * ST + sp<Np>(line_node_rt<DIM, Np>(d, line, p))];
+                    cb[d][i] = a * acc;
+                }
+                if (valid && (pos == 0 || pos == N)) {
+                    // the face column enters out_a with + fsc A / 2 and out_b with - fsc A / 2
+                    const double h = 0.5 * fsc * C_AREA(c)[d];
+                    const int64_t other = __ldg(P.nbr + e * 2 * DIM + 2 * d + (pos == N ? 1 : 0));
+                    const int no = line_node_rt<DIM, Np>(d, line, pos == N ? 0 : N);
+#pragma unroll
+                    for (int i = 0; i <= DIM; i++) {
+                        const double lo = __ldg(cot + (int64_t)(1 + i) * nn + other * NDOF + no);
+                        const double le = wv[(1 + i) * ST + m];
+                        cb[d][i] += pos == N ? h * (le - lo) : h * (lo - le);
+                    }
+                }
+            }
+            const Prim<DIM> q = make_prim<DIM>(s, P.gamma, P.gm1);
+            PBar<DIM> qb;
+            pbar_zero(qb);
+            double dqb[DIM][NV];
+#pragma unroll
+            for (int d = 0; d < DIM; d++)
+#pragma unroll
+                for (int v = 0; v < NV; v++) dqb[d][v] = 0.0;
+#pragma unroll
+            for (int d = 0; d < DIM; d++) viscous_col_vjp<DIM>(q, dq, d, P.gm1inv, P.mu, P.lambda_k, cb[d], qb, dqb);
+            double sk[NV];
+#pragma unroll
+            for (int v = 0; v < NV; v++) sk[v] = 0.0;
+            pbar_to_cons<DIM>(s, qb, nullptr, P.gm1, sk);
+#pragma unroll
+            for (int d = 0; d < DIM; d++) {
+                double gb[NV];
+                entgrad_vjp<DIM>(s, gin[d], dqb[d], P.gm1, P.gm1inv, gb, sk);
+#pragma unroll
+                for (int v = 0; v < NV; v++) g[(d * NV + v) * ST + m] = gb[v];
+                const int pos = idx[d];
+                if (valid && (pos == 0 || pos == N)) {
+                    const int line = line_of<DIM, Np>(d, idx);
+                    double *dst = gcol + (((int64_t)(d * 2 + (pos == N ? 1 : 0)) * P.ne + e) * NFN + line) * NV;
+#pragma unroll
+                    for (int v = 0; v < NV; v++) dst[v] = gb[v];
+                }
+            }
+#pragma unroll
+            for (int kk = 0; kk < S::NPL; kk++)
+                if (kk == k)
+#pragma unroll
+                    for (int v = 0; v < NV; v++) sacc[kk][v] = sk[v];
+        }
+        __syncwarp();
+        // (iv) volume lifting in reverse: wbar_l = sum_d adj_d / J sum_p D(p, l) gbar_d(p)
+#pragma unroll
+        for (int k = 0; k < S::NPL; k++) {
+            const int n = gl + k * L;
+            if (n < NDOF) {
+                const int idx[3] = {n % Np, (n / Np) % Np, n / (Np * Np)};
+#pragma unroll
+                for (int v = 0; v < NV; v++) {
+                    double acc = 0.0;
+#pragma unroll
+                    for (int d = 0; d < DIM; d++) {
+                        const int pos = idx[d];
+                        const int line = line_of<DIM, Np>(d, idx);
+                        double t = 0.0;
+#pragma unroll
+                        for (int p = 0; p < Np; p++)
+                            t += Dm[p * Np + pos] * g[(d * NV + v) * ST + sp<Np>(line_node_rt<DIM, Np>(d, line, p))];
+                        acc += C_ADJ(c)[d] * invJ * t;
+                    }
+                    wv[v * ST + sp<Np>(n)] = acc;
+                }
+            }
+        }
+        __syncwarp();
+        // (v) entropy variables in reverse, and the node's total
+        if (valid) {
+#pragma unroll
+            for (int k = 0; k < S::NPL; k++) {
+                const int n = gl + k * L;
+                if (n < NDOF) {
+                    double s[NV], wb[NV];
+#pragma unroll
+                    for (int v = 0; v < NV; v++) {
+                        s[v] = __ldg(P.u + v * nn + e * NDOF + n);
+                        wb[v] = wv[v * ST + sp<Np>(n)];
+                    }
+                    entropy_vars_vjp<DIM>(s, wb, P.gamma, P.gm1, P.gm1inv, sacc[k]);
+#pragma unroll
+                    for (int v = 0; v < NV; v++) ubar[v * nn + e * NDOF + n] += sacc[k][v];
+                }
+            }
+        }
+        __syncwarp();
+    }
+}
+
+// Adjoint of one direction's face terms: element a's +D face node fn and
+// its neighbour b's -D face node (face_node_terms in reverse), plus for
+// Navier-Stokes the BR1 jump 0.5 fsc A (w_b - w_a) that lift_face_node adds to
+// both sides' face gradients.
+template <int DIM, int N, int D, bool NS>
+__global__ void __launch_bounds__(256) adj_face_kernel(const KParams P, const double *__restrict__ cot,
+                                                       double *__restrict__ ubar, const double *__restrict__ gcol)
+{
+    using S = Shape<DIM, N>;
+    constexpr int Np = S::Np, NDOF = S::NDOF, NV = S::NV, NFN = S::NFN;
+    __shared__ double c[CONST_SLOTS];
+    load_consts(P.K, c, Np);
+    __syncthreads();
+    const int64_t nn = P.nnodes;
+    for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < P.ne * NFN;
+         t += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t a = t / NFN;
+        const int fn = (int)(t - a * NFN);
+        const int64_t b = __ldg(P.nbr + a * 2 * DIM + 2 * D + 1);
+        const int na = line_node<DIM, Np, D>(fn, N), nb = line_node<DIM, Np, D>(fn, 0);
+        double sa[NV], sb[NV], la[NV], lb[NV];
+#pragma unroll
+        for (int v = 0; v < NV; v++) {
+            sa[v] = __ldg(P.u + v * nn + a * NDOF + na);
+            sb[v] = __ldg(P.u + v * nn + b * NDOF + nb);
+            la[v] = __ldg(cot + v * nn + a * NDOF + na);
+            lb[v] = __ldg(cot + v * nn + b * NDOF + nb);
+        }
+        const Prim<DIM> qa = make_prim<DIM>(sa, P.gamma, P.gm1), qb = make_prim<DIM>(sb, P.gamma, P.gm1);
+        const bool a_is_1 = a <= b;
+        const double nrm = a_is_1 ? C_AREA(c)[D] : -C_AREA(c)[D];
+        const double sc = C_FACE(c);
+        // out_a += C, out_b -= C with C = sc (a_is_1 ? -F : F) (+ the viscous part)
+        double Fb[NV];
+#pragma unroll
+        for (int v = 0; v < NV; v++) Fb[v] = (a_is_1 ? -sc : sc) * (la[v] - lb[v]);
+        PBar<DIM> ab, bb;
+        pbar_zero(ab);
+        pbar_zero(bb);
+        double mab[DIM], mbb[DIM];
+#pragma unroll
+        for (int d = 0; d < DIM; d++) mab[d] = mbb[d] = 0.0;
+        if (a_is_1) face_flux_vjp<DIM>(qa, qb, sa + 1, sb + 1, D, nrm, P.gamma, P.gm1inv, P.diss_scale, Fb, ab, bb, mab, mbb);
+        else face_flux_vjp<DIM>(qb, qa, sb + 1, sa + 1, D, nrm, P.gamma, P.gm1inv, P.diss_scale, Fb, bb, ab, mbb, mab);
+        double ga[NV], gb[NV];
+#pragma unroll
+        for (int v = 0; v < NV; v++) ga[v] = gb[v] = 0.0;
+        pbar_to_cons<DIM>(sa, ab, mab, P.gm1, ga);
+        pbar_to_cons<DIM>(sb, bb, mbb, P.gm1, gb);
+        if (NS) {
+            const double h = 0.5 * C_FACE(c) * C_AREA(c)[D];
+            double wb[NV], wa[NV];
+#pragma unroll
+            for (int v = 0; v < NV; v++) {
+                const double s = h * (__ldg(gcol + (((int64_t)(D * 2 + 1) * P.ne + a) * NFN + fn) * NV + v) +
+                                      __ldg(gcol + (((int64_t)(D * 2 + 0) * P.ne + b) * NFN + fn) * NV + v));
+                wb[v] = s;
+                wa[v] = -s;
+            }
+            entropy_vars_vjp<DIM>(sa, wa, P.gamma, P.gm1, P.gm1inv, ga);
+            entropy_vars_vjp<DIM>(sb, wb, P.gamma, P.gm1, P.gm1inv, gb);
+        }
+#pragma unroll
+        for (int v = 0; v < NV; v++) {
+            ubar[v * nn + a * NDOF + na] += ga[v];
+            ubar[v * nn + b * NDOF + nb] += gb[v];
+        }
+    }
+}
+
+}  // namespace pdg

@@ -46,6 +46,8 @@ struct pdg_ctx {
     unsigned int *err = nullptr;
     double *ent_own = nullptr;                // filter: per-element entropy minimum at the stage input
     unsigned long long *filter_count = nullptr;
+    double *gcol = nullptr;   // adjoint: cotangents of the face-normal entropy gradients
+    bool adj_ready = false;
     // launch configuration per kernel kind
     KernelInfo kinfo[KIND_COUNT];
     int wpb[KIND_COUNT];
@@ -286,6 +288,7 @@ int kernel_config(int dim, int N, int kind, int64_t ne, int device, LaunchCfg *c
 bool kind_used(int kind, int dim, bool parabolic, bool filter)
 {
     if (kind == KIND_FILTER_BOUNDS || kind == KIND_FILTER) return filter;
+    if (kind >= KIND_ADJ_RHS) return false;  // configured by the first pdg_rhs_vjp
     const bool ns_kind = kind == KIND_NS || kind == KIND_LIFT || kind == KIND_LIFT_FACE ||
                          (kind >= KIND_FACE_NS0 && kind <= KIND_FACE_NS2);
     if (ns_kind != parabolic) return false;
@@ -372,8 +375,32 @@ cudaEvent_t pooled_event(pdg_ctx *c)
 int launch(pdg_ctx *c, int kind, KParams P, cudaStream_t s)
 {
     const KernelInfo &ki = c->kinfo[kind];
+    if (!ki.fn || ki.epw < 1) return fail(c, PDG_ERR_UNSUPPORTED, "kernel %d is not configured", kind);
     P.nwt = (c->ne + ki.epw - 1) / ki.epw;
     void *args[] = {&P};
+    cudaEvent_t ea = nullptr, eb = nullptr;
+    if (c->profile) {
+        ea = pooled_event(c);
+        eb = pooled_event(c);
+        if (!ea || !eb) return fail(c, PDG_ERR_CUDA, "event creation failed");
+        CK(cudaEventRecord(ea, s), "event record");
+    }
+    CK(cudaLaunchKernel(ki.fn, dim3(c->grid[kind]), dim3(32 * c->wpb[kind]), args, c->smem[kind], s), "kernel launch");
+    if (c->profile) {
+        CK(cudaEventRecord(eb, s), "event record");
+        c->timed.push_back({kind, ea, eb});
+    }
+    c->launches++;
+    return PDG_OK;
+}
+
+// Launch of a kernel whose arguments follow the KParams (adjoint kernels).
+int launch_with(pdg_ctx *c, int kind, KParams P, void *a1, void *a2, void *a3, cudaStream_t s)
+{
+    const KernelInfo &ki = c->kinfo[kind];
+    if (!ki.fn || ki.epw < 1) return fail(c, PDG_ERR_UNSUPPORTED, "kernel %d is not configured", kind);
+    P.nwt = (c->ne + ki.epw - 1) / ki.epw;
+    void *args[] = {&P, a1, a2, a3};
     cudaEvent_t ea = nullptr, eb = nullptr;
     if (c->profile) {
         ea = pooled_event(c);
@@ -538,6 +565,7 @@ int pdg_destroy(pdg_ctx *c)
     cudaFree(c->lam_bits);
     cudaFree(c->err);
     cudaFree(c->ent_own);
+    cudaFree(c->gcol);
     cudaFree(c->filter_count);
     for (auto &t : c->timed) {
         cudaEventDestroy(t.a);
@@ -703,6 +731,47 @@ int pdg_check(pdg_ctx *c, uint32_t *flags)
 const char *pdg_last_error(const pdg_ctx *c) { return c ? c->last_error.c_str() : "null context"; }
 
 int64_t pdg_launch_count(const pdg_ctx *c) { return c ? c->launches : -1; }
+
+int pdg_rhs_vjp(pdg_ctx *c, const double *u, const double *cot, double *ubar, void *stream)
+{
+    if (!c) return PDG_ERR_ARG;
+    if (!u || !cot || !ubar || ubar == u || ubar == cot) return fail(c, PDG_ERR_ARG, "pdg_rhs_vjp: null or aliased buffers");
+    if (c->p.compat) return fail(c, PDG_ERR_UNSUPPORTED, "pdg_rhs_vjp: the adjoint is of the fixed operator (compat = 0)");
+    cudaStream_t s = (cudaStream_t)stream;
+    int r;
+    if (!c->adj_ready) {
+        const int kinds[] = {KIND_ADJ_RHS, KIND_ADJ_LIFT, KIND_ADJ_FACE_E0, KIND_ADJ_FACE_E1, KIND_ADJ_FACE_E2,
+                             KIND_ADJ_FACE_NS0, KIND_ADJ_FACE_NS1, KIND_ADJ_FACE_NS2};
+        for (int kind : kinds) {
+            const bool ns_kind = kind == KIND_ADJ_LIFT || kind >= KIND_ADJ_FACE_NS0;
+            const bool euler_kind = kind >= KIND_ADJ_FACE_E0 && kind <= KIND_ADJ_FACE_E2;
+            if ((ns_kind && !c->p.parabolic) || (euler_kind && c->p.parabolic)) continue;
+            if ((kind == KIND_ADJ_FACE_E2 || kind == KIND_ADJ_FACE_NS2) && c->dim < 3) continue;
+            if ((r = configure_launch(c, kind))) return r;
+        }
+        if (c->p.parabolic) {
+            const size_t nfn = c->dim == 2 ? c->Np : c->Np * c->Np;
+            if (cudaMalloc(&c->gcol, sizeof(double) * 2 * c->dim * c->ne * nfn * c->nv) != cudaSuccess)
+                return fail(c, PDG_ERR_NOMEM, "pdg_rhs_vjp: scratch allocation failed");
+        }
+        c->adj_ready = true;
+    }
+    KParams P = base_params(c);
+    P.u = u;
+    c->last_stream = s;
+    void *a_cot = (void *)&cot, *a_bar = (void *)&ubar, *a_g = (void *)&c->gcol;
+    if (c->p.parabolic && (r = launch(c, KIND_LIFT_FACE, P, s))) return r;
+    if ((r = launch_with(c, KIND_ADJ_RHS, P, a_cot, a_bar, nullptr, s))) return r;
+    if (c->p.parabolic) {
+        if ((r = launch_with(c, KIND_ADJ_LIFT, P, a_cot, a_bar, a_g, s))) return r;
+        for (int d = 0; d < c->dim; d++)
+            if ((r = launch_with(c, KIND_ADJ_FACE_NS0 + d, P, a_cot, a_bar, a_g, s))) return r;
+    } else {
+        for (int d = 0; d < c->dim; d++)
+            if ((r = launch_with(c, KIND_ADJ_FACE_E0 + d, P, a_cot, a_bar, a_g, s))) return r;
+    }
+    return PDG_OK;
+}
 
 int pdg_filter_count(pdg_ctx *c, int64_t *filtered)
 {

@@ -16,7 +16,15 @@ enum KernelKind {
     KIND_FACE_NS2 = 9,
     KIND_FILTER_BOUNDS = 10,  // filter_bounds_kernel<dim, N>: per-element entropy minimum
     KIND_FILTER = 11,         // filter_kernel<dim, N>: entropy/positivity filter of the stage output
-    KIND_COUNT = 12
+    KIND_ADJ_RHS = 12,        // adj_rhs_kernel<dim, N>: adjoint of the inviscid volume terms and blending
+    KIND_ADJ_LIFT = 13,       // adj_lift_kernel<dim, N>: adjoint of the viscous terms
+    KIND_ADJ_FACE_E0 = 14,    // adj_face_kernel<dim, N, d, false>, d = 0, 1, 2
+    KIND_ADJ_FACE_E1 = 15,
+    KIND_ADJ_FACE_E2 = 16,
+    KIND_ADJ_FACE_NS0 = 17,   // adj_face_kernel<dim, N, d, true>
+    KIND_ADJ_FACE_NS1 = 18,
+    KIND_ADJ_FACE_NS2 = 19,
+    KIND_COUNT = 20
 };
 
 struct KernelInfo {
@@ -26,6 +34,8 @@ struct KernelInfo {
 };
 
 bool kernel_info_2d(int N, int kind, KernelInfo *out);
+bool adj_kernel_info_2d(int N, int kind, KernelInfo *out);
+bool adj_kernel_info_3d(int N, int kind, KernelInfo *out);
 bool kernel_info_3d(int N, int kind, KernelInfo *out);
 
 }  // namespace pdg

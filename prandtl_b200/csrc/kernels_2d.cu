@@ -28,7 +28,7 @@ template <int N> static bool info_n(int kind, KernelInfo *out)
         out->el_doubles = FilterShape<2, N>::EL;
         out->epw = 1;
         break;
-    default: return false;
+    default: return adj_kernel_info_2d(N, kind, out);
     }
     return true;
 }
