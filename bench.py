@@ -49,6 +49,7 @@ def parse():
     ap.add_argument("--e2e-steps", type=int, default=5)
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-adjoint", action="store_true", help="skip the adjoint cost measurement")
     ap.add_argument("--sweep-steps", type=int, default=100,
                     help="SSP-RK3 steps of the 256-case vortex sweep (0 skips it)")
     return ap.parse_args()
@@ -255,6 +256,8 @@ def run_ours(args):
            "roofline": roofline, "clocks": clocks}
     if args.sweep_steps > 0:
         out["sweep"] = run_sweep(args, dev)
+    if not args.no_adjoint:
+        out["adjoint"] = run_adjoint(args, dev)
     if rank == 0 and world == 1 and not args.no_cpu:
         out["cpu_baseline"] = cpu_baseline(mesh, u0, params, args.cpu_seconds)
     if rank == 0:
@@ -324,6 +327,72 @@ def run_sweep(args, dev):
     res["autotuner"] = dict(cfg, best_rhs_launch_ms=tuned_ms)
     res["unit"] = UNIT
     return res
+
+
+def run_adjoint(args, dev):
+    """Adjoint cost on Taylor-Green 16^3, N=3 (fixed operator): one VJP of
+    the right-hand side against one forward right-hand side, and the gradient
+    of the kinetic energy after 20 SSP-RK3 steps checkpointed every 5."""
+    import torch
+
+    import prandtl_b200 as pb
+    from prandtl_b200 import adjoint
+    mesh = cases.tgv_mesh(16, 3)
+    u0 = cases.taylor_green(mesh)
+    op = pb.DGSEMOperator(mesh, parabolic=1, blending=1, compat=0, mu=1.0 / 1600.0, Pr=0.71, gamma=1.4)
+    u = torch.from_numpy(u0).to(dev)
+    cot = torch.from_numpy(np.random.default_rng(1).standard_normal(u0.size)).to(dev)
+    out, bar = torch.empty_like(u), torch.empty_like(u)
+    reps = 50
+
+    def timed(fn, n):
+        for _ in range(3):
+            fn()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(n):
+            fn()
+        e1.record()
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / n
+
+    fwd = timed(lambda: op.Mult(u, out), reps)
+    vjp = timed(lambda: op.vjp(u, cot, out=bar), reps)
+    op.profile(True)
+    for k in (pb.KERNEL_ADJ_RHS, pb.KERNEL_ADJ_LIFT, pb.KERNEL_LIFT_FACE) + pb.KERNEL_ADJ_FACE_NS:
+        op.profile_read(k)
+    for _ in range(10):
+        op.vjp(u, cot, out=bar)
+    kernels = {}
+    for name, kinds in (("lift_face_kernel", (pb.KERNEL_LIFT_FACE,)), ("adj_rhs_kernel", (pb.KERNEL_ADJ_RHS,)),
+                        ("adj_lift_kernel", (pb.KERNEL_ADJ_LIFT,)), ("adj_face_kernel", pb.KERNEL_ADJ_FACE_NS)):
+        t = sum(op.profile_read(k)[0] for k in kinds)
+        kernels[name] = {"ms_per_vjp": t / 10}
+    op.profile(False)
+    tmp = torch.empty_like(u)
+    op.Mult(u, tmp)
+    dt = op.cfl_dt(0.5)
+
+    def ke_grad():
+        x0 = u.clone().requires_grad_(True)
+        ke = adjoint.kinetic_energy(mesh, adjoint.rk3(op, x0, dt, 20, 5))
+        return torch.autograd.grad(ke, x0)[0]
+
+    xs = u.clone()
+
+    def forward20():
+        xs.copy_(u)
+        for _ in range(20):
+            op.rk3_step(xs, dt)
+    fwd20 = timed(forward20, 1)
+    grad20 = timed(ke_grad, 1)
+    op.check()
+    return {"workload": "taylor_green_3d_16^3_N3_navier_stokes_br1_blending_fixed_operator",
+            "vdofs": mesh.size, "rhs_ms": fwd, "vjp_ms": vjp, "adjoint_over_forward": vjp / fwd,
+            "vjp_kernels": kernels,
+            "ke_gradient_20_steps": {"forward_20_steps_ms": fwd20, "gradient_ms": grad20,
+                                     "checkpoint_every": 5, "ratio": grad20 / fwd20}}
 
 
 def _ref_worker(payload):
