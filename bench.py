@@ -50,6 +50,8 @@ def parse():
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-adjoint", action="store_true", help="skip the adjoint cost measurement")
+    ap.add_argument("--slab", action="store_true",
+                    help="run the slab-decomposition driver also on one GPU (no exchange partner)")
     ap.add_argument("--sweep-steps", type=int, default=100,
                     help="SSP-RK3 steps of the 256-case vortex sweep (0 skips it)")
     return ap.parse_args()
@@ -63,6 +65,14 @@ def workload(n, order):
 
 
 def config_dict(mesh, n_gpus):
+    if n_gpus > 1:
+        return {"workload": f"taylor_green_3d_{mesh.n[0]}x{mesh.n[1]}x{mesh.n[0] * n_gpus}_N{mesh.order}"
+                            f"_navier_stokes_br1_blending_ssprk3",
+                "elements_per_gpu": mesh.n[0] ** 3, "order": mesh.order, "nodes_per_element": mesh.ndof,
+                "vdofs": mesh.n[0] ** 3 * mesh.ndof * mesh.nv * n_gpus, "stages_per_step": 3, "compat": 1,
+                "l2": "working set per GPU ~0.5 GB > 126 MB L2 (no flush needed)",
+                "parallelism": f"slab decomposition x{n_gpus} along z, one ghost element layer per side "
+                               f"exchanged before every stage (NCCL point-to-point)"}
     return {"workload": f"taylor_green_3d_{mesh.n[0]}^3_N{mesh.order}_navier_stokes_br1_blending_ssprk3",
             "elements": mesh.num_elements, "order": mesh.order, "nodes_per_element": mesh.ndof,
             "vdofs": mesh.size, "stages_per_step": 3, "compat": 1,
@@ -160,14 +170,39 @@ def run_ours(args):
         dist.init_process_group("nccl", timeout=timedelta(seconds=120))
     dev = torch.device("cuda", local if world > 1 else 0)
     torch.cuda.set_device(dev)
-    mesh, u0, params = workload(args.n, args.order)
-    op = pb.DGSEMOperator(mesh, **params)
+    slab = world > 1 or args.slab
+    if slab:
+        # weak scaling: each rank owns an n^3 slab of an n x n x (n world)
+        # periodic box (length 2 pi per n elements), one ghost layer per side
+        from prandtl_b200.distributed import DistributedRK3, SlabDecomposition
+        _, _, params = workload(2, args.order)
+        dec = SlabDecomposition(3, args.order, (args.n, args.n, args.n * world), 0.0,
+                                (2 * np.pi, 2 * np.pi, 2 * np.pi * world), world, rank)
+        mesh = dec.mesh
+        u0 = cases.taylor_green(dec)
+        op = pb.DGSEMOperator(mesh, **params)
+        drv = DistributedRK3(dec, op)
+        V = dec.glob.size // world  # owned vdofs per rank
+    else:
+        mesh, u0, params = workload(args.n, args.order)
+        op = pb.DGSEMOperator(mesh, **params)
+        V = mesh.size
     x = torch.from_numpy(u0).to(dev)
     tmp = torch.empty_like(x)
     op.Mult(x, tmp)
-    dt = op.cfl_dt(0.5)
+    if slab:
+        lam = drv.max_char_speed(op.GetMaxCharSpeed(), device=dev)
+        dt = 0.5 * min(mesh.h) / (lam * (args.order + 1) ** 2)
+
+        def step(y):
+            drv.step(y, dt)
+    else:
+        dt = op.cfl_dt(0.5)
+
+        def step(y):
+            op.rk3_step(y, dt)
     for _ in range(args.warmup):
-        op.rk3_step(x, dt)
+        step(x)
     torch.cuda.synchronize()
     op.check()
 
@@ -187,7 +222,7 @@ def run_ours(args):
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     ev0.record()
     for _ in range(args.steps):
-        op.rk3_step(x, dt)
+        step(x)
     ev1.record()
     torch.cuda.synchronize()
     barrier()
@@ -207,24 +242,38 @@ def run_ours(args):
         t = torch.tensor([ms], device=dev, dtype=torch.float64)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         ms = float(t.item())
-    V = mesh.size
     value = V * 3 * args.steps * world / (ms * 1e-3)
 
     # end to end through the host-buffer step: H2D + 3 stages + D2H per step
-    host = torch.from_numpy(x.cpu().numpy()).pin_memory().numpy()
-    op.rk3_step_host(host, dt)
+    if slab:
+        hbuf = x.cpu().pin_memory()
+
+        def e2e_step():
+            x.copy_(hbuf, non_blocking=True)
+            drv.step(x, dt)
+            hbuf.copy_(x, non_blocking=True)
+            torch.cuda.synchronize()
+        io_bytes = 8 * x.numel()
+        e2e_path = "pinned host slab in, ghost exchange + 3 fused stages, slab out (DistributedRK3)"
+    else:
+        host = torch.from_numpy(x.cpu().numpy()).pin_memory().numpy()
+
+        def e2e_step():
+            op.rk3_step_host(host, dt)
+        io_bytes = 8 * V
+        e2e_path = "pdg_rk3_step_host (pinned host state in, 3 fused stages, state out)"
+    e2e_step()
     barrier()
     t0 = time.perf_counter()
     for _ in range(args.e2e_steps):
-        op.rk3_step_host(host, dt)
+        e2e_step()
     e2e_s = time.perf_counter() - t0
     if world > 1:
         t = torch.tensor([e2e_s], device=dev, dtype=torch.float64)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         e2e_s = float(t.item())
     e2e = {"value": V * 3 * args.e2e_steps * world / e2e_s, "unit": UNIT,
-           "h2d_bytes_per_step": 8 * V, "d2h_bytes_per_step": 8 * V,
-           "path": "pdg_rk3_step_host (pinned host state in, 3 fused stages, state out)"}
+           "h2d_bytes_per_step": io_bytes, "d2h_bytes_per_step": io_bytes, "path": e2e_path}
 
     peak, peak_kind = measured_peaks()
     stages = 3 * args.steps
@@ -254,9 +303,9 @@ def run_ours(args):
            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
            "config": config_dict(mesh, world), "e2e": e2e, "gpu_launches": launches,
            "roofline": roofline, "clocks": clocks}
-    if args.sweep_steps > 0:
+    if args.sweep_steps > 0 and world == 1:
         out["sweep"] = run_sweep(args, dev)
-    if not args.no_adjoint:
+    if not args.no_adjoint and world == 1:
         out["adjoint"] = run_adjoint(args, dev)
     if rank == 0 and world == 1 and not args.no_cpu:
         out["cpu_baseline"] = cpu_baseline(mesh, u0, params, args.cpu_seconds)

@@ -64,6 +64,7 @@ class CartesianMesh:
     lo: tuple[float, ...]
     hi: tuple[float, ...]
     nbr: np.ndarray             # (ne, 2*dim) int32
+    spacing: tuple[float, ...] | None = None  # element extents, when not (hi - lo) / n exactly
 
     @property
     def Np(self) -> int:
@@ -91,14 +92,17 @@ class CartesianMesh:
 
     @property
     def h(self) -> tuple[float, ...]:
+        if self.spacing is not None:
+            return tuple(self.spacing)
         return tuple((self.hi[d] - self.lo[d]) / self.n[d] for d in range(self.dim))
 
-    def node_coords(self) -> np.ndarray:
-        """Physical coordinates, shape (dim, num_nodes), in the byNODES order."""
+    def node_coords(self, elements=None) -> np.ndarray:
+        """Physical coordinates, shape (dim, num_nodes), in the byNODES order
+        (of the listed elements only, when `elements` is given)."""
         x1, _ = gll_nodes(self.Np)
         Np, dim = self.Np, self.dim
-        ne = self.num_elements
-        e = np.arange(ne)
+        e = np.arange(self.num_elements) if elements is None else np.asarray(elements, dtype=np.int64)
+        ne = e.size
         eidx = []
         r = e.copy()
         for d in range(dim):
