@@ -250,12 +250,13 @@ int pdg_batch_rhs(pdg_batch *batch, const double *u, double *dudt, void *stream)
  * Simulation.cpp:1010), three launches per step; with use_graph the step is
  * captured once in a CUDA graph and replayed. */
 int pdg_batch_rk3_step(pdg_batch *batch, double *u, int nsteps, int use_graph, void *stream);
-/* Autotuner: times the batch kernel on u for each warps-per-block x
- * tiles-per-fetch x tile-order candidate and keeps the fastest (synchronises).
+/* Autotuner: times the batch kernel on u for each register budget (255, 170
+ * or 128 registers per thread: variant 0, 1, 2) x warps per block x tiles per
+ * fetch x tile order candidate and keeps the fastest (synchronises).
  * best_ms (may be null) receives the fastest launch time. */
 int pdg_batch_tune(pdg_batch *batch, const double *u, void *stream, float *best_ms);
 int pdg_batch_config(const pdg_batch *batch, int *warps_per_block, int *blocks, int *tiles_per_fetch,
-                     int *tile_order);
+                     int *tile_order, int *register_variant);
 /* Per-case running maximum wave speed (host array of ncases; synchronises). */
 int pdg_batch_max_char_speed(pdg_batch *batch, double *lam);
 int pdg_batch_check(pdg_batch *batch, uint32_t *flags);

@@ -106,7 +106,7 @@ def library():
     L.pdg_batch_rhs.argtypes = [vp, vp, vp, vp]
     L.pdg_batch_rk3_step.argtypes = [vp, vp, C.c_int, C.c_int, vp]
     L.pdg_batch_tune.argtypes = [vp, vp, vp, C.POINTER(C.c_float)]
-    L.pdg_batch_config.argtypes = [vp] + [C.POINTER(C.c_int)] * 4
+    L.pdg_batch_config.argtypes = [vp] + [C.POINTER(C.c_int)] * 5
     L.pdg_batch_max_char_speed.argtypes = [vp, _dp]
     L.pdg_batch_check.argtypes = [vp, C.POINTER(C.c_uint32)]
     L.pdg_batch_launch_count.restype = C.c_int64
@@ -366,9 +366,10 @@ class DGSEMBatch:
         return ms.value
 
     def config(self) -> dict:
-        v = [C.c_int() for _ in range(4)]
+        v = [C.c_int() for _ in range(5)]
         self._call(library().pdg_batch_config(self._b, *[C.byref(x) for x in v]), "pdg_batch_config")
-        return dict(zip(("warps_per_block", "blocks", "tiles_per_fetch", "tile_order"), (x.value for x in v)))
+        return dict(zip(("warps_per_block", "blocks", "tiles_per_fetch", "tile_order", "register_variant"),
+                        (x.value for x in v)))
 
     def max_char_speed(self) -> np.ndarray:
         lam = np.empty(len(self.meshes))

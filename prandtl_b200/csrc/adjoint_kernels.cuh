@@ -45,13 +45,13 @@ __device__ __forceinline__ void modal_pass_t(const double *src, double *dst, int
         if (line < S::NFN) {
             double x[Np];
 #pragma unroll
-            for (int k = 0; k < Np; k++) x[k] = src[sp<Np>(line_node<DIM, Np, D>(line, k))];
+            for (int k = 0; k < Np; k++) x[k] = src[sp<DIM, Np>(line_node<DIM, Np, D>(line, k))];
 #pragma unroll
             for (int l = 0; l < Np; l++) {
                 double s = 0.0;
 #pragma unroll
                 for (int k = 0; k < Np; k++) s += Vinv[k * Np + l] * x[k];
-                dst[sp<Np>(line_node<DIM, Np, D>(line, l))] = s;
+                dst[sp<DIM, Np>(line_node<DIM, Np, D>(line, l))] = s;
             }
         }
     }
@@ -78,15 +78,15 @@ __device__ __forceinline__ void ec_lines_vjp(const KParams &P, int d, const doub
             PBar<DIM> qb[Np];
 #pragma unroll
             for (int l = 0; l < Np; l++) {
-                q[l] = slot_prim<DIM>(pr, sp<Np>(line_node_rt<DIM, Np>(d, line, l)), ST);
+                q[l] = slot_prim<DIM>(pr, sp<DIM, Np>(line_node_rt<DIM, Np>(d, line, l)), ST);
                 pbar_zero(qb[l]);
             }
 #pragma unroll
             for (int a = 0; a < Np; a++)
 #pragma unroll
                 for (int b = a + 1; b < Np; b++) {
-                    const int na = sp<Np>(line_node_rt<DIM, Np>(d, line, a));
-                    const int nb = sp<Np>(line_node_rt<DIM, Np>(d, line, b));
+                    const int na = sp<DIM, Np>(line_node_rt<DIM, Np>(d, line, a));
+                    const int nb = sp<DIM, Np>(line_node_rt<DIM, Np>(d, line, b));
                     const double cab = scale * D2[a * Np + b], cba = scale * D2[b * Np + a];
                     double Fb[NV];
 #pragma unroll
@@ -95,7 +95,7 @@ __device__ __forceinline__ void ec_lines_vjp(const KParams &P, int d, const doub
                 }
 #pragma unroll
             for (int l = 0; l < Np; l++) {
-                const int n = sp<Np>(line_node_rt<DIM, Np>(d, line, l));
+                const int n = sp<DIM, Np>(line_node_rt<DIM, Np>(d, line, l));
                 pb[P_RHO * ST + n] += qb[l].rho;
 #pragma unroll
                 for (int k = 0; k < DIM; k++) pb[(P_V + k) * ST + n] += qb[l].v[k];
@@ -123,7 +123,7 @@ __device__ __forceinline__ void fv_lines_vjp(const KParams &P, const double *pr,
         if (line < S::NFN) {
 #pragma unroll 1
             for (int l = 0; l < N; l++) {
-                const int na = sp<Np>(line_node<DIM, Np, D>(line, l)), nb = sp<Np>(line_node<DIM, Np, D>(line, l + 1));
+                const int na = sp<DIM, Np>(line_node<DIM, Np, D>(line, l)), nb = sp<DIM, Np>(line_node<DIM, Np, D>(line, l + 1));
                 Prim<DIM> qa = slot_prim<DIM>(pr, na, ST), qb = slot_prim<DIM>(pr, nb, ST);
                 complete_prim<DIM>(qa, P.gamma);
                 complete_prim<DIM>(qb, P.gamma);
@@ -177,7 +177,7 @@ __device__ __forceinline__ void indicator_vjp(const double *pr, double *pb, doub
     for (int k = 0; k < S::NPL; k++) {
         const int n = gl + k * L;
         if (n < NDOF) {
-            const int m = sp<Np>(n);
+            const int m = sp<DIM, Np>(n);
             const double rho = pr[P_RHO * ST + m], beta = pr[PS::BETA * ST + m];
             scr[m] = rho * (0.5 * rho / beta);
         }
@@ -196,7 +196,7 @@ __device__ __forceinline__ void indicator_vjp(const double *pr, double *pb, doub
             const int i = t % Np, j = (t / Np) % Np, kk = DIM == 3 ? t / (Np * Np) : 0;
             int mx = i > j ? i : j;
             if (DIM == 3) mx = mx > kk ? mx : kk;
-            const double v = mo[sp<Np>(t)] * mo[sp<Np>(t)];
+            const double v = mo[sp<DIM, Np>(t)] * mo[sp<DIM, Np>(t)];
             mm += v;
             if (mx <= N - 1) m1 += v;
             if (mx <= N - 2) m2 += v;
@@ -223,7 +223,7 @@ __device__ __forceinline__ void indicator_vjp(const double *pr, double *pb, doub
             int mx = i > j ? i : j;
             if (DIM == 3) mx = mx > kk ? mx : kk;
             const double w = mmb + (mx <= N - 1 ? m1b : 0.0) + (mx <= N - 2 ? m2b : 0.0);
-            mo[sp<Np>(t)] = 2.0 * mo[sp<Np>(t)] * w;
+            mo[sp<DIM, Np>(t)] = 2.0 * mo[sp<DIM, Np>(t)] * w;
         }
     }
     __syncwarp();
@@ -241,7 +241,7 @@ __device__ __forceinline__ void indicator_vjp(const double *pr, double *pb, doub
     for (int k = 0; k < S::NPL; k++) {
         const int n = gl + k * L;
         if (n < NDOF) {
-            const int m = sp<Np>(n);
+            const int m = sp<DIM, Np>(n);
             const double rho = pr[P_RHO * ST + m], beta = pr[PS::BETA * ST + m];
             const double p = 0.5 * rho / beta, g = qbar[m];
             const double pbar = g * rho;
@@ -269,7 +269,7 @@ __global__ void __launch_bounds__(128) adj_rhs_kernel(const KParams P, const dou
     const int grp = lane / L, gl = lane % L;
     const int wpb = blockDim.x >> 5;
     // EPW * L = 32: every lane belongs to an element slot
-    double *pr = smem + CONST_SLOTS + (size_t)(warp * EPW + grp) * AdjShape<DIM, N>::EL;
+    double *pr = smem + const_slots(Np) + (size_t)(warp * EPW + grp) * AdjShape<DIM, N>::EL;
     double *lm = pr + NV * ST, *pb = lm + NV * ST, *scr = pb + NV * ST;
     const int64_t nn = P.nnodes;
     const int64_t wstride = (int64_t)gridDim.x * wpb;
@@ -286,7 +286,7 @@ __global__ void __launch_bounds__(128) adj_rhs_kernel(const KParams P, const dou
                 for (int v = 0; v < NV; v++)
                     s[v] = valid ? __ldg(P.u + v * nn + e * NDOF + n) : (v == 0 ? 1.0 : (v == NV - 1 ? P.gm1inv : 0.0));
                 const Prim<DIM> q = make_prim<DIM>(s, P.gamma, P.gm1);
-                const int m = sp<Np>(n);
+                const int m = sp<DIM, Np>(n);
                 pr[P_RHO * ST + m] = q.rho;
 #pragma unroll
                 for (int d = 0; d < DIM; d++) pr[(P_V + d) * ST + m] = q.v[d];
@@ -321,7 +321,7 @@ __global__ void __launch_bounds__(128) adj_rhs_kernel(const KParams P, const dou
                 const int n = gl + k * L;
                 if (n < NDOF)
 #pragma unroll
-                    for (int v = 0; v < NV; v++) abar += lm[v * ST + sp<Np>(n)] * scr[v * ST + sp<Np>(n)];
+                    for (int v = 0; v < NV; v++) abar += lm[v * ST + sp<DIM, Np>(n)] * scr[v * ST + sp<DIM, Np>(n)];
             }
             abar = group_sum<L>(abar);
             __syncwarp();
@@ -340,7 +340,7 @@ __global__ void __launch_bounds__(128) adj_rhs_kernel(const KParams P, const dou
             for (int k = 0; k < S::NPL; k++) {
                 const int n = gl + k * L;
                 if (n < NDOF) {
-                    const int m = sp<Np>(n);
+                    const int m = sp<DIM, Np>(n);
                     double s[NV], sb[NV];
 #pragma unroll
                     for (int v = 0; v < NV; v++) {
@@ -380,7 +380,7 @@ __global__ void __launch_bounds__(128) adj_lift_kernel(const KParams P, const do
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int grp = lane / L, gl = lane % L;
     const int wpb = blockDim.x >> 5;
-    double *wv = smem + CONST_SLOTS + (size_t)(warp * EPW + grp) * S::EL_LIFT;
+    double *wv = smem + const_slots(Np) + (size_t)(warp * EPW + grp) * S::EL_LIFT;
     double *g = wv + NV * ST;
     const int64_t nn = P.nnodes;
     const int64_t wstride = (int64_t)gridDim.x * wpb;
@@ -401,7 +401,7 @@ __global__ void __launch_bounds__(128) adj_lift_kernel(const KParams P, const do
                     s[v] = valid ? __ldg(P.u + v * nn + e * NDOF + n) : (v == 0 ? 1.0 : (v == NV - 1 ? P.gm1inv : 0.0));
                 entropy_vars<DIM>(s, P.gamma, P.gm1, P.gm1inv, w);
 #pragma unroll
-                for (int v = 0; v < NV; v++) wv[v * ST + sp<Np>(n)] = w[v];
+                for (int v = 0; v < NV; v++) wv[v * ST + sp<DIM, Np>(n)] = w[v];
             }
         }
         __syncwarp();
@@ -415,7 +415,7 @@ __global__ void __launch_bounds__(128) adj_lift_kernel(const KParams P, const do
             const int n = gl + k * L;
             if (n < NDOF) {
 #pragma unroll
-                for (int v = 0; v < NV; v++) wv[v * ST + sp<Np>(n)] = valid ? __ldg(cot + v * nn + e * NDOF + n) : 0.0;
+                for (int v = 0; v < NV; v++) wv[v * ST + sp<DIM, Np>(n)] = valid ? __ldg(cot + v * nn + e * NDOF + n) : 0.0;
             }
         }
         __syncwarp();
@@ -429,7 +429,7 @@ __global__ void __launch_bounds__(128) adj_lift_kernel(const KParams P, const do
         for (int k = 0; k < S::NPL; k++) {
             const int n = gl + k * L;
             if (n >= NDOF) break;
-            const int m = sp<Np>(n);
+            const int m = sp<DIM, Np>(n);
             double s[NV];
 #pragma unroll
             for (int v = 0; v < NV; v++) s[v] = valid ? __ldg(P.u + v * nn + e * NDOF + n) : (v == 0 ? 1.0 : (v == NV - 1 ? P.gm1inv : 0.0));
@@ -464,7 +464,7 @@ __global__ void __launch_bounds__(128) adj_lift_kernel(const KParams P, const do
                     double acc = 0.0;
 #pragma unroll
                     for (int p = 0; p < Np; p++)
-                        acc += Dh[p * Np + pos] * wv[(1 + i) * ST + sp<Np>(line_node_rt<DIM, Np>(d, line, p))];
+                        acc += Dh[p * Np + pos] * wv[(1 + i) * ST + sp<DIM, Np>(line_node_rt<DIM, Np>(d, line, p))];
                     cb[d][i] = a * acc;
                 }
                 if (valid && (pos == 0 || pos == N)) {
@@ -531,10 +531,10 @@ __global__ void __launch_bounds__(128) adj_lift_kernel(const KParams P, const do
                         double t = 0.0;
 #pragma unroll
                         for (int p = 0; p < Np; p++)
-                            t += Dm[p * Np + pos] * g[(d * NV + v) * ST + sp<Np>(line_node_rt<DIM, Np>(d, line, p))];
+                            t += Dm[p * Np + pos] * g[(d * NV + v) * ST + sp<DIM, Np>(line_node_rt<DIM, Np>(d, line, p))];
                         acc += C_ADJ(c)[d] * invJ * t;
                     }
-                    wv[v * ST + sp<Np>(n)] = acc;
+                    wv[v * ST + sp<DIM, Np>(n)] = acc;
                 }
             }
         }
@@ -549,7 +549,7 @@ __global__ void __launch_bounds__(128) adj_lift_kernel(const KParams P, const do
 #pragma unroll
                     for (int v = 0; v < NV; v++) {
                         s[v] = __ldg(P.u + v * nn + e * NDOF + n);
-                        wb[v] = wv[v * ST + sp<Np>(n)];
+                        wb[v] = wv[v * ST + sp<DIM, Np>(n)];
                     }
                     entropy_vars_vjp<DIM>(s, wb, P.gamma, P.gm1, P.gm1inv, sacc[k]);
 #pragma unroll

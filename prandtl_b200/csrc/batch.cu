@@ -54,7 +54,11 @@ __device__ __forceinline__ void batch_tile(const KParams &P, const double *c, do
     rhs_tile<2, N, false, true>(P, c, pr, e_base, grp, gl, lane_used, flags, lam);
 }
 
-__global__ void __launch_bounds__(256) batch_stage_kernel(const BatchArgs A)
+// MINB = minimum resident blocks per SM the compiler must allow (register
+// budget): MINB = 1 with 256 threads gives up to 255 registers, MINB = 3 with
+// 128 threads 170, MINB = 4 with 128 threads 128.  The autotuner chooses.
+template <int MINB>
+__global__ void __launch_bounds__(MINB == 1 ? 256 : 128, MINB) batch_stage_kernel(const BatchArgs A)
 {
     extern __shared__ double smem[];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -94,6 +98,15 @@ __global__ void __launch_bounds__(256) batch_stage_kernel(const BatchArgs A)
     if (lane == 0 && flags) atomicOr(A.err, flags);
 }
 
+struct BatchVariant {
+    const void *fn;
+    int max_wpb;
+};
+static const BatchVariant BATCH_VARIANTS[] = {{(const void *)&batch_stage_kernel<1>, 8},
+                                              {(const void *)&batch_stage_kernel<3>, 4},
+                                              {(const void *)&batch_stage_kernel<4>, 4}};
+constexpr int BATCH_NVARIANTS = 3;
+
 }  // namespace pdg
 
 using namespace pdg;
@@ -121,7 +134,7 @@ struct pdg_batch {
     double *stage_a = nullptr, *stage_b = nullptr;
     const double *params_x = nullptr;
     bool params_dirty = true;
-    int wpb = 4, grid = 0, chunk = 2;
+    int wpb = 4, grid = 0, chunk = 2, variant = 0;
     size_t smem = 0;
     cudaStream_t cap = nullptr;
     cudaGraph_t graph = nullptr;
@@ -160,21 +173,22 @@ void drop_graph(pdg_batch *b)
     b->graph = nullptr;
 }
 
-int configure(pdg_batch *b, int wpb, int chunk)
+int configure(pdg_batch *b, int wpb, int chunk, int variant)
 {
+    const void *fn = BATCH_VARIANTS[variant].fn;
+    if (wpb > BATCH_VARIANTS[variant].max_wpb) return bfail(b, PDG_ERR_UNSUPPORTED, "block too large for the variant");
     const size_t smem = (size_t)wpb * BATCH_WARP_DOUBLES * sizeof(double);
     int max_smem = 0;
     BCK(cudaDeviceGetAttribute(&max_smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, b->device), "device attribute");
     if (smem > (size_t)max_smem) return bfail(b, PDG_ERR_UNSUPPORTED, "batch block does not fit in shared memory");
-    BCK(cudaFuncSetAttribute((const void *)batch_stage_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem),
-        "smem attribute");
+    BCK(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem), "smem attribute");
     int per_sm = 0;
-    BCK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, (const void *)batch_stage_kernel, 32 * wpb, smem),
-        "occupancy");
+    BCK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, 32 * wpb, smem), "occupancy");
     if (per_sm < 1) return bfail(b, PDG_ERR_UNSUPPORTED, "batch kernel cannot be resident");
-    if (wpb != b->wpb || chunk != b->chunk) drop_graph(b);
+    if (wpb != b->wpb || chunk != b->chunk || variant != b->variant) drop_graph(b);
     b->wpb = wpb;
     b->chunk = chunk;
+    b->variant = variant;
     b->smem = smem;
     b->grid = b->sms * per_sm;
     return PDG_OK;
@@ -249,7 +263,7 @@ int launch_stage(pdg_batch *b, int slot, cudaStream_t s)
     A.ntiles = b->ntiles;
     A.chunk = b->chunk;
     void *args[] = {&A};
-    BCK(cudaLaunchKernel((const void *)batch_stage_kernel, dim3(b->grid), dim3(32 * b->wpb), args, b->smem, s),
+    BCK(cudaLaunchKernel(BATCH_VARIANTS[b->variant].fn, dim3(b->grid), dim3(32 * b->wpb), args, b->smem, s),
         "batch kernel launch");
     b->launches++;
     return PDG_OK;
@@ -340,7 +354,7 @@ int pdg_batch_create(int ncases, const pdg_mesh *meshes, const pdg_params *param
         cudaMemset(b->eta, 0, sizeof(double) * b->total_ne) || cudaMemset(b->alpha, 0, sizeof(double) * b->total_ne))
         return cleanup(PDG_ERR_CUDA);
     if (cudaStreamCreateWithFlags(&b->cap, cudaStreamNonBlocking) != cudaSuccess) return cleanup(PDG_ERR_CUDA);
-    const int r = configure(b, 4, 2);
+    const int r = configure(b, 4, 2, 0);
     if (r) return cleanup(r);
     *out = b;
     return PDG_OK;
@@ -441,13 +455,14 @@ int pdg_batch_tune(pdg_batch *b, const double *u, void *stream, float *best_ms)
     }
     const int wpbs[] = {1, 2, 4, 8}, chunks[] = {1, 2, 4, 8};
     float best = 1e30f;
-    int bw = b->wpb, bc = b->chunk, bo = b->tile_order;
+    int bw = b->wpb, bc = b->chunk, bo = b->tile_order, bv = b->variant;
     int r = PDG_OK;
     for (int order = 0; order < 2 && r == PDG_OK; order++) {
         if ((r = upload_tiles(b, order, s))) break;
+        for (int variant = 0; variant < BATCH_NVARIANTS && r == PDG_OK; variant++)
         for (int wpb : wpbs) {
             for (int chunk : chunks) {
-                if (configure(b, wpb, chunk) != PDG_OK) continue;  // does not fit: skip the candidate
+                if (configure(b, wpb, chunk, variant) != PDG_OK) continue;  // does not fit: skip the candidate
                 if ((r = rhs_launch(b, u, b->stage_a, s))) break;  // warm-up
                 if (cudaEventRecord(e0, s) != cudaSuccess) { r = PDG_ERR_CUDA; break; }
                 for (int k = 0; k < 3 && r == PDG_OK; k++) r = rhs_launch(b, u, b->stage_a, s);
@@ -463,6 +478,7 @@ int pdg_batch_tune(pdg_batch *b, const double *u, void *stream, float *best_ms)
                     bw = wpb;
                     bc = chunk;
                     bo = order;
+                    bv = variant;
                 }
             }
             if (r) break;
@@ -472,7 +488,7 @@ int pdg_batch_tune(pdg_batch *b, const double *u, void *stream, float *best_ms)
     cudaEventDestroy(e1);
     if (r) return r;
     if ((r = upload_tiles(b, bo, s))) return r;
-    if ((r = configure(b, bw, bc))) return r;
+    if ((r = configure(b, bw, bc, bv))) return r;
     drop_graph(b);
     b->tuned_ms = best;
     if (best_ms) *best_ms = best;
@@ -480,9 +496,11 @@ int pdg_batch_tune(pdg_batch *b, const double *u, void *stream, float *best_ms)
     return PDG_OK;
 }
 
-int pdg_batch_config(const pdg_batch *b, int *warps_per_block, int *blocks, int *chunk, int *tile_order)
+int pdg_batch_config(const pdg_batch *b, int *warps_per_block, int *blocks, int *chunk, int *tile_order,
+                     int *register_variant)
 {
     if (!b) return PDG_ERR_ARG;
+    if (register_variant) *register_variant = b->variant;
     if (warps_per_block) *warps_per_block = b->wpb;
     if (blocks) *blocks = b->grid;
     if (chunk) *chunk = b->chunk;

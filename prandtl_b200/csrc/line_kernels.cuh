@@ -94,7 +94,9 @@ template <int DIM, int N> struct Shape {
     static constexpr int NPL = (NDOF + L - 1) / L;      // nodes per lane
     static constexpr int LPL = (NFN + L - 1) / L;       // lines per lane per direction
     static constexpr int NPRIM = DIM + 2;               // rho, v[DIM], beta
-    static constexpr int NS_ = NDOF + NDOF / Np;        // padded per-variable stride in shared memory
+    // per-variable stride in shared memory: swizzled (no padding) for 3D
+    // Np = 4, one padding slot per x line otherwise
+    static constexpr int NS_ = (DIM == 3 && Np == 4) ? NDOF : NDOF + NDOF / Np;
     // rhs element slot: primitives, accumulator (which also holds the modal
     // transform of the indicator before the first flux pass), and the compat
     // z-fill buffer
@@ -105,9 +107,19 @@ template <int DIM, int N> struct Shape {
     static constexpr int EL_LIFT = NV * NS_ + DIM * NV * NS_;
 };
 
-// Shared-memory position of node n: one padding slot per x line, so that
-// line tasks of every direction read (nearly) distinct banks.
-template <int Np> __device__ __forceinline__ constexpr int sp(int n) { return n + n / Np; }
+// Shared-memory position of node n, chosen so that the lanes of a line task
+// (one node of each line of a direction: a plane of the element) hit
+// distinct banks.  3D Np = 4, n = i + 4j + 16k: row k, column
+// 4((j + k) mod 4) + (i + k) mod 4 — a bijection on every x, y and z plane.
+// Otherwise one padding slot per x line.
+template <int DIM, int Np> __device__ __forceinline__ constexpr int sp(int n)
+{
+    if (DIM == 3 && Np == 4) {
+        const int i = n & 3, j = (n >> 2) & 3, k = n >> 4;
+        return (k << 4) + (((j + k) & 3) << 2) + ((i + k) & 3);
+    }
+    return n + n / Np;
+}
 
 // Prefetch a byte range into L2 (TMA bulk prefetch); the range is shrunk to
 // whole 16-byte blocks inside it.
@@ -159,41 +171,50 @@ template <int G> __device__ __forceinline__ double group_max(double x)
 }
 
 // ---- constants in shared memory ----
+// Packed for the element's Np (each matrix Np x Np): D, Dhat, Dhat2, Vinv,
+// w, subcell normals (Np + 1 per direction), 1/(J w), adj, area, J, 1/J,
+// face scale.  The macros need a constant `Np` in scope.
+__host__ __device__ constexpr int cs_snor(int Np) { return 4 * Np * Np + Np; }
+__host__ __device__ constexpr int cs_fvs(int Np) { return cs_snor(Np) + 3 * (Np + 1); }
+__host__ __device__ constexpr int cs_adj(int Np) { return cs_fvs(Np) + Np; }
+__host__ __device__ constexpr int const_slots(int Np) { return (cs_adj(Np) + 9 + 1) & ~1; }
 #define C_D(c) (c)
-#define C_DHAT(c) ((c) + 36)
-#define C_DHAT2(c) ((c) + 72)
-#define C_VINV(c) ((c) + 108)
-#define C_W(c) ((c) + 144)
-#define C_SNOR(c, d) ((c) + 150 + 7 * (d))
-#define C_FVS(c) ((c) + 171)
-#define C_ADJ(c) ((c) + 177)
-#define C_AREA(c) ((c) + 180)
-#define C_J(c) ((c)[183])
-#define C_INVJ(c) ((c)[184])
-#define C_FACE(c) ((c)[185])
-constexpr int CONST_SLOTS = 192;
+#define C_DHAT(c) ((c) + Np * Np)
+#define C_DHAT2(c) ((c) + 2 * Np * Np)
+#define C_VINV(c) ((c) + 3 * Np * Np)
+#define C_W(c) ((c) + 4 * Np * Np)
+#define C_SNOR(c, d) ((c) + cs_snor(Np) + (Np + 1) * (d))
+#define C_FVS(c) ((c) + cs_fvs(Np))
+#define C_ADJ(c) ((c) + cs_adj(Np))
+#define C_AREA(c) ((c) + cs_adj(Np) + 3)
+#define C_J(c) ((c)[cs_adj(Np) + 6])
+#define C_INVJ(c) ((c)[cs_adj(Np) + 7])
+#define C_FACE(c) ((c)[cs_adj(Np) + 8])
+constexpr int CONST_SLOTS = 192;  // the largest packing (Np = 6) fits
+static_assert(const_slots(6) <= CONST_SLOTS, "constant slots");
 
 __device__ __forceinline__ void load_consts(const DevConst *K, double *c, int Np, int tid, int nth)
 {
-    for (int t = tid; t < Np * Np; t += nth) {
+    const int n2 = Np * Np;
+    for (int t = tid; t < n2; t += nth) {
         c[t] = K->D[t];
-        c[36 + t] = K->Dhat[t];
-        c[72 + t] = K->Dhat2[t];
-        c[108 + t] = K->Vinv1[t];
+        c[n2 + t] = K->Dhat[t];
+        c[2 * n2 + t] = K->Dhat2[t];
+        c[3 * n2 + t] = K->Vinv1[t];
     }
     for (int t = tid; t < Np; t += nth) {
-        c[144 + t] = K->w[t];
-        c[171 + t] = K->fv_scale[t];
+        c[4 * n2 + t] = K->w[t];
+        c[cs_fvs(Np) + t] = K->fv_scale[t];
     }
-    for (int t = tid; t < 3 * 7; t += nth) c[150 + t] = (&K->snor[0][0])[t];
+    for (int t = tid; t < 3 * (Np + 1); t += nth) c[cs_snor(Np) + t] = K->snor[t / (Np + 1)][t % (Np + 1)];
     for (int t = tid; t < 3; t += nth) {
-        c[177 + t] = K->adj[t];
-        c[180 + t] = K->area[t];
+        c[cs_adj(Np) + t] = K->adj[t];
+        c[cs_adj(Np) + 3 + t] = K->area[t];
     }
     if (tid == 0) {
-        c[183] = K->J;
-        c[184] = K->invJ;
-        c[185] = K->face_scale;
+        c[cs_adj(Np) + 6] = K->J;
+        c[cs_adj(Np) + 7] = K->invJ;
+        c[cs_adj(Np) + 8] = K->face_scale;
     }
 }
 __device__ __forceinline__ void load_consts(const DevConst *K, double *c, int Np)
@@ -248,13 +269,13 @@ __device__ __forceinline__ void modal_pass(const double *src, double *dst, int g
         if (line < S::NFN) {
             double x[Np];
 #pragma unroll
-            for (int l = 0; l < Np; l++) x[l] = src[sp<Np>(line_node<DIM, Np, D>(line, l))];
+            for (int l = 0; l < Np; l++) x[l] = src[sp<DIM, Np>(line_node<DIM, Np, D>(line, l))];
 #pragma unroll
             for (int k = 0; k < Np; k++) {
                 double s = 0.0;
 #pragma unroll
                 for (int l = 0; l < Np; l++) s += Vinv[k * Np + l] * x[l];
-                dst[sp<Np>(line_node<DIM, Np, D>(line, k))] = s;
+                dst[sp<DIM, Np>(line_node<DIM, Np, D>(line, k))] = s;
             }
         }
     }
@@ -282,7 +303,7 @@ __device__ __forceinline__ double indicator_eta(double *buf, int gl, const doubl
             const int i = t % Np, j = (t / Np) % Np, k = DIM == 3 ? t / (Np * Np) : 0;
             int mx = i > j ? i : j;
             if (DIM == 3) mx = mx > k ? mx : k;
-            const double v = m[sp<Np>(t)] * m[sp<Np>(t)];
+            const double v = m[sp<DIM, Np>(t)] * m[sp<DIM, Np>(t)];
             mm += v;
             if (mx <= N - 1) m1 += v;
             if (mx <= N - 2) m2 += v;
@@ -315,7 +336,7 @@ __device__ __forceinline__ double stage_nodes(const KParams &P, int64_t e, bool 
                 s[v] = valid ? __ldg(P.u + (int64_t)v * P.nnodes + e * NDOF + n) : (v == 0 ? 1.0 : (v == NV - 1 ? P.gm1inv : 0.0));
             const Prim<DIM> q = make_prim<DIM>(s, P.gamma, P.gm1);
             constexpr int ST = S::NS_;
-            const int m = sp<S::Np>(n);
+            const int m = sp<DIM, S::Np>(n);
             pr[P_RHO * ST + m] = q.rho;
 #pragma unroll
             for (int d = 0; d < DIM; d++) pr[(P_V + d) * ST + m] = q.v[d];
@@ -358,7 +379,7 @@ __device__ __forceinline__ void ec_lines_rt(const KParams &P, int d, const doubl
         if (line < S::NFN) {
             Prim<DIM> q[Np];
 #pragma unroll
-            for (int l = 0; l < Np; l++) q[l] = slot_prim<DIM>(pr, sp<Np>(line_node_rt<DIM, Np>(d, line, l)), S::NS_);
+            for (int l = 0; l < Np; l++) q[l] = slot_prim<DIM>(pr, sp<DIM, Np>(line_node_rt<DIM, Np>(d, line, l)), S::NS_);
             double la[Np][NV];
 #pragma unroll
             for (int l = 0; l < Np; l++)
@@ -397,7 +418,7 @@ __device__ __forceinline__ void ec_lines_rt(const KParams &P, int d, const doubl
             }
 #pragma unroll
             for (int l = 0; l < Np; l++) {
-                const int n = sp<Np>(line_node_rt<DIM, Np>(d, line, l));
+                const int n = sp<DIM, Np>(line_node_rt<DIM, Np>(d, line, l));
 #pragma unroll
                 for (int v = 0; v < NV; v++) {
                     const double x = scale * la[l][v];
@@ -427,15 +448,15 @@ __device__ __forceinline__ void fv_lines(const KParams &P, const double *pr, dou
             double prev[NV];
 #pragma unroll
             for (int v = 0; v < NV; v++) prev[v] = 0.0;
-            Prim<DIM> qa = slot_prim<DIM>(pr, sp<Np>(line_node<DIM, Np, D>(line, 0)), S::NS_);
+            Prim<DIM> qa = slot_prim<DIM>(pr, sp<DIM, Np>(line_node<DIM, Np, D>(line, 0)), S::NS_);
             complete_prim<DIM>(qa, P.gamma);
 #pragma unroll
             for (int l = 0; l < Np; l++) {
-                const int n = sp<Np>(line_node<DIM, Np, D>(line, l));
+                const int n = sp<DIM, Np>(line_node<DIM, Np, D>(line, l));
                 double F[NV];
                 Prim<DIM> qb;
                 if (l < N) {
-                    qb = slot_prim<DIM>(pr, sp<Np>(line_node<DIM, Np, D>(line, l + 1)), S::NS_);
+                    qb = slot_prim<DIM>(pr, sp<DIM, Np>(line_node<DIM, Np, D>(line, l + 1)), S::NS_);
                     complete_prim<DIM>(qb, P.gamma);
                     double ma[DIM], mb[DIM];
 #pragma unroll
@@ -542,7 +563,7 @@ __device__ __forceinline__ void rhs_tile(const KParams &P, const double *c, doub
 #pragma unroll
                     for (int v = 0; v < NV; v++) {
                         const int64_t gi = (int64_t)v * P.nnodes + e * NDOF + n;
-                        P.out[gi] = stage_combine(P, gi, acc[v * ST + sp<Np>(n)]);
+                        P.out[gi] = stage_combine(P, gi, acc[v * ST + sp<DIM, Np>(n)]);
                     }
                 }
             }
@@ -560,7 +581,7 @@ __device__ __forceinline__ void rhs_tile(const KParams &P, const double *c, doub
 #pragma unroll
                 for (int v = 0; v < NV; v++) {
                     const int64_t gi = (int64_t)v * P.nnodes + e * NDOF + n;
-                    acc[v * ST + sp<Np>(n)] = stage_combine(P, gi, acc[v * ST + sp<Np>(n)]);
+                    acc[v * ST + sp<DIM, Np>(n)] = stage_combine(P, gi, acc[v * ST + sp<DIM, Np>(n)]);
                 }
             }
         }
@@ -579,7 +600,7 @@ __device__ __forceinline__ void rhs_tile(const KParams &P, const double *c, doub
                 if (d == 0) face_contrib<DIM, N, 0>(P, c, a, fn, coef, C);
                 else if (d == 1) face_contrib<DIM, N, 1>(P, c, a, fn, coef, C);
                 else face_contrib<DIM, N, (DIM == 3 ? 2 : 0)>(P, c, a, fn, coef, C);
-                const int n = sp<Np>(line_node_rt<DIM, Np>(d, fn, side ? N : 0));
+                const int n = sp<DIM, Np>(line_node_rt<DIM, Np>(d, fn, side ? N : 0));
 #pragma unroll
                 for (int v = 0; v < NV; v++) {
                     if (side) acc[v * ST + n] += C[v];
@@ -595,7 +616,7 @@ __device__ __forceinline__ void rhs_tile(const KParams &P, const double *c, doub
             const int n = gl + k * L;
             if (n < NDOF) {
 #pragma unroll
-                for (int v = 0; v < NV; v++) P.out[(int64_t)v * P.nnodes + e * NDOF + n] = acc[v * ST + sp<Np>(n)];
+                for (int v = 0; v < NV; v++) P.out[(int64_t)v * P.nnodes + e * NDOF + n] = acc[v * ST + sp<DIM, Np>(n)];
             }
         }
     }
@@ -604,8 +625,14 @@ __device__ __forceinline__ void rhs_tile(const KParams &P, const double *c, doub
 
 // Right-hand side element kernel (Euler or Navier-Stokes volume terms,
 // optional SSP-RK3 stage).
+// Resident blocks the register budget must allow: 4 for 3D N = 3 (whose
+// swizzled slots let four 4-warp blocks share an SM), 1 otherwise.
+template <int DIM, int N> struct RhsOccupancy {
+    static constexpr int min_blocks = (DIM == 3 && N == 3) ? 4 : 1;
+};
+
 template <int DIM, int N, bool NS>
-__global__ void __launch_bounds__(128) rhs_kernel(const KParams P)
+__global__ void __launch_bounds__(128, RhsOccupancy<DIM, N>::min_blocks) rhs_kernel(const KParams P)
 {
     using S = Shape<DIM, N>;
     constexpr int Np = S::Np, L = S::L, EPW = S::EPW;
@@ -617,7 +644,7 @@ __global__ void __launch_bounds__(128) rhs_kernel(const KParams P)
     const int grp = lane / L, gl = lane % L;
     const int wpb = blockDim.x >> 5;
     const bool lane_used = grp < EPW;
-    double *pr = smem + CONST_SLOTS + (size_t)(warp * EPW + (lane_used ? grp : 0)) * S::EL_RHS;
+    double *pr = smem + const_slots(Np) + (size_t)(warp * EPW + (lane_used ? grp : 0)) * S::EL_RHS;
     const int64_t wstride = (int64_t)gridDim.x * wpb;
     unsigned int flags = 0;
     double lam = 0.0;
@@ -837,13 +864,13 @@ __device__ __forceinline__ void grad_lines(const double *wv, double *g, const do
             for (int v = 0; v < NV; v++) {
                 double x[Np];
 #pragma unroll
-                for (int l = 0; l < Np; l++) x[l] = wv[v * ST + sp<Np>(line_node<DIM, Np, D>(line, l))];
+                for (int l = 0; l < Np; l++) x[l] = wv[v * ST + sp<DIM, Np>(line_node<DIM, Np, D>(line, l))];
 #pragma unroll
                 for (int p = 0; p < Np; p++) {
                     double a = 0.0;
 #pragma unroll
                     for (int l = 0; l < Np; l++) a += Dm[p * Np + l] * x[l];
-                    g[(D * NV + v) * ST + sp<Np>(line_node<DIM, Np, D>(line, p))] = (a * sc) * invJ;
+                    g[(D * NV + v) * ST + sp<DIM, Np>(line_node<DIM, Np, D>(line, p))] = (a * sc) * invJ;
                 }
             }
         }
@@ -868,13 +895,13 @@ __device__ __forceinline__ void divergence_lines(const double *fvs, double *dv, 
             for (int i = 0; i < NV - 1; i++) {
                 double x[Np];
 #pragma unroll
-                for (int l = 0; l < Np; l++) x[l] = fvs[(D * (NV - 1) + i) * ST + sp<Np>(line_node<DIM, Np, D>(line, l))];
+                for (int l = 0; l < Np; l++) x[l] = fvs[(D * (NV - 1) + i) * ST + sp<DIM, Np>(line_node<DIM, Np, D>(line, l))];
 #pragma unroll
                 for (int p = 0; p < Np; p++) {
                     double a = 0.0;
 #pragma unroll
                     for (int l = 0; l < Np; l++) a += Dh[p * Np + l] * x[l];
-                    const int m = i * ST + sp<Np>(line_node<DIM, Np, D>(line, p));
+                    const int m = i * ST + sp<DIM, Np>(line_node<DIM, Np, D>(line, p));
                     if (FIRST) dv[m] = invJ * a;
                     else dv[m] += invJ * a;
                 }
@@ -905,7 +932,7 @@ __global__ void __launch_bounds__(128) lift_kernel(const KParams P)
     const int grp = lane / L, gl = lane % L;
     const int wpb = blockDim.x >> 5;
     const bool lane_used = grp < EPW;
-    double *wv = smem + CONST_SLOTS + (size_t)(warp * EPW + (lane_used ? grp : 0)) * S::EL_LIFT;
+    double *wv = smem + const_slots(Np) + (size_t)(warp * EPW + (lane_used ? grp : 0)) * S::EL_LIFT;
     double *g = wv + NV * ST;
     const int64_t nn = P.nnodes;
     const bool compat = P.compat != 0;
@@ -930,7 +957,7 @@ __global__ void __launch_bounds__(128) lift_kernel(const KParams P)
                         s[v] = valid ? __ldg(P.u + v * nn + e * NDOF + n) : (v == 0 ? 1.0 : (v == NV - 1 ? P.gm1inv : 0.0));
                     entropy_vars<DIM>(s, P.gamma, P.gm1, P.gm1inv, w);
 #pragma unroll
-                    for (int v = 0; v < NV; v++) wv[v * ST + sp<Np>(n)] = w[v];
+                    for (int v = 0; v < NV; v++) wv[v * ST + sp<DIM, Np>(n)] = w[v];
                 }
             }
         }
@@ -951,7 +978,7 @@ __global__ void __launch_bounds__(128) lift_kernel(const KParams P)
             for (int k = 0; k < S::NPL; k++) {
                 const int n = gl + k * L;
                 if (n >= NDOF) break;
-                const int m = sp<Np>(n);
+                const int m = sp<DIM, Np>(n);
                 double s[NV];
 #pragma unroll
                 for (int v = 0; v < NV; v++) s[v] = valid ? __ldg(P.u + v * nn + e * NDOF + n) : (v == 0 ? 1.0 : (v == NV - 1 ? P.gm1inv : 0.0));
@@ -1020,7 +1047,7 @@ __global__ void __launch_bounds__(128) lift_kernel(const KParams P)
                 const int n = gl + k * L;
                 if (n < NDOF) {
 #pragma unroll
-                    for (int i = 0; i < NV - 1; i++) P.out[(int64_t)(1 + i) * nn + e * NDOF + n] += coef * wv[i * ST + sp<Np>(n)];
+                    for (int i = 0; i < NV - 1; i++) P.out[(int64_t)(1 + i) * nn + e * NDOF + n] += coef * wv[i * ST + sp<DIM, Np>(n)];
                 }
             }
         }
