@@ -102,9 +102,11 @@ template <int DIM, int N> struct Shape {
     // z-fill buffer
     static constexpr int ZFILL = NFN * N * NV;
     static constexpr int EL_RHS = NPRIM * NS_ + NV * NS_ + ZFILL;
-    // lift element slot: entropy variables (later the viscous RHS), gradients
-    // along each direction (later the contravariant viscous fluxes)
+    // adjoint lift slot: entropy variables, gradients along each direction
     static constexpr int EL_LIFT = NV * NS_ + DIM * NV * NS_;
+    // forward lift slot: entropy variables (later the viscous RHS) and the
+    // contravariant viscous fluxes (gradients are formed per node)
+    static constexpr int EL_LIFTF = NV * NS_ + DIM * (NV - 1) * NS_;
 };
 
 // Shared-memory position of node n, chosen so that the lanes of a line task
@@ -932,7 +934,7 @@ __global__ void __launch_bounds__(128) lift_kernel(const KParams P)
     const int grp = lane / L, gl = lane % L;
     const int wpb = blockDim.x >> 5;
     const bool lane_used = grp < EPW;
-    double *wv = smem + const_slots(Np) + (size_t)(warp * EPW + (lane_used ? grp : 0)) * S::EL_LIFT;
+    double *wv = smem + const_slots(Np) + (size_t)(warp * EPW + (lane_used ? grp : 0)) * S::EL_LIFTF;
     double *g = wv + NV * ST;
     const int64_t nn = P.nnodes;
     const bool compat = P.compat != 0;
@@ -963,12 +965,6 @@ __global__ void __launch_bounds__(128) lift_kernel(const KParams P)
         }
         __syncwarp();
         if (lane_used) {
-            grad_lines<DIM, N, 0>(wv, g, c, gl);
-            grad_lines<DIM, N, 1>(wv, g, c, gl);
-            if (DIM == 3) grad_lines<DIM, N, (DIM == 3 ? 2 : 0)>(wv, g, c, gl);
-        }
-        __syncwarp();
-        if (lane_used) {
             // state of the element's last node (compat volume viscous flux)
             double sl[NV];
 #pragma unroll
@@ -984,11 +980,22 @@ __global__ void __launch_bounds__(128) lift_kernel(const KParams P)
                 for (int v = 0; v < NV; v++) s[v] = valid ? __ldg(P.u + v * nn + e * NDOF + n) : (v == 0 ? 1.0 : (v == NV - 1 ? P.gm1inv : 0.0));
                 const int idx[3] = {n % Np, (n / Np) % Np, n / (Np * Np)};
                 double dq[DIM][NV];
+                const double *Dm = C_D(c);
 #pragma unroll
                 for (int d = 0; d < DIM; d++) {
-#pragma unroll
-                    for (int v = 0; v < NV; v++) dq[d][v] = g[(d * NV + v) * ST + m];
+                    // strong-form gradient along d at this node:
+                    // (sum_l D(pos, l) w_l) adj_d / J along the node's d line
                     const int pos = idx[d];
+                    const int gline = d == 0 ? (DIM == 2 ? idx[1] : idx[1] + Np * idx[2])
+                                             : (d == 1 ? (DIM == 2 ? idx[0] : idx[0] + Np * idx[2]) : idx[0] + Np * idx[1]);
+#pragma unroll
+                    for (int v = 0; v < NV; v++) {
+                        double a = 0.0;
+#pragma unroll
+                        for (int l = 0; l < Np; l++)
+                            a += Dm[pos * Np + l] * wv[v * ST + sp<DIM, Np>(line_node_rt<DIM, Np>(d, gline, l))];
+                        dq[d][v] = (a * C_ADJ(c)[d]) * C_INVJ(c);
+                    }
                     if (valid && (pos == 0 || pos == N)) {
                         const int line = d == 0 ? (DIM == 2 ? idx[1] : idx[1] + Np * idx[2])
                                                 : (d == 1 ? (DIM == 2 ? idx[0] : idx[0] + Np * idx[2]) : idx[0] + Np * idx[1]);
