@@ -780,7 +780,7 @@ __device__ __forceinline__ void face_contrib(const KParams &P, const double *c, 
 // direction every output entry belongs to exactly one face, so the
 // read-modify-write updates need no atomics.
 template <int DIM, int N, int D, bool NS>
-__global__ void __launch_bounds__(256) face_kernel(const KParams P)
+__global__ void __launch_bounds__(256, 3) face_kernel(const KParams P)
 {
     using S = Shape<DIM, N>;
     constexpr int NFN = S::NFN;
