@@ -970,6 +970,11 @@ __global__ void __launch_bounds__(128) lift_kernel(const KParams P)
 #pragma unroll
             for (int v = 0; v < NV; v++) sl[v] = valid ? __ldg(P.u + v * nn + e * NDOF + NDOF - 1) : (v == 0 ? 1.0 : (v == NV - 1 ? P.gm1inv : 0.0));
             const Prim<DIM> ql = make_prim<DIM>(sl, P.gamma, P.gm1);
+            // the next node's state is loaded one node ahead
+            double snext[NV];
+#pragma unroll
+            for (int v = 0; v < NV; v++)
+                snext[v] = (valid && gl < NDOF) ? __ldg(P.u + v * nn + e * NDOF + gl) : (v == 0 ? 1.0 : (v == NV - 1 ? P.gm1inv : 0.0));
 #pragma unroll 1
             for (int k = 0; k < S::NPL; k++) {
                 const int n = gl + k * L;
@@ -977,7 +982,11 @@ __global__ void __launch_bounds__(128) lift_kernel(const KParams P)
                 const int m = sp<DIM, Np>(n);
                 double s[NV];
 #pragma unroll
-                for (int v = 0; v < NV; v++) s[v] = valid ? __ldg(P.u + v * nn + e * NDOF + n) : (v == 0 ? 1.0 : (v == NV - 1 ? P.gm1inv : 0.0));
+                for (int v = 0; v < NV; v++) s[v] = snext[v];
+                const int nn2 = n + L;
+#pragma unroll
+                for (int v = 0; v < NV; v++)
+                    if (valid && k + 1 < S::NPL && nn2 < NDOF) snext[v] = __ldg(P.u + v * nn + e * NDOF + nn2);
                 const int idx[3] = {n % Np, (n / Np) % Np, n / (Np * Np)};
                 double dq[DIM][NV];
                 const double *Dm = C_D(c);
