@@ -990,6 +990,7 @@ __global__ void __launch_bounds__(128) lift_kernel(const KParams P)
                 const int idx[3] = {n % Np, (n / Np) % Np, n / (Np * Np)};
                 double dq[DIM][NV];
                 const double *Dm = C_D(c);
+                const NodeState<DIM> ns = node_state<DIM>(s, P.gm1);
 #pragma unroll
                 for (int d = 0; d < DIM; d++) {
                     // strong-form gradient along d at this node:
@@ -1013,7 +1014,7 @@ __global__ void __launch_bounds__(128) lift_kernel(const KParams P)
 #pragma unroll
                         for (int v = 0; v < NV; v++) dq[d][v] += __ldg(F + v);
                     }
-                    entgrad_to_primgrad<DIM>(s, P.gm1, P.gm1inv, compat, dq[d]);
+                    entgrad_to_primgrad_q<DIM>(ns, s, P.gm1inv, compat, dq[d]);
                     if (valid) {
 #pragma unroll
                         for (int v = 0; v < NV; v++) {
@@ -1023,7 +1024,14 @@ __global__ void __launch_bounds__(128) lift_kernel(const KParams P)
                     }
                 }
                 auto GQ = [&](int d, int v) { return dq[d][v]; };
-                const Prim<DIM> qn = make_prim<DIM>(s, P.gamma, P.gm1);
+                // the viscous flux reads v, p and 1/rho only
+                Prim<DIM> qn;
+                qn.rho = ns.rho;
+                qn.irho = ns.irho;
+#pragma unroll
+                for (int d = 0; d < DIM; d++) qn.v[d] = ns.vel[d];
+                qn.p = ns.p;
+                qn.beta = qn.ib = qn.lam = 0.0;
                 const Prim<DIM> &qv = compat ? ql : qn;
 #pragma unroll
                 for (int d = 0; d < DIM; d++) {

@@ -264,4 +264,43 @@ PDG_FN void entgrad_to_primgrad(const double *s, double gm1, double gm1inv, bool
     g[DIM + 1] = pr * (g[0] + p * gl);
 }
 
+// State quantities entgrad_to_primgrad and viscous_col derive from a node's
+// conservative state, formed once per node when all directions need them.
+template <int DIM> struct NodeState {
+    double rho, irho, vel[DIM], v_sq, p, pr, rop, KE;
+};
+template <int DIM> PDG_FN NodeState<DIM> node_state(const double *s, double gm1)
+{
+    NodeState<DIM> q;
+    q.rho = s[0];
+    q.irho = 1.0 / q.rho;
+    double vv = 0.0;
+#pragma unroll
+    for (int d = 0; d < DIM; d++) {
+        q.vel[d] = s[1 + d] * q.irho;
+        vv += q.vel[d] * q.vel[d];
+    }
+    q.v_sq = 0.5 * vv;
+    q.p = gm1 * (s[DIM + 1] - q.rho * q.v_sq);
+    q.KE = q.v_sq * q.rho;
+    q.pr = q.p * q.irho;
+    q.rop = q.rho / q.p;
+    return q;
+}
+// entgrad_to_primgrad with the node quantities formed beforehand (same
+// arithmetic, so the same values).
+template <int DIM>
+PDG_FN void entgrad_to_primgrad_q(const NodeState<DIM> &q, const double *s, double gm1inv, bool compat, double *g)
+{
+    const double gl = g[DIM + 1];
+    double acc = 0.0;
+#pragma unroll
+    for (int d = 0; d < DIM; d++) {
+        g[1 + d] = q.pr * (g[1 + d] + q.vel[d] * gl);
+        acc += (compat ? q.vel[d] : s[1 + d]) * g[1 + d];
+    }
+    g[0] = q.rho * g[0] - gl * (q.KE - q.p * gm1inv) + q.rop * acc;
+    g[DIM + 1] = q.pr * (g[0] + q.p * gl);
+}
+
 }  // namespace pdg
