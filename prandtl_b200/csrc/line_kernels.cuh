@@ -970,6 +970,10 @@ __global__ void __launch_bounds__(128) lift_kernel(const KParams P)
 #pragma unroll
             for (int v = 0; v < NV; v++) sl[v] = valid ? __ldg(P.u + v * nn + e * NDOF + NDOF - 1) : (v == 0 ? 1.0 : (v == NV - 1 ? P.gm1inv : 0.0));
             const Prim<DIM> ql = make_prim<DIM>(sl, P.gamma, P.gm1);
+            // the -d neighbours (owners of the -d faces' jumps)
+            int64_t enb[DIM];
+#pragma unroll
+            for (int d = 0; d < DIM; d++) enb[d] = valid ? (int64_t)__ldg(P.nbr + e * 2 * DIM + 2 * d) : 0;
             // the next node's state is loaded one node ahead
             double snext[NV];
 #pragma unroll
@@ -991,6 +995,20 @@ __global__ void __launch_bounds__(128) lift_kernel(const KParams P)
                 double dq[DIM][NV];
                 const double *Dm = C_D(c);
                 const NodeState<DIM> ns = node_state<DIM>(s, P.gm1);
+                // BR1 face jumps of the node's faces, loaded before the
+                // gradient arithmetic so that their latency overlaps it
+                double jf[DIM][NV];
+#pragma unroll
+                for (int d = 0; d < DIM; d++) {
+                    const int pos = idx[d];
+                    const bool face = valid && (pos == 0 || pos == N);
+                    const int line = d == 0 ? (DIM == 2 ? idx[1] : idx[1] + Np * idx[2])
+                                            : (d == 1 ? (DIM == 2 ? idx[0] : idx[0] + Np * idx[2]) : idx[0] + Np * idx[1]);
+                    const int64_t owner = pos == N ? e : enb[d];
+                    const double *F = P.lbuf + ((d * P.ne + owner) * NFN + line) * NV;
+#pragma unroll
+                    for (int v = 0; v < NV; v++) jf[d][v] = face ? __ldg(F + v) : 0.0;
+                }
 #pragma unroll
                 for (int d = 0; d < DIM; d++) {
                     // strong-form gradient along d at this node:
@@ -1007,12 +1025,8 @@ __global__ void __launch_bounds__(128) lift_kernel(const KParams P)
                         dq[d][v] = (a * C_ADJ(c)[d]) * C_INVJ(c);
                     }
                     if (valid && (pos == 0 || pos == N)) {
-                        const int line = d == 0 ? (DIM == 2 ? idx[1] : idx[1] + Np * idx[2])
-                                                : (d == 1 ? (DIM == 2 ? idx[0] : idx[0] + Np * idx[2]) : idx[0] + Np * idx[1]);
-                        const int64_t owner = pos == N ? e : (int64_t)__ldg(P.nbr + e * 2 * DIM + 2 * d);
-                        const double *F = P.lbuf + ((d * P.ne + owner) * NFN + line) * NV;
 #pragma unroll
-                        for (int v = 0; v < NV; v++) dq[d][v] += __ldg(F + v);
+                        for (int v = 0; v < NV; v++) dq[d][v] += jf[d][v];
                     }
                     entgrad_to_primgrad_q<DIM>(ns, s, P.gm1inv, compat, dq[d]);
                     if (valid) {
@@ -1055,6 +1069,16 @@ __global__ void __launch_bounds__(128) lift_kernel(const KParams P)
             }
         }
         __syncwarp();
+        // the output values the divergence is added to, loaded before the
+        // divergence line tasks
+        double oprev[S::NPL][NV - 1];
+#pragma unroll
+        for (int k = 0; k < S::NPL; k++) {
+            const int n = gl + k * L;
+#pragma unroll
+            for (int i = 0; i < NV - 1; i++)
+                oprev[k][i] = (valid && P.out && n < NDOF) ? P.out[(int64_t)(1 + i) * nn + e * NDOF + n] : 0.0;
+        }
         if (lane_used) {
             divergence_lines<DIM, N, 0, true>(g, wv, c, gl);
             divergence_lines<DIM, N, 1, false>(g, wv, c, gl);
@@ -1071,7 +1095,8 @@ __global__ void __launch_bounds__(128) lift_kernel(const KParams P)
                 const int n = gl + k * L;
                 if (n < NDOF) {
 #pragma unroll
-                    for (int i = 0; i < NV - 1; i++) P.out[(int64_t)(1 + i) * nn + e * NDOF + n] += coef * wv[i * ST + sp<DIM, Np>(n)];
+                    for (int i = 0; i < NV - 1; i++)
+                        P.out[(int64_t)(1 + i) * nn + e * NDOF + n] = oprev[k][i] + coef * wv[i * ST + sp<DIM, Np>(n)];
                 }
             }
         }
