@@ -755,13 +755,21 @@ __device__ __forceinline__ double face_node(const KParams &P, const double *c, i
     constexpr int Np = S::Np, NDOF = S::NDOF, NV = S::NV;
     const int64_t nn = P.nnodes;
     const int64_t b = __ldg(P.nbr + a * 2 * DIM + 2 * D + 1);
-    double C[NV];
-    const double lam = face_node_terms<DIM, N, D, NS>(P, c, a, b, fn, coef, C);
     const int na = line_node<DIM, Np, D>(fn, N), nb = line_node<DIM, Np, D>(fn, 0);
+    // the output values are loaded before the flux arithmetic, so that their
+    // latency overlaps it
+    double oa[NV], ob[NV];
 #pragma unroll
     for (int v = 0; v < NV; v++) {
-        P.out[v * nn + a * NDOF + na] += C[v];
-        P.out[v * nn + b * NDOF + nb] -= C[v];
+        oa[v] = P.out[v * nn + a * NDOF + na];
+        ob[v] = P.out[v * nn + b * NDOF + nb];
+    }
+    double C[NV];
+    const double lam = face_node_terms<DIM, N, D, NS>(P, c, a, b, fn, coef, C);
+#pragma unroll
+    for (int v = 0; v < NV; v++) {
+        P.out[v * nn + a * NDOF + na] = oa[v] + C[v];
+        P.out[v * nn + b * NDOF + nb] = ob[v] - C[v];
     }
     return lam;
 }
