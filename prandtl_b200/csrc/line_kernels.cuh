@@ -526,6 +526,9 @@ __device__ __forceinline__ void rhs_tile(const KParams &P, const double *c, doub
     const int64_t e0 = e_base + grp;
     const bool valid = lane_used && e0 < P.ne;
     const int64_t e = valid ? e0 : 0;
+    // the RK base state is first read by the final combine: bring the
+    // element's block of each variable into L2 now
+    if (!FACES && valid && P.stage > 0 && gl < NV) prefetch_l2(P.un + (int64_t)gl * P.nnodes + e * NDOF, sizeof(double) * NDOF);
     if (lane_used) {
         const double ls = stage_nodes<DIM, N>(P, e, valid, gl, pr, scratch, flags);
         if (valid) lam = fmax(lam, ls);
