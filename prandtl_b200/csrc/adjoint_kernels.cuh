@@ -420,6 +420,9 @@ __global__ void __launch_bounds__(128) adj_lift_kernel(const KParams P, const do
         }
         __syncwarp();
         // (iii) per node: viscous fluxes and gradient conversion in reverse
+        int64_t enb[2 * DIM];
+#pragma unroll
+        for (int f = 0; f < 2 * DIM; f++) enb[f] = valid ? (int64_t)__ldg(P.nbr + e * 2 * DIM + f) : 0;
         double sacc[S::NPL][NV];
 #pragma unroll
         for (int k = 0; k < S::NPL; k++)
@@ -434,6 +437,23 @@ __global__ void __launch_bounds__(128) adj_lift_kernel(const KParams P, const do
 #pragma unroll
             for (int v = 0; v < NV; v++) s[v] = valid ? __ldg(P.u + v * nn + e * NDOF + n) : (v == 0 ? 1.0 : (v == NV - 1 ? P.gm1inv : 0.0));
             const int idx[3] = {n % Np, (n / Np) % Np, n / (Np * Np)};
+            // global operands of the node's face terms, loaded first: the
+            // forward BR1 jumps and the neighbour's cotangent at each face
+            double jf[DIM][NV], lo[DIM][DIM + 1];
+#pragma unroll
+            for (int d = 0; d < DIM; d++) {
+                const int pos = idx[d];
+                const bool face = valid && (pos == 0 || pos == N);
+                const int line = line_of<DIM, Np>(d, idx);
+                const int64_t owner = pos == N ? e : enb[2 * d];
+                const double *F = P.lbuf + ((d * P.ne + owner) * NFN + line) * NV;
+#pragma unroll
+                for (int v = 0; v < NV; v++) jf[d][v] = face ? __ldg(F + v) : 0.0;
+                const int64_t other = enb[2 * d + (pos == N ? 1 : 0)];
+                const int no = line_node_rt<DIM, Np>(d, line, pos == N ? 0 : N);
+#pragma unroll
+                for (int i = 0; i <= DIM; i++) lo[d][i] = face ? __ldg(cot + (int64_t)(1 + i) * nn + other * NDOF + no) : 0.0;
+            }
             double gin[DIM][NV], dq[DIM][NV];
 #pragma unroll
             for (int d = 0; d < DIM; d++) {
@@ -441,11 +461,8 @@ __global__ void __launch_bounds__(128) adj_lift_kernel(const KParams P, const do
                 for (int v = 0; v < NV; v++) gin[d][v] = g[(d * NV + v) * ST + m];
                 const int pos = idx[d];
                 if (valid && (pos == 0 || pos == N)) {
-                    const int line = line_of<DIM, Np>(d, idx);
-                    const int64_t owner = pos == N ? e : (int64_t)__ldg(P.nbr + e * 2 * DIM + 2 * d);
-                    const double *F = P.lbuf + ((d * P.ne + owner) * NFN + line) * NV;
 #pragma unroll
-                    for (int v = 0; v < NV; v++) gin[d][v] += __ldg(F + v);
+                    for (int v = 0; v < NV; v++) gin[d][v] += jf[d][v];
                 }
 #pragma unroll
                 for (int v = 0; v < NV; v++) dq[d][v] = gin[d][v];
@@ -470,13 +487,10 @@ __global__ void __launch_bounds__(128) adj_lift_kernel(const KParams P, const do
                 if (valid && (pos == 0 || pos == N)) {
                     // the face column enters out_a with + fsc A / 2 and out_b with - fsc A / 2
                     const double h = 0.5 * fsc * C_AREA(c)[d];
-                    const int64_t other = __ldg(P.nbr + e * 2 * DIM + 2 * d + (pos == N ? 1 : 0));
-                    const int no = line_node_rt<DIM, Np>(d, line, pos == N ? 0 : N);
 #pragma unroll
                     for (int i = 0; i <= DIM; i++) {
-                        const double lo = __ldg(cot + (int64_t)(1 + i) * nn + other * NDOF + no);
                         const double le = wv[(1 + i) * ST + m];
-                        cb[d][i] += pos == N ? h * (le - lo) : h * (lo - le);
+                        cb[d][i] += pos == N ? h * (le - lo[d][i]) : h * (lo[d][i] - le);
                     }
                 }
             }
@@ -589,6 +603,12 @@ __global__ void __launch_bounds__(256) adj_face_kernel(const KParams P, const do
             la[v] = __ldg(cot + v * nn + a * NDOF + na);
             lb[v] = __ldg(cot + v * nn + b * NDOF + nb);
         }
+        double pa[NV], pb[NV];  // ubar before this direction's terms, loaded ahead
+#pragma unroll
+        for (int v = 0; v < NV; v++) {
+            pa[v] = ubar[v * nn + a * NDOF + na];
+            pb[v] = ubar[v * nn + b * NDOF + nb];
+        }
         const Prim<DIM> qa = make_prim<DIM>(sa, P.gamma, P.gm1), qb = make_prim<DIM>(sb, P.gamma, P.gm1);
         const bool a_is_1 = a <= b;
         const double nrm = a_is_1 ? C_AREA(c)[D] : -C_AREA(c)[D];
@@ -625,8 +645,8 @@ __global__ void __launch_bounds__(256) adj_face_kernel(const KParams P, const do
         }
 #pragma unroll
         for (int v = 0; v < NV; v++) {
-            ubar[v * nn + a * NDOF + na] += ga[v];
-            ubar[v * nn + b * NDOF + nb] += gb[v];
+            ubar[v * nn + a * NDOF + na] = pa[v] + ga[v];
+            ubar[v * nn + b * NDOF + nb] = pb[v] + gb[v];
         }
     }
 }
