@@ -383,6 +383,18 @@ def run_sweep(args, dev):
     res["per_case_launches"] = {"value": V * 3 * K / (ms * 1e-3), "ms_per_step": ms / K,
                                 "gpu_launches": sum(op.launch_count() for op in ops) - l0}
     res["batched_vs_per_case"] = res["batched_graph"]["value"] / res["per_case_launches"]["value"]
+    # one small case (the 32 x 32, N = 3 vortex): plain launches vs a replayed step graph
+    vm = cases.vortex_mesh(32, 3)
+    vop = pb.DGSEMOperator(vm)
+    vx = torch.from_numpy(cases.isentropic_vortex(vm)).to(dev)
+    vop.Mult(vx, torch.empty_like(vx))
+    vdt = vop.cfl_dt(0.5)
+    small = {"workload": "isentropic_vortex_32x32_N3_euler_blending", "vdofs": vm.size, "steps": K}
+    for graph in (False, True):
+        vop.rk3_step(vx, vdt, nsteps=args.warmup, graph=graph)
+        ms = timed(lambda: vop.rk3_step(vx, vdt, nsteps=K, graph=graph))
+        small["graph" if graph else "plain"] = {"value": vm.size * 3 * K / (ms * 1e-3), "ms_per_step": ms / K}
+    res["single_small_case"] = small
     res["autotuner"] = dict(cfg, best_rhs_launch_ms=tuned_ms)
     res["unit"] = UNIT
     return res

@@ -151,6 +151,12 @@ int pdg_rk_stage(pdg_ctx *ctx, int stage, double dt, const double *un,
  * in place by one step of size dt using context-owned stage buffers. */
 int pdg_rk3_step(pdg_ctx *ctx, double dt, double *u, void *stream);
 
+/* nsteps of pdg_rk3_step replayed from a CUDA graph: the first call for a
+ * (u, dt) pair captures one step (all its stage kernels) on an internal
+ * stream; later calls with the same pair only launch the graph.  Same values
+ * as pdg_rk3_step.  For small meshes, whose steps are bound by launch cost. */
+int pdg_rk3_steps(pdg_ctx *ctx, double dt, double *u, int nsteps, void *stream);
+
 /* Same step with a HOST state (the path an MFEM adapter would take for
  * ODESolver::Step on host Vectors): copies u in, runs the three fused stages,
  * copies the result back and synchronises.  u_host may be pinned or pageable. */

@@ -85,6 +85,7 @@ def library():
     L.pdg_rhs_host.argtypes = [C.c_void_p, _dp, _dp]
     L.pdg_rk_stage.argtypes = [C.c_void_p, C.c_int, C.c_double, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
     L.pdg_rk3_step.argtypes = [C.c_void_p, C.c_double, C.c_void_p, C.c_void_p]
+    L.pdg_rk3_steps.argtypes = [C.c_void_p, C.c_double, C.c_void_p, C.c_int, C.c_void_p]
     L.pdg_max_char_speed.argtypes = [C.c_void_p, _dp]
     L.pdg_cfl_dt.argtypes = [C.c_void_p, C.c_double, _dp]
     L.pdg_get_blending.argtypes = [C.c_void_p, _dp, _dp]
@@ -221,10 +222,17 @@ class DGSEMOperator:
                                           C.c_void_p(_stream_handle(stream))), "pdg_rk_stage")
         return uout
 
-    def rk3_step(self, u, dt: float, stream=None):
+    def rk3_step(self, u, dt: float, stream=None, nsteps: int = 1, graph: bool = False):
+        """nsteps SSP-RK3 steps of a device state in place; with graph=True
+        they are replayed from a CUDA graph captured for (u, dt)."""
         self._check_dev(u)
-        self._call(library().pdg_rk3_step(self._ctx, dt, C.c_void_p(u.data_ptr()), C.c_void_p(_stream_handle(stream))),
-                   "pdg_rk3_step")
+        if graph:
+            self._call(library().pdg_rk3_steps(self._ctx, dt, C.c_void_p(u.data_ptr()), int(nsteps),
+                                               C.c_void_p(_stream_handle(stream))), "pdg_rk3_steps")
+            return u
+        for _ in range(nsteps):
+            self._call(library().pdg_rk3_step(self._ctx, dt, C.c_void_p(u.data_ptr()),
+                                              C.c_void_p(_stream_handle(stream))), "pdg_rk3_step")
         return u
 
     def rk3_step_host(self, u: np.ndarray, dt: float):

@@ -47,6 +47,13 @@ struct pdg_ctx {
     double *ent_own = nullptr;                // filter: per-element entropy minimum at the stage input
     unsigned long long *filter_count = nullptr;
     double *gcol = nullptr;   // adjoint: cotangents of the face-normal entropy gradients
+    // pdg_rk3_steps: one step captured in a CUDA graph for a (state, dt) pair
+    cudaStream_t cap = nullptr;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t graph_exec = nullptr;
+    double *graph_u = nullptr;
+    double graph_dt = 0.0;
+    int64_t graph_launches = 0;
     bool adj_ready = false;
     // launch configuration per kernel kind
     KernelInfo kinfo[KIND_COUNT];
@@ -566,6 +573,9 @@ int pdg_destroy(pdg_ctx *c)
     cudaFree(c->err);
     cudaFree(c->ent_own);
     cudaFree(c->gcol);
+    if (c->graph_exec) cudaGraphExecDestroy(c->graph_exec);
+    if (c->graph) cudaGraphDestroy(c->graph);
+    if (c->cap) cudaStreamDestroy(c->cap);
     cudaFree(c->filter_count);
     for (auto &t : c->timed) {
         cudaEventDestroy(t.a);
@@ -623,6 +633,48 @@ int pdg_rk3_step(pdg_ctx *c, double dt, double *u, void *stream)
     // result can overwrite u in place
     if (!r) r = evaluate(c, 2, dt, u, c->stage_b, u, s);
     return r;
+}
+
+int pdg_rk3_steps(pdg_ctx *c, double dt, double *u, int nsteps, void *stream)
+{
+    if (!c) return PDG_ERR_ARG;
+    if (!u || nsteps < 0) return fail(c, PDG_ERR_ARG, "pdg_rk3_steps: bad arguments");
+    cudaStream_t s = (cudaStream_t)stream;
+    if (!c->graph_exec || c->graph_u != u || c->graph_dt != dt) {
+        if (c->graph_exec) cudaGraphExecDestroy(c->graph_exec);
+        if (c->graph) cudaGraphDestroy(c->graph);
+        c->graph_exec = nullptr;
+        c->graph = nullptr;
+        if (!c->cap && cudaStreamCreateWithFlags(&c->cap, cudaStreamNonBlocking) != cudaSuccess)
+            return fail(c, PDG_ERR_CUDA, "pdg_rk3_steps: stream creation failed");
+        const bool prof = c->profile;
+        c->profile = false;  // no timing events inside the graph
+        const int64_t l0 = c->launches;
+        CK(cudaStreamBeginCapture(c->cap, cudaStreamCaptureModeThreadLocal), "begin capture");
+        int r = evaluate(c, 0, dt, u, u, c->stage_a, c->cap);
+        if (!r) r = evaluate(c, 1, dt, u, c->stage_a, c->stage_b, c->cap);
+        if (!r) r = evaluate(c, 2, dt, u, c->stage_b, u, c->cap);
+        cudaGraph_t g = nullptr;
+        const cudaError_t e = cudaStreamEndCapture(c->cap, &g);
+        c->profile = prof;
+        c->graph_launches = c->launches - l0;
+        c->launches = l0;
+        if (r) {
+            if (g) cudaGraphDestroy(g);
+            return r;
+        }
+        if (e != cudaSuccess) return cuda_fail(c, e, "end capture");
+        c->graph = g;
+        CK(cudaGraphInstantiate(&c->graph_exec, c->graph, 0), "graph instantiate");
+        c->graph_u = u;
+        c->graph_dt = dt;
+    }
+    c->last_stream = s;
+    for (int i = 0; i < nsteps; i++) {
+        CK(cudaGraphLaunch(c->graph_exec, s), "graph launch");
+        c->launches += c->graph_launches;
+    }
+    return PDG_OK;
 }
 
 int pdg_rk3_step_host(pdg_ctx *c, double dt, double *u_host)

@@ -155,3 +155,27 @@ def test_error_word_flags_negative_density(cuda_device):
         op.check()
     assert ei.value.code == 4
     assert op.check() == 0  # the word was cleared
+
+
+@pytest.mark.parametrize("kind,dim,order,par", [("vortex", 2, 3, 0), ("tgv", 3, 2, 1)])
+def test_graph_replayed_steps_equal_plain_steps(kind, dim, order, par, cuda_device):
+    """pdg_rk3_steps (one captured step, replayed) gives pdg_rk3_step's values."""
+    import torch
+    mesh, u = make_case(kind, dim, order)
+    kw = dict(parabolic=par, mu=0.01 if par else 0.0, Pr=0.71)
+    op = pb.DGSEMOperator(mesh, **kw)
+    a = torch.from_numpy(u).to(cuda_device)
+    b = a.clone()
+    tmp = torch.empty_like(a)
+    op.Mult(a, tmp)
+    dt = op.cfl_dt(0.5)
+    op.rk3_step(a, dt, nsteps=4)
+    l0 = op.launch_count()
+    op.rk3_step(b, dt, nsteps=4, graph=True)
+    per_step = (op.launch_count() - l0) / 4
+    assert torch.equal(a, b)
+    assert per_step == (6 if par else 1 + dim) * 3
+    op.rk3_step(b, dt, nsteps=2, graph=True)   # replay without capture
+    op.rk3_step(a, dt, nsteps=2)
+    assert torch.equal(a, b)
+    assert op.check() == 0
