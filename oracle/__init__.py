@@ -99,9 +99,12 @@ class Oracle:
             raise ValueError("orc_create rejected the mesh/params")
 
     def __del__(self):
-        if getattr(self, "h", None):
-            lib().orc_destroy(self.h)
-            self.h = None
+        try:
+            if getattr(self, "h", None) and _lib is not None:
+                _lib.orc_destroy(self.h)
+                self.h = None
+        except Exception:
+            pass  # interpreter shutdown
 
     def rhs(self, u: np.ndarray) -> np.ndarray:
         u = np.ascontiguousarray(u, dtype=np.float64)

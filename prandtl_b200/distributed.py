@@ -97,11 +97,15 @@ class SlabDecomposition:
 
 
 class GhostExchange:
-    """Point-to-point exchange of the ghost layers of a local state tensor."""
+    """Point-to-point exchange of the ghost layers of a local state tensor.
+    Ghost layers are received in place (they are contiguous per variable);
+    only when a rank's two ghost layers are the same layer (two ranks, one
+    layer each) does the second message land in a scratch buffer."""
 
     def __init__(self, dec: SlabDecomposition, group=None):
         self.dec = dec
         self.group = group
+        self._scratch = None
 
     def _layer_views(self, u, pos):
         dec = self.dec
@@ -122,26 +126,21 @@ class GhostExchange:
         first = self._layer_views(u, dec.owned_first)
         last = self._layer_views(u, dec.owned_first + dec.owned_count - 1)
         ghost_hi = self._layer_views(u, dec.ghost_hi_pos)
-        ghost_lo = self._layer_views(u, dec.ghost_lo_pos)
-        recv_hi = [t.clone() for t in ghost_hi]
-        recv_lo = [t.clone() for t in ghost_lo]
+        if dec.ghost_lo_pos == dec.ghost_hi_pos:
+            nd = dec.layer_size * dec.glob.ndof
+            if self._scratch is None or self._scratch.device != u.device or self._scratch.dtype != u.dtype:
+                self._scratch = u.new_empty((dec.glob.nv, nd))
+            ghost_lo = [self._scratch[k] for k in range(dec.glob.nv)]
+        else:
+            ghost_lo = self._layer_views(u, dec.ghost_lo_pos)
         # the same order on every rank: to prev (first owned layer), to next
         # (last owned layer); from next (ghost_hi), from prev (ghost_lo)
-        ops = []
-        for t in first:
-            ops.append(dist.P2POp(dist.isend, t.contiguous(), prev, self.group))
-        for t in last:
-            ops.append(dist.P2POp(dist.isend, t.contiguous(), nxt, self.group))
-        for t in recv_hi:
-            ops.append(dist.P2POp(dist.irecv, t, nxt, self.group))
-        for t in recv_lo:
-            ops.append(dist.P2POp(dist.irecv, t, prev, self.group))
+        ops = [dist.P2POp(dist.isend, t, prev, self.group) for t in first]
+        ops += [dist.P2POp(dist.isend, t, nxt, self.group) for t in last]
+        ops += [dist.P2POp(dist.irecv, t, nxt, self.group) for t in ghost_hi]
+        ops += [dist.P2POp(dist.irecv, t, prev, self.group) for t in ghost_lo]
         for r in dist.batch_isend_irecv(ops):
             r.wait()
-        for dst, src in zip(ghost_hi, recv_hi):
-            dst.copy_(src)
-        for dst, src in zip(ghost_lo, recv_lo):
-            dst.copy_(src)
 
 
 class DistributedRK3:

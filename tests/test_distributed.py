@@ -31,6 +31,8 @@ class OracleStages:
 CASES = {
     "ns3d": dict(dim=3, order=2, n=(3, 2, 6), lo=0.0, hi=2 * np.pi, params=dict(parabolic=1, mu=0.02, Pr=0.71)),
     "euler2d": dict(dim=2, order=3, n=(4, 5), lo=-1.0, hi=1.0, params=dict(parabolic=0)),
+    # two layers on two ranks: each rank's two ghost layers are the same layer
+    "euler2d_thin": dict(dim=2, order=2, n=(4, 2), lo=-1.0, hi=1.0, params=dict(parabolic=0)),
 }
 
 
@@ -83,8 +85,8 @@ def _free_port():
     return p
 
 
-@pytest.mark.parametrize("world", [2, 3])
-@pytest.mark.parametrize("case,compat", [("ns3d", 1), ("ns3d", 0), ("euler2d", 1)])
+@pytest.mark.parametrize("world,case,compat", [(2, "ns3d", 1), (2, "ns3d", 0), (2, "euler2d", 1), (3, "ns3d", 1),
+                                               (3, "ns3d", 0), (3, "euler2d", 1), (2, "euler2d_thin", 1)])
 def test_slab_decomposition_matches_undivided(world, case, compat):
     ctx = mp.get_context("spawn")
     q = ctx.Queue()
