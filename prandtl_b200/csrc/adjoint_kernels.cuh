@@ -22,8 +22,8 @@ namespace pdg {
 template <int DIM, int N> struct AdjShape {
     using S = Shape<DIM, N>;
     // slot: primitives (rho, v, beta), cotangent lam, primitive cotangents,
-    // scratch (indicator input / modal buffers / forward volume sums)
-    static constexpr int EL = 4 * S::NV * S::NS_;
+    // two scratch fields (indicator input / modal buffers)
+    static constexpr int EL = (3 * S::NV + 2) * S::NS_;
 };
 
 // Line index (within direction d) and position of node n = (i, j, k).
@@ -161,6 +161,77 @@ __device__ __forceinline__ void fv_lines_vjp(const KParams &P, const double *pr,
         }
     }
     __syncwarp();
+}
+
+// This lane's share of lam . (d acc / d alpha) for the flux-differencing
+// terms: sum over its lines' pairs of scale F (Dhat2(a,b) lam_a + Dhat2(b,a)
+// lam_b), the forward volume sums contracted with lam without storing them.
+template <int DIM, int N>
+__device__ __forceinline__ double ec_lines_dot(const KParams &P, int d, const double *pr, const double *lm,
+                                               const double *c, int gl, double scale)
+{
+    using S = Shape<DIM, N>;
+    constexpr int Np = S::Np, NV = S::NV, ST = S::NS_;
+    const double metric = C_ADJ(c)[d];
+    const double *D2 = C_DHAT2(c);
+    double dot = 0.0;
+#pragma unroll 1
+    for (int r = 0; r < S::LPL; r++) {
+        const int line = gl + r * S::L;
+        if (line < S::NFN) {
+            Prim<DIM> q[Np];
+#pragma unroll
+            for (int l = 0; l < Np; l++) q[l] = slot_prim<DIM>(pr, sp<DIM, Np>(line_node_rt<DIM, Np>(d, line, l)), ST);
+#pragma unroll
+            for (int a = 0; a < Np; a++)
+#pragma unroll
+                for (int b = a + 1; b < Np; b++) {
+                    const int na = sp<DIM, Np>(line_node_rt<DIM, Np>(d, line, a));
+                    const int nb = sp<DIM, Np>(line_node_rt<DIM, Np>(d, line, b));
+                    double F[NV];
+                    volume_flux_rt<DIM>(q[a], q[b], d, metric, P.gm1inv, F);
+                    const double cab = scale * D2[a * Np + b], cba = scale * D2[b * Np + a];
+#pragma unroll
+                    for (int v = 0; v < NV; v++) dot += F[v] * (cab * lm[v * ST + na] + cba * lm[v * ST + nb]);
+                }
+        }
+    }
+    return dot;
+}
+
+// The same for the subcell FV terms along D (alpha = 1).
+template <int DIM, int N, int D>
+__device__ __forceinline__ double fv_lines_dot(const KParams &P, const double *pr, const double *lm, const double *c,
+                                               int gl)
+{
+    using S = Shape<DIM, N>;
+    constexpr int Np = S::Np, NV = S::NV, ST = S::NS_;
+    const double *sn = C_SNOR(c, D), *fvs = C_FVS(c);
+    double dot = 0.0;
+#pragma unroll
+    for (int r = 0; r < S::LPL; r++) {
+        const int line = gl + r * S::L;
+        if (line < S::NFN) {
+#pragma unroll 1
+            for (int l = 0; l < N; l++) {
+                const int na = sp<DIM, Np>(line_node<DIM, Np, D>(line, l)), nb = sp<DIM, Np>(line_node<DIM, Np, D>(line, l + 1));
+                Prim<DIM> qa = slot_prim<DIM>(pr, na, ST), qb = slot_prim<DIM>(pr, nb, ST);
+                complete_prim<DIM>(qa, P.gamma);
+                complete_prim<DIM>(qb, P.gamma);
+                double ma[DIM], mb[DIM];
+#pragma unroll
+                for (int k = 0; k < DIM; k++) {
+                    ma[k] = qa.rho * qa.v[k];
+                    mb[k] = qb.rho * qb.v[k];
+                }
+                double F[NV];
+                face_flux<DIM, D>(qa, qb, ma, mb, sn[l + 1], P.gm1inv, P.compat != 0, P.diss_scale, F);
+#pragma unroll
+                for (int v = 0; v < NV; v++) dot += F[v] * (fvs[l + 1] * lm[v * ST + nb] - fvs[l] * lm[v * ST + na]);
+            }
+        }
+    }
+    return dot;
 }
 
 // Reverse of the blending coefficient for one lane group (an element):
@@ -310,19 +381,12 @@ __global__ void __launch_bounds__(128) adj_rhs_kernel(const KParams P, const dou
         }
         // blending coefficient: d(acc)/d(alpha) = invJ EC + FV; alpha <- eta <- rho p
         if (__any_sync(0xffffffffu, dalpha != 0.0)) {
-#pragma unroll 1
-            for (int d = 0; d < DIM; d++) ec_lines_rt<DIM, N>(P, d, pr, scr, nullptr, c, gl, C_INVJ(c), false, false);
-            fv_lines<DIM, N, 0>(P, pr, scr, c, gl, 1.0);
-            fv_lines<DIM, N, 1>(P, pr, scr, c, gl, 1.0);
-            if (DIM == 3) fv_lines<DIM, N, (DIM == 3 ? 2 : 0)>(P, pr, scr, c, gl, 1.0);
             double abar = 0.0;
-#pragma unroll
-            for (int k = 0; k < S::NPL; k++) {
-                const int n = gl + k * L;
-                if (n < NDOF)
-#pragma unroll
-                    for (int v = 0; v < NV; v++) abar += lm[v * ST + sp<DIM, Np>(n)] * scr[v * ST + sp<DIM, Np>(n)];
-            }
+#pragma unroll 1
+            for (int d = 0; d < DIM; d++) abar += ec_lines_dot<DIM, N>(P, d, pr, lm, c, gl, C_INVJ(c));
+            abar += fv_lines_dot<DIM, N, 0>(P, pr, lm, c, gl);
+            abar += fv_lines_dot<DIM, N, 1>(P, pr, lm, c, gl);
+            if (DIM == 3) abar += fv_lines_dot<DIM, N, (DIM == 3 ? 2 : 0)>(P, pr, lm, c, gl);
             abar = group_sum<L>(abar);
             __syncwarp();
             indicator_vjp<DIM, N>(pr, pb, scr, c, gl, valid ? abar * dalpha : 0.0);
