@@ -503,9 +503,9 @@ __device__ __forceinline__ double stage_coef(const KParams &P)
     return 2. / 3 * P.dt;
 }
 
-template <int DIM, int N, int D>
-__device__ __forceinline__ void face_contrib(const KParams &P, const double *c, int64_t a, int fn, double coef,
-                                             double *C);
+template <int DIM, int N, int D, bool NS>
+__device__ __forceinline__ double face_node_terms(const KParams &P, const double *c, int64_t a, int64_t b, int fn,
+                                                  double coef, double *C);
 
 // One warp tile of the right-hand side element kernel: EPW elements from
 // e_base, one lane group each.  Volume terms (flux differencing, subcell FV
@@ -600,11 +600,12 @@ __device__ __forceinline__ void rhs_tile(const KParams &P, const double *c, doub
                 const int side = t >= NFN, fn = side ? t - NFN : t;
                 // side 1: this element's +d face (it is element a); side 0:
                 // its -d face, whose element a is the -d neighbour
-                const int64_t a = side ? e : (int64_t)__ldg(P.nbr + e * 2 * DIM + 2 * d);
+                const int64_t other = __ldg(P.nbr + e * 2 * DIM + 2 * d + side);
+                const int64_t a = side ? e : other, b = side ? other : e;
                 double C[NV];
-                if (d == 0) face_contrib<DIM, N, 0>(P, c, a, fn, coef, C);
-                else if (d == 1) face_contrib<DIM, N, 1>(P, c, a, fn, coef, C);
-                else face_contrib<DIM, N, (DIM == 3 ? 2 : 0)>(P, c, a, fn, coef, C);
+                if (d == 0) face_node_terms<DIM, N, 0, false>(P, c, a, b, fn, coef, C);
+                else if (d == 1) face_node_terms<DIM, N, 1, false>(P, c, a, b, fn, coef, C);
+                else face_node_terms<DIM, N, (DIM == 3 ? 2 : 0), false>(P, c, a, b, fn, coef, C);
                 const int n = sp<DIM, Np>(line_node_rt<DIM, Np>(d, fn, side ? N : 0));
 #pragma unroll
                 for (int v = 0; v < NV; v++) {
@@ -777,15 +778,6 @@ __device__ __forceinline__ double face_node(const KParams &P, const double *c, i
     return lam;
 }
 
-// Euler face terms C of the face node (a's +D face, node fn) for the
-// element-centric face pass of rhs_tile.
-template <int DIM, int N, int D>
-__device__ __forceinline__ void face_contrib(const KParams &P, const double *c, int64_t a, int fn, double coef,
-                                             double *C)
-{
-    const int64_t b = __ldg(P.nbr + a * 2 * DIM + 2 * D + 1);
-    face_node_terms<DIM, N, D, false>(P, c, a, b, fn, coef, C);
-}
 
 // Face kernel of direction D: one thread per (element, face node).  Within one
 // direction every output entry belongs to exactly one face, so the

@@ -87,7 +87,7 @@ def test_batch_steps_match_per_case(graph, cuda_device):
 
 
 def test_batch_tuner_keeps_results(cuda_device):
-    """The autotuner picks a configuration; results do not depend on it."""
+    """The autotuner picks a configuration; results do not depend on it beyond rounding."""
     import torch
     cs = _mixed_cases(num=8, seed=5)
     batch = pb.DGSEMBatch([m for m, _ in cs])
@@ -99,4 +99,7 @@ def test_batch_tuner_keeps_results(cuda_device):
     assert ms > 0 and cfg["warps_per_block"] in (1, 2, 4, 8) and cfg["tiles_per_fetch"] in (1, 2, 4, 8)
     assert cfg["blocks"] >= 148
     batch.Mult(u, b)
-    assert rel_maxnorm(b.cpu().numpy(), a.cpu().numpy()) == 0.0
+    # warps per block, tiles per fetch and tile order leave the arithmetic
+    # unchanged; the register-budget variants are separate compilations whose
+    # instruction selection may differ in the last bit
+    assert rel_maxnorm(b.cpu().numpy(), a.cpu().numpy()) < 1e-14
