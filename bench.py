@@ -317,6 +317,8 @@ def run_ours(args):
         out["sweep"] = run_sweep(args, dev)
     if not args.no_adjoint and world == 1:
         out["adjoint"] = run_adjoint(args, dev)
+    if args.sweep_steps > 0 and world == 1:
+        out["filter_case"] = run_filter_case(args, dev)
     if rank == 0 and world == 1 and not args.no_cpu:
         out["cpu_baseline"] = cpu_baseline(mesh, u0, params, args.cpu_seconds)
     if rank == 0:
@@ -464,6 +466,34 @@ def run_adjoint(args, dev):
             "vjp_kernels": kernels,
             "ke_gradient_20_steps": {"forward_20_steps_ms": fwd20, "gradient_ms": grad20,
                                      "checkpoint_every": 5, "ratio": grad20 / fwd20}}
+
+
+def run_filter_case(args, dev):
+    """Kelvin-Helmholtz 64 x 64, N = 4, Euler with the entropy filter after
+    every stage: 200 SSP-RK3 steps, CFL 0.5."""
+    import torch
+
+    import prandtl_b200 as pb
+    m = cases.kh_mesh(64, 4)
+    op = pb.DGSEMOperator(m, filter=1)
+    x = torch.from_numpy(cases.kelvin_helmholtz(m)).to(dev)
+    op.Mult(x, torch.empty_like(x))
+    dt = op.cfl_dt(0.5)
+    steps = 200
+    op.rk3_step(x, dt, nsteps=args.warmup, graph=True)
+    f0 = op.filter_count()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    op.rk3_step(x, dt, nsteps=steps, graph=True)
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    filtered = op.filter_count() - f0
+    op.check()
+    return {"workload": "kelvin_helmholtz_64x64_N4_euler_blending_entropy_filter", "vdofs": m.size, "steps": steps,
+            "value": m.size * 3 * steps / (ms * 1e-3), "unit": UNIT, "ms_per_step": ms / steps,
+            "element_filterings": filtered, "path": "pdg_rk3_steps (graph-replayed steps)"}
 
 
 def _ref_worker(payload):
