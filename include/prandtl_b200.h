@@ -229,6 +229,8 @@ int64_t pdg_launch_count(const pdg_ctx *ctx);
 #define PDG_KERNEL_ADJ_LIFT  13  /* adjoint: viscous terms */
 #define PDG_KERNEL_ADJ_FACE_E0  14  /* adjoint Euler face kernels, x / y / z (14, 15, 16) */
 #define PDG_KERNEL_ADJ_FACE_NS0 17  /* adjoint Navier-Stokes face kernels (17, 18, 19) */
+#define PDG_KERNEL_EULER_FACES 20   /* Euler volume + face terms (+ stage), fixed operator */
+#define PDG_KERNEL_NS_FACES  21     /* Navier-Stokes inviscid volume + all face terms (+ stage), fixed operator */
 int pdg_profile_enable(pdg_ctx *ctx, int on);
 int pdg_profile_read(pdg_ctx *ctx, int kind, double *total_ms, int64_t *launches);
 

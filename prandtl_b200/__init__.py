@@ -37,6 +37,7 @@ KERNEL_FILTER_BOUNDS, KERNEL_FILTER = 10, 11
 KERNEL_ADJ_RHS, KERNEL_ADJ_LIFT = 12, 13
 KERNEL_ADJ_FACE_EULER = (14, 15, 16)
 KERNEL_ADJ_FACE_NS = (17, 18, 19)
+KERNEL_EULER_FACES, KERNEL_NS_FACES = 20, 21
 PDG_FLAG_NONFINITE = 1
 PDG_FLAG_NONPHYSICAL = 2
 _STATUS = {1: "bad argument", 2: "CUDA error", 3: "non-finite state", 4: "non-physical state",

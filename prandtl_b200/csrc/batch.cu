@@ -51,7 +51,7 @@ __device__ __forceinline__ void batch_tile(const KParams &P, const double *c, do
     const int grp = lane / S::L, gl = lane % S::L;
     const bool lane_used = grp < S::EPW;
     double *pr = slot + (lane_used ? grp : 0) * S::EL_RHS;
-    rhs_tile<2, N, false, true>(P, c, pr, e_base, grp, gl, lane_used, flags, lam);
+    rhs_tile<2, N, false, true, false>(P, c, pr, e_base, grp, gl, lane_used, flags, lam);
 }
 
 // MINB = minimum resident blocks per SM the compiler must allow (register

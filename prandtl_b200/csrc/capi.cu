@@ -40,6 +40,7 @@ struct pdg_ctx {
     double *eta = nullptr, *alpha = nullptr;
     double *lbuf = nullptr;                         // BR1 lifting jumps [d][e][fn][v]
     double *fcol = nullptr;                         // viscous normal columns at faces
+    double *vbuf = nullptr;                         // viscous volume term [v-1][node] (element-side faces)
     double *stage_a = nullptr, *stage_b = nullptr;  // RK stage buffers
     double *io_a = nullptr, *io_b = nullptr;        // host-path staging
     unsigned long long *lam_bits = nullptr;
@@ -62,6 +63,9 @@ struct pdg_ctx {
     size_t smem[KIND_COUNT];
     int64_t launches = 0;
     int prefetch = 1;  // PDG_PREFETCH=0 in the environment turns the L2 prefetch off
+    // fixed operator: face terms inside the volume kernel, each face evaluated
+    // by both of its elements (PDG_ELEMENT_FACES=0: separate face kernels)
+    bool element_faces = true;
     bool profile = false;
     struct TimedLaunch { int kind; cudaEvent_t a, b; };
     std::vector<TimedLaunch> timed;
@@ -295,8 +299,8 @@ int kernel_config(int dim, int N, int kind, int64_t ne, int device, LaunchCfg *c
 bool kind_used(int kind, int dim, bool parabolic, bool filter)
 {
     if (kind == KIND_FILTER_BOUNDS || kind == KIND_FILTER) return filter;
-    if (kind >= KIND_ADJ_RHS) return false;  // configured by the first pdg_rhs_vjp
-    const bool ns_kind = kind == KIND_NS || kind == KIND_LIFT || kind == KIND_LIFT_FACE ||
+    if (kind >= KIND_ADJ_RHS && kind <= KIND_ADJ_FACE_NS2) return false;  // configured by the first pdg_rhs_vjp
+    const bool ns_kind = kind == KIND_NS || kind == KIND_NS_FACES || kind == KIND_LIFT || kind == KIND_LIFT_FACE ||
                          (kind >= KIND_FACE_NS0 && kind <= KIND_FACE_NS2);
     if (ns_kind != parabolic) return false;
     if ((kind == KIND_FACE_E2 || kind == KIND_FACE_NS2) && dim < 3) return false;
@@ -436,8 +440,12 @@ int lift(pdg_ctx *c, KParams P, const double *u, double *grads_out, cudaStream_t
     return launch(c, KIND_LIFT, P, s);
 }
 
-// RHS (stage < 0) or fused SSP-RK3 stage of the operator on device buffers:
-// the volume kernel writes the output, the lifting kernel (NS) and the face
+// RHS (stage < 0) or fused SSP-RK3 stage of the operator on device buffers.
+// Fixed operator: (NS: BR1 face jumps, then the lifting kernel, which stores
+// the viscous volume term to vbuf and the face columns to fcol) one volume
+// kernel that also evaluates every face from both sides and writes the
+// finished output.  Reference-value operator (or PDG_ELEMENT_FACES=0): the
+// volume kernel writes the output, the lifting kernel (NS) and the face
 // kernels of each direction add their terms.
 int evaluate(pdg_ctx *c, int stage, double dt, const double *un, const double *us, double *out, cudaStream_t s)
 {
@@ -450,19 +458,29 @@ int evaluate(pdg_ctx *c, int stage, double dt, const double *un, const double *u
     P.dt = dt;
     c->last_stream = s;
     int r;
+    const bool element_faces = c->element_faces && !c->p.compat;
     if (c->p.parabolic) {
-        KParams Lf = P;
         if (c->p.filter && stage >= 0 && (r = launch(c, KIND_FILTER_BOUNDS, P, s))) return r;
-        if ((r = launch(c, KIND_LIFT_FACE, Lf, s))) return r;
-        if ((r = launch(c, KIND_NS, P, s))) return r;
-        if ((r = launch(c, KIND_LIFT, P, s))) return r;
-        for (int d = 0; d < c->dim; d++)
-            if ((r = launch(c, KIND_FACE_NS0 + d, P, s))) return r;
+        if ((r = launch(c, KIND_LIFT_FACE, P, s))) return r;
+        if (element_faces) {
+            P.vbuf = c->vbuf;
+            if ((r = launch(c, KIND_LIFT, P, s))) return r;
+            if ((r = launch(c, KIND_NS_FACES, P, s))) return r;
+        } else {
+            if ((r = launch(c, KIND_NS, P, s))) return r;
+            if ((r = launch(c, KIND_LIFT, P, s))) return r;
+            for (int d = 0; d < c->dim; d++)
+                if ((r = launch(c, KIND_FACE_NS0 + d, P, s))) return r;
+        }
     } else {
         if (c->p.filter && stage >= 0 && (r = launch(c, KIND_FILTER_BOUNDS, P, s))) return r;
-        if ((r = launch(c, KIND_EULER, P, s))) return r;
-        for (int d = 0; d < c->dim; d++)
-            if ((r = launch(c, KIND_FACE_E0 + d, P, s))) return r;
+        if (element_faces) {
+            if ((r = launch(c, KIND_EULER_FACES, P, s))) return r;
+        } else {
+            if ((r = launch(c, KIND_EULER, P, s))) return r;
+            for (int d = 0; d < c->dim; d++)
+                if ((r = launch(c, KIND_FACE_E0 + d, P, s))) return r;
+        }
     }
     // entropy filter of the stage output (EntropyFilter::FilterSolution)
     if (c->p.filter && stage >= 0 && (r = launch(c, KIND_FILTER, P, s))) return r;
@@ -523,6 +541,7 @@ int pdg_create(const pdg_mesh *mesh, const pdg_params *params, pdg_ctx **out)
     };
     if (cudaGetDevice(&c->device) != cudaSuccess) return cleanup(PDG_ERR_CUDA);
     if (const char *pf = std::getenv("PDG_PREFETCH")) c->prefetch = std::atoi(pf) != 0;
+    if (const char *ef = std::getenv("PDG_ELEMENT_FACES")) c->element_faces = std::atoi(ef) != 0;
     build_constants(c);
     const size_t fbytes = sizeof(double) * (size_t)c->size;
     if (cudaMalloc(&c->K, sizeof(DevConst)) != cudaSuccess || cudaMalloc(&c->nbr, sizeof(int32_t) * c->ne * 2 * c->dim) ||
@@ -539,7 +558,8 @@ int pdg_create(const pdg_mesh *mesh, const pdg_params *params, pdg_ctx **out)
     if (c->p.parabolic) {
         const size_t nfn = c->dim == 2 ? c->Np : c->Np * c->Np;
         if (cudaMalloc(&c->lbuf, sizeof(double) * c->dim * c->ne * nfn * c->nv) != cudaSuccess ||
-            cudaMalloc(&c->fcol, sizeof(double) * 2 * c->dim * c->ne * nfn * (c->nv - 1)) != cudaSuccess)
+            cudaMalloc(&c->fcol, sizeof(double) * 2 * c->dim * c->ne * nfn * (c->nv - 1)) != cudaSuccess ||
+            cudaMalloc(&c->vbuf, sizeof(double) * (c->nv - 1) * c->nnodes) != cudaSuccess)
             return cleanup(PDG_ERR_NOMEM);
     }
     if (cudaMemcpy(c->K, &c->hK, sizeof(DevConst), cudaMemcpyHostToDevice) ||
@@ -565,6 +585,7 @@ int pdg_destroy(pdg_ctx *c)
     cudaFree(c->alpha);
     cudaFree(c->lbuf);
     cudaFree(c->fcol);
+    cudaFree(c->vbuf);
     cudaFree(c->stage_a);
     cudaFree(c->stage_b);
     cudaFree(c->io_a);

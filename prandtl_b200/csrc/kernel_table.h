@@ -24,7 +24,9 @@ enum KernelKind {
     KIND_ADJ_FACE_NS0 = 17,   // adj_face_kernel<dim, N, d, true>
     KIND_ADJ_FACE_NS1 = 18,
     KIND_ADJ_FACE_NS2 = 19,
-    KIND_COUNT = 20
+    KIND_EULER_FACES = 20,    // rhs_kernel<dim, N, false, true>: Euler volume + face terms (+ stage)
+    KIND_NS_FACES = 21,       // rhs_kernel<dim, N, true, true>: NS inviscid volume + all face terms (+ stage)
+    KIND_COUNT = 22
 };
 
 struct KernelInfo {

@@ -63,6 +63,7 @@ struct KParams {
     double *lbuf;         // BR1 lifting jumps [d][e][face node][v]
     double *fcol;         // viscous flux normal columns at faces [d][side][e][face node][i]
     double *grads_out;    // optional: primitive gradients [d][v][node] (diagnostics)
+    double *vbuf;         // NS with element-side faces: viscous volume term [v-1][node]
     const int32_t *nbr;   // [ne][2*dim]
     const DevConst *K;
     double *eta_out, *alpha_out;
@@ -506,15 +507,107 @@ __device__ __forceinline__ double stage_coef(const KParams &P)
 template <int DIM, int N, int D, bool NS>
 __device__ __forceinline__ double face_node_terms(const KParams &P, const double *c, int64_t a, int64_t b, int fn,
                                                   double coef, double *C);
+template <int DIM, bool NS> struct FaceIn;
+template <int DIM, int N, int D, bool NS>
+__device__ __forceinline__ void load_face_in(const KParams &P, int64_t a, int64_t b, int fn, FaceIn<DIM, NS> &in);
+template <int DIM, int N, int D, bool NS>
+__device__ __forceinline__ double face_terms_from(const KParams &P, const double *c, bool a_is_1,
+                                                  const FaceIn<DIM, NS> &in, double coef, double *C);
+
+// Face terms of direction D for one element e (its lane group): slot t <
+// NFN is face node t of the -D face (element a = the -D neighbour), slot
+// NFN + t face node t of the +D face (a = e).  Every slot of a lane is loaded
+// before any is evaluated, so their load latencies overlap.  The inviscid
+// flux comes first; NS then adds the central viscous flux, which for either
+// orientation of the face is C_FACE coef (fa + fb)/2 |n_D| for element a and
+// its negative for b (fixed operator only: the reference-value operator's
+// face fluxes read velocities from the momentum slots).
+template <int DIM, int N, bool NS, int D>
+__device__ __forceinline__ void face_terms_dir(const KParams &P, const double *c, double *acc, int64_t e,
+                                               const int32_t *enb, int gl, bool valid, double coef)
+{
+    using S = Shape<DIM, N>;
+    constexpr int Np = S::Np, NV = S::NV, NFN = S::NFN, L = S::L, ST = S::NS_;
+    constexpr int R = (2 * NFN + L - 1) / L;
+    if (valid) {
+        {
+            FaceIn<DIM, false> in[R];
+#pragma unroll
+            for (int r = 0; r < R; r++) {
+                const int t = gl + r * L;
+                if (t < 2 * NFN) {
+                    const int side = t >= NFN, fn = side ? t - NFN : t;
+                    const int64_t other = enb[2 * D + side];
+                    load_face_in<DIM, N, D, false>(P, side ? e : other, side ? other : e, fn, in[r]);
+                }
+            }
+#pragma unroll
+            for (int r = 0; r < R; r++) {
+                const int t = gl + r * L;
+                if (t < 2 * NFN) {
+                    const int side = t >= NFN, fn = side ? t - NFN : t;
+                    const int64_t other = enb[2 * D + side];
+                    const int64_t a = side ? e : other, b = side ? other : e;
+                    double C[NV];
+                    face_terms_from<DIM, N, D, false>(P, c, a <= b, in[r], coef, C);
+                    const int n = sp<DIM, Np>(line_node<DIM, Np, D>(fn, side ? N : 0));
+#pragma unroll
+                    for (int v = 0; v < NV; v++) {
+                        if (side) acc[v * ST + n] += C[v];
+                        else acc[v * ST + n] -= C[v];
+                    }
+                }
+            }
+        }
+        if (NS) {
+            const int64_t ne = P.ne;
+            double fv[R][DIM + 1];
+#pragma unroll
+            for (int r = 0; r < R; r++) {
+                const int t = gl + r * L;
+                if (t < 2 * NFN) {
+                    const int side = t >= NFN, fn = side ? t - NFN : t;
+                    const int64_t other = enb[2 * D + side];
+                    const int64_t a = side ? e : other, b = side ? other : e;
+                    const double *fa = P.fcol + (((D * 2 + 1) * ne + a) * NFN + fn) * (NV - 1);
+                    const double *fb = P.fcol + (((D * 2 + 0) * ne + b) * NFN + fn) * (NV - 1);
+#pragma unroll
+                    for (int i = 0; i <= DIM; i++) fv[r][i] = __ldg(fa + i) + __ldg(fb + i);
+                }
+            }
+            const double sc = (C_FACE(c) * coef) * (0.5 * C_AREA(c)[D]);
+#pragma unroll
+            for (int r = 0; r < R; r++) {
+                const int t = gl + r * L;
+                if (t < 2 * NFN) {
+                    const int side = t >= NFN, fn = side ? t - NFN : t;
+                    const int n = sp<DIM, Np>(line_node<DIM, Np, D>(fn, side ? N : 0));
+#pragma unroll
+                    for (int i = 0; i <= DIM; i++) {
+                        const double x = sc * fv[r][i];
+                        if (side) acc[(1 + i) * ST + n] += x;
+                        else acc[(1 + i) * ST + n] -= x;
+                    }
+                }
+            }
+        }
+    }
+    __syncwarp();
+}
 
 // One warp tile of the right-hand side element kernel: EPW elements from
 // e_base, one lane group each.  Volume terms (flux differencing, subcell FV
 // blending) into acc, then either the stage output is stored and the face
-// terms are left to the face kernels (FACES = false), or (FACES = true, Euler)
-// every element also adds the face terms of its own face nodes, evaluated
-// with the same element-1 rule and in the same order (x faces, then y [, z])
-// as the face kernels use, and stores the finished stage.
-template <int DIM, int N, bool NS, bool FACES>
+// terms are left to the face kernels (FACES = false), or (FACES = true) every
+// element also adds the face terms of its own face nodes, evaluated with the
+// same element-1 rule and in the same order (x faces, then y [, z]) as the
+// face kernels use, and stores the finished stage.  With NS and FACES the
+// lifting kernel has run first: its viscous volume term (P.vbuf) enters after
+// the stage combine, where the other path's lifting kernel adds it, and the
+// face terms include the central viscous flux of both sides' face columns.
+// Each face is thus evaluated twice, once by each of its elements, on the
+// same inputs in the same order, so both get the same value.
+template <int DIM, int N, bool NS, bool FACES, bool PRELOAD = true>
 __device__ __forceinline__ void rhs_tile(const KParams &P, const double *c, double *pr, int64_t e_base, int grp,
                                          int gl, bool lane_used, unsigned int &flags, double &lam)
 {
@@ -528,7 +621,9 @@ __device__ __forceinline__ void rhs_tile(const KParams &P, const double *c, doub
     const int64_t e = valid ? e0 : 0;
     // the RK base state is first read by the final combine: bring the
     // element's block of each variable into L2 now
-    if (!FACES && valid && P.stage > 0 && gl < NV) prefetch_l2(P.un + (int64_t)gl * P.nnodes + e * NDOF, sizeof(double) * NDOF);
+    if ((!FACES || NS) && valid && P.stage > 0 && gl < NV) prefetch_l2(P.un + (int64_t)gl * P.nnodes + e * NDOF, sizeof(double) * NDOF);
+    if (FACES && NS && valid && gl >= NV && gl < 2 * NV - 1)
+        prefetch_l2(P.vbuf + (int64_t)(gl - NV) * P.nnodes + e * NDOF, sizeof(double) * NDOF);
     if (lane_used) {
         const double ls = stage_nodes<DIM, N>(P, e, valid, gl, pr, scratch, flags);
         if (valid) lam = fmax(lam, ls);
@@ -576,8 +671,15 @@ __device__ __forceinline__ void rhs_tile(const KParams &P, const double *c, doub
         __syncwarp();
         return;
     }
-    // element-centric faces: combine first, then add each direction's face
-    // terms in turn, then store
+    // element-centric faces: combine first (plus the viscous volume term),
+    // then add each direction's face terms in turn, then store
+    const double coef = stage_coef(P);
+    // the face neighbours, requested before the combine's loads
+    int32_t enb[2 * DIM];
+    if (PRELOAD) {
+#pragma unroll
+        for (int k = 0; k < 2 * DIM; k++) enb[k] = valid ? __ldg(P.nbr + e * 2 * DIM + k) : 0;
+    }
     if (valid) {
 #pragma unroll
         for (int k = 0; k < S::NPL; k++) {
@@ -586,35 +688,44 @@ __device__ __forceinline__ void rhs_tile(const KParams &P, const double *c, doub
 #pragma unroll
                 for (int v = 0; v < NV; v++) {
                     const int64_t gi = (int64_t)v * P.nnodes + e * NDOF + n;
-                    acc[v * ST + sp<DIM, Np>(n)] = stage_combine(P, gi, acc[v * ST + sp<DIM, Np>(n)]);
+                    double x = stage_combine(P, gi, acc[v * ST + sp<DIM, Np>(n)]);
+                    if (NS && v > 0) x = x + coef * __ldg(P.vbuf + gi - P.nnodes);
+                    acc[v * ST + sp<DIM, Np>(n)] = x;
                 }
             }
         }
     }
     __syncwarp();
-    const double coef = stage_coef(P);
+    if (PRELOAD) {
+        face_terms_dir<DIM, N, NS, 0>(P, c, acc, e, enb, gl, valid, coef);
+        face_terms_dir<DIM, N, NS, 1>(P, c, acc, e, enb, gl, valid, coef);
+        if (DIM == 3) face_terms_dir<DIM, N, NS, (DIM == 3 ? 2 : 0)>(P, c, acc, e, enb, gl, valid, coef);
+    } else {
+        // one face node at a time (Euler): the batched sweep's register
+        // variants are tuned for this form
 #pragma unroll 1
-    for (int d = 0; d < DIM; d++) {
-        if (valid) {
-            for (int t = gl; t < 2 * NFN; t += L) {
-                const int side = t >= NFN, fn = side ? t - NFN : t;
-                // side 1: this element's +d face (it is element a); side 0:
-                // its -d face, whose element a is the -d neighbour
-                const int64_t other = __ldg(P.nbr + e * 2 * DIM + 2 * d + side);
-                const int64_t a = side ? e : other, b = side ? other : e;
-                double C[NV];
-                if (d == 0) face_node_terms<DIM, N, 0, false>(P, c, a, b, fn, coef, C);
-                else if (d == 1) face_node_terms<DIM, N, 1, false>(P, c, a, b, fn, coef, C);
-                else face_node_terms<DIM, N, (DIM == 3 ? 2 : 0), false>(P, c, a, b, fn, coef, C);
-                const int n = sp<DIM, Np>(line_node_rt<DIM, Np>(d, fn, side ? N : 0));
+        for (int d = 0; d < DIM; d++) {
+            if (valid) {
+                for (int t = gl; t < 2 * NFN; t += L) {
+                    const int side = t >= NFN, fn = side ? t - NFN : t;
+                    // side 1: this element's +d face (it is element a); side
+                    // 0: its -d face, whose element a is the -d neighbour
+                    const int64_t other = __ldg(P.nbr + e * 2 * DIM + 2 * d + side);
+                    const int64_t a = side ? e : other, b = side ? other : e;
+                    double C[NV];
+                    if (d == 0) face_node_terms<DIM, N, 0, false>(P, c, a, b, fn, coef, C);
+                    else if (d == 1) face_node_terms<DIM, N, 1, false>(P, c, a, b, fn, coef, C);
+                    else face_node_terms<DIM, N, (DIM == 3 ? 2 : 0), false>(P, c, a, b, fn, coef, C);
+                    const int n = sp<DIM, Np>(line_node_rt<DIM, Np>(d, fn, side ? N : 0));
 #pragma unroll
-                for (int v = 0; v < NV; v++) {
-                    if (side) acc[v * ST + n] += C[v];
-                    else acc[v * ST + n] -= C[v];
+                    for (int v = 0; v < NV; v++) {
+                        if (side) acc[v * ST + n] += C[v];
+                        else acc[v * ST + n] -= C[v];
+                    }
                 }
             }
+            __syncwarp();
         }
-        __syncwarp();
     }
     if (valid) {
 #pragma unroll
@@ -637,7 +748,7 @@ template <int DIM, int N> struct RhsOccupancy {
     static constexpr int min_blocks = (DIM == 3 && N == 3) ? 4 : 1;
 };
 
-template <int DIM, int N, bool NS>
+template <int DIM, int N, bool NS, bool FACES = false>
 __global__ void __launch_bounds__(128, RhsOccupancy<DIM, N>::min_blocks) rhs_kernel(const KParams P)
 {
     using S = Shape<DIM, N>;
@@ -655,7 +766,7 @@ __global__ void __launch_bounds__(128, RhsOccupancy<DIM, N>::min_blocks) rhs_ker
     unsigned int flags = 0;
     double lam = 0.0;
     for (int64_t wt = (int64_t)blockIdx.x * wpb + warp; wt < P.nwt; wt += wstride)
-        rhs_tile<DIM, N, NS, false>(P, c, pr, wt * EPW, grp, gl, lane_used, flags, lam);
+        rhs_tile<DIM, N, NS, FACES>(P, c, pr, wt * EPW, grp, gl, lane_used, flags, lam);
     lam = group_max<32>(lam);
     if (lane == 0) atomic_max_pos(P.lam_bits, lam);
     flags = __reduce_or_sync(0xffffffffu, flags);
@@ -696,28 +807,39 @@ __device__ __forceinline__ Prim<DIM> velocity_slot_prim(const Prim<DIM> &q, doub
 // the momentum slots, as the reference does (its ComputeViscousFlux divides
 // the face states' momenta in place before ComputeFaceFlux reads them,
 // BasicOperations.cpp:33-34, DGSEMIntegrator.cpp:467-481).
+// Inputs of one face node: both traces and (NS) both normal viscous columns.
+template <int DIM, bool NS> struct FaceIn {
+    double sa[DIM + 2], sb[DIM + 2];
+    double fa[NS ? DIM + 1 : 1], fb[NS ? DIM + 1 : 1];
+};
+
 template <int DIM, int N, int D, bool NS>
-__device__ __forceinline__ double face_node_terms(const KParams &P, const double *c, int64_t a, int64_t b, int fn,
-                                                  double coef, double *C)
+__device__ __forceinline__ void load_face_in(const KParams &P, int64_t a, int64_t b, int fn, FaceIn<DIM, NS> &in)
 {
     using S = Shape<DIM, N>;
     constexpr int Np = S::Np, NDOF = S::NDOF, NV = S::NV, NFN = S::NFN;
     const int64_t nn = P.nnodes;
     const int na = line_node<DIM, Np, D>(fn, N), nb = line_node<DIM, Np, D>(fn, 0);
-    double sa[NV], sb[NV];
 #pragma unroll
     for (int v = 0; v < NV; v++) {
-        sa[v] = __ldg(P.u + v * nn + a * NDOF + na);
-        sb[v] = __ldg(P.u + v * nn + b * NDOF + nb);
+        in.sa[v] = __ldg(P.u + v * nn + a * NDOF + na);
+        in.sb[v] = __ldg(P.u + v * nn + b * NDOF + nb);
     }
-    double fa[DIM + 1], fb[DIM + 1];
     if (NS) {
 #pragma unroll
         for (int i = 0; i <= DIM; i++) {
-            fa[i] = __ldg(P.fcol + (((D * 2 + 1) * P.ne + a) * NFN + fn) * (NV - 1) + i);
-            fb[i] = __ldg(P.fcol + (((D * 2 + 0) * P.ne + b) * NFN + fn) * (NV - 1) + i);
+            in.fa[i] = __ldg(P.fcol + (((D * 2 + 1) * P.ne + a) * NFN + fn) * (NV - 1) + i);
+            in.fb[i] = __ldg(P.fcol + (((D * 2 + 0) * P.ne + b) * NFN + fn) * (NV - 1) + i);
         }
     }
+}
+
+template <int DIM, int N, int D, bool NS>
+__device__ __forceinline__ double face_terms_from(const KParams &P, const double *c, bool a_is_1,
+                                                  const FaceIn<DIM, NS> &in, double coef, double *C)
+{
+    constexpr int NV = DIM + 2, Np = N + 1;  // Np: constant layout
+    const double *sa = in.sa, *sb = in.sb;
     Prim<DIM> qa = make_prim<DIM>(sa, P.gamma, P.gm1), qb = make_prim<DIM>(sb, P.gamma, P.gm1);
     double ma[DIM], mb[DIM];
     double lam = 0.0;
@@ -733,7 +855,6 @@ __device__ __forceinline__ double face_node_terms(const KParams &P, const double
             mb[d] = sb[1 + d];
         }
     }
-    const bool a_is_1 = a <= b;
     const double nrm = a_is_1 ? C_AREA(c)[D] : -C_AREA(c)[D];
     double F[NV];
     if (a_is_1) face_flux<DIM, D>(qa, qb, ma, mb, nrm, P.gm1inv, compat, P.diss_scale, F);
@@ -744,12 +865,21 @@ __device__ __forceinline__ double face_node_terms(const KParams &P, const double
     for (int i = 0; i <= DIM; i++) {
         double du = a_is_1 ? -F[1 + i] : F[1 + i];
         if (NS) {
-            const double fvn = ((fa[i] + fb[i]) * 0.5) * nrm;
+            const double fvn = ((in.fa[i] + in.fb[i]) * 0.5) * nrm;
             du = a_is_1 ? du + fvn : du - fvn;
         }
         C[1 + i] = sc * du;
     }
     return lam;
+}
+
+template <int DIM, int N, int D, bool NS>
+__device__ __forceinline__ double face_node_terms(const KParams &P, const double *c, int64_t a, int64_t b, int fn,
+                                                  double coef, double *C)
+{
+    FaceIn<DIM, NS> in;
+    load_face_in<DIM, N, D, NS>(P, a, b, fn, in);
+    return face_terms_from<DIM, N, D, NS>(P, c, a <= b, in, coef, C);
 }
 
 template <int DIM, int N, int D, bool NS>
@@ -920,10 +1050,11 @@ __device__ __forceinline__ void divergence_lines(const double *fvs, double *dv, 
 // jumps from lbuf, conversion to primitive gradients, then the viscous fluxes:
 // contravariant volume fluxes at every node (with the state of the element's
 // last node in compat mode, as the reference's member id1 gives,
-// DGSEMIntegrator.cpp:620, :770), their divergence (the viscous volume term,
-// added to the output the volume kernel wrote, times the stage factor) and the
-// normal column at every face node (with the node's own state,
-// DGSEMIntegrator.cpp:467-477, written to P.fcol).
+// DGSEMIntegrator.cpp:620, :770), their divergence (the viscous volume term:
+// added to the output the volume kernel wrote, times the stage factor, or
+// stored to P.vbuf when the volume kernel with element-side faces runs after
+// this one) and the normal column at every face node (with the node's own
+// state, DGSEMIntegrator.cpp:467-477, written to P.fcol).
 template <int DIM, int N>
 __global__ void __launch_bounds__(128) lift_kernel(const KParams P)
 {
@@ -1073,14 +1204,15 @@ __global__ void __launch_bounds__(128) lift_kernel(const KParams P)
         }
         __syncwarp();
         // the output values the divergence is added to, loaded before the
-        // divergence line tasks
+        // divergence line tasks (none when it goes to vbuf)
+        const bool add_out = valid && P.out && !P.vbuf;
         double oprev[S::NPL][NV - 1];
 #pragma unroll
         for (int k = 0; k < S::NPL; k++) {
             const int n = gl + k * L;
 #pragma unroll
             for (int i = 0; i < NV - 1; i++)
-                oprev[k][i] = (valid && P.out && n < NDOF) ? P.out[(int64_t)(1 + i) * nn + e * NDOF + n] : 0.0;
+                oprev[k][i] = (add_out && n < NDOF) ? P.out[(int64_t)(1 + i) * nn + e * NDOF + n] : 0.0;
         }
         if (lane_used) {
             divergence_lines<DIM, N, 0, true>(g, wv, c, gl);
@@ -1091,7 +1223,17 @@ __global__ void __launch_bounds__(128) lift_kernel(const KParams P)
             __syncwarp();
             if (DIM == 3) __syncwarp();
         }
-        if (valid && P.out) {
+        if (valid && P.vbuf) {
+            // element-side faces: the right-hand side kernel adds it
+#pragma unroll
+            for (int k = 0; k < S::NPL; k++) {
+                const int n = gl + k * L;
+                if (n < NDOF) {
+#pragma unroll
+                    for (int i = 0; i < NV - 1; i++) P.vbuf[(int64_t)i * nn + e * NDOF + n] = wv[i * ST + sp<DIM, Np>(n)];
+                }
+            }
+        } else if (add_out) {
             const double coef = stage_coef(P);
 #pragma unroll
             for (int k = 0; k < S::NPL; k++) {

@@ -101,11 +101,12 @@ def test_host_path_matches_device_path(cuda_device):
     assert np.array_equal(a, b)
 
 
+@pytest.mark.parametrize("compat", [1, 0])
 @pytest.mark.parametrize("kind,dim,order,par", [("vortex", 2, 3, 0), ("rough3d", 3, 3, 1), ("kh", 2, 4, 0)])
-def test_rk_stages_match_oracle(kind, dim, order, par, cuda_device):
+def test_rk_stages_match_oracle(kind, dim, order, par, compat, cuda_device):
     import torch
     mesh, u = make_case(kind, dim, order)
-    kw = dict(parabolic=par, mu=0.01 if par else 0.0, Pr=0.71, compat=1)
+    kw = dict(parabolic=par, mu=0.01 if par else 0.0, Pr=0.71, compat=compat)
     op = pb.DGSEMOperator(mesh, **kw)
     orc = oracle.Oracle(mesh, **kw)
     orc.rhs(u)
@@ -157,12 +158,13 @@ def test_error_word_flags_negative_density(cuda_device):
     assert op.check() == 0  # the word was cleared
 
 
+@pytest.mark.parametrize("compat", [1, 0])
 @pytest.mark.parametrize("kind,dim,order,par", [("vortex", 2, 3, 0), ("tgv", 3, 2, 1)])
-def test_graph_replayed_steps_equal_plain_steps(kind, dim, order, par, cuda_device):
+def test_graph_replayed_steps_equal_plain_steps(kind, dim, order, par, compat, cuda_device):
     """pdg_rk3_steps (one captured step, replayed) gives pdg_rk3_step's values."""
     import torch
     mesh, u = make_case(kind, dim, order)
-    kw = dict(parabolic=par, mu=0.01 if par else 0.0, Pr=0.71)
+    kw = dict(parabolic=par, mu=0.01 if par else 0.0, Pr=0.71, compat=compat)
     op = pb.DGSEMOperator(mesh, **kw)
     a = torch.from_numpy(u).to(cuda_device)
     b = a.clone()
@@ -174,8 +176,39 @@ def test_graph_replayed_steps_equal_plain_steps(kind, dim, order, par, cuda_devi
     op.rk3_step(b, dt, nsteps=4, graph=True)
     per_step = (op.launch_count() - l0) / 4
     assert torch.equal(a, b)
-    assert per_step == (6 if par else 1 + dim) * 3
+    if compat:   # (face jumps,) volume, (lifting,) face passes per stage
+        assert per_step == (6 if par else 1 + dim) * 3
+    else:        # (face jumps, lifting,) volume with faces per stage
+        assert per_step == (3 if par else 1) * 3
     op.rk3_step(b, dt, nsteps=2, graph=True)   # replay without capture
     op.rk3_step(a, dt, nsteps=2)
     assert torch.equal(a, b)
     assert op.check() == 0
+
+
+@pytest.mark.parametrize("kind,dim,order,par", [("rough2d", 2, 3, 0), ("rough3d", 3, 3, 1), ("rough2dns", 2, 4, 1),
+                                                ("rough3d", 3, 2, 0)])
+def test_element_side_faces_equal_face_kernels(kind, dim, order, par, cuda_device, monkeypatch):
+    """The fixed operator's volume kernel with both sides' face terms gives the
+    separate face kernels' outputs (PDG_ELEMENT_FACES=0 selects those)."""
+    import torch
+    mesh, u = make_case(kind, dim, order)
+    kw = dict(parabolic=par, mu=0.01 if par else 0.0, Pr=0.71, compat=0)
+    op = pb.DGSEMOperator(mesh, **kw)
+    monkeypatch.setenv("PDG_ELEMENT_FACES", "0")
+    op_sep = pb.DGSEMOperator(mesh, **kw)
+    monkeypatch.delenv("PDG_ELEMENT_FACES")
+    un = dev(u, cuda_device)
+    us = dev(rough(u, mesh, 9, 0.01, 0.001), cuda_device)
+    for stage in (-1, 0, 1, 2):
+        a = torch.empty_like(un)
+        b = torch.empty_like(un)
+        if stage < 0:
+            op.Mult(us, a)
+            op_sep.Mult(us, b)
+        else:
+            op.rk_stage(stage, 1e-3, un, us, a)
+            op_sep.rk_stage(stage, 1e-3, un, us, b)
+        torch.cuda.synchronize()
+        assert rel_maxnorm(a.cpu().numpy(), b.cpu().numpy()) < 1e-14
+    assert op.check() == 0 and op_sep.check() == 0
