@@ -17,7 +17,9 @@
  * the same layout and hold primitive-variable gradients (rho, u, v[, w], p).
  *
  * Mesh: affine, axis-aligned quads/hexes of extent h[0..dim-1] with a face
- * neighbour table nbr[e*2*dim + f], f = (-x, +x, -y, +y, -z, +z).  Element
+ * neighbour table nbr[e*2*dim + f], f = (-x, +x, -y, +y, -z, +z); an entry
+ * -1 - b marks a boundary face with boundary condition b (pdg_set_boundary,
+ * Euler only).  Element
  * numbering is free; the face orientation rule is: the face between element a's
  * +d face and element b's -d face has element 1 = a when a <= b (normal +d),
  * else element 1 = b (normal -d) — MFEM gives element 1 to the lower-numbered
@@ -99,6 +101,24 @@ void pdg_default_params(pdg_params *p);
  * fields, error word) on the current device. */
 int pdg_create(const pdg_mesh *mesh, const pdg_params *params, pdg_ctx **out);
 int pdg_destroy(pdg_ctx *ctx);
+
+/* Boundary conditions (the integrators of src/Integrators/BoundaryConditions/, attached to
+ * boundary attributes by DGSEMOperator::AddBdrFaceIntegrator,
+ * src/Operators/DGSEMOperator.cpp:593 and src/Simulation/Simulation.cpp:
+ * 490-798).  A neighbour entry -1 - b (0 <= b < PDG_MAX_BOUNDARIES) marks a
+ * boundary face with condition b; every condition the mesh uses must be set
+ * before the first evaluation (else PDG_ERR_ARG).  Euler only: pdg_create
+ * returns PDG_ERR_UNSUPPORTED for a Navier-Stokes mesh with boundary faces,
+ * and pdg_rhs_vjp for any mesh with them.  `state` (conserved, dim + 2
+ * values, rho > 0 and p > 0) is read for the two types with a prescribed
+ * state and may be NULL otherwise. */
+#define PDG_MAX_BOUNDARIES 16
+#define PDG_BC_SUPERSONIC_INFLOW  1  /* SupersonicInflowBdrFaceIntegrator: prescribed outer state */
+#define PDG_BC_SUPERSONIC_OUTFLOW 2  /* SupersonicOutflowBdrFaceIntegrator: outer state = interior */
+#define PDG_BC_SPECIFIED_STATE    3  /* SpecifiedStateBdrFaceIntegrator: prescribed outer state */
+#define PDG_BC_SLIP_WALL          4  /* SlipWallBdrFaceIntegrator: pressure flux from the wall Riemann problem */
+#define PDG_BC_SYMMETRY           5  /* SymmetryBdrFaceIntegrator: normal momentum mirrored */
+int pdg_set_boundary(pdg_ctx *ctx, int index, int type, const double *state);
 
 /* TimeDependentOperator::Height (DGSEMOperator.cpp:18): number of vdofs. */
 int64_t pdg_size(const pdg_ctx *ctx);

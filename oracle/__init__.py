@@ -61,6 +61,7 @@ def lib():
         L.orc_create.restype = C.c_void_p
         L.orc_create.argtypes = [C.POINTER(PdgMesh), C.POINTER(PdgParams)]
         L.orc_destroy.argtypes = [C.c_void_p]
+        L.orc_set_boundary.argtypes = [C.c_void_p, C.c_int, C.c_int, _dp]
         L.orc_rhs.argtypes = [C.c_void_p, _dp, _dp]
         L.orc_rk3_step.argtypes = [C.c_void_p, C.c_double, _dp]
         L.orc_rk_stage.argtypes = [C.c_void_p, C.c_int, C.c_double, _dp, _dp, _dp]
@@ -97,6 +98,12 @@ class Oracle:
         self.h = lib().orc_create(C.byref(self._m), C.byref(self.params))
         if not self.h:
             raise ValueError("orc_create rejected the mesh/params")
+        for b, (typ, state) in (getattr(mesh, "boundaries", None) or {}).items():
+            self.set_boundary(b, typ, state)
+
+    def set_boundary(self, index: int, typ: int, state=None):
+        st = None if state is None else np.ascontiguousarray(state, dtype=np.float64)
+        lib().orc_set_boundary(self.h, int(index), int(typ), None if st is None else _ptr(st))
 
     def __del__(self):
         try:
@@ -160,6 +167,7 @@ def ref_lib(parabolic: bool):
         L.ref_create.argtypes = [C.c_int, C.c_int, C.c_int, _dp, _ip, C.c_double, C.c_double,
                                  C.c_double, C.c_double, C.c_double]
         L.ref_destroy.argtypes = [C.c_void_p]
+        L.ref_set_boundary.argtypes = [C.c_void_p, C.c_int, C.c_int, _dp]
         L.ref_rhs.restype = C.c_double
         L.ref_rhs.argtypes = [C.c_void_p, _dp, _dp]
         L.ref_get_blending.argtypes = [C.c_void_p, _dp, _dp]
@@ -188,6 +196,10 @@ class Reference:
         self._h = h
         self.h = self.L.ref_create(mesh.dim, mesh.order, mesh.num_elements, _ptr(h),
                                    self._nbr.ctypes.data_as(_ip), gamma, Pr, mu, alpha_max, alpha_min)
+        for b, (typ, state) in (getattr(mesh, "boundaries", None) or {}).items():
+            st = None if state is None else np.ascontiguousarray(state, dtype=np.float64)
+            if self.L.ref_set_boundary(self.h, int(b), int(typ), None if st is None else _ptr(st)):
+                raise ValueError(f"boundary condition {b}: type {typ} rejected")
 
     def __del__(self):
         if getattr(self, "h", None):

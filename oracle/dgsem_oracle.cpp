@@ -397,6 +397,7 @@ struct Ctx {
     double last_rhs_speed;              // max of the last RHS
     std::vector<double> k1, y1, z1;     // RK scratch
     int64_t filtered_elements;
+    double bc[16][8] = {};              // boundary conditions: type, prescribed state
 };
 
 static inline int64_t idx(const Ctx &c, int v, int64_t e, int n)
@@ -777,6 +778,8 @@ static inline int face_node(const Ctx &c, int d, int side, int t)
     return (l * Np + b) * Np + a;
 }
 
+static double bdr_face_vector(const Ctx &c, const double *u, int64_t e, int d, int side, int b, double *out);
+
 // AssembleFaceVector, Euler (DGSEMIntegrator.cpp:151-222) and NS
 // (:435-494 3D, :496-549 2D) for the face between element a's +d face and its
 // neighbour b's -d face.  Writes contributions for both sides into buf:
@@ -786,6 +789,7 @@ static double face_vector(const Ctx &c, const double *u, const double *gr, int64
 {
     const int nv = c.nv, dim = c.dim, nfn = c.ndof / c.Np;
     const int64_t b = c.nbr[a * 2 * dim + 2 * d + 1];
+    if (b < 0) return bdr_face_vector(c, u, a, d, 1, (int)(-1 - b), buf);  // a's side only
     const bool a_is_1 = a <= b;
     const int64_t e1 = a_is_1 ? a : b, e2 = a_is_1 ? b : a;
     const int side1 = a_is_1 ? 1 : 0, side2 = a_is_1 ? 0 : 1;
@@ -845,6 +849,108 @@ static double face_vector(const Ctx &c, const double *u, const double *gr, int64
             ba[t * nv + v] = scale * dU1[v];
             bb[t * nv + v] = scale * dU2[v];
         }
+    }
+    return lam;
+}
+
+// ---------------------------------------------------------------------------
+// Boundary faces (src/Integrators/BoundaryConditions/), Euler.
+// ---------------------------------------------------------------------------
+// MFEM-style helpers as BasicOperations restates them: Normalize
+// (BasicOperations.hpp:39-42), Normal and Cross (BasicOperations.cpp:211-235),
+// RotateState (:238-258).
+static void unit_normal(int dim, const double *nor, double *un)
+{
+    double nn = 0.0;
+    for (int d = 0; d < dim; d++) nn += nor[d] * nor[d];
+    const double inv = 1.0 / std::sqrt(nn);
+    for (int d = 0; d < dim; d++) un[d] = nor[d] * inv;
+}
+static void rotate_state(int dim, double *state, const double *n)
+{
+    double t1[3] = {0, 0, 0}, t2[3] = {0, 0, 0};
+    if (dim == 2) {
+        t1[0] = -n[1];
+        t1[1] = n[0];
+    } else {
+        const bool gen = std::abs(n[0]) > 1e-10;
+        const double q = gen ? n[1] / n[0] : 0.0;
+        t1[0] = gen ? -q / std::sqrt(1.0 + std::pow(q, 2)) : -1.0;
+        t1[1] = gen ? 1.0 / std::sqrt(1.0 + std::pow(q, 2)) : 0.0;
+        t1[2] = 0.0;
+        t2[0] = n[1] * t1[2] - n[2] * t1[1];
+        t2[1] = n[2] * t1[0] - n[0] * t1[2];
+        t2[2] = n[0] * t1[1] - n[1] * t1[0];
+    }
+    double *m = state + 1;
+    double ru = 0.0, rv = 0.0, rw = 0.0;
+    for (int d = 0; d < dim; d++) { ru += m[d] * n[d]; rv += m[d] * t1[d]; }
+    if (dim == 3) {
+        for (int d = 0; d < 3; d++) rw += m[d] * t2[d];
+        m[2] = rw;
+    }
+    m[0] = ru;
+    m[1] = rv;
+}
+
+// Normal flux of boundary condition b for interior state s1 and outward
+// normal nor (ComputeBdrFaceInviscidFlux); returns the reported wave speed.
+static double bdr_flux(const Ctx &c, int b, const double *s1, const double *nor, double *flux)
+{
+    const int dim = c.dim, nv = c.nv;
+    const double gamma = c.p.gamma, gammaM1 = gamma - 1.0, gammaM1Inverse = 1.0 / gammaM1;
+    const int type = (int)c.bc[b][0];
+    double s2[5], un[3];
+    for (int v = 0; v < nv; v++) s2[v] = s1[v];
+    if (type == 4) {
+        // SlipWallBdrFaceIntegrator::ComputeBdrFaceInviscidFlux (:15-58)
+        const double gammaP1 = 1.0 + gamma, gammaP1Inverse = 1.0 / gammaP1;
+        unit_normal(dim, nor, un);
+        rotate_state(dim, s2, un);
+        const double rho = s2[0];
+        double V[3], vv = 0.0;
+        for (int d = 0; d < dim; d++) { V[d] = s2[1 + d] / rho; vv += V[d] * V[d]; }
+        const double p = gammaM1 * (s2[nv - 1] - 0.5 * rho * vv);
+        const double an = sound_speed(p, rho, gamma);
+        const double u = V[0];
+        double p_star;
+        if (u > 0.0)
+            p_star = p + 0.25 * u * gammaP1 * rho *
+                             (u + std::sqrt(std::pow(u, 2) + 8.0 * gammaP1Inverse / rho * p * (gammaM1 * gammaP1Inverse + 1.0)));
+        else
+            p_star = p * std::pow(std::max(1.0 + 0.5 * gammaM1 * u / an, 0.0001), 2.0 * gamma * gammaM1Inverse);
+        for (int v = 0; v < nv; v++) flux[v] = 0.0;
+        for (int d = 0; d < dim; d++) flux[1 + d] = p_star * nor[d];
+        return std::sqrt(vv) + an;
+    }
+    if (type == 1 || type == 3) {
+        // SupersonicInflow / SpecifiedState: the prescribed state (:22-35, :21-35)
+        for (int v = 0; v < nv; v++) s2[v] = c.bc[b][1 + v];
+    } else if (type == 5) {
+        // SymmetryBdrFaceIntegrator (:12-37): mirrored normal momentum
+        unit_normal(dim, nor, un);
+        double mn = 0.0;
+        for (int d = 0; d < dim; d++) mn += s2[1 + d] * un[d];
+        for (int d = 0; d < dim; d++) s2[1 + d] += -2.0 * mn * un[d];
+    }  // type 2, SupersonicOutflow (:10-13): the interior state
+    return face_flux(dim, gamma, c.p.compat, c.p.face_dissipation, s1, s2, nor, flux);
+}
+
+// BdrFaceIntegrator::AssembleFaceVector (BdrFaceIntegrator.cpp:64-130): the
+// boundary face of element e on its +d (side 1) or -d (side 0) side, with
+// the outward normal; out[t][v] = -flux / (w0 J1) at face node t.
+static double bdr_face_vector(const Ctx &c, const double *u, int64_t e, int d, int side, int b, double *out)
+{
+    const int nv = c.nv, nfn = c.ndof / c.Np;
+    double nor[3] = {0, 0, 0};
+    nor[d] = side ? c.area[d] : -c.area[d];
+    const double scale = 1.0 / (c.w[0] * c.J);
+    double lam = -1.0, s1[5], flux[5];
+    for (int t = 0; t < nfn; t++) {
+        const int n = face_node(c, d, side, t);
+        for (int v = 0; v < nv; v++) s1[v] = u[idx(c, v, e, n)];
+        lam = std::max(lam, bdr_flux(c, b, s1, nor, flux));
+        for (int v = 0; v < nv; v++) out[t * nv + v] = scale * -flux[v];
     }
     return lam;
 }
@@ -965,9 +1071,17 @@ static void rhs(Ctx &c, const double *u, double *dudt)
             for (int v = 0; v < nv; v++) dudt[idx(c, v, e, n)] = 0.0 + el_d[n * nv + v];
         for (int d = 0; d < dim; d++) {
             // -d face: stored at (nbr_minus, d); this element is its "b" side.
+            // A boundary -d face is evaluated here.
             int64_t em = c.nbr[e * 2 * dim + 2 * d];
-            const double *bm = &c.facebuf[((size_t)em * dim + d) * fstride];
-            const double *mine = bm + (size_t)nfn * nv;
+            std::vector<double> bface;
+            const double *mine;
+            if (em < 0) {
+                bface.resize((size_t)nfn * nv);
+                lam = std::max(lam, bdr_face_vector(c, u, e, d, 0, (int)(-1 - em), bface.data()));
+                mine = bface.data();
+            } else {
+                mine = &c.facebuf[((size_t)em * dim + d) * fstride] + (size_t)nfn * nv;
+            }
             for (int t = 0; t < nfn; t++) {
                 int n = face_node(c, d, 0, t);
                 for (int v = 0; v < nv; v++) dudt[idx(c, v, e, n)] += mine[t * nv + v];
@@ -1010,7 +1124,8 @@ static void filter_bounds(Ctx &c, const double *u)
 #pragma omp parallel for schedule(static)
     for (int64_t e = 0; e < c.ne; e++) {
         double mn = own[e];
-        for (int f = 0; f < 2 * dim; f++) mn = std::min(mn, own[c.nbr[e * 2 * dim + f]]);
+        for (int f = 0; f < 2 * dim; f++)
+            if (c.nbr[e * 2 * dim + f] >= 0) mn = std::min(mn, own[c.nbr[e * 2 * dim + f]]);
         c.emin[e] = mn;
     }
 }
@@ -1138,6 +1253,8 @@ void *orc_create(const pdg_mesh *m, const pdg_params *p)
     c->size = c->nnodes * c->nv;
     for (int d = 0; d < 3; d++) c->h[d] = d < c->dim ? m->h[d] : 1.0;
     c->nbr.assign(m->nbr, m->nbr + (size_t)c->ne * 2 * c->dim);
+    for (int32_t nb : c->nbr)  // boundary faces: Euler only, conditions 0..15
+        if (nb >= c->ne || nb < -16 || (nb < 0 && p->parabolic)) { delete c; return nullptr; }
     orc::gll(c->Np, c->x, c->w);
     orc::build_derivative_matrices(*c);
     if (c->dim == 2) {
@@ -1176,6 +1293,14 @@ void *orc_create(const pdg_mesh *m, const pdg_params *p)
 }
 
 void orc_destroy(void *h) { delete (Ctx *)h; }
+
+void orc_set_boundary(void *h, int index, int type, const double *state)
+{
+    Ctx &c = *(Ctx *)h;
+    if (index < 0 || index >= 16) return;
+    c.bc[index][0] = type;
+    for (int v = 0; v < c.nv; v++) c.bc[index][1 + v] = state ? state[v] : 0.0;
+}
 
 void orc_rhs(void *h, const double *u, double *dudt) { orc::rhs(*(Ctx *)h, u, dudt); }
 

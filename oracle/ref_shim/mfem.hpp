@@ -23,6 +23,7 @@
 #include <cmath>
 #include <cstdlib>
 #include <cstring>
+#include <functional>
 #include <iostream>
 #include <limits>
 #include <memory>
@@ -40,11 +41,17 @@
         std::abort();                                                                              \
     } while (0);
 #define MFEM_HOST_DEVICE
+#define MFEM_WARNING(msg) do { } while (0)
 
 namespace mfem {
 
 typedef double real_t;
 inline real_t infinity() { return std::numeric_limits<real_t>::infinity(); }
+inline void mfem_error(const char *msg)
+{
+    std::cerr << "stand-in MFEM error: " << msg << "\n";
+    std::abort();
+}
 
 template <class T> class Array {
     std::vector<T> v_;
@@ -182,6 +189,11 @@ public:
     void Neg()
     {
         for (int i = 0; i < size_; i++) data_[i] = -data_[i];
+    }
+    // this += a * v
+    void Add(real_t a, const Vector &v)
+    {
+        for (int i = 0; i < size_; i++) data_[i] += a * v.data_[i];
     }
     void Reciprocal()
     {
@@ -650,7 +662,7 @@ public:
 // elements; the face Jacobian is oriented so CalcOrtho points out of element 1.
 class FaceElementTransformations {
 public:
-    int Elem1No = 0, Elem2No = 0;
+    int Elem1No = 0, Elem2No = 0, ElementNo = 0;
     int dim = 2, dir = 0;
     int side1 = 1;  // 1: element 1's +dir face, 0: its -dir face
     ElementTransformation T1, T2;
@@ -679,6 +691,27 @@ public:
     const IntegrationPoint &GetElement1IntPoint() { return ip1; }
     const IntegrationPoint &GetElement2IntPoint() { return ip2; }
     const DenseMatrix &Jacobian() { return FJ; }
+    // physical point of the face point set by SetAllIntPoints
+    void Transform(const IntegrationPoint &, Vector &phys) { T1.Transform(ip1, phys); }
+};
+
+// Vector-valued function of the physical point (boundary states).
+class VectorFunctionCoefficient {
+public:
+    VectorFunctionCoefficient(int vd, std::function<void(const Vector &, Vector &)> f) : vdim(vd), F(std::move(f)) {}
+    void SetTime(real_t tt) { t = tt; }
+    template <class Tr> void Eval(Vector &V, Tr &T, const IntegrationPoint &ip)
+    {
+        Vector x;
+        T.Transform(ip, x);
+        V.SetSize(vdim);
+        F(x, V);
+    }
+
+private:
+    int vdim;
+    std::function<void(const Vector &, Vector &)> F;
+    real_t t = 0.0;
 };
 
 class FiniteElement {

@@ -16,6 +16,11 @@
 
 #include "BasicOperations.hpp"
 #include "ChandrashekarFlux.hpp"
+#include "SlipWallBdrFaceIntegrator.hpp"
+#include "SpecifiedStateBdrFaceIntegrator.hpp"
+#include "SupersonicInflowBdrFaceIntegrator.hpp"
+#include "SupersonicOutflowBdrFaceIntegrator.hpp"
+#include "SymmetryBdrFaceIntegrator.hpp"
 #include "DGSEMIntegrator.hpp"
 #include "ModalBasis.hpp"
 #include "NavierStokesFlux.hpp"
@@ -144,6 +149,12 @@ struct RefCtx {
     double h[3];
     struct Face { int e1, e2, dir, side1; };
     std::vector<Face> faces;
+    // boundary faces (negative neighbour entries -1 - b) and the reference's
+    // boundary integrator of each condition b
+    struct BFace { int e, dir, side, b; };
+    std::vector<BFace> bfaces;
+    std::unique_ptr<BdrFaceIntegrator> bfi[16];
+    double time = 0.0;
 };
 
 // Face between element a's +d face and its neighbour b's -d face; element 1
@@ -152,7 +163,12 @@ void build_faces(RefCtx &c)
 {
     for (int e = 0; e < c.ne; e++)
         for (int d = 0; d < c.dim; d++) {
+            for (int side = 0; side < 2; side++) {
+                const int nb = c.nbr[e * 2 * c.dim + 2 * d + side];
+                if (nb < 0) c.bfaces.push_back({e, d, side, -1 - nb});
+            }
             int b = c.nbr[e * 2 * c.dim + 2 * d + 1];
+            if (b < 0) continue;
             RefCtx::Face f;
             f.dir = d;
             if (e <= b) { f.e1 = e; f.e2 = b; f.side1 = 1; }
@@ -187,6 +203,16 @@ void setup_face(RefCtx &c, const RefCtx::Face &f, FaceElementTransformations &T)
         T.FJ(a, 0) = h[a];
         T.FJ(b, 1) = h[b];
     }
+}
+
+// Boundary face of element e on its +dir (side 1) or -dir (side 0) side: the
+// element is element 1 and the face Jacobian points out of it.
+void setup_bdr_face(RefCtx &c, const RefCtx::BFace &f, FaceElementTransformations &T)
+{
+    RefCtx::Face g{f.e, f.e, f.dir, f.side};
+    setup_face(c, g, T);
+    T.Elem2No = -1;
+    T.ElementNo = f.e;
 }
 
 // DGSEMOperator::ComputeBlendingCoefficient (DGSEMOperator.cpp:60-80).
@@ -270,6 +296,28 @@ void *ref_create(int dim, int order, int ne, const double *h, const int32_t *nbr
 }
 
 void ref_destroy(void *h) { delete (RefCtx *)h; }
+
+// Boundary condition `index` as the reference's integrator of `type` (1
+// supersonic inflow, 2 supersonic outflow, 3 specified state, 4 slip wall,
+// 5 symmetry) with constant state `state` where the type takes one.
+int ref_set_boundary(void *h, int index, int type, const double *state)
+{
+    RefCtx &c = *(RefCtx *)h;
+    if (index < 0 || index >= 16) return 1;
+    Vector st(c.nv);
+    for (int v = 0; v < c.nv; v++) st(v) = state ? state[v] : 0.0;
+    BdrFaceIntegrator *b = nullptr;
+    switch (type) {
+    case 1: b = new SupersonicInflowBdrFaceIntegrator(c.lifting, *c.rsolver, c.Np, c.time, c.gamma, st); break;
+    case 2: b = new SupersonicOutflowBdrFaceIntegrator(c.lifting, *c.rsolver, c.Np, c.time, c.gamma); break;
+    case 3: b = new SpecifiedStateBdrFaceIntegrator(c.lifting, *c.rsolver, c.Np, c.time, c.gamma, st); break;
+    case 4: b = new SlipWallBdrFaceIntegrator(c.lifting, *c.rsolver, c.Np, c.time, c.gamma); break;
+    case 5: b = new SymmetryBdrFaceIntegrator(c.lifting, *c.rsolver, c.Np, c.time, c.gamma); break;
+    default: return 1;
+    }
+    c.bfi[index].reset(b);
+    return 0;
+}
 
 // DGSEMOperator::Mult.  u, dudt: byNODES vectors of the full size.
 double ref_rhs(void *h, const double *u_in, double *dudt_out)
@@ -394,10 +442,22 @@ double ref_rhs(void *h, const double *u_in, double *dudt_out)
             c.integ->AssembleFaceVector(fe, fe, T, el_u, el_dudt);
             dudt.AddElementVector(vdofs, el_dudt);
         }
+        // boundary faces (DGSEMNonlinearForm::Mult's boundary-face loop)
+        for (auto &f : c.bfaces) {
+            setup_bdr_face(c, f, T);
+            c.vfes->GetElementVDofs(f.e, vdofs);
+            u.GetSubVector(vdofs, el_u);
+            c.bfi[f.b]->AssembleFaceVector(fe, fe, T, el_u, el_dudt);
+            dudt.AddElementVector(vdofs, el_dudt);
+        }
     }
 #endif
     for (int i = 0; i < size; i++) dudt_out[i] = dudt(i);
-    return c.integ->GetMaxCharSpeed();
+    // DGSEMOperator::Mult (DGSEMOperator.cpp:585-589)
+    double lam = c.integ->GetMaxCharSpeed();
+    for (auto &b : c.bfi)
+        if (b) lam = std::max(lam, b->GetMaxCharSpeed());
+    return lam;
 }
 
 void ref_get_blending(void *h, double *eta, double *alpha)

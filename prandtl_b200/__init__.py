@@ -37,7 +37,10 @@ KERNEL_FILTER_BOUNDS, KERNEL_FILTER = 10, 11
 KERNEL_ADJ_RHS, KERNEL_ADJ_LIFT = 12, 13
 KERNEL_ADJ_FACE_EULER = (14, 15, 16)
 KERNEL_ADJ_FACE_NS = (17, 18, 19)
-KERNEL_EULER_FACES, KERNEL_NS_FACES = 20, 21
+KERNEL_EULER_FACES, KERNEL_NS_FACES, KERNEL_BOUNDARY = 20, 21, 22
+# boundary condition types (pdg_set_boundary)
+BC_SUPERSONIC_INFLOW, BC_SUPERSONIC_OUTFLOW, BC_SPECIFIED_STATE, BC_SLIP_WALL, BC_SYMMETRY = 1, 2, 3, 4, 5
+MAX_BOUNDARIES = 16
 PDG_FLAG_NONFINITE = 1
 PDG_FLAG_NONPHYSICAL = 2
 _STATUS = {1: "bad argument", 2: "CUDA error", 3: "non-finite state", 4: "non-physical state",
@@ -118,6 +121,7 @@ def library():
     L.pdg_filter_count.argtypes = [C.c_void_p, C.POINTER(C.c_int64)]
     L.pdg_rhs_vjp.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
     L.pdg_rhs_noalloc.argtypes = [C.POINTER(PdgMesh), C.POINTER(PdgParams), C.c_void_p, C.c_void_p, C.c_void_p]
+    L.pdg_set_boundary.argtypes = [C.c_void_p, C.c_int, C.c_int, _dp]
     _lib = L
     return L
 
@@ -159,6 +163,19 @@ class DGSEMOperator:
                           self._nbr.ctypes.data_as(_ip))
         self._ctx = C.c_void_p()
         self._call(library().pdg_create(C.byref(self._m), C.byref(self.params), C.byref(self._ctx)), "pdg_create")
+        for b, spec in (getattr(mesh, "boundaries", None) or {}).items():
+            self.set_boundary(b, *spec)
+
+    def set_boundary(self, index: int, type: int, state=None):
+        """Boundary condition ``index`` of the mesh's negative neighbour
+        entries (pdg_set_boundary; the reference's BdrFaceIntegrators)."""
+        st = None
+        if state is not None:
+            st = np.ascontiguousarray(state, dtype=np.float64)
+            self._bc_state = getattr(self, "_bc_state", {})
+            self._bc_state[index] = st
+        ptr = st.ctypes.data_as(_dp) if st is not None else None
+        self._call(library().pdg_set_boundary(self._ctx, int(index), int(type), ptr), "pdg_set_boundary")
 
     def _call(self, code: int, what: str):
         if code != PDG_OK:

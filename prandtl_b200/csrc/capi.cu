@@ -41,6 +41,11 @@ struct pdg_ctx {
     double *lbuf = nullptr;                         // BR1 lifting jumps [d][e][fn][v]
     double *fcol = nullptr;                         // viscous normal columns at faces
     double *vbuf = nullptr;                         // viscous volume term [v-1][node] (element-side faces)
+    // boundary conditions: host table, its device copy, which entries the
+    // mesh uses and which pdg_set_boundary has set
+    double bc_host[PDG_MAX_BOUNDARIES * BC_SLOT] = {};
+    double *bc = nullptr;
+    unsigned int bc_used = 0, bc_set = 0;
     double *stage_a = nullptr, *stage_b = nullptr;  // RK stage buffers
     double *io_a = nullptr, *io_b = nullptr;        // host-path staging
     unsigned long long *lam_bits = nullptr;
@@ -266,7 +271,8 @@ int kernel_config(int dim, int N, int kind, int64_t ne, int device, LaunchCfg *c
             *why = "occupancy query failed";
             return PDG_ERR_CUDA;
         }
-        const int64_t threads = kind == KIND_FILTER_BOUNDS ? 32 * ne : (kind == KIND_LIFT_FACE ? (int64_t)dim : 1) * ne * nfn;
+        const int64_t threads = kind == KIND_FILTER_BOUNDS ? 32 * ne
+                                : kind == KIND_BOUNDARY ? ne : (kind == KIND_LIFT_FACE ? (int64_t)dim : 1) * ne * nfn;
         cfg->wpb = 8;
         cfg->grid = (int)std::max<int64_t>(1, std::min<int64_t>((threads + 255) / 256, (int64_t)sms * std::max(1, blocks_per_sm)));
         cfg->smem = 0;
@@ -368,6 +374,8 @@ KParams base_params(pdg_ctx *c)
     P.blending = c->p.blending;
     P.compat = c->p.compat;
     P.prefetch = c->prefetch;
+    P.bc = c->bc;
+    P.has_bdr = c->bc_used != 0;
     return P;
 }
 
@@ -449,6 +457,11 @@ int lift(pdg_ctx *c, KParams P, const double *u, double *grads_out, cudaStream_t
 // kernels of each direction add their terms.
 int evaluate(pdg_ctx *c, int stage, double dt, const double *un, const double *us, double *out, cudaStream_t s)
 {
+    if (c->bc_used & ~c->bc_set) {
+        for (int b = 0; b < PDG_MAX_BOUNDARIES; b++)
+            if ((c->bc_used & ~c->bc_set) >> b & 1u)
+                return fail(c, PDG_ERR_ARG, "boundary condition %d is used by the mesh but not set (pdg_set_boundary)", b);
+    }
     if (!c->p.compat) CK(cudaMemsetAsync(c->lam_bits, 0, sizeof(unsigned long long), s), "reset wave speed");
     KParams P = base_params(c);
     P.u = us;
@@ -480,6 +493,7 @@ int evaluate(pdg_ctx *c, int stage, double dt, const double *un, const double *u
             if ((r = launch(c, KIND_EULER, P, s))) return r;
             for (int d = 0; d < c->dim; d++)
                 if ((r = launch(c, KIND_FACE_E0 + d, P, s))) return r;
+            if (c->bc_used && (r = launch(c, KIND_BOUNDARY, P, s))) return r;
         }
     }
     // entropy filter of the stage output (EntropyFilter::FilterSolution)
@@ -533,8 +547,13 @@ int pdg_create(const pdg_mesh *mesh, const pdg_params *params, pdg_ctx **out)
             c->hmin = std::min(c->hmin, c->h[d]);
         }
     }
-    for (int64_t i = 0; i < c->ne * 2 * c->dim; i++)
-        if (mesh->nbr[i] < 0 || mesh->nbr[i] >= c->ne) { delete c; return PDG_ERR_ARG; }
+    for (int64_t i = 0; i < c->ne * 2 * c->dim; i++) {
+        const int32_t nb = mesh->nbr[i];
+        if (nb >= c->ne || nb < -PDG_MAX_BOUNDARIES) { delete c; return PDG_ERR_ARG; }
+        if (nb < 0) c->bc_used |= 1u << (-1 - nb);
+    }
+    // boundary faces: Euler only (the BR1 boundary lifting is not built)
+    if (c->bc_used && params->parabolic) { delete c; return PDG_ERR_UNSUPPORTED; }
     auto cleanup = [&](int code) {
         pdg_destroy(c);
         return code;
@@ -547,8 +566,10 @@ int pdg_create(const pdg_mesh *mesh, const pdg_params *params, pdg_ctx **out)
     if (cudaMalloc(&c->K, sizeof(DevConst)) != cudaSuccess || cudaMalloc(&c->nbr, sizeof(int32_t) * c->ne * 2 * c->dim) ||
         cudaMalloc(&c->eta, sizeof(double) * c->ne) || cudaMalloc(&c->alpha, sizeof(double) * c->ne) ||
         cudaMalloc(&c->lam_bits, sizeof(unsigned long long)) || cudaMalloc(&c->err, sizeof(unsigned int)) ||
-        cudaMalloc(&c->stage_a, fbytes) || cudaMalloc(&c->stage_b, fbytes))
+        cudaMalloc(&c->stage_a, fbytes) || cudaMalloc(&c->stage_b, fbytes) ||
+        cudaMalloc(&c->bc, sizeof(double) * PDG_MAX_BOUNDARIES * BC_SLOT))
         return cleanup(PDG_ERR_NOMEM);
+    if (cudaMemset(c->bc, 0, sizeof(double) * PDG_MAX_BOUNDARIES * BC_SLOT) != cudaSuccess) return cleanup(PDG_ERR_CUDA);
     if (c->p.filter) {
         if (cudaMalloc(&c->ent_own, sizeof(double) * c->ne) != cudaSuccess ||
             cudaMalloc(&c->filter_count, sizeof(unsigned long long)) != cudaSuccess ||
@@ -576,6 +597,29 @@ int pdg_create(const pdg_mesh *mesh, const pdg_params *params, pdg_ctx **out)
     return PDG_OK;
 }
 
+int pdg_set_boundary(pdg_ctx *c, int index, int type, const double *state)
+{
+    if (!c) return PDG_ERR_ARG;
+    if (index < 0 || index >= PDG_MAX_BOUNDARIES)
+        return fail(c, PDG_ERR_ARG, "pdg_set_boundary: index %d outside [0, %d)", index, PDG_MAX_BOUNDARIES);
+    if (type < PDG_BC_SUPERSONIC_INFLOW || type > PDG_BC_SYMMETRY)
+        return fail(c, PDG_ERR_ARG, "pdg_set_boundary: unknown boundary type %d", type);
+    double slot[BC_SLOT] = {(double)type};
+    if (type == PDG_BC_SUPERSONIC_INFLOW || type == PDG_BC_SPECIFIED_STATE) {
+        if (!state) return fail(c, PDG_ERR_ARG, "pdg_set_boundary: type %d needs a state", type);
+        double msq = 0.0;
+        for (int d = 0; d < c->dim; d++) msq += state[1 + d] * state[1 + d];
+        const double p = (c->p.gamma - 1.0) * (state[c->dim + 1] - 0.5 * msq / state[0]);
+        if (!(state[0] > 0.0) || !(p > 0.0) || !std::isfinite(p))
+            return fail(c, PDG_ERR_ARG, "pdg_set_boundary: the state of condition %d is not physical", index);
+        for (int v = 0; v < c->nv; v++) slot[1 + v] = state[v];
+    }
+    std::memcpy(c->bc_host + index * BC_SLOT, slot, sizeof(slot));
+    CK(cudaMemcpy(c->bc + index * BC_SLOT, slot, sizeof(slot), cudaMemcpyHostToDevice), "boundary table upload");
+    c->bc_set |= 1u << index;
+    return PDG_OK;
+}
+
 int pdg_destroy(pdg_ctx *c)
 {
     if (!c) return PDG_OK;
@@ -586,6 +630,7 @@ int pdg_destroy(pdg_ctx *c)
     cudaFree(c->lbuf);
     cudaFree(c->fcol);
     cudaFree(c->vbuf);
+    cudaFree(c->bc);
     cudaFree(c->stage_a);
     cudaFree(c->stage_b);
     cudaFree(c->io_a);
@@ -810,6 +855,7 @@ int pdg_rhs_vjp(pdg_ctx *c, const double *u, const double *cot, double *ubar, vo
     if (!c) return PDG_ERR_ARG;
     if (!u || !cot || !ubar || ubar == u || ubar == cot) return fail(c, PDG_ERR_ARG, "pdg_rhs_vjp: null or aliased buffers");
     if (c->p.compat) return fail(c, PDG_ERR_UNSUPPORTED, "pdg_rhs_vjp: the adjoint is of the fixed operator (compat = 0)");
+    if (c->bc_used) return fail(c, PDG_ERR_UNSUPPORTED, "pdg_rhs_vjp: boundary faces are not differentiated");
     cudaStream_t s = (cudaStream_t)stream;
     int r;
     if (!c->adj_ready) {

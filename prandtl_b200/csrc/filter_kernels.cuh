@@ -134,7 +134,10 @@ __global__ void __launch_bounds__(128) filter_kernel(const KParams P)
         }
         double bound = P.ent_own[e];
 #pragma unroll
-        for (int f = 0; f < 2 * DIM; f++) bound = fmin(bound, P.ent_own[P.nbr[e * 2 * DIM + f]]);
+        for (int f = 0; f < 2 * DIM; f++) {
+            const int32_t nb = P.nbr[e * 2 * DIM + f];
+            if (nb >= 0) bound = fmin(bound, P.ent_own[nb]);  // boundary faces have no neighbour
+        }
         // NaN-safe: the element is filtered only when a constraint is met as false
         if (!(mr < FILTER_RHO_MIN || mp < FILTER_P_MIN || me < bound - FILTER_ENT_TOL)) {
             __syncwarp();

@@ -26,7 +26,8 @@ enum KernelKind {
     KIND_ADJ_FACE_NS2 = 19,
     KIND_EULER_FACES = 20,    // rhs_kernel<dim, N, false, true>: Euler volume + face terms (+ stage)
     KIND_NS_FACES = 21,       // rhs_kernel<dim, N, true, true>: NS inviscid volume + all face terms (+ stage)
-    KIND_COUNT = 22
+    KIND_BOUNDARY = 22,       // boundary_kernel<dim, N>: boundary faces of the separate-face path (Euler)
+    KIND_COUNT = 23
 };
 
 struct KernelInfo {

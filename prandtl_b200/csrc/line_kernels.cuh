@@ -8,16 +8,19 @@
 // and evaluates every two-point flux of that line (Np(Np-1)/2 independent
 // evaluations, which the scheduler overlaps), sums the line's contributions
 // in registers and adds them to a per-node accumulator in shared memory.
-// Element faces are evaluated once per face node by separate face kernels
-// (one thread per face node): the element on the -d side receives C and the
-// one on the +d side -C for the inviscid and viscous fluxes; both receive the
-// same BR1 lifting jump.  Both sides therefore see bit-identical face fluxes.
-// The volume kernel writes the output (RHS or SSP-RK3 stage) and the other
-// kernels add their terms to it, scaled by the stage factor.
+// Element faces are evaluated with the element-1 rule, either by separate
+// face kernels (one thread per face node: the element on the -d side
+// receives C and the one on the +d side -C) or, for the fixed operator,
+// inside the volume kernel by each of the face's two elements from the same
+// inputs in the same order; both sides therefore see bit-identical face
+// fluxes.  Both receive the same BR1 lifting jump.  Boundary faces (a
+// negative neighbour entry, Euler) take the boundary condition's flux.
 //
 // Kernels per right-hand side:
-//   Euler:          rhs_kernel<false> -> face_kernel<x>, <y>[, <z>]
-//   Navier-Stokes:  lift_face_kernel -> rhs_kernel<true> -> lift_kernel -> face_kernel<x>, <y>[, <z>]
+//   Euler, fixed:     rhs_kernel<false, faces>
+//   NS, fixed:        lift_face_kernel -> lift_kernel (viscous volume term to vbuf) -> rhs_kernel<true, faces>
+//   Euler, reference: rhs_kernel<false> -> face_kernel<x>, <y>[, <z>]
+//   NS, reference:    lift_face_kernel -> rhs_kernel<true> -> lift_kernel -> face_kernel<x>, <y>[, <z>]
 // lift_kernel turns the state into BR1 primitive gradients and from them the
 // viscous terms the other kernels need (the volume divergence of the viscous
 // flux at every node and its normal column at every face node), so neither
@@ -81,7 +84,15 @@ struct KParams {
     double diss_scale;
     int blending, compat;
     int prefetch;         // L2-prefetch the next element's inputs
+    const double *bc;     // boundary conditions, BC_SLOT doubles each (type, state)
+    int has_bdr;          // the neighbour table holds boundary faces (negative entries)
 };
+
+// Boundary conditions (src/Integrators/BoundaryConditions/): a neighbour
+// entry -1 - b marks a boundary face with condition b of the table P.bc.
+constexpr int BC_SLOT = 8;
+constexpr int BC_SUPERSONIC_INFLOW = 1, BC_SUPERSONIC_OUTFLOW = 2, BC_SPECIFIED_STATE = 3, BC_SLIP_WALL = 4,
+              BC_SYMMETRY = 5;
 
 constexpr int pow2_at_least(int x) { return x <= 1 ? 1 : x <= 2 ? 2 : x <= 4 ? 4 : x <= 8 ? 8 : x <= 16 ? 16 : 32; }
 
@@ -508,6 +519,9 @@ template <int DIM, int N, int D, bool NS>
 __device__ __forceinline__ double face_node_terms(const KParams &P, const double *c, int64_t a, int64_t b, int fn,
                                                   double coef, double *C);
 template <int DIM, bool NS> struct FaceIn;
+template <int DIM, int N, int D>
+__device__ __noinline__ double boundary_node_terms(const KParams &P, const double *c, const double *s, int b,
+                                                   double sgn, double coef, double *C);
 template <int DIM, int N, int D, bool NS>
 __device__ __forceinline__ void load_face_in(const KParams &P, int64_t a, int64_t b, int fn, FaceIn<DIM, NS> &in);
 template <int DIM, int N, int D, bool NS>
@@ -524,7 +538,7 @@ __device__ __forceinline__ double face_terms_from(const KParams &P, const double
 // face fluxes read velocities from the momentum slots).
 template <int DIM, int N, bool NS, int D>
 __device__ __forceinline__ void face_terms_dir(const KParams &P, const double *c, double *acc, int64_t e,
-                                               const int32_t *enb, int gl, bool valid, double coef)
+                                               const int32_t *enb, int gl, bool valid, double coef, double &lam)
 {
     using S = Shape<DIM, N>;
     constexpr int Np = S::Np, NV = S::NV, NFN = S::NFN, L = S::L, ST = S::NS_;
@@ -538,7 +552,14 @@ __device__ __forceinline__ void face_terms_dir(const KParams &P, const double *c
                 if (t < 2 * NFN) {
                     const int side = t >= NFN, fn = side ? t - NFN : t;
                     const int64_t other = enb[2 * D + side];
-                    load_face_in<DIM, N, D, false>(P, side ? e : other, side ? other : e, fn, in[r]);
+                    if (NS || other >= 0) {  // NS meshes have no boundary faces
+                        load_face_in<DIM, N, D, false>(P, side ? e : other, side ? other : e, fn, in[r]);
+                    } else {
+                        // boundary face: this element's trace only
+                        const int n = line_node<DIM, Np, D>(fn, side ? N : 0);
+#pragma unroll
+                        for (int v = 0; v < NV; v++) in[r].sa[v] = __ldg(P.u + v * P.nnodes + e * S::NDOF + n);
+                    }
                 }
             }
 #pragma unroll
@@ -548,13 +569,20 @@ __device__ __forceinline__ void face_terms_dir(const KParams &P, const double *c
                     const int side = t >= NFN, fn = side ? t - NFN : t;
                     const int64_t other = enb[2 * D + side];
                     const int64_t a = side ? e : other, b = side ? other : e;
-                    double C[NV];
-                    face_terms_from<DIM, N, D, false>(P, c, a <= b, in[r], coef, C);
                     const int n = sp<DIM, Np>(line_node<DIM, Np, D>(fn, side ? N : 0));
+                    double C[NV];
+                    if (NS || other >= 0) {
+                        face_terms_from<DIM, N, D, false>(P, c, a <= b, in[r], coef, C);
 #pragma unroll
-                    for (int v = 0; v < NV; v++) {
-                        if (side) acc[v * ST + n] += C[v];
-                        else acc[v * ST + n] -= C[v];
+                        for (int v = 0; v < NV; v++) {
+                            if (side) acc[v * ST + n] += C[v];
+                            else acc[v * ST + n] -= C[v];
+                        }
+                    } else {
+                        lam = fmax(lam, boundary_node_terms<DIM, N, D>(P, c, in[r].sa, (int)(-1 - other),
+                                                                        side ? 1.0 : -1.0, coef, C));
+#pragma unroll
+                        for (int v = 0; v < NV; v++) acc[v * ST + n] += C[v];
                     }
                 }
             }
@@ -567,7 +595,7 @@ __device__ __forceinline__ void face_terms_dir(const KParams &P, const double *c
                 const int t = gl + r * L;
                 if (t < 2 * NFN) {
                     const int side = t >= NFN, fn = side ? t - NFN : t;
-                    const int64_t other = enb[2 * D + side];
+                    const int64_t other = enb[2 * D + side];  // >= 0: NS meshes have no boundary faces
                     const int64_t a = side ? e : other, b = side ? other : e;
                     const double *fa = P.fcol + (((D * 2 + 1) * ne + a) * NFN + fn) * (NV - 1);
                     const double *fb = P.fcol + (((D * 2 + 0) * ne + b) * NFN + fn) * (NV - 1);
@@ -697,9 +725,9 @@ __device__ __forceinline__ void rhs_tile(const KParams &P, const double *c, doub
     }
     __syncwarp();
     if (PRELOAD) {
-        face_terms_dir<DIM, N, NS, 0>(P, c, acc, e, enb, gl, valid, coef);
-        face_terms_dir<DIM, N, NS, 1>(P, c, acc, e, enb, gl, valid, coef);
-        if (DIM == 3) face_terms_dir<DIM, N, NS, (DIM == 3 ? 2 : 0)>(P, c, acc, e, enb, gl, valid, coef);
+        face_terms_dir<DIM, N, NS, 0>(P, c, acc, e, enb, gl, valid, coef, lam);
+        face_terms_dir<DIM, N, NS, 1>(P, c, acc, e, enb, gl, valid, coef, lam);
+        if (DIM == 3) face_terms_dir<DIM, N, NS, (DIM == 3 ? 2 : 0)>(P, c, acc, e, enb, gl, valid, coef, lam);
     } else {
         // one face node at a time (Euler): the batched sweep's register
         // variants are tuned for this form
@@ -873,6 +901,85 @@ __device__ __forceinline__ double face_terms_from(const KParams &P, const double
     return lam;
 }
 
+// Boundary face node of an element with interior trace s on its +D (sgn = 1)
+// or -D (sgn = -1) face, boundary condition b (BdrFaceIntegrator::
+// AssembleFaceVector, src/Integrators/BoundaryConditions/BdrFaceIntegrator.cpp:
+// 64-130): the outer state of the condition and the face flux with the
+// outward normal sgn |n_D| e_D, or the slip wall's pressure flux; the element
+// receives C = -F / (w0 J) times the stage factor.  Returns the wave speed the
+// condition reports.  Outer states: supersonic inflow and specified state the
+// prescribed state (SupersonicInflowBdrFaceIntegrator.cpp:22-35,
+// SpecifiedStateBdrFaceIntegrator.cpp:21-35), supersonic outflow the interior
+// state (SupersonicOutflowBdrFaceIntegrator.cpp:10-13), symmetry the interior
+// state with its normal momentum reversed (SymmetryBdrFaceIntegrator.cpp:
+// 12-37).  Slip wall (SlipWallBdrFaceIntegrator.cpp:15-58): with the normal
+// velocity vn and pressure p of the interior state rotated to the face frame,
+// p* = p + (g+1)/4 rho vn (vn + sqrt(vn^2 + 8 p / ((g+1) rho) ((g-1)/(g+1) +
+// 1))) for vn > 0, else p max(1 + (g-1)/2 vn/c, 1e-4)^(2g/(g-1)), and the
+// flux is p* n in the momentum rows only.  The rotation to the face frame
+// lists the normal component first and the others in ascending order, so
+// |v|^2 is summed in that order.
+// Not inlined: a rare path that would otherwise raise the register demand
+// of every face loop.
+template <int DIM, int N, int D>
+__device__ __noinline__ double boundary_node_terms(const KParams &P, const double *c, const double *s, int b,
+                                                   double sgn, double coef, double *C)
+{
+    constexpr int NV = DIM + 2, Np = N + 1;  // Np: constant layout
+    const double *bc = P.bc + b * BC_SLOT;
+    const int type = (int)bc[0];
+    const double nrm = sgn * C_AREA(c)[D];
+    double F[NV];
+    double lam;
+    if (type == BC_SLIP_WALL) {
+        const double rho = s[0];
+        double vsq = 0.0;
+        {
+            const double vD = s[1 + D] / rho;
+            vsq += vD * vD;
+#pragma unroll
+            for (int q = 0; q < DIM; q++)
+                if (q != D) {
+                    const double vq = s[1 + q] / rho;
+                    vsq += vq * vq;
+                }
+        }
+        const double p = P.gm1 * (s[DIM + 1] - 0.5 * rho * vsq);
+        const double vn = (sgn * s[1 + D]) / rho;
+        const double an = sqrt(P.gamma * p / rho);
+        const double gp1 = 1.0 + P.gamma, gp1inv = 1.0 / gp1;
+        double ps;
+        if (vn > 0.0) {
+            ps = p + 0.25 * vn * gp1 * rho * (vn + sqrt(vn * vn + 8.0 * gp1inv / rho * p * (P.gm1 * gp1inv + 1.0)));
+        } else {
+            ps = p * pow(fmax(1.0 + 0.5 * P.gm1 * vn / an, 0.0001), 2.0 * P.gamma * P.gm1inv);
+        }
+#pragma unroll
+        for (int v = 0; v < NV; v++) F[v] = 0.0;
+        F[1 + D] = ps * nrm;
+        lam = sqrt(vsq) + an;
+    } else {
+        double s2[NV];
+        const bool given = type == BC_SUPERSONIC_INFLOW || type == BC_SPECIFIED_STATE;
+#pragma unroll
+        for (int v = 0; v < NV; v++) s2[v] = given ? bc[1 + v] : s[v];
+        if (type == BC_SYMMETRY) s2[1 + D] = -s[1 + D];
+        const Prim<DIM> qa = make_prim<DIM>(s, P.gamma, P.gm1), qb = make_prim<DIM>(s2, P.gamma, P.gm1);
+        double ma[DIM], mb[DIM];
+#pragma unroll
+        for (int d = 0; d < DIM; d++) {
+            ma[d] = s[1 + d];
+            mb[d] = s2[1 + d];
+        }
+        face_flux<DIM, D>(qa, qb, ma, mb, nrm, P.gm1inv, P.compat != 0, P.diss_scale, F);
+        lam = fmax(qa.lam, qb.lam);
+    }
+    const double sc = C_FACE(c) * coef;
+#pragma unroll
+    for (int v = 0; v < NV; v++) C[v] = sc * (-F[v]);
+    return lam;
+}
+
 template <int DIM, int N, int D, bool NS>
 __device__ __forceinline__ double face_node_terms(const KParams &P, const double *c, int64_t a, int64_t b, int fn,
                                                   double coef, double *C)
@@ -883,12 +990,12 @@ __device__ __forceinline__ double face_node_terms(const KParams &P, const double
 }
 
 template <int DIM, int N, int D, bool NS>
-__device__ __forceinline__ double face_node(const KParams &P, const double *c, int64_t a, int fn, double coef)
+__device__ __forceinline__ double face_node(const KParams &P, const double *c, int64_t a, int64_t b, int fn,
+                                            double coef)
 {
     using S = Shape<DIM, N>;
     constexpr int Np = S::Np, NDOF = S::NDOF, NV = S::NV;
     const int64_t nn = P.nnodes;
-    const int64_t b = __ldg(P.nbr + a * 2 * DIM + 2 * D + 1);
     const int na = line_node<DIM, Np, D>(fn, N), nb = line_node<DIM, Np, D>(fn, 0);
     // the output values are loaded before the flux arithmetic, so that their
     // latency overlaps it
@@ -909,9 +1016,32 @@ __device__ __forceinline__ double face_node(const KParams &P, const double *c, i
 }
 
 
+// Boundary face node fn of element a's +D (side 1) or -D (side 0) face:
+// read-modify-write of a's output node.
+template <int DIM, int N, int D>
+__device__ __forceinline__ double boundary_node(const KParams &P, const double *c, int64_t a, int fn, int side, int b,
+                                                double coef)
+{
+    using S = Shape<DIM, N>;
+    constexpr int Np = S::Np, NDOF = S::NDOF, NV = S::NV;
+    const int64_t nn = P.nnodes;
+    const int n = line_node<DIM, Np, D>(fn, side ? N : 0);
+    double s[NV], o[NV], C[NV];
+#pragma unroll
+    for (int v = 0; v < NV; v++) {
+        s[v] = __ldg(P.u + v * nn + a * NDOF + n);
+        o[v] = P.out[v * nn + a * NDOF + n];
+    }
+    const double lam = boundary_node_terms<DIM, N, D>(P, c, s, b, side ? 1.0 : -1.0, coef, C);
+#pragma unroll
+    for (int v = 0; v < NV; v++) P.out[v * nn + a * NDOF + n] = o[v] + C[v];
+    return lam;
+}
+
 // Face kernel of direction D: one thread per (element, face node).  Within one
 // direction every output entry belongs to exactly one face, so the
-// read-modify-write updates need no atomics.
+// read-modify-write updates need no atomics.  Boundary faces are left to
+// boundary_kernel.
 template <int DIM, int N, int D, bool NS>
 __global__ void __launch_bounds__(256, 3) face_kernel(const KParams P)
 {
@@ -926,7 +1056,41 @@ __global__ void __launch_bounds__(256, 3) face_kernel(const KParams P)
          t += (int64_t)gridDim.x * blockDim.x) {
         const int64_t a = t / NFN;
         const int fn = (int)(t - a * NFN);
-        lam = fmax(lam, face_node<DIM, N, D, NS>(P, c, a, fn, coef));
+        const int64_t b = __ldg(P.nbr + a * 2 * DIM + 2 * D + 1);
+        if (b >= 0) lam = fmax(lam, face_node<DIM, N, D, NS>(P, c, a, b, fn, coef));  // else: boundary_kernel
+    }
+    lam = group_max<32>(lam);
+    if ((threadIdx.x & 31) == 0) atomic_max_pos(P.lam_bits, lam);
+}
+
+// Boundary faces for the separate-face path (Euler): one thread per element
+// walks its boundary faces one after another, so an edge or corner node on
+// two boundary faces is updated by one thread; threads of interior elements
+// return at once.  Launched after the face kernels, so its
+// read-modify-writes do not overlap theirs.
+template <int DIM, int N>
+__global__ void __launch_bounds__(256) boundary_kernel(const KParams P)
+{
+    using S = Shape<DIM, N>;
+    constexpr int NFN = S::NFN;
+    __shared__ double c[CONST_SLOTS];
+    load_consts(P.K, c, S::Np);
+    __syncthreads();
+    const double coef = stage_coef(P);
+    double lam = 0.0;
+    for (int64_t a = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; a < P.ne; a += (int64_t)gridDim.x * blockDim.x) {
+#pragma unroll 1
+        for (int f = 0; f < 2 * DIM; f++) {
+            const int32_t nb = __ldg(P.nbr + a * 2 * DIM + f);
+            if (nb >= 0) continue;
+            const int d = f >> 1, side = f & 1;
+#pragma unroll 1
+            for (int fn = 0; fn < NFN; fn++) {
+                if (d == 0) lam = fmax(lam, boundary_node<DIM, N, 0>(P, c, a, fn, side, -1 - nb, coef));
+                else if (d == 1) lam = fmax(lam, boundary_node<DIM, N, 1>(P, c, a, fn, side, -1 - nb, coef));
+                else lam = fmax(lam, boundary_node<DIM, N, (DIM == 3 ? 2 : 0)>(P, c, a, fn, side, -1 - nb, coef));
+            }
+        }
     }
     lam = group_max<32>(lam);
     if ((threadIdx.x & 31) == 0) atomic_max_pos(P.lam_bits, lam);

@@ -65,6 +65,8 @@ class CartesianMesh:
     hi: tuple[float, ...]
     nbr: np.ndarray             # (ne, 2*dim) int32
     spacing: tuple[float, ...] | None = None  # element extents, when not (hi - lo) / n exactly
+    # boundary conditions of negative neighbour entries -1 - b: {b: (type, state or None)}
+    boundaries: dict | None = None
 
     @property
     def Np(self) -> int:
@@ -145,3 +147,29 @@ def periodic_box(dim: int, order: int, n, lo, hi) -> CartesianMesh:
         nbr[:, 2 * d] = base + ((idx[d] - 1) % n[d]) * strides[d]
         nbr[:, 2 * d + 1] = base + ((idx[d] + 1) % n[d]) * strides[d]
     return CartesianMesh(dim, order, n, tuple(lo), tuple(hi), nbr)
+
+
+def box(dim: int, order: int, n, lo, hi, bdr=None, boundaries=None) -> CartesianMesh:
+    """Box [lo, hi] with n[d] elements per direction.  bdr[d] = None keeps
+    direction d periodic; bdr[d] = (b_lo, b_hi) makes its -d and +d sides
+    boundary faces with conditions b_lo and b_hi (neighbour entry -1 - b).
+    ``boundaries`` maps each condition to (type, state), the arguments of
+    DGSEMOperator.set_boundary (the reference's boundary attributes and
+    BdrFaceIntegrators, src/Simulation/Simulation.cpp:490-798)."""
+    m = periodic_box(dim, order, n, lo, hi)
+    if bdr is None:
+        bdr = [None] * dim
+    nbr = m.nbr.copy()
+    e = np.arange(m.num_elements)
+    r = e.copy()
+    for d in range(dim):
+        i = r % m.n[d]
+        r //= m.n[d]
+        if bdr[d] is None:
+            continue
+        b_lo, b_hi = bdr[d]
+        nbr[i == 0, 2 * d] = -1 - int(b_lo)
+        nbr[i == m.n[d] - 1, 2 * d + 1] = -1 - int(b_hi)
+    m.nbr = nbr
+    m.boundaries = dict(boundaries or {})
+    return m

@@ -1,0 +1,128 @@
+"""Boundary faces on the GPU (Euler) against the oracle, whose boundary
+conditions are pinned to the reference's own integrators
+(tests/test_boundaries.py): both face paths (element-side for the fixed
+operator, separate face kernels + boundary_kernel for the reference-value
+operator), RK stages, graph-replayed steps, the filter, and the errors."""
+import numpy as np
+import pytest
+
+import oracle
+import prandtl_b200 as pb
+from prandtl_b200.mesh import box
+
+from helpers import rel_maxnorm, rough
+from test_boundaries import freestream_box, layout_case, layouts, uniform
+
+pytestmark = pytest.mark.gpu
+TOL = 1e-12
+
+
+def dev(x, device):
+    import torch
+    return torch.from_numpy(np.ascontiguousarray(x)).to(device)
+
+
+@pytest.mark.parametrize("compat", [1, 0])
+@pytest.mark.parametrize("order", [1, 3, 4])
+@pytest.mark.parametrize("name", sorted(layouts()))
+def test_gpu_boundaries_match_oracle(name, order, compat, cuda_device):
+    import torch
+    mesh, u = layout_case(name, order)
+    op = pb.DGSEMOperator(mesh, compat=compat)
+    orc = oracle.Oracle(mesh, compat=compat)
+    ref = orc.rhs(u)
+    out = torch.empty(u.size, dtype=torch.float64, device=cuda_device)
+    op.Mult(dev(u, cuda_device), out)
+    torch.cuda.synchronize()
+    assert rel_maxnorm(out.cpu().numpy(), ref) < TOL
+    assert abs(op.GetMaxCharSpeed() - orc.max_char_speed()) <= 1e-12 * orc.max_char_speed()
+    assert op.check() == 0
+
+
+@pytest.mark.parametrize("compat", [1, 0])
+@pytest.mark.parametrize("name", ["2d_in_out_walls", "3d_all"])
+def test_gpu_boundary_stages_and_graph_steps(name, compat, cuda_device):
+    import torch
+    mesh, u = layout_case(name, 3)
+    op = pb.DGSEMOperator(mesh, compat=compat)
+    orc = oracle.Oracle(mesh, compat=compat)
+    orc.rhs(u)
+    dt = 0.2 * min(mesh.h) / (orc.max_char_speed() * 16)
+    un = dev(u, cuda_device)
+    us = dev(rough(u, mesh, 5, 0.01, 0.001), cuda_device)
+    for stage in (0, 1, 2):
+        out = torch.empty_like(un)
+        op.rk_stage(stage, dt, un, us, out)
+        torch.cuda.synchronize()
+        assert rel_maxnorm(out.cpu().numpy(), orc.rk_stage(stage, dt, un.cpu().numpy(), us.cpu().numpy())) < TOL
+    a = un.clone()
+    b = un.clone()
+    op.rk3_step(a, dt, nsteps=3)
+    op.rk3_step(b, dt, nsteps=3, graph=True)
+    y = u
+    for _ in range(3):
+        y = orc.rk3_step(y, dt)
+    torch.cuda.synchronize()
+    assert torch.equal(a, b)
+    assert rel_maxnorm(a.cpu().numpy(), y) < 1e-11
+
+
+@pytest.mark.parametrize("dim,order", [(2, 3), (3, 2)])
+def test_gpu_freestream_is_preserved(dim, order, cuda_device):
+    import torch
+    mesh = freestream_box(dim, order)
+    u = uniform(mesh)
+    for compat in (0, 1):
+        op = pb.DGSEMOperator(mesh, compat=compat)
+        out = torch.empty(u.size, dtype=torch.float64, device=cuda_device)
+        op.Mult(dev(u, cuda_device), out)
+        torch.cuda.synchronize()
+        assert np.abs(out.cpu().numpy()).max() < 1e-12 * np.abs(u).max()
+
+
+def test_gpu_filter_with_boundaries(cuda_device):
+    import torch
+    mesh, u = layout_case("2d_in_out_walls", 3)
+    u = rough(u, mesh, 3, 0.2, 0.05)   # rougher, still positive
+    assert u[:mesh.num_nodes].min() > 0
+    op = pb.DGSEMOperator(mesh, compat=0, filter=1)
+    orc = oracle.Oracle(mesh, compat=0, filter=1)
+    orc.rhs(u)
+    dt = 0.2 * min(mesh.h) / (orc.max_char_speed() * 16)
+    x = dev(u, cuda_device)
+    op.rk3_step(x, dt)
+    torch.cuda.synchronize()
+    y = orc.rk3_step(u, dt)
+    assert np.isfinite(y).all()
+    assert rel_maxnorm(x.cpu().numpy(), y) < 1e-11
+    assert op.filter_count() == orc.filtered_elements()
+
+
+def test_boundary_errors(cuda_device):
+    import torch
+    mesh, u = layout_case("2d_symmetry_state", 2)
+    bcs = mesh.boundaries
+    mesh.boundaries = {0: bcs[0]}              # condition 1 left unset
+    op = pb.DGSEMOperator(mesh)
+    out = torch.empty(u.size, dtype=torch.float64, device=cuda_device)
+    with pytest.raises(pb.PdgError) as ei:
+        op.Mult(dev(u, cuda_device), out)
+    assert ei.value.code == 1 and "not set" in str(ei.value)
+    with pytest.raises(pb.PdgError):
+        op.set_boundary(1, 9)                  # unknown type
+    with pytest.raises(pb.PdgError):
+        op.set_boundary(1, pb.BC_SPECIFIED_STATE)  # a state is needed
+    with pytest.raises(pb.PdgError):
+        op.set_boundary(1, pb.BC_SPECIFIED_STATE, [1.0, 0.0, 0.0, -1.0])  # p < 0
+    with pytest.raises(pb.PdgError):
+        op.set_boundary(pb.MAX_BOUNDARIES, pb.BC_SLIP_WALL)
+    op.set_boundary(1, *bcs[1])
+    op.Mult(dev(u, cuda_device), out)
+    mesh.boundaries = bcs
+    with pytest.raises(pb.PdgError) as ei:
+        pb.DGSEMOperator(mesh, parabolic=1, mu=0.01)
+    assert ei.value.code == 5
+    op0 = pb.DGSEMOperator(mesh, compat=0)
+    with pytest.raises(pb.PdgError) as ei:
+        op0.vjp(dev(u, cuda_device), dev(u, cuda_device))
+    assert ei.value.code == 5
