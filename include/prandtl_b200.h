@@ -109,15 +109,24 @@ int pdg_destroy(pdg_ctx *ctx);
  * boundary face with condition b; every condition the mesh uses must be set
  * before the first evaluation (else PDG_ERR_ARG).  Euler only: pdg_create
  * returns PDG_ERR_UNSUPPORTED for a Navier-Stokes mesh with boundary faces,
- * and pdg_rhs_vjp for any mesh with them.  `state` (conserved, dim + 2
- * values, rho > 0 and p > 0) is read for the two types with a prescribed
- * state and may be NULL otherwise. */
+ * and pdg_rhs_vjp for any mesh with them.  `state` holds the condition's
+ * data as listed beside each type (conserved, dim + 2 values, for the two
+ * prescribed-state types) and may be NULL for types without data.  With
+ * compat = 1 the subsonic and Riemann-invariant conditions keep the
+ * reference's in-place division of the interior momenta before the face flux
+ * reads them; compat = 0 uses the interior state as it is.  The total-
+ * pressure inflow is 2D only (the reference's 3D branch writes past its
+ * direction vector): PDG_ERR_UNSUPPORTED in 3D. */
 #define PDG_MAX_BOUNDARIES 16
 #define PDG_BC_SUPERSONIC_INFLOW  1  /* SupersonicInflowBdrFaceIntegrator: prescribed outer state */
 #define PDG_BC_SUPERSONIC_OUTFLOW 2  /* SupersonicOutflowBdrFaceIntegrator: outer state = interior */
 #define PDG_BC_SPECIFIED_STATE    3  /* SpecifiedStateBdrFaceIntegrator: prescribed outer state */
 #define PDG_BC_SLIP_WALL          4  /* SlipWallBdrFaceIntegrator: pressure flux from the wall Riemann problem */
 #define PDG_BC_SYMMETRY           5  /* SymmetryBdrFaceIntegrator: normal momentum mirrored */
+#define PDG_BC_SUBSONIC_OUTFLOW_P 6  /* SubsonicOutflowPBdrFaceIntegrator: state = {p} */
+#define PDG_BC_SUBSONIC_INFLOW_RV 7  /* SubsonicInflowRVBdrFaceIntegrator: state = {rho, V[dim]} */
+#define PDG_BC_SUBSONIC_INFLOW_PTTT 8  /* SubsonicInflowPtTtAngBdrFaceIntegrator, 2D: state = {cp, pt, Tt, theta, phi} (degrees) */
+#define PDG_BC_RIEMANN_INVARIANT  9  /* RiemannInvariantBdrFaceIntegrator: state = primitive {rho, v[dim], p} */
 int pdg_set_boundary(pdg_ctx *ctx, int index, int type, const double *state);
 
 /* TimeDependentOperator::Height (DGSEMOperator.cpp:18): number of vdofs. */

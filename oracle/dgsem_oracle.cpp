@@ -923,6 +923,100 @@ static double bdr_flux(const Ctx &c, int b, const double *s1, const double *nor,
         for (int d = 0; d < dim; d++) flux[1 + d] = p_star * nor[d];
         return std::sqrt(vv) + an;
     }
+    // s1 as the face flux sees it: the subsonic conditions of the reference
+    // divide the interior state's momenta in place through Vector views
+    // (ComputePressure, BasicOperations.cpp:31-37, and the views V_i / vel);
+    // compat keeps that, fixed uses the interior state as it is.
+    double s1c[5];
+    for (int v = 0; v < nv; v++) s1c[v] = s1[v];
+    const double *prm = c.bc[b] + 1;
+    const bool compat = c.p.compat != 0;
+    if (type == 6) {
+        // SubsonicOutflowPBdrFaceIntegrator::ComputeOuterInviscidState (:17-31)
+        double vel[3], vv = 0.0;
+        const double r1 = 1.0 / s1[0];
+        for (int d = 0; d < dim; d++) vel[d] = compat ? s1[1 + d] * r1 : s1[1 + d] / s1[0];
+        for (int d = 0; d < dim; d++) vv += vel[d] * vel[d];
+        if (compat)
+            for (int d = 0; d < dim; d++) s1c[1 + d] = vel[d];
+        for (int v = 0; v < nv; v++) s2[v] = s1c[v];
+        s2[nv - 1] = prm[0] * gammaM1Inverse + 0.5 * s1[0] * vv;
+        return face_flux(dim, gamma, c.p.compat, c.p.face_dissipation, s1c, s2, nor, flux);
+    }
+    if (type == 7) {
+        // SubsonicInflowRVBdrFaceIntegrator::ComputeOuterInviscidState (:20-50)
+        const double r = prm[0];
+        s2[0] = r;
+        double dke = -s1[1] * s1[1];
+        double uu = 0.0;
+        for (int d = 0; d < dim; d++) {
+            s2[1 + d] = r * prm[1 + d];
+            if (d > 0) dke -= s1[1 + d] * s1[1 + d];
+            uu += prm[1 + d] * prm[1 + d];
+        }
+        dke *= 0.5 / s1[0];
+        dke += 0.5 * uu * r;
+        s2[nv - 1] = s1[nv - 1] + dke;
+        return face_flux(dim, gamma, c.p.compat, c.p.face_dissipation, s1, s2, nor, flux);
+    }
+    if (type == 8) {
+        // SubsonicInflowPtTtAngBdrFaceIntegrator::ComputeOuterInviscidState
+        // (:52-80), 2D: prm = cp, p0, T0, cos(theta), sin(theta)
+        const double cp = prm[0], p0 = prm[1], T0 = prm[2];
+        double V[3], vv = 0.0;
+        const double r1 = 1.0 / s1[0];
+        for (int d = 0; d < dim; d++) V[d] = compat ? s1[1 + d] * r1 : s1[1 + d] / s1[0];
+        for (int d = 0; d < dim; d++) vv += V[d] * V[d];
+        if (compat)
+            for (int d = 0; d < dim; d++) s1c[1 + d] = V[d];
+        const double p = gammaM1 * (s1[nv - 1] - 0.5 * s1[0] * vv);
+        double V_sq = 2.0 * cp * T0 * (1.0 - std::pow(p / p0, gammaM1 / gamma));
+        V_sq = std::max(0.0, V_sq);
+        s2[0] = gamma * gammaM1Inverse * p / (cp * T0 - 0.5 * V_sq);
+        for (int d = 0; d < dim; d++) s2[1 + d] = s2[0] * std::sqrt(V_sq) * prm[3 + d];
+        s2[nv - 1] = p * gammaM1Inverse + 0.5 * s2[0] * V_sq;
+        return face_flux(dim, gamma, c.p.compat, c.p.face_dissipation, s1c, s2, nor, flux);
+    }
+    if (type == 9) {
+        // RiemannInvariantBdrFaceIntegrator::ComputeOuterInviscidState
+        // (:43-112): prm = primitive outer state (rho, v, p)
+        const double gammaInverse = 1.0 / gamma;
+        unit_normal(dim, nor, un);
+        const double rho_o = prm[0], p_o = prm[nv - 1];
+        const double *V_o = prm + 1;
+        const double r1 = 1.0 / s1[0];
+        double V_i[3], Vn_i = 0.0, Vn_o = 0.0;
+        for (int d = 0; d < dim; d++) V_i[d] = compat ? s1[1 + d] * r1 : s1[1 + d] / s1[0];
+        for (int d = 0; d < dim; d++) { Vn_i += V_i[d] * un[d]; Vn_o += V_o[d] * un[d]; }
+        // ComputePressure(state1): in compat its view divides the (already
+        // divided) momenta once more, and V_i, a view of them, follows
+        double W[3], ww = 0.0;
+        for (int d = 0; d < dim; d++) W[d] = compat ? V_i[d] * r1 : V_i[d];
+        for (int d = 0; d < dim; d++) ww += W[d] * W[d];
+        const double p_i = gammaM1 * (s1[nv - 1] - 0.5 * s1[0] * ww);
+        if (compat)
+            for (int d = 0; d < dim; d++) { V_i[d] = W[d]; s1c[1 + d] = W[d]; }
+        const double a_o = sound_speed(p_o, rho_o, gamma), a_i = sound_speed(p_i, s1[0], gamma);
+        const double R_minus = (std::abs(Vn_o) >= a_o && Vn_i >= 0.0) ? Vn_i - 2.0 * a_i * gammaM1Inverse
+                                                                       : Vn_o - 2.0 * a_o * gammaM1Inverse;
+        const double R_plus = (std::abs(Vn_o) >= a_o && Vn_i < 0.0) ? Vn_o + 2.0 * a_o * gammaM1Inverse
+                                                                     : Vn_i + 2.0 * a_i * gammaM1Inverse;
+        const double Vn_b = 0.5 * (R_plus + R_minus);
+        const double a_b = 0.25 * gammaM1 * (R_plus - R_minus);
+        const double dVn_i = Vn_b - Vn_i, dVn_o = Vn_b - Vn_o;
+        s2[0] = (Vn_i < 0.0) ? std::pow(a_b * a_b * gammaInverse * rho_o / p_o, gammaM1Inverse) * rho_o
+                             : std::pow(a_b * a_b * gammaInverse * s1[0] / p_i, gammaM1Inverse) * s1[0];
+        double e2 = 0.0;
+        for (int d = 0; d < dim; d++) {
+            s2[1 + d] = (Vn_i >= 0.0) ? s2[0] * (V_i[d] + dVn_i * un[d]) : s2[0] * (V_o[d] + dVn_o * un[d]);
+            e2 = d == 0 ? s2[1] * s2[1] : e2 + s2[1 + d] * s2[1 + d];
+        }
+        const double p_b = a_b * a_b * s2[0] * gammaInverse;
+        e2 *= (0.5 / s2[0]);
+        e2 += p_b * gammaM1Inverse;
+        s2[nv - 1] = e2;
+        return face_flux(dim, gamma, c.p.compat, c.p.face_dissipation, s1c, s2, nor, flux);
+    }
     if (type == 1 || type == 3) {
         // SupersonicInflow / SpecifiedState: the prescribed state (:22-35, :21-35)
         for (int v = 0; v < nv; v++) s2[v] = c.bc[b][1 + v];
@@ -1294,12 +1388,22 @@ void *orc_create(const pdg_mesh *m, const pdg_params *p)
 
 void orc_destroy(void *h) { delete (Ctx *)h; }
 
+// Boundary condition `index`: its type and parameters as pdg_set_boundary
+// takes them (types 1, 3: conserved state; 6: p; 7: rho, velocity; 8: cp,
+// pt, Tt, theta, phi in degrees, stored as cp, pt, Tt, cos theta, sin theta;
+// 9: primitive state rho, velocity, p).
 void orc_set_boundary(void *h, int index, int type, const double *state)
 {
     Ctx &c = *(Ctx *)h;
     if (index < 0 || index >= 16) return;
+    const int n = type == 6 ? 1 : type == 7 ? 1 + c.dim : type == 8 ? 5 : c.nv;
     c.bc[index][0] = type;
-    for (int v = 0; v < c.nv; v++) c.bc[index][1 + v] = state ? state[v] : 0.0;
+    for (int v = 0; v < 7; v++) c.bc[index][1 + v] = (state && v < n) ? state[v] : 0.0;
+    if (type == 8) {
+        const double theta = c.bc[index][4];
+        c.bc[index][4] = std::cos(theta * M_PI / 180.0);
+        c.bc[index][5] = std::sin(theta * M_PI / 180.0);
+    }
 }
 
 void orc_rhs(void *h, const double *u, double *dudt) { orc::rhs(*(Ctx *)h, u, dudt); }

@@ -695,6 +695,23 @@ public:
     void Transform(const IntegrationPoint &, Vector &phys) { T1.Transform(ip1, phys); }
 };
 
+// Scalar function of the physical point (boundary data).
+class FunctionCoefficient {
+public:
+    FunctionCoefficient(std::function<real_t(const Vector &)> f) : F(std::move(f)) {}
+    void SetTime(real_t tt) { t = tt; }
+    template <class Tr> real_t Eval(Tr &T, const IntegrationPoint &ip)
+    {
+        Vector x;
+        T.Transform(ip, x);
+        return F(x);
+    }
+
+private:
+    std::function<real_t(const Vector &)> F;
+    real_t t = 0.0;
+};
+
 // Vector-valued function of the physical point (boundary states).
 class VectorFunctionCoefficient {
 public:

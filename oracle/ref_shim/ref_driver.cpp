@@ -21,6 +21,10 @@
 #include "SupersonicInflowBdrFaceIntegrator.hpp"
 #include "SupersonicOutflowBdrFaceIntegrator.hpp"
 #include "SymmetryBdrFaceIntegrator.hpp"
+#include "SubsonicOutflowPBdrFaceIntegrator.hpp"
+#include "SubsonicInflowRVBdrFaceIntegrator.hpp"
+#include "SubsonicInflowPtTtAngBdrFaceIntegrator.hpp"
+#include "RiemannInvariantBdrFaceIntegrator.hpp"
 #include "DGSEMIntegrator.hpp"
 #include "ModalBasis.hpp"
 #include "NavierStokesFlux.hpp"
@@ -299,13 +303,17 @@ void ref_destroy(void *h) { delete (RefCtx *)h; }
 
 // Boundary condition `index` as the reference's integrator of `type` (1
 // supersonic inflow, 2 supersonic outflow, 3 specified state, 4 slip wall,
-// 5 symmetry) with constant state `state` where the type takes one.
+// 5 symmetry, 6 subsonic outflow p, 7 subsonic inflow rho + V, 8 subsonic
+// inflow pt, Tt, theta, phi, 9 Riemann invariant from a primitive state)
+// with the constant data `state` where the type takes some.
 int ref_set_boundary(void *h, int index, int type, const double *state)
 {
     RefCtx &c = *(RefCtx *)h;
     if (index < 0 || index >= 16) return 1;
+    const bool full = type == 1 || type == 3 || type == 9;  // a whole (conserved or primitive) state
     Vector st(c.nv);
-    for (int v = 0; v < c.nv; v++) st(v) = state ? state[v] : 0.0;
+    for (int v = 0; v < c.nv; v++) st(v) = (state && full) ? state[v] : 0.0;
+    if (!state && type >= 6) return 1;
     BdrFaceIntegrator *b = nullptr;
     switch (type) {
     case 1: b = new SupersonicInflowBdrFaceIntegrator(c.lifting, *c.rsolver, c.Np, c.time, c.gamma, st); break;
@@ -313,6 +321,18 @@ int ref_set_boundary(void *h, int index, int type, const double *state)
     case 3: b = new SpecifiedStateBdrFaceIntegrator(c.lifting, *c.rsolver, c.Np, c.time, c.gamma, st); break;
     case 4: b = new SlipWallBdrFaceIntegrator(c.lifting, *c.rsolver, c.Np, c.time, c.gamma); break;
     case 5: b = new SymmetryBdrFaceIntegrator(c.lifting, *c.rsolver, c.Np, c.time, c.gamma); break;
+    case 6: b = new SubsonicOutflowPBdrFaceIntegrator(c.lifting, *c.rsolver, c.Np, c.time, c.gamma, state[0]); break;
+    case 7: {
+        Vector V(c.dim);
+        for (int d = 0; d < c.dim; d++) V(d) = state[1 + d];
+        b = new SubsonicInflowRVBdrFaceIntegrator(c.lifting, *c.rsolver, c.Np, c.time, c.gamma, state[0], V);
+        break;
+    }
+    case 8:
+        b = new SubsonicInflowPtTtAngBdrFaceIntegrator(c.lifting, *c.rsolver, c.Np, c.time, c.gamma, state[0], state[1],
+                                                       state[2], state[3], state[4]);
+        break;
+    case 9: b = new RiemannInvariantBdrFaceIntegrator(c.lifting, *c.rsolver, c.Np, c.time, c.gamma, st); break;
     default: return 1;
     }
     c.bfi[index].reset(b);

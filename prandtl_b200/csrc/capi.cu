@@ -602,17 +602,39 @@ int pdg_set_boundary(pdg_ctx *c, int index, int type, const double *state)
     if (!c) return PDG_ERR_ARG;
     if (index < 0 || index >= PDG_MAX_BOUNDARIES)
         return fail(c, PDG_ERR_ARG, "pdg_set_boundary: index %d outside [0, %d)", index, PDG_MAX_BOUNDARIES);
-    if (type < PDG_BC_SUPERSONIC_INFLOW || type > PDG_BC_SYMMETRY)
+    if (type < PDG_BC_SUPERSONIC_INFLOW || type > PDG_BC_RIEMANN_INVARIANT)
         return fail(c, PDG_ERR_ARG, "pdg_set_boundary: unknown boundary type %d", type);
+    if (type == PDG_BC_SUBSONIC_INFLOW_PTTT && c->dim != 2)
+        return fail(c, PDG_ERR_UNSUPPORTED, "pdg_set_boundary: the total-pressure inflow is 2D only");
     double slot[BC_SLOT] = {(double)type};
-    if (type == PDG_BC_SUPERSONIC_INFLOW || type == PDG_BC_SPECIFIED_STATE) {
-        if (!state) return fail(c, PDG_ERR_ARG, "pdg_set_boundary: type %d needs a state", type);
-        double msq = 0.0;
-        for (int d = 0; d < c->dim; d++) msq += state[1 + d] * state[1 + d];
-        const double p = (c->p.gamma - 1.0) * (state[c->dim + 1] - 0.5 * msq / state[0]);
-        if (!(state[0] > 0.0) || !(p > 0.0) || !std::isfinite(p))
-            return fail(c, PDG_ERR_ARG, "pdg_set_boundary: the state of condition %d is not physical", index);
-        for (int v = 0; v < c->nv; v++) slot[1 + v] = state[v];
+    const int n = type == PDG_BC_SUBSONIC_OUTFLOW_P ? 1
+                  : type == PDG_BC_SUBSONIC_INFLOW_RV ? 1 + c->dim
+                  : type == PDG_BC_SUBSONIC_INFLOW_PTTT ? 5
+                  : (type == PDG_BC_SUPERSONIC_INFLOW || type == PDG_BC_SPECIFIED_STATE || type == PDG_BC_RIEMANN_INVARIANT)
+                      ? c->nv : 0;
+    if (n > 0) {
+        if (!state) return fail(c, PDG_ERR_ARG, "pdg_set_boundary: type %d needs its data", type);
+        bool ok = true;
+        for (int v = 0; v < n; v++) ok = ok && std::isfinite(state[v]);
+        if (type == PDG_BC_SUPERSONIC_INFLOW || type == PDG_BC_SPECIFIED_STATE) {
+            double msq = 0.0;
+            for (int d = 0; d < c->dim; d++) msq += state[1 + d] * state[1 + d];
+            const double p = (c->p.gamma - 1.0) * (state[c->dim + 1] - 0.5 * msq / state[0]);
+            ok = ok && state[0] > 0.0 && p > 0.0;
+        } else if (type == PDG_BC_RIEMANN_INVARIANT) {
+            ok = ok && state[0] > 0.0 && state[c->nv - 1] > 0.0;
+        } else if (type == PDG_BC_SUBSONIC_INFLOW_PTTT) {
+            ok = ok && state[0] > 0.0 && state[1] > 0.0 && state[2] > 0.0;
+        } else {
+            ok = ok && state[0] > 0.0;
+        }
+        if (!ok) return fail(c, PDG_ERR_ARG, "pdg_set_boundary: the data of condition %d is not physical", index);
+        for (int v = 0; v < n; v++) slot[1 + v] = state[v];
+        if (type == PDG_BC_SUBSONIC_INFLOW_PTTT) {  // flow angle -> direction (the integrator's constructor)
+            const double theta = state[3];
+            slot[4] = std::cos(theta * M_PI / 180.0);
+            slot[5] = std::sin(theta * M_PI / 180.0);
+        }
     }
     std::memcpy(c->bc_host + index * BC_SLOT, slot, sizeof(slot));
     CK(cudaMemcpy(c->bc + index * BC_SLOT, slot, sizeof(slot), cudaMemcpyHostToDevice), "boundary table upload");

@@ -92,7 +92,8 @@ struct KParams {
 // entry -1 - b marks a boundary face with condition b of the table P.bc.
 constexpr int BC_SLOT = 8;
 constexpr int BC_SUPERSONIC_INFLOW = 1, BC_SUPERSONIC_OUTFLOW = 2, BC_SPECIFIED_STATE = 3, BC_SLIP_WALL = 4,
-              BC_SYMMETRY = 5;
+              BC_SYMMETRY = 5, BC_SUBSONIC_OUTFLOW_P = 6, BC_SUBSONIC_INFLOW_RV = 7, BC_SUBSONIC_INFLOW_PTTT = 8,
+              BC_RIEMANN_INVARIANT = 9;
 
 constexpr int pow2_at_least(int x) { return x <= 1 ? 1 : x <= 2 ? 2 : x <= 4 ? 4 : x <= 8 ? 8 : x <= 16 ? 16 : 32; }
 
@@ -901,6 +902,105 @@ __device__ __forceinline__ double face_terms_from(const KParams &P, const double
     return lam;
 }
 
+// Outer states of the subsonic conditions and the Riemann-invariant
+// condition; s1 enters as the interior state and leaves as the face flux
+// will see it (momenta divided in place for the reference-value operator).
+// prm: 6 p; 7 rho, velocity; 8 (2D) cp, pt, Tt, cos theta, sin theta;
+// 9 primitive outer state rho, velocity, p.  The normal is sgn e_D.
+//   6  SubsonicOutflowPBdrFaceIntegrator.cpp:17-31: interior state with
+//      E = p / (g-1) + rho |v|^2 / 2
+//   7  SubsonicInflowRVBdrFaceIntegrator.cpp:20-50: (rho, rho V) with the
+//      interior's E less its kinetic energy plus the outer one
+//   8  SubsonicInflowPtTtAngBdrFaceIntegrator.cpp:52-80: |V|^2 = 2 cp Tt
+//      (1 - (p/pt)^((g-1)/g)) along the flow angle, rho from p and
+//      cp Tt - |V|^2/2
+//   9  RiemannInvariantBdrFaceIntegrator.cpp:43-112: boundary normal speed
+//      and sound speed from the outgoing and incoming invariants
+template <int DIM, int D>
+__device__ __noinline__ void subsonic_outer_state(const KParams &P, int type, const double *prm, double sgn,
+                                                  double *s1, double *s2)
+{
+    constexpr int NV = DIM + 2;
+    const bool compat = P.compat != 0;
+    const double gm1 = P.gm1, gm1inv = P.gm1inv, gamma = P.gamma;
+    const double rho = s1[0], r1 = 1.0 / rho;
+    double V[DIM], vv = 0.0;
+#pragma unroll
+    for (int d = 0; d < DIM; d++) V[d] = compat ? s1[1 + d] * r1 : s1[1 + d] / rho;
+    if (type == BC_SUBSONIC_INFLOW_RV) {
+        const double r = prm[0];
+        s2[0] = r;
+        double dke = -s1[1] * s1[1], uu = 0.0;
+#pragma unroll
+        for (int d = 0; d < DIM; d++) {
+            s2[1 + d] = r * prm[1 + d];
+            if (d > 0) dke -= s1[1 + d] * s1[1 + d];
+            uu += prm[1 + d] * prm[1 + d];
+        }
+        dke *= 0.5 / rho;
+        dke += 0.5 * uu * r;
+        s2[NV - 1] = s1[NV - 1] + dke;
+        return;
+    }
+    if (type == BC_RIEMANN_INVARIANT) {
+        const double ginv = 1.0 / gamma;
+        const double rho_o = prm[0], p_o = prm[NV - 1];
+        const double Vn_i = sgn * V[D], Vn_o = sgn * prm[1 + D];
+        // ComputePressure(state1): once more through the view for compat
+        double W[DIM];
+#pragma unroll
+        for (int d = 0; d < DIM; d++) {
+            W[d] = compat ? V[d] * r1 : V[d];
+            vv += W[d] * W[d];
+        }
+        const double p_i = gm1 * (s1[NV - 1] - 0.5 * rho * vv);
+        if (compat) {
+#pragma unroll
+            for (int d = 0; d < DIM; d++) V[d] = s1[1 + d] = W[d];
+        }
+        const double a_o = sqrt(gamma * p_o / rho_o), a_i = sqrt(gamma * p_i / rho);
+        const double R_minus = (fabs(Vn_o) >= a_o && Vn_i >= 0.0) ? Vn_i - 2.0 * a_i * gm1inv : Vn_o - 2.0 * a_o * gm1inv;
+        const double R_plus = (fabs(Vn_o) >= a_o && Vn_i < 0.0) ? Vn_o + 2.0 * a_o * gm1inv : Vn_i + 2.0 * a_i * gm1inv;
+        const double Vn_b = 0.5 * (R_plus + R_minus), a_b = 0.25 * gm1 * (R_plus - R_minus);
+        const double dVn_i = Vn_b - Vn_i, dVn_o = Vn_b - Vn_o;
+        s2[0] = (Vn_i < 0.0) ? pow(a_b * a_b * ginv * rho_o / p_o, gm1inv) * rho_o
+                             : pow(a_b * a_b * ginv * rho / p_i, gm1inv) * rho;
+        double e2 = 0.0;
+#pragma unroll
+        for (int d = 0; d < DIM; d++) {
+            const double nd = d == D ? sgn : 0.0;
+            s2[1 + d] = (Vn_i >= 0.0) ? s2[0] * (V[d] + dVn_i * nd) : s2[0] * (prm[1 + d] + dVn_o * nd);
+            e2 = d == 0 ? s2[1] * s2[1] : e2 + s2[1 + d] * s2[1 + d];
+        }
+        const double p_b = a_b * a_b * s2[0] * ginv;
+        e2 *= (0.5 / s2[0]);
+        e2 += p_b * gm1inv;
+        s2[NV - 1] = e2;
+        return;
+    }
+#pragma unroll
+    for (int d = 0; d < DIM; d++) vv += V[d] * V[d];
+    if (compat) {
+#pragma unroll
+        for (int d = 0; d < DIM; d++) s1[1 + d] = V[d];
+    }
+    if (type == BC_SUBSONIC_OUTFLOW_P) {
+#pragma unroll
+        for (int v = 0; v < NV; v++) s2[v] = s1[v];
+        s2[NV - 1] = prm[0] * gm1inv + 0.5 * rho * vv;
+        return;
+    }
+    // BC_SUBSONIC_INFLOW_PTTT
+    const double cp = prm[0], p0 = prm[1], T0 = prm[2];
+    const double p = gm1 * (s1[NV - 1] - 0.5 * rho * vv);
+    double V_sq = 2.0 * cp * T0 * (1.0 - pow(p / p0, gm1 / gamma));
+    V_sq = fmax(0.0, V_sq);
+    s2[0] = gamma * gm1inv * p / (cp * T0 - 0.5 * V_sq);
+#pragma unroll
+    for (int d = 0; d < DIM; d++) s2[1 + d] = s2[0] * sqrt(V_sq) * prm[3 + d];
+    s2[NV - 1] = p * gm1inv + 0.5 * s2[0] * V_sq;
+}
+
 // Boundary face node of an element with interior trace s on its +D (sgn = 1)
 // or -D (sgn = -1) face, boundary condition b (BdrFaceIntegrator::
 // AssembleFaceVector, src/Integrators/BoundaryConditions/BdrFaceIntegrator.cpp:
@@ -959,16 +1059,25 @@ __device__ __noinline__ double boundary_node_terms(const KParams &P, const doubl
         F[1 + D] = ps * nrm;
         lam = sqrt(vsq) + an;
     } else {
-        double s2[NV];
+        // s1: the interior state as the face flux sees it.  The reference's
+        // subsonic conditions divide its momenta in place through Vector
+        // views (ComputePressure, BasicOperations.cpp:31-37, and their own
+        // velocity views); the reference-value operator keeps that.
+        double s1[NV], s2[NV];
         const bool given = type == BC_SUPERSONIC_INFLOW || type == BC_SPECIFIED_STATE;
 #pragma unroll
-        for (int v = 0; v < NV; v++) s2[v] = given ? bc[1 + v] : s[v];
+        for (int v = 0; v < NV; v++) {
+            s1[v] = s[v];
+            s2[v] = given ? bc[1 + v] : s[v];
+        }
         if (type == BC_SYMMETRY) s2[1 + D] = -s[1 + D];
-        const Prim<DIM> qa = make_prim<DIM>(s, P.gamma, P.gm1), qb = make_prim<DIM>(s2, P.gamma, P.gm1);
+        if (type >= BC_SUBSONIC_OUTFLOW_P)
+            subsonic_outer_state<DIM, D>(P, type, bc + 1, sgn, s1, s2);
+        const Prim<DIM> qa = make_prim<DIM>(s1, P.gamma, P.gm1), qb = make_prim<DIM>(s2, P.gamma, P.gm1);
         double ma[DIM], mb[DIM];
 #pragma unroll
         for (int d = 0; d < DIM; d++) {
-            ma[d] = s[1 + d];
+            ma[d] = s1[1 + d];
             mb[d] = s2[1 + d];
         }
         face_flux<DIM, D>(qa, qb, ma, mb, nrm, P.gm1inv, P.compat != 0, P.diss_scale, F);

@@ -126,3 +126,10 @@ def test_boundary_errors(cuda_device):
     with pytest.raises(pb.PdgError) as ei:
         op0.vjp(dev(u, cuda_device), dev(u, cuda_device))
     assert ei.value.code == 5
+    mesh3, _ = layout_case("3d_subsonic", 1)
+    op3 = pb.DGSEMOperator(mesh3)
+    with pytest.raises(pb.PdgError) as ei:      # total-pressure inflow: 2D only
+        op3.set_boundary(0, pb.BC_SUBSONIC_INFLOW_PTTT, [3.5, 3.0, 2.0, 0.0, 0.0])
+    assert ei.value.code == 5
+    with pytest.raises(pb.PdgError):            # outflow pressure must be positive
+        op3.set_boundary(1, pb.BC_SUBSONIC_OUTFLOW_P, [-1.0])
