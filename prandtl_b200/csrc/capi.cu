@@ -266,15 +266,18 @@ int kernel_config(int dim, int N, int kind, int64_t ne, int device, LaunchCfg *c
     }
     const int Np = N + 1, nfn = dim == 2 ? Np : Np * Np;
     if (ki.el_doubles == 0) {  // thread-per-face-node kernel
+        const int64_t threads = kind == KIND_FILTER_BOUNDS ? 32 * ne
+                                : kind == KIND_BOUNDARY ? ne : (kind == KIND_LIFT_FACE ? (int64_t)dim : 1) * ne * nfn;
+        // 256-thread blocks; 128 when that gives fewer than four blocks per
+        // SM, so that a small mesh still spreads evenly over the SMs
+        cfg->wpb = threads < 4LL * 256 * sms ? 4 : 8;
+        const int bs = 32 * cfg->wpb;
         int blocks_per_sm = 0;
-        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks_per_sm, ki.fn, 256, 0) != cudaSuccess) {
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks_per_sm, ki.fn, bs, 0) != cudaSuccess) {
             *why = "occupancy query failed";
             return PDG_ERR_CUDA;
         }
-        const int64_t threads = kind == KIND_FILTER_BOUNDS ? 32 * ne
-                                : kind == KIND_BOUNDARY ? ne : (kind == KIND_LIFT_FACE ? (int64_t)dim : 1) * ne * nfn;
-        cfg->wpb = 8;
-        cfg->grid = (int)std::max<int64_t>(1, std::min<int64_t>((threads + 255) / 256, (int64_t)sms * std::max(1, blocks_per_sm)));
+        cfg->grid = (int)std::max<int64_t>(1, std::min<int64_t>((threads + bs - 1) / bs, (int64_t)sms * std::max(1, blocks_per_sm)));
         cfg->smem = 0;
         return PDG_OK;
     }
