@@ -108,8 +108,9 @@ int pdg_destroy(pdg_ctx *ctx);
  * 490-798).  A neighbour entry -1 - b (0 <= b < PDG_MAX_BOUNDARIES) marks a
  * boundary face with condition b; every condition the mesh uses must be set
  * before the first evaluation (else PDG_ERR_ARG).  Euler only: pdg_create
- * returns PDG_ERR_UNSUPPORTED for a Navier-Stokes mesh with boundary faces,
- * and pdg_rhs_vjp for any mesh with them.  `state` holds the condition's
+ * returns PDG_ERR_UNSUPPORTED for a Navier-Stokes mesh with boundary faces;
+ * pdg_rhs_vjp differentiates conditions 1-5 and returns PDG_ERR_UNSUPPORTED
+ * for a mesh that uses 6-9.  `state` holds the condition's
  * data as listed beside each type (conserved, dim + 2 values, for the two
  * prescribed-state types) and may be NULL for types without data.  With
  * compat = 1 the subsonic and Riemann-invariant conditions keep the
@@ -260,6 +261,8 @@ int64_t pdg_launch_count(const pdg_ctx *ctx);
 #define PDG_KERNEL_ADJ_FACE_NS0 17  /* adjoint Navier-Stokes face kernels (17, 18, 19) */
 #define PDG_KERNEL_EULER_FACES 20   /* Euler volume + face terms (+ stage), fixed operator */
 #define PDG_KERNEL_NS_FACES  21     /* Navier-Stokes inviscid volume + all face terms (+ stage), fixed operator */
+#define PDG_KERNEL_BOUNDARY  22     /* boundary faces of the separate-face path (Euler) */
+#define PDG_KERNEL_ADJ_BOUNDARY 23  /* adjoint of the boundary faces (Euler) */
 int pdg_profile_enable(pdg_ctx *ctx, int on);
 int pdg_profile_read(pdg_ctx *ctx, int kind, double *total_ms, int64_t *launches);
 

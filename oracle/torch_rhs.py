@@ -89,7 +89,8 @@ def _norm(vsq):
 
 
 class TorchDGSEM:
-    """RHS of the fixed DGSEM operator on a periodic Cartesian mesh."""
+    """RHS of the fixed DGSEM operator on a Cartesian mesh: periodic, or with
+    the boundary conditions 1-5 of mesh.boundaries (Euler)."""
 
     def __init__(self, mesh: CartesianMesh, parabolic=False, blending=True, gamma=1.4, Pr=0.72, mu=0.0,
                  alpha_max=0.5, alpha_min=0.001, face_dissipation=1.0):
@@ -129,6 +130,12 @@ class TorchDGSEM:
         self.maxdeg = torch.tensor(md)
         self.T = 0.5 * 10 ** (-1.8 * self.N ** 0.25)
         self.nbr = torch.tensor(np.asarray(mesh.nbr, dtype=np.int64).reshape(self.ne, 2 * self.dim))
+        self.bcs = dict(getattr(mesh, "boundaries", None) or {})
+        if self.bcs and parabolic:
+            raise ValueError("boundary faces: Euler only")
+        for b, (typ, _) in self.bcs.items():
+            if typ not in (1, 2, 3, 4, 5):
+                raise ValueError(f"boundary condition {b}: type {typ} has no differentiable form here")
 
     # ---- layout ----
     def shape(self, u):
@@ -181,6 +188,31 @@ class TorchDGSEM:
             F.append(fm * vm[k] + (p_hat * nrm if k == d else 0.0) - lam * (sb[1 + k] - sa[1 + k]))
         F.append(fm * h - lam * diss)
         return F
+
+    def boundary_flux(self, s1, d, sgn, typ, state):
+        """Normal flux of a boundary face (src/Integrators/BoundaryConditions):
+        interior trace s1, outward normal sgn |n_d| e_d."""
+        nrm = sgn * self.area[d]
+        if typ == 4:  # slip wall (SlipWallBdrFaceIntegrator.cpp:15-58)
+            rho, vel, p = self.prims(s1)
+            vn = sgn * vel[d]
+            an = torch.sqrt(self.gamma * p / rho)
+            gp1 = 1.0 + self.gamma
+            K = self.gm1 / gp1 + 1.0
+            S = torch.sqrt(vn * vn + 8.0 / gp1 / rho * p * K)
+            ps_pos = p + 0.25 * vn * gp1 * rho * (vn + S)
+            X = torch.clamp(1.0 + 0.5 * self.gm1 * vn / an, min=0.0001)
+            ps_neg = p * X ** (2.0 * self.gamma / self.gm1)
+            ps = torch.where(vn > 0, ps_pos, ps_neg)
+            z = torch.zeros_like(ps)
+            return [z] + [ps * nrm if k == d else z for k in range(self.dim)] + [z]
+        if typ in (1, 3):
+            s2 = [torch.full_like(s1[0], float(state[v])) for v in range(self.nv)]
+        else:
+            s2 = list(s1)
+            if typ == 5:
+                s2[1 + d] = -s1[1 + d]
+        return self.face_flux(s1, s2, d, torch.full_like(s1[0], nrm))
 
     def entropy_vars(self, s):
         rho, vel, p = self.prims(s)
@@ -349,9 +381,11 @@ class TorchDGSEM:
         out = out / self.J
         if self.blending:
             out = out + a * self.fv_volume(s)
-        # faces
+        # faces (boundary faces: a negative neighbour entry -1 - b)
         for d in range(self.dim):
-            nb = self.nbr[:, 2 * d + 1]
+            nb_raw = self.nbr[:, 2 * d + 1]
+            inner = nb_raw >= 0
+            nb = torch.where(inner, nb_raw, torch.arange(self.ne))
             sa = self.trace(s, d, 1)
             sb = self.trace(s, d, 0)[:, nb]
             a1 = (torch.arange(self.ne) <= nb)
@@ -373,9 +407,22 @@ class TorchDGSEM:
                     dU1[1 + i] = dU1[1 + i] + fn
                     dU2[1 + i] = dU2[1 + i] - fn
             # element a (= e) gets dU1 when it is element 1, else dU2
+            mi = inner.reshape(sh)
             ca_ = torch.stack([torch.where(m1, dU1[v], dU2[v]) for v in range(self.nv)]) * self.face_scale
             cb_ = torch.stack([torch.where(m1, dU2[v], dU1[v]) for v in range(self.nv)]) * self.face_scale
+            ca_ = torch.where(mi, ca_, torch.zeros_like(ca_))
+            cb_ = torch.where(mi, cb_, torch.zeros_like(cb_))
             out = self.add_trace(out, d, 1, ca_)
             add_b = torch.zeros_like(cb_).index_add(1, nb, cb_)
             out = self.add_trace(out, d, 0, add_b)
+            for side in (0, 1):
+                nbs = self.nbr[:, 2 * d + side]
+                for b, (typ, state) in self.bcs.items():
+                    mb = (nbs == -1 - b).reshape(sh)
+                    if not bool(mb.any()):
+                        continue
+                    s1 = [self.trace(s[v], d, side) for v in range(self.nv)]
+                    F = self.boundary_flux(s1, d, 1.0 if side else -1.0, typ, state)
+                    add = torch.stack([torch.where(mb, -F[v], torch.zeros_like(F[v])) for v in range(self.nv)])
+                    out = self.add_trace(out, d, side, add * self.face_scale)
         return out.reshape(-1)

@@ -19,6 +19,7 @@ template <int N> static bool adj_info_n(int kind, KernelInfo *out)
     case KIND_ADJ_FACE_E1: out->fn = (const void *)&adj_face_kernel<2, N, 1, false>; break;
     case KIND_ADJ_FACE_NS0: out->fn = (const void *)&adj_face_kernel<2, N, 0, true>; break;
     case KIND_ADJ_FACE_NS1: out->fn = (const void *)&adj_face_kernel<2, N, 1, true>; break;
+    case KIND_ADJ_BOUNDARY: out->fn = (const void *)&adj_boundary_kernel<2, N>; break;
     default: return false;
     }
     return true;

@@ -21,6 +21,7 @@ template <int N> static bool adj_info_n(int kind, KernelInfo *out)
     case KIND_ADJ_FACE_NS1: out->fn = (const void *)&adj_face_kernel<3, N, 1, true>; break;
     case KIND_ADJ_FACE_E2: out->fn = (const void *)&adj_face_kernel<3, N, 2, false>; break;
     case KIND_ADJ_FACE_NS2: out->fn = (const void *)&adj_face_kernel<3, N, 2, true>; break;
+    case KIND_ADJ_BOUNDARY: out->fn = (const void *)&adj_boundary_kernel<3, N>; break;
     default: return false;
     }
     return true;

@@ -658,6 +658,7 @@ __global__ void __launch_bounds__(256) adj_face_kernel(const KParams P, const do
         const int64_t a = t / NFN;
         const int fn = (int)(t - a * NFN);
         const int64_t b = __ldg(P.nbr + a * 2 * DIM + 2 * D + 1);
+        if (b < 0) continue;  // boundary face: adj_boundary_kernel
         const int na = line_node<DIM, Np, D>(fn, N), nb = line_node<DIM, Np, D>(fn, 0);
         double sa[NV], sb[NV], la[NV], lb[NV];
 #pragma unroll
@@ -711,6 +712,119 @@ __global__ void __launch_bounds__(256) adj_face_kernel(const KParams P, const do
         for (int v = 0; v < NV; v++) {
             ubar[v * nn + a * NDOF + na] = pa[v] + ga[v];
             ubar[v * nn + b * NDOF + nb] = pb[v] + gb[v];
+        }
+    }
+}
+
+// Reverse of the slip wall's pressure flux F[1+D] = p* nrm (boundary_node_terms):
+// p* of the interior density, normal velocity vn = sgn m_D / rho and pressure
+// p = (g-1)(E - |m|^2 / (2 rho)); adds the conservative cotangent to g.
+template <int DIM>
+__device__ __forceinline__ void slip_wall_vjp(const KParams &P, const double *s, int D, double sgn, double psb,
+                                              double *g)
+{
+    const double rho = s[0], irho = 1.0 / rho;
+    double vsq = 0.0;
+#pragma unroll
+    for (int q = 0; q < DIM; q++) vsq += (s[1 + q] * irho) * (s[1 + q] * irho);
+    const double gm1 = P.gm1, gamma = P.gamma;
+    const double p = gm1 * (s[DIM + 1] - 0.5 * rho * vsq);
+    const double vn = sgn * s[1 + D] * irho;
+    const double an = sqrt(gamma * p * irho);
+    double dp, dvn, drho;  // partial derivatives of p*
+    if (vn > 0.0) {
+        const double gp1 = 1.0 + gamma, A = 8.0 / gp1 * (gm1 / gp1 + 1.0);
+        const double S = sqrt(vn * vn + A * p * irho);
+        dp = 1.0 + 0.125 * gp1 * vn * A / S;
+        dvn = 0.25 * gp1 * rho * (2.0 * vn + S + vn * vn / S);
+        drho = 0.25 * gp1 * vn * (vn + S) - 0.125 * gp1 * vn * A * p * irho / S;
+    } else {
+        const double E = 2.0 * gamma / gm1;
+        const double X0 = 1.0 + 0.5 * gm1 * vn / an;
+        if (X0 > 0.0001) {
+            const double XE1 = pow(X0, E - 1.0), pEX = p * E * XE1;
+            dp = XE1 * X0 + pEX * (-0.25 * gm1 * vn / (an * p));
+            dvn = pEX * 0.5 * gm1 / an;
+            drho = pEX * 0.25 * gm1 * vn / (an * rho);
+        } else {
+            dp = pow(0.0001, E);
+            dvn = drho = 0.0;
+        }
+    }
+    // through p(rho, m, E) and vn(rho, m_D)
+    g[0] += psb * (drho + dvn * (-vn * irho) + dp * 0.5 * gm1 * vsq);
+#pragma unroll
+    for (int q = 0; q < DIM; q++) g[1 + q] += psb * (dp * (-gm1 * s[1 + q] * irho) + (q == D ? dvn * sgn * irho : 0.0));
+    g[DIM + 1] += psb * dp * gm1;
+}
+
+// Adjoint of the boundary faces (Euler, conditions 1-5): one thread per
+// element walks its boundary faces, as boundary_kernel does forward, and
+// adds (dC/du)^T cot at each boundary node, C = -F(s, s2(s)) / (w0 J):
+// prescribed outer states are constants, outflow has s2 = s, symmetry
+// s2 = s with the normal momentum reversed, the slip wall's flux depends on
+// s through p*.
+template <int DIM, int N>
+__global__ void __launch_bounds__(256) adj_boundary_kernel(const KParams P, const double *__restrict__ cot,
+                                                           double *__restrict__ ubar, const double *__restrict__)
+{
+    using S = Shape<DIM, N>;
+    constexpr int Np = S::Np, NDOF = S::NDOF, NV = S::NV, NFN = S::NFN;
+    __shared__ double c[CONST_SLOTS];
+    load_consts(P.K, c, Np);
+    __syncthreads();
+    const int64_t nn = P.nnodes;
+    for (int64_t a = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; a < P.ne; a += (int64_t)gridDim.x * blockDim.x) {
+#pragma unroll 1
+        for (int f = 0; f < 2 * DIM; f++) {
+            const int32_t nb = __ldg(P.nbr + a * 2 * DIM + f);
+            if (nb >= 0) continue;
+            const int D = f >> 1, side = f & 1;
+            const double sgn = side ? 1.0 : -1.0;
+            const double *bc = P.bc + (-1 - nb) * BC_SLOT;
+            const int type = (int)bc[0];
+            const double nrm = sgn * C_AREA(c)[D];
+#pragma unroll 1
+            for (int fn = 0; fn < NFN; fn++) {
+                const int n = line_node_rt<DIM, Np>(D, fn, side ? N : 0);
+                double s1[NV], Fb[NV], g[NV];
+#pragma unroll
+                for (int v = 0; v < NV; v++) {
+                    s1[v] = __ldg(P.u + v * nn + a * NDOF + n);
+                    Fb[v] = -C_FACE(c) * __ldg(cot + v * nn + a * NDOF + n);
+                    g[v] = 0.0;
+                }
+                if (type == BC_SLIP_WALL) {
+                    slip_wall_vjp<DIM>(P, s1, D, sgn, Fb[1 + D] * nrm, g);
+                } else {
+                    double s2[NV];
+                    const bool given = type == BC_SUPERSONIC_INFLOW || type == BC_SPECIFIED_STATE;
+#pragma unroll
+                    for (int v = 0; v < NV; v++) s2[v] = given ? bc[1 + v] : s1[v];
+                    if (type == BC_SYMMETRY) s2[1 + D] = -s1[1 + D];
+                    const Prim<DIM> qa = make_prim<DIM>(s1, P.gamma, P.gm1), qb = make_prim<DIM>(s2, P.gamma, P.gm1);
+                    PBar<DIM> ab, bb;
+                    pbar_zero(ab);
+                    pbar_zero(bb);
+                    double mab[DIM], mbb[DIM];
+#pragma unroll
+                    for (int d = 0; d < DIM; d++) mab[d] = mbb[d] = 0.0;
+                    face_flux_vjp<DIM>(qa, qb, s1 + 1, s2 + 1, D, nrm, P.gamma, P.gm1inv, P.diss_scale, Fb, ab, bb, mab,
+                                       mbb);
+                    pbar_to_cons<DIM>(s1, ab, mab, P.gm1, g);
+                    if (!given) {
+                        double g2[NV];
+#pragma unroll
+                        for (int v = 0; v < NV; v++) g2[v] = 0.0;
+                        pbar_to_cons<DIM>(s2, bb, mbb, P.gm1, g2);
+                        if (type == BC_SYMMETRY) g2[1 + D] = -g2[1 + D];
+#pragma unroll
+                        for (int v = 0; v < NV; v++) g[v] += g2[v];
+                    }
+                }
+#pragma unroll
+                for (int v = 0; v < NV; v++) ubar[v * nn + a * NDOF + n] += g[v];
+            }
         }
     }
 }

@@ -267,7 +267,8 @@ int kernel_config(int dim, int N, int kind, int64_t ne, int device, LaunchCfg *c
     const int Np = N + 1, nfn = dim == 2 ? Np : Np * Np;
     if (ki.el_doubles == 0) {  // thread-per-face-node kernel
         const int64_t threads = kind == KIND_FILTER_BOUNDS ? 32 * ne
-                                : kind == KIND_BOUNDARY ? ne : (kind == KIND_LIFT_FACE ? (int64_t)dim : 1) * ne * nfn;
+                                : (kind == KIND_BOUNDARY || kind == KIND_ADJ_BOUNDARY) ? ne
+                                : (kind == KIND_LIFT_FACE ? (int64_t)dim : 1) * ne * nfn;
         // 256-thread blocks; 128 when that gives fewer than four blocks per
         // SM, so that a small mesh still spreads evenly over the SMs
         cfg->wpb = threads < 4LL * 256 * sms ? 4 : 8;
@@ -308,7 +309,8 @@ int kernel_config(int dim, int N, int kind, int64_t ne, int device, LaunchCfg *c
 bool kind_used(int kind, int dim, bool parabolic, bool filter)
 {
     if (kind == KIND_FILTER_BOUNDS || kind == KIND_FILTER) return filter;
-    if (kind >= KIND_ADJ_RHS && kind <= KIND_ADJ_FACE_NS2) return false;  // configured by the first pdg_rhs_vjp
+    if ((kind >= KIND_ADJ_RHS && kind <= KIND_ADJ_FACE_NS2) || kind == KIND_ADJ_BOUNDARY)
+        return false;  // configured by the first pdg_rhs_vjp
     const bool ns_kind = kind == KIND_NS || kind == KIND_NS_FACES || kind == KIND_LIFT || kind == KIND_LIFT_FACE ||
                          (kind >= KIND_FACE_NS0 && kind <= KIND_FACE_NS2);
     if (ns_kind != parabolic) return false;
@@ -880,7 +882,11 @@ int pdg_rhs_vjp(pdg_ctx *c, const double *u, const double *cot, double *ubar, vo
     if (!c) return PDG_ERR_ARG;
     if (!u || !cot || !ubar || ubar == u || ubar == cot) return fail(c, PDG_ERR_ARG, "pdg_rhs_vjp: null or aliased buffers");
     if (c->p.compat) return fail(c, PDG_ERR_UNSUPPORTED, "pdg_rhs_vjp: the adjoint is of the fixed operator (compat = 0)");
-    if (c->bc_used) return fail(c, PDG_ERR_UNSUPPORTED, "pdg_rhs_vjp: boundary faces are not differentiated");
+    for (int b = 0; b < PDG_MAX_BOUNDARIES; b++)
+        if ((c->bc_used >> b & 1u) && c->bc_host[b * BC_SLOT] > PDG_BC_SYMMETRY)
+            return fail(c, PDG_ERR_UNSUPPORTED,
+                        "pdg_rhs_vjp: boundary condition %d: only types 1-5 are differentiated", b);
+    if (c->bc_used & ~c->bc_set) return fail(c, PDG_ERR_ARG, "pdg_rhs_vjp: a boundary condition is not set");
     cudaStream_t s = (cudaStream_t)stream;
     int r;
     if (!c->adj_ready) {
@@ -893,6 +899,7 @@ int pdg_rhs_vjp(pdg_ctx *c, const double *u, const double *cot, double *ubar, vo
             if ((kind == KIND_ADJ_FACE_E2 || kind == KIND_ADJ_FACE_NS2) && c->dim < 3) continue;
             if ((r = configure_launch(c, kind))) return r;
         }
+        if (!c->p.parabolic && (r = configure_launch(c, KIND_ADJ_BOUNDARY))) return r;
         if (c->p.parabolic) {
             const size_t nfn = c->dim == 2 ? c->Np : c->Np * c->Np;
             if (cudaMalloc(&c->gcol, sizeof(double) * 2 * c->dim * c->ne * nfn * c->nv) != cudaSuccess)
@@ -913,6 +920,7 @@ int pdg_rhs_vjp(pdg_ctx *c, const double *u, const double *cot, double *ubar, vo
     } else {
         for (int d = 0; d < c->dim; d++)
             if ((r = launch_with(c, KIND_ADJ_FACE_E0 + d, P, a_cot, a_bar, a_g, s))) return r;
+        if (c->bc_used && (r = launch_with(c, KIND_ADJ_BOUNDARY, P, a_cot, a_bar, a_g, s))) return r;
     }
     return PDG_OK;
 }

@@ -27,7 +27,8 @@ enum KernelKind {
     KIND_EULER_FACES = 20,    // rhs_kernel<dim, N, false, true>: Euler volume + face terms (+ stage)
     KIND_NS_FACES = 21,       // rhs_kernel<dim, N, true, true>: NS inviscid volume + all face terms (+ stage)
     KIND_BOUNDARY = 22,       // boundary_kernel<dim, N>: boundary faces of the separate-face path (Euler)
-    KIND_COUNT = 23
+    KIND_ADJ_BOUNDARY = 23,   // adj_boundary_kernel<dim, N>: adjoint of the boundary faces (Euler)
+    KIND_COUNT = 24
 };
 
 struct KernelInfo {

@@ -132,3 +132,16 @@ def test_subsonic_conditions_differ_between_operators(name):
     a = oracle.Oracle(mesh, compat=1).rhs(u)
     b = oracle.Oracle(mesh, compat=0).rhs(u)
     assert np.abs(a - b).max() > 1e-6 * np.abs(a).max()
+
+
+@pytest.mark.parametrize("order", [2, 3])
+@pytest.mark.parametrize("name", ["2d_in_out_walls", "2d_symmetry_state", "3d_all"])
+def test_torch_reference_boundaries_match_oracle(name, order):
+    """The differentiable restatement (the adjoint's reference gradient) on
+    boundary layouts of conditions 1-5, fixed operator."""
+    import torch
+    from oracle.torch_rhs import TorchDGSEM
+    mesh, u = layout_case(name, order)
+    got = TorchDGSEM(mesh).rhs(torch.tensor(u)).numpy()
+    ref = oracle.Oracle(mesh, compat=0).rhs(u)
+    assert np.abs(got - ref).max() <= 1e-12 * np.abs(ref).max()
