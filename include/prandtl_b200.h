@@ -144,8 +144,10 @@ int pdg_rhs(pdg_ctx *ctx, const double *u, double *dudt, void *stream);
  * integrator that must keep its footprint fixed — so it takes no context and
  * calls no cudaMalloc, cudaFree or allocating library routine.  It computes
  * the same dudt = L(u) as pdg_rhs for the given mesh and parameters, except
- * that the wave-speed maximum starts from zero on every call.  u, dudt:
- * DEVICE pointers, byNODES, not aliased.
+ * that the wave-speed maximum starts from zero on every call; the mesh must
+ * be periodic (boundary faces need pdg_set_boundary on a context, so a
+ * negative neighbour entry returns PDG_ERR_ARG).  u, dudt: DEVICE pointers,
+ * byNODES, not aliased.
  *
  * All device scratch (constants, neighbour table, blending outputs, the
  * Navier-Stokes lifting jumps and face columns) lives in one file-scope
