@@ -98,7 +98,11 @@ void pdg_default_params(pdg_params *p);
  * DGSEMIntegrator.cpp:8-149; src/Simulation/Simulation.cpp:486-488).
  * Builds LGL D / D-hat / D-hat2, subcell normals, the modal Vandermonde and
  * uploads the neighbour table.  Allocates its scratch (alpha, eta, gradient
- * fields, error word) on the current device. */
+ * fields, error word) on the current device.  Two environment switches,
+ * read here, exist for measurements: PDG_ELEMENT_FACES=0 makes the fixed
+ * operator use the separate face kernels instead of face terms inside the
+ * volume kernel (same results to rounding), PDG_PREFETCH=0 turns off the
+ * lifting kernel's L2 prefetch of the next element. */
 int pdg_create(const pdg_mesh *mesh, const pdg_params *params, pdg_ctx **out);
 int pdg_destroy(pdg_ctx *ctx);
 
