@@ -269,6 +269,7 @@ int64_t pdg_launch_count(const pdg_ctx *ctx);
 #define PDG_KERNEL_NS_FACES  21     /* Navier-Stokes inviscid volume + all face terms (+ stage), fixed operator */
 #define PDG_KERNEL_BOUNDARY  22     /* boundary faces of the separate-face path (Euler) */
 #define PDG_KERNEL_ADJ_BOUNDARY 23  /* adjoint of the boundary faces (Euler) */
+#define PDG_KERNEL_EULER_FACES_BDR 24  /* PDG_KERNEL_EULER_FACES for meshes with boundary faces */
 int pdg_profile_enable(pdg_ctx *ctx, int on);
 int pdg_profile_read(pdg_ctx *ctx, int kind, double *total_ms, int64_t *launches);
 

@@ -493,7 +493,7 @@ int evaluate(pdg_ctx *c, int stage, double dt, const double *un, const double *u
     } else {
         if (c->p.filter && stage >= 0 && (r = launch(c, KIND_FILTER_BOUNDS, P, s))) return r;
         if (element_faces) {
-            if ((r = launch(c, KIND_EULER_FACES, P, s))) return r;
+            if ((r = launch(c, c->bc_used ? KIND_EULER_FACES_BDR : KIND_EULER_FACES, P, s))) return r;
         } else {
             if ((r = launch(c, KIND_EULER, P, s))) return r;
             for (int d = 0; d < c->dim; d++)

@@ -28,7 +28,8 @@ enum KernelKind {
     KIND_NS_FACES = 21,       // rhs_kernel<dim, N, true, true>: NS inviscid volume + all face terms (+ stage)
     KIND_BOUNDARY = 22,       // boundary_kernel<dim, N>: boundary faces of the separate-face path (Euler)
     KIND_ADJ_BOUNDARY = 23,   // adj_boundary_kernel<dim, N>: adjoint of the boundary faces (Euler)
-    KIND_COUNT = 24
+    KIND_EULER_FACES_BDR = 24,  // rhs_kernel<dim, N, false, true, true>: KIND_EULER_FACES for meshes with boundaries
+    KIND_COUNT = 25
 };
 
 struct KernelInfo {

@@ -537,7 +537,7 @@ __device__ __forceinline__ double face_terms_from(const KParams &P, const double
 // orientation of the face is C_FACE coef (fa + fb)/2 |n_D| for element a and
 // its negative for b (fixed operator only: the reference-value operator's
 // face fluxes read velocities from the momentum slots).
-template <int DIM, int N, bool NS, int D>
+template <int DIM, int N, bool NS, int D, bool BDR>
 __device__ __forceinline__ void face_terms_dir(const KParams &P, const double *c, double *acc, int64_t e,
                                                const int32_t *enb, int gl, bool valid, double coef, double &lam)
 {
@@ -553,7 +553,7 @@ __device__ __forceinline__ void face_terms_dir(const KParams &P, const double *c
                 if (t < 2 * NFN) {
                     const int side = t >= NFN, fn = side ? t - NFN : t;
                     const int64_t other = enb[2 * D + side];
-                    if (NS || other >= 0) {  // NS meshes have no boundary faces
+                    if (!BDR || other >= 0) {  // BDR: the mesh has boundary faces (Euler)
                         load_face_in<DIM, N, D, false>(P, side ? e : other, side ? other : e, fn, in[r]);
                     } else {
                         // boundary face: this element's trace only
@@ -572,7 +572,7 @@ __device__ __forceinline__ void face_terms_dir(const KParams &P, const double *c
                     const int64_t a = side ? e : other, b = side ? other : e;
                     const int n = sp<DIM, Np>(line_node<DIM, Np, D>(fn, side ? N : 0));
                     double C[NV];
-                    if (NS || other >= 0) {
+                    if (!BDR || other >= 0) {
                         face_terms_from<DIM, N, D, false>(P, c, a <= b, in[r], coef, C);
 #pragma unroll
                         for (int v = 0; v < NV; v++) {
@@ -636,7 +636,7 @@ __device__ __forceinline__ void face_terms_dir(const KParams &P, const double *c
 // face terms include the central viscous flux of both sides' face columns.
 // Each face is thus evaluated twice, once by each of its elements, on the
 // same inputs in the same order, so both get the same value.
-template <int DIM, int N, bool NS, bool FACES, bool PRELOAD = true>
+template <int DIM, int N, bool NS, bool FACES, bool PRELOAD = true, bool BDR = false>
 __device__ __forceinline__ void rhs_tile(const KParams &P, const double *c, double *pr, int64_t e_base, int grp,
                                          int gl, bool lane_used, unsigned int &flags, double &lam)
 {
@@ -726,9 +726,9 @@ __device__ __forceinline__ void rhs_tile(const KParams &P, const double *c, doub
     }
     __syncwarp();
     if (PRELOAD) {
-        face_terms_dir<DIM, N, NS, 0>(P, c, acc, e, enb, gl, valid, coef, lam);
-        face_terms_dir<DIM, N, NS, 1>(P, c, acc, e, enb, gl, valid, coef, lam);
-        if (DIM == 3) face_terms_dir<DIM, N, NS, (DIM == 3 ? 2 : 0)>(P, c, acc, e, enb, gl, valid, coef, lam);
+        face_terms_dir<DIM, N, NS, 0, BDR>(P, c, acc, e, enb, gl, valid, coef, lam);
+        face_terms_dir<DIM, N, NS, 1, BDR>(P, c, acc, e, enb, gl, valid, coef, lam);
+        if (DIM == 3) face_terms_dir<DIM, N, NS, (DIM == 3 ? 2 : 0), BDR>(P, c, acc, e, enb, gl, valid, coef, lam);
     } else {
         // one face node at a time (Euler): the batched sweep's register
         // variants are tuned for this form
@@ -777,7 +777,9 @@ template <int DIM, int N> struct RhsOccupancy {
     static constexpr int min_blocks = (DIM == 3 && N == 3) ? 4 : 1;
 };
 
-template <int DIM, int N, bool NS, bool FACES = false>
+// BDR: a variant for meshes with boundary faces (Euler), whose boundary
+// branch would otherwise cost registers in every face loop.
+template <int DIM, int N, bool NS, bool FACES = false, bool BDR = false>
 __global__ void __launch_bounds__(128, RhsOccupancy<DIM, N>::min_blocks) rhs_kernel(const KParams P)
 {
     using S = Shape<DIM, N>;
@@ -795,7 +797,7 @@ __global__ void __launch_bounds__(128, RhsOccupancy<DIM, N>::min_blocks) rhs_ker
     unsigned int flags = 0;
     double lam = 0.0;
     for (int64_t wt = (int64_t)blockIdx.x * wpb + warp; wt < P.nwt; wt += wstride)
-        rhs_tile<DIM, N, NS, FACES>(P, c, pr, wt * EPW, grp, gl, lane_used, flags, lam);
+        rhs_tile<DIM, N, NS, FACES, true, BDR>(P, c, pr, wt * EPW, grp, gl, lane_used, flags, lam);
     lam = group_max<32>(lam);
     if (lane == 0) atomic_max_pos(P.lam_bits, lam);
     flags = __reduce_or_sync(0xffffffffu, flags);
