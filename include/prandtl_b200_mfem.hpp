@@ -59,6 +59,14 @@ public:
         check_status(pdg_max_char_speed(ctx_, &lam), ctx_, "pdg_max_char_speed");
         return lam;
     }
+    // DGSEMOperator::AddBdrFaceIntegrator (DGSEMOperator.cpp:593) for the
+    // faces marked -1 - index in the neighbour table; `data` as
+    // pdg_set_boundary takes it (may be empty for types without data)
+    void SetBoundary(int index, int type, const mfem::Vector &data)
+    {
+        check_status(pdg_set_boundary(ctx_, index, type, data.Size() ? data.GetData() : nullptr), ctx_,
+                     "pdg_set_boundary");
+    }
     pdg_ctx *context() const { return ctx_; }
 
 private:

@@ -19,6 +19,9 @@ int main()
     }
     try {
         prandtl_b200::GpuDGSEMOperator op(m, p);
+        double pout[1] = {2.0};
+        mfem::Vector bdata(pout, 1);
+        op.SetBoundary(0, PDG_BC_SUBSONIC_OUTFLOW_P, bdata);  // compiles the boundary setter
         prandtl_b200::GpuRK3SSPSolver ode;
         ode.Init(op);
         std::printf("constructed %d\n", op.Height());
