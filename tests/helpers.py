@@ -20,6 +20,10 @@ def load_golden(name):
     mesh = periodic_box(int(z["dim"]), int(z["order"]), tuple(int(v) for v in z["n"]),
                         tuple(float(v) for v in z["lo"]), tuple(float(v) for v in z["hi"]))
     params = dict(parabolic=int(z["parabolic"]), mu=float(z["mu"]), Pr=float(z["Pr"]))
+    if "nbr" in z.files:  # boundary faces and their conditions
+        mesh.nbr = z["nbr"].reshape(mesh.num_elements, 2 * mesh.dim)
+        mesh.boundaries = {int(b): (int(t), (z["bc_data"][r, :int(n)] if int(n) else None))
+                           for r, (b, t, n) in enumerate(zip(z["bc_index"], z["bc_type"], z["bc_n"]))}
     return mesh, params, {k: z[k] for k in z.files}
 
 
