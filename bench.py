@@ -163,8 +163,19 @@ def cpu_baseline(mesh, u, params, seconds):
         el = time.perf_counter() - t0
         if el >= seconds or steps >= 50:
             break
-    return {"value": mesh.size * 3 * steps / el, "unit": UNIT, "cores": cores, "kind": "port",
-            "sample": f"{steps} SSP-RK3 steps of the full workload ({el:.1f} s, OpenMP over elements)"}
+    out = {"value": mesh.size * 3 * steps / el, "unit": UNIT, "cores": cores, "kind": "port",
+           "sample": f"{steps} SSP-RK3 steps of the full workload ({el:.1f} s, OpenMP over elements)"}
+    # the same oracle on one core: one SSP-RK3 stage of the full workload
+    oracle.lib().orc_set_num_threads(1)
+    try:
+        t0 = time.perf_counter()
+        o.rk_stage(0, dt, x, x)
+        el1 = time.perf_counter() - t0
+    finally:
+        oracle.lib().orc_set_num_threads(cores)
+    out["single_core"] = {"value": mesh.size / el1, "unit": UNIT, "cores": 1,
+                          "sample": f"one RK stage of the full workload ({el1:.2f} s)"}
+    return out
 
 
 def run_ours(args):
