@@ -67,6 +67,9 @@ class CartesianMesh:
     spacing: tuple[float, ...] | None = None  # element extents, when not (hi - lo) / n exactly
     # boundary conditions of negative neighbour entries -1 - b: {b: (type, state or None)}
     boundaries: dict | None = None
+    # the grid cells (x-fastest index into the n grid) that are elements, when
+    # the domain is a subset of the box (a step, a channel with an obstacle)
+    cells: np.ndarray | None = None
 
     @property
     def Np(self) -> int:
@@ -78,7 +81,7 @@ class CartesianMesh:
 
     @property
     def num_elements(self) -> int:
-        return int(np.prod(self.n))
+        return int(np.prod(self.n)) if self.cells is None else int(len(self.cells))
 
     @property
     def num_nodes(self) -> int:
@@ -104,6 +107,8 @@ class CartesianMesh:
         x1, _ = gll_nodes(self.Np)
         Np, dim = self.Np, self.dim
         e = np.arange(self.num_elements) if elements is None else np.asarray(elements, dtype=np.int64)
+        if self.cells is not None:
+            e = np.asarray(self.cells, dtype=np.int64)[e]
         ne = e.size
         eidx = []
         r = e.copy()
@@ -149,13 +154,17 @@ def periodic_box(dim: int, order: int, n, lo, hi) -> CartesianMesh:
     return CartesianMesh(dim, order, n, tuple(lo), tuple(hi), nbr)
 
 
-def box(dim: int, order: int, n, lo, hi, bdr=None, boundaries=None) -> CartesianMesh:
+def box(dim: int, order: int, n, lo, hi, bdr=None, boundaries=None, keep=None, cut=None) -> CartesianMesh:
     """Box [lo, hi] with n[d] elements per direction.  bdr[d] = None keeps
     direction d periodic; bdr[d] = (b_lo, b_hi) makes its -d and +d sides
     boundary faces with conditions b_lo and b_hi (neighbour entry -1 - b).
     ``boundaries`` maps each condition to (type, state), the arguments of
     DGSEMOperator.set_boundary (the reference's boundary attributes and
-    BdrFaceIntegrators, src/Simulation/Simulation.cpp:490-798)."""
+    BdrFaceIntegrators, src/Simulation/Simulation.cpp:490-798).  ``keep``, a
+    boolean array of shape n (index [i_x, i_y(, i_z)]), keeps only those
+    cells as elements (in the box's x-fastest order): a face towards a removed
+    cell becomes a boundary face with condition ``cut`` (a forward or
+    backward facing step, an obstacle)."""
     m = periodic_box(dim, order, n, lo, hi)
     if bdr is None:
         bdr = [None] * dim
@@ -172,4 +181,20 @@ def box(dim: int, order: int, n, lo, hi, bdr=None, boundaries=None) -> Cartesian
         nbr[i == m.n[d] - 1, 2 * d + 1] = -1 - int(b_hi)
     m.nbr = nbr
     m.boundaries = dict(boundaries or {})
+    if keep is not None:
+        k = np.asarray(keep, dtype=bool)
+        if k.shape != tuple(m.n):
+            raise ValueError(f"keep has shape {k.shape}, the grid {tuple(m.n)}")
+        flat = k.reshape(-1, order="F")            # x-fastest cell order
+        cells = np.nonzero(flat)[0]
+        if cells.size == 0 or cut is None:
+            raise ValueError("keep needs at least one cell and a boundary condition `cut`")
+        new = np.full(flat.size, -1, dtype=np.int64)
+        new[cells] = np.arange(cells.size)
+        sub = nbr[cells].astype(np.int64)
+        inner = sub >= 0
+        tgt = np.where(inner, sub, 0)
+        sub = np.where(inner, np.where(flat[tgt], new[tgt], -1 - int(cut)), sub)
+        m.nbr = sub.astype(np.int32)
+        m.cells = cells
     return m

@@ -75,6 +75,12 @@ def test_navier_stokes_mesh_with_boundaries_is_rejected():
         oracle.Oracle(mesh, parabolic=1, mu=0.01)
 
 
+def _step_keep(n):
+    keep = np.ones(n, dtype=bool)
+    keep[2:, 0] = False
+    return keep
+
+
 def layouts():
     """Boundary layouts covering every condition type on every side."""
     fs2 = np.array([1.2, 0.3, -0.2, 2.6])
@@ -92,6 +98,10 @@ def layouts():
         "2d_subsonic": (2, dict(bdr=[(0, 1), (2, 3)], boundaries={
             0: (pb.BC_SUBSONIC_INFLOW_PTTT, [3.5, 3.0, 2.0, 10.0, 0.0]), 1: (pb.BC_SUBSONIC_OUTFLOW_P, [2.2]),
             2: (pb.BC_RIEMANN_INVARIANT, [1.0, 0.3, -0.1, 2.0]), 3: (pb.BC_SUBSONIC_INFLOW_RV, [1.3, 0.2, 0.05])})),
+        # forward-facing step: the bottom row is removed from x = -1 + 2/5 * 2 on
+        "2d_step": (2, dict(bdr=[(0, 1), (2, 2)], keep=_step_keep((5, 4)), cut=2, boundaries={
+            0: (pb.BC_SUPERSONIC_INFLOW, np.array([1.4, 4.2, 0.0, 8.8])), 1: (pb.BC_SUPERSONIC_OUTFLOW, None),
+            2: (pb.BC_SLIP_WALL, None)})),
         "3d_subsonic": (3, dict(bdr=[(0, 1), (2, 2), None], boundaries={
             0: (pb.BC_SUBSONIC_INFLOW_RV, [1.2, 0.1, 0.05, -0.02]), 1: (pb.BC_SUBSONIC_OUTFLOW_P, [2.0]),
             2: (pb.BC_RIEMANN_INVARIANT, [1.0, 0.2, 0.1, -0.1, 2.0])})),
@@ -100,6 +110,9 @@ def layouts():
 
 def layout_case(name, order):
     dim, kw = layouts()[name]
+    if "keep" in kw:
+        mesh = box(2, order, kw["keep"].shape, (-1.0, -1.0), (1.0, 1.0), **kw)
+        return mesh, rough(cases.kelvin_helmholtz(mesh), mesh, 11, 0.05, 0.02)
     if dim == 2:
         mesh = box(2, order, (4, 3), (-1.0, -1.0), (1.0, 1.0), **kw)
         u = cases.kelvin_helmholtz(periodic_box(2, order, (4, 3), -1.0, 1.0))
@@ -135,7 +148,7 @@ def test_subsonic_conditions_differ_between_operators(name):
 
 
 @pytest.mark.parametrize("order", [2, 3])
-@pytest.mark.parametrize("name", ["2d_in_out_walls", "2d_symmetry_state", "3d_all"])
+@pytest.mark.parametrize("name", ["2d_in_out_walls", "2d_symmetry_state", "3d_all", "2d_step"])
 def test_torch_reference_boundaries_match_oracle(name, order):
     """The differentiable restatement (the adjoint's reference gradient) on
     boundary layouts of conditions 1-5, fixed operator."""

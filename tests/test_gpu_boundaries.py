@@ -138,7 +138,7 @@ def test_boundary_errors(cuda_device):
 
 @pytest.mark.parametrize("blending", [1, 0])
 @pytest.mark.parametrize("order", [2, 3])
-@pytest.mark.parametrize("name", ["2d_in_out_walls", "2d_symmetry_state", "3d_all"])
+@pytest.mark.parametrize("name", ["2d_in_out_walls", "2d_symmetry_state", "3d_all", "2d_step"])
 def test_gpu_vjp_with_boundaries_matches_autograd(name, order, blending, cuda_device):
     """pdg_rhs_vjp on meshes with boundary conditions 1-5 against torch
     autograd through the differentiable restatement (fixed operator)."""
