@@ -113,8 +113,7 @@ int pdg_destroy(pdg_ctx *ctx);
  * boundary face with condition b; every condition the mesh uses must be set
  * before the first evaluation (else PDG_ERR_ARG).  Euler only: pdg_create
  * returns PDG_ERR_UNSUPPORTED for a Navier-Stokes mesh with boundary faces;
- * pdg_rhs_vjp differentiates conditions 1-5 and returns PDG_ERR_UNSUPPORTED
- * for a mesh that uses 6-9.  `state` holds the condition's
+ * pdg_rhs_vjp differentiates every condition (fixed operator).  `state` holds the condition's
  * data as listed beside each type (conserved, dim + 2 values, for the two
  * prescribed-state types) and may be NULL for types without data.  With
  * compat = 1 the subsonic and Riemann-invariant conditions keep the

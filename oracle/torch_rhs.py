@@ -134,8 +134,10 @@ class TorchDGSEM:
         if self.bcs and parabolic:
             raise ValueError("boundary faces: Euler only")
         for b, (typ, _) in self.bcs.items():
-            if typ not in (1, 2, 3, 4, 5):
-                raise ValueError(f"boundary condition {b}: type {typ} has no differentiable form here")
+            if typ not in range(1, 10):
+                raise ValueError(f"boundary condition {b}: unknown type {typ}")
+            if typ == 8 and self.dim != 2:
+                raise ValueError("the total-pressure inflow is 2D only")
 
     # ---- layout ----
     def shape(self, u):
@@ -206,13 +208,56 @@ class TorchDGSEM:
             ps = torch.where(vn > 0, ps_pos, ps_neg)
             z = torch.zeros_like(ps)
             return [z] + [ps * nrm if k == d else z for k in range(self.dim)] + [z]
-        if typ in (1, 3):
+        if typ >= 6:
+            s2 = self.subsonic_outer_state(s1, d, sgn, typ, [float(x) for x in state])
+        elif typ in (1, 3):
             s2 = [torch.full_like(s1[0], float(state[v])) for v in range(self.nv)]
         else:
             s2 = list(s1)
             if typ == 5:
                 s2[1 + d] = -s1[1 + d]
         return self.face_flux(s1, s2, d, torch.full_like(s1[0], nrm))
+
+    def subsonic_outer_state(self, s1, d, sgn, typ, prm):
+        """Outer states of the subsonic and Riemann-invariant conditions as
+        the fixed operator takes them (the interior state as it is)."""
+        g, gm1 = self.gamma, self.gm1
+        rho = s1[0]
+        V = [s1[1 + q] / rho for q in range(self.dim)]
+        vv = sum(v * v for v in V)
+        msq = sum(s1[1 + q] * s1[1 + q] for q in range(self.dim))
+        if typ == 6:   # SubsonicOutflowPBdrFaceIntegrator.cpp:17-31
+            return list(s1[:-1]) + [prm[0] / gm1 + 0.5 * rho * vv]
+        if typ == 7:   # SubsonicInflowRVBdrFaceIntegrator.cpp:20-50
+            r = prm[0]
+            uu = sum(prm[1 + q] ** 2 for q in range(self.dim))
+            z = torch.zeros_like(rho)
+            return ([z + r] + [z + r * prm[1 + q] for q in range(self.dim)]
+                    + [s1[-1] - 0.5 * msq / rho + 0.5 * uu * r])
+        p = gm1 * (s1[-1] - 0.5 * rho * vv)
+        if typ == 8:   # SubsonicInflowPtTtAngBdrFaceIntegrator.cpp:52-80 (2D)
+            cp, p0, T0, th = prm[0], prm[1], prm[2], prm[3] * np.pi / 180.0
+            dirs = [np.cos(th), np.sin(th)]
+            V_sq = torch.clamp(2.0 * cp * T0 * (1.0 - (p / p0) ** (gm1 / g)), min=0.0)
+            r2 = g / gm1 * p / (cp * T0 - 0.5 * V_sq)
+            return [r2] + [r2 * torch.sqrt(V_sq) * dirs[q] for q in range(self.dim)] + [p / gm1 + 0.5 * r2 * V_sq]
+        # typ 9, RiemannInvariantBdrFaceIntegrator.cpp:43-112: prm = rho, v, p
+        rho_o, p_o, V_o = prm[0], prm[-1], prm[1:1 + self.dim]
+        nq = [sgn if q == d else 0.0 for q in range(self.dim)]
+        Vn_i, Vn_o = sgn * V[d], sgn * V_o[d]
+        a_o = float(np.sqrt(g * p_o / rho_o))
+        a_i = torch.sqrt(g * p / rho)
+        sup = abs(Vn_o) >= a_o
+        R_minus = torch.where(sup & (Vn_i >= 0), Vn_i - 2.0 * a_i / gm1, Vn_o - 2.0 * a_o / gm1)
+        R_plus = torch.where(sup & (Vn_i < 0), Vn_o + 2.0 * a_o / gm1, Vn_i + 2.0 * a_i / gm1)
+        Vn_b = 0.5 * (R_plus + R_minus)
+        a_b = 0.25 * gm1 * (R_plus - R_minus)
+        r2 = torch.where(Vn_i < 0, (a_b * a_b / g * rho_o / p_o) ** (1.0 / gm1) * rho_o,
+                         (a_b * a_b / g * rho / p) ** (1.0 / gm1) * rho)
+        m2 = [torch.where(Vn_i >= 0, r2 * (V[q] + (Vn_b - Vn_i) * nq[q]), r2 * (V_o[q] + (Vn_b - Vn_o) * nq[q]))
+              for q in range(self.dim)]
+        p_b = a_b * a_b * r2 / g
+        return [r2] + m2 + [0.5 * sum(m * m for m in m2) / r2 + p_b / gm1]
 
     def entropy_vars(self, s):
         rho, vel, p = self.prims(s)

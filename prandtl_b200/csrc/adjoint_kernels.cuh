@@ -758,12 +758,110 @@ __device__ __forceinline__ void slip_wall_vjp(const KParams &P, const double *s,
     g[DIM + 1] += psb * dp * gm1;
 }
 
-// Adjoint of the boundary faces (Euler, conditions 1-5): one thread per
+// Forward-mode number (value, derivative) for the Jacobian of the subsonic
+// and Riemann-invariant outer states with respect to the interior state.
+struct Dual {
+    double v, d;
+};
+__device__ __forceinline__ Dual operator+(Dual a, Dual b) { return {a.v + b.v, a.d + b.d}; }
+__device__ __forceinline__ Dual operator-(Dual a, Dual b) { return {a.v - b.v, a.d - b.d}; }
+__device__ __forceinline__ Dual operator-(Dual a) { return {-a.v, -a.d}; }
+__device__ __forceinline__ Dual operator*(Dual a, Dual b) { return {a.v * b.v, a.d * b.v + a.v * b.d}; }
+__device__ __forceinline__ Dual operator*(double c, Dual a) { return {c * a.v, c * a.d}; }
+__device__ __forceinline__ Dual operator*(Dual a, double c) { return {c * a.v, c * a.d}; }
+__device__ __forceinline__ Dual operator+(double c, Dual a) { return {c + a.v, a.d}; }
+__device__ __forceinline__ Dual operator-(double c, Dual a) { return {c - a.v, -a.d}; }
+__device__ __forceinline__ Dual operator/(Dual a, Dual b)
+{
+    const double q = a.v / b.v;
+    return {q, (a.d - q * b.d) / b.v};
+}
+__device__ __forceinline__ Dual operator/(Dual a, double c) { return {a.v / c, a.d / c}; }
+__device__ __forceinline__ Dual dsqrt(Dual a)
+{
+    const double r = sqrt(a.v);
+    return {r, r > 0.0 ? a.d * 0.5 / r : 0.0};
+}
+__device__ __forceinline__ Dual dpow(Dual a, double e)
+{
+    const double pv = pow(a.v, e);
+    return {pv, a.d * e * pow(a.v, e - 1.0)};
+}
+
+// The fixed operator's outer states of conditions 6-9 (boundary_node_terms
+// with compat = 0) in forward mode: type 6 subsonic outflow at a pressure, 7
+// inflow from rho and V, 8 (2D) inflow from total pressure, temperature and
+// direction, 9 Riemann invariants; prm as the boundary table stores it.
+template <int DIM>
+__device__ void outer_state_dual(const KParams &P, int type, const double *prm, int D, double sgn, const Dual *s1,
+                                 Dual *s2)
+{
+    constexpr int NV = DIM + 2;
+    const double gamma = P.gamma, gm1 = P.gm1, gm1inv = P.gm1inv;
+    const Dual rho = s1[0];
+    Dual V[DIM], vv = {0.0, 0.0}, msq = {0.0, 0.0};
+    for (int q = 0; q < DIM; q++) {
+        V[q] = s1[1 + q] / rho;
+        vv = vv + V[q] * V[q];
+        msq = msq + s1[1 + q] * s1[1 + q];
+    }
+    if (type == BC_SUBSONIC_OUTFLOW_P) {
+        for (int v = 0; v < NV - 1; v++) s2[v] = s1[v];
+        s2[NV - 1] = prm[0] * gm1inv + 0.5 * (rho * vv);
+        return;
+    }
+    if (type == BC_SUBSONIC_INFLOW_RV) {
+        const double r = prm[0];
+        double uu = 0.0;
+        s2[0] = {r, 0.0};
+        for (int q = 0; q < DIM; q++) {
+            s2[1 + q] = {r * prm[1 + q], 0.0};
+            uu += prm[1 + q] * prm[1 + q];
+        }
+        s2[NV - 1] = s1[NV - 1] - 0.5 * (msq / rho) + Dual{0.5 * uu * r, 0.0};
+        return;
+    }
+    const Dual p = gm1 * (s1[NV - 1] - 0.5 * (rho * vv));
+    if (type == BC_SUBSONIC_INFLOW_PTTT) {
+        const double cp = prm[0], p0 = prm[1], T0 = prm[2];
+        Dual V_sq = (2.0 * cp * T0) * (1.0 - dpow(p / p0, gm1 / gamma));
+        if (V_sq.v < 0.0) V_sq = {0.0, 0.0};
+        const Dual r2 = (gamma * gm1inv) * p / ((cp * T0) - 0.5 * V_sq);
+        const Dual sv = dsqrt(V_sq);
+        s2[0] = r2;
+        for (int q = 0; q < DIM; q++) s2[1 + q] = prm[3 + q] * (r2 * sv);
+        s2[NV - 1] = gm1inv * p + 0.5 * (r2 * V_sq);
+        return;
+    }
+    // BC_RIEMANN_INVARIANT
+    const double rho_o = prm[0], p_o = prm[NV - 1];
+    const Dual Vn_i = sgn * V[D];
+    const double Vn_o = sgn * prm[1 + D];
+    const double a_o = sqrt(gamma * p_o / rho_o);
+    const Dual a_i = dsqrt(gamma * p / rho);
+    const bool sup = fabs(Vn_o) >= a_o;
+    const Dual R_minus = (sup && Vn_i.v >= 0.0) ? Vn_i - 2.0 * gm1inv * a_i : Dual{Vn_o - 2.0 * a_o * gm1inv, 0.0};
+    const Dual R_plus = (sup && Vn_i.v < 0.0) ? Dual{Vn_o + 2.0 * a_o * gm1inv, 0.0} : Vn_i + 2.0 * gm1inv * a_i;
+    const Dual Vn_b = 0.5 * (R_plus + R_minus), a_b = (0.25 * gm1) * (R_plus - R_minus);
+    const Dual r2 = Vn_i.v < 0.0 ? rho_o * dpow((a_b * a_b) * (rho_o / (gamma * p_o)), gm1inv)
+                                 : dpow((a_b * a_b) * rho / (gamma * p), gm1inv) * rho;
+    Dual e2 = {0.0, 0.0};
+    for (int q = 0; q < DIM; q++) {
+        const double nq = q == D ? sgn : 0.0;
+        s2[1 + q] = Vn_i.v >= 0.0 ? r2 * (V[q] + nq * (Vn_b - Vn_i)) : r2 * (prm[1 + q] + nq * (Vn_b - Dual{Vn_o, 0.0}));
+        e2 = e2 + s2[1 + q] * s2[1 + q];
+    }
+    s2[0] = r2;
+    s2[NV - 1] = 0.5 * (e2 / r2) + gm1inv * ((a_b * a_b) * r2 / gamma);
+}
+
+// Adjoint of the boundary faces (Euler, fixed operator): one thread per
 // element walks its boundary faces, as boundary_kernel does forward, and
 // adds (dC/du)^T cot at each boundary node, C = -F(s, s2(s)) / (w0 J):
 // prescribed outer states are constants, outflow has s2 = s, symmetry
-// s2 = s with the normal momentum reversed, the slip wall's flux depends on
-// s through p*.
+// s2 = s with the normal momentum reversed, the subsonic and Riemann-
+// invariant states enter through their Jacobian (forward mode), and the slip
+// wall's flux depends on s through p*.
 template <int DIM, int N>
 __global__ void __launch_bounds__(256) adj_boundary_kernel(const KParams P, const double *__restrict__ cot,
                                                            double *__restrict__ ubar, const double *__restrict__)
@@ -799,9 +897,26 @@ __global__ void __launch_bounds__(256) adj_boundary_kernel(const KParams P, cons
                 } else {
                     double s2[NV];
                     const bool given = type == BC_SUPERSONIC_INFLOW || type == BC_SPECIFIED_STATE;
+                    const bool sub = type >= BC_SUBSONIC_OUTFLOW_P;
+                    // Jacobian of the outer state (columns by forward mode)
+                    double Jm[NV][NV];
 #pragma unroll
                     for (int v = 0; v < NV; v++) s2[v] = given ? bc[1 + v] : s1[v];
                     if (type == BC_SYMMETRY) s2[1 + D] = -s1[1 + D];
+                    if (sub) {
+#pragma unroll 1
+                        for (int j = 0; j < NV; j++) {
+                            Dual x[NV], y[NV];
+#pragma unroll
+                            for (int v = 0; v < NV; v++) x[v] = {s1[v], v == j ? 1.0 : 0.0};
+                            outer_state_dual<DIM>(P, type, bc + 1, D, sgn, x, y);
+#pragma unroll
+                            for (int i = 0; i < NV; i++) {
+                                Jm[i][j] = y[i].d;
+                                s2[i] = y[i].v;
+                            }
+                        }
+                    }
                     const Prim<DIM> qa = make_prim<DIM>(s1, P.gamma, P.gm1), qb = make_prim<DIM>(s2, P.gamma, P.gm1);
                     PBar<DIM> ab, bb;
                     pbar_zero(ab);
@@ -818,8 +933,18 @@ __global__ void __launch_bounds__(256) adj_boundary_kernel(const KParams P, cons
                         for (int v = 0; v < NV; v++) g2[v] = 0.0;
                         pbar_to_cons<DIM>(s2, bb, mbb, P.gm1, g2);
                         if (type == BC_SYMMETRY) g2[1 + D] = -g2[1 + D];
+                        if (sub) {
 #pragma unroll
-                        for (int v = 0; v < NV; v++) g[v] += g2[v];
+                            for (int j = 0; j < NV; j++) {
+                                double a = 0.0;
+#pragma unroll
+                                for (int i = 0; i < NV; i++) a += g2[i] * Jm[i][j];
+                                g[j] += a;
+                            }
+                        } else {
+#pragma unroll
+                            for (int v = 0; v < NV; v++) g[v] += g2[v];
+                        }
                     }
                 }
 #pragma unroll

@@ -882,10 +882,6 @@ int pdg_rhs_vjp(pdg_ctx *c, const double *u, const double *cot, double *ubar, vo
     if (!c) return PDG_ERR_ARG;
     if (!u || !cot || !ubar || ubar == u || ubar == cot) return fail(c, PDG_ERR_ARG, "pdg_rhs_vjp: null or aliased buffers");
     if (c->p.compat) return fail(c, PDG_ERR_UNSUPPORTED, "pdg_rhs_vjp: the adjoint is of the fixed operator (compat = 0)");
-    for (int b = 0; b < PDG_MAX_BOUNDARIES; b++)
-        if ((c->bc_used >> b & 1u) && c->bc_host[b * BC_SLOT] > PDG_BC_SYMMETRY)
-            return fail(c, PDG_ERR_UNSUPPORTED,
-                        "pdg_rhs_vjp: boundary condition %d: only types 1-5 are differentiated", b);
     if (c->bc_used & ~c->bc_set) return fail(c, PDG_ERR_ARG, "pdg_rhs_vjp: a boundary condition is not set");
     cudaStream_t s = (cudaStream_t)stream;
     int r;

@@ -148,7 +148,7 @@ def test_subsonic_conditions_differ_between_operators(name):
 
 
 @pytest.mark.parametrize("order", [2, 3])
-@pytest.mark.parametrize("name", ["2d_in_out_walls", "2d_symmetry_state", "3d_all", "2d_step"])
+@pytest.mark.parametrize("name", sorted(layouts()))
 def test_torch_reference_boundaries_match_oracle(name, order):
     """The differentiable restatement (the adjoint's reference gradient) on
     boundary layouts of conditions 1-5, fixed operator."""
