@@ -902,8 +902,9 @@ static double bdr_flux(const Ctx &c, int b, const double *s1, const double *nor,
     const int type = (int)c.bc[b][0];
     double s2[5], un[3];
     for (int v = 0; v < nv; v++) s2[v] = s1[v];
-    if (type == 4) {
-        // SlipWallBdrFaceIntegrator::ComputeBdrFaceInviscidFlux (:15-58)
+    if (type == 4 || type == 10) {
+        // SlipWallBdrFaceIntegrator::ComputeBdrFaceInviscidFlux (:15-58); the
+        // no-slip wall derives from it
         const double gammaP1 = 1.0 + gamma, gammaP1Inverse = 1.0 / gammaP1;
         unit_normal(dim, nor, un);
         rotate_state(dim, s2, un);
@@ -1035,18 +1036,90 @@ static double bdr_flux(const Ctx &c, int b, const double *s1, const double *nor,
 // the outward normal; out[t][v] = -flux / (w0 J1) at face node t.
 static double bdr_face_vector(const Ctx &c, const double *u, int64_t e, int d, int side, int b, double *out)
 {
-    const int nv = c.nv, nfn = c.ndof / c.Np;
+    const int nv = c.nv, nfn = c.ndof / c.Np, dim = c.dim;
     double nor[3] = {0, 0, 0};
     nor[d] = side ? c.area[d] : -c.area[d];
     const double scale = 1.0 / (c.w[0] * c.J);
-    double lam = -1.0, s1[5], flux[5];
+    const int type = (int)c.bc[b][0];
+    double lam = -1.0, s1[5], flux[5], dq[15], fm[15];
     for (int t = 0; t < nfn; t++) {
         const int n = face_node(c, d, side, t);
         for (int v = 0; v < nv; v++) s1[v] = u[idx(c, v, e, n)];
         lam = std::max(lam, bdr_flux(c, b, s1, nor, flux));
-        for (int v = 0; v < nv; v++) out[t * nv + v] = scale * -flux[v];
+        double dU[5];
+        for (int v = 0; v < nv; v++) dU[v] = -flux[v];
+        if (c.p.parabolic && (type == 2 || type == 10)) {
+            // ComputeBdrFaceViscousFlux: the interior state's viscous flux
+            // with its own gradients (SupersonicOutflowBdrFaceIntegrator.cpp:
+            // 15-20); the no-slip wall replaces the energy row by the wall
+            // velocity's work, its heat flux qn being zero
+            // (NoSlipAdiabWallBdrFaceIntegrator.cpp:21-36)
+            for (int q = 0; q < dim; q++)
+                for (int v = 0; v < nv; v++) dq[q * nv + v] = c.grads[(size_t)q * c.size + idx(c, v, e, n)];
+            viscous_flux(dim, c.p.gamma, c.p.Pr, c.p.mu, s1, dq, fm);
+            double fn[5];
+            for (int v = 0; v < nv; v++) {
+                fn[v] = 0.0;
+                for (int q = 0; q < dim; q++) fn[v] += fm[v * dim + q] * nor[q];
+            }
+            if (type == 10) {
+                double en = 0.0;
+                for (int q = 0; q < dim; q++) en += c.bc[b][1 + q] * fn[1 + q];
+                fn[nv - 1] = en + 0.0;
+            }
+            for (int v = 0; v < nv; v++) dU[v] += fn[v];
+        }  // types 1, 3: the viscous flux of the outer state with zero gradients, 0
+        for (int v = 0; v < nv; v++) out[t * nv + v] = scale * dU[v];
     }
     return lam;
+}
+
+// ComputeBdrFaceLiftingFlux (BdrFaceIntegrator.cpp:275-282; the no-slip wall's
+// NoSlipAdiabWallBdrFaceIntegrator.cpp:74-95): the BR1 boundary jump of the
+// entropy variables w1 at a boundary node with interior state s1.  Default:
+// 0.5 (w(s2) - w1) with s2 the outer state; the reference reaches s2 through
+// Entropy2Conserv(w1) (BasicOperations.cpp:106-124), whose velocity view
+// divides w1's momentum entries by beta in place before they are
+// subtracted; compat keeps that.  No-slip: (w1_0, beta V, -beta) - w1.
+static void bdr_lifting_flux(const Ctx &c, int b, const double *s1, const double *w1_in, double *f)
+{
+    const int nv = c.nv, dim = c.dim;
+    const double gamma = c.p.gamma, gm1 = gamma - 1.0, gm1inv = 1.0 / gm1;
+    const int type = (int)c.bc[b][0];
+    double w1[5];
+    for (int v = 0; v < nv; v++) w1[v] = w1_in[v];
+    if (type == 10) {
+        const double beta = -w1[nv - 1];
+        f[0] = w1[0];
+        for (int q = 0; q < dim; q++) f[1 + q] = c.bc[b][1 + q] * beta;
+        f[nv - 1] = -beta;
+        for (int v = 0; v < nv; v++) f[v] -= w1[v];
+        return;
+    }
+    double s2[5];
+    if (c.p.compat) {
+        // Entropy2Conserv(w1) with its in-place division of w1's momenta
+        const double beta = -w1[nv - 1], ib = 1.0 / beta;
+        double vv = 0.0;
+        for (int q = 0; q < dim; q++) { w1[1 + q] *= ib; vv += w1[1 + q] * w1[1 + q]; }
+        const double sent = gamma - (w1[0] + 0.5 * beta * vv) * gm1;
+        double cons[5];
+        cons[0] = std::pow(std::exp(-sent) / beta, gm1inv);
+        for (int q = 0; q < dim; q++) cons[1 + q] = cons[0] * w1[1 + q];
+        cons[nv - 1] = cons[0] * (1.0 / beta * gm1inv + 0.5 * vv);
+        for (int v = 0; v < nv; v++) s2[v] = cons[v];
+    } else {
+        for (int v = 0; v < nv; v++) s2[v] = s1[v];
+    }
+    if (type == 1 || type == 3)
+        for (int v = 0; v < nv; v++) s2[v] = c.bc[b][1 + v];
+    double w2[5];
+    conserv2entropy(dim, gamma, s2, w2);
+    for (int v = 0; v < nv; v++) {
+        f[v] = w2[v];
+        f[v] -= w1[v];
+        f[v] *= 0.5;
+    }
 }
 
 // ---------------------------------------------------------------------------
@@ -1097,6 +1170,27 @@ static void lifting(Ctx &c, const double *u)
         for (int d = 0; d < dim; d++)
             for (int side = 0; side < 2; side++) {
                 int64_t nb = c.nbr[e * 2 * dim + 2 * d + side];
+                if (nb < 0) {
+                    // boundary face (LiftingBR1::AssembleLiftingBdrFaceVector,
+                    // LiftingBR1.cpp:311-345): the element is element 1, the
+                    // normal points out of it
+                    const double ndb = side ? c.area[d] : -c.area[d];
+                    double s1[5], w1[5], f[5];
+                    for (int t = 0; t < nfn; t++) {
+                        const int n = face_node(c, d, side, t);
+                        for (int v = 0; v < nv; v++) {
+                            s1[v] = u[idx(c, v, e, n)];
+                            w1[v] = W[idx(c, v, e, n)];
+                        }
+                        bdr_lifting_flux(c, (int)(-1 - nb), s1, w1, f);
+                        for (int v = 0; v < nv; v++) {
+                            double fval = f[v];
+                            fval *= ndb;
+                            G[(size_t)d * c.size + idx(c, v, e, n)] += scale * fval;
+                        }
+                    }
+                    continue;
+                }
                 // The face between (e, side) and nb: element 1 rule.
                 int64_t a = side ? e : nb;  // element on the -d side of the face
                 int64_t bb = side ? nb : e;
@@ -1347,8 +1441,8 @@ void *orc_create(const pdg_mesh *m, const pdg_params *p)
     c->size = c->nnodes * c->nv;
     for (int d = 0; d < 3; d++) c->h[d] = d < c->dim ? m->h[d] : 1.0;
     c->nbr.assign(m->nbr, m->nbr + (size_t)c->ne * 2 * c->dim);
-    for (int32_t nb : c->nbr)  // boundary faces: Euler only, conditions 0..15
-        if (nb >= c->ne || nb < -16 || (nb < 0 && p->parabolic)) { delete c; return nullptr; }
+    for (int32_t nb : c->nbr)  // boundary faces: conditions 0..15
+        if (nb >= c->ne || nb < -16) { delete c; return nullptr; }
     orc::gll(c->Np, c->x, c->w);
     orc::build_derivative_matrices(*c);
     if (c->dim == 2) {
@@ -1391,12 +1485,12 @@ void orc_destroy(void *h) { delete (Ctx *)h; }
 // Boundary condition `index`: its type and parameters as pdg_set_boundary
 // takes them (types 1, 3: conserved state; 6: p; 7: rho, velocity; 8: cp,
 // pt, Tt, theta, phi in degrees, stored as cp, pt, Tt, cos theta, sin theta;
-// 9: primitive state rho, velocity, p).
+// 9: primitive state rho, velocity, p; 10: wall velocity).
 void orc_set_boundary(void *h, int index, int type, const double *state)
 {
     Ctx &c = *(Ctx *)h;
     if (index < 0 || index >= 16) return;
-    const int n = type == 6 ? 1 : type == 7 ? 1 + c.dim : type == 8 ? 5 : c.nv;
+    const int n = type == 6 ? 1 : type == 7 ? 1 + c.dim : type == 8 ? 5 : type == 10 ? c.dim : c.nv;
     c.bc[index][0] = type;
     for (int v = 0; v < 7; v++) c.bc[index][1 + v] = (state && v < n) ? state[v] : 0.0;
     if (type == 8) {

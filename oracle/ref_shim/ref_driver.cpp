@@ -25,6 +25,7 @@
 #include "SubsonicInflowRVBdrFaceIntegrator.hpp"
 #include "SubsonicInflowPtTtAngBdrFaceIntegrator.hpp"
 #include "RiemannInvariantBdrFaceIntegrator.hpp"
+#include "NoSlipAdiabWallBdrFaceIntegrator.hpp"
 #include "DGSEMIntegrator.hpp"
 #include "ModalBasis.hpp"
 #include "NavierStokesFlux.hpp"
@@ -311,6 +312,7 @@ int ref_set_boundary(void *h, int index, int type, const double *state)
     RefCtx &c = *(RefCtx *)h;
     if (index < 0 || index >= 16) return 1;
     const bool full = type == 1 || type == 3 || type == 9;  // a whole (conserved or primitive) state
+    if (!state && type == 10) return 1;
     Vector st(c.nv);
     for (int v = 0; v < c.nv; v++) st(v) = (state && full) ? state[v] : 0.0;
     if (!state && type >= 6) return 1;
@@ -333,6 +335,13 @@ int ref_set_boundary(void *h, int index, int type, const double *state)
                                                        state[2], state[3], state[4]);
         break;
     case 9: b = new RiemannInvariantBdrFaceIntegrator(c.lifting, *c.rsolver, c.Np, c.time, c.gamma, st); break;
+    case 10: {  // no-slip adiabatic wall, zero heat flux, wall velocity `state`
+        Vector V(3);
+        V = 0.0;
+        for (int d = 0; d < c.dim; d++) V(d) = state[d];
+        b = new NoSlipAdiabWallBdrFaceIntegrator(c.lifting, *c.rsolver, c.Np, c.time, c.gamma, 0.0, V);
+        break;
+    }
     default: return 1;
     }
     c.bfi[index].reset(b);
@@ -396,6 +405,20 @@ double ref_rhs(void *h, const double *u_in, double *dudt_out)
             G[0]->AddElementVector(vdofs, gx);
             G[1]->AddElementVector(vdofs, gy);
         }
+        // boundary faces (MultLifting's boundary-face loop)
+        for (auto &f : c.bfaces) {
+            setup_bdr_face(c, f, T);
+            c.vfes->GetElementVDofs(f.e, vdofs);
+            c.went->GetSubVector(vdofs, el_u);
+            if (c.dim == 3) {
+                c.bfi[f.b]->AssembleLiftingFaceVector(fe, fe, T, el_u, gx, gy, gz);
+                G[2]->AddElementVector(vdofs, gz);
+            } else {
+                c.bfi[f.b]->AssembleLiftingFaceVector(fe, fe, T, el_u, gx, gy);
+            }
+            G[0]->AddElementVector(vdofs, gx);
+            G[1]->AddElementVector(vdofs, gy);
+        }
         // ComputeGlobalPrimitiveGradVector (DGSEMOperator.cpp:112-159)
         Vector grad_vdofs;
         for (int el = 0; el < c.ne; el++) {
@@ -438,6 +461,20 @@ double ref_rhs(void *h, const double *u_in, double *dudt_out)
                 c.integ->AssembleFaceVector(fe, fe, T, el_u, el_gx, el_gy, el_gz, el_dudt);
             } else {
                 c.integ->AssembleFaceVector(fe, fe, T, el_u, el_gx, el_gy, el_dudt);
+            }
+            dudt.AddElementVector(vdofs, el_dudt);
+        }
+        for (auto &f : c.bfaces) {
+            setup_bdr_face(c, f, T);
+            c.vfes->GetElementVDofs(f.e, vdofs);
+            u.GetSubVector(vdofs, el_u);
+            G[0]->GetSubVector(vdofs, el_gx);
+            G[1]->GetSubVector(vdofs, el_gy);
+            if (c.dim == 3) {
+                G[2]->GetSubVector(vdofs, el_gz);
+                c.bfi[f.b]->AssembleFaceVector(fe, fe, T, el_u, el_gx, el_gy, el_gz, el_dudt);
+            } else {
+                c.bfi[f.b]->AssembleFaceVector(fe, fe, T, el_u, el_gx, el_gy, el_dudt);
             }
             dudt.AddElementVector(vdofs, el_dudt);
         }

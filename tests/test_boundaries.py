@@ -158,3 +158,50 @@ def test_torch_reference_boundaries_match_oracle(name, order):
     got = TorchDGSEM(mesh).rhs(torch.tensor(u)).numpy()
     ref = oracle.Oracle(mesh, compat=0).rhs(u)
     assert np.abs(got - ref).max() <= 1e-12 * np.abs(ref).max()
+
+
+NOSLIP = 10  # no-slip adiabatic wall (data: wall velocity)
+
+
+def ns_layouts():
+    """Navier-Stokes boundary layouts: inflow/outflow channels with no-slip
+    walls and a lid-driven cavity."""
+    fs2 = np.array([1.2, 0.3, -0.2, 2.6])
+    fs3 = np.array([1.1, 0.2, -0.1, 0.15, 2.8])
+    return {
+        "ns_2d_channel": (2, dict(bdr=[(0, 1), (2, 2)], boundaries={
+            0: (pb.BC_SUPERSONIC_INFLOW, fs2), 1: (pb.BC_SUPERSONIC_OUTFLOW, None), 2: (NOSLIP, [0.0, 0.0])})),
+        "ns_2d_cavity": (2, dict(bdr=[(0, 0), (0, 1)], boundaries={
+            0: (NOSLIP, [0.0, 0.0]), 1: (NOSLIP, [1.0, 0.0])})),
+        "ns_3d_channel": (3, dict(bdr=[(0, 1), (2, 2), None], boundaries={
+            0: (pb.BC_SPECIFIED_STATE, fs3), 1: (pb.BC_SUPERSONIC_OUTFLOW, None), 2: (NOSLIP, [0.1, 0.0, 0.0])})),
+    }
+
+
+def ns_layout_case(name, order):
+    dim, kw = ns_layouts()[name]
+    if dim == 2:
+        mesh = box(2, order, (4, 3), (-1.0, -1.0), (1.0, 1.0), **kw)
+        u = cases.kelvin_helmholtz(periodic_box(2, order, (4, 3), -1.0, 1.0))
+    else:
+        mesh = box(3, order, (3, 2, 3), 0.0, 2 * np.pi, **kw)
+        u = cases.taylor_green(periodic_box(3, order, (3, 2, 3), 0.0, 2 * np.pi), Ma=0.4)
+    return mesh, rough(u, mesh, 21, 0.05, 0.02)
+
+
+NS_KW = dict(parabolic=1, mu=0.02, Pr=0.71)
+
+
+@pytest.mark.skipif(not oracle.ref_available(True), reason="reference build (oracle/_ref) not present")
+@pytest.mark.parametrize("order", [1, 3])
+@pytest.mark.parametrize("name", sorted(ns_layouts()))
+def test_oracle_ns_boundaries_match_live_reference(name, order):
+    """BR1 boundary lifting and viscous boundary fluxes against the
+    reference's own boundary integrators and LiftingBR1."""
+    mesh, u = ns_layout_case(name, order)
+    o = oracle.Oracle(mesh, compat=1, **NS_KW)
+    r = oracle.Reference(mesh, parabolic=True, mu=NS_KW["mu"], Pr=NS_KW["Pr"])
+    ro, rr = o.rhs(u), r.rhs(u)
+    assert np.abs(ro - rr).max() <= 1e-12 * np.abs(rr).max()
+    go, gr = o.gradients(), r.gradients()
+    assert np.abs(go - gr).max() <= 1e-11 * np.abs(gr).max()
