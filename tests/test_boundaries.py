@@ -69,10 +69,13 @@ def test_symmetry_equals_mirrored_periodic_domain(order):
     assert np.abs(r_half - r_full[:, ny:]).max() < 1e-12 * scale
 
 
-def test_navier_stokes_mesh_with_boundaries_is_rejected():
+def test_torch_reference_rejects_navier_stokes_boundaries():
+    """The differentiable restatement (the adjoint's reference) has no
+    Navier-Stokes boundary faces."""
+    from oracle.torch_rhs import TorchDGSEM
     mesh = freestream_box(2, 2)
     with pytest.raises(ValueError):
-        oracle.Oracle(mesh, parabolic=1, mu=0.01)
+        TorchDGSEM(mesh, parabolic=True, mu=0.01)
 
 
 def _step_keep(n):
