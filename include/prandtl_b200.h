@@ -111,9 +111,11 @@ int pdg_destroy(pdg_ctx *ctx);
  * src/Operators/DGSEMOperator.cpp:593 and src/Simulation/Simulation.cpp:
  * 490-798).  A neighbour entry -1 - b (0 <= b < PDG_MAX_BOUNDARIES) marks a
  * boundary face with condition b; every condition the mesh uses must be set
- * before the first evaluation (else PDG_ERR_ARG).  Euler only: pdg_create
- * returns PDG_ERR_UNSUPPORTED for a Navier-Stokes mesh with boundary faces;
- * pdg_rhs_vjp differentiates every condition (fixed operator).  `state` holds the condition's
+ * before the first evaluation (else PDG_ERR_ARG).  Navier-Stokes boundary
+ * faces: fixed operator only (pdg_create returns PDG_ERR_UNSUPPORTED with
+ * compat = 1) and types 1, 2, 3 and 10 (others: PDG_ERR_UNSUPPORTED at the
+ * first evaluation); pdg_rhs_vjp differentiates every condition of an Euler
+ * mesh and none of a Navier-Stokes one.  `state` holds the condition's
  * data as listed beside each type (conserved, dim + 2 values, for the two
  * prescribed-state types) and may be NULL for types without data.  With
  * compat = 1 the subsonic and Riemann-invariant conditions keep the
@@ -131,6 +133,7 @@ int pdg_destroy(pdg_ctx *ctx);
 #define PDG_BC_SUBSONIC_INFLOW_RV 7  /* SubsonicInflowRVBdrFaceIntegrator: state = {rho, V[dim]} */
 #define PDG_BC_SUBSONIC_INFLOW_PTTT 8  /* SubsonicInflowPtTtAngBdrFaceIntegrator, 2D: state = {cp, pt, Tt, theta, phi} (degrees) */
 #define PDG_BC_RIEMANN_INVARIANT  9  /* RiemannInvariantBdrFaceIntegrator: state = primitive {rho, v[dim], p} */
+#define PDG_BC_NOSLIP_ADIABATIC  10  /* NoSlipAdiabWallBdrFaceIntegrator, zero heat flux: state = wall velocity {V[dim]} */
 int pdg_set_boundary(pdg_ctx *ctx, int index, int type, const double *state);
 
 /* TimeDependentOperator::Height (DGSEMOperator.cpp:18): number of vdofs. */
@@ -269,6 +272,9 @@ int64_t pdg_launch_count(const pdg_ctx *ctx);
 #define PDG_KERNEL_BOUNDARY  22     /* boundary faces of the separate-face path (Euler) */
 #define PDG_KERNEL_ADJ_BOUNDARY 23  /* adjoint of the boundary faces (Euler) */
 #define PDG_KERNEL_EULER_FACES_BDR 24  /* PDG_KERNEL_EULER_FACES for meshes with boundary faces */
+#define PDG_KERNEL_LIFT_FACE_BDR 25  /* Navier-Stokes meshes with boundary faces: face jumps, */
+#define PDG_KERNEL_LIFT_BDR  26      /* lifting kernel, */
+#define PDG_KERNEL_NS_FACES_BDR 27   /* volume kernel with element-side faces */
 int pdg_profile_enable(pdg_ctx *ctx, int on);
 int pdg_profile_read(pdg_ctx *ctx, int kind, double *total_ms, int64_t *launches);
 

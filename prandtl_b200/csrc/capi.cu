@@ -46,6 +46,7 @@ struct pdg_ctx {
     double bc_host[PDG_MAX_BOUNDARIES * BC_SLOT] = {};
     double *bc = nullptr;
     unsigned int bc_used = 0, bc_set = 0;
+    double *lbuf_lo = nullptr;  // NS boundary faces: BR1 jumps of -d boundary faces
     double *stage_a = nullptr, *stage_b = nullptr;  // RK stage buffers
     double *io_a = nullptr, *io_b = nullptr;        // host-path staging
     unsigned long long *lam_bits = nullptr;
@@ -268,7 +269,7 @@ int kernel_config(int dim, int N, int kind, int64_t ne, int device, LaunchCfg *c
     if (ki.el_doubles == 0) {  // thread-per-face-node kernel
         const int64_t threads = kind == KIND_FILTER_BOUNDS ? 32 * ne
                                 : (kind == KIND_BOUNDARY || kind == KIND_ADJ_BOUNDARY) ? ne
-                                : (kind == KIND_LIFT_FACE ? (int64_t)dim : 1) * ne * nfn;
+                                : ((kind == KIND_LIFT_FACE || kind == KIND_LIFT_FACE_BDR) ? (int64_t)dim : 1) * ne * nfn;
         // 256-thread blocks; 128 when that gives fewer than four blocks per
         // SM, so that a small mesh still spreads evenly over the SMs
         cfg->wpb = threads < 4LL * 256 * sms ? 4 : 8;
@@ -312,7 +313,8 @@ bool kind_used(int kind, int dim, bool parabolic, bool filter)
     if ((kind >= KIND_ADJ_RHS && kind <= KIND_ADJ_FACE_NS2) || kind == KIND_ADJ_BOUNDARY)
         return false;  // configured by the first pdg_rhs_vjp
     const bool ns_kind = kind == KIND_NS || kind == KIND_NS_FACES || kind == KIND_LIFT || kind == KIND_LIFT_FACE ||
-                         (kind >= KIND_FACE_NS0 && kind <= KIND_FACE_NS2);
+                         (kind >= KIND_FACE_NS0 && kind <= KIND_FACE_NS2) || kind == KIND_LIFT_FACE_BDR ||
+                         kind == KIND_LIFT_BDR || kind == KIND_NS_FACES_BDR;
     if (ns_kind != parabolic) return false;
     if ((kind == KIND_FACE_E2 || kind == KIND_FACE_NS2) && dim < 3) return false;
     return true;
@@ -381,6 +383,7 @@ KParams base_params(pdg_ctx *c)
     P.prefetch = c->prefetch;
     P.bc = c->bc;
     P.has_bdr = c->bc_used != 0;
+    P.lbuf_lo = c->lbuf_lo;
     return P;
 }
 
@@ -448,9 +451,11 @@ int lift(pdg_ctx *c, KParams P, const double *u, double *grads_out, cudaStream_t
 {
     P.u = u;
     P.grads_out = grads_out;
-    int r = launch(c, KIND_LIFT_FACE, P, s);
+    if (c->bc_used && (c->bc_used & ~c->bc_set))
+        return fail(c, PDG_ERR_ARG, "a boundary condition the mesh uses is not set (pdg_set_boundary)");
+    int r = launch(c, c->bc_used ? KIND_LIFT_FACE_BDR : KIND_LIFT_FACE, P, s);
     if (r) return r;
-    return launch(c, KIND_LIFT, P, s);
+    return launch(c, c->bc_used ? KIND_LIFT_BDR : KIND_LIFT, P, s);
 }
 
 // RHS (stage < 0) or fused SSP-RK3 stage of the operator on device buffers.
@@ -479,12 +484,27 @@ int evaluate(pdg_ctx *c, int stage, double dt, const double *un, const double *u
     const bool element_faces = c->element_faces && !c->p.compat;
     if (c->p.parabolic) {
         if (c->p.filter && stage >= 0 && (r = launch(c, KIND_FILTER_BOUNDS, P, s))) return r;
-        if ((r = launch(c, KIND_LIFT_FACE, P, s))) return r;
-        if (element_faces) {
+        if (c->bc_used) {
+            // boundary faces of the fixed operator's element-side path
+            for (int b = 0; b < PDG_MAX_BOUNDARIES; b++) {
+                const int t = (int)c->bc_host[b * BC_SLOT];
+                if ((c->bc_used >> b & 1u) && t != PDG_BC_SUPERSONIC_INFLOW && t != PDG_BC_SUPERSONIC_OUTFLOW &&
+                    t != PDG_BC_SPECIFIED_STATE && t != PDG_BC_NOSLIP_ADIABATIC)
+                    return fail(c, PDG_ERR_UNSUPPORTED,
+                                "boundary condition %d: type %d has no viscous boundary flux here", b, t);
+            }
+            if (!element_faces) return fail(c, PDG_ERR_UNSUPPORTED, "Navier-Stokes boundary faces need element-side faces");
+            if ((r = launch(c, KIND_LIFT_FACE_BDR, P, s))) return r;
+            P.vbuf = c->vbuf;
+            if ((r = launch(c, KIND_LIFT_BDR, P, s))) return r;
+            if ((r = launch(c, KIND_NS_FACES_BDR, P, s))) return r;
+        } else if (element_faces) {
+            if ((r = launch(c, KIND_LIFT_FACE, P, s))) return r;
             P.vbuf = c->vbuf;
             if ((r = launch(c, KIND_LIFT, P, s))) return r;
             if ((r = launch(c, KIND_NS_FACES, P, s))) return r;
         } else {
+            if ((r = launch(c, KIND_LIFT_FACE, P, s))) return r;
             if ((r = launch(c, KIND_NS, P, s))) return r;
             if ((r = launch(c, KIND_LIFT, P, s))) return r;
             for (int d = 0; d < c->dim; d++)
@@ -557,8 +577,8 @@ int pdg_create(const pdg_mesh *mesh, const pdg_params *params, pdg_ctx **out)
         if (nb >= c->ne || nb < -PDG_MAX_BOUNDARIES) { delete c; return PDG_ERR_ARG; }
         if (nb < 0) c->bc_used |= 1u << (-1 - nb);
     }
-    // boundary faces: Euler only (the BR1 boundary lifting is not built)
-    if (c->bc_used && params->parabolic) { delete c; return PDG_ERR_UNSUPPORTED; }
+    // Navier-Stokes boundary faces: fixed operator (its element-side faces) only
+    if (c->bc_used && params->parabolic && params->compat) { delete c; return PDG_ERR_UNSUPPORTED; }
     auto cleanup = [&](int code) {
         pdg_destroy(c);
         return code;
@@ -585,7 +605,8 @@ int pdg_create(const pdg_mesh *mesh, const pdg_params *params, pdg_ctx **out)
         const size_t nfn = c->dim == 2 ? c->Np : c->Np * c->Np;
         if (cudaMalloc(&c->lbuf, sizeof(double) * c->dim * c->ne * nfn * c->nv) != cudaSuccess ||
             cudaMalloc(&c->fcol, sizeof(double) * 2 * c->dim * c->ne * nfn * (c->nv - 1)) != cudaSuccess ||
-            cudaMalloc(&c->vbuf, sizeof(double) * (c->nv - 1) * c->nnodes) != cudaSuccess)
+            cudaMalloc(&c->vbuf, sizeof(double) * (c->nv - 1) * c->nnodes) != cudaSuccess ||
+            (c->bc_used && cudaMalloc(&c->lbuf_lo, sizeof(double) * c->dim * c->ne * nfn * c->nv) != cudaSuccess))
             return cleanup(PDG_ERR_NOMEM);
     }
     if (cudaMemcpy(c->K, &c->hK, sizeof(DevConst), cudaMemcpyHostToDevice) ||
@@ -607,13 +628,14 @@ int pdg_set_boundary(pdg_ctx *c, int index, int type, const double *state)
     if (!c) return PDG_ERR_ARG;
     if (index < 0 || index >= PDG_MAX_BOUNDARIES)
         return fail(c, PDG_ERR_ARG, "pdg_set_boundary: index %d outside [0, %d)", index, PDG_MAX_BOUNDARIES);
-    if (type < PDG_BC_SUPERSONIC_INFLOW || type > PDG_BC_RIEMANN_INVARIANT)
+    if (type < PDG_BC_SUPERSONIC_INFLOW || type > PDG_BC_NOSLIP_ADIABATIC)
         return fail(c, PDG_ERR_ARG, "pdg_set_boundary: unknown boundary type %d", type);
     if (type == PDG_BC_SUBSONIC_INFLOW_PTTT && c->dim != 2)
         return fail(c, PDG_ERR_UNSUPPORTED, "pdg_set_boundary: the total-pressure inflow is 2D only");
     double slot[BC_SLOT] = {(double)type};
     const int n = type == PDG_BC_SUBSONIC_OUTFLOW_P ? 1
                   : type == PDG_BC_SUBSONIC_INFLOW_RV ? 1 + c->dim
+                  : type == PDG_BC_NOSLIP_ADIABATIC ? c->dim
                   : type == PDG_BC_SUBSONIC_INFLOW_PTTT ? 5
                   : (type == PDG_BC_SUPERSONIC_INFLOW || type == PDG_BC_SPECIFIED_STATE || type == PDG_BC_RIEMANN_INVARIANT)
                       ? c->nv : 0;
@@ -630,6 +652,8 @@ int pdg_set_boundary(pdg_ctx *c, int index, int type, const double *state)
             ok = ok && state[0] > 0.0 && state[c->nv - 1] > 0.0;
         } else if (type == PDG_BC_SUBSONIC_INFLOW_PTTT) {
             ok = ok && state[0] > 0.0 && state[1] > 0.0 && state[2] > 0.0;
+        } else if (type == PDG_BC_NOSLIP_ADIABATIC) {
+            // any wall velocity
         } else {
             ok = ok && state[0] > 0.0;
         }
@@ -658,6 +682,7 @@ int pdg_destroy(pdg_ctx *c)
     cudaFree(c->fcol);
     cudaFree(c->vbuf);
     cudaFree(c->bc);
+    cudaFree(c->lbuf_lo);
     cudaFree(c->stage_a);
     cudaFree(c->stage_b);
     cudaFree(c->io_a);
@@ -882,6 +907,8 @@ int pdg_rhs_vjp(pdg_ctx *c, const double *u, const double *cot, double *ubar, vo
     if (!c) return PDG_ERR_ARG;
     if (!u || !cot || !ubar || ubar == u || ubar == cot) return fail(c, PDG_ERR_ARG, "pdg_rhs_vjp: null or aliased buffers");
     if (c->p.compat) return fail(c, PDG_ERR_UNSUPPORTED, "pdg_rhs_vjp: the adjoint is of the fixed operator (compat = 0)");
+    if (c->p.parabolic && c->bc_used)
+        return fail(c, PDG_ERR_UNSUPPORTED, "pdg_rhs_vjp: Navier-Stokes boundary faces are not differentiated");
     if (c->bc_used & ~c->bc_set) return fail(c, PDG_ERR_ARG, "pdg_rhs_vjp: a boundary condition is not set");
     cudaStream_t s = (cudaStream_t)stream;
     int r;

@@ -29,7 +29,10 @@ enum KernelKind {
     KIND_BOUNDARY = 22,       // boundary_kernel<dim, N>: boundary faces of the separate-face path (Euler)
     KIND_ADJ_BOUNDARY = 23,   // adj_boundary_kernel<dim, N>: adjoint of the boundary faces (Euler)
     KIND_EULER_FACES_BDR = 24,  // rhs_kernel<dim, N, false, true, true>: KIND_EULER_FACES for meshes with boundaries
-    KIND_COUNT = 25
+    KIND_LIFT_FACE_BDR = 25,    // lift_face_kernel<dim, N, true>: NS meshes with boundary faces
+    KIND_LIFT_BDR = 26,         // lift_kernel<dim, N, true>
+    KIND_NS_FACES_BDR = 27,     // rhs_kernel<dim, N, true, true, true>
+    KIND_COUNT = 28
 };
 
 struct KernelInfo {

@@ -21,6 +21,12 @@ template <int N> static bool info_n(int kind, KernelInfo *out)
         out->fn = (const void *)&rhs_kernel<3, N, false, true, true>;
         out->el_doubles = S::EL_RHS;
         break;
+    case KIND_NS_FACES_BDR:
+        out->fn = (const void *)&rhs_kernel<3, N, true, true, true>;
+        out->el_doubles = S::EL_RHS;
+        break;
+    case KIND_LIFT_FACE_BDR: out->fn = (const void *)&lift_face_kernel<3, N, true>; break;
+    case KIND_LIFT_BDR: out->fn = (const void *)&lift_kernel<3, N, true>; out->el_doubles = S::EL_LIFTF; break;
     case KIND_LIFT: out->fn = (const void *)&lift_kernel<3, N>; out->el_doubles = S::EL_LIFTF; break;
     case KIND_LIFT_FACE: out->fn = (const void *)&lift_face_kernel<3, N>; break;
     case KIND_FACE_E0: out->fn = (const void *)&face_kernel<3, N, 0, false>; break;

@@ -85,6 +85,7 @@ struct KParams {
     int blending, compat;
     int prefetch;         // L2-prefetch the next element's inputs
     const double *bc;     // boundary conditions, BC_SLOT doubles each (type, state)
+    double *lbuf_lo;      // NS boundary faces: BR1 jumps of -d boundary faces [d][e][face node][v]
     int has_bdr;          // the neighbour table holds boundary faces (negative entries)
 };
 
@@ -93,7 +94,7 @@ struct KParams {
 constexpr int BC_SLOT = 8;
 constexpr int BC_SUPERSONIC_INFLOW = 1, BC_SUPERSONIC_OUTFLOW = 2, BC_SPECIFIED_STATE = 3, BC_SLIP_WALL = 4,
               BC_SYMMETRY = 5, BC_SUBSONIC_OUTFLOW_P = 6, BC_SUBSONIC_INFLOW_RV = 7, BC_SUBSONIC_INFLOW_PTTT = 8,
-              BC_RIEMANN_INVARIANT = 9;
+              BC_RIEMANN_INVARIANT = 9, BC_NOSLIP_ADIABATIC = 10;
 
 constexpr int pow2_at_least(int x) { return x <= 1 ? 1 : x <= 2 ? 2 : x <= 4 ? 4 : x <= 8 ? 8 : x <= 16 ? 16 : 32; }
 
@@ -553,7 +554,7 @@ __device__ __forceinline__ void face_terms_dir(const KParams &P, const double *c
                 if (t < 2 * NFN) {
                     const int side = t >= NFN, fn = side ? t - NFN : t;
                     const int64_t other = enb[2 * D + side];
-                    if (!BDR || other >= 0) {  // BDR: the mesh has boundary faces (Euler)
+                    if (!BDR || other >= 0) {  // BDR: the mesh has boundary faces
                         load_face_in<DIM, N, D, false>(P, side ? e : other, side ? other : e, fn, in[r]);
                     } else {
                         // boundary face: this element's trace only
@@ -591,12 +592,34 @@ __device__ __forceinline__ void face_terms_dir(const KParams &P, const double *c
         if (NS) {
             const int64_t ne = P.ne;
             double fv[R][DIM + 1];
+            bool bslot[R];  // boundary face: fv holds the element's whole viscous term
 #pragma unroll
             for (int r = 0; r < R; r++) {
                 const int t = gl + r * L;
+                bslot[r] = false;
                 if (t < 2 * NFN) {
                     const int side = t >= NFN, fn = side ? t - NFN : t;
-                    const int64_t other = enb[2 * D + side];  // >= 0: NS meshes have no boundary faces
+                    const int64_t other = enb[2 * D + side];
+                    if (BDR && other < 0) {
+                        // ComputeBdrFaceViscousFlux: the element's own column
+                        // (outflow, no-slip wall) or nothing (prescribed
+                        // states: the outer state with zero gradients)
+                        bslot[r] = true;
+                        const double *bc = P.bc + (-1 - other) * BC_SLOT;
+                        const int type = (int)bc[0];
+                        const double nrm = side ? C_AREA(c)[D] : -C_AREA(c)[D];
+                        const double *fo = P.fcol + (((D * 2 + side) * ne + e) * NFN + fn) * (NV - 1);
+                        const bool own = type == BC_SUPERSONIC_OUTFLOW || type == BC_NOSLIP_ADIABATIC;
+#pragma unroll
+                        for (int i = 0; i <= DIM; i++) fv[r][i] = own ? __ldg(fo + i) * nrm : 0.0;
+                        if (type == BC_NOSLIP_ADIABATIC) {  // energy row: the wall velocity's work, qn = 0
+                            double en = 0.0;
+#pragma unroll
+                            for (int q = 0; q < DIM; q++) en += bc[1 + q] * fv[r][q];
+                            fv[r][DIM] = en + 0.0;
+                        }
+                        continue;
+                    }
                     const int64_t a = side ? e : other, b = side ? other : e;
                     const double *fa = P.fcol + (((D * 2 + 1) * ne + a) * NFN + fn) * (NV - 1);
                     const double *fb = P.fcol + (((D * 2 + 0) * ne + b) * NFN + fn) * (NV - 1);
@@ -605,6 +628,7 @@ __device__ __forceinline__ void face_terms_dir(const KParams &P, const double *c
                 }
             }
             const double sc = (C_FACE(c) * coef) * (0.5 * C_AREA(c)[D]);
+            const double sb = C_FACE(c) * coef;
 #pragma unroll
             for (int r = 0; r < R; r++) {
                 const int t = gl + r * L;
@@ -613,6 +637,10 @@ __device__ __forceinline__ void face_terms_dir(const KParams &P, const double *c
                     const int n = sp<DIM, Np>(line_node<DIM, Np, D>(fn, side ? N : 0));
 #pragma unroll
                     for (int i = 0; i <= DIM; i++) {
+                        if (BDR && bslot[r]) {
+                            acc[(1 + i) * ST + n] += sb * fv[r][i];
+                            continue;
+                        }
                         const double x = sc * fv[r][i];
                         if (side) acc[(1 + i) * ST + n] += x;
                         else acc[(1 + i) * ST + n] -= x;
@@ -1033,7 +1061,7 @@ __device__ __noinline__ double boundary_node_terms(const KParams &P, const doubl
     const double nrm = sgn * C_AREA(c)[D];
     double F[NV];
     double lam;
-    if (type == BC_SLIP_WALL) {
+    if (type == BC_SLIP_WALL || type == BC_NOSLIP_ADIABATIC) {  // the no-slip wall derives from the slip wall
         const double rho = s[0];
         double vsq = 0.0;
         {
@@ -1236,7 +1264,51 @@ __device__ __forceinline__ void lift_face_node(const KParams &P, const double *c
     }
 }
 
-template <int DIM, int N>
+// BR1 jump of a boundary face node (LiftingBR1::AssembleLiftingBdrFaceVector,
+// LiftingBR1.cpp:311-345, with ComputeBdrFaceLiftingFlux): the element is
+// element 1 and the normal points out of it; 0.5 (w(s2) - w1) for the
+// prescribed states (BdrFaceIntegrator.cpp:275-282, without the reference's
+// in-place division of w1, which the reference-value operator would need),
+// 0 for the outflow, (w1_0, beta V, -beta) - w1 for the no-slip wall
+// (NoSlipAdiabWallBdrFaceIntegrator.cpp:74-95).  Fixed operator only.
+template <int DIM, int N, int D>
+__device__ __noinline__ void lift_boundary_node(const KParams &P, const double *c, int64_t a, int fn, int side, int b,
+                                                double *dst)
+{
+    using S = Shape<DIM, N>;
+    constexpr int Np = S::Np, NDOF = S::NDOF, NV = S::NV;
+    const int64_t nn = P.nnodes;
+    const int n = line_node<DIM, Np, D>(fn, side ? N : 0);
+    double s[NV], w1[NV], f[NV];
+#pragma unroll
+    for (int v = 0; v < NV; v++) s[v] = __ldg(P.u + v * nn + a * NDOF + n);
+    entropy_vars<DIM>(s, P.gamma, P.gm1, P.gm1inv, w1);
+    const double *bc = P.bc + b * BC_SLOT;
+    const int type = (int)bc[0];
+    if (type == BC_NOSLIP_ADIABATIC) {
+        const double beta = -w1[NV - 1];
+        f[0] = w1[0] - w1[0];
+#pragma unroll
+        for (int q = 0; q < DIM; q++) f[1 + q] = bc[1 + q] * beta - w1[1 + q];
+        f[NV - 1] = -beta - w1[NV - 1];
+    } else if (type == BC_SUPERSONIC_INFLOW || type == BC_SPECIFIED_STATE) {
+        double w2[NV];
+        entropy_vars<DIM>(bc + 1, P.gamma, P.gm1, P.gm1inv, w2);
+#pragma unroll
+        for (int v = 0; v < NV; v++) f[v] = (w2[v] - w1[v]) * 0.5;
+    } else {
+#pragma unroll
+        for (int v = 0; v < NV; v++) f[v] = 0.0;
+    }
+    const double nrm = side ? C_AREA(c)[D] : -C_AREA(c)[D];
+#pragma unroll
+    for (int v = 0; v < NV; v++) dst[v] = C_FACE(c) * (f[v] * nrm);
+}
+
+// BDR: the mesh has boundary faces (Navier-Stokes): a face towards the
+// boundary takes its jump from lift_boundary_node, the -D boundary faces into
+// P.lbuf_lo.
+template <int DIM, int N, bool BDR = false>
 __global__ void __launch_bounds__(256) lift_face_kernel(const KParams P)
 {
     using S = Shape<DIM, N>;
@@ -1251,6 +1323,22 @@ __global__ void __launch_bounds__(256) lift_face_kernel(const KParams P)
         const int64_t r = t - d * per_dir;
         const int64_t a = r / NFN;
         const int fn = (int)(r - a * NFN);
+        if (BDR) {
+            const int32_t bp = __ldg(P.nbr + a * 2 * DIM + 2 * d + 1), bm = __ldg(P.nbr + a * 2 * DIM + 2 * d);
+            double *dp = P.lbuf + ((d * P.ne + a) * NFN + fn) * (DIM + 2);
+            double *dm = P.lbuf_lo + ((d * P.ne + a) * NFN + fn) * (DIM + 2);
+            if (bp < 0) {
+                if (d == 0) lift_boundary_node<DIM, N, 0>(P, c, a, fn, 1, -1 - bp, dp);
+                else if (d == 1) lift_boundary_node<DIM, N, 1>(P, c, a, fn, 1, -1 - bp, dp);
+                else lift_boundary_node<DIM, N, (DIM == 3 ? 2 : 0)>(P, c, a, fn, 1, -1 - bp, dp);
+            }
+            if (bm < 0) {
+                if (d == 0) lift_boundary_node<DIM, N, 0>(P, c, a, fn, 0, -1 - bm, dm);
+                else if (d == 1) lift_boundary_node<DIM, N, 1>(P, c, a, fn, 0, -1 - bm, dm);
+                else lift_boundary_node<DIM, N, (DIM == 3 ? 2 : 0)>(P, c, a, fn, 0, -1 - bm, dm);
+            }
+            if (bp < 0) continue;
+        }
         if (d == 0) lift_face_node<DIM, N, 0>(P, c, a, fn);
         else if (d == 1) lift_face_node<DIM, N, 1>(P, c, a, fn);
         else lift_face_node<DIM, N, (DIM == 3 ? 2 : 0)>(P, c, a, fn);
@@ -1330,7 +1418,9 @@ __device__ __forceinline__ void divergence_lines(const double *fvs, double *dv, 
 // stored to P.vbuf when the volume kernel with element-side faces runs after
 // this one) and the normal column at every face node (with the node's own
 // state, DGSEMIntegrator.cpp:467-477, written to P.fcol).
-template <int DIM, int N>
+// BDR: jumps of -d boundary faces come from P.lbuf_lo (Navier-Stokes meshes
+// with boundary faces).
+template <int DIM, int N, bool BDR = false>
 __global__ void __launch_bounds__(128) lift_kernel(const KParams P)
 {
     using S = Shape<DIM, N>;
@@ -1414,7 +1504,8 @@ __global__ void __launch_bounds__(128) lift_kernel(const KParams P)
                     const int line = d == 0 ? (DIM == 2 ? idx[1] : idx[1] + Np * idx[2])
                                             : (d == 1 ? (DIM == 2 ? idx[0] : idx[0] + Np * idx[2]) : idx[0] + Np * idx[1]);
                     const int64_t owner = pos == N ? e : enb[d];
-                    const double *F = P.lbuf + ((d * P.ne + owner) * NFN + line) * NV;
+                    const double *F = (BDR && owner < 0) ? P.lbuf_lo + ((d * P.ne + e) * NFN + line) * NV
+                                                         : P.lbuf + ((d * P.ne + owner) * NFN + line) * NV;
 #pragma unroll
                     for (int v = 0; v < NV; v++) jf[d][v] = face ? __ldg(F + v) : 0.0;
                 }

@@ -147,3 +147,55 @@ def test_gpu_vjp_with_boundaries_matches_autograd(name, order, blending, cuda_de
     got = op.vjp(dev(u, cuda_device), dev(c, cuda_device)).cpu().numpy()
     assert rel_maxnorm(got, want.numpy()) < 1e-11
     assert op.check() == 0
+
+
+@pytest.mark.parametrize("order", [1, 2, 3])
+@pytest.mark.parametrize("name", ["ns_2d_channel", "ns_2d_cavity", "ns_3d_channel"])
+def test_gpu_ns_boundaries_match_oracle(name, order, cuda_device):
+    """Navier-Stokes boundary faces (BR1 boundary lifting, viscous boundary
+    fluxes, no-slip wall) of the fixed operator against the oracle, whose
+    boundary code is pinned to the reference's (tests/test_boundaries.py)."""
+    import torch
+    from test_boundaries import NS_KW, ns_layout_case
+    mesh, u = ns_layout_case(name, order)
+    op = pb.DGSEMOperator(mesh, compat=0, **NS_KW)
+    orc = oracle.Oracle(mesh, compat=0, **NS_KW)
+    ref = orc.rhs(u)
+    x = dev(u, cuda_device)
+    out = torch.empty_like(x)
+    op.Mult(x, out)
+    torch.cuda.synchronize()
+    assert rel_maxnorm(out.cpu().numpy(), ref) < TOL
+    g = op.gradients(x).cpu().numpy()
+    assert rel_maxnorm(g, orc.gradients()) < 1e-11
+    dt = 0.2 * min(mesh.h) / (orc.max_char_speed() * (order + 1) ** 2)
+    us = dev(rough(u, mesh, 8, 0.01, 0.001), cuda_device)
+    for stage in (0, 1, 2):
+        y = torch.empty_like(x)
+        op.rk_stage(stage, dt, x, us, y)
+        torch.cuda.synchronize()
+        assert rel_maxnorm(y.cpu().numpy(), orc.rk_stage(stage, dt, u, us.cpu().numpy())) < TOL
+    a, b = x.clone(), x.clone()
+    op.rk3_step(a, dt, nsteps=2)
+    op.rk3_step(b, dt, nsteps=2, graph=True)
+    torch.cuda.synchronize()
+    assert torch.equal(a, b)
+    assert op.check() == 0
+
+
+def test_ns_boundary_errors(cuda_device):
+    import torch
+    from test_boundaries import NS_KW, ns_layout_case
+    mesh, u = ns_layout_case("ns_2d_channel", 2)
+    with pytest.raises(pb.PdgError) as ei:          # reference-value operator: not built
+        pb.DGSEMOperator(mesh, compat=1, **NS_KW)
+    assert ei.value.code == 5
+    op = pb.DGSEMOperator(mesh, compat=0, **NS_KW)
+    x = dev(u, cuda_device)
+    with pytest.raises(pb.PdgError) as ei:          # no adjoint of NS boundary faces
+        op.vjp(x, x)
+    assert ei.value.code == 5
+    op.set_boundary(2, pb.BC_SLIP_WALL)             # no viscous flux in the reference
+    with pytest.raises(pb.PdgError) as ei:
+        op.Mult(x, torch.empty_like(x))
+    assert ei.value.code == 5
