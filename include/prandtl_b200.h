@@ -113,7 +113,7 @@ int pdg_destroy(pdg_ctx *ctx);
  * boundary face with condition b; every condition the mesh uses must be set
  * before the first evaluation (else PDG_ERR_ARG).  Navier-Stokes boundary
  * faces: fixed operator only (pdg_create returns PDG_ERR_UNSUPPORTED with
- * compat = 1) and types 1, 2, 3 and 10 (others: PDG_ERR_UNSUPPORTED at the
+ * compat = 1) and types 1, 2, 3, 10 and 11 (others: PDG_ERR_UNSUPPORTED at the
  * first evaluation); pdg_rhs_vjp differentiates every condition of an Euler
  * mesh and none of a Navier-Stokes one.  `state` holds the condition's
  * data as listed beside each type (conserved, dim + 2 values, for the two
@@ -134,6 +134,7 @@ int pdg_destroy(pdg_ctx *ctx);
 #define PDG_BC_SUBSONIC_INFLOW_PTTT 8  /* SubsonicInflowPtTtAngBdrFaceIntegrator, 2D: state = {cp, pt, Tt, theta, phi} (degrees) */
 #define PDG_BC_RIEMANN_INVARIANT  9  /* RiemannInvariantBdrFaceIntegrator: state = primitive {rho, v[dim], p} */
 #define PDG_BC_NOSLIP_ADIABATIC  10  /* NoSlipAdiabWallBdrFaceIntegrator, zero heat flux: state = wall velocity {V[dim]} */
+#define PDG_BC_NOSLIP_ISOTHERMAL 11  /* NoSlipIsothWallBdrFaceIntegrator: state = {T_wall, V[dim]}, with params.R_gas */
 int pdg_set_boundary(pdg_ctx *ctx, int index, int type, const double *state);
 
 /* TimeDependentOperator::Height (DGSEMOperator.cpp:18): number of vdofs. */

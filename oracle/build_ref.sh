@@ -26,7 +26,7 @@ FILES="$SRC/BasicOperations/BasicOperations.cpp $SRC/RiemannSolvers/Chandrasheka
  $SRC/Integrators/BoundaryConditions/SupersonicOutflowBdrFaceIntegrator.cpp $SRC/Integrators/BoundaryConditions/SpecifiedStateBdrFaceIntegrator.cpp $SRC/Integrators/BoundaryConditions/SymmetryBdrFaceIntegrator.cpp \
  $SRC/Integrators/BoundaryConditions/SubsonicOutflowPBdrFaceIntegrator.cpp $SRC/Integrators/BoundaryConditions/SubsonicInflowRVBdrFaceIntegrator.cpp \
  $SRC/Integrators/BoundaryConditions/SubsonicInflowPtTtAngBdrFaceIntegrator.cpp $SRC/Integrators/BoundaryConditions/RiemannInvariantBdrFaceIntegrator.cpp \
- $SRC/Integrators/BoundaryConditions/NoSlipAdiabWallBdrFaceIntegrator.cpp \
+ $SRC/Integrators/BoundaryConditions/NoSlipAdiabWallBdrFaceIntegrator.cpp $SRC/Integrators/BoundaryConditions/NoSlipIsothWallBdrFaceIntegrator.cpp \
  $HERE/ref_shim/ref_driver.cpp"
 CXXFLAGS="-O2 -ffp-contract=off -std=c++17 -shared -fPIC -w"
 g++ $CXXFLAGS $INC -DSUBCELL_FV_BLENDING $FILES -o "$OUT/libref_euler.so"

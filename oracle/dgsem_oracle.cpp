@@ -902,7 +902,7 @@ static double bdr_flux(const Ctx &c, int b, const double *s1, const double *nor,
     const int type = (int)c.bc[b][0];
     double s2[5], un[3];
     for (int v = 0; v < nv; v++) s2[v] = s1[v];
-    if (type == 4 || type == 10) {
+    if (type == 4 || type == 10 || type == 11) {
         // SlipWallBdrFaceIntegrator::ComputeBdrFaceInviscidFlux (:15-58); the
         // no-slip wall derives from it
         const double gammaP1 = 1.0 + gamma, gammaP1Inverse = 1.0 / gammaP1;
@@ -1048,7 +1048,7 @@ static double bdr_face_vector(const Ctx &c, const double *u, int64_t e, int d, i
         lam = std::max(lam, bdr_flux(c, b, s1, nor, flux));
         double dU[5];
         for (int v = 0; v < nv; v++) dU[v] = -flux[v];
-        if (c.p.parabolic && (type == 2 || type == 10)) {
+        if (c.p.parabolic && (type == 2 || type == 10 || type == 11)) {
             // ComputeBdrFaceViscousFlux: the interior state's viscous flux
             // with its own gradients (SupersonicOutflowBdrFaceIntegrator.cpp:
             // 15-20); the no-slip wall replaces the energy row by the wall
@@ -1088,8 +1088,10 @@ static void bdr_lifting_flux(const Ctx &c, int b, const double *s1, const double
     const int type = (int)c.bc[b][0];
     double w1[5];
     for (int v = 0; v < nv; v++) w1[v] = w1_in[v];
-    if (type == 10) {
-        const double beta = -w1[nv - 1];
+    if (type == 10 || type == 11) {
+        // the isothermal wall (NoSlipIsothWallBdrFaceIntegrator.cpp:41-65)
+        // takes 1/(R T_wall), stored after the wall velocity, for beta
+        const double beta = type == 10 ? -w1[nv - 1] : c.bc[b][1 + dim];
         f[0] = w1[0];
         for (int q = 0; q < dim; q++) f[1 + q] = c.bc[b][1 + q] * beta;
         f[nv - 1] = -beta;
@@ -1485,14 +1487,19 @@ void orc_destroy(void *h) { delete (Ctx *)h; }
 // Boundary condition `index`: its type and parameters as pdg_set_boundary
 // takes them (types 1, 3: conserved state; 6: p; 7: rho, velocity; 8: cp,
 // pt, Tt, theta, phi in degrees, stored as cp, pt, Tt, cos theta, sin theta;
-// 9: primitive state rho, velocity, p; 10: wall velocity).
+// 9: primitive state rho, velocity, p; 10: wall velocity; 11: wall
+// temperature and velocity, stored as velocity, 1/(R T)).
 void orc_set_boundary(void *h, int index, int type, const double *state)
 {
     Ctx &c = *(Ctx *)h;
     if (index < 0 || index >= 16) return;
-    const int n = type == 6 ? 1 : type == 7 ? 1 + c.dim : type == 8 ? 5 : type == 10 ? c.dim : c.nv;
+    const int n = type == 6 ? 1 : type == 7 ? 1 + c.dim : type == 8 ? 5 : type == 10 ? c.dim : type == 11 ? 1 + c.dim : c.nv;
     c.bc[index][0] = type;
     for (int v = 0; v < 7; v++) c.bc[index][1 + v] = (state && v < n) ? state[v] : 0.0;
+    if (type == 11 && state) {  // {T, V} -> V, 1/(R T)
+        for (int q = 0; q < c.dim; q++) c.bc[index][1 + q] = state[1 + q];
+        c.bc[index][1 + c.dim] = 1.0 / (c.p.R_gas * state[0]);
+    }
     if (type == 8) {
         const double theta = c.bc[index][4];
         c.bc[index][4] = std::cos(theta * M_PI / 180.0);

@@ -26,6 +26,7 @@
 #include "SubsonicInflowPtTtAngBdrFaceIntegrator.hpp"
 #include "RiemannInvariantBdrFaceIntegrator.hpp"
 #include "NoSlipAdiabWallBdrFaceIntegrator.hpp"
+#include "NoSlipIsothWallBdrFaceIntegrator.hpp"
 #include "DGSEMIntegrator.hpp"
 #include "ModalBasis.hpp"
 #include "NavierStokesFlux.hpp"
@@ -312,7 +313,7 @@ int ref_set_boundary(void *h, int index, int type, const double *state)
     RefCtx &c = *(RefCtx *)h;
     if (index < 0 || index >= 16) return 1;
     const bool full = type == 1 || type == 3 || type == 9;  // a whole (conserved or primitive) state
-    if (!state && type == 10) return 1;
+    if (!state && (type == 10 || type == 11)) return 1;
     Vector st(c.nv);
     for (int v = 0; v < c.nv; v++) st(v) = (state && full) ? state[v] : 0.0;
     if (!state && type >= 6) return 1;
@@ -340,6 +341,14 @@ int ref_set_boundary(void *h, int index, int type, const double *state)
         V = 0.0;
         for (int d = 0; d < c.dim; d++) V(d) = state[d];
         b = new NoSlipAdiabWallBdrFaceIntegrator(c.lifting, *c.rsolver, c.Np, c.time, c.gamma, 0.0, V);
+        break;
+    }
+    case 11: {  // no-slip isothermal wall: state = {T, V}; R = 287 as in ref_create
+        Vector V(3);
+        V = 0.0;
+        for (int d = 0; d < c.dim; d++) V(d) = state[1 + d];
+        double T = state[0];
+        b = new NoSlipIsothWallBdrFaceIntegrator(c.lifting, *c.rsolver, c.Np, c.time, c.gamma, 287.0, T, V);
         break;
     }
     default: return 1;

@@ -134,7 +134,7 @@ class TorchDGSEM:
         if self.bcs and parabolic:
             raise ValueError("boundary faces: Euler only")
         for b, (typ, _) in self.bcs.items():
-            if typ not in range(1, 10):
+            if typ not in range(1, 12):
                 raise ValueError(f"boundary condition {b}: unknown type {typ}")
             if typ == 8 and self.dim != 2:
                 raise ValueError("the total-pressure inflow is 2D only")
@@ -195,7 +195,7 @@ class TorchDGSEM:
         """Normal flux of a boundary face (src/Integrators/BoundaryConditions):
         interior trace s1, outward normal sgn |n_d| e_d."""
         nrm = sgn * self.area[d]
-        if typ == 4:  # slip wall (SlipWallBdrFaceIntegrator.cpp:15-58)
+        if typ in (4, 10, 11):  # slip wall (SlipWallBdrFaceIntegrator.cpp:15-58); no-slip walls derive from it
             rho, vel, p = self.prims(s1)
             vn = sgn * vel[d]
             an = torch.sqrt(self.gamma * p / rho)

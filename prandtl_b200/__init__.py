@@ -42,7 +42,7 @@ KERNEL_LIFT_FACE_BDR, KERNEL_LIFT_BDR, KERNEL_NS_FACES_BDR = 25, 26, 27
 # boundary condition types (pdg_set_boundary)
 BC_SUPERSONIC_INFLOW, BC_SUPERSONIC_OUTFLOW, BC_SPECIFIED_STATE, BC_SLIP_WALL, BC_SYMMETRY = 1, 2, 3, 4, 5
 BC_SUBSONIC_OUTFLOW_P, BC_SUBSONIC_INFLOW_RV, BC_SUBSONIC_INFLOW_PTTT, BC_RIEMANN_INVARIANT = 6, 7, 8, 9
-BC_NOSLIP_ADIABATIC = 10
+BC_NOSLIP_ADIABATIC, BC_NOSLIP_ISOTHERMAL = 10, 11
 MAX_BOUNDARIES = 16
 PDG_FLAG_NONFINITE = 1
 PDG_FLAG_NONPHYSICAL = 2

@@ -892,12 +892,12 @@ __global__ void __launch_bounds__(256) adj_boundary_kernel(const KParams P, cons
                     Fb[v] = -C_FACE(c) * __ldg(cot + v * nn + a * NDOF + n);
                     g[v] = 0.0;
                 }
-                if (type == BC_SLIP_WALL) {
+                if (type == BC_SLIP_WALL || type == BC_NOSLIP_ADIABATIC || type == BC_NOSLIP_ISOTHERMAL) {
                     slip_wall_vjp<DIM>(P, s1, D, sgn, Fb[1 + D] * nrm, g);
                 } else {
                     double s2[NV];
                     const bool given = type == BC_SUPERSONIC_INFLOW || type == BC_SPECIFIED_STATE;
-                    const bool sub = type >= BC_SUBSONIC_OUTFLOW_P;
+                    const bool sub = type >= BC_SUBSONIC_OUTFLOW_P && type <= BC_RIEMANN_INVARIANT;
                     // Jacobian of the outer state (columns by forward mode)
                     double Jm[NV][NV];
 #pragma unroll

@@ -489,7 +489,7 @@ int evaluate(pdg_ctx *c, int stage, double dt, const double *un, const double *u
             for (int b = 0; b < PDG_MAX_BOUNDARIES; b++) {
                 const int t = (int)c->bc_host[b * BC_SLOT];
                 if ((c->bc_used >> b & 1u) && t != PDG_BC_SUPERSONIC_INFLOW && t != PDG_BC_SUPERSONIC_OUTFLOW &&
-                    t != PDG_BC_SPECIFIED_STATE && t != PDG_BC_NOSLIP_ADIABATIC)
+                    t != PDG_BC_SPECIFIED_STATE && t != PDG_BC_NOSLIP_ADIABATIC && t != PDG_BC_NOSLIP_ISOTHERMAL)
                     return fail(c, PDG_ERR_UNSUPPORTED,
                                 "boundary condition %d: type %d has no viscous boundary flux here", b, t);
             }
@@ -628,7 +628,7 @@ int pdg_set_boundary(pdg_ctx *c, int index, int type, const double *state)
     if (!c) return PDG_ERR_ARG;
     if (index < 0 || index >= PDG_MAX_BOUNDARIES)
         return fail(c, PDG_ERR_ARG, "pdg_set_boundary: index %d outside [0, %d)", index, PDG_MAX_BOUNDARIES);
-    if (type < PDG_BC_SUPERSONIC_INFLOW || type > PDG_BC_NOSLIP_ADIABATIC)
+    if (type < PDG_BC_SUPERSONIC_INFLOW || type > PDG_BC_NOSLIP_ISOTHERMAL)
         return fail(c, PDG_ERR_ARG, "pdg_set_boundary: unknown boundary type %d", type);
     if (type == PDG_BC_SUBSONIC_INFLOW_PTTT && c->dim != 2)
         return fail(c, PDG_ERR_UNSUPPORTED, "pdg_set_boundary: the total-pressure inflow is 2D only");
@@ -636,6 +636,7 @@ int pdg_set_boundary(pdg_ctx *c, int index, int type, const double *state)
     const int n = type == PDG_BC_SUBSONIC_OUTFLOW_P ? 1
                   : type == PDG_BC_SUBSONIC_INFLOW_RV ? 1 + c->dim
                   : type == PDG_BC_NOSLIP_ADIABATIC ? c->dim
+                  : type == PDG_BC_NOSLIP_ISOTHERMAL ? 1 + c->dim
                   : type == PDG_BC_SUBSONIC_INFLOW_PTTT ? 5
                   : (type == PDG_BC_SUPERSONIC_INFLOW || type == PDG_BC_SPECIFIED_STATE || type == PDG_BC_RIEMANN_INVARIANT)
                       ? c->nv : 0;
@@ -654,11 +655,17 @@ int pdg_set_boundary(pdg_ctx *c, int index, int type, const double *state)
             ok = ok && state[0] > 0.0 && state[1] > 0.0 && state[2] > 0.0;
         } else if (type == PDG_BC_NOSLIP_ADIABATIC) {
             // any wall velocity
+        } else if (type == PDG_BC_NOSLIP_ISOTHERMAL) {
+            ok = ok && state[0] > 0.0 && c->p.R_gas > 0.0;
         } else {
             ok = ok && state[0] > 0.0;
         }
         if (!ok) return fail(c, PDG_ERR_ARG, "pdg_set_boundary: the data of condition %d is not physical", index);
         for (int v = 0; v < n; v++) slot[1 + v] = state[v];
+        if (type == PDG_BC_NOSLIP_ISOTHERMAL) {  // {T, V} -> V, 1/(R T) (the integrator's constructor)
+            for (int q = 0; q < c->dim; q++) slot[1 + q] = state[1 + q];
+            slot[1 + c->dim] = 1.0 / (c->p.R_gas * state[0]);
+        }
         if (type == PDG_BC_SUBSONIC_INFLOW_PTTT) {  // flow angle -> direction (the integrator's constructor)
             const double theta = state[3];
             slot[4] = std::cos(theta * M_PI / 180.0);

@@ -94,7 +94,7 @@ struct KParams {
 constexpr int BC_SLOT = 8;
 constexpr int BC_SUPERSONIC_INFLOW = 1, BC_SUPERSONIC_OUTFLOW = 2, BC_SPECIFIED_STATE = 3, BC_SLIP_WALL = 4,
               BC_SYMMETRY = 5, BC_SUBSONIC_OUTFLOW_P = 6, BC_SUBSONIC_INFLOW_RV = 7, BC_SUBSONIC_INFLOW_PTTT = 8,
-              BC_RIEMANN_INVARIANT = 9, BC_NOSLIP_ADIABATIC = 10;
+              BC_RIEMANN_INVARIANT = 9, BC_NOSLIP_ADIABATIC = 10, BC_NOSLIP_ISOTHERMAL = 11;
 
 constexpr int pow2_at_least(int x) { return x <= 1 ? 1 : x <= 2 ? 2 : x <= 4 ? 4 : x <= 8 ? 8 : x <= 16 ? 16 : 32; }
 
@@ -609,7 +609,8 @@ __device__ __forceinline__ void face_terms_dir(const KParams &P, const double *c
                         const int type = (int)bc[0];
                         const double nrm = side ? C_AREA(c)[D] : -C_AREA(c)[D];
                         const double *fo = P.fcol + (((D * 2 + side) * ne + e) * NFN + fn) * (NV - 1);
-                        const bool own = type == BC_SUPERSONIC_OUTFLOW || type == BC_NOSLIP_ADIABATIC;
+                        const bool own = type == BC_SUPERSONIC_OUTFLOW || type == BC_NOSLIP_ADIABATIC ||
+                                         type == BC_NOSLIP_ISOTHERMAL;
 #pragma unroll
                         for (int i = 0; i <= DIM; i++) fv[r][i] = own ? __ldg(fo + i) * nrm : 0.0;
                         if (type == BC_NOSLIP_ADIABATIC) {  // energy row: the wall velocity's work, qn = 0
@@ -1061,7 +1062,7 @@ __device__ __noinline__ double boundary_node_terms(const KParams &P, const doubl
     const double nrm = sgn * C_AREA(c)[D];
     double F[NV];
     double lam;
-    if (type == BC_SLIP_WALL || type == BC_NOSLIP_ADIABATIC) {  // the no-slip wall derives from the slip wall
+    if (type == BC_SLIP_WALL || type == BC_NOSLIP_ADIABATIC || type == BC_NOSLIP_ISOTHERMAL) {  // no-slip walls derive from the slip wall
         const double rho = s[0];
         double vsq = 0.0;
         {
@@ -1101,7 +1102,7 @@ __device__ __noinline__ double boundary_node_terms(const KParams &P, const doubl
             s2[v] = given ? bc[1 + v] : s[v];
         }
         if (type == BC_SYMMETRY) s2[1 + D] = -s[1 + D];
-        if (type >= BC_SUBSONIC_OUTFLOW_P)
+        if (type >= BC_SUBSONIC_OUTFLOW_P && type <= BC_RIEMANN_INVARIANT)
             subsonic_outer_state<DIM, D>(P, type, bc + 1, sgn, s1, s2);
         const Prim<DIM> qa = make_prim<DIM>(s1, P.gamma, P.gm1), qb = make_prim<DIM>(s2, P.gamma, P.gm1);
         double ma[DIM], mb[DIM];
@@ -1285,8 +1286,10 @@ __device__ __noinline__ void lift_boundary_node(const KParams &P, const double *
     entropy_vars<DIM>(s, P.gamma, P.gm1, P.gm1inv, w1);
     const double *bc = P.bc + b * BC_SLOT;
     const int type = (int)bc[0];
-    if (type == BC_NOSLIP_ADIABATIC) {
-        const double beta = -w1[NV - 1];
+    if (type == BC_NOSLIP_ADIABATIC || type == BC_NOSLIP_ISOTHERMAL) {
+        // the isothermal wall (NoSlipIsothWallBdrFaceIntegrator.cpp:41-65)
+        // takes 1/(R T_wall), stored after the wall velocity, for beta
+        const double beta = type == BC_NOSLIP_ADIABATIC ? -w1[NV - 1] : bc[1 + DIM];
         f[0] = w1[0] - w1[0];
 #pragma unroll
         for (int q = 0; q < DIM; q++) f[1 + q] = bc[1 + q] * beta - w1[1 + q];

@@ -101,6 +101,10 @@ def layouts():
         "2d_subsonic": (2, dict(bdr=[(0, 1), (2, 3)], boundaries={
             0: (pb.BC_SUBSONIC_INFLOW_PTTT, [3.5, 3.0, 2.0, 10.0, 0.0]), 1: (pb.BC_SUBSONIC_OUTFLOW_P, [2.2]),
             2: (pb.BC_RIEMANN_INVARIANT, [1.0, 0.3, -0.1, 2.0]), 3: (pb.BC_SUBSONIC_INFLOW_RV, [1.3, 0.2, 0.05])})),
+        # no-slip walls in an Euler run act as slip walls (their viscous parts
+        # are not evaluated)
+        "2d_noslip_euler": (2, dict(bdr=[None, (0, 1)], boundaries={
+            0: (pb.BC_NOSLIP_ADIABATIC, [0.0, 0.0]), 1: (pb.BC_NOSLIP_ISOTHERMAL, [0.009, 0.2, 0.0])})),
         # forward-facing step: the bottom row is removed from x = -1 + 2/5 * 2 on
         "2d_step": (2, dict(bdr=[(0, 1), (2, 2)], keep=_step_keep((5, 4)), cut=2, boundaries={
             0: (pb.BC_SUPERSONIC_INFLOW, np.array([1.4, 4.2, 0.0, 8.8])), 1: (pb.BC_SUPERSONIC_OUTFLOW, None),
@@ -176,6 +180,9 @@ def ns_layouts():
             0: (pb.BC_SUPERSONIC_INFLOW, fs2), 1: (pb.BC_SUPERSONIC_OUTFLOW, None), 2: (NOSLIP, [0.0, 0.0])})),
         "ns_2d_cavity": (2, dict(bdr=[(0, 0), (0, 1)], boundaries={
             0: (NOSLIP, [0.0, 0.0]), 1: (NOSLIP, [1.0, 0.0])})),
+        "ns_2d_isothermal": (2, dict(bdr=[(0, 1), (2, 3)], boundaries={
+            0: (pb.BC_SPECIFIED_STATE, fs2), 1: (pb.BC_SUPERSONIC_OUTFLOW, None),
+            2: (pb.BC_NOSLIP_ISOTHERMAL, [0.009, 0.0, 0.0]), 3: (pb.BC_NOSLIP_ISOTHERMAL, [0.007, 0.3, 0.0])})),
         "ns_3d_channel": (3, dict(bdr=[(0, 1), (2, 2), None], boundaries={
             0: (pb.BC_SPECIFIED_STATE, fs3), 1: (pb.BC_SUPERSONIC_OUTFLOW, None), 2: (NOSLIP, [0.1, 0.0, 0.0])})),
     }

@@ -150,7 +150,7 @@ def test_gpu_vjp_with_boundaries_matches_autograd(name, order, blending, cuda_de
 
 
 @pytest.mark.parametrize("order", [1, 2, 3])
-@pytest.mark.parametrize("name", ["ns_2d_channel", "ns_2d_cavity", "ns_3d_channel"])
+@pytest.mark.parametrize("name", ["ns_2d_channel", "ns_2d_cavity", "ns_2d_isothermal", "ns_3d_channel"])
 def test_gpu_ns_boundaries_match_oracle(name, order, cuda_device):
     """Navier-Stokes boundary faces (BR1 boundary lifting, viscous boundary
     fluxes, no-slip wall) of the fixed operator against the oracle, whose
