@@ -1,5 +1,6 @@
-"""Slab decomposition of a periodic Cartesian mesh over ranks, with a ghost
-layer exchange per RK stage.
+"""Slab decomposition of a Cartesian mesh (periodic along its last axis,
+optionally with boundary faces on the others) over ranks, with a ghost layer
+exchange per RK stage.
 
 The reference partitions elements over MPI ranks and exchanges face-neighbour
 data once per right-hand-side pass (``ExchangeFaceNbrData``,
@@ -25,15 +26,18 @@ from __future__ import annotations
 
 import numpy as np
 
-from .mesh import CartesianMesh, periodic_box
+from .mesh import CartesianMesh, box
 
 
 class SlabDecomposition:
-    """Rank `rank`'s share of periodic_box(dim, order, n, lo, hi) split into
-    `world` slabs of element layers along the last axis."""
+    """Rank `rank`'s share of box(dim, order, n, lo, hi, bdr, boundaries)
+    split into `world` slabs of element layers along the last axis, which
+    stays periodic; boundary faces of the other axes keep their conditions."""
 
-    def __init__(self, dim: int, order: int, n, lo, hi, world: int, rank: int):
-        self.glob = periodic_box(dim, order, n, lo, hi)
+    def __init__(self, dim: int, order: int, n, lo, hi, world: int, rank: int, bdr=None, boundaries=None):
+        if bdr is not None and bdr[-1] is not None:
+            raise ValueError("the last axis (the slab axis) must stay periodic")
+        self.glob = box(dim, order, n, lo, hi, bdr=bdr, boundaries=boundaries)
         self.dim, self.order, self.world, self.rank = dim, order, world, rank
         n = self.glob.n
         nz = n[-1]
@@ -55,14 +59,15 @@ class SlabDecomposition:
         self.ghost_lo_pos = pos[self.lo_layer] if world > 1 else None
         self.ghost_hi_pos = pos[self.hi_layer] if world > 1 else None
         # local neighbour table: global neighbours mapped to local indices, a
-        # neighbour that is not held maps to the element itself
+        # neighbour that is not held maps to the element itself, a boundary
+        # face (negative entry) keeps its condition
         gl = np.array([g * ls + k for g in self.layers for k in range(ls)], dtype=np.int64)
         g2l = {int(g): i for i, g in enumerate(gl)}
         gn = self.glob.nbr[gl]
         ln = np.empty_like(gn)
         for i in range(gn.shape[0]):
             for f in range(gn.shape[1]):
-                ln[i, f] = g2l.get(int(gn[i, f]), i)
+                ln[i, f] = gn[i, f] if gn[i, f] < 0 else g2l.get(int(gn[i, f]), i)
         self.global_elements = gl
         h = self.glob.h
         nloc = tuple(n[:-1]) + (len(self.layers),)
@@ -70,7 +75,8 @@ class SlabDecomposition:
         hi_l = tuple(self.glob.lo[d] + nloc[d] * h[d] for d in range(dim))
         # the global element extents exactly (a slab's own (hi - lo) / n can
         # differ in the last bit, which would change every metric term)
-        self.mesh = CartesianMesh(dim, order, nloc, lo_l, hi_l, ln.astype(np.int32), spacing=tuple(h))
+        self.mesh = CartesianMesh(dim, order, nloc, lo_l, hi_l, ln.astype(np.int32), spacing=tuple(h),
+                                  boundaries=dict(self.glob.boundaries or {}))
 
     # ---- state scatter / gather (host numpy, byNODES) ----
     def scatter(self, u_global: np.ndarray) -> np.ndarray:

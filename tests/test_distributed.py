@@ -33,13 +33,19 @@ CASES = {
     "euler2d": dict(dim=2, order=3, n=(4, 5), lo=-1.0, hi=1.0, params=dict(parabolic=0)),
     # two layers on two ranks: each rank's two ghost layers are the same layer
     "euler2d_thin": dict(dim=2, order=2, n=(4, 2), lo=-1.0, hi=1.0, params=dict(parabolic=0)),
+    # boundary faces across the slab axis: a Navier-Stokes channel (specified
+    # state in, outflow out) and Euler slip / symmetry walls
+    "ns2d_channel": dict(dim=2, order=2, n=(4, 6), lo=-1.0, hi=1.0, params=dict(parabolic=1, mu=0.02, Pr=0.71),
+                         bdr=[(0, 1), None], boundaries={0: (3, [1.2, 0.3, -0.2, 2.6]), 1: (2, None)}),
+    "euler3d_walls": dict(dim=3, order=2, n=(3, 2, 6), lo=0.0, hi=2 * np.pi, params=dict(parabolic=0),
+                          bdr=[(0, 0), (1, 1), None], boundaries={0: (4, None), 1: (5, None)}),
 }
 
 
 def initial(case):
     c = CASES[case]
-    from prandtl_b200.mesh import periodic_box
-    m = periodic_box(c["dim"], c["order"], c["n"], c["lo"], c["hi"])
+    from prandtl_b200.mesh import box
+    m = box(c["dim"], c["order"], c["n"], c["lo"], c["hi"], bdr=c.get("bdr"), boundaries=c.get("boundaries"))
     u = cases.taylor_green(m) if c["dim"] == 3 else cases.kelvin_helmholtz(m)
     rng = np.random.default_rng(7)
     u[: m.num_nodes] *= 1 + 0.05 * rng.standard_normal(m.num_nodes)
@@ -55,7 +61,8 @@ def _worker(rank, world, port, case, compat, q):
     try:
         c = CASES[case]
         gm, u0 = initial(case)
-        dec = SlabDecomposition(c["dim"], c["order"], c["n"], c["lo"], c["hi"], world, rank)
+        dec = SlabDecomposition(c["dim"], c["order"], c["n"], c["lo"], c["hi"], world, rank,
+                                bdr=c.get("bdr"), boundaries=c.get("boundaries"))
         op = OracleStages(dec.mesh, compat=compat, **c["params"])
         drv = DistributedRK3(dec, op)
         x = torch.from_numpy(dec.scatter(u0))
@@ -86,7 +93,9 @@ def _free_port():
 
 
 @pytest.mark.parametrize("world,case,compat", [(2, "ns3d", 1), (2, "ns3d", 0), (2, "euler2d", 1), (3, "ns3d", 1),
-                                               (3, "ns3d", 0), (3, "euler2d", 1), (2, "euler2d_thin", 1)])
+                                               (3, "ns3d", 0), (3, "euler2d", 1), (2, "euler2d_thin", 1),
+                                               (2, "ns2d_channel", 0), (3, "ns2d_channel", 1), (2, "euler3d_walls", 1),
+                                               (3, "euler3d_walls", 0)])
 def test_slab_decomposition_matches_undivided(world, case, compat):
     ctx = mp.get_context("spawn")
     q = ctx.Queue()
