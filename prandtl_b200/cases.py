@@ -10,7 +10,7 @@ from __future__ import annotations
 
 import numpy as np
 
-from .mesh import CartesianMesh, periodic_box
+from .mesh import CartesianMesh, box, periodic_box
 
 GAMMA = 1.4
 
@@ -98,3 +98,36 @@ def sweep_cases(num: int = 256, seed: int = 3):
     Ns = 2 + np.minimum((u[:, 1] * 4).astype(int), 3)
     eps = 1.0 + 4.0 * u[:, 2]
     return [(int(a), int(b), float(c)) for a, b, c in zip(ns, Ns, eps)]
+
+
+# Boundary-condition types as pdg_set_boundary numbers them.
+_INFLOW, _OUTFLOW, _SLIP, _NOSLIP = 1, 2, 4, 10
+
+
+def forward_facing_step(order: int = 3, cells_per_unit: int = 10, mach: float = 3.0, gamma=GAMMA):
+    """Mach-3 wind tunnel with a forward-facing step (the classic Euler
+    setup: a 3 x 1 channel, a step of height 0.2 from x = 0.6): mesh and
+    uniform initial state.  Supersonic inflow on the left, outflow on the
+    right, slip walls elsewhere (the step's faces included)."""
+    h = 1.0 / cells_per_unit
+    nx, ny = 3 * cells_per_unit, cells_per_unit
+    keep = np.ones((nx, ny), dtype=bool)
+    keep[int(round(0.6 / h)):, :int(round(0.2 / h))] = False
+    rho, p = gamma, 1.0
+    fs = prim_to_cons(2, np.array([rho]), [np.array([mach]), np.array([0.0])], np.array([p]), gamma).reshape(-1)
+    mesh = box(2, order, (nx, ny), (0.0, 0.0), (3.0, 1.0), bdr=[(0, 1), (2, 2)], keep=keep, cut=2,
+               boundaries={0: (_INFLOW, fs), 1: (_OUTFLOW, None), 2: (_SLIP, None)})
+    u = np.repeat(fs[:, None], mesh.num_nodes, axis=1).reshape(-1)
+    return mesh, u
+
+
+def lid_driven_cavity(n: int = 16, order: int = 3, lid_speed: float = 1.0, mach: float = 0.1, gamma=GAMMA):
+    """Lid-driven cavity on [0,1]^2 (Navier-Stokes): no-slip adiabatic walls,
+    the top one moving at lid_speed; fluid at rest with p = 1/(gamma Ma^2).
+    Returns the mesh and the initial state; viscosity is the caller's."""
+    mesh = box(2, order, (n, n), 0.0, 1.0, bdr=[(0, 0), (0, 1)],
+               boundaries={0: (_NOSLIP, [0.0, 0.0]), 1: (_NOSLIP, [lid_speed, 0.0])})
+    p = 1.0 / (gamma * mach * mach)
+    nn = mesh.num_nodes
+    u = prim_to_cons(2, np.ones(nn), [np.zeros(nn), np.zeros(nn)], np.full(nn, p), gamma)
+    return mesh, u.reshape(-1)

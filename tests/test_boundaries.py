@@ -215,3 +215,14 @@ def test_oracle_ns_boundaries_match_live_reference(name, order):
     assert np.abs(ro - rr).max() <= 1e-12 * np.abs(rr).max()
     go, gr = o.gradients(), r.gradients()
     assert np.abs(go - gr).max() <= 1e-11 * np.abs(gr).max()
+
+
+def test_case_builders():
+    """The forward-facing step and lid-driven cavity builders: cell masks and
+    conditions as documented; the step's walls get the slip condition."""
+    m, u = cases.forward_facing_step(2, 5)
+    assert m.num_elements == 15 * 5 - 12 * 1 and u.size == m.size
+    assert set(m.boundaries) == {0, 1, 2} and m.boundaries[2][0] == pb.BC_SLIP_WALL
+    assert (m.nbr == -3).sum() == 12 + 15 + 3 + 1   # top, bottom before the step, step front and top
+    mc, uc = cases.lid_driven_cavity(4, 2)
+    assert mc.boundaries[1] == (pb.BC_NOSLIP_ADIABATIC, [1.0, 0.0]) and uc.size == mc.size

@@ -199,3 +199,29 @@ def test_ns_boundary_errors(cuda_device):
     with pytest.raises(pb.PdgError) as ei:
         op.Mult(x, torch.empty_like(x))
     assert ei.value.code == 5
+
+
+@pytest.mark.parametrize("which", ["ffs", "cavity"])
+def test_gpu_case_builders_match_oracle(which, cuda_device):
+    """A few SSP-RK3 steps of the forward-facing step (Euler) and the
+    lid-driven cavity (Navier-Stokes) against the oracle."""
+    import torch
+    from prandtl_b200 import cases
+    if which == "ffs":
+        mesh, u = cases.forward_facing_step(2, 5)
+        kw = dict(compat=0)
+    else:
+        mesh, u = cases.lid_driven_cavity(4, 3)
+        kw = dict(compat=0, parabolic=1, mu=0.01, Pr=0.71)
+    op = pb.DGSEMOperator(mesh, **kw)
+    orc = oracle.Oracle(mesh, **kw)
+    orc.rhs(u)
+    dt = 0.2 * min(mesh.h) / (orc.max_char_speed() * (mesh.order + 1) ** 2)
+    x = dev(u, cuda_device)
+    op.rk3_step(x, dt, nsteps=3)
+    y = u
+    for _ in range(3):
+        y = orc.rk3_step(y, dt)
+    torch.cuda.synchronize()
+    assert rel_maxnorm(x.cpu().numpy(), y) < 1e-11
+    assert op.check() == 0
