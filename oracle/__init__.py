@@ -2,7 +2,7 @@
 hot-path sources built against the stand-in MFEM header (_ref/libref_*.so).
 
 TEST INFRASTRUCTURE ONLY: imported by tests/, __graft_entry__.smoke() and
-bench.py's CPU-baseline leg, always as the checker.  The product package
+bench.py's CPU-baseline leg, always as the reference result.  The product package
 (prandtl_b200) never imports this module.
 """
 from __future__ import annotations

@@ -4,7 +4,7 @@
 //
 // TEST INFRASTRUCTURE ONLY.  Nothing in the product (prandtl_b200/) links or
 // calls this file; only tests/, __graft_entry__.smoke() and bench.py's CPU
-// baseline load it, always as the checker.
+// baseline load it, always as the reference result.
 //
 // Parity status: the pointwise physics (log-mean, Chandrashekar volume and
 // face fluxes, viscous flux, entropy-variable transforms) is pinned bit for
