@@ -43,7 +43,7 @@ KERNELS = [("lift_face_kernel", (3,)), ("lift_kernel", (1,)), ("rhs_kernel<NS,fa
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=100)
+    ap.add_argument("--steps", type=int, default=300)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--n", type=int, default=32, help="elements per direction (32 = the benchmark workload)")
@@ -93,7 +93,7 @@ def config_dict(mesh, n_gpus):
 
 
 class ClockSampler:
-    """nvidia-smi clocks/throttle reasons sampled every 200 ms while running."""
+    """nvidia-smi clocks/throttle reasons sampled every 50 ms while running."""
 
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
@@ -111,13 +111,18 @@ class ClockSampler:
             self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.dev}", f"--query-gpu={self.FIELDS}",
                                           "--format=csv,noheader,nounits", "-lms", "50"],
                                          stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+            # nvidia-smi takes a moment to start: wait (up to 3 s) for its
+            # first sample so that the timed region is sampled from its start
+            t0 = time.perf_counter()
+            while time.perf_counter() - t0 < 3.0 and os.path.getsize(self.path) == 0:
+                time.sleep(0.01)
         except Exception:
             self.proc = None
 
     def stop(self):
         if self.proc is None:
             return None
-        time.sleep(0.25)
+        time.sleep(0.06)  # the sample in flight
         self.proc.terminate()
         try:
             self.proc.wait(timeout=5)
@@ -347,6 +352,7 @@ def run_ours(args):
         out["adjoint"] = run_adjoint(args, dev)
     if args.sweep_steps > 0 and world == 1:
         out["filter_case"] = run_filter_case(args, dev)
+        out["boundary_case"] = run_boundary_case(args, dev)
     if rank == 0 and world == 1 and not args.no_cpu:
         out["cpu_baseline"] = cpu_baseline(mesh, u0, params, args.cpu_seconds)
     if rank == 0:
@@ -522,6 +528,33 @@ def run_filter_case(args, dev):
     return {"workload": "kelvin_helmholtz_64x64_N4_euler_blending_entropy_filter", "vdofs": m.size, "steps": steps,
             "value": m.size * 3 * steps / (ms * 1e-3), "unit": UNIT, "ms_per_step": ms / steps,
             "element_filterings": filtered, "path": "pdg_rk3_steps (graph-replayed steps)"}
+
+
+def run_boundary_case(args, dev):
+    """Lid-driven cavity 64 x 64, N = 3, Navier-Stokes (Re = 1000 on the lid)
+    with no-slip adiabatic walls, fixed operator: 200 SSP-RK3 steps, CFL 0.5,
+    graph-replayed."""
+    import torch
+
+    import prandtl_b200 as pb
+    m, u = cases.lid_driven_cavity(64, 3)
+    op = pb.DGSEMOperator(m, parabolic=1, compat=0, mu=1e-3, Pr=0.71)
+    x = torch.from_numpy(u).to(dev)
+    op.Mult(x, torch.empty_like(x))
+    dt = op.cfl_dt(0.5)
+    steps = 200
+    op.rk3_step(x, dt, nsteps=args.warmup, graph=True)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    op.rk3_step(x, dt, nsteps=steps, graph=True)
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    op.check()
+    return {"workload": "lid_driven_cavity_64x64_N3_navier_stokes_noslip_walls", "vdofs": m.size, "steps": steps,
+            "value": m.size * 3 * steps / (ms * 1e-3), "unit": UNIT, "ms_per_step": ms / steps,
+            "path": "pdg_rk3_steps (graph-replayed steps)"}
 
 
 def _ref_worker(payload):
