@@ -537,7 +537,10 @@ __device__ __forceinline__ double face_terms_from(const KParams &P, const double
 // flux comes first; NS then adds the central viscous flux, which for either
 // orientation of the face is C_FACE coef (fa + fb)/2 |n_D| for element a and
 // its negative for b (fixed operator only: the reference-value operator's
-// face fluxes read velocities from the momentum slots).
+// face fluxes read velocities from the momentum slots).  BDR (a mesh with
+// boundary faces): a slot whose neighbour entry is negative takes the
+// boundary condition's inviscid flux (boundary_node_terms) and, NS, its
+// viscous boundary flux, both for this element alone.
 template <int DIM, int N, bool NS, int D, bool BDR>
 __device__ __forceinline__ void face_terms_dir(const KParams &P, const double *c, double *acc, int64_t e,
                                                const int32_t *enb, int gl, bool valid, double coef, double &lam)
