@@ -112,9 +112,8 @@ int pdg_destroy(pdg_ctx *ctx);
  * 490-798).  A neighbour entry -1 - b (0 <= b < PDG_MAX_BOUNDARIES) marks a
  * boundary face with condition b; every condition the mesh uses must be set
  * before the first evaluation (else PDG_ERR_ARG).  Navier-Stokes boundary
- * faces: fixed operator only (pdg_create returns PDG_ERR_UNSUPPORTED with
- * compat = 1) and types 1, 2, 3, 10 and 11 (others: PDG_ERR_UNSUPPORTED at the
- * first evaluation); pdg_rhs_vjp differentiates every condition of an Euler
+ * faces: types 1, 2, 3, 10 and 11 (others: PDG_ERR_UNSUPPORTED at the first
+ * evaluation); pdg_rhs_vjp differentiates every condition of an Euler
  * mesh and none of a Navier-Stokes one.  `state` holds the condition's
  * data as listed beside each type (conserved, dim + 2 values, for the two
  * prescribed-state types) and may be NULL for types without data.  With
@@ -276,6 +275,7 @@ int64_t pdg_launch_count(const pdg_ctx *ctx);
 #define PDG_KERNEL_LIFT_FACE_BDR 25  /* Navier-Stokes meshes with boundary faces: face jumps, */
 #define PDG_KERNEL_LIFT_BDR  26      /* lifting kernel, */
 #define PDG_KERNEL_NS_FACES_BDR 27   /* volume kernel with element-side faces */
+#define PDG_KERNEL_BOUNDARY_NS 28    /* boundary faces of the separate-face path (Navier-Stokes) */
 int pdg_profile_enable(pdg_ctx *ctx, int on);
 int pdg_profile_read(pdg_ctx *ctx, int kind, double *total_ms, int64_t *launches);
 

@@ -268,7 +268,7 @@ int kernel_config(int dim, int N, int kind, int64_t ne, int device, LaunchCfg *c
     const int Np = N + 1, nfn = dim == 2 ? Np : Np * Np;
     if (ki.el_doubles == 0) {  // thread-per-face-node kernel
         const int64_t threads = kind == KIND_FILTER_BOUNDS ? 32 * ne
-                                : (kind == KIND_BOUNDARY || kind == KIND_ADJ_BOUNDARY) ? ne
+                                : (kind == KIND_BOUNDARY || kind == KIND_ADJ_BOUNDARY || kind == KIND_BOUNDARY_NS) ? ne
                                 : ((kind == KIND_LIFT_FACE || kind == KIND_LIFT_FACE_BDR) ? (int64_t)dim : 1) * ne * nfn;
         // 256-thread blocks; 128 when that gives fewer than four blocks per
         // SM, so that a small mesh still spreads evenly over the SMs
@@ -314,7 +314,7 @@ bool kind_used(int kind, int dim, bool parabolic, bool filter)
         return false;  // configured by the first pdg_rhs_vjp
     const bool ns_kind = kind == KIND_NS || kind == KIND_NS_FACES || kind == KIND_LIFT || kind == KIND_LIFT_FACE ||
                          (kind >= KIND_FACE_NS0 && kind <= KIND_FACE_NS2) || kind == KIND_LIFT_FACE_BDR ||
-                         kind == KIND_LIFT_BDR || kind == KIND_NS_FACES_BDR;
+                         kind == KIND_LIFT_BDR || kind == KIND_NS_FACES_BDR || kind == KIND_BOUNDARY_NS;
     if (ns_kind != parabolic) return false;
     if ((kind == KIND_FACE_E2 || kind == KIND_FACE_NS2) && dim < 3) return false;
     return true;
@@ -485,7 +485,7 @@ int evaluate(pdg_ctx *c, int stage, double dt, const double *un, const double *u
     if (c->p.parabolic) {
         if (c->p.filter && stage >= 0 && (r = launch(c, KIND_FILTER_BOUNDS, P, s))) return r;
         if (c->bc_used) {
-            // boundary faces of the fixed operator's element-side path
+            // Navier-Stokes boundary faces: the conditions with a viscous boundary flux
             for (int b = 0; b < PDG_MAX_BOUNDARIES; b++) {
                 const int t = (int)c->bc_host[b * BC_SLOT];
                 if ((c->bc_used >> b & 1u) && t != PDG_BC_SUPERSONIC_INFLOW && t != PDG_BC_SUPERSONIC_OUTFLOW &&
@@ -493,11 +493,18 @@ int evaluate(pdg_ctx *c, int stage, double dt, const double *un, const double *u
                     return fail(c, PDG_ERR_UNSUPPORTED,
                                 "boundary condition %d: type %d has no viscous boundary flux here", b, t);
             }
-            if (!element_faces) return fail(c, PDG_ERR_UNSUPPORTED, "Navier-Stokes boundary faces need element-side faces");
             if ((r = launch(c, KIND_LIFT_FACE_BDR, P, s))) return r;
-            P.vbuf = c->vbuf;
-            if ((r = launch(c, KIND_LIFT_BDR, P, s))) return r;
-            if ((r = launch(c, KIND_NS_FACES_BDR, P, s))) return r;
+            if (element_faces) {
+                P.vbuf = c->vbuf;
+                if ((r = launch(c, KIND_LIFT_BDR, P, s))) return r;
+                if ((r = launch(c, KIND_NS_FACES_BDR, P, s))) return r;
+            } else {  // separate face passes, then the boundary faces
+                if ((r = launch(c, KIND_NS, P, s))) return r;
+                if ((r = launch(c, KIND_LIFT_BDR, P, s))) return r;
+                for (int d = 0; d < c->dim; d++)
+                    if ((r = launch(c, KIND_FACE_NS0 + d, P, s))) return r;
+                if ((r = launch(c, KIND_BOUNDARY_NS, P, s))) return r;
+            }
         } else if (element_faces) {
             if ((r = launch(c, KIND_LIFT_FACE, P, s))) return r;
             P.vbuf = c->vbuf;
@@ -577,8 +584,6 @@ int pdg_create(const pdg_mesh *mesh, const pdg_params *params, pdg_ctx **out)
         if (nb >= c->ne || nb < -PDG_MAX_BOUNDARIES) { delete c; return PDG_ERR_ARG; }
         if (nb < 0) c->bc_used |= 1u << (-1 - nb);
     }
-    // Navier-Stokes boundary faces: fixed operator (its element-side faces) only
-    if (c->bc_used && params->parabolic && params->compat) { delete c; return PDG_ERR_UNSUPPORTED; }
     auto cleanup = [&](int code) {
         pdg_destroy(c);
         return code;

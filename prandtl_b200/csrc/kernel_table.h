@@ -32,7 +32,8 @@ enum KernelKind {
     KIND_LIFT_FACE_BDR = 25,    // lift_face_kernel<dim, N, true>: NS meshes with boundary faces
     KIND_LIFT_BDR = 26,         // lift_kernel<dim, N, true>
     KIND_NS_FACES_BDR = 27,     // rhs_kernel<dim, N, true, true, true>
-    KIND_COUNT = 28
+    KIND_BOUNDARY_NS = 28,      // boundary_kernel<dim, N, true>: NS boundary faces of the separate-face path
+    KIND_COUNT = 29
 };
 
 struct KernelInfo {

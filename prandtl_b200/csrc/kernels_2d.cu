@@ -17,6 +17,7 @@ template <int N> static bool info_n(int kind, KernelInfo *out)
     case KIND_EULER_FACES: out->fn = (const void *)&rhs_kernel<2, N, false, true>; out->el_doubles = S::EL_RHS; break;
     case KIND_NS_FACES: out->fn = (const void *)&rhs_kernel<2, N, true, true>; out->el_doubles = S::EL_RHS; break;
     case KIND_BOUNDARY: out->fn = (const void *)&boundary_kernel<2, N>; break;
+    case KIND_BOUNDARY_NS: out->fn = (const void *)&boundary_kernel<2, N, true>; break;
     case KIND_EULER_FACES_BDR:
         out->fn = (const void *)&rhs_kernel<2, N, false, true, true>;
         out->el_doubles = S::EL_RHS;

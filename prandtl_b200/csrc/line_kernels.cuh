@@ -1160,8 +1160,10 @@ __device__ __forceinline__ double face_node(const KParams &P, const double *c, i
 
 
 // Boundary face node fn of element a's +D (side 1) or -D (side 0) face:
-// read-modify-write of a's output node.
-template <int DIM, int N, int D>
+// read-modify-write of a's output node.  NS adds the viscous boundary flux
+// from a's own face column (outflow, no-slip walls; none for prescribed
+// states), as the element-side path does.
+template <int DIM, int N, int D, bool NS = false>
 __device__ __forceinline__ double boundary_node(const KParams &P, const double *c, int64_t a, int fn, int side, int b,
                                                 double coef)
 {
@@ -1177,7 +1179,29 @@ __device__ __forceinline__ double boundary_node(const KParams &P, const double *
     }
     const double lam = boundary_node_terms<DIM, N, D>(P, c, s, b, side ? 1.0 : -1.0, coef, C);
 #pragma unroll
-    for (int v = 0; v < NV; v++) P.out[v * nn + a * NDOF + n] = o[v] + C[v];
+    for (int v = 0; v < NV; v++) o[v] = o[v] + C[v];
+    if (NS) {
+        const double *bc = P.bc + b * BC_SLOT;
+        const int type = (int)bc[0];
+        if (type == BC_SUPERSONIC_OUTFLOW || type == BC_NOSLIP_ADIABATIC || type == BC_NOSLIP_ISOTHERMAL) {
+            const double nrm = side ? C_AREA(c)[D] : -C_AREA(c)[D];
+            const double *fo = P.fcol + (((D * 2 + side) * P.ne + a) * S::NFN + fn) * (NV - 1);
+            double fv[DIM + 1];
+#pragma unroll
+            for (int i = 0; i <= DIM; i++) fv[i] = __ldg(fo + i) * nrm;
+            if (type == BC_NOSLIP_ADIABATIC) {
+                double en = 0.0;
+#pragma unroll
+                for (int q = 0; q < DIM; q++) en += bc[1 + q] * fv[q];
+                fv[DIM] = en + 0.0;
+            }
+            const double sb = C_FACE(c) * coef;
+#pragma unroll
+            for (int i = 0; i <= DIM; i++) o[1 + i] += sb * fv[i];
+        }
+    }
+#pragma unroll
+    for (int v = 0; v < NV; v++) P.out[v * nn + a * NDOF + n] = o[v];
     return lam;
 }
 
@@ -1211,7 +1235,7 @@ __global__ void __launch_bounds__(256, 3) face_kernel(const KParams P)
 // two boundary faces is updated by one thread; threads of interior elements
 // return at once.  Launched after the face kernels, so its
 // read-modify-writes do not overlap theirs.
-template <int DIM, int N>
+template <int DIM, int N, bool NS = false>
 __global__ void __launch_bounds__(256) boundary_kernel(const KParams P)
 {
     using S = Shape<DIM, N>;
@@ -1229,9 +1253,9 @@ __global__ void __launch_bounds__(256) boundary_kernel(const KParams P)
             const int d = f >> 1, side = f & 1;
 #pragma unroll 1
             for (int fn = 0; fn < NFN; fn++) {
-                if (d == 0) lam = fmax(lam, boundary_node<DIM, N, 0>(P, c, a, fn, side, -1 - nb, coef));
-                else if (d == 1) lam = fmax(lam, boundary_node<DIM, N, 1>(P, c, a, fn, side, -1 - nb, coef));
-                else lam = fmax(lam, boundary_node<DIM, N, (DIM == 3 ? 2 : 0)>(P, c, a, fn, side, -1 - nb, coef));
+                if (d == 0) lam = fmax(lam, boundary_node<DIM, N, 0, NS>(P, c, a, fn, side, -1 - nb, coef));
+                else if (d == 1) lam = fmax(lam, boundary_node<DIM, N, 1, NS>(P, c, a, fn, side, -1 - nb, coef));
+                else lam = fmax(lam, boundary_node<DIM, N, (DIM == 3 ? 2 : 0), NS>(P, c, a, fn, side, -1 - nb, coef));
             }
         }
     }
@@ -1271,10 +1295,10 @@ __device__ __forceinline__ void lift_face_node(const KParams &P, const double *c
 // BR1 jump of a boundary face node (LiftingBR1::AssembleLiftingBdrFaceVector,
 // LiftingBR1.cpp:311-345, with ComputeBdrFaceLiftingFlux): the element is
 // element 1 and the normal points out of it; 0.5 (w(s2) - w1) for the
-// prescribed states (BdrFaceIntegrator.cpp:275-282, without the reference's
-// in-place division of w1, which the reference-value operator would need),
+// prescribed states (BdrFaceIntegrator.cpp:275-282),
 // 0 for the outflow, (w1_0, beta V, -beta) - w1 for the no-slip wall
-// (NoSlipAdiabWallBdrFaceIntegrator.cpp:74-95).  Fixed operator only.
+// (NoSlipAdiabWallBdrFaceIntegrator.cpp:74-95); the reference-value operator
+// keeps the reference's in-place division (below).
 template <int DIM, int N, int D>
 __device__ __noinline__ void lift_boundary_node(const KParams &P, const double *c, int64_t a, int fn, int side, int b,
                                                 double *dst)
@@ -1297,6 +1321,31 @@ __device__ __noinline__ void lift_boundary_node(const KParams &P, const double *
 #pragma unroll
         for (int q = 0; q < DIM; q++) f[1 + q] = bc[1 + q] * beta - w1[1 + q];
         f[NV - 1] = -beta - w1[NV - 1];
+    } else if (P.compat) {
+        // the reference reaches the outer state through Entropy2Conserv(w1)
+        // (BasicOperations.cpp:106-124), whose velocity view divides w1's
+        // momentum entries by beta in place before they are subtracted
+        const double beta = -w1[NV - 1], ib = 1.0 / beta;
+        double vv = 0.0;
+#pragma unroll
+        for (int q = 0; q < DIM; q++) {
+            w1[1 + q] *= ib;
+            vv += w1[1 + q] * w1[1 + q];
+        }
+        double s2[NV], w2[NV];
+        if (type == BC_SUPERSONIC_INFLOW || type == BC_SPECIFIED_STATE) {
+#pragma unroll
+            for (int v = 0; v < NV; v++) s2[v] = bc[1 + v];
+        } else {
+            const double sent = P.gamma - (w1[0] + 0.5 * beta * vv) * P.gm1;
+            s2[0] = pow(exp(-sent) / beta, P.gm1inv);
+#pragma unroll
+            for (int q = 0; q < DIM; q++) s2[1 + q] = s2[0] * w1[1 + q];
+            s2[NV - 1] = s2[0] * (1.0 / beta * P.gm1inv + 0.5 * vv);
+        }
+        entropy_vars<DIM>(s2, P.gamma, P.gm1, P.gm1inv, w2);
+#pragma unroll
+        for (int v = 0; v < NV; v++) f[v] = (w2[v] - w1[v]) * 0.5;
     } else if (type == BC_SUPERSONIC_INFLOW || type == BC_SPECIFIED_STATE) {
         double w2[NV];
         entropy_vars<DIM>(bc + 1, P.gamma, P.gm1, P.gm1inv, w2);

@@ -119,8 +119,9 @@ def test_boundary_errors(cuda_device):
     op.set_boundary(1, *bcs[1])
     op.Mult(dev(u, cuda_device), out)
     mesh.boundaries = bcs
+    op_ns = pb.DGSEMOperator(mesh, parabolic=1, mu=0.01)   # symmetry plane: no viscous flux
     with pytest.raises(pb.PdgError) as ei:
-        pb.DGSEMOperator(mesh, parabolic=1, mu=0.01)
+        op_ns.Mult(dev(u, cuda_device), out)
     assert ei.value.code == 5
     mesh3, _ = layout_case("3d_subsonic", 1)
     op3 = pb.DGSEMOperator(mesh3)
@@ -149,17 +150,20 @@ def test_gpu_vjp_with_boundaries_matches_autograd(name, order, blending, cuda_de
     assert op.check() == 0
 
 
+@pytest.mark.parametrize("compat", [0, 1])
 @pytest.mark.parametrize("order", [1, 2, 3])
 @pytest.mark.parametrize("name", ["ns_2d_channel", "ns_2d_cavity", "ns_2d_isothermal", "ns_3d_channel"])
-def test_gpu_ns_boundaries_match_oracle(name, order, cuda_device):
+def test_gpu_ns_boundaries_match_oracle(name, order, compat, cuda_device):
     """Navier-Stokes boundary faces (BR1 boundary lifting, viscous boundary
-    fluxes, no-slip wall) of the fixed operator against the oracle, whose
-    boundary code is pinned to the reference's (tests/test_boundaries.py)."""
+    fluxes, no-slip walls) of both operators against the oracle, whose
+    boundary code is pinned to the reference's (tests/test_boundaries.py);
+    the reference-value operator runs the separate face passes and the
+    boundary kernel, the fixed one its element-side faces."""
     import torch
     from test_boundaries import NS_KW, ns_layout_case
     mesh, u = ns_layout_case(name, order)
-    op = pb.DGSEMOperator(mesh, compat=0, **NS_KW)
-    orc = oracle.Oracle(mesh, compat=0, **NS_KW)
+    op = pb.DGSEMOperator(mesh, compat=compat, **NS_KW)
+    orc = oracle.Oracle(mesh, compat=compat, **NS_KW)
     ref = orc.rhs(u)
     x = dev(u, cuda_device)
     out = torch.empty_like(x)
@@ -187,9 +191,6 @@ def test_ns_boundary_errors(cuda_device):
     import torch
     from test_boundaries import NS_KW, ns_layout_case
     mesh, u = ns_layout_case("ns_2d_channel", 2)
-    with pytest.raises(pb.PdgError) as ei:          # reference-value operator: not built
-        pb.DGSEMOperator(mesh, compat=1, **NS_KW)
-    assert ei.value.code == 5
     op = pb.DGSEMOperator(mesh, compat=0, **NS_KW)
     x = dev(u, cuda_device)
     with pytest.raises(pb.PdgError) as ei:          # no adjoint of NS boundary faces
