@@ -25,6 +25,7 @@ import os
 import numpy as np
 
 from .mesh import CartesianMesh, periodic_box  # noqa: F401
+from .meshio import read_mesh  # noqa: F401
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "_lib", "libprandtl_b200.so")

@@ -70,6 +70,11 @@ class CartesianMesh:
     # the grid cells (x-fastest index into the n grid) that are elements, when
     # the domain is a subset of the box (a step, a channel with an obstacle)
     cells: np.ndarray | None = None
+    # meshes read from a file (prandtl_b200.meshio): boundary name -> condition
+    # index, and the element attributes
+    boundary_names: dict | None = None
+    attributes: np.ndarray | None = None
+    reoriented: np.ndarray | None = None   # elements whose corner order the reader relabelled
 
     @property
     def Np(self) -> int:

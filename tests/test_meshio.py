@@ -1,0 +1,348 @@
+"""Mesh files of the reference's formats (MFEM v1.0, Gmsh 2.2 ASCII) read into
+the neighbour table (prandtl_b200.meshio).
+
+Files written here from box meshes, with shuffled element and vertex
+numbers and rotated or mirrored corner orders, must read back as the same
+mesh; the reference's own mesh files are read when its source tree is
+present (they do not travel with the repository)."""
+import os
+
+import numpy as np
+import pytest
+
+import prandtl_b200 as pb
+from prandtl_b200 import meshio
+from prandtl_b200.mesh import box, periodic_box
+
+CORNERS = meshio._CORNER_BITS
+REF_CASES = os.path.join(os.environ.get("PRANDTL_REFERENCE", "/root/reference"), "TestCases")
+
+
+def grid_points(mesh):
+    """Vertex grid of a box mesh: index of grid point (i, j, k) and its
+    coordinates; element corners by _CORNER_BITS."""
+    n = [v + 1 for v in mesh.n]
+
+    def pid(idx):
+        out, stride = 0, 1
+        for d in range(mesh.dim):
+            out = out + idx[d] * stride
+            stride *= n[d]
+        return out
+    coords = np.empty((int(np.prod(n)), mesh.dim))
+    for flat in range(coords.shape[0]):
+        r, idx = flat, []
+        for d in range(mesh.dim):
+            idx.append(r % n[d])
+            r //= n[d]
+        coords[flat] = [mesh.lo[d] + idx[d] * mesh.h[d] for d in range(mesh.dim)]
+    return pid, coords
+
+
+def element_corners(mesh, pid):
+    cells = mesh.cells if mesh.cells is not None else np.arange(mesh.num_elements)
+    out = []
+    for c in cells:
+        r, idx = int(c), []
+        for d in range(mesh.dim):
+            idx.append(r % mesh.n[d])
+            r //= mesh.n[d]
+        out.append([pid([idx[d] + bits[d] for d in range(mesh.dim)]) for bits in CORNERS[mesh.dim]])
+    return np.array(out)
+
+
+def boundary_faces(mesh, corners):
+    """(attribute, corner vertex list) of every boundary face."""
+    faces = []
+    for e in range(mesh.num_elements):
+        for d in range(mesh.dim):
+            for side in (0, 1):
+                nb = mesh.nbr[e, 2 * d + side]
+                if nb < 0:
+                    sel = [k for k in range(2 ** mesh.dim) if CORNERS[mesh.dim][k][d] == side]
+                    faces.append((int(-nb), [int(corners[e, k]) for k in sel]))
+    return faces
+
+
+def rotate(corners, dim, rng):
+    """A rotated or mirrored listing of each element's corners."""
+    out = corners.copy()
+    for e in range(len(corners)):
+        if dim == 2:
+            cyc = [0, 1, 2, 3]
+            r = rng.integers(4)
+            seq = cyc[r:] + cyc[:r]
+            if rng.integers(2):
+                seq = seq[::-1]
+            out[e] = corners[e, seq]
+        else:                       # quarter turns about z keep bottom then top
+            r = rng.integers(4)
+            bot = [0, 1, 2, 3][r:] + [0, 1, 2, 3][:r]
+            out[e] = corners[e, bot + [k + 4 for k in bot]]
+    return out
+
+
+def write_gmsh(path, mesh, rng, names=None):
+    pid, coords = grid_points(mesh)
+    corners = element_corners(mesh, pid)
+    bfaces = boundary_faces(mesh, corners)
+    perm = rng.permutation(mesh.num_elements)             # file element i = mesh element perm[i]
+    node_ids = rng.permutation(np.arange(7, 7 + 3 * len(coords)))[:len(coords)]   # sparse 1-based ids
+    listed = rotate(corners[perm], mesh.dim, rng)
+    dom, bnd = (3, 1) if mesh.dim == 2 else (5, 3)
+    lines = ["$MeshFormat", "2.2 0 8", "$EndMeshFormat"]
+    if names:
+        lines += ["$PhysicalNames", str(len(names))]
+        lines += [f'{mesh.dim - 1} {a} "{nm}"' for nm, a in names.items()]
+        lines += ["$EndPhysicalNames"]
+    lines += ["$Nodes", str(len(coords))]
+    for k in rng.permutation(len(coords)):
+        xyz = list(coords[k]) + [0.0] * (3 - mesh.dim)
+        lines.append(f"{node_ids[k]} " + " ".join(f"{v:.17g}" for v in xyz))
+    lines += ["$EndNodes", "$Elements", str(1 + len(bfaces) + len(listed))]
+    eid = 1
+    lines.append(f"{eid} 15 2 0 1 {node_ids[0]}")     # a point entity, ignored
+    for a, fv in bfaces:
+        eid += 1
+        lines.append(f"{eid} {bnd} 2 {a} {a} " + " ".join(str(node_ids[v]) for v in fv))
+    for c in listed:
+        eid += 1
+        lines.append(f"{eid} {dom} 2 99 1 " + " ".join(str(node_ids[v]) for v in c))
+    lines.append("$EndElements")
+    with open(path, "w") as f:
+        f.write("\n".join(lines) + "\n")
+    return perm
+
+
+def same_mesh(read, orig, perm):
+    """read element i is orig element perm[i]: same cells, neighbours and
+    boundary entries."""
+    inv = np.empty_like(perm)
+    inv[perm] = np.arange(len(perm))
+    assert read.dim == orig.dim and tuple(read.n) == tuple(orig.n)
+    np.testing.assert_allclose(read.h, orig.h, rtol=1e-13)
+    np.testing.assert_allclose(read.lo, orig.lo, atol=1e-13)
+    oc = orig.cells if orig.cells is not None else np.arange(orig.num_elements)
+    assert np.array_equal(read.cells, oc[perm])
+    on = orig.nbr[perm].astype(np.int64)
+    expect = np.where(on >= 0, inv[np.maximum(on, 0)], on)
+    assert np.array_equal(read.nbr, expect)
+    np.testing.assert_allclose(read.node_coords(), orig.node_coords(perm), atol=1e-12)
+
+
+@pytest.mark.parametrize("dim", [2, 3])
+def test_gmsh_round_trip(tmp_path, dim):
+    rng = np.random.default_rng(dim)
+    n = (6, 4) if dim == 2 else (4, 3, 3)
+    keep = np.ones(n, dtype=bool)
+    keep[:2, :2] = False                                   # a step
+    bdr = [(0, 1), (2, 3), (2, 3)][:dim]                   # a Gmsh file has no periodic sides here
+    orig = box(dim, 2, n, 0.0, [3.0, 2.0, 1.5][:dim], bdr=bdr, keep=keep, cut=4)
+    names = {"inflow": 1, "outflow": 2, "bottom": 3, "top": 4, "step": 5}
+    path = str(tmp_path / "m.msh")
+    perm = write_gmsh(path, orig, rng, names)
+    m = meshio.read_mesh(path, 2)
+    same_mesh(m, orig, perm)
+    assert m.boundary_names == {k: v - 1 for k, v in names.items()}
+    assert len(m.reoriented) > 0 and np.all(m.attributes == 99)
+
+
+def write_mfem_periodic(path, mesh):
+    """A periodic MFEM v1.0 mesh: topological vertices identified across the
+    periodic sides, coordinates in a discontinuous L2_T1 P1 nodes section."""
+    n = mesh.n
+    def vid(idx):
+        out, stride = 0, 1
+        for d in range(mesh.dim):
+            out += (idx[d] % n[d]) * stride
+            stride *= n[d]
+        return out
+    rows, nodes = [], []
+    for e in range(mesh.num_elements):
+        r, idx = e, []
+        for d in range(mesh.dim):
+            idx.append(r % n[d])
+            r //= n[d]
+        cs = [vid([idx[d] + b[d] for d in range(mesh.dim)]) for b in CORNERS[mesh.dim]]
+        rows.append(f"1 {3 if mesh.dim == 2 else 5} " + " ".join(map(str, cs)))
+        for lex in range(2 ** mesh.dim):                   # corners in lexicographic order
+            nodes.append(" ".join(f"{mesh.lo[d] + (idx[d] + ((lex >> d) & 1)) * mesh.h[d]:.17g}"
+                                  for d in range(mesh.dim)))
+    text = ["MFEM mesh v1.0", "", "# a comment", "dimension", str(mesh.dim), "", "elements", str(len(rows))]
+    text += rows + ["", "boundary", "0", "", "vertices", str(int(np.prod(n))), "", "nodes",
+                    "FiniteElementSpace", f"FiniteElementCollection: L2_T1_{mesh.dim}D_P1",
+                    f"VDim: {mesh.dim}", "Ordering: 1", ""] + nodes
+    with open(path, "w") as f:
+        f.write("\n".join(text) + "\n")
+
+
+@pytest.mark.parametrize("dim,n", [(2, (3, 4)), (3, (3, 4, 3))])
+def test_mfem_periodic(tmp_path, dim, n):
+    orig = periodic_box(dim, 3, n, -1.0, 1.0)
+    path = str(tmp_path / "p.mesh")
+    write_mfem_periodic(path, orig)
+    m = meshio.read_mesh(path, 3)
+    same_mesh(m, orig, np.arange(orig.num_elements))
+    assert len(m.reoriented) == 0 and m.boundary_names == {}
+
+
+@pytest.mark.parametrize("dim", [2, 3])
+def test_refinement(dim):
+    """Two refinements of a 3 x 2 (x 2) box with boundaries equal the 12 x 8
+    (x 8) box under the children's numbering."""
+    n = (3, 2, 2)[:dim]
+    bdr = [(0, 1), None, (2, 3)][:dim]
+    coarse = box(dim, 1, n, 0.0, 1.0, bdr=bdr)
+    coarse.cells = np.arange(coarse.num_elements)
+    fine = box(dim, 1, tuple(4 * v for v in n), 0.0, 1.0, bdr=bdr)
+    m = meshio.refine_mesh(meshio.refine_mesh(coarse))
+    perm = np.asarray(m.cells)                             # refined element i = fine element cells[i]
+    assert sorted(perm.tolist()) == list(range(fine.num_elements))
+    same_mesh(m, fine, perm)
+
+
+def test_rejections(tmp_path):
+    rng = np.random.default_rng(1)
+    orig = box(2, 1, (3, 2), 0.0, 1.0, bdr=[(0, 1), (2, 3)])
+    path = str(tmp_path / "m.msh")
+    write_gmsh(path, orig, rng)
+    text = open(path).read()
+    lines = text.splitlines()
+    i = lines.index("$Nodes") + 2
+    r = lines[i].split()
+    lines[i] = " ".join([r[0], str(float(r[1]) + 0.01)] + r[2:])      # skew one vertex
+    open(path, "w").write("\n".join(lines))
+    with pytest.raises(ValueError, match="box|sizes|grid"):
+        meshio.read_mesh(path, 1)
+    open(path, "w").write(text.replace("$MeshFormat\n2.2 0 8", "$MeshFormat\n2.2 1 8"))
+    with pytest.raises(ValueError, match="ASCII"):
+        meshio.read_mesh(path, 1)
+    open(path, "w").write(text.replace(" 15 2 0 1 ", " 9 2 0 1 "))   # a second-order triangle
+    with pytest.raises(ValueError, match="element type 9"):
+        meshio.read_mesh(path, 1)
+    # a boundary face with no boundary element
+    keep = [ln for ln in text.splitlines() if not (len(ln.split()) == 7 and ln.split()[1] == "1")]
+    open(path, "w").write("\n".join(keep))
+    with pytest.raises(ValueError, match="without a boundary element"):
+        meshio.read_mesh(path, 1)
+    pmesh = periodic_box(2, 1, (3, 3), 0.0, 1.0)
+    p2 = str(tmp_path / "p.mesh")
+    write_mfem_periodic(p2, pmesh)
+    ptext = open(p2).read()
+    open(p2, "w").write(ptext.replace("L2_T1_2D_P1", "H1_2D_P2"))
+    with pytest.raises(ValueError, match="curved"):
+        meshio.read_mesh(p2, 1)
+
+
+def ref_file(rel):
+    path = os.path.join(REF_CASES, rel)
+    if not os.path.exists(path):
+        pytest.skip("the reference's test cases are not present")
+    return path
+
+
+def test_reference_periodic_meshes():
+    """IsentropicVortex.mesh with ser_ref_levels = 3 (its configuration) is
+    the periodic 24 x 24 box on [-1, 1]^2."""
+    for rel in ("Euler/2D/IsentropicVortex/IsentropicVortex.mesh",
+                "Euler/2D/KelvinHelmholtzInstability/KelvinHelmholtzInstability.mesh"):
+        m = meshio.read_mesh(ref_file(rel), 3, refine=3)
+        fine = periodic_box(2, 3, 24, -1.0, 1.0)
+        same_mesh(m, fine, np.asarray(m.cells))
+
+
+def test_reference_gmsh_meshes():
+    m = meshio.read_mesh(ref_file("NavierStokes/2D/LidDrivenCavity/LidDrivenCavity.msh"), 3)
+    assert tuple(m.n) == (16, 16) and m.boundary_names == {"bottom": 0, "right": 1, "lid": 2, "left": 3}
+    full = box(2, 3, 16, 0.0, 2.0, bdr=[(3, 1), (0, 2)])
+    same_mesh(m, full, np.asarray(m.cells))
+    m = meshio.read_mesh(ref_file("Euler/2D/DoubleMachReflection/DoubleMachReflection.msh"), 3)
+    assert tuple(m.n) == (384, 96)
+    nb = m.boundary_names
+    x0 = m.node_coords(np.arange(m.num_elements))[0].reshape(m.num_elements, -1).min(axis=1)
+    bottom = m.nbr[:, 2]
+    on = bottom < 0
+    assert np.all(bottom[on & (x0 < 1 / 6 - 1e-9)] == -1 - nb["bottom1"])
+    assert np.all(bottom[on & (x0 > 1 / 6 - 1e-9)] == -1 - nb["bottom2"])
+    m = meshio.read_mesh(ref_file("Euler/2D/BackwardFacingStep/BackwardFacingStep.msh"), 2)
+    assert m.num_elements == 35000 and len(m.reoriented) > 0
+    for rel, why in (("Euler/2D/ForwardFacingStep/ForwardFacingStep.msh", "sizes"),
+                     ("Euler/2D/Ramp/Ramp15deg_v2.msh", "axis-aligned"),
+                     ("Euler/2D/Nagashima_Ramjet/TR0/Nagashima_TR0_11kQuad_v2.msh", "box")):
+        with pytest.raises(ValueError, match=why):
+            meshio.read_mesh(ref_file(rel), 2)
+
+
+def test_read_mesh_runs_in_the_oracle(tmp_path):
+    """A shuffled, rotated Gmsh copy of a channel with a step gives the same
+    right-hand side as the box it came from (permuted), in the oracle."""
+    import oracle
+    from test_boundaries import uniform
+    rng = np.random.default_rng(5)
+    keep = np.ones((6, 4), dtype=bool)
+    keep[:2, :1] = False
+    orig = box(2, 2, (6, 4), 0.0, [3.0, 2.0], bdr=[(0, 1), (2, 3)], keep=keep, cut=2)
+    path = str(tmp_path / "c.msh")
+    perm = write_gmsh(path, orig, rng, {"in": 1, "out": 2, "wall": 3, "top": 4})
+    m = meshio.read_mesh(path, 2)
+    fs = [1.0, 2.0, 0.0, 1.0 / 0.4 + 0.5 * 4.0]
+    conds = {"in": (pb.BC_SUPERSONIC_INFLOW, fs), "out": (pb.BC_SUPERSONIC_OUTFLOW, None),
+             "wall": (pb.BC_SLIP_WALL, None), "top": (pb.BC_SLIP_WALL, None)}
+    m.boundaries = {m.boundary_names[k]: v for k, v in conds.items()}
+    orig.boundaries = {i: conds[k] for k, i in {"in": 0, "out": 1, "wall": 2, "top": 3}.items()}
+    u0 = uniform(orig, vel=(2.0, 0.0))
+    x = orig.node_coords()
+    u0 = u0.reshape(4, -1)
+    u0[0] *= 1.0 + 0.05 * np.sin(2.0 * x[0]) * np.cos(3.0 * x[1])
+    u0 = u0.reshape(-1)
+    nd = orig.ndof
+    um = u0.reshape(4, orig.num_elements, nd)[:, perm].reshape(-1)
+    reo = np.zeros(m.num_elements, dtype=bool)
+    reo[m.reoriented] = True
+    assert reo.any()
+    # reoriented elements keep the box frame here, so node orders agree
+    r0 = oracle.Oracle(orig, compat=0).rhs(u0).reshape(4, orig.num_elements, nd)[:, perm]
+    r1 = oracle.Oracle(m, compat=0).rhs(um).reshape(4, m.num_elements, nd)
+    assert np.max(np.abs(r1 - r0)) <= 1e-12 * np.max(np.abs(r0))
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("compat", [0, 1])
+@pytest.mark.parametrize("parabolic", [0, 1])
+def test_gpu_read_mesh_matches_oracle(tmp_path, compat, parabolic, cuda_device):
+    """The operator on a mesh read from a shuffled, rotated Gmsh file
+    (elements in file order, a step cut out, named boundaries) against the
+    oracle on the same mesh, Euler with a slip wall and Navier-Stokes with
+    no-slip walls, for both operators and graph-replayed steps."""
+    import torch
+    import oracle
+    from helpers import rel_maxnorm, rough
+    from test_boundaries import uniform
+    rng = np.random.default_rng(11 + parabolic)
+    keep = np.ones((8, 5), dtype=bool)
+    keep[:3, :2] = False
+    orig = box(2, 3, (8, 5), 0.0, [4.0, 2.5], bdr=[(0, 1), (2, 3)], keep=keep, cut=2)
+    path = str(tmp_path / "g.msh")
+    write_gmsh(path, orig, rng, {"in": 1, "out": 2, "wall": 3, "top": 4})
+    m = meshio.read_mesh(path, 3)
+    fs = [1.0, 2.0, 0.0, 1.0 / 0.4 + 0.5 * 4.0]
+    wall = (pb.BC_NOSLIP_ADIABATIC, [0.0, 0.0]) if parabolic else (pb.BC_SLIP_WALL, None)
+    conds = {"in": (pb.BC_SUPERSONIC_INFLOW, fs), "out": (pb.BC_SUPERSONIC_OUTFLOW, None),
+             "wall": wall, "top": wall}
+    m.boundaries = {m.boundary_names[k]: v for k, v in conds.items()}
+    kw = dict(compat=compat, parabolic=parabolic, mu=0.02 if parabolic else 0.0, Pr=0.71)
+    u = rough(uniform(m, vel=(2.0, 0.0)), m, 4, 0.02, 0.002)
+    orc = oracle.Oracle(m, **kw)
+    ref = orc.rhs(u)
+    op = pb.DGSEMOperator(m, **kw)
+    x = torch.from_numpy(u).to(cuda_device)
+    out = torch.empty_like(x)
+    op.Mult(x, out)
+    torch.cuda.synchronize()
+    assert rel_maxnorm(out.cpu().numpy(), ref) < 1e-12
+    dt = 0.2 * min(m.h) / (orc.max_char_speed() * 16)
+    y = orc.rk3_step(u, dt)
+    op.rk3_step(x, dt, nsteps=1, graph=True)
+    torch.cuda.synchronize()
+    assert rel_maxnorm(x.cpu().numpy(), y) < 1e-11
+    assert op.check() == 0
