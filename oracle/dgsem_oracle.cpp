@@ -895,7 +895,10 @@ static void rotate_state(int dim, double *state, const double *n)
 
 // Normal flux of boundary condition b for interior state s1 and outward
 // normal nor (ComputeBdrFaceInviscidFlux); returns the reported wave speed.
-static double bdr_flux(const Ctx &c, int b, const double *s1, const double *nor, double *flux)
+// outer (optional): receives the outer state the face flux is given (the
+// conditions other than the walls), for the boundary lifting flux.
+static double bdr_flux(const Ctx &c, int b, const double *s1, const double *nor, double *flux,
+                       double *outer = nullptr)
 {
     const int dim = c.dim, nv = c.nv;
     const double gamma = c.p.gamma, gammaM1 = gamma - 1.0, gammaM1Inverse = 1.0 / gammaM1;
@@ -942,6 +945,7 @@ static double bdr_flux(const Ctx &c, int b, const double *s1, const double *nor,
             for (int d = 0; d < dim; d++) s1c[1 + d] = vel[d];
         for (int v = 0; v < nv; v++) s2[v] = s1c[v];
         s2[nv - 1] = prm[0] * gammaM1Inverse + 0.5 * s1[0] * vv;
+        if (outer) for (int v = 0; v < nv; v++) outer[v] = s2[v];
         return face_flux(dim, gamma, c.p.compat, c.p.face_dissipation, s1c, s2, nor, flux);
     }
     if (type == 7) {
@@ -958,6 +962,7 @@ static double bdr_flux(const Ctx &c, int b, const double *s1, const double *nor,
         dke *= 0.5 / s1[0];
         dke += 0.5 * uu * r;
         s2[nv - 1] = s1[nv - 1] + dke;
+        if (outer) for (int v = 0; v < nv; v++) outer[v] = s2[v];
         return face_flux(dim, gamma, c.p.compat, c.p.face_dissipation, s1, s2, nor, flux);
     }
     if (type == 8) {
@@ -976,6 +981,7 @@ static double bdr_flux(const Ctx &c, int b, const double *s1, const double *nor,
         s2[0] = gamma * gammaM1Inverse * p / (cp * T0 - 0.5 * V_sq);
         for (int d = 0; d < dim; d++) s2[1 + d] = s2[0] * std::sqrt(V_sq) * prm[3 + d];
         s2[nv - 1] = p * gammaM1Inverse + 0.5 * s2[0] * V_sq;
+        if (outer) for (int v = 0; v < nv; v++) outer[v] = s2[v];
         return face_flux(dim, gamma, c.p.compat, c.p.face_dissipation, s1c, s2, nor, flux);
     }
     if (type == 9) {
@@ -1016,6 +1022,7 @@ static double bdr_flux(const Ctx &c, int b, const double *s1, const double *nor,
         e2 *= (0.5 / s2[0]);
         e2 += p_b * gammaM1Inverse;
         s2[nv - 1] = e2;
+        if (outer) for (int v = 0; v < nv; v++) outer[v] = s2[v];
         return face_flux(dim, gamma, c.p.compat, c.p.face_dissipation, s1c, s2, nor, flux);
     }
     if (type == 1 || type == 3) {
@@ -1028,6 +1035,7 @@ static double bdr_flux(const Ctx &c, int b, const double *s1, const double *nor,
         for (int d = 0; d < dim; d++) mn += s2[1 + d] * un[d];
         for (int d = 0; d < dim; d++) s2[1 + d] += -2.0 * mn * un[d];
     }  // type 2, SupersonicOutflow (:10-13): the interior state
+    if (outer) for (int v = 0; v < nv; v++) outer[v] = s2[v];
     return face_flux(dim, gamma, c.p.compat, c.p.face_dissipation, s1, s2, nor, flux);
 }
 
@@ -1081,7 +1089,8 @@ static double bdr_face_vector(const Ctx &c, const double *u, int64_t e, int d, i
 // Entropy2Conserv(w1) (BasicOperations.cpp:106-124), whose velocity view
 // divides w1's momentum entries by beta in place before they are
 // subtracted; compat keeps that.  No-slip: (w1_0, beta V, -beta) - w1.
-static void bdr_lifting_flux(const Ctx &c, int b, const double *s1, const double *w1_in, double *f)
+static void bdr_lifting_flux(const Ctx &c, int b, const double *s1, const double *w1_in, const double *nor,
+                             double *f)
 {
     const int nv = c.nv, dim = c.dim;
     const double gamma = c.p.gamma, gm1 = gamma - 1.0, gm1inv = 1.0 / gm1;
@@ -1115,6 +1124,15 @@ static void bdr_lifting_flux(const Ctx &c, int b, const double *s1, const double
     }
     if (type == 1 || type == 3)
         for (int v = 0; v < nv; v++) s2[v] = c.bc[b][1 + v];
+    if (type == 6 || type == 7 || type == 9) {
+        // ComputeOuterInviscidState of the subsonic outflow, the subsonic
+        // inflow (rho, V) and the Riemann invariants, from s2 (the interior
+        // state, or in compat what Entropy2Conserv made of w1), with their
+        // own in-place divisions in compat
+        double so[5], fl[5];
+        bdr_flux(c, b, s2, nor, fl, so);
+        for (int v = 0; v < nv; v++) s2[v] = so[v];
+    }
     double w2[5];
     conserv2entropy(dim, gamma, s2, w2);
     for (int v = 0; v < nv; v++) {
@@ -1177,14 +1195,15 @@ static void lifting(Ctx &c, const double *u)
                     // LiftingBR1.cpp:311-345): the element is element 1, the
                     // normal points out of it
                     const double ndb = side ? c.area[d] : -c.area[d];
-                    double s1[5], w1[5], f[5];
+                    double s1[5], w1[5], f[5], norb[3] = {0.0, 0.0, 0.0};
+                    norb[d] = ndb;
                     for (int t = 0; t < nfn; t++) {
                         const int n = face_node(c, d, side, t);
                         for (int v = 0; v < nv; v++) {
                             s1[v] = u[idx(c, v, e, n)];
                             w1[v] = W[idx(c, v, e, n)];
                         }
-                        bdr_lifting_flux(c, (int)(-1 - nb), s1, w1, f);
+                        bdr_lifting_flux(c, (int)(-1 - nb), s1, w1, norb, f);
                         for (int v = 0; v < nv; v++) {
                             double fval = f[v];
                             fval *= ndb;

@@ -1295,8 +1295,9 @@ __device__ __forceinline__ void lift_face_node(const KParams &P, const double *c
 // BR1 jump of a boundary face node (LiftingBR1::AssembleLiftingBdrFaceVector,
 // LiftingBR1.cpp:311-345, with ComputeBdrFaceLiftingFlux): the element is
 // element 1 and the normal points out of it; 0.5 (w(s2) - w1) for the
-// prescribed states (BdrFaceIntegrator.cpp:275-282),
-// 0 for the outflow, (w1_0, beta V, -beta) - w1 for the no-slip wall
+// prescribed states and the outer states of the subsonic conditions and the
+// Riemann invariants (BdrFaceIntegrator.cpp:275-282), 0 for the outflow,
+// (w1_0, beta V, -beta) - w1 for the no-slip wall
 // (NoSlipAdiabWallBdrFaceIntegrator.cpp:74-95); the reference-value operator
 // keeps the reference's in-place division (below).
 template <int DIM, int N, int D>
@@ -1342,6 +1343,13 @@ __device__ __noinline__ void lift_boundary_node(const KParams &P, const double *
 #pragma unroll
             for (int q = 0; q < DIM; q++) s2[1 + q] = s2[0] * w1[1 + q];
             s2[NV - 1] = s2[0] * (1.0 / beta * P.gm1inv + 0.5 * vv);
+            if (type == BC_SUBSONIC_OUTFLOW_P || type == BC_SUBSONIC_INFLOW_RV) {
+                // ComputeOuterInviscidState of that state (BdrFaceIntegrator.cpp:278)
+                double so[NV];
+                subsonic_outer_state<DIM, D>(P, type, bc + 1, side ? 1.0 : -1.0, s2, so);
+#pragma unroll
+                for (int v = 0; v < NV; v++) s2[v] = so[v];
+            }
         }
         entropy_vars<DIM>(s2, P.gamma, P.gm1, P.gm1inv, w2);
 #pragma unroll
@@ -1349,6 +1357,13 @@ __device__ __noinline__ void lift_boundary_node(const KParams &P, const double *
     } else if (type == BC_SUPERSONIC_INFLOW || type == BC_SPECIFIED_STATE) {
         double w2[NV];
         entropy_vars<DIM>(bc + 1, P.gamma, P.gm1, P.gm1inv, w2);
+#pragma unroll
+        for (int v = 0; v < NV; v++) f[v] = (w2[v] - w1[v]) * 0.5;
+    } else if (type == BC_SUBSONIC_OUTFLOW_P || type == BC_SUBSONIC_INFLOW_RV || type == BC_RIEMANN_INVARIANT) {
+        // the outer state of the inviscid flux (BdrFaceIntegrator.cpp:275-282)
+        double so[NV], w2[NV];
+        subsonic_outer_state<DIM, D>(P, type, bc + 1, side ? 1.0 : -1.0, s, so);
+        entropy_vars<DIM>(so, P.gamma, P.gm1, P.gm1inv, w2);
 #pragma unroll
         for (int v = 0; v < NV; v++) f[v] = (w2[v] - w1[v]) * 0.5;
     } else {

@@ -152,7 +152,8 @@ def test_gpu_vjp_with_boundaries_matches_autograd(name, order, blending, cuda_de
 
 @pytest.mark.parametrize("compat", [0, 1])
 @pytest.mark.parametrize("order", [1, 2, 3])
-@pytest.mark.parametrize("name", ["ns_2d_channel", "ns_2d_cavity", "ns_2d_isothermal", "ns_3d_channel"])
+@pytest.mark.parametrize("name", ["ns_2d_channel", "ns_2d_cavity", "ns_2d_isothermal", "ns_3d_channel",
+                                  "ns_2d_subsonic", "ns_3d_subsonic", "ns_2d_riemann"])
 def test_gpu_ns_boundaries_match_oracle(name, order, compat, cuda_device):
     """Navier-Stokes boundary faces (BR1 boundary lifting, viscous boundary
     fluxes, no-slip walls) of both operators against the oracle, whose
@@ -161,6 +162,8 @@ def test_gpu_ns_boundaries_match_oracle(name, order, compat, cuda_device):
     boundary kernel, the fixed one its element-side faces."""
     import torch
     from test_boundaries import NS_KW, ns_layout_case
+    if compat and name == "ns_2d_riemann":
+        pytest.skip("Riemann invariants with Navier-Stokes: fixed operator only")
     mesh, u = ns_layout_case(name, order)
     op = pb.DGSEMOperator(mesh, compat=compat, **NS_KW)
     orc = oracle.Oracle(mesh, compat=compat, **NS_KW)
@@ -199,6 +202,15 @@ def test_ns_boundary_errors(cuda_device):
     op.set_boundary(2, pb.BC_SLIP_WALL)             # no viscous flux in the reference
     with pytest.raises(pb.PdgError) as ei:
         op.Mult(x, torch.empty_like(x))
+    assert ei.value.code == 5
+    op.set_boundary(2, pb.BC_SUBSONIC_INFLOW_PTTT, [3.5, 3.0, 2.0, 10.0, 0.0])
+    with pytest.raises(pb.PdgError) as ei:          # its viscous flux is not built
+        op.Mult(x, torch.empty_like(x))
+    assert ei.value.code == 5
+    mr, ur = ns_layout_case("ns_2d_riemann", 2)
+    opr = pb.DGSEMOperator(mr, compat=1, **NS_KW)
+    with pytest.raises(pb.PdgError) as ei:          # reference-value Riemann invariants
+        opr.Mult(dev(ur, cuda_device), torch.empty(ur.size, dtype=torch.float64, device=cuda_device))
     assert ei.value.code == 5
 
 
