@@ -75,6 +75,7 @@ class CartesianMesh:
     boundary_names: dict | None = None
     attributes: np.ndarray | None = None
     reoriented: np.ndarray | None = None   # elements whose corner order the reader relabelled
+    frames: np.ndarray | None = None       # (ne, dim) file frame of each element, +-(axis + 1)
 
     @property
     def Np(self) -> int:

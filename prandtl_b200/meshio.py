@@ -27,7 +27,9 @@ axis-aligned box of the same size.  An element whose corners the file lists
 in a rotated or mirrored order (Gmsh does this in the step meshes) is
 relabelled so that its first corner is its lowest one and its second lies
 along +x (fourth along +y, fifth along +z); its DG nodes are then numbered in
-that frame, not the reference's, and ``mesh.reoriented`` lists it.  Curved,
+that frame, not the reference's, ``mesh.reoriented`` lists it and
+``to_reference_order`` / ``from_reference_order`` move fields between the two
+node orders.  Curved,
 skewed or graded meshes (the ramp, the ramjet) raise ``ValueError``.  Elements keep the
 file's order; faces are paired by their corner vertices, so periodic
 identifications of an MFEM mesh carry over (a periodic direction needs three
@@ -203,9 +205,10 @@ def _canonical_corners(dim, verts, coords):
     position of _CORNER_BITS[k] (first corner lowest, second along +x, ...).
     Gmsh writes some elements of a structured mesh with a rotated or mirrored
     corner order; the kernels need every element's axes along +x, +y (+z).
-    Returns the relabelled arrays and the indices of the elements whose
-    corners moved (their DG nodes are numbered in the relabelled frame, not
-    in the file's)."""
+    Returns the relabelled arrays, the indices of the elements whose corners
+    moved (their DG nodes are numbered in the relabelled frame, not in the
+    file's) and each element's file frame: frames[e, a] = +-(d + 1) when the
+    file's local axis a (corner 0 -> 1, 0 -> 3, 0 -> 4) runs along +-axis d."""
     ne, nc = verts.shape
     centre = coords.mean(axis=1, keepdims=True)
     hb = (coords > centre).astype(np.int64)                           # (ne, nc, dim) corner bits
@@ -222,8 +225,15 @@ def _canonical_corners(dim, verts, coords):
         raise ValueError(f"element {bad} is not a box (degenerate or non-convex corners)")
     pos = inv[:, want]
     moved = np.nonzero(np.any(pos != np.arange(nc), axis=1))[0]
+    cbits = np.array(_CORNER_BITS[dim], dtype=np.int64)
+    kpos = np.argsort(pos, axis=1)                   # file corner f sits at box position kpos[e, f]
+    frames = np.zeros((ne, dim), dtype=np.int8)
+    for a, f in enumerate((1, 3, 4)[:dim]):
+        step = cbits[kpos[:, f]] - cbits[kpos[:, 0]]  # (ne, dim): +-e_d
+        d = np.argmax(np.abs(step), axis=1)
+        frames[:, a] = (d + 1) * step[np.arange(ne), d]
     return (np.take_along_axis(verts, pos, axis=1),
-            np.take_along_axis(coords, pos[:, :, None], axis=1), moved)
+            np.take_along_axis(coords, pos[:, :, None], axis=1), moved, frames)
 
 
 def build_mesh(dim, order, verts, coords, bdr, names, attrs=None, tol=1e-8) -> CartesianMesh:
@@ -236,7 +246,7 @@ def build_mesh(dim, order, verts, coords, bdr, names, attrs=None, tol=1e-8) -> C
     if nc != 2 ** dim:
         raise ValueError(f"elements with {nc} corners in {dim}D")
     bits = np.array(_CORNER_BITS[dim], dtype=np.float64)              # (nc, dim)
-    verts, coords, reoriented = _canonical_corners(dim, verts, coords)
+    verts, coords, reoriented, frames = _canonical_corners(dim, verts, coords)
     origin = coords[:, 0, :]
     # extents: corner 1 lies along +x, corner 3 along +y, corner 4 along +z
     ext = np.stack([coords[:, (1, 3, 4)[d], d] - origin[:, d] for d in range(dim)], axis=1)
@@ -295,7 +305,8 @@ def build_mesh(dim, order, verts, coords, bdr, names, attrs=None, tol=1e-8) -> C
     return CartesianMesh(dim, int(order), n, tuple(float(v) for v in lo), tuple(float(v) for v in hi),
                          nbr.astype(np.int32), spacing=tuple(float(v) for v in h), boundaries={}, cells=cells,
                          boundary_names={k: int(v) - 1 for k, v in names.items() if int(v) in used},
-                         attributes=None if attrs is None else np.asarray(attrs), reoriented=reoriented)
+                         attributes=None if attrs is None else np.asarray(attrs), reoriented=reoriented,
+                         frames=frames)
 
 
 def refine_mesh(mesh: CartesianMesh) -> CartesianMesh:
@@ -331,7 +342,48 @@ def refine_mesh(mesh: CartesianMesh) -> CartesianMesh:
                     new[child, 2 * d + side] = np.where(nb >= 0, nb * K + sib, nb)
         new_cells[child] = cell
     h = tuple(v / 2 for v in mesh.h)
+    # no file frames: the children are numbered here, not by the reference
     return CartesianMesh(dim, mesh.order, n2, mesh.lo, mesh.hi, new.astype(np.int32), spacing=h,
                          boundaries=dict(mesh.boundaries or {}), cells=new_cells,
                          boundary_names=dict(mesh.boundary_names or {}),
                          attributes=None if mesh.attributes is None else np.repeat(mesh.attributes, K))
+
+
+def node_permutation(mesh: CartesianMesh) -> np.ndarray:
+    """perm[e, i]: this mesh's node of element e at the reference's node i.
+
+    The reference numbers an element's DG nodes lexicographically in the
+    element's own frame (its corner 0 -> 1 axis fastest); an element the
+    reader relabelled has another frame here (``mesh.frames``).  Only for
+    meshes as read (refinement renumbers the elements)."""
+    if mesh.frames is None:
+        raise ValueError("the mesh has no file frames (not read from a file, or refined)")
+    Np, dim, ne = mesh.Np, mesh.dim, mesh.num_elements
+    i = np.arange(Np ** dim)
+    idx = [(i // Np ** a) % Np for a in range(dim)]            # file-frame multi-index, axis 0 fastest
+    fr = np.asarray(mesh.frames, dtype=np.int64)
+    out = np.zeros((ne, Np ** dim), dtype=np.int64)
+    for a in range(dim):
+        d = np.abs(fr[:, a]) - 1
+        j = np.where(fr[:, a][:, None] > 0, idx[a][None, :], mesh.order - idx[a][None, :])
+        out += j * (Np ** d)[:, None]
+    return out
+
+
+def from_reference_order(mesh: CartesianMesh, u: np.ndarray) -> np.ndarray:
+    """A byNODES field (components x elements x nodes) in the reference's
+    per-element node order, in this mesh's order."""
+    perm = node_permutation(mesh)
+    x = np.asarray(u).reshape(-1, mesh.num_elements, mesh.ndof)
+    out = np.empty_like(x)
+    rows = np.arange(mesh.num_elements)[:, None]
+    out[:, rows, perm] = x
+    return out.reshape(np.shape(u))
+
+
+def to_reference_order(mesh: CartesianMesh, u: np.ndarray) -> np.ndarray:
+    """This mesh's byNODES field in the reference's per-element node order."""
+    perm = node_permutation(mesh)
+    x = np.asarray(u).reshape(-1, mesh.num_elements, mesh.ndof)
+    rows = np.arange(mesh.num_elements)[:, None]
+    return x[:, rows, perm].reshape(np.shape(u))

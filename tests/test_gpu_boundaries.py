@@ -238,3 +238,30 @@ def test_gpu_case_builders_match_oracle(which, cuda_device):
     torch.cuda.synchronize()
     assert rel_maxnorm(x.cpu().numpy(), y) < 1e-11
     assert op.check() == 0
+
+
+@pytest.mark.parametrize("name", ["ns_2d_subsonic", "ns_3d_channel", "ns_2d_riemann"])
+def test_gpu_ns_boundary_face_paths_agree(name, cuda_device, monkeypatch):
+    """The fixed operator's element-side faces and its separate face passes
+    (PDG_ELEMENT_FACES=0: lifting, face kernels, boundary_kernel) give the
+    same Navier-Stokes result on meshes with boundary faces."""
+    import torch
+    from test_boundaries import NS_KW, ns_layout_case
+    mesh, u = ns_layout_case(name, 3)
+    op = pb.DGSEMOperator(mesh, compat=0, **NS_KW)
+    monkeypatch.setenv("PDG_ELEMENT_FACES", "0")
+    op_sep = pb.DGSEMOperator(mesh, compat=0, **NS_KW)
+    monkeypatch.delenv("PDG_ELEMENT_FACES")
+    un = dev(u, cuda_device)
+    us = dev(rough(u, mesh, 9, 0.01, 0.001), cuda_device)
+    for stage in (-1, 0, 2):
+        a, b = torch.empty_like(un), torch.empty_like(un)
+        if stage < 0:
+            op.Mult(us, a)
+            op_sep.Mult(us, b)
+        else:
+            op.rk_stage(stage, 1e-3, un, us, a)
+            op_sep.rk_stage(stage, 1e-3, un, us, b)
+        torch.cuda.synchronize()
+        assert rel_maxnorm(a.cpu().numpy(), b.cpu().numpy()) < 1e-13
+    assert op.check() == 0 and op_sep.check() == 0

@@ -82,13 +82,15 @@ def rotate(corners, dim, rng):
     return out
 
 
-def write_gmsh(path, mesh, rng, names=None):
+def write_gmsh(path, mesh, rng, names=None, info=None):
     pid, coords = grid_points(mesh)
     corners = element_corners(mesh, pid)
     bfaces = boundary_faces(mesh, corners)
     perm = rng.permutation(mesh.num_elements)             # file element i = mesh element perm[i]
     node_ids = rng.permutation(np.arange(7, 7 + 3 * len(coords)))[:len(coords)]   # sparse 1-based ids
     listed = rotate(corners[perm], mesh.dim, rng)
+    if info is not None:
+        info.update(listed=listed, coords=coords)
     dom, bnd = (3, 1) if mesh.dim == 2 else (5, 3)
     lines = ["$MeshFormat", "2.2 0 8", "$EndMeshFormat"]
     if names:
@@ -304,6 +306,39 @@ def test_read_mesh_runs_in_the_oracle(tmp_path):
     r0 = oracle.Oracle(orig, compat=0).rhs(u0).reshape(4, orig.num_elements, nd)[:, perm]
     r1 = oracle.Oracle(m, compat=0).rhs(um).reshape(4, m.num_elements, nd)
     assert np.max(np.abs(r1 - r0)) <= 1e-12 * np.max(np.abs(r0))
+
+
+
+@pytest.mark.parametrize("dim", [2, 3])
+def test_reference_node_order(tmp_path, dim):
+    """Fields move between the reference's per-element node order (each
+    element's own frame from its listed corners, LGL nodes lexicographic)
+    and this mesh's: node coordinates computed in the file frames match."""
+    from prandtl_b200.mesh import gll_nodes
+    rng = np.random.default_rng(7 + dim)
+    n = (4, 3) if dim == 2 else (3, 2, 2)
+    orig = box(dim, 3, n, 0.0, [2.0, 1.5, 1.0][:dim], bdr=[(0, 1), (2, 3), (2, 3)][:dim])
+    info = {}
+    write_gmsh(str(tmp_path / "f.msh"), orig, rng, info=info)
+    m = meshio.read_mesh(str(tmp_path / "f.msh"), 3)
+    assert len(m.reoriented) > 0
+    x1, _ = gll_nodes(m.Np)
+    Np = m.Np
+    want = np.empty((dim, m.num_elements, Np ** dim))
+    for e in range(m.num_elements):
+        c = info["coords"][info["listed"][e]]                  # listed corners, file order
+        axes = [c[1] - c[0], c[3] - c[0]] + ([c[4] - c[0]] if dim == 3 else [])
+        for i in range(Np ** dim):
+            p = c[0].copy()
+            for a in range(dim):
+                p = p + x1[(i // Np ** a) % Np] * axes[a]
+            want[:, e, i] = p
+    ours = m.node_coords().reshape(dim, m.num_elements, -1)
+    got = meshio.to_reference_order(m, ours)
+    np.testing.assert_allclose(got, want, atol=1e-12)
+    np.testing.assert_allclose(meshio.from_reference_order(m, want), ours, atol=1e-12)
+    with pytest.raises(ValueError, match="frames"):
+        meshio.node_permutation(meshio.refine_mesh(m))
 
 
 @pytest.mark.gpu
