@@ -112,7 +112,7 @@ int pdg_destroy(pdg_ctx *ctx);
  * 490-798).  A neighbour entry -1 - b (0 <= b < PDG_MAX_BOUNDARIES) marks a
  * boundary face with condition b; every condition the mesh uses must be set
  * before the first evaluation (else PDG_ERR_ARG).  Navier-Stokes boundary
- * faces: types 1, 2, 3, 6, 7, 10 and 11, and 9 with compat = 0 (others:
+ * faces: types 1, 2, 3, 6, 7, 8 (2D), 10 and 11, and 9 with compat = 0 (others:
  * PDG_ERR_UNSUPPORTED at the first evaluation; the reference has no viscous
  * flux for 4 and 5); pdg_rhs_vjp differentiates every condition of an Euler
  * mesh and none of a Navier-Stokes one.  `state` holds the condition's

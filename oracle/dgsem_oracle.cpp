@@ -1056,7 +1056,7 @@ static double bdr_face_vector(const Ctx &c, const double *u, int64_t e, int d, i
         lam = std::max(lam, bdr_flux(c, b, s1, nor, flux));
         double dU[5];
         for (int v = 0; v < nv; v++) dU[v] = -flux[v];
-        if (c.p.parabolic && (type == 2 || type == 10 || type == 11)) {
+        if (c.p.parabolic && (type == 2 || type == 10 || type == 11 || type == 8)) {
             // ComputeBdrFaceViscousFlux: the interior state's viscous flux
             // with its own gradients (SupersonicOutflowBdrFaceIntegrator.cpp:
             // 15-20); the no-slip wall replaces the energy row by the wall
@@ -1064,7 +1064,15 @@ static double bdr_face_vector(const Ctx &c, const double *u, int64_t e, int d, i
             // (NoSlipAdiabWallBdrFaceIntegrator.cpp:21-36)
             for (int q = 0; q < dim; q++)
                 for (int v = 0; v < nv; v++) dq[q * nv + v] = c.grads[(size_t)q * c.size + idx(c, v, e, n)];
-            viscous_flux(dim, c.p.gamma, c.p.Pr, c.p.mu, s1, dq, fm);
+            if (type == 8) {
+                // the total-pressure inflow: the outer state's viscous flux with
+                // the interior gradients (SubsonicInflowPtTtAngBdrFaceIntegrator.cpp:88-92)
+                double so[5], fl[5];
+                bdr_flux(c, b, s1, nor, fl, so);
+                viscous_flux(dim, c.p.gamma, c.p.Pr, c.p.mu, so, dq, fm);
+            } else {
+                viscous_flux(dim, c.p.gamma, c.p.Pr, c.p.mu, s1, dq, fm);
+            }
             double fn[5];
             for (int v = 0; v < nv; v++) {
                 fn[v] = 0.0;
@@ -1124,7 +1132,7 @@ static void bdr_lifting_flux(const Ctx &c, int b, const double *s1, const double
     }
     if (type == 1 || type == 3)
         for (int v = 0; v < nv; v++) s2[v] = c.bc[b][1 + v];
-    if (type == 6 || type == 7 || type == 9) {
+    if (type == 6 || type == 7 || type == 8 || type == 9) {
         // ComputeOuterInviscidState of the subsonic outflow, the subsonic
         // inflow (rho, V) and the Riemann invariants, from s2 (the interior
         // state, or in compat what Entropy2Conserv made of w1), with their

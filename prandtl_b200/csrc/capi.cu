@@ -487,15 +487,16 @@ int evaluate(pdg_ctx *c, int stage, double dt, const double *un, const double *u
         if (c->bc_used) {
             // Navier-Stokes boundary faces: the conditions with a viscous boundary flux
             // slip wall and symmetry have no viscous flux in the reference
-            // (BdrFaceIntegrator.cpp:260-273 raise mfem_error); the total-
-            // pressure inflow's viscous flux and the reference-value Riemann
-            // invariants' lifting (a normal left from another face) are not built
+            // (BdrFaceIntegrator.cpp:260-273 raise mfem_error); the
+            // reference-value Riemann invariants' lifting (a normal left from
+            // another face) is not built
             for (int b = 0; b < PDG_MAX_BOUNDARIES; b++) {
                 const int t = (int)c->bc_host[b * BC_SLOT];
                 const bool ok = t == PDG_BC_SUPERSONIC_INFLOW || t == PDG_BC_SUPERSONIC_OUTFLOW ||
                                 t == PDG_BC_SPECIFIED_STATE || t == PDG_BC_NOSLIP_ADIABATIC ||
                                 t == PDG_BC_NOSLIP_ISOTHERMAL || t == PDG_BC_SUBSONIC_OUTFLOW_P ||
-                                t == PDG_BC_SUBSONIC_INFLOW_RV || (t == PDG_BC_RIEMANN_INVARIANT && !c->p.compat);
+                                t == PDG_BC_SUBSONIC_INFLOW_RV || t == PDG_BC_SUBSONIC_INFLOW_PTTT ||
+                                (t == PDG_BC_RIEMANN_INVARIANT && !c->p.compat);
                 if ((c->bc_used >> b & 1u) && !ok)
                     return fail(c, PDG_ERR_UNSUPPORTED,
                                 "boundary condition %d: type %d has no viscous boundary flux here", b, t);

@@ -613,7 +613,7 @@ __device__ __forceinline__ void face_terms_dir(const KParams &P, const double *c
                         const double nrm = side ? C_AREA(c)[D] : -C_AREA(c)[D];
                         const double *fo = P.fcol + (((D * 2 + side) * ne + e) * NFN + fn) * (NV - 1);
                         const bool own = type == BC_SUPERSONIC_OUTFLOW || type == BC_NOSLIP_ADIABATIC ||
-                                         type == BC_NOSLIP_ISOTHERMAL;
+                                         type == BC_NOSLIP_ISOTHERMAL || type == BC_SUBSONIC_INFLOW_PTTT;
 #pragma unroll
                         for (int i = 0; i <= DIM; i++) fv[r][i] = own ? __ldg(fo + i) * nrm : 0.0;
                         if (type == BC_NOSLIP_ADIABATIC) {  // energy row: the wall velocity's work, qn = 0
@@ -1183,7 +1183,8 @@ __device__ __forceinline__ double boundary_node(const KParams &P, const double *
     if (NS) {
         const double *bc = P.bc + b * BC_SLOT;
         const int type = (int)bc[0];
-        if (type == BC_SUPERSONIC_OUTFLOW || type == BC_NOSLIP_ADIABATIC || type == BC_NOSLIP_ISOTHERMAL) {
+        if (type == BC_SUPERSONIC_OUTFLOW || type == BC_NOSLIP_ADIABATIC || type == BC_NOSLIP_ISOTHERMAL ||
+            type == BC_SUBSONIC_INFLOW_PTTT) {
             const double nrm = side ? C_AREA(c)[D] : -C_AREA(c)[D];
             const double *fo = P.fcol + (((D * 2 + side) * P.ne + a) * S::NFN + fn) * (NV - 1);
             double fv[DIM + 1];
@@ -1343,7 +1344,7 @@ __device__ __noinline__ void lift_boundary_node(const KParams &P, const double *
 #pragma unroll
             for (int q = 0; q < DIM; q++) s2[1 + q] = s2[0] * w1[1 + q];
             s2[NV - 1] = s2[0] * (1.0 / beta * P.gm1inv + 0.5 * vv);
-            if (type == BC_SUBSONIC_OUTFLOW_P || type == BC_SUBSONIC_INFLOW_RV) {
+            if (type == BC_SUBSONIC_OUTFLOW_P || type == BC_SUBSONIC_INFLOW_RV || type == BC_SUBSONIC_INFLOW_PTTT) {
                 // ComputeOuterInviscidState of that state (BdrFaceIntegrator.cpp:278)
                 double so[NV];
                 subsonic_outer_state<DIM, D>(P, type, bc + 1, side ? 1.0 : -1.0, s2, so);
@@ -1359,7 +1360,8 @@ __device__ __noinline__ void lift_boundary_node(const KParams &P, const double *
         entropy_vars<DIM>(bc + 1, P.gamma, P.gm1, P.gm1inv, w2);
 #pragma unroll
         for (int v = 0; v < NV; v++) f[v] = (w2[v] - w1[v]) * 0.5;
-    } else if (type == BC_SUBSONIC_OUTFLOW_P || type == BC_SUBSONIC_INFLOW_RV || type == BC_RIEMANN_INVARIANT) {
+    } else if (type == BC_SUBSONIC_OUTFLOW_P || type == BC_SUBSONIC_INFLOW_RV || type == BC_RIEMANN_INVARIANT ||
+               type == BC_SUBSONIC_INFLOW_PTTT) {
         // the outer state of the inviscid flux (BdrFaceIntegrator.cpp:275-282)
         double so[NV], w2[NV];
         subsonic_outer_state<DIM, D>(P, type, bc + 1, side ? 1.0 : -1.0, s, so);
@@ -1488,6 +1490,31 @@ __device__ __forceinline__ void divergence_lines(const double *fvs, double *dv, 
 // stored to P.vbuf when the volume kernel with element-side faces runs after
 // this one) and the normal column at every face node (with the node's own
 // state, DGSEMIntegrator.cpp:467-477, written to P.fcol).
+// Viscous column of the total-pressure inflow's outer state with the
+// interior's primitive gradients dq[d * NV + v]
+// (SubsonicInflowPtTtAngBdrFaceIntegrator.cpp:88-92), stored in place of the
+// element's own column at that boundary face node.
+template <int DIM, int D>
+__device__ __noinline__ void outer_viscous_col(const KParams &P, const double *s, int b, double sgn,
+                                               const double *dq, double *col)
+{
+    constexpr int NV = DIM + 2;
+    double s1[NV], so[NV];
+#pragma unroll
+    for (int v = 0; v < NV; v++) s1[v] = s[v];
+    subsonic_outer_state<DIM, D>(P, BC_SUBSONIC_INFLOW_PTTT, P.bc + b * BC_SLOT + 1, sgn, s1, so);
+    const NodeState<DIM> ns = node_state<DIM>(so, P.gm1);
+    Prim<DIM> q;
+    q.rho = ns.rho;
+    q.irho = ns.irho;
+#pragma unroll
+    for (int d = 0; d < DIM; d++) q.v[d] = ns.vel[d];
+    q.p = ns.p;
+    q.beta = q.ib = q.lam = 0.0;
+    auto G = [&](int d, int v) { return dq[d * NV + v]; };
+    viscous_col<DIM>(q, G, D, P.gm1inv, P.mu, P.lambda_k, col);
+}
+
 // BDR: jumps of -d boundary faces come from P.lbuf_lo (Navier-Stokes meshes
 // with boundary faces).
 template <int DIM, int N, bool BDR = false>
@@ -1628,6 +1655,14 @@ __global__ void __launch_bounds__(128) lift_kernel(const KParams P)
                     const int pos = idx[d];
                     if (valid && (pos == 0 || pos == N)) {
                         if (compat) viscous_col<DIM>(qn, GQ, d, P.gm1inv, P.mu, P.lambda_k, col);
+                        if (BDR && DIM == 2) {
+                            const int64_t nbf = pos == N ? (int64_t)__ldg(P.nbr + e * 2 * DIM + 2 * d + 1) : enb[d];
+                            if (nbf < 0 && (int)P.bc[(-1 - nbf) * BC_SLOT] == BC_SUBSONIC_INFLOW_PTTT) {
+                                const double sgn = pos == N ? 1.0 : -1.0;
+                                if (d == 0) outer_viscous_col<DIM, 0>(P, s, (int)(-1 - nbf), sgn, &dq[0][0], col);
+                                else outer_viscous_col<DIM, (DIM > 1 ? 1 : 0)>(P, s, (int)(-1 - nbf), sgn, &dq[0][0], col);
+                            }
+                        }
                         const int line = d == 0 ? (DIM == 2 ? idx[1] : idx[1] + Np * idx[2])
                                                 : (d == 1 ? (DIM == 2 ? idx[0] : idx[0] + Np * idx[2]) : idx[0] + Np * idx[1]);
                         const int side = pos == N ? 1 : 0;

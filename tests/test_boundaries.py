@@ -193,6 +193,11 @@ def ns_layouts():
         "ns_3d_subsonic": (3, dict(bdr=[(0, 1), (2, 2), None], boundaries={
             0: (pb.BC_SUBSONIC_INFLOW_RV, [1.2, 0.1, 0.05, -0.02]), 1: (pb.BC_SUBSONIC_OUTFLOW_P, [2.0]),
             2: (NOSLIP, [0.0, 0.0, 0.0])})),
+        # total-pressure inflow: the outer state's viscous flux with the
+        # interior gradients (2D)
+        "ns_2d_pttt": (2, dict(bdr=[(0, 1), (2, 2)], boundaries={
+            0: (pb.BC_SUBSONIC_INFLOW_PTTT, [3.5, 3.0, 2.0, 10.0, 0.0]), 1: (pb.BC_SUBSONIC_OUTFLOW_P, [2.2]),
+            2: (NOSLIP, [0.0, 0.0])})),
         # Riemann invariants: fixed operator only (the reference's lifting
         # flux reads the normal left by the last face evaluation)
         "ns_2d_riemann": (2, dict(bdr=[(0, 0), (1, 1)], boundaries={
@@ -201,7 +206,7 @@ def ns_layouts():
 
 
 NS_PINNED = ["ns_2d_channel", "ns_2d_cavity", "ns_2d_isothermal", "ns_3d_channel", "ns_2d_subsonic",
-             "ns_3d_subsonic"]
+             "ns_3d_subsonic", "ns_2d_pttt"]
 
 
 def ns_layout_case(name, order):
