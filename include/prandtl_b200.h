@@ -277,6 +277,7 @@ int64_t pdg_launch_count(const pdg_ctx *ctx);
 #define PDG_KERNEL_LIFT_BDR  26      /* lifting kernel, */
 #define PDG_KERNEL_NS_FACES_BDR 27   /* volume kernel with element-side faces */
 #define PDG_KERNEL_BOUNDARY_NS 28    /* boundary faces of the separate-face path (Navier-Stokes) */
+#define PDG_KERNEL_LIFT_BDR_PTTT 29  /* lifting kernel of a 2D mesh with a total-pressure inflow */
 int pdg_profile_enable(pdg_ctx *ctx, int on);
 int pdg_profile_read(pdg_ctx *ctx, int kind, double *total_ms, int64_t *launches);
 

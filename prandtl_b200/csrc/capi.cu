@@ -314,8 +314,10 @@ bool kind_used(int kind, int dim, bool parabolic, bool filter)
         return false;  // configured by the first pdg_rhs_vjp
     const bool ns_kind = kind == KIND_NS || kind == KIND_NS_FACES || kind == KIND_LIFT || kind == KIND_LIFT_FACE ||
                          (kind >= KIND_FACE_NS0 && kind <= KIND_FACE_NS2) || kind == KIND_LIFT_FACE_BDR ||
-                         kind == KIND_LIFT_BDR || kind == KIND_NS_FACES_BDR || kind == KIND_BOUNDARY_NS;
+                         kind == KIND_LIFT_BDR || kind == KIND_NS_FACES_BDR || kind == KIND_BOUNDARY_NS ||
+                         kind == KIND_LIFT_BDR_PTTT;
     if (ns_kind != parabolic) return false;
+    if (kind == KIND_LIFT_BDR_PTTT && dim != 2) return false;
     if ((kind == KIND_FACE_E2 || kind == KIND_FACE_NS2) && dim < 3) return false;
     return true;
 }
@@ -447,6 +449,16 @@ int launch_with(pdg_ctx *c, int kind, KParams P, void *a1, void *a2, void *a3, c
 // BR1 lifting of state u: face jumps, then gradients (to grads_out when it
 // is not null) and, with P.out set, the viscous volume term added to the
 // output and the face columns of the viscous flux.
+// The lifting kernel of a Navier-Stokes mesh with boundary faces: the
+// total-pressure inflow has its own instantiation.
+int lift_bdr_kind(const pdg_ctx *c)
+{
+    for (int b = 0; b < PDG_MAX_BOUNDARIES; b++)
+        if ((c->bc_used >> b & 1u) && (int)c->bc_host[b * BC_SLOT] == PDG_BC_SUBSONIC_INFLOW_PTTT)
+            return KIND_LIFT_BDR_PTTT;
+    return KIND_LIFT_BDR;
+}
+
 int lift(pdg_ctx *c, KParams P, const double *u, double *grads_out, cudaStream_t s)
 {
     P.u = u;
@@ -455,7 +467,7 @@ int lift(pdg_ctx *c, KParams P, const double *u, double *grads_out, cudaStream_t
         return fail(c, PDG_ERR_ARG, "a boundary condition the mesh uses is not set (pdg_set_boundary)");
     int r = launch(c, c->bc_used ? KIND_LIFT_FACE_BDR : KIND_LIFT_FACE, P, s);
     if (r) return r;
-    return launch(c, c->bc_used ? KIND_LIFT_BDR : KIND_LIFT, P, s);
+    return launch(c, c->bc_used ? lift_bdr_kind(c) : KIND_LIFT, P, s);
 }
 
 // RHS (stage < 0) or fused SSP-RK3 stage of the operator on device buffers.
@@ -504,11 +516,11 @@ int evaluate(pdg_ctx *c, int stage, double dt, const double *un, const double *u
             if ((r = launch(c, KIND_LIFT_FACE_BDR, P, s))) return r;
             if (element_faces) {
                 P.vbuf = c->vbuf;
-                if ((r = launch(c, KIND_LIFT_BDR, P, s))) return r;
+                if ((r = launch(c, lift_bdr_kind(c), P, s))) return r;
                 if ((r = launch(c, KIND_NS_FACES_BDR, P, s))) return r;
             } else {  // separate face passes, then the boundary faces
                 if ((r = launch(c, KIND_NS, P, s))) return r;
-                if ((r = launch(c, KIND_LIFT_BDR, P, s))) return r;
+                if ((r = launch(c, lift_bdr_kind(c), P, s))) return r;
                 for (int d = 0; d < c->dim; d++)
                     if ((r = launch(c, KIND_FACE_NS0 + d, P, s))) return r;
                 if ((r = launch(c, KIND_BOUNDARY_NS, P, s))) return r;

@@ -33,7 +33,8 @@ enum KernelKind {
     KIND_LIFT_BDR = 26,         // lift_kernel<dim, N, true>
     KIND_NS_FACES_BDR = 27,     // rhs_kernel<dim, N, true, true, true>
     KIND_BOUNDARY_NS = 28,      // boundary_kernel<dim, N, true>: NS boundary faces of the separate-face path
-    KIND_COUNT = 29
+    KIND_LIFT_BDR_PTTT = 29,    // lift_kernel<2, N, true, true>: a mesh with a total-pressure inflow (2D)
+    KIND_COUNT = 30
 };
 
 struct KernelInfo {

@@ -28,6 +28,7 @@ template <int N> static bool info_n(int kind, KernelInfo *out)
         break;
     case KIND_LIFT_FACE_BDR: out->fn = (const void *)&lift_face_kernel<2, N, true>; break;
     case KIND_LIFT_BDR: out->fn = (const void *)&lift_kernel<2, N, true>; out->el_doubles = S::EL_LIFTF; break;
+    case KIND_LIFT_BDR_PTTT: out->fn = (const void *)&lift_kernel<2, N, true, true>; out->el_doubles = S::EL_LIFTF; break;
     case KIND_LIFT: out->fn = (const void *)&lift_kernel<2, N>; out->el_doubles = S::EL_LIFTF; break;
     case KIND_LIFT_FACE: out->fn = (const void *)&lift_face_kernel<2, N>; break;
     case KIND_FACE_E0: out->fn = (const void *)&face_kernel<2, N, 0, false>; break;

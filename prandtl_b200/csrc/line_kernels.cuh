@@ -1516,8 +1516,11 @@ __device__ __noinline__ void outer_viscous_col(const KParams &P, const double *s
 }
 
 // BDR: jumps of -d boundary faces come from P.lbuf_lo (Navier-Stokes meshes
-// with boundary faces).
-template <int DIM, int N, bool BDR = false>
+// with boundary faces).  PTTT (2D, a mesh with a total-pressure inflow): the
+// face columns of those boundary faces come from outer_viscous_col; a
+// separate instantiation, since the out-of-line call gives the kernel a stack
+// frame that slowed the other boundary meshes by ~8 %.
+template <int DIM, int N, bool BDR = false, bool PTTT = false>
 __global__ void __launch_bounds__(128) lift_kernel(const KParams P)
 {
     using S = Shape<DIM, N>;
@@ -1655,12 +1658,18 @@ __global__ void __launch_bounds__(128) lift_kernel(const KParams P)
                     const int pos = idx[d];
                     if (valid && (pos == 0 || pos == N)) {
                         if (compat) viscous_col<DIM>(qn, GQ, d, P.gm1inv, P.mu, P.lambda_k, col);
-                        if (BDR && DIM == 2) {
+                        if constexpr (BDR && PTTT && DIM == 2) {
                             const int64_t nbf = pos == N ? (int64_t)__ldg(P.nbr + e * 2 * DIM + 2 * d + 1) : enb[d];
                             if (nbf < 0 && (int)P.bc[(-1 - nbf) * BC_SLOT] == BC_SUBSONIC_INFLOW_PTTT) {
+                                // a copy, so that dq itself stays in registers
+                                double dqc[DIM * NV];
+#pragma unroll
+                                for (int q = 0; q < DIM; q++)
+#pragma unroll
+                                    for (int v = 0; v < NV; v++) dqc[q * NV + v] = dq[q][v];
                                 const double sgn = pos == N ? 1.0 : -1.0;
-                                if (d == 0) outer_viscous_col<DIM, 0>(P, s, (int)(-1 - nbf), sgn, &dq[0][0], col);
-                                else outer_viscous_col<DIM, (DIM > 1 ? 1 : 0)>(P, s, (int)(-1 - nbf), sgn, &dq[0][0], col);
+                                if (d == 0) outer_viscous_col<DIM, 0>(P, s, (int)(-1 - nbf), sgn, dqc, col);
+                                else outer_viscous_col<DIM, (DIM > 1 ? 1 : 0)>(P, s, (int)(-1 - nbf), sgn, dqc, col);
                             }
                         }
                         const int line = d == 0 ? (DIM == 2 ? idx[1] : idx[1] + Np * idx[2])
