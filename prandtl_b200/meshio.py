@@ -158,6 +158,9 @@ def _parse_gmsh(text: str) -> dict:
     pn = _section(lines, "PhysicalNames") or []
     phys = [ln.split(None, 2) for ln in pn[1:] if ln]
     node_sec = _section(lines, "Nodes")
+    elem_sec = _section(lines, "Elements")
+    if node_sec is None or elem_sec is None:
+        raise ValueError("Gmsh mesh without a $Nodes or $Elements section")
     ids, xyz = [], []
     for ln in node_sec[1:]:
         if not ln:
@@ -168,7 +171,7 @@ def _parse_gmsh(text: str) -> dict:
     index = {v: k for k, v in enumerate(ids)}
     xyz = np.array(xyz)
     quads, hexes, lines1 = [], [], []
-    for ln in _section(lines, "Elements")[1:]:
+    for ln in elem_sec[1:]:
         if not ln:
             continue
         r = [int(v) for v in ln.split()]
@@ -252,7 +255,7 @@ def build_mesh(dim, order, verts, coords, bdr, names, attrs=None, tol=1e-8) -> C
     ext = np.stack([coords[:, (1, 3, 4)[d], d] - origin[:, d] for d in range(dim)], axis=1)
     if np.any(ext <= 0):
         bad = int(np.nonzero(np.any(ext <= 0, axis=1))[0][0])
-        raise ValueError(f"element {bad}: its first corner is not its lowest one (rotated or inverted element)")
+        raise ValueError(f"element {bad} is degenerate (an extent of zero)")
     h = ext.mean(axis=0)
     expect = origin[:, None, :] + bits[None, :, :] * ext[:, None, :]
     if np.any(np.abs(coords - expect) > tol * h):
@@ -301,7 +304,8 @@ def build_mesh(dim, order, verts, coords, bdr, names, attrs=None, tol=1e-8) -> C
             nbr[e, 2 * d + side] = -a
             used.add(a)
         else:
-            raise ValueError(f"a face shared by {len(owners)} elements (non-conforming mesh)")
+            raise ValueError(f"a face shared by {len(owners)} elements (a non-conforming mesh, or a periodic "
+                             "direction of fewer than three elements)")
     return CartesianMesh(dim, int(order), n, tuple(float(v) for v in lo), tuple(float(v) for v in hi),
                          nbr.astype(np.int32), spacing=tuple(float(v) for v in h), boundaries={}, cells=cells,
                          boundary_names={k: int(v) - 1 for k, v in names.items() if int(v) in used},

@@ -219,6 +219,9 @@ def test_rejections(tmp_path):
     open(path, "w").write(text.replace("$MeshFormat\n2.2 0 8", "$MeshFormat\n2.2 1 8"))
     with pytest.raises(ValueError, match="ASCII"):
         meshio.read_mesh(path, 1)
+    open(path, "w").write(text.replace("$Nodes", "$Knots").replace("$EndNodes", "$EndKnots"))
+    with pytest.raises(ValueError, match="Nodes"):
+        meshio.read_mesh(path, 1)
     open(path, "w").write(text.replace(" 15 2 0 1 ", " 9 2 0 1 "))   # a second-order triangle
     with pytest.raises(ValueError, match="element type 9"):
         meshio.read_mesh(path, 1)
