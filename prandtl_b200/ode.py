@@ -22,6 +22,8 @@ are not provided.
 """
 from __future__ import annotations
 
+from contextlib import nullcontext
+
 
 class ExplicitRKSolver:
     """x_{n+1} = x_n + dt sum_i b_i k_i, k_i = L(x_n + dt sum_{j<i} A_ij k_j)."""
@@ -33,6 +35,7 @@ class ExplicitRKSolver:
         self.A, self.b, self.c = [list(r) for r in A], list(b), list(c)
         self.op = None
         self._k = []
+        self._y = None
 
     def Init(self, op):
         self.op = op
@@ -47,7 +50,7 @@ class ExplicitRKSolver:
         if len(self._k) != s or self._k[0].shape != x.shape or self._k[0].device != x.device:
             self._k = [torch.empty_like(x) for _ in range(s)]
             self._y = torch.empty_like(x)
-        ctx = torch.cuda.stream(stream) if stream is not None else _nullcontext()
+        ctx = torch.cuda.stream(stream) if stream is not None else nullcontext()
         with ctx:
             for i in range(s):
                 if i == 0:
@@ -63,14 +66,6 @@ class ExplicitRKSolver:
                 if bj != 0.0:
                     x.add_(self._k[j], alpha=dt * bj)
         return t + dt
-
-
-class _nullcontext:
-    def __enter__(self):
-        return None
-
-    def __exit__(self, *exc):
-        return False
 
 
 class ForwardEulerSolver(ExplicitRKSolver):
