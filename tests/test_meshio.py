@@ -345,9 +345,10 @@ def test_reference_node_order(tmp_path, dim):
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("dim", [2, 3])
 @pytest.mark.parametrize("compat", [0, 1])
 @pytest.mark.parametrize("parabolic", [0, 1])
-def test_gpu_read_mesh_matches_oracle(tmp_path, compat, parabolic, cuda_device):
+def test_gpu_read_mesh_matches_oracle(tmp_path, compat, parabolic, dim, cuda_device):
     """The operator on a mesh read from a shuffled, rotated Gmsh file
     (elements in file order, a step cut out, named boundaries) against the
     oracle on the same mesh, Euler with a slip wall and Navier-Stokes with
@@ -356,20 +357,27 @@ def test_gpu_read_mesh_matches_oracle(tmp_path, compat, parabolic, cuda_device):
     import oracle
     from helpers import rel_maxnorm, rough
     from test_boundaries import uniform
-    rng = np.random.default_rng(11 + parabolic)
-    keep = np.ones((8, 5), dtype=bool)
-    keep[:3, :2] = False
-    orig = box(2, 3, (8, 5), 0.0, [4.0, 2.5], bdr=[(0, 1), (2, 3)], keep=keep, cut=2)
+    rng = np.random.default_rng(11 + parabolic + 2 * dim)
+    if dim == 2:
+        keep = np.ones((8, 5), dtype=bool)
+        keep[:3, :2] = False
+        orig = box(2, 3, (8, 5), 0.0, [4.0, 2.5], bdr=[(0, 1), (2, 3)], keep=keep, cut=2)
+        order = 3
+    else:                       # hexahedra, every side bounded, a step cut out
+        keep = np.ones((5, 3, 3), dtype=bool)
+        keep[:2, :1, :] = False
+        orig = box(3, 2, (5, 3, 3), 0.0, [2.5, 1.5, 1.5], bdr=[(0, 1), (2, 3), (3, 3)], keep=keep, cut=2)
+        order = 2
     path = str(tmp_path / "g.msh")
     write_gmsh(path, orig, rng, {"in": 1, "out": 2, "wall": 3, "top": 4})
-    m = meshio.read_mesh(path, 3)
-    fs = [1.0, 2.0, 0.0, 1.0 / 0.4 + 0.5 * 4.0]
-    wall = (pb.BC_NOSLIP_ADIABATIC, [0.0, 0.0]) if parabolic else (pb.BC_SLIP_WALL, None)
+    m = meshio.read_mesh(path, order)
+    fs = [1.0, 2.0, 0.0, 1.0 / 0.4 + 0.5 * 4.0] if dim == 2 else [1.0, 2.0, 0.0, 0.0, 1.0 / 0.4 + 0.5 * 4.0]
+    wall = (pb.BC_NOSLIP_ADIABATIC, [0.0] * dim) if parabolic else (pb.BC_SLIP_WALL, None)
     conds = {"in": (pb.BC_SUPERSONIC_INFLOW, fs), "out": (pb.BC_SUPERSONIC_OUTFLOW, None),
              "wall": wall, "top": wall}
     m.boundaries = {m.boundary_names[k]: v for k, v in conds.items()}
     kw = dict(compat=compat, parabolic=parabolic, mu=0.02 if parabolic else 0.0, Pr=0.71)
-    u = rough(uniform(m, vel=(2.0, 0.0)), m, 4, 0.02, 0.002)
+    u = rough(uniform(m, vel=(2.0, 0.0, 0.0)[:dim]), m, 4, 0.02, 0.002)
     orc = oracle.Oracle(m, **kw)
     ref = orc.rhs(u)
     op = pb.DGSEMOperator(m, **kw)
