@@ -88,22 +88,22 @@ def _parse_mfem(text: str) -> dict:
     dim = int(lines[pos["dimension"] + 1])
     if dim not in (2, 3):
         raise ValueError(f"MFEM mesh of dimension {dim}: only 2 and 3 are read")
-    geom = 3 if dim == 2 else 5
     nc = 2 ** dim
 
-    def cells(key):
+    def cells(key, geom, what):
         i = pos[key] + 1
         n = int(lines[i])
         rows = [lines[i + 1 + k].split() for k in range(n)]
         out = []
         for r in rows:
             if int(r[1]) != geom:
-                raise ValueError(f"MFEM {key} of geometry {r[1]}: only squares and cubes are read")
+                raise ValueError(f"MFEM {key} of geometry {r[1]}: only {what} are read")
             out.append((int(r[0]), [int(v) for v in r[2:]]))
         return out
 
-    elements = cells("elements")
-    boundary = cells("boundary")
+    # MFEM geometries: 1 segment, 3 square, 5 cube
+    elements = cells("elements", 3 if dim == 2 else 5, "squares and cubes")
+    boundary = cells("boundary", 1 if dim == 2 else 3, "segments (2D) and squares (3D)")
     verts = np.array([e[1] for e in elements], dtype=np.int64).reshape(-1, nc)
     i = pos["vertices"] + 1
     nvert = int(lines[i])

@@ -188,6 +188,40 @@ def test_mfem_periodic(tmp_path, dim, n):
     assert len(m.reoriented) == 0 and m.boundary_names == {}
 
 
+def write_mfem_bounded(path, mesh, rng):
+    """An MFEM v1.0 mesh with vertex coordinates and boundary elements,
+    elements shuffled; returns the permutation (file element i = perm[i])."""
+    pid, coords = grid_points(mesh)
+    corners = element_corners(mesh, pid)
+    bfaces = boundary_faces(mesh, corners)
+    perm = rng.permutation(mesh.num_elements)
+    geom = 3 if mesh.dim == 2 else 5
+    text = ["MFEM mesh v1.0", "", "dimension", str(mesh.dim), "", "elements", str(len(perm))]
+    text += [f"7 {geom} " + " ".join(map(str, corners[e])) for e in perm]
+    text += ["", "boundary", str(len(bfaces))]
+    text += [f"{a} {geom - 2} " + " ".join(map(str, fv)) for a, fv in bfaces]
+    text += ["", "vertices", str(len(coords)), str(mesh.dim)]
+    text += [" ".join(f"{v:.17g}" for v in x) for x in coords]
+    with open(path, "w") as f:
+        f.write("\n".join(text) + "\n")
+    return perm
+
+
+@pytest.mark.parametrize("dim", [2, 3])
+def test_mfem_bounded(tmp_path, dim):
+    rng = np.random.default_rng(20 + dim)
+    n = (5, 3) if dim == 2 else (3, 3, 2)
+    keep = np.ones(n, dtype=bool)
+    keep[-1, -1] = False
+    orig = box(dim, 2, n, -1.0, 1.0, bdr=[(0, 1), (2, 3), (0, 1)][:dim], keep=keep, cut=4)
+    path = str(tmp_path / "b.mesh")
+    perm = write_mfem_bounded(path, orig, rng)
+    m = meshio.read_mesh(path, 2)
+    same_mesh(m, orig, perm)
+    assert m.boundary_names == {str(a): a - 1 for a in range(1, 6)}
+    assert np.all(m.attributes == 7) and len(m.reoriented) == 0
+
+
 @pytest.mark.parametrize("dim", [2, 3])
 def test_refinement(dim):
     """Two refinements of a 3 x 2 (x 2) box with boundaries equal the 12 x 8
