@@ -1388,13 +1388,21 @@ __global__ void __launch_bounds__(256) lift_face_kernel(const KParams P)
     __shared__ double c[CONST_SLOTS];
     load_consts(P.K, c, S::Np);
     __syncthreads();
-    const int64_t per_dir = P.ne * NFN;
-    for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < DIM * per_dir;
+    // chunks of CH elements, direction-major inside a chunk: a warp works on
+    // one direction of consecutive elements, and a chunk's traces are still
+    // in L2 for its later directions (direction-major order over the whole
+    // mesh read the state from DRAM about twice per launch)
+    constexpr int CH = 64, PER_CH = DIM * CH * NFN;
+    const int64_t nch = (P.ne + CH - 1) / CH;
+    for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < nch * PER_CH;
          t += (int64_t)gridDim.x * blockDim.x) {
-        const int d = (int)(t / per_dir);
-        const int64_t r = t - d * per_dir;
-        const int64_t a = r / NFN;
-        const int fn = (int)(r - a * NFN);
+        const int64_t ch = t / PER_CH;
+        const int r = (int)(t - ch * PER_CH);
+        const int d = r / (CH * NFN);
+        const int r2 = r - d * (CH * NFN);
+        const int64_t a = ch * CH + r2 / NFN;
+        const int fn = r2 % NFN;
+        if (a >= P.ne) continue;
         if (BDR) {
             const int32_t bp = __ldg(P.nbr + a * 2 * DIM + 2 * d + 1), bm = __ldg(P.nbr + a * 2 * DIM + 2 * d);
             double *dp = P.lbuf + ((d * P.ne + a) * NFN + fn) * (DIM + 2);
