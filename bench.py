@@ -350,6 +350,8 @@ def run_ours(args):
         out["sweep"] = run_sweep(args, dev)
     if not args.no_adjoint and world == 1:
         out["adjoint"] = run_adjoint(args, dev)
+    if args.sweep_steps > 0 and world == 1 and COMPAT == 0:
+        out["reference_operator"] = run_reference_operator(args, dev)
     if args.sweep_steps > 0 and world == 1:
         out["filter_case"] = run_filter_case(args, dev)
         out["boundary_case"] = run_boundary_case(args, dev)
@@ -372,7 +374,9 @@ def run_sweep(args, dev):
     specs = cases.sweep_cases(256, seed=3)
     meshes = [periodic_box(2, N, n, -5.0, 5.0) for n, N, _ in specs]
     states = [cases.isentropic_vortex(m, strength=e) for m, (_, _, e) in zip(meshes, specs)]
-    batch = pb.DGSEMBatch(meshes)
+    # the fixed operator (compat = 0): on 2D Euler it gives the reference-value
+    # operator's results to 1e-15 and runs one launch per stage per case
+    batch = pb.DGSEMBatch(meshes, compat=0)
     u0 = np.concatenate(states)
     assert u0.size == batch.size
     u = torch.from_numpy(u0).to(dev)
@@ -404,21 +408,39 @@ def run_sweep(args, dev):
         res["batched_graph" if graph else "batched_launches"] = {
             "value": V * 3 * K / (ms * 1e-3), "ms_per_step": ms / K, "gpu_launches": batch.launch_count() - l0}
     batch.check()
-    ops = [pb.DGSEMOperator(m) for m in meshes]
-    xs = [torch.from_numpy(s).to(dev) for s in states]
-    for _ in range(args.warmup):
+    # per-case forms: plain launches of the fixed operator (one kernel per
+    # stage), the same with each case's steps replayed from its own CUDA graph,
+    # and plain launches of the reference-value operator (a volume kernel and
+    # one face pass per direction per stage)
+    per_case = {}
+    for name, compat, graph in (("per_case_launches", 0, False), ("per_case_graphs", 0, True),
+                                ("per_case_launches_reference_operator", 1, False)):
+        ops = [pb.DGSEMOperator(m, compat=compat) for m in meshes]
+        xs = [torch.from_numpy(s).to(dev) for s in states]
         for op, x, d in zip(ops, xs, dt):
-            op.rk3_step(x, float(d))
-    l0 = sum(op.launch_count() for op in ops)
-
-    def plain():
-        for _ in range(K):
-            for op, x, d in zip(ops, xs, dt):
-                op.rk3_step(x, float(d))
-    ms = timed(plain)
-    res["per_case_launches"] = {"value": V * 3 * K / (ms * 1e-3), "ms_per_step": ms / K,
-                                "gpu_launches": sum(op.launch_count() for op in ops) - l0}
-    res["batched_vs_per_case"] = res["batched_graph"]["value"] / res["per_case_launches"]["value"]
+            op.rk3_step(x, float(d), nsteps=args.warmup, graph=graph)
+        l0 = sum(op.launch_count() for op in ops)
+        if graph:
+            def run():
+                for op, x, d in zip(ops, xs, dt):
+                    op.rk3_step(x, float(d), nsteps=K, graph=True)
+        else:
+            def run():
+                for _ in range(K):
+                    for op, x, d in zip(ops, xs, dt):
+                        op.rk3_step(x, float(d))
+        ms = timed(run)
+        per_case[name] = {"value": V * 3 * K / (ms * 1e-3), "ms_per_step": ms / K, "compat": compat,
+                          "gpu_launches": sum(op.launch_count() for op in ops) - l0}
+        for op in ops:
+            op.check()
+            op.close()
+    res.update(per_case)
+    best = max(per_case, key=lambda k: per_case[k]["value"])
+    res["batched_vs_per_case"] = res["batched_graph"]["value"] / per_case[best]["value"]
+    res["batched_vs_per_case_against"] = best
+    res["batched_vs_per_case_reference_operator"] = (
+        res["batched_graph"]["value"] / per_case["per_case_launches_reference_operator"]["value"])
     # one small case (the 32 x 32, N = 3 vortex): plain launches vs a replayed step graph
     vm = cases.vortex_mesh(32, 3)
     vop = pb.DGSEMOperator(vm)
@@ -502,6 +524,40 @@ def run_adjoint(args, dev):
                                      "checkpoint_every": 5, "ratio": grad20 / fwd20}}
 
 
+def run_reference_operator(args, dev):
+    """The benchmark workload on the reference-value operator (compat = 1:
+    the reference's stale viscous state, z-direction fill and 3D energy
+    dissipation term, with separate face passes): 20 graph-replayed SSP-RK3
+    steps from the initial state, within the range where that operator stays
+    stable on Taylor-Green."""
+    import torch
+
+    import prandtl_b200 as pb
+    mesh, u0, params = workload(args.n, args.order)
+    params = dict(params, compat=1)
+    op = pb.DGSEMOperator(mesh, **params)
+    x = torch.from_numpy(u0).to(dev)
+    op.Mult(x, torch.empty_like(x))
+    dt = op.cfl_dt(0.5)
+    steps = 20
+    op.rk3_step(x, dt, nsteps=args.warmup, graph=True)
+    torch.cuda.synchronize()
+    l0 = op.launch_count()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    op.rk3_step(x, dt, nsteps=steps, graph=True)
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    launches = op.launch_count() - l0
+    op.check()
+    op.close()
+    return {"workload": config_dict(mesh, 1)["workload"] + "_reference_value_operator", "compat": 1,
+            "vdofs": mesh.size, "steps": steps, "warmup": args.warmup, "value": mesh.size * 3 * steps / (ms * 1e-3),
+            "unit": UNIT, "ms_per_step": ms / steps, "gpu_launches": launches,
+            "path": "pdg_rk3_steps (graph-replayed steps)"}
+
+
 def run_filter_case(args, dev):
     """Kelvin-Helmholtz 64 x 64, N = 4, Euler with the entropy filter after
     every stage: 200 SSP-RK3 steps, CFL 0.5."""
@@ -562,7 +618,10 @@ def _ref_worker(payload):
     n_el, order, steps, seconds = payload
     sys.path.insert(0, ROOT)
     import oracle as orc
-    mesh = periodic_box(3, order, (32, 32, n_el), 0.0, 2 * np.pi)
+    # a slab of n_el element layers of the 32^3 mesh (same element size),
+    # periodic in itself
+    mesh = periodic_box(3, order, (32, 32, n_el), (0.0, 0.0, 0.0),
+                        (2 * np.pi, 2 * np.pi, 2 * np.pi * n_el / 32.0))
     u = cases.taylor_green(mesh)
     r = orc.Reference(mesh, parabolic=True, mu=1.0 / 1600.0, Pr=0.71)
     k = r.rhs(u)
@@ -598,12 +657,16 @@ def run_reference(args):
     cores = os.cpu_count() or 1
     procs = min(cores, 32)
     n_el = max(1, args.n // procs) if args.n >= procs else 1
-    seconds = max(5.0, args.cpu_seconds)
+    # about 1.8 s per step on 16 cores: the driver's 20 timed + 5 warm-up
+    # steps run in full; longer runs are capped so the arm ends in minutes
+    steps = max(1, min(args.steps, 60))
+    warmup = max(0, min(args.warmup, 5))
     ctx = mp.get_context("spawn")
     per_step = []
     with ctx.Pool(procs) as pool:
-        pool.map(_ref_worker, [(n_el, args.order, 1, 1e9)] * procs)  # warm-up: one step each
-        for _ in range(max(1, min(args.steps, 3))):
+        for _ in range(warmup):
+            pool.map(_ref_worker, [(n_el, args.order, 1, 1e9)] * procs)
+        for _ in range(steps):
             res = pool.map(_ref_worker, [(n_el, args.order, 1, 1e9)] * procs)
             per_step.append((sum(r[0] for r in res), max(r[1] for r in res)))
     # all processes run concurrently: throughput = work / slowest process time
@@ -611,11 +674,16 @@ def run_reference(args):
     wall = sum(p[1] for p in per_step)
     value = dofs / wall
     sample = (f"{procs} processes x {len(per_step)} timed SSP-RK3 steps, each process on its own periodic "
-              f"32x32x{n_el} N={args.order} TGV block (reference DGSEMIntegrator/ChandrashekarFlux/LiftingBR1 "
-              f"compiled from the reference tree against a stand-in MFEM header)")
+              f"32x32x{n_el} N={args.order} slab of the TGV mesh (reference DGSEMIntegrator/ChandrashekarFlux/"
+              f"LiftingBR1 compiled from the reference tree against a stand-in MFEM header)")
+    config = config_dict(mesh, args.gpus)
+    # the reference's own code computes the reference-value operator, on
+    # independent periodic slabs (one per process, as MPI ranks would hold)
+    config.update({"compat": 1, "decomposition": f"{procs} independent periodic 32x32x{n_el} slabs, one per process",
+                   "vdofs_timed": 32 * 32 * n_el * procs * mesh.ndof * mesh.nv})
     out = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus, "steps": len(per_step),
-           "warmup": 1, "ms_per_step": wall / len(per_step) * 1e3, "higher_is_better": True, "scaling": "weak",
-           "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": config_dict(mesh, args.gpus),
+           "warmup": warmup, "ms_per_step": wall / len(per_step) * 1e3, "higher_is_better": True, "scaling": "weak",
+           "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": config,
            "impl": "reference",
            "cpu_baseline": {"value": value, "unit": UNIT, "cores": procs, "kind": "reference", "sample": sample},
            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}

@@ -163,11 +163,19 @@ int pdg_rhs(pdg_ctx *ctx, const double *u, double *dudt, void *stream);
  * more returns PDG_ERR_CAPACITY: at order 3 that is above about 5,000
  * elements for Navier-Stokes in 3D and above about 600,000 for Euler.
  * The first call on a device looks up the array's device address on that
- * device (the current device); make that first call before any stream
- * capture.  Every call on a device shares the array and leaves its contents
- * behind: calls that overlap on the GPU race.  The constants and the
- * neighbour table are copied from host memory on `stream` in every call.
- * The device error word is cleared on entry and not reported. */
+ * device (the current device) and keeps it for the process; make that first
+ * call before any stream capture.  The kept address does not survive
+ * cudaDeviceReset.  Every call on a device shares the array and leaves its
+ * contents behind: calls that overlap on the GPU race.
+ * Every call copies the constants and the neighbour table from (pageable)
+ * host memory with cudaMemcpyAsync on `stream`; CUDA may perform such copies
+ * synchronously with respect to the host.
+ * The kernels are the separate-face sequence (volume kernel, then one face
+ * pass per direction) for both operators; for compat = 0 pdg_rhs evaluates
+ * the faces inside the volume kernel instead, and the two agree to rounding
+ * (1e-14 relative), not bit for bit.
+ * The device error word is cleared on entry and not reported: a caller that
+ * needs to detect a non-finite or non-physical state checks dudt itself. */
 #define PDG_NOALLOC_SCRATCH_DOUBLES (3 * 1024 * 1024)
 int pdg_rhs_noalloc(const pdg_mesh *mesh, const pdg_params *params, const double *u, double *dudt,
                     void *stream);

@@ -31,4 +31,6 @@ FILES="$SRC/BasicOperations/BasicOperations.cpp $SRC/RiemannSolvers/Chandrasheka
 CXXFLAGS="-O2 -ffp-contract=off -std=c++17 -shared -fPIC -w"
 g++ $CXXFLAGS $INC -DSUBCELL_FV_BLENDING $FILES -o "$OUT/libref_euler.so"
 g++ $CXXFLAGS $INC -DPARABOLIC -DSUBCELL_FV_BLENDING $FILES -o "$OUT/libref_ns.so"
+# where the tree was found, for the tests that read its mesh files
+echo "$REF" > "$OUT/REFERENCE_TREE"
 echo "built $OUT/libref_euler.so $OUT/libref_ns.so"

@@ -1,0 +1,196 @@
+"""Parity at the benchmark workloads' full sizes, and discrete entropy
+conservation of the CUDA right-hand side.
+
+The other parity tests use meshes of a few dozen elements; these run the
+benchmark meshes themselves through the C ABI and compare with the oracle
+(the C++ restatement of DGSEMOperator::Mult, src/Operators/DGSEMOperator.cpp:
+537-591, and RK3SSPSolver::Step as driven at src/Simulation/Simulation.cpp:1010)
+on the same states:
+
+* isentropic vortex 32 x 32, N = 3, Euler (both operators);
+* Taylor-Green 32^3, N = 3, Navier-Stokes with BR1 lifting, the reference-value
+  operator (compat = 1) and the fixed one (compat = 0), on the initial state
+  and on a roughened state where the subcell blending is active;
+* Kelvin-Helmholtz 64 x 64, N = 4, Euler with the entropy filter after every
+  stage: the stages of one step and the number of filtered elements;
+* 16 cases of the 256-case vortex sweep through the batched persistent kernel.
+
+Tolerance: 1e-12 relative in max norm per right-hand side and per stage.
+
+Entropy conservation: with the face dissipation switched off (the pure
+Chandrashekar face flux) and no blending, the flux-differencing operator is
+entropy conservative on a periodic mesh, sum_i J w_i w(u_i) . (du/dt)_i = 0
+(Tadmor's condition, summed by parts).  The test evaluates that sum for the
+CUDA right-hand side at 1e-12 of sum_i J w_i |w(u_i) . (du/dt)_i|.
+"""
+import numpy as np
+import pytest
+
+import oracle
+import prandtl_b200 as pb
+from prandtl_b200 import cases
+from prandtl_b200.mesh import gll_nodes, periodic_box
+
+from helpers import rel_maxnorm, rough
+
+TOL = 1e-12
+pytestmark = pytest.mark.gpu
+
+
+def _dev(x, device):
+    import torch
+    return torch.from_numpy(np.ascontiguousarray(x)).to(device)
+
+
+def _rhs(op, u, device):
+    import torch
+    ud = _dev(u, device)
+    out = torch.full_like(ud, float("nan"))
+    op.Mult(ud, out)
+    torch.cuda.synchronize()
+    return out.cpu().numpy()
+
+
+def _stage(op, stage, dt, un, us, device):
+    import torch
+    a, b = _dev(un, device), _dev(us, device)
+    out = torch.full_like(a, float("nan"))
+    op.rk_stage(stage, dt, a, b, out)
+    torch.cuda.synchronize()
+    return out.cpu().numpy()
+
+
+def _vortex():
+    m = cases.vortex_mesh(32, 3)
+    return m, cases.isentropic_vortex(m), dict(parabolic=0)
+
+
+def _tgv(rough_state):
+    m = cases.tgv_mesh(32, 3)
+    u = cases.taylor_green(m)
+    if rough_state:
+        u = rough(u, m, 11, 0.02, 0.002)
+    return m, u, dict(parabolic=1, mu=1.0 / 1600.0, Pr=0.71)
+
+
+@pytest.mark.parametrize("compat", [1, 0])
+@pytest.mark.parametrize("case", ["vortex32", "tgv32", "tgv32_rough"])
+def test_benchmark_mesh_rhs_and_stage(case, compat, cuda_device):
+    mesh, u, par = _vortex() if case == "vortex32" else _tgv(case.endswith("rough"))
+    kw = dict(par, compat=compat)
+    op = pb.DGSEMOperator(mesh, **kw)
+    orc = oracle.Oracle(mesh, **kw)
+    ref = orc.rhs(u)
+    assert rel_maxnorm(_rhs(op, u, cuda_device), ref) < TOL
+    _, a1 = op.blending()
+    _, a0 = orc.blending()
+    np.testing.assert_allclose(a1, a0, rtol=0, atol=1e-10)
+    if case == "tgv32_rough":
+        assert (a0 > 0).any(), "the roughened state must switch the subcell blending on"
+    lam = orc.max_char_speed()
+    assert abs(op.GetMaxCharSpeed() - lam) <= 1e-12 * lam
+    dt = 0.5 * min(mesh.h) / (lam * (mesh.order + 1) ** 2)
+    us = u + dt * ref  # a stage input that differs from un
+    for stage in (0, 1, 2):
+        want = orc.rk_stage(stage, dt, u, us)
+        assert rel_maxnorm(_stage(op, stage, dt, u, us, cuda_device), want) < TOL, f"stage {stage}"
+    assert op.check() == 0
+
+
+@pytest.mark.parametrize("compat", [1, 0])
+@pytest.mark.parametrize("rough_state", [False, True])
+def test_kelvin_helmholtz_64_filtered_step(rough_state, compat, cuda_device):
+    mesh = cases.kh_mesh(64, 4)
+    u = cases.kelvin_helmholtz(mesh)
+    if rough_state:
+        u = rough(u, mesh, 13, 0.1, 0.02)
+    kw = dict(parabolic=0, filter=1, compat=compat)
+    orc = oracle.Oracle(mesh, **kw)
+    op = pb.DGSEMOperator(mesh, **kw)
+    orc0 = oracle.Oracle(mesh, parabolic=0, compat=compat)
+    orc0.rhs(u)
+    dt = (2.0 if rough_state else 0.5) * min(mesh.h) / (orc0.max_char_speed() * 25)
+    us = u
+    for stage in (0, 1, 2):
+        want = orc.rk_stage(stage, dt, u, us)
+        got = _stage(op, stage, dt, u, us, cuda_device)
+        assert rel_maxnorm(got, want) < TOL, f"stage {stage}"
+        assert op.filter_count() == orc.filtered_elements()
+        us = want
+    if rough_state:
+        assert orc.filtered_elements() > 0, "the roughened state must exercise the filter"
+    assert op.check() == 0
+
+
+def test_sweep_sample_batched(cuda_device):
+    """16 cases of the 256-case sweep (seed 3), every fifteenth and the largest."""
+    import torch
+    specs = cases.sweep_cases(256, seed=3)
+    pick = sorted(set(list(range(0, 256, 17))[:15] + [int(np.argmax([n * n * (N + 1) ** 2 for n, N, _ in specs]))]))
+    while len(pick) < 16:
+        pick.append(pick[-1] + 1)
+    meshes = [periodic_box(2, specs[i][1], specs[i][0], -5.0, 5.0) for i in pick]
+    states = [cases.isentropic_vortex(m, strength=specs[i][2]) for m, i in zip(meshes, pick)]
+    assert {m.order for m in meshes} == {2, 3, 4, 5}
+    batch = pb.DGSEMBatch(meshes, compat=0)
+    u = torch.from_numpy(np.concatenate(states)).to(cuda_device)
+    out = torch.full_like(u, float("nan"))
+    batch.Mult(u, out)
+    got = out.cpu().numpy()
+    lam = batch.max_char_speed()
+    orcs = [oracle.Oracle(m, compat=0) for m in meshes]
+    for c, (o, s) in enumerate(zip(orcs, states)):
+        assert rel_maxnorm(got[batch.offsets[c]:batch.offsets[c + 1]], o.rhs(s)) < TOL, f"case {pick[c]}"
+        assert abs(lam[c] - o.max_char_speed()) <= 1e-12 * lam[c]
+    dt = batch.cfl_dt(0.5)
+    batch.set_dt(dt)
+    batch.rk3_step(u, nsteps=2, graph=True)
+    got = u.cpu().numpy()
+    for c, (o, s) in enumerate(zip(orcs, states)):
+        y = o.rk3_step(o.rk3_step(s, float(dt[c])), float(dt[c]))
+        assert rel_maxnorm(got[batch.offsets[c]:batch.offsets[c + 1]], y) < TOL, f"case {pick[c]} steps"
+    assert batch.check() == 0
+
+
+def _entropy_vars(u, dim, nn, gamma=1.4):
+    U = u.reshape(dim + 2, nn)
+    rho = U[0]
+    vel = U[1:1 + dim] / rho
+    vsq = np.sum(vel * vel, axis=0)
+    p = (gamma - 1.0) * (U[-1] - 0.5 * rho * vsq)
+    beta = rho / p
+    s = np.log(p * rho ** (-gamma))
+    return np.vstack([(gamma - s) / (gamma - 1.0) - 0.5 * beta * vsq, beta * vel, -beta])
+
+
+@pytest.mark.parametrize("case", ["vortex32", "tgv32", "tgv32_rough", "kh64"])
+def test_discrete_entropy_conservation_on_gpu(case, cuda_device):
+    if case == "vortex32":
+        mesh = cases.vortex_mesh(32, 3)
+        u = rough(cases.isentropic_vortex(mesh), mesh, 17, 0.05, 0.01)
+    elif case == "kh64":
+        mesh = cases.kh_mesh(64, 4)
+        u = cases.kelvin_helmholtz(mesh)
+    else:
+        mesh = cases.tgv_mesh(32, 3)
+        u = cases.taylor_green(mesh)
+        if case.endswith("rough"):
+            u = rough(u, mesh, 19, 0.05, 0.01)
+    dim, nn = mesh.dim, mesh.num_nodes
+    op = pb.DGSEMOperator(mesh, parabolic=0, blending=0, compat=0, face_dissipation=0.0)
+    dudt = _rhs(op, u, cuda_device)
+    _, w1 = gll_nodes(mesh.Np)
+    wq = w1
+    for _ in range(dim - 1):
+        wq = np.kron(w1, wq)
+    W = np.tile(wq, mesh.num_elements) * np.prod(mesh.h)
+    local = np.sum(_entropy_vars(u, dim, nn) * dudt.reshape(dim + 2, nn), axis=0)
+    total = float(np.sum(W * local))
+    scale = float(np.sum(W * np.abs(local)))
+    assert scale > 0
+    assert abs(total) < 1e-12 * scale, f"entropy production {total:.3e} against scale {scale:.3e}"
+    # with the dissipation on, the same sum is negative (entropy stable)
+    op_d = pb.DGSEMOperator(mesh, parabolic=0, blending=0, compat=0)
+    dd = _rhs(op_d, u, cuda_device)
+    prod = float(np.sum(W * np.sum(_entropy_vars(u, dim, nn) * dd.reshape(dim + 2, nn), axis=0)))
+    assert prod < 1e-12 * scale

@@ -15,7 +15,18 @@ from prandtl_b200 import meshio
 from prandtl_b200.mesh import box, periodic_box
 
 CORNERS = meshio._CORNER_BITS
-REF_CASES = os.path.join(os.environ.get("PRANDTL_REFERENCE", "/root/reference"), "TestCases")
+
+
+def _reference_tree():
+    """The reference tree: PRANDTL_REFERENCE, else where oracle/build_ref.sh
+    found it (it records that in oracle/_ref/REFERENCE_TREE); '' when unknown."""
+    if os.environ.get("PRANDTL_REFERENCE"):
+        return os.environ["PRANDTL_REFERENCE"]
+    rec = os.path.join(os.path.dirname(__file__), "..", "oracle", "_ref", "REFERENCE_TREE")
+    return open(rec).read().strip() if os.path.exists(rec) else ""
+
+
+REF_CASES = os.path.join(_reference_tree(), "TestCases")
 
 
 def grid_points(mesh):

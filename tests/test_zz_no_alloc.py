@@ -70,23 +70,39 @@ def test_noalloc_matches_pdg_rhs(name, make, order, params, cuda_device):
     op.close()
 
 
-def test_noalloc_rejects_oversized_mesh():
-    """A mesh beyond the fixed scratch returns PDG_ERR_CAPACITY before any
-    device work (the buffers are never touched)."""
+@pytest.mark.gpu
+def test_noalloc_rejects_oversized_mesh(cuda_device):
+    """A mesh beyond the fixed scratch returns PDG_ERR_CAPACITY.  The state
+    and output are real device buffers of the mesh's size, so the call is
+    safe whatever order its checks run in."""
+    import torch
     mesh = periodic_box(3, 3, (18, 18, 18), 0.0, 1.0)  # 5832 elements of NS scratch
     m, nbr = _abi_mesh(mesh)
     p = pb.default_params(parabolic=1, mu=0.01)
-    rc = pb.library().pdg_rhs_noalloc(C.byref(m), C.byref(p), C.c_void_p(16), C.c_void_p(32), None)
+    u = torch.from_numpy(cases.taylor_green(periodic_box(3, 3, (18, 18, 18), 0.0, 2 * np.pi))).to(cuda_device)
+    out = torch.zeros_like(u)
+    rc = pb.library().pdg_rhs_noalloc(C.byref(m), C.byref(p), C.c_void_p(u.data_ptr()), C.c_void_p(out.data_ptr()),
+                                      None)
+    torch.cuda.synchronize()
     assert rc == 7
+    assert not out.any()  # nothing was written
     del nbr
 
 
-def test_noalloc_rejects_bad_arguments():
+@pytest.mark.gpu
+def test_noalloc_rejects_bad_arguments(cuda_device):
+    import torch
     mesh = periodic_box(2, 3, (4, 4), 0.0, 1.0)
     m, nbr = _abi_mesh(mesh)
     p = pb.default_params()
     L = pb.library()
-    assert L.pdg_rhs_noalloc(None, C.byref(p), C.c_void_p(16), C.c_void_p(32), None) == 1
-    assert L.pdg_rhs_noalloc(C.byref(m), C.byref(p), C.c_void_p(16), C.c_void_p(16), None) == 1
-    nbr[0] = 99
-    assert L.pdg_rhs_noalloc(C.byref(m), C.byref(p), C.c_void_p(16), C.c_void_p(32), None) == 1
+    u = torch.from_numpy(cases.kelvin_helmholtz(mesh)).to(cuda_device)
+    out = torch.zeros_like(u)
+    pu, po = C.c_void_p(u.data_ptr()), C.c_void_p(out.data_ptr())
+    assert L.pdg_rhs_noalloc(None, C.byref(p), pu, po, None) == 1
+    assert L.pdg_rhs_noalloc(C.byref(m), C.byref(p), pu, pu, None) == 1   # aliased
+    assert L.pdg_rhs_noalloc(C.byref(m), C.byref(p), pu, None, None) == 1  # no output
+    nbr[0] = 99  # a neighbour outside the mesh
+    assert L.pdg_rhs_noalloc(C.byref(m), C.byref(p), pu, po, None) == 1
+    torch.cuda.synchronize()
+    assert not out.any()
