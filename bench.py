@@ -34,9 +34,11 @@ from prandtl_b200.mesh import periodic_box  # noqa: E402
 METRIC = "DOF-stage updates/s on 1 B200 (plain vs batched+graph); adjoint/forward cost"
 UNIT = "DOF-stage updates/s"
 # kernels a Navier-Stokes stage may launch, with their PDG_KERNEL_* kinds: the
-# fixed operator runs lift_face, lift, rhs with faces; the reference-value
-# operator (or PDG_ELEMENT_FACES=0) lift_face, rhs, lift, three face passes
-KERNELS = [("lift_face_kernel", (3,)), ("lift_kernel", (1,)), ("rhs_kernel<NS,faces>", (21,)),
+# fixed operator runs lift_face (jumps and face fluxes), lift, rhs with faces
+# from the face buffer; the reference-value operator (or PDG_ELEMENT_FACES=0)
+# lift_face, rhs, lift, three face passes
+KERNELS = [("lift_face_kernel<jumps,fluxes>", (32,)), ("lift_face_kernel", (3,)), ("lift_kernel", (1,)),
+           ("rhs_kernel<NS,faces,buffer>", (30,)), ("rhs_kernel<NS,faces>", (21,)),
            ("rhs_kernel<NS>", (2,)), ("face_kernel<NS>", (7, 8, 9))]
 
 

@@ -49,12 +49,16 @@ def _ptr(a: np.ndarray):
 
 
 _lib = None
+_lib_fma = None
 
 
-def lib():
-    global _lib
-    if _lib is None:
-        path = os.path.join(HERE, "liboracle.so")
+def lib(fma: bool = False):
+    """The oracle library; fma=True: the same source compiled with fused
+    multiply-adds (liboracle_fma.so), whose spread from the plain build is
+    the rounding floor of a state."""
+    global _lib, _lib_fma
+    if (_lib_fma if fma else _lib) is None:
+        path = os.path.join(HERE, "liboracle_fma.so" if fma else "liboracle.so")
         if not os.path.exists(path):
             raise RuntimeError(f"{path} missing: run oracle/build_oracle.sh")
         L = C.CDLL(path)
@@ -84,18 +88,22 @@ def lib():
         L.orc_entgrad2primgrad.argtypes = [C.c_int, C.c_double, C.c_int, _dp, _dp]
         L.orc_num_threads.restype = C.c_int
         L.orc_set_num_threads.argtypes = [C.c_int]
-        _lib = L
-    return _lib
+        if fma:
+            _lib_fma = L
+        else:
+            _lib = L
+    return _lib_fma if fma else _lib
 
 
 class Oracle:
     """CPU restatement of DGSEMOperator (+ RK3SSPSolver) on one mesh."""
 
-    def __init__(self, mesh, **params):
+    def __init__(self, mesh, fma=False, **params):
         self.mesh = mesh
         self.params = make_params(**params)
         self._m, self._nbr = make_mesh(mesh)
-        self.h = lib().orc_create(C.byref(self._m), C.byref(self.params))
+        self._L = lib(fma)
+        self.h = self._L.orc_create(C.byref(self._m), C.byref(self.params))
         if not self.h:
             raise ValueError("orc_create rejected the mesh/params")
         for b, (typ, state) in (getattr(mesh, "boundaries", None) or {}).items():
@@ -103,12 +111,12 @@ class Oracle:
 
     def set_boundary(self, index: int, typ: int, state=None):
         st = None if state is None else np.ascontiguousarray(state, dtype=np.float64)
-        lib().orc_set_boundary(self.h, int(index), int(typ), None if st is None else _ptr(st))
+        self._L.orc_set_boundary(self.h, int(index), int(typ), None if st is None else _ptr(st))
 
     def __del__(self):
         try:
-            if getattr(self, "h", None) and _lib is not None:
-                _lib.orc_destroy(self.h)
+            if getattr(self, "h", None) and getattr(self, "_L", None) is not None:
+                self._L.orc_destroy(self.h)
                 self.h = None
         except Exception:
             pass  # interpreter shutdown
@@ -116,37 +124,37 @@ class Oracle:
     def rhs(self, u: np.ndarray) -> np.ndarray:
         u = np.ascontiguousarray(u, dtype=np.float64)
         out = np.empty_like(u)
-        lib().orc_rhs(self.h, _ptr(u), _ptr(out))
+        self._L.orc_rhs(self.h, _ptr(u), _ptr(out))
         return out
 
     def rk_stage(self, stage, dt, un, us):
         un = np.ascontiguousarray(un, dtype=np.float64)
         us = np.ascontiguousarray(us, dtype=np.float64)
         out = np.empty_like(un)
-        lib().orc_rk_stage(self.h, stage, dt, _ptr(un), _ptr(us), _ptr(out))
+        self._L.orc_rk_stage(self.h, stage, dt, _ptr(un), _ptr(us), _ptr(out))
         return out
 
     def rk3_step(self, u: np.ndarray, dt: float) -> np.ndarray:
         x = np.array(u, dtype=np.float64, copy=True)
-        lib().orc_rk3_step(self.h, dt, _ptr(x))
+        self._L.orc_rk3_step(self.h, dt, _ptr(x))
         return x
 
     def max_char_speed(self) -> float:
-        return lib().orc_max_char_speed(self.h)
+        return self._L.orc_max_char_speed(self.h)
 
     def blending(self):
         ne = self.mesh.num_elements
         eta, alpha = np.empty(ne), np.empty(ne)
-        lib().orc_get_blending(self.h, _ptr(eta), _ptr(alpha))
+        self._L.orc_get_blending(self.h, _ptr(eta), _ptr(alpha))
         return eta, alpha
 
     def gradients(self):
         g = np.empty(self.mesh.dim * self.mesh.size)
-        lib().orc_get_gradients(self.h, _ptr(g))
+        self._L.orc_get_gradients(self.h, _ptr(g))
         return g
 
     def filtered_elements(self) -> int:
-        return lib().orc_filtered_elements(self.h)
+        return self._L.orc_filtered_elements(self.h)
 
 
 _ref_libs = {}

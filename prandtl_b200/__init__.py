@@ -41,6 +41,7 @@ KERNEL_ADJ_FACE_NS = (17, 18, 19)
 KERNEL_EULER_FACES, KERNEL_NS_FACES, KERNEL_BOUNDARY, KERNEL_ADJ_BOUNDARY, KERNEL_EULER_FACES_BDR = 20, 21, 22, 23, 24
 KERNEL_LIFT_FACE_BDR, KERNEL_LIFT_BDR, KERNEL_NS_FACES_BDR, KERNEL_BOUNDARY_NS = 25, 26, 27, 28
 KERNEL_LIFT_BDR_PTTT = 29
+KERNEL_NS_FACES_FB, KERNEL_EULER_FACES_FB, KERNEL_LIFT_FACE_FLUX, KERNEL_FACE_FLUX = 30, 31, 32, 33
 # boundary condition types (pdg_set_boundary)
 BC_SUPERSONIC_INFLOW, BC_SUPERSONIC_OUTFLOW, BC_SPECIFIED_STATE, BC_SLIP_WALL, BC_SYMMETRY = 1, 2, 3, 4, 5
 BC_SUBSONIC_OUTFLOW_P, BC_SUBSONIC_INFLOW_RV, BC_SUBSONIC_INFLOW_PTTT, BC_RIEMANN_INVARIANT = 6, 7, 8, 9

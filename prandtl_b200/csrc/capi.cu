@@ -41,6 +41,7 @@ struct pdg_ctx {
     double *lbuf = nullptr;                         // BR1 lifting jumps [d][e][fn][v]
     double *fcol = nullptr;                         // viscous normal columns at faces
     double *vbuf = nullptr;                         // viscous volume term [v-1][node] (element-side faces)
+    double *fbuf = nullptr;                         // inviscid face fluxes [d][e][v][fn] (element-side faces)
     // boundary conditions: host table, its device copy, which entries the
     // mesh uses and which pdg_set_boundary has set
     double bc_host[PDG_MAX_BOUNDARIES * BC_SLOT] = {};
@@ -72,6 +73,10 @@ struct pdg_ctx {
     // fixed operator: face terms inside the volume kernel, each face evaluated
     // by both of its elements (PDG_ELEMENT_FACES=0: separate face kernels)
     bool element_faces = true;
+    // periodic fixed operator: every face's inviscid flux evaluated once into
+    // fbuf by the face-node kernel, read by both elements' volume kernels
+    // (PDG_FACE_BUFFER=0: each element evaluates its faces itself)
+    bool face_buffer = true;
     bool profile = false;
     struct TimedLaunch { int kind; cudaEvent_t a, b; };
     std::vector<TimedLaunch> timed;
@@ -269,7 +274,8 @@ int kernel_config(int dim, int N, int kind, int64_t ne, int device, LaunchCfg *c
     if (ki.el_doubles == 0) {  // thread-per-face-node kernel
         const int64_t threads = kind == KIND_FILTER_BOUNDS ? 32 * ne
                                 : (kind == KIND_BOUNDARY || kind == KIND_ADJ_BOUNDARY || kind == KIND_BOUNDARY_NS) ? ne
-                                : ((kind == KIND_LIFT_FACE || kind == KIND_LIFT_FACE_BDR) ? (int64_t)dim : 1) * ne * nfn;
+                                : ((kind == KIND_LIFT_FACE || kind == KIND_LIFT_FACE_BDR || kind == KIND_LIFT_FACE_FLUX ||
+                                    kind == KIND_FACE_FLUX) ? (int64_t)dim : 1) * ne * nfn;
         // 256-thread blocks; 128 when that gives fewer than four blocks per
         // SM, so that a small mesh still spreads evenly over the SMs
         cfg->wpb = threads < 4LL * 256 * sms ? 4 : 8;
@@ -314,6 +320,7 @@ bool kind_used(int kind, int dim, bool parabolic, bool filter)
         return false;  // configured by the first pdg_rhs_vjp
     const bool ns_kind = kind == KIND_NS || kind == KIND_NS_FACES || kind == KIND_LIFT || kind == KIND_LIFT_FACE ||
                          (kind >= KIND_FACE_NS0 && kind <= KIND_FACE_NS2) || kind == KIND_LIFT_FACE_BDR ||
+                         kind == KIND_NS_FACES_FB || kind == KIND_LIFT_FACE_FLUX ||
                          kind == KIND_LIFT_BDR || kind == KIND_NS_FACES_BDR || kind == KIND_BOUNDARY_NS ||
                          kind == KIND_LIFT_BDR_PTTT;
     if (ns_kind != parabolic) return false;
@@ -386,6 +393,7 @@ KParams base_params(pdg_ctx *c)
     P.bc = c->bc;
     P.has_bdr = c->bc_used != 0;
     P.lbuf_lo = c->lbuf_lo;
+    P.fbuf = c->fbuf;
     return P;
 }
 
@@ -526,10 +534,11 @@ int evaluate(pdg_ctx *c, int stage, double dt, const double *un, const double *u
                 if ((r = launch(c, KIND_BOUNDARY_NS, P, s))) return r;
             }
         } else if (element_faces) {
-            if ((r = launch(c, KIND_LIFT_FACE, P, s))) return r;
+            const bool fb = c->fbuf != nullptr;
+            if ((r = launch(c, fb ? KIND_LIFT_FACE_FLUX : KIND_LIFT_FACE, P, s))) return r;
             P.vbuf = c->vbuf;
             if ((r = launch(c, KIND_LIFT, P, s))) return r;
-            if ((r = launch(c, KIND_NS_FACES, P, s))) return r;
+            if ((r = launch(c, fb ? KIND_NS_FACES_FB : KIND_NS_FACES, P, s))) return r;
         } else {
             if ((r = launch(c, KIND_LIFT_FACE, P, s))) return r;
             if ((r = launch(c, KIND_NS, P, s))) return r;
@@ -539,7 +548,10 @@ int evaluate(pdg_ctx *c, int stage, double dt, const double *un, const double *u
         }
     } else {
         if (c->p.filter && stage >= 0 && (r = launch(c, KIND_FILTER_BOUNDS, P, s))) return r;
-        if (element_faces) {
+        if (element_faces && c->fbuf) {
+            if ((r = launch(c, KIND_FACE_FLUX, P, s))) return r;
+            if ((r = launch(c, KIND_EULER_FACES_FB, P, s))) return r;
+        } else if (element_faces) {
             if ((r = launch(c, c->bc_used ? KIND_EULER_FACES_BDR : KIND_EULER_FACES, P, s))) return r;
         } else {
             if ((r = launch(c, KIND_EULER, P, s))) return r;
@@ -611,6 +623,7 @@ int pdg_create(const pdg_mesh *mesh, const pdg_params *params, pdg_ctx **out)
     if (cudaGetDevice(&c->device) != cudaSuccess) return cleanup(PDG_ERR_CUDA);
     if (const char *pf = std::getenv("PDG_PREFETCH")) c->prefetch = std::atoi(pf) != 0;
     if (const char *ef = std::getenv("PDG_ELEMENT_FACES")) c->element_faces = std::atoi(ef) != 0;
+    if (const char *fb = std::getenv("PDG_FACE_BUFFER")) c->face_buffer = std::atoi(fb) != 0;
     build_constants(c);
     const size_t fbytes = sizeof(double) * (size_t)c->size;
     if (cudaMalloc(&c->K, sizeof(DevConst)) != cudaSuccess || cudaMalloc(&c->nbr, sizeof(int32_t) * c->ne * 2 * c->dim) ||
@@ -624,6 +637,11 @@ int pdg_create(const pdg_mesh *mesh, const pdg_params *params, pdg_ctx **out)
         if (cudaMalloc(&c->ent_own, sizeof(double) * c->ne) != cudaSuccess ||
             cudaMalloc(&c->filter_count, sizeof(unsigned long long)) != cudaSuccess ||
             cudaMemset(c->filter_count, 0, sizeof(unsigned long long)) != cudaSuccess)
+            return cleanup(PDG_ERR_NOMEM);
+    }
+    if (c->element_faces && c->face_buffer && !c->p.compat && !c->bc_used) {
+        const size_t nfn = c->dim == 2 ? c->Np : c->Np * c->Np;
+        if (cudaMalloc(&c->fbuf, sizeof(double) * c->dim * c->ne * nfn * c->nv) != cudaSuccess)
             return cleanup(PDG_ERR_NOMEM);
     }
     if (c->p.parabolic) {
@@ -713,6 +731,7 @@ int pdg_destroy(pdg_ctx *c)
     cudaFree(c->lbuf);
     cudaFree(c->fcol);
     cudaFree(c->vbuf);
+    cudaFree(c->fbuf);
     cudaFree(c->bc);
     cudaFree(c->lbuf_lo);
     cudaFree(c->stage_a);

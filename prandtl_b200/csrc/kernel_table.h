@@ -34,7 +34,11 @@ enum KernelKind {
     KIND_NS_FACES_BDR = 27,     // rhs_kernel<dim, N, true, true, true>
     KIND_BOUNDARY_NS = 28,      // boundary_kernel<dim, N, true>: NS boundary faces of the separate-face path
     KIND_LIFT_BDR_PTTT = 29,    // lift_kernel<2, N, true, true>: a mesh with a total-pressure inflow (2D)
-    KIND_COUNT = 30
+    KIND_NS_FACES_FB = 30,      // rhs_kernel<dim, N, true, true, false, true>: KIND_NS_FACES reading the face-flux buffer
+    KIND_EULER_FACES_FB = 31,   // rhs_kernel<dim, N, false, true, false, true>: KIND_EULER_FACES reading it
+    KIND_LIFT_FACE_FLUX = 32,   // lift_face_kernel<dim, N, false, FACE_JUMP | FACE_FLUX>: jumps + face fluxes (NS)
+    KIND_FACE_FLUX = 33,        // lift_face_kernel<dim, N, false, FACE_FLUX>: face fluxes (Euler)
+    KIND_COUNT = 34
 };
 
 struct KernelInfo {

@@ -30,6 +30,16 @@ template <int N> static bool info_n(int kind, KernelInfo *out)
     case KIND_LIFT_BDR: out->fn = (const void *)&lift_kernel<3, N, true>; out->el_doubles = S::EL_LIFTF; break;
     case KIND_LIFT: out->fn = (const void *)&lift_kernel<3, N>; out->el_doubles = S::EL_LIFTF; break;
     case KIND_LIFT_FACE: out->fn = (const void *)&lift_face_kernel<3, N>; break;
+    case KIND_LIFT_FACE_FLUX: out->fn = (const void *)&lift_face_kernel<3, N, false, FACE_JUMP | FACE_FLUX>; break;
+    case KIND_FACE_FLUX: out->fn = (const void *)&lift_face_kernel<3, N, false, FACE_FLUX>; break;
+    case KIND_NS_FACES_FB:
+        out->fn = (const void *)&rhs_kernel<3, N, true, true, false, true>;
+        out->el_doubles = S::EL_RHS_FB;
+        break;
+    case KIND_EULER_FACES_FB:
+        out->fn = (const void *)&rhs_kernel<3, N, false, true, false, true>;
+        out->el_doubles = S::EL_RHS_FB;
+        break;
     case KIND_FACE_E0: out->fn = (const void *)&face_kernel<3, N, 0, false>; break;
     case KIND_FACE_E1: out->fn = (const void *)&face_kernel<3, N, 1, false>; break;
     case KIND_FACE_E2: out->fn = (const void *)&face_kernel<3, N, 2, false>; break;

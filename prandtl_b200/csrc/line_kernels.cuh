@@ -87,6 +87,10 @@ struct KParams {
     const double *bc;     // boundary conditions, BC_SLOT doubles each (type, state)
     double *lbuf_lo;      // NS boundary faces: BR1 jumps of -d boundary faces [d][e][face node][v]
     int has_bdr;          // the neighbour table holds boundary faces (negative entries)
+    // inviscid face flux of every interior face, evaluated once per face
+    // node: [d][e][v][face node] for the face between e's +d face and its
+    // +d neighbour, signed as element e receives it (see face_flux_oriented)
+    double *fbuf;
 };
 
 // Boundary conditions (src/Integrators/BoundaryConditions/): a neighbour
@@ -116,6 +120,8 @@ template <int DIM, int N> struct Shape {
     // z-fill buffer
     static constexpr int ZFILL = NFN * N * NV;
     static constexpr int EL_RHS = NPRIM * NS_ + NV * NS_ + ZFILL;
+    // the fixed operator's volume kernel reading the face buffer: no z-fill
+    static constexpr int EL_RHS_FB = NPRIM * NS_ + NV * NS_;
     // adjoint lift slot: entropy variables, gradients along each direction
     static constexpr int EL_LIFT = NV * NS_ + DIM * NV * NS_;
     // forward lift slot: entropy variables (later the viscous RHS) and the
@@ -541,15 +547,46 @@ __device__ __forceinline__ double face_terms_from(const KParams &P, const double
 // boundary faces): a slot whose neighbour entry is negative takes the
 // boundary condition's inviscid flux (boundary_node_terms) and, NS, its
 // viscous boundary flux, both for this element alone.
-template <int DIM, int N, bool NS, int D, bool BDR>
+// FB: the inviscid fluxes come from P.fbuf (evaluated once per face by the
+// face-flux kernel) instead of being evaluated here.
+template <int DIM, int N, bool NS, int D, bool BDR, bool FB = false>
 __device__ __forceinline__ void face_terms_dir(const KParams &P, const double *c, double *acc, int64_t e,
                                                const int32_t *enb, int gl, bool valid, double coef, double &lam)
 {
     using S = Shape<DIM, N>;
     constexpr int Np = S::Np, NV = S::NV, NFN = S::NFN, L = S::L, ST = S::NS_;
     constexpr int R = (2 * NFN + L - 1) / L;
+    if (valid && FB) {
+        double Fa[R][NV];
+#pragma unroll
+        for (int r = 0; r < R; r++) {
+            const int t = gl + r * L;
+            if (t < 2 * NFN) {
+                const int side = t >= NFN, fn = side ? t - NFN : t;
+                const int64_t a = side ? e : (int64_t)enb[2 * D];
+                const double *src = P.fbuf + ((D * P.ne + a) * NV) * NFN + fn;
+#pragma unroll
+                for (int v = 0; v < NV; v++) Fa[r][v] = __ldg(src + v * NFN);
+            }
+        }
+        const double sc = C_FACE(c) * coef;
+#pragma unroll
+        for (int r = 0; r < R; r++) {
+            const int t = gl + r * L;
+            if (t < 2 * NFN) {
+                const int side = t >= NFN, fn = side ? t - NFN : t;
+                const int n = sp<DIM, Np>(line_node<DIM, Np, D>(fn, side ? N : 0));
+#pragma unroll
+                for (int v = 0; v < NV; v++) {
+                    const double C = sc * Fa[r][v];
+                    if (side) acc[v * ST + n] += C;
+                    else acc[v * ST + n] -= C;
+                }
+            }
+        }
+    }
     if (valid) {
-        {
+        if (!FB) {
             FaceIn<DIM, false> in[R];
 #pragma unroll
             for (int r = 0; r < R; r++) {
@@ -668,7 +705,7 @@ __device__ __forceinline__ void face_terms_dir(const KParams &P, const double *c
 // face terms include the central viscous flux of both sides' face columns.
 // Each face is thus evaluated twice, once by each of its elements, on the
 // same inputs in the same order, so both get the same value.
-template <int DIM, int N, bool NS, bool FACES, bool PRELOAD = true, bool BDR = false>
+template <int DIM, int N, bool NS, bool FACES, bool PRELOAD = true, bool BDR = false, bool FB = false>
 __device__ __forceinline__ void rhs_tile(const KParams &P, const double *c, double *pr, int64_t e_base, int grp,
                                          int gl, bool lane_used, unsigned int &flags, double &lam)
 {
@@ -701,7 +738,9 @@ __device__ __forceinline__ void rhs_tile(const KParams &P, const double *c, doub
     }
     const double sc = -(1.0 - alpha) * C_INVJ(c);
     if (lane_used) {
-        const bool zfill = DIM == 3 && NS && compat;
+        // (the face-buffer variant's slot has no z-fill buffer; the host runs
+        // it for the fixed operator only)
+        const bool zfill = DIM == 3 && NS && compat && !FB;
 #pragma unroll 1
         for (int d = 0; d < DIM; d++)
             ec_lines_rt<DIM, N>(P, d, pr, acc, zf, c, gl, sc, zfill && d == 1, zfill && d == 2);
@@ -758,9 +797,9 @@ __device__ __forceinline__ void rhs_tile(const KParams &P, const double *c, doub
     }
     __syncwarp();
     if (PRELOAD) {
-        face_terms_dir<DIM, N, NS, 0, BDR>(P, c, acc, e, enb, gl, valid, coef, lam);
-        face_terms_dir<DIM, N, NS, 1, BDR>(P, c, acc, e, enb, gl, valid, coef, lam);
-        if (DIM == 3) face_terms_dir<DIM, N, NS, (DIM == 3 ? 2 : 0), BDR>(P, c, acc, e, enb, gl, valid, coef, lam);
+        face_terms_dir<DIM, N, NS, 0, BDR, FB>(P, c, acc, e, enb, gl, valid, coef, lam);
+        face_terms_dir<DIM, N, NS, 1, BDR, FB>(P, c, acc, e, enb, gl, valid, coef, lam);
+        if (DIM == 3) face_terms_dir<DIM, N, NS, (DIM == 3 ? 2 : 0), BDR, FB>(P, c, acc, e, enb, gl, valid, coef, lam);
     } else {
         // one face node at a time (Euler): the batched sweep's register
         // variants are tuned for this form
@@ -805,13 +844,23 @@ __device__ __forceinline__ void rhs_tile(const KParams &P, const double *c, doub
 // optional SSP-RK3 stage).
 // Resident blocks the register budget must allow: 4 for 3D N = 3 (whose
 // swizzled slots let four 4-warp blocks share an SM), 1 otherwise.
+#ifndef PDG_RHS3_MIN_BLOCKS
+#define PDG_RHS3_MIN_BLOCKS 4
+#endif
+#ifndef PDG_LIFT3_MIN_BLOCKS
+#define PDG_LIFT3_MIN_BLOCKS 1
+#endif
 template <int DIM, int N> struct RhsOccupancy {
-    static constexpr int min_blocks = (DIM == 3 && N == 3) ? 4 : 1;
+    static constexpr int min_blocks = (DIM == 3 && N == 3) ? PDG_RHS3_MIN_BLOCKS : 1;
+};
+template <int DIM, int N> struct LiftOccupancy {
+    static constexpr int min_blocks = (DIM == 3 && N == 3) ? PDG_LIFT3_MIN_BLOCKS : 1;
 };
 
 // BDR: a variant for meshes with boundary faces (Euler), whose boundary
-// branch would otherwise cost registers in every face loop.
-template <int DIM, int N, bool NS, bool FACES = false, bool BDR = false>
+// branch would otherwise cost registers in every face loop.  FB: the
+// inviscid face fluxes come from P.fbuf (periodic meshes, FACES only).
+template <int DIM, int N, bool NS, bool FACES = false, bool BDR = false, bool FB = false>
 __global__ void __launch_bounds__(128, RhsOccupancy<DIM, N>::min_blocks) rhs_kernel(const KParams P)
 {
     using S = Shape<DIM, N>;
@@ -824,12 +873,13 @@ __global__ void __launch_bounds__(128, RhsOccupancy<DIM, N>::min_blocks) rhs_ker
     const int grp = lane / L, gl = lane % L;
     const int wpb = blockDim.x >> 5;
     const bool lane_used = grp < EPW;
-    double *pr = smem + const_slots(Np) + (size_t)(warp * EPW + (lane_used ? grp : 0)) * S::EL_RHS;
+    constexpr int EL = FB ? S::EL_RHS_FB : S::EL_RHS;
+    double *pr = smem + const_slots(Np) + (size_t)(warp * EPW + (lane_used ? grp : 0)) * EL;
     const int64_t wstride = (int64_t)gridDim.x * wpb;
     unsigned int flags = 0;
     double lam = 0.0;
     for (int64_t wt = (int64_t)blockIdx.x * wpb + warp; wt < P.nwt; wt += wstride)
-        rhs_tile<DIM, N, NS, FACES, true, BDR>(P, c, pr, wt * EPW, grp, gl, lane_used, flags, lam);
+        rhs_tile<DIM, N, NS, FACES, true, BDR, FB>(P, c, pr, wt * EPW, grp, gl, lane_used, flags, lam);
     lam = group_max<32>(lam);
     if (lane == 0) atomic_max_pos(P.lam_bits, lam);
     flags = __reduce_or_sync(0xffffffffu, flags);
@@ -897,17 +947,22 @@ __device__ __forceinline__ void load_face_in(const KParams &P, int64_t a, int64_
     }
 }
 
-template <int DIM, int N, int D, bool NS>
-__device__ __forceinline__ double face_terms_from(const KParams &P, const double *c, bool a_is_1,
-                                                  const FaceIn<DIM, NS> &in, double coef, double *C)
+// Inviscid flux of one face node between element a's +D trace sa and its
+// +D neighbour b's -D trace sb, signed as element a receives it: Fa = -F for
+// a = element 1 (the lower index, normal out of it), +F otherwise, F being
+// the Chandrashekar + LLF flux with the element-1 normal.  NSC: the
+// reference-value Navier-Stokes face states, whose momentum slots hold
+// velocities (returns their wave speed; 0 otherwise).
+template <int DIM, int N, int D, bool NSC>
+__device__ __forceinline__ double face_flux_oriented(const KParams &P, const double *c, bool a_is_1, const double *sa,
+                                                     const double *sb, double *Fa)
 {
     constexpr int NV = DIM + 2, Np = N + 1;  // Np: constant layout
-    const double *sa = in.sa, *sb = in.sb;
     Prim<DIM> qa = make_prim<DIM>(sa, P.gamma, P.gm1), qb = make_prim<DIM>(sb, P.gamma, P.gm1);
     double ma[DIM], mb[DIM];
     double lam = 0.0;
     const bool compat = P.compat != 0;
-    if (NS && compat) {
+    if (NSC && compat) {
         qa = velocity_slot_prim<DIM>(qa, sa[DIM + 1], P.gamma, P.gm1, ma);
         qb = velocity_slot_prim<DIM>(qb, sb[DIM + 1], P.gamma, P.gm1, mb);
         lam = fmax(qa.lam, qb.lam);
@@ -922,17 +977,41 @@ __device__ __forceinline__ double face_terms_from(const KParams &P, const double
     double F[NV];
     if (a_is_1) face_flux<DIM, D>(qa, qb, ma, mb, nrm, P.gm1inv, compat, P.diss_scale, F);
     else face_flux<DIM, D>(qb, qa, mb, ma, nrm, P.gm1inv, compat, P.diss_scale, F);
+#pragma unroll
+    for (int v = 0; v < NV; v++) Fa[v] = a_is_1 ? -F[v] : F[v];
+    return lam;
+}
+
+// Element a's face terms C (element b receives -C) from the signed inviscid
+// flux Fa and, NS, both sides' normal viscous columns: C = C_FACE coef
+// (Fa +/- (fa + fb)/2 n).
+template <int DIM, int N, int D, bool NS>
+__device__ __forceinline__ void face_terms_signed(const double *c, bool a_is_1, const double *Fa, const double *fa,
+                                                  const double *fb, double coef, double *C)
+{
+    constexpr int Np = N + 1;  // Np: constant layout
+    const double nrm = a_is_1 ? C_AREA(c)[D] : -C_AREA(c)[D];
     const double sc = C_FACE(c) * coef;
-    C[0] = sc * (a_is_1 ? -F[0] : F[0]);
+    C[0] = sc * Fa[0];
 #pragma unroll
     for (int i = 0; i <= DIM; i++) {
-        double du = a_is_1 ? -F[1 + i] : F[1 + i];
+        double du = Fa[1 + i];
         if (NS) {
-            const double fvn = ((in.fa[i] + in.fb[i]) * 0.5) * nrm;
+            const double fvn = ((fa[i] + fb[i]) * 0.5) * nrm;
             du = a_is_1 ? du + fvn : du - fvn;
         }
         C[1 + i] = sc * du;
     }
+}
+
+template <int DIM, int N, int D, bool NS>
+__device__ __forceinline__ double face_terms_from(const KParams &P, const double *c, bool a_is_1,
+                                                  const FaceIn<DIM, NS> &in, double coef, double *C)
+{
+    constexpr int NV = DIM + 2;
+    double Fa[NV];
+    const double lam = face_flux_oriented<DIM, N, D, NS>(P, c, a_is_1, in.sa, in.sb, Fa);
+    face_terms_signed<DIM, N, D, NS>(c, a_is_1, Fa, in.fa, in.fb, coef, C);
     return lam;
 }
 
@@ -1264,9 +1343,16 @@ __global__ void __launch_bounds__(256) boundary_kernel(const KParams P)
     if ((threadIdx.x & 31) == 0) atomic_max_pos(P.lam_bits, lam);
 }
 
+// Face-node kernel modes: the BR1 jump (lift_face_node) and/or the signed
+// inviscid face flux to P.fbuf (the fixed operator's element-side faces then
+// read it instead of evaluating each face from both sides).
+constexpr int FACE_JUMP = 1, FACE_FLUX = 2;
+
 // BR1 lifting face node: 0.5 (w2 - w1) n1_D / (w0 J), the same value for both
 // sides (LiftingBR1.cpp:10-115).  Written to P.lbuf for the -D-side element a.
-template <int DIM, int N, int D>
+// MODE & FACE_FLUX: also the inviscid flux of the face node, signed for a
+// (face_flux_oriented), to P.fbuf[D][a][v][fn].
+template <int DIM, int N, int D, int MODE = FACE_JUMP>
 __device__ __forceinline__ void lift_face_node(const KParams &P, const double *c, int64_t a, int fn)
 {
     using S = Shape<DIM, N>;
@@ -1274,22 +1360,32 @@ __device__ __forceinline__ void lift_face_node(const KParams &P, const double *c
     const int64_t nn = P.nnodes;
     const int64_t b = __ldg(P.nbr + a * 2 * DIM + 2 * D + 1);
     const int na = line_node<DIM, Np, D>(fn, N), nb = line_node<DIM, Np, D>(fn, 0);
-    double sa[NV], sb[NV], wa[NV], wb[NV];
+    double sa[NV], sb[NV];
 #pragma unroll
     for (int v = 0; v < NV; v++) {
         sa[v] = __ldg(P.u + v * nn + a * NDOF + na);
         sb[v] = __ldg(P.u + v * nn + b * NDOF + nb);
     }
-    entropy_vars<DIM>(sa, P.gamma, P.gm1, P.gm1inv, wa);
-    entropy_vars<DIM>(sb, P.gamma, P.gm1, P.gm1inv, wb);
     const bool a_is_1 = a <= b;
-    const double nrm = a_is_1 ? C_AREA(c)[D] : -C_AREA(c)[D];
-    const double sc = C_FACE(c);
-    double *dst = P.lbuf + ((D * P.ne + a) * NFN + fn) * NV;
+    if (MODE & FACE_JUMP) {
+        double wa[NV], wb[NV];
+        entropy_vars<DIM>(sa, P.gamma, P.gm1, P.gm1inv, wa);
+        entropy_vars<DIM>(sb, P.gamma, P.gm1, P.gm1inv, wb);
+        const double nrm = a_is_1 ? C_AREA(c)[D] : -C_AREA(c)[D];
+        const double sc = C_FACE(c);
+        double *dst = P.lbuf + ((D * P.ne + a) * NFN + fn) * NV;
 #pragma unroll
-    for (int v = 0; v < NV; v++) {
-        const double w1 = a_is_1 ? wa[v] : wb[v], w2 = a_is_1 ? wb[v] : wa[v];
-        dst[v] = sc * ((0.5 * (w2 - w1)) * nrm);
+        for (int v = 0; v < NV; v++) {
+            const double w1 = a_is_1 ? wa[v] : wb[v], w2 = a_is_1 ? wb[v] : wa[v];
+            dst[v] = sc * ((0.5 * (w2 - w1)) * nrm);
+        }
+    }
+    if (MODE & FACE_FLUX) {
+        double Fa[NV];
+        face_flux_oriented<DIM, N, D, false>(P, c, a_is_1, sa, sb, Fa);
+        double *dst = P.fbuf + ((D * P.ne + a) * NV) * NFN + fn;
+#pragma unroll
+        for (int v = 0; v < NV; v++) dst[v * NFN] = Fa[v];
     }
 }
 
@@ -1379,8 +1475,9 @@ __device__ __noinline__ void lift_boundary_node(const KParams &P, const double *
 
 // BDR: the mesh has boundary faces (Navier-Stokes): a face towards the
 // boundary takes its jump from lift_boundary_node, the -D boundary faces into
-// P.lbuf_lo.
-template <int DIM, int N, bool BDR = false>
+// P.lbuf_lo.  MODE: FACE_JUMP (the jumps), FACE_FLUX (the inviscid face
+// fluxes, periodic meshes) or both.
+template <int DIM, int N, bool BDR = false, int MODE = FACE_JUMP>
 __global__ void __launch_bounds__(256) lift_face_kernel(const KParams P)
 {
     using S = Shape<DIM, N>;
@@ -1419,9 +1516,9 @@ __global__ void __launch_bounds__(256) lift_face_kernel(const KParams P)
             }
             if (bp < 0) continue;
         }
-        if (d == 0) lift_face_node<DIM, N, 0>(P, c, a, fn);
-        else if (d == 1) lift_face_node<DIM, N, 1>(P, c, a, fn);
-        else lift_face_node<DIM, N, (DIM == 3 ? 2 : 0)>(P, c, a, fn);
+        if (d == 0) lift_face_node<DIM, N, 0, MODE>(P, c, a, fn);
+        else if (d == 1) lift_face_node<DIM, N, 1, MODE>(P, c, a, fn);
+        else lift_face_node<DIM, N, (DIM == 3 ? 2 : 0), MODE>(P, c, a, fn);
     }
 }
 
@@ -1529,7 +1626,7 @@ __device__ __noinline__ void outer_viscous_col(const KParams &P, const double *s
 // separate instantiation, since the out-of-line call gives the kernel a stack
 // frame that slowed the other boundary meshes by ~8 %.
 template <int DIM, int N, bool BDR = false, bool PTTT = false>
-__global__ void __launch_bounds__(128) lift_kernel(const KParams P)
+__global__ void __launch_bounds__(128, LiftOccupancy<DIM, N>::min_blocks) lift_kernel(const KParams P)
 {
     using S = Shape<DIM, N>;
     constexpr int Np = S::Np, NDOF = S::NDOF, NV = S::NV, NFN = S::NFN, L = S::L, EPW = S::EPW, ST = S::NS_;

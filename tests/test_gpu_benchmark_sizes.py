@@ -15,7 +15,15 @@ on the same states:
   stage: the stages of one step and the number of filtered elements;
 * 16 cases of the 256-case vortex sweep through the batched persistent kernel.
 
-Tolerance: 1e-12 relative in max norm per right-hand side and per stage.
+Tolerance: 1e-12 relative in max norm per right-hand side and per stage, or
+twice the state's rounding floor where that is larger.  The floor is the
+spread between two FP64 builds of the oracle that differ only in fused
+multiply-adds (liboracle.so, liboracle_fma.so), measured in the test on the
+same state.  It matters for the fixed operator on the Taylor-Green initial
+state: at Ma = 0.1 (p0 = 71) its right-hand side (max 0.64) is about 5e4
+times smaller than the flux terms it sums, so the two oracle builds differ
+by ~4e-11 relative to it; the reference-value operator's right-hand side on
+the same state is 2e4 times larger (its quirks) and meets 1e-12 outright.
 
 Entropy conservation: with the face dissipation switched off (the pure
 Chandrashekar face flux) and no blending, the flux-differencing operator is
@@ -81,7 +89,10 @@ def test_benchmark_mesh_rhs_and_stage(case, compat, cuda_device):
     op = pb.DGSEMOperator(mesh, **kw)
     orc = oracle.Oracle(mesh, **kw)
     ref = orc.rhs(u)
-    assert rel_maxnorm(_rhs(op, u, cuda_device), ref) < TOL
+    floor = rel_maxnorm(oracle.Oracle(mesh, fma=True, **kw).rhs(u), ref)
+    tol = max(TOL, 2.0 * floor)
+    err = rel_maxnorm(_rhs(op, u, cuda_device), ref)
+    assert err < tol, f"relative error {err:.3e}, rounding floor {floor:.3e}"
     _, a1 = op.blending()
     _, a0 = orc.blending()
     np.testing.assert_allclose(a1, a0, rtol=0, atol=1e-10)
@@ -123,7 +134,7 @@ def test_kelvin_helmholtz_64_filtered_step(rough_state, compat, cuda_device):
 
 
 def test_sweep_sample_batched(cuda_device):
-    """16 cases of the 256-case sweep (seed 3), every fifteenth and the largest."""
+    """16 cases of the 256-case sweep (seed 3): every seventeenth and the largest."""
     import torch
     specs = cases.sweep_cases(256, seed=3)
     pick = sorted(set(list(range(0, 256, 17))[:15] + [int(np.argmax([n * n * (N + 1) ** 2 for n, N, _ in specs]))]))

@@ -178,8 +178,8 @@ def test_graph_replayed_steps_equal_plain_steps(kind, dim, order, par, compat, c
     assert torch.equal(a, b)
     if compat:   # (face jumps,) volume, (lifting,) face passes per stage
         assert per_step == (6 if par else 1 + dim) * 3
-    else:        # (face jumps, lifting,) volume with faces per stage
-        assert per_step == (3 if par else 1) * 3
+    else:        # face fluxes (with the jumps), (lifting,) volume with faces per stage
+        assert per_step == (3 if par else 2) * 3
     op.rk3_step(b, dt, nsteps=2, graph=True)   # replay without capture
     op.rk3_step(a, dt, nsteps=2)
     assert torch.equal(a, b)
@@ -212,3 +212,33 @@ def test_element_side_faces_equal_face_kernels(kind, dim, order, par, cuda_devic
         torch.cuda.synchronize()
         assert rel_maxnorm(a.cpu().numpy(), b.cpu().numpy()) < 1e-14
     assert op.check() == 0 and op_sep.check() == 0
+
+
+@pytest.mark.parametrize("kind,dim,order,par", [("rough2d", 2, 3, 0), ("rough3d", 3, 3, 1), ("rough2dns", 2, 4, 1),
+                                                ("rough3d", 3, 2, 0), ("rough2d", 2, 5, 0), ("rough3d", 3, 4, 1)])
+def test_face_buffer_equals_element_faces(kind, dim, order, par, cuda_device, monkeypatch):
+    """Each face's inviscid flux evaluated once into the face buffer gives,
+    bit for bit, the values of both elements evaluating it themselves
+    (PDG_FACE_BUFFER=0): the same arithmetic on the same inputs."""
+    import torch
+    mesh, u = make_case(kind, dim, order)
+    kw = dict(parabolic=par, mu=0.01 if par else 0.0, Pr=0.71, compat=0)
+    op = pb.DGSEMOperator(mesh, **kw)
+    monkeypatch.setenv("PDG_FACE_BUFFER", "0")
+    op_el = pb.DGSEMOperator(mesh, **kw)
+    monkeypatch.delenv("PDG_FACE_BUFFER")
+    un = dev(u, cuda_device)
+    us = dev(rough(u, mesh, 9, 0.01, 0.001), cuda_device)
+    for stage in (-1, 0, 1, 2):
+        a = torch.empty_like(un)
+        b = torch.empty_like(un)
+        if stage < 0:
+            op.Mult(us, a)
+            op_el.Mult(us, b)
+        else:
+            op.rk_stage(stage, 1e-3, un, us, a)
+            op_el.rk_stage(stage, 1e-3, un, us, b)
+        torch.cuda.synchronize()
+        assert torch.equal(a, b), f"stage {stage}"
+    assert op.GetMaxCharSpeed() == op_el.GetMaxCharSpeed()
+    assert op.check() == 0 and op_el.check() == 0
