@@ -239,8 +239,24 @@ int pdg_gradients(pdg_ctx *ctx, const double *u, double *grads, void *stream);
  * differentiated where its sigmoid is active and is constant where it is
  * snapped or capped.  u, cot, ubar: DEVICE pointers, byNODES; ubar is
  * overwritten and aliases neither input.  The first call allocates the
- * Navier-Stokes adjoint scratch. */
+ * adjoint scratch. */
 int pdg_rhs_vjp(pdg_ctx *ctx, const double *u, const double *cot, double *ubar, void *stream);
+
+/* Adjoint of one SSP-RK3 stage (pdg_rk_stage, the stage bodies of MFEM's
+ * RK3SSPSolver::Step as called at src/Simulation/Simulation.cpp:1010) with the
+ * stage algebra fused into the vector-Jacobian product's last kernel.  For
+ * stage s, out = a_s un + b_s (us + dt L(us)), and the cotangent lam of out,
+ * with g = (dL/dus)^T lam:
+ *   stage 2: out = 2/3 (lam + dt g),  bx = 1/3 lam
+ *   stage 1: out = 1/4 (lam + dt g),  bx = bx + 3/4 lam
+ *   stage 0: bx = bx + lam + dt g     (us = un; out is scratch)
+ * so that a step's adjoint is stages 2, 1, 0 with lam = the previous stage's
+ * out, leaving the cotangent of the step's input in bx.  The reference has
+ * no adjoint.  Fixed operator, meshes without boundary faces
+ * (PDG_ERR_UNSUPPORTED otherwise; use pdg_rhs_vjp).  DEVICE pointers; out and
+ * bx alias no other argument. */
+int pdg_rk_stage_vjp(pdg_ctx *ctx, int stage, double dt, const double *us, const double *lam, double *out,
+                     double *bx, void *stream);
 
 /* Entropy filter (params.filter = 1): EntropyFilter::FilterSolution
  * (src/Filters/EntropyFilter.cpp:171-242) after every RK stage, with the

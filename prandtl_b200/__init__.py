@@ -36,8 +36,8 @@ KERNEL_FACE_EULER = (4, 5, 6)
 KERNEL_FACE_NS = (7, 8, 9)
 KERNEL_FILTER_BOUNDS, KERNEL_FILTER = 10, 11
 KERNEL_ADJ_RHS, KERNEL_ADJ_LIFT = 12, 13
-KERNEL_ADJ_FACE_EULER = (14, 15, 16)
-KERNEL_ADJ_FACE_NS = (17, 18, 19)
+KERNEL_ADJ_FACE_EULER = (14,)   # adj_faces_kernel: every direction in one launch
+KERNEL_ADJ_FACE_NS = (17,)
 KERNEL_EULER_FACES, KERNEL_NS_FACES, KERNEL_BOUNDARY, KERNEL_ADJ_BOUNDARY, KERNEL_EULER_FACES_BDR = 20, 21, 22, 23, 24
 KERNEL_LIFT_FACE_BDR, KERNEL_LIFT_BDR, KERNEL_NS_FACES_BDR, KERNEL_BOUNDARY_NS = 25, 26, 27, 28
 KERNEL_LIFT_BDR_PTTT = 29
@@ -126,6 +126,8 @@ def library():
     L.pdg_batch_last_error.argtypes = [vp]
     L.pdg_filter_count.argtypes = [C.c_void_p, C.POINTER(C.c_int64)]
     L.pdg_rhs_vjp.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
+    L.pdg_rk_stage_vjp.argtypes = [C.c_void_p, C.c_int, C.c_double, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                   C.c_void_p]
     L.pdg_rhs_noalloc.argtypes = [C.POINTER(PdgMesh), C.POINTER(PdgParams), C.c_void_p, C.c_void_p, C.c_void_p]
     L.pdg_set_boundary.argtypes = [C.c_void_p, C.c_int, C.c_int, _dp]
     _lib = L
@@ -312,6 +314,18 @@ class DGSEMOperator:
                                          C.c_void_p(ubar.data_ptr()), C.c_void_p(_stream_handle(stream))),
                    "pdg_rhs_vjp")
         return ubar
+
+    def rk_stage_vjp(self, stage: int, dt: float, us, lam, out, bx, stream=None):
+        """Adjoint of rk_stage(stage, dt, un, us, .) for the cotangent lam of its
+        output (pdg_rk_stage_vjp): stage 2 sets out and bx, stage 1 sets out and
+        adds to bx, stage 0 adds to bx (out is scratch).  Fixed operator,
+        meshes without boundary faces."""
+        self._check_dev(us, lam, out, bx)
+        self._call(library().pdg_rk_stage_vjp(self._ctx, int(stage), float(dt), C.c_void_p(us.data_ptr()),
+                                              C.c_void_p(lam.data_ptr()), C.c_void_p(out.data_ptr()),
+                                              C.c_void_p(bx.data_ptr()), C.c_void_p(_stream_handle(stream))),
+                   "pdg_rk_stage_vjp")
+        return out
 
     def filter_count(self) -> int:
         """Element filterings by the entropy filter since creation (synchronises)."""

@@ -67,6 +67,10 @@ def _rk3_function():
             op, dt, nsteps, every = ctx.op, ctx.dt, ctx.nsteps, ctx.every
             ubar = gN.contiguous().clone()
             tmp = torch.empty_like(ubar)
+            # fused stage adjoints (pdg_rk_stage_vjp) on meshes without boundary faces
+            fused = not getattr(op.mesh, "boundaries", None)
+            if fused:
+                b1, b2, bx = torch.empty_like(ubar), torch.empty_like(ubar), torch.empty_like(ubar)
             for seg in reversed(range(len(ctx.checkpoints))):
                 first = seg * every
                 last = min(first + every, nsteps)
@@ -82,15 +86,22 @@ def _rk3_function():
                     x = u3
                 # u3 = u/3 + 2/3 (u2 + dt L(u2)); u2 = 3/4 u + 1/4 (u1 + dt L(u1)); u1 = u + dt L(u)
                 for x, u1, u2 in reversed(stages):
+                    if fused:
+                        # the stage algebra runs inside the VJP's last kernel
+                        op.rk_stage_vjp(2, dt, u2, ubar, b2, bx)
+                        op.rk_stage_vjp(1, dt, u1, b2, b1, bx)
+                        op.rk_stage_vjp(0, dt, x, b1, b2, bx)
+                        ubar, bx = bx, ubar
+                        continue
                     op.vjp(u2, ubar, out=tmp)
                     b2 = (2.0 / 3.0) * (ubar + dt * tmp)
-                    bx = (1.0 / 3.0) * ubar
+                    bxs = (1.0 / 3.0) * ubar
                     op.vjp(u1, b2, out=tmp)
                     b1 = 0.25 * (b2 + dt * tmp)
-                    bx += 0.75 * b2
+                    bxs += 0.75 * b2
                     op.vjp(x, b1, out=tmp)
-                    bx += b1 + dt * tmp
-                    ubar = bx
+                    bxs += b1 + dt * tmp
+                    ubar = bxs
             ctx.checkpoints = None
             return ubar, None, None, None, None
 

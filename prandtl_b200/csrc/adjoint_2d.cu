@@ -15,10 +15,8 @@ template <int N> static bool adj_info_n(int kind, KernelInfo *out)
         out->el_doubles = AdjShape<2, N>::EL;
         break;
     case KIND_ADJ_LIFT: out->fn = (const void *)&adj_lift_kernel<2, N>; out->el_doubles = S::EL_LIFT; break;
-    case KIND_ADJ_FACE_E0: out->fn = (const void *)&adj_face_kernel<2, N, 0, false>; break;
-    case KIND_ADJ_FACE_E1: out->fn = (const void *)&adj_face_kernel<2, N, 1, false>; break;
-    case KIND_ADJ_FACE_NS0: out->fn = (const void *)&adj_face_kernel<2, N, 0, true>; break;
-    case KIND_ADJ_FACE_NS1: out->fn = (const void *)&adj_face_kernel<2, N, 1, true>; break;
+    case KIND_ADJ_FACE_E0: out->fn = (const void *)&adj_faces_kernel<2, N, false>; break;
+    case KIND_ADJ_FACE_NS0: out->fn = (const void *)&adj_faces_kernel<2, N, true>; break;
     case KIND_ADJ_BOUNDARY: out->fn = (const void *)&adj_boundary_kernel<2, N>; break;
     default: return false;
     }

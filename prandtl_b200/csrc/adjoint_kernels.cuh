@@ -8,8 +8,11 @@
 //                    columns, viscous fluxes, primitive-gradient conversion
 //                    and the BR1 volume lifting — adds to ubar and leaves the
 //                    cotangents of the face-normal entropy gradients in gcol;
-//   adj_face_kernel  per direction: Riemann fluxes and (Navier-Stokes) the
-//                    BR1 face jumps — adds to ubar at face nodes.
+//   adj_faces_kernel every direction's Riemann fluxes and (Navier-Stokes) the
+//                    BR1 face jumps — stores both sides' cotangents per face
+//                    node to a buffer that adj_rhs_kernel adds to ubar.
+// Order of a product: (NS: lift_face_kernel for the forward jumps,
+// adj_lift_kernel,) adj_faces_kernel, adj_rhs_kernel.
 // The reference has no adjoint; each reversed step names the forward
 // function it reverses.
 #pragma once
@@ -323,8 +326,14 @@ __device__ __forceinline__ void indicator_vjp(const double *pr, double *pb, doub
     __syncwarp();
 }
 
-// Adjoint of the inviscid volume terms and the blending coefficient; stores
-// ubar = cotangent of u through those terms.
+// Adjoint of the inviscid volume terms and the blending coefficient, the
+// last kernel of a vector-Jacobian product: ubar = its terms, plus (NS,
+// P.adj_visc) the viscous terms adj_lift_kernel stored in ubar and (P.gbuf)
+// the face terms adj_faces_kernel stored there, added in that order.  With
+// P.stage >= 0 the RK stage's adjoint follows in the same store: for stage s
+// of out = a_s un + b_s (us + dt L(us)) and the cotangent lam of out, with g
+// = (dL/dus)^T lam, stage 2: ubar = 2/3 (lam + dt g), bx = 1/3 lam; stage 1:
+// ubar = 1/4 (lam + dt g), bx += 3/4 lam; stage 0 (us = un): bx += lam + dt g.
 template <int DIM, int N>
 __global__ void __launch_bounds__(128) adj_rhs_kernel(const KParams P, const double *__restrict__ cot,
                                                       double *__restrict__ ubar)
@@ -348,6 +357,9 @@ __global__ void __launch_bounds__(128) adj_rhs_kernel(const KParams P, const dou
         const int64_t e0 = wt * EPW + grp;
         const bool valid = e0 < P.ne;
         const int64_t e = valid ? e0 : 0;
+        int32_t enb[2 * DIM];  // the face neighbours (negative: a boundary face)
+#pragma unroll
+        for (int f = 0; f < 2 * DIM; f++) enb[f] = valid ? __ldg(P.nbr + e * 2 * DIM + f) : 0;
 #pragma unroll
         for (int k = 0; k < S::NPL; k++) {
             const int n = gl + k * L;
@@ -418,8 +430,40 @@ __global__ void __launch_bounds__(128) adj_rhs_kernel(const KParams P, const dou
                     for (int d = 0; d < DIM; d++) b.v[d] = pb[(P_V + d) * ST + m];
                     b.beta = pb[PS::BETA * ST + m];
                     pbar_to_cons<DIM>(s, b, nullptr, P.gm1, sb);
+                    const int idx[3] = {n % Np, (n / Np) % Np, n / (Np * Np)};
 #pragma unroll
-                    for (int v = 0; v < NV; v++) ubar[v * nn + e * NDOF + n] = sb[v];
+                    for (int v = 0; v < NV; v++) {
+                        const int64_t gi = v * nn + e * NDOF + n;
+                        double x = sb[v];
+                        if (P.adj_visc) x = x + ubar[gi];
+                        if (P.gbuf) {
+#pragma unroll
+                            for (int d = 0; d < DIM; d++) {
+                                const int pos = idx[d];
+                                if (pos == 0 || pos == N) {
+                                    const int side = pos == N ? 1 : 0;
+                                    if (enb[2 * d + side] >= 0)
+                                        x += __ldg(P.gbuf + (((int64_t)(d * 2 + side) * P.ne + e) * NV + v) * S::NFN +
+                                                   line_of<DIM, Np>(d, idx));
+                                }
+                            }
+                        }
+                        if (P.stage < 0) {
+                            ubar[gi] = x;
+                        } else {
+                            const double lam = lm[v * ST + m];
+                            const double z = lam + P.dt * x;
+                            if (P.stage == 2) {
+                                ubar[gi] = 2. / 3 * z;
+                                P.bx[gi] = 1. / 3 * lam;
+                            } else if (P.stage == 1) {
+                                ubar[gi] = 1. / 4 * z;
+                                P.bx[gi] = P.bx[gi] + 3. / 4 * lam;
+                            } else {
+                                P.bx[gi] = P.bx[gi] + z;
+                            }
+                        }
+                    }
                 }
             }
         }
@@ -427,10 +471,11 @@ __global__ void __launch_bounds__(128) adj_rhs_kernel(const KParams P, const dou
     }
 }
 
-// Adjoint of the viscous terms (lift_kernel in reverse).  cot: cotangent of
-// dudt; P.lbuf holds the forward BR1 face jumps (lift_face_kernel of u);
-// gcol receives, at every face node, the cotangent of the face-normal
-// entropy-variable gradient ([d][side][e][face node][v]).
+// Adjoint of the viscous terms (lift_kernel in reverse), the first kernel of
+// a Navier-Stokes vector-Jacobian product: stores them to ubar.  cot:
+// cotangent of dudt; P.lbuf holds the forward BR1 face jumps
+// (lift_face_kernel of u); gcol receives, at every face node, the cotangent
+// of the face-normal entropy-variable gradient ([d][side][e][face node][v]).
 template <int DIM, int N>
 __global__ void __launch_bounds__(128) adj_lift_kernel(const KParams P, const double *__restrict__ cot,
                                                        double *__restrict__ ubar, double *__restrict__ gcol)
@@ -631,7 +676,7 @@ __global__ void __launch_bounds__(128) adj_lift_kernel(const KParams P, const do
                     }
                     entropy_vars_vjp<DIM>(s, wb, P.gamma, P.gm1, P.gm1inv, sacc[k]);
 #pragma unroll
-                    for (int v = 0; v < NV; v++) ubar[v * nn + e * NDOF + n] += sacc[k][v];
+                    for (int v = 0; v < NV; v++) ubar[v * nn + e * NDOF + n] = sacc[k][v];
                 }
             }
         }
@@ -639,79 +684,105 @@ __global__ void __launch_bounds__(128) adj_lift_kernel(const KParams P, const do
     }
 }
 
-// Adjoint of one direction's face terms: element a's +D face node fn and
-// its neighbour b's -D face node (face_node_terms in reverse), plus for
+// Adjoint of one face node's terms: element a's +D face node fn and its
+// neighbour b's -D face node (face_node_terms in reverse), plus for
 // Navier-Stokes the BR1 jump 0.5 fsc A (w_b - w_a) that lift_face_node adds to
-// both sides' face gradients.
+// both sides' face gradients.  ga, gb: the cotangents of a's and b's states
+// at the face node.
 template <int DIM, int N, int D, bool NS>
-__global__ void __launch_bounds__(256) adj_face_kernel(const KParams P, const double *__restrict__ cot,
-                                                       double *__restrict__ ubar, const double *__restrict__ gcol)
+__device__ __forceinline__ void adj_face_node(const KParams &P, const double *c, const double *__restrict__ cot,
+                                              const double *__restrict__ gcol, int64_t a, int64_t b, int fn,
+                                              double *ga, double *gb)
 {
     using S = Shape<DIM, N>;
     constexpr int Np = S::Np, NDOF = S::NDOF, NV = S::NV, NFN = S::NFN;
-    __shared__ double c[CONST_SLOTS];
-    load_consts(P.K, c, Np);
-    __syncthreads();
     const int64_t nn = P.nnodes;
-    for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < P.ne * NFN;
+    const int na = line_node<DIM, Np, D>(fn, N), nb = line_node<DIM, Np, D>(fn, 0);
+    double sa[NV], sb[NV], la[NV], lb[NV];
+#pragma unroll
+    for (int v = 0; v < NV; v++) {
+        sa[v] = __ldg(P.u + v * nn + a * NDOF + na);
+        sb[v] = __ldg(P.u + v * nn + b * NDOF + nb);
+        la[v] = __ldg(cot + v * nn + a * NDOF + na);
+        lb[v] = __ldg(cot + v * nn + b * NDOF + nb);
+    }
+    double hs[NV];
+    if (NS) {  // loaded ahead of the flux arithmetic
+        const double h = 0.5 * C_FACE(c) * C_AREA(c)[D];
+#pragma unroll
+        for (int v = 0; v < NV; v++)
+            hs[v] = h * (__ldg(gcol + (((int64_t)(D * 2 + 1) * P.ne + a) * NFN + fn) * NV + v) +
+                         __ldg(gcol + (((int64_t)(D * 2 + 0) * P.ne + b) * NFN + fn) * NV + v));
+    }
+    const Prim<DIM> qa = make_prim<DIM>(sa, P.gamma, P.gm1), qb = make_prim<DIM>(sb, P.gamma, P.gm1);
+    const bool a_is_1 = a <= b;
+    const double nrm = a_is_1 ? C_AREA(c)[D] : -C_AREA(c)[D];
+    const double sc = C_FACE(c);
+    // out_a += C, out_b -= C with C = sc (a_is_1 ? -F : F) (+ the viscous part)
+    double Fb[NV];
+#pragma unroll
+    for (int v = 0; v < NV; v++) Fb[v] = (a_is_1 ? -sc : sc) * (la[v] - lb[v]);
+    PBar<DIM> ab, bb;
+    pbar_zero(ab);
+    pbar_zero(bb);
+    double mab[DIM], mbb[DIM];
+#pragma unroll
+    for (int d = 0; d < DIM; d++) mab[d] = mbb[d] = 0.0;
+    if (a_is_1) face_flux_vjp<DIM>(qa, qb, sa + 1, sb + 1, D, nrm, P.gamma, P.gm1inv, P.diss_scale, Fb, ab, bb, mab, mbb);
+    else face_flux_vjp<DIM>(qb, qa, sb + 1, sa + 1, D, nrm, P.gamma, P.gm1inv, P.diss_scale, Fb, bb, ab, mbb, mab);
+#pragma unroll
+    for (int v = 0; v < NV; v++) ga[v] = gb[v] = 0.0;
+    pbar_to_cons<DIM>(sa, ab, mab, P.gm1, ga);
+    pbar_to_cons<DIM>(sb, bb, mbb, P.gm1, gb);
+    if (NS) {
+        double wb[NV], wa[NV];
+#pragma unroll
+        for (int v = 0; v < NV; v++) {
+            wb[v] = hs[v];
+            wa[v] = -hs[v];
+        }
+        entropy_vars_vjp<DIM>(sa, wa, P.gamma, P.gm1, P.gm1inv, ga);
+        entropy_vars_vjp<DIM>(sb, wb, P.gamma, P.gm1, P.gm1inv, gb);
+    }
+}
+
+// The adjoint face terms of every direction in one launch, each face node's
+// two cotangents stored to gbuf[d][side][e][v][fn] (side 1: element a's +d
+// face node, side 0: its +d neighbour's -d face node, under that
+// neighbour's index); adj_rhs_kernel adds them to ubar.  Threads run
+// direction-major inside chunks of 64 elements, as lift_face_kernel.
+template <int DIM, int N, bool NS>
+__global__ void __launch_bounds__(256) adj_faces_kernel(const KParams P, const double *__restrict__ cot,
+                                                        double *__restrict__ gbuf, const double *__restrict__ gcol)
+{
+    using S = Shape<DIM, N>;
+    constexpr int NV = S::NV, NFN = S::NFN;
+    __shared__ double c[CONST_SLOTS];
+    load_consts(P.K, c, S::Np);
+    __syncthreads();
+    constexpr int CH = 64, PER_CH = DIM * CH * NFN;
+    const int64_t nch = (P.ne + CH - 1) / CH;
+    for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < nch * PER_CH;
          t += (int64_t)gridDim.x * blockDim.x) {
-        const int64_t a = t / NFN;
-        const int fn = (int)(t - a * NFN);
-        const int64_t b = __ldg(P.nbr + a * 2 * DIM + 2 * D + 1);
+        const int64_t ch = t / PER_CH;
+        const int r = (int)(t - ch * PER_CH);
+        const int d = r / (CH * NFN);
+        const int r2 = r - d * (CH * NFN);
+        const int64_t a = ch * CH + r2 / NFN;
+        const int fn = r2 % NFN;
+        if (a >= P.ne) continue;
+        const int64_t b = __ldg(P.nbr + a * 2 * DIM + 2 * d + 1);
         if (b < 0) continue;  // boundary face: adj_boundary_kernel
-        const int na = line_node<DIM, Np, D>(fn, N), nb = line_node<DIM, Np, D>(fn, 0);
-        double sa[NV], sb[NV], la[NV], lb[NV];
-#pragma unroll
-        for (int v = 0; v < NV; v++) {
-            sa[v] = __ldg(P.u + v * nn + a * NDOF + na);
-            sb[v] = __ldg(P.u + v * nn + b * NDOF + nb);
-            la[v] = __ldg(cot + v * nn + a * NDOF + na);
-            lb[v] = __ldg(cot + v * nn + b * NDOF + nb);
-        }
-        double pa[NV], pb[NV];  // ubar before this direction's terms, loaded ahead
-#pragma unroll
-        for (int v = 0; v < NV; v++) {
-            pa[v] = ubar[v * nn + a * NDOF + na];
-            pb[v] = ubar[v * nn + b * NDOF + nb];
-        }
-        const Prim<DIM> qa = make_prim<DIM>(sa, P.gamma, P.gm1), qb = make_prim<DIM>(sb, P.gamma, P.gm1);
-        const bool a_is_1 = a <= b;
-        const double nrm = a_is_1 ? C_AREA(c)[D] : -C_AREA(c)[D];
-        const double sc = C_FACE(c);
-        // out_a += C, out_b -= C with C = sc (a_is_1 ? -F : F) (+ the viscous part)
-        double Fb[NV];
-#pragma unroll
-        for (int v = 0; v < NV; v++) Fb[v] = (a_is_1 ? -sc : sc) * (la[v] - lb[v]);
-        PBar<DIM> ab, bb;
-        pbar_zero(ab);
-        pbar_zero(bb);
-        double mab[DIM], mbb[DIM];
-#pragma unroll
-        for (int d = 0; d < DIM; d++) mab[d] = mbb[d] = 0.0;
-        if (a_is_1) face_flux_vjp<DIM>(qa, qb, sa + 1, sb + 1, D, nrm, P.gamma, P.gm1inv, P.diss_scale, Fb, ab, bb, mab, mbb);
-        else face_flux_vjp<DIM>(qb, qa, sb + 1, sa + 1, D, nrm, P.gamma, P.gm1inv, P.diss_scale, Fb, bb, ab, mbb, mab);
         double ga[NV], gb[NV];
-#pragma unroll
-        for (int v = 0; v < NV; v++) ga[v] = gb[v] = 0.0;
-        pbar_to_cons<DIM>(sa, ab, mab, P.gm1, ga);
-        pbar_to_cons<DIM>(sb, bb, mbb, P.gm1, gb);
-        if (NS) {
-            const double h = 0.5 * C_FACE(c) * C_AREA(c)[D];
-            double wb[NV], wa[NV];
-#pragma unroll
-            for (int v = 0; v < NV; v++) {
-                const double s = h * (__ldg(gcol + (((int64_t)(D * 2 + 1) * P.ne + a) * NFN + fn) * NV + v) +
-                                      __ldg(gcol + (((int64_t)(D * 2 + 0) * P.ne + b) * NFN + fn) * NV + v));
-                wb[v] = s;
-                wa[v] = -s;
-            }
-            entropy_vars_vjp<DIM>(sa, wa, P.gamma, P.gm1, P.gm1inv, ga);
-            entropy_vars_vjp<DIM>(sb, wb, P.gamma, P.gm1, P.gm1inv, gb);
-        }
+        if (d == 0) adj_face_node<DIM, N, 0, NS>(P, c, cot, gcol, a, b, fn, ga, gb);
+        else if (d == 1) adj_face_node<DIM, N, 1, NS>(P, c, cot, gcol, a, b, fn, ga, gb);
+        else adj_face_node<DIM, N, (DIM == 3 ? 2 : 0), NS>(P, c, cot, gcol, a, b, fn, ga, gb);
+        double *da = gbuf + (((int64_t)(d * 2 + 1) * P.ne + a) * NV) * NFN + fn;
+        double *db = gbuf + (((int64_t)(d * 2 + 0) * P.ne + b) * NV) * NFN + fn;
 #pragma unroll
         for (int v = 0; v < NV; v++) {
-            ubar[v * nn + a * NDOF + na] = pa[v] + ga[v];
-            ubar[v * nn + b * NDOF + nb] = pb[v] + gb[v];
+            da[v * NFN] = ga[v];
+            db[v * NFN] = gb[v];
         }
     }
 }

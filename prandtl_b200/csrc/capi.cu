@@ -55,6 +55,7 @@ struct pdg_ctx {
     double *ent_own = nullptr;                // filter: per-element entropy minimum at the stage input
     unsigned long long *filter_count = nullptr;
     double *gcol = nullptr;   // adjoint: cotangents of the face-normal entropy gradients
+    double *gbuf = nullptr;   // adjoint: face-term cotangents of both sides of every face node
     // pdg_rk3_steps: one step captured in a CUDA graph for a (state, dt) pair
     cudaStream_t cap = nullptr;
     cudaGraph_t graph = nullptr;
@@ -275,7 +276,8 @@ int kernel_config(int dim, int N, int kind, int64_t ne, int device, LaunchCfg *c
         const int64_t threads = kind == KIND_FILTER_BOUNDS ? 32 * ne
                                 : (kind == KIND_BOUNDARY || kind == KIND_ADJ_BOUNDARY || kind == KIND_BOUNDARY_NS) ? ne
                                 : ((kind == KIND_LIFT_FACE || kind == KIND_LIFT_FACE_BDR || kind == KIND_LIFT_FACE_FLUX ||
-                                    kind == KIND_FACE_FLUX) ? (int64_t)dim : 1) * ne * nfn;
+                                    kind == KIND_FACE_FLUX || kind == KIND_ADJ_FACE_E0 || kind == KIND_ADJ_FACE_NS0)
+                                       ? (int64_t)dim : 1) * ne * nfn;
         // 256-thread blocks; 128 when that gives fewer than four blocks per
         // SM, so that a small mesh still spreads evenly over the SMs
         cfg->wpb = threads < 4LL * 256 * sms ? 4 : 8;
@@ -742,6 +744,7 @@ int pdg_destroy(pdg_ctx *c)
     cudaFree(c->err);
     cudaFree(c->ent_own);
     cudaFree(c->gcol);
+    cudaFree(c->gbuf);
     if (c->graph_exec) cudaGraphExecDestroy(c->graph_exec);
     if (c->graph) cudaGraphDestroy(c->graph);
     if (c->cap) cudaStreamDestroy(c->cap);
@@ -953,50 +956,95 @@ const char *pdg_last_error(const pdg_ctx *c) { return c ? c->last_error.c_str() 
 
 int64_t pdg_launch_count(const pdg_ctx *c) { return c ? c->launches : -1; }
 
+}  // extern "C"
+
+namespace {
+
+// Configures the adjoint kernels and their scratch on the first use.
+int vjp_setup(pdg_ctx *c)
+{
+    if (c->adj_ready) return PDG_OK;
+    int r;
+    const int kinds[] = {KIND_ADJ_RHS, KIND_ADJ_LIFT, KIND_ADJ_FACE_E0, KIND_ADJ_FACE_NS0};
+    for (int kind : kinds) {
+        const bool ns_kind = kind == KIND_ADJ_LIFT || kind == KIND_ADJ_FACE_NS0;
+        if ((ns_kind && !c->p.parabolic) || (kind == KIND_ADJ_FACE_E0 && c->p.parabolic)) continue;
+        if ((r = configure_launch(c, kind))) return r;
+    }
+    if (!c->p.parabolic && (r = configure_launch(c, KIND_ADJ_BOUNDARY))) return r;
+    const size_t nfn = c->dim == 2 ? c->Np : c->Np * c->Np;
+    if (c->p.parabolic && cudaMalloc(&c->gcol, sizeof(double) * 2 * c->dim * c->ne * nfn * c->nv) != cudaSuccess)
+        return fail(c, PDG_ERR_NOMEM, "pdg_rhs_vjp: scratch allocation failed");
+    if (cudaMalloc(&c->gbuf, sizeof(double) * 2 * c->dim * c->ne * nfn * c->nv) != cudaSuccess)
+        return fail(c, PDG_ERR_NOMEM, "pdg_rhs_vjp: scratch allocation failed");
+    c->adj_ready = true;
+    return PDG_OK;
+}
+
+// (NS: the forward BR1 jumps, the viscous terms to ubar,) every face's
+// adjoint terms to gbuf, then the volume terms, which add the others and, for
+// stage >= 0, the RK stage's adjoint (adj_rhs_kernel).  Boundary faces
+// (Euler) are added to ubar last.
+int vjp(pdg_ctx *c, int stage, double dt, const double *u, const double *cot, double *ubar, double *bx,
+        cudaStream_t s)
+{
+    int r;
+    if ((r = vjp_setup(c))) return r;
+    KParams P = base_params(c);
+    P.u = u;
+    P.gbuf = c->gbuf;
+    P.stage = stage;
+    P.dt = dt;
+    P.bx = bx;
+    P.adj_visc = c->p.parabolic ? 1 : 0;
+    c->last_stream = s;
+    void *a_cot = (void *)&cot, *a_bar = (void *)&ubar, *a_g = (void *)&c->gcol, *a_gb = (void *)&c->gbuf;
+    if (c->p.parabolic) {
+        if ((r = launch(c, KIND_LIFT_FACE, P, s))) return r;
+        if ((r = launch_with(c, KIND_ADJ_LIFT, P, a_cot, a_bar, a_g, s))) return r;
+        if ((r = launch_with(c, KIND_ADJ_FACE_NS0, P, a_cot, a_gb, a_g, s))) return r;
+    } else {
+        if ((r = launch_with(c, KIND_ADJ_FACE_E0, P, a_cot, a_gb, a_g, s))) return r;
+    }
+    if ((r = launch_with(c, KIND_ADJ_RHS, P, a_cot, a_bar, nullptr, s))) return r;
+    if (!c->p.parabolic && c->bc_used && (r = launch_with(c, KIND_ADJ_BOUNDARY, P, a_cot, a_bar, a_g, s))) return r;
+    return PDG_OK;
+}
+
+int vjp_check(pdg_ctx *c, const char *what)
+{
+    if (c->p.compat) return fail(c, PDG_ERR_UNSUPPORTED, "%s: the adjoint is of the fixed operator (compat = 0)", what);
+    if (c->p.parabolic && c->bc_used)
+        return fail(c, PDG_ERR_UNSUPPORTED, "%s: Navier-Stokes boundary faces are not differentiated", what);
+    if (c->bc_used & ~c->bc_set) return fail(c, PDG_ERR_ARG, "%s: a boundary condition is not set", what);
+    return PDG_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
 int pdg_rhs_vjp(pdg_ctx *c, const double *u, const double *cot, double *ubar, void *stream)
 {
     if (!c) return PDG_ERR_ARG;
     if (!u || !cot || !ubar || ubar == u || ubar == cot) return fail(c, PDG_ERR_ARG, "pdg_rhs_vjp: null or aliased buffers");
-    if (c->p.compat) return fail(c, PDG_ERR_UNSUPPORTED, "pdg_rhs_vjp: the adjoint is of the fixed operator (compat = 0)");
-    if (c->p.parabolic && c->bc_used)
-        return fail(c, PDG_ERR_UNSUPPORTED, "pdg_rhs_vjp: Navier-Stokes boundary faces are not differentiated");
-    if (c->bc_used & ~c->bc_set) return fail(c, PDG_ERR_ARG, "pdg_rhs_vjp: a boundary condition is not set");
-    cudaStream_t s = (cudaStream_t)stream;
     int r;
-    if (!c->adj_ready) {
-        const int kinds[] = {KIND_ADJ_RHS, KIND_ADJ_LIFT, KIND_ADJ_FACE_E0, KIND_ADJ_FACE_E1, KIND_ADJ_FACE_E2,
-                             KIND_ADJ_FACE_NS0, KIND_ADJ_FACE_NS1, KIND_ADJ_FACE_NS2};
-        for (int kind : kinds) {
-            const bool ns_kind = kind == KIND_ADJ_LIFT || kind >= KIND_ADJ_FACE_NS0;
-            const bool euler_kind = kind >= KIND_ADJ_FACE_E0 && kind <= KIND_ADJ_FACE_E2;
-            if ((ns_kind && !c->p.parabolic) || (euler_kind && c->p.parabolic)) continue;
-            if ((kind == KIND_ADJ_FACE_E2 || kind == KIND_ADJ_FACE_NS2) && c->dim < 3) continue;
-            if ((r = configure_launch(c, kind))) return r;
-        }
-        if (!c->p.parabolic && (r = configure_launch(c, KIND_ADJ_BOUNDARY))) return r;
-        if (c->p.parabolic) {
-            const size_t nfn = c->dim == 2 ? c->Np : c->Np * c->Np;
-            if (cudaMalloc(&c->gcol, sizeof(double) * 2 * c->dim * c->ne * nfn * c->nv) != cudaSuccess)
-                return fail(c, PDG_ERR_NOMEM, "pdg_rhs_vjp: scratch allocation failed");
-        }
-        c->adj_ready = true;
-    }
-    KParams P = base_params(c);
-    P.u = u;
-    c->last_stream = s;
-    void *a_cot = (void *)&cot, *a_bar = (void *)&ubar, *a_g = (void *)&c->gcol;
-    if (c->p.parabolic && (r = launch(c, KIND_LIFT_FACE, P, s))) return r;
-    if ((r = launch_with(c, KIND_ADJ_RHS, P, a_cot, a_bar, nullptr, s))) return r;
-    if (c->p.parabolic) {
-        if ((r = launch_with(c, KIND_ADJ_LIFT, P, a_cot, a_bar, a_g, s))) return r;
-        for (int d = 0; d < c->dim; d++)
-            if ((r = launch_with(c, KIND_ADJ_FACE_NS0 + d, P, a_cot, a_bar, a_g, s))) return r;
-    } else {
-        for (int d = 0; d < c->dim; d++)
-            if ((r = launch_with(c, KIND_ADJ_FACE_E0 + d, P, a_cot, a_bar, a_g, s))) return r;
-        if (c->bc_used && (r = launch_with(c, KIND_ADJ_BOUNDARY, P, a_cot, a_bar, a_g, s))) return r;
-    }
-    return PDG_OK;
+    if ((r = vjp_check(c, "pdg_rhs_vjp"))) return r;
+    return vjp(c, -1, 0.0, u, cot, ubar, nullptr, (cudaStream_t)stream);
+}
+
+int pdg_rk_stage_vjp(pdg_ctx *c, int stage, double dt, const double *us, const double *lam, double *out, double *bx,
+                     void *stream)
+{
+    if (!c) return PDG_ERR_ARG;
+    if (stage < 0 || stage > 2) return fail(c, PDG_ERR_ARG, "pdg_rk_stage_vjp: stage must be 0, 1 or 2");
+    if (!us || !lam || !out || !bx || out == us || out == lam || out == bx || bx == us || bx == lam)
+        return fail(c, PDG_ERR_ARG, "pdg_rk_stage_vjp: null or aliased buffers");
+    int r;
+    if ((r = vjp_check(c, "pdg_rk_stage_vjp"))) return r;
+    if (c->bc_used)  // their adjoint is added after the volume kernel's store
+        return fail(c, PDG_ERR_UNSUPPORTED, "pdg_rk_stage_vjp: boundary faces (use pdg_rhs_vjp)");
+    return vjp(c, stage, dt, us, lam, out, bx, (cudaStream_t)stream);
 }
 
 int pdg_filter_count(pdg_ctx *c, int64_t *filtered)

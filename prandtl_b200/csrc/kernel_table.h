@@ -18,12 +18,12 @@ enum KernelKind {
     KIND_FILTER = 11,         // filter_kernel<dim, N>: entropy/positivity filter of the stage output
     KIND_ADJ_RHS = 12,        // adj_rhs_kernel<dim, N>: adjoint of the inviscid volume terms and blending
     KIND_ADJ_LIFT = 13,       // adj_lift_kernel<dim, N>: adjoint of the viscous terms
-    KIND_ADJ_FACE_E0 = 14,    // adj_face_kernel<dim, N, d, false>, d = 0, 1, 2
-    KIND_ADJ_FACE_E1 = 15,
-    KIND_ADJ_FACE_E2 = 16,
-    KIND_ADJ_FACE_NS0 = 17,   // adj_face_kernel<dim, N, d, true>
-    KIND_ADJ_FACE_NS1 = 18,
-    KIND_ADJ_FACE_NS2 = 19,
+    KIND_ADJ_FACE_E0 = 14,    // adj_faces_kernel<dim, N, false>: every direction's adjoint face terms (Euler)
+    KIND_ADJ_FACE_E1 = 15,    // (unused)
+    KIND_ADJ_FACE_E2 = 16,    // (unused)
+    KIND_ADJ_FACE_NS0 = 17,   // adj_faces_kernel<dim, N, true>: the same with the BR1 jumps (NS)
+    KIND_ADJ_FACE_NS1 = 18,   // (unused)
+    KIND_ADJ_FACE_NS2 = 19,   // (unused)
     KIND_EULER_FACES = 20,    // rhs_kernel<dim, N, false, true>: Euler volume + face terms (+ stage)
     KIND_NS_FACES = 21,       // rhs_kernel<dim, N, true, true>: NS inviscid volume + all face terms (+ stage)
     KIND_BOUNDARY = 22,       // boundary_kernel<dim, N>: boundary faces of the separate-face path (Euler)

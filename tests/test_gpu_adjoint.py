@@ -149,3 +149,39 @@ def test_kinetic_energy_gradient_checkpointed(par, cuda_device):
     ke_t = adjoint.kinetic_energy(m, _torch_rk3(T, ut, dt, 20))
     (gt,) = torch.autograd.grad(ke_t, ut)
     assert rel_maxnorm(grads[0], gt.numpy()) < 1e-9
+
+
+@pytest.mark.parametrize("kind,dim,order,par", [("rough2d", 2, 3, 0), ("rough3d", 3, 3, 1), ("rough3d", 3, 2, 0),
+                                                ("rough2d", 2, 4, 1)])
+def test_stage_vjp_fuses_the_stage_algebra(kind, dim, order, par, cuda_device):
+    """pdg_rk_stage_vjp equals the VJP followed by the stage algebra in torch:
+    stage 2 out = 2/3 (lam + dt g), bx = 1/3 lam; stage 1 out = 1/4 (lam + dt g),
+    bx += 3/4 lam; stage 0 bx += lam + dt g (1e-13: one rounding of each term)."""
+    m, u = make(kind, dim, order)
+    op = pb.DGSEMOperator(m, **params(par))
+    us = torch.from_numpy(u).to(cuda_device)
+    rng = np.random.default_rng(11)
+    lam = torch.from_numpy(rng.standard_normal(u.size)).to(cuda_device)
+    bx0 = torch.from_numpy(rng.standard_normal(u.size)).to(cuda_device)
+    dt = 1e-3
+    g = op.vjp(us, lam)
+    z = lam + dt * g
+    want = {2: (2.0 / 3.0 * z, 1.0 / 3.0 * lam), 1: (0.25 * z, bx0 + 0.75 * lam), 0: (None, bx0 + z)}
+    for stage in (2, 1, 0):
+        out = torch.full_like(us, float("nan"))
+        bx = bx0.clone()
+        op.rk_stage_vjp(stage, dt, us, lam, out, bx)
+        w_out, w_bx = want[stage]
+        if w_out is not None:
+            assert rel_maxnorm(out.cpu().numpy(), w_out.cpu().numpy()) < 1e-13, f"stage {stage} out"
+        assert rel_maxnorm(bx.cpu().numpy(), w_bx.cpu().numpy()) < 1e-13, f"stage {stage} bx"
+    assert op.check() == 0
+
+
+def test_stage_vjp_rejects_boundary_meshes(cuda_device):
+    mesh, u = cases.forward_facing_step(order=2, cells_per_unit=4)
+    op = pb.DGSEMOperator(mesh, compat=0)
+    x = torch.from_numpy(u).to(cuda_device)
+    a, b = torch.empty_like(x), torch.zeros_like(x)
+    with pytest.raises(pb.PdgError):
+        op.rk_stage_vjp(1, 1e-3, x, x.clone(), a, b)

@@ -217,9 +217,10 @@ def test_element_side_faces_equal_face_kernels(kind, dim, order, par, cuda_devic
 @pytest.mark.parametrize("kind,dim,order,par", [("rough2d", 2, 3, 0), ("rough3d", 3, 3, 1), ("rough2dns", 2, 4, 1),
                                                 ("rough3d", 3, 2, 0), ("rough2d", 2, 5, 0), ("rough3d", 3, 4, 1)])
 def test_face_buffer_equals_element_faces(kind, dim, order, par, cuda_device, monkeypatch):
-    """Each face's inviscid flux evaluated once into the face buffer gives,
-    bit for bit, the values of both elements evaluating it themselves
-    (PDG_FACE_BUFFER=0): the same arithmetic on the same inputs."""
+    """Each face's inviscid flux evaluated once into the face buffer gives the
+    values of both elements evaluating it themselves (PDG_FACE_BUFFER=0): the
+    same arithmetic on the same inputs, inlined into different kernels, so
+    equal up to the compiler's choice of fused multiply-adds (1e-14)."""
     import torch
     mesh, u = make_case(kind, dim, order)
     kw = dict(parabolic=par, mu=0.01 if par else 0.0, Pr=0.71, compat=0)
@@ -239,6 +240,6 @@ def test_face_buffer_equals_element_faces(kind, dim, order, par, cuda_device, mo
             op.rk_stage(stage, 1e-3, un, us, a)
             op_el.rk_stage(stage, 1e-3, un, us, b)
         torch.cuda.synchronize()
-        assert torch.equal(a, b), f"stage {stage}"
+        assert rel_maxnorm(a.cpu().numpy(), b.cpu().numpy()) < 1e-14, f"stage {stage}"
     assert op.GetMaxCharSpeed() == op_el.GetMaxCharSpeed()
     assert op.check() == 0 and op_el.check() == 0
