@@ -38,6 +38,7 @@ KERNEL_FILTER_BOUNDS, KERNEL_FILTER = 10, 11
 KERNEL_ADJ_RHS, KERNEL_ADJ_LIFT = 12, 13
 KERNEL_ADJ_FACE_EULER = (14,)   # adj_faces_kernel: every direction in one launch
 KERNEL_ADJ_FACE_NS = (17,)
+KERNEL_ADJ_GATHER = 15
 KERNEL_EULER_FACES, KERNEL_NS_FACES, KERNEL_BOUNDARY, KERNEL_ADJ_BOUNDARY, KERNEL_EULER_FACES_BDR = 20, 21, 22, 23, 24
 KERNEL_LIFT_FACE_BDR, KERNEL_LIFT_BDR, KERNEL_NS_FACES_BDR, KERNEL_BOUNDARY_NS = 25, 26, 27, 28
 KERNEL_LIFT_BDR_PTTT = 29

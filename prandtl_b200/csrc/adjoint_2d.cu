@@ -17,6 +17,7 @@ template <int N> static bool adj_info_n(int kind, KernelInfo *out)
     case KIND_ADJ_LIFT: out->fn = (const void *)&adj_lift_kernel<2, N>; out->el_doubles = S::EL_LIFT; break;
     case KIND_ADJ_FACE_E0: out->fn = (const void *)&adj_faces_kernel<2, N, false>; break;
     case KIND_ADJ_FACE_NS0: out->fn = (const void *)&adj_faces_kernel<2, N, true>; break;
+    case KIND_ADJ_GATHER: out->fn = (const void *)&adj_gather_kernel<2, N>; break;
     case KIND_ADJ_BOUNDARY: out->fn = (const void *)&adj_boundary_kernel<2, N>; break;
     default: return false;
     }

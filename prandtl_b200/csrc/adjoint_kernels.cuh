@@ -10,9 +10,11 @@
 //                    cotangents of the face-normal entropy gradients in gcol;
 //   adj_faces_kernel every direction's Riemann fluxes and (Navier-Stokes) the
 //                    BR1 face jumps — stores both sides' cotangents per face
-//                    node to a buffer that adj_rhs_kernel adds to ubar.
-// Order of a product: (NS: lift_face_kernel for the forward jumps,
-// adj_lift_kernel,) adj_faces_kernel, adj_rhs_kernel.
+//                    node to a buffer;
+//   adj_gather_kernel adds them to ubar, then (an RK stage's adjoint) the
+//                    stage algebra.
+// Order of a product: (NS: lift_face_kernel for the forward jumps,)
+// adj_rhs_kernel, (NS: adj_lift_kernel,) adj_faces_kernel, adj_gather_kernel.
 // The reference has no adjoint; each reversed step names the forward
 // function it reverses.
 #pragma once
@@ -327,15 +329,10 @@ __device__ __forceinline__ void indicator_vjp(const double *pr, double *pb, doub
 }
 
 // Adjoint of the inviscid volume terms and the blending coefficient, the
-// last kernel of a vector-Jacobian product: ubar = its terms, plus (NS,
-// P.adj_visc) the viscous terms adj_lift_kernel stored in ubar and (P.gbuf)
-// the face terms adj_faces_kernel stored there, added in that order.  With
-// P.stage >= 0 the RK stage's adjoint follows in the same store: for stage s
-// of out = a_s un + b_s (us + dt L(us)) and the cotangent lam of out, with g
-// = (dL/dus)^T lam, stage 2: ubar = 2/3 (lam + dt g), bx = 1/3 lam; stage 1:
-// ubar = 1/4 (lam + dt g), bx += 3/4 lam; stage 0 (us = un): bx += lam + dt g.
+// first kernel of a vector-Jacobian product: stores ubar = cotangent of u
+// through those terms.
 template <int DIM, int N>
-__global__ void __launch_bounds__(128) adj_rhs_kernel(const KParams P, const double *__restrict__ cot,
+__global__ void __launch_bounds__(128, 3) adj_rhs_kernel(const KParams P, const double *__restrict__ cot,
                                                       double *__restrict__ ubar)
 {
     using S = Shape<DIM, N>;
@@ -357,9 +354,6 @@ __global__ void __launch_bounds__(128) adj_rhs_kernel(const KParams P, const dou
         const int64_t e0 = wt * EPW + grp;
         const bool valid = e0 < P.ne;
         const int64_t e = valid ? e0 : 0;
-        int32_t enb[2 * DIM];  // the face neighbours (negative: a boundary face)
-#pragma unroll
-        for (int f = 0; f < 2 * DIM; f++) enb[f] = valid ? __ldg(P.nbr + e * 2 * DIM + f) : 0;
 #pragma unroll
         for (int k = 0; k < S::NPL; k++) {
             const int n = gl + k * L;
@@ -430,40 +424,8 @@ __global__ void __launch_bounds__(128) adj_rhs_kernel(const KParams P, const dou
                     for (int d = 0; d < DIM; d++) b.v[d] = pb[(P_V + d) * ST + m];
                     b.beta = pb[PS::BETA * ST + m];
                     pbar_to_cons<DIM>(s, b, nullptr, P.gm1, sb);
-                    const int idx[3] = {n % Np, (n / Np) % Np, n / (Np * Np)};
 #pragma unroll
-                    for (int v = 0; v < NV; v++) {
-                        const int64_t gi = v * nn + e * NDOF + n;
-                        double x = sb[v];
-                        if (P.adj_visc) x = x + ubar[gi];
-                        if (P.gbuf) {
-#pragma unroll
-                            for (int d = 0; d < DIM; d++) {
-                                const int pos = idx[d];
-                                if (pos == 0 || pos == N) {
-                                    const int side = pos == N ? 1 : 0;
-                                    if (enb[2 * d + side] >= 0)
-                                        x += __ldg(P.gbuf + (((int64_t)(d * 2 + side) * P.ne + e) * NV + v) * S::NFN +
-                                                   line_of<DIM, Np>(d, idx));
-                                }
-                            }
-                        }
-                        if (P.stage < 0) {
-                            ubar[gi] = x;
-                        } else {
-                            const double lam = lm[v * ST + m];
-                            const double z = lam + P.dt * x;
-                            if (P.stage == 2) {
-                                ubar[gi] = 2. / 3 * z;
-                                P.bx[gi] = 1. / 3 * lam;
-                            } else if (P.stage == 1) {
-                                ubar[gi] = 1. / 4 * z;
-                                P.bx[gi] = P.bx[gi] + 3. / 4 * lam;
-                            } else {
-                                P.bx[gi] = P.bx[gi] + z;
-                            }
-                        }
-                    }
+                    for (int v = 0; v < NV; v++) ubar[v * nn + e * NDOF + n] = sb[v];
                 }
             }
         }
@@ -471,9 +433,8 @@ __global__ void __launch_bounds__(128) adj_rhs_kernel(const KParams P, const dou
     }
 }
 
-// Adjoint of the viscous terms (lift_kernel in reverse), the first kernel of
-// a Navier-Stokes vector-Jacobian product: stores them to ubar.  cot:
-// cotangent of dudt; P.lbuf holds the forward BR1 face jumps
+// Adjoint of the viscous terms (lift_kernel in reverse): adds them to ubar.
+// cot: cotangent of dudt; P.lbuf holds the forward BR1 face jumps
 // (lift_face_kernel of u); gcol receives, at every face node, the cotangent
 // of the face-normal entropy-variable gradient ([d][side][e][face node][v]).
 template <int DIM, int N>
@@ -676,7 +637,7 @@ __global__ void __launch_bounds__(128) adj_lift_kernel(const KParams P, const do
                     }
                     entropy_vars_vjp<DIM>(s, wb, P.gamma, P.gm1, P.gm1inv, sacc[k]);
 #pragma unroll
-                    for (int v = 0; v < NV; v++) ubar[v * nn + e * NDOF + n] = sacc[k][v];
+                    for (int v = 0; v < NV; v++) ubar[v * nn + e * NDOF + n] += sacc[k][v];
                 }
             }
         }
@@ -752,7 +713,7 @@ __device__ __forceinline__ void adj_face_node(const KParams &P, const double *c,
 // neighbour's index); adj_rhs_kernel adds them to ubar.  Threads run
 // direction-major inside chunks of 64 elements, as lift_face_kernel.
 template <int DIM, int N, bool NS>
-__global__ void __launch_bounds__(256) adj_faces_kernel(const KParams P, const double *__restrict__ cot,
+__global__ void __launch_bounds__(256, 2) adj_faces_kernel(const KParams P, const double *__restrict__ cot,
                                                         double *__restrict__ gbuf, const double *__restrict__ gcol)
 {
     using S = Shape<DIM, N>;
@@ -783,6 +744,61 @@ __global__ void __launch_bounds__(256) adj_faces_kernel(const KParams P, const d
         for (int v = 0; v < NV; v++) {
             da[v * NFN] = ga[v];
             db[v * NFN] = gb[v];
+        }
+    }
+}
+
+// ubar += the face-term cotangents of gbuf at every face node (in the order
+// x, y [, z] faces), one thread per node.  With P.stage >= 0 the RK stage's
+// adjoint follows: for stage s of out = a_s un + b_s (us + dt L(us)) and the
+// cotangent lam (cot) of out, with g = ubar = (dL/dus)^T lam,
+//   stage 2: ubar = 2/3 (lam + dt g), bx = 1/3 lam;
+//   stage 1: ubar = 1/4 (lam + dt g), bx += 3/4 lam;
+//   stage 0 (us = un): bx += lam + dt g.
+template <int DIM, int N>
+__global__ void __launch_bounds__(256) adj_gather_kernel(const KParams P, const double *__restrict__ cot,
+                                                         double *__restrict__ ubar)
+{
+    using S = Shape<DIM, N>;
+    constexpr int Np = S::Np, NDOF = S::NDOF, NV = S::NV, NFN = S::NFN;
+    const int64_t nn = P.nnodes;
+    for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < nn; t += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t e = t / NDOF;
+        const int n = (int)(t - e * NDOF);
+        const int idx[3] = {n % Np, (n / Np) % Np, n / (Np * Np)};
+        const double *src[DIM];
+#pragma unroll
+        for (int d = 0; d < DIM; d++) {
+            const int pos = idx[d];
+            src[d] = nullptr;
+            if (pos == 0 || pos == N) {
+                const int side = pos == N ? 1 : 0;
+                if (__ldg(P.nbr + e * 2 * DIM + 2 * d + side) >= 0)  // boundary faces: adj_boundary_kernel
+                    src[d] = P.gbuf + (((int64_t)(d * 2 + side) * P.ne + e) * NV) * NFN + line_of<DIM, Np>(d, idx);
+            }
+        }
+#pragma unroll
+        for (int v = 0; v < NV; v++) {
+            const int64_t gi = v * nn + t;
+            double x = ubar[gi];
+#pragma unroll
+            for (int d = 0; d < DIM; d++)
+                if (src[d]) x += __ldg(src[d] + v * NFN);
+            if (P.stage < 0) {
+                ubar[gi] = x;
+            } else {
+                const double lam = __ldg(cot + gi);
+                const double z = lam + P.dt * x;
+                if (P.stage == 2) {
+                    ubar[gi] = 2. / 3 * z;
+                    P.bx[gi] = 1. / 3 * lam;
+                } else if (P.stage == 1) {
+                    ubar[gi] = 1. / 4 * z;
+                    P.bx[gi] = P.bx[gi] + 3. / 4 * lam;
+                } else {
+                    P.bx[gi] = P.bx[gi] + z;
+                }
+            }
         }
     }
 }

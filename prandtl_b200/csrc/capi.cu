@@ -275,6 +275,7 @@ int kernel_config(int dim, int N, int kind, int64_t ne, int device, LaunchCfg *c
     if (ki.el_doubles == 0) {  // thread-per-face-node kernel
         const int64_t threads = kind == KIND_FILTER_BOUNDS ? 32 * ne
                                 : (kind == KIND_BOUNDARY || kind == KIND_ADJ_BOUNDARY || kind == KIND_BOUNDARY_NS) ? ne
+                                : kind == KIND_ADJ_GATHER ? ne * nfn * (N + 1)  // thread per node
                                 : ((kind == KIND_LIFT_FACE || kind == KIND_LIFT_FACE_BDR || kind == KIND_LIFT_FACE_FLUX ||
                                     kind == KIND_FACE_FLUX || kind == KIND_ADJ_FACE_E0 || kind == KIND_ADJ_FACE_NS0)
                                        ? (int64_t)dim : 1) * ne * nfn;
@@ -965,7 +966,7 @@ int vjp_setup(pdg_ctx *c)
 {
     if (c->adj_ready) return PDG_OK;
     int r;
-    const int kinds[] = {KIND_ADJ_RHS, KIND_ADJ_LIFT, KIND_ADJ_FACE_E0, KIND_ADJ_FACE_NS0};
+    const int kinds[] = {KIND_ADJ_RHS, KIND_ADJ_LIFT, KIND_ADJ_FACE_E0, KIND_ADJ_FACE_NS0, KIND_ADJ_GATHER};
     for (int kind : kinds) {
         const bool ns_kind = kind == KIND_ADJ_LIFT || kind == KIND_ADJ_FACE_NS0;
         if ((ns_kind && !c->p.parabolic) || (kind == KIND_ADJ_FACE_E0 && c->p.parabolic)) continue;
@@ -981,10 +982,10 @@ int vjp_setup(pdg_ctx *c)
     return PDG_OK;
 }
 
-// (NS: the forward BR1 jumps, the viscous terms to ubar,) every face's
-// adjoint terms to gbuf, then the volume terms, which add the others and, for
-// stage >= 0, the RK stage's adjoint (adj_rhs_kernel).  Boundary faces
-// (Euler) are added to ubar last.
+// (NS: the forward BR1 jumps,) the volume terms to ubar, (NS: the viscous
+// terms added,) every face's adjoint terms to gbuf, then their sum into ubar
+// with, for stage >= 0, the RK stage's adjoint (adj_gather_kernel).  Boundary
+// faces (Euler, stage < 0 only) are added to ubar last.
 int vjp(pdg_ctx *c, int stage, double dt, const double *u, const double *cot, double *ubar, double *bx,
         cudaStream_t s)
 {
@@ -996,17 +997,13 @@ int vjp(pdg_ctx *c, int stage, double dt, const double *u, const double *cot, do
     P.stage = stage;
     P.dt = dt;
     P.bx = bx;
-    P.adj_visc = c->p.parabolic ? 1 : 0;
     c->last_stream = s;
     void *a_cot = (void *)&cot, *a_bar = (void *)&ubar, *a_g = (void *)&c->gcol, *a_gb = (void *)&c->gbuf;
-    if (c->p.parabolic) {
-        if ((r = launch(c, KIND_LIFT_FACE, P, s))) return r;
-        if ((r = launch_with(c, KIND_ADJ_LIFT, P, a_cot, a_bar, a_g, s))) return r;
-        if ((r = launch_with(c, KIND_ADJ_FACE_NS0, P, a_cot, a_gb, a_g, s))) return r;
-    } else {
-        if ((r = launch_with(c, KIND_ADJ_FACE_E0, P, a_cot, a_gb, a_g, s))) return r;
-    }
+    if (c->p.parabolic && (r = launch(c, KIND_LIFT_FACE, P, s))) return r;
     if ((r = launch_with(c, KIND_ADJ_RHS, P, a_cot, a_bar, nullptr, s))) return r;
+    if (c->p.parabolic && (r = launch_with(c, KIND_ADJ_LIFT, P, a_cot, a_bar, a_g, s))) return r;
+    if ((r = launch_with(c, c->p.parabolic ? KIND_ADJ_FACE_NS0 : KIND_ADJ_FACE_E0, P, a_cot, a_gb, a_g, s))) return r;
+    if ((r = launch_with(c, KIND_ADJ_GATHER, P, a_cot, a_bar, nullptr, s))) return r;
     if (!c->p.parabolic && c->bc_used && (r = launch_with(c, KIND_ADJ_BOUNDARY, P, a_cot, a_bar, a_g, s))) return r;
     return PDG_OK;
 }

@@ -19,7 +19,7 @@ enum KernelKind {
     KIND_ADJ_RHS = 12,        // adj_rhs_kernel<dim, N>: adjoint of the inviscid volume terms and blending
     KIND_ADJ_LIFT = 13,       // adj_lift_kernel<dim, N>: adjoint of the viscous terms
     KIND_ADJ_FACE_E0 = 14,    // adj_faces_kernel<dim, N, false>: every direction's adjoint face terms (Euler)
-    KIND_ADJ_FACE_E1 = 15,    // (unused)
+    KIND_ADJ_GATHER = 15,     // adj_gather_kernel<dim, N>: adds the face terms to ubar (+ an RK stage's adjoint)
     KIND_ADJ_FACE_E2 = 16,    // (unused)
     KIND_ADJ_FACE_NS0 = 17,   // adj_faces_kernel<dim, N, true>: the same with the BR1 jumps (NS)
     KIND_ADJ_FACE_NS1 = 18,   // (unused)

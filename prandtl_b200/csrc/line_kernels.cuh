@@ -91,12 +91,11 @@ struct KParams {
     // node: [d][e][v][face node] for the face between e's +d face and its
     // +d neighbour, signed as element e receives it (see face_flux_oriented)
     double *fbuf;
-    // adjoint: face-term cotangents [d][side][e][v][face node] (adj_faces_kernel),
-    // the RK base state's cotangent accumulator of an adjoint stage, and
-    // whether ubar already holds the viscous terms (adj_lift_kernel ran first)
+    // adjoint: face-term cotangents [d][side][e][v][face node]
+    // (adj_faces_kernel) and the RK base state's cotangent accumulator of an
+    // adjoint stage
     const double *gbuf;
     double *bx;
-    int adj_visc;
 };
 
 // Boundary conditions (src/Integrators/BoundaryConditions/): a neighbour
@@ -711,60 +710,9 @@ __device__ __forceinline__ void face_terms_dir(const KParams &P, const double *c
 // face terms include the central viscous flux of both sides' face columns.
 // Each face is thus evaluated twice, once by each of its elements, on the
 // same inputs in the same order, so both get the same value.
-#ifndef PDG_RHS_PREFETCH
-#define PDG_RHS_PREFETCH 1
-#endif
-
-// FB tiles: every block the tile reads after its volume work is brought into
-// L2 at its start — the RK base state and (NS) viscous volume term of the
-// element, its own and its -d neighbours' face-flux blocks and (NS) face
-// columns — and the next tile's state for its first loads.  Items are spread
-// over the element's L lanes; each is one contiguous block.
-template <int DIM, int N, bool NS>
-__device__ __forceinline__ void prefetch_fb_tile(const KParams &P, int64_t e, int64_t e_next, const int32_t *enb, int gl)
-{
-    using S = Shape<DIM, N>;
-    constexpr int NDOF = S::NDOF, NV = S::NV, NFN = S::NFN, L = S::L;
-    constexpr int NFB = 2 * DIM;                       // own + -d neighbours' face-flux blocks
-    constexpr int NFC = NS ? 4 * DIM : 0;              // own 2 DIM + neighbours' 2 DIM face-column blocks
-    constexpr int NVB = NS ? NV - 1 : 0;               // viscous volume term
-    constexpr int ITEMS = NV + NVB + NFB + NFC + NV;   // + next tile's state
-    const int64_t ne = P.ne, nn = P.nnodes;
-    for (int t = gl; t < ITEMS; t += L) {
-        int k = t;
-        if (k < NV) {
-            if (P.stage > 0) prefetch_l2(P.un + (int64_t)k * nn + e * NDOF, sizeof(double) * NDOF);
-            continue;
-        }
-        k -= NV;
-        if (k < NVB) {
-            prefetch_l2(P.vbuf + (int64_t)k * nn + e * NDOF, sizeof(double) * NDOF);
-            continue;
-        }
-        k -= NVB;
-        if (k < NFB) {
-            const int d = k >> 1;
-            const int64_t a = (k & 1) ? (int64_t)enb[2 * d] : e;
-            prefetch_l2(P.fbuf + ((d * ne + a) * NV) * NFN, sizeof(double) * NV * NFN);
-            continue;
-        }
-        k -= NFB;
-        if (k < NFC) {
-            // own (d, side) blocks, then the neighbours' blocks the faces pair them with
-            const int own = k < 2 * DIM, q = own ? k : k - 2 * DIM, d = q >> 1, side = q & 1;
-            const int64_t el = own ? e : (int64_t)enb[2 * d + side];
-            const int sd = own ? side : 1 - side;
-            prefetch_l2(P.fcol + (((d * 2 + sd) * ne + el) * NFN) * (NV - 1), sizeof(double) * NFN * (NV - 1));
-            continue;
-        }
-        k -= NFC;
-        if (e_next >= 0) prefetch_l2(P.u + (int64_t)k * nn + e_next * NDOF, sizeof(double) * NDOF);
-    }
-}
-
 template <int DIM, int N, bool NS, bool FACES, bool PRELOAD = true, bool BDR = false, bool FB = false>
 __device__ __forceinline__ void rhs_tile(const KParams &P, const double *c, double *pr, int64_t e_base, int grp,
-                                         int gl, bool lane_used, unsigned int &flags, double &lam, int64_t e_next = -1)
+                                         int gl, bool lane_used, unsigned int &flags, double &lam)
 {
     using S = Shape<DIM, N>;
     constexpr int Np = S::Np, NDOF = S::NDOF, NV = S::NV, NFN = S::NFN, L = S::L;
@@ -774,22 +722,11 @@ __device__ __forceinline__ void rhs_tile(const KParams &P, const double *c, doub
     const int64_t e0 = e_base + grp;
     const bool valid = lane_used && e0 < P.ne;
     const int64_t e = valid ? e0 : 0;
-    // the face neighbours, requested first (the face phase and, FB, the
-    // prefetch need them)
-    int32_t enb[2 * DIM];
-    if (PRELOAD && FACES) {
-#pragma unroll
-        for (int k = 0; k < 2 * DIM; k++) enb[k] = valid ? __ldg(P.nbr + e * 2 * DIM + k) : 0;
-    }
-    if (FB && PDG_RHS_PREFETCH) {
-        if (valid) prefetch_fb_tile<DIM, N, NS>(P, e, e_next, enb, gl);
-    } else {
-        // the RK base state is first read by the final combine: bring the
-        // element's block of each variable into L2 now
-        if ((!FACES || NS) && valid && P.stage > 0 && gl < NV) prefetch_l2(P.un + (int64_t)gl * P.nnodes + e * NDOF, sizeof(double) * NDOF);
-        if (FACES && NS && valid && gl >= NV && gl < 2 * NV - 1)
-            prefetch_l2(P.vbuf + (int64_t)(gl - NV) * P.nnodes + e * NDOF, sizeof(double) * NDOF);
-    }
+    // the RK base state is first read by the final combine: bring the
+    // element's block of each variable into L2 now
+    if ((!FACES || NS) && valid && P.stage > 0 && gl < NV) prefetch_l2(P.un + (int64_t)gl * P.nnodes + e * NDOF, sizeof(double) * NDOF);
+    if (FACES && NS && valid && gl >= NV && gl < 2 * NV - 1)
+        prefetch_l2(P.vbuf + (int64_t)(gl - NV) * P.nnodes + e * NDOF, sizeof(double) * NDOF);
     if (lane_used) {
         const double ls = stage_nodes<DIM, N>(P, e, valid, gl, pr, scratch, flags);
         if (valid) lam = fmax(lam, ls);
@@ -842,6 +779,12 @@ __device__ __forceinline__ void rhs_tile(const KParams &P, const double *c, doub
     // element-centric faces: combine first (plus the viscous volume term),
     // then add each direction's face terms in turn, then store
     const double coef = stage_coef(P);
+    // the face neighbours, requested before the combine's loads
+    int32_t enb[2 * DIM];
+    if (PRELOAD) {
+#pragma unroll
+        for (int k = 0; k < 2 * DIM; k++) enb[k] = valid ? __ldg(P.nbr + e * 2 * DIM + k) : 0;
+    }
     if (valid) {
 #pragma unroll
         for (int k = 0; k < S::NPL; k++) {
@@ -940,11 +883,8 @@ __global__ void __launch_bounds__(128, RhsOccupancy<DIM, N>::min_blocks) rhs_ker
     const int64_t wstride = (int64_t)gridDim.x * wpb;
     unsigned int flags = 0;
     double lam = 0.0;
-    for (int64_t wt = (int64_t)blockIdx.x * wpb + warp; wt < P.nwt; wt += wstride) {
-        const int64_t en = (wt + wstride) * EPW + grp;
-        rhs_tile<DIM, N, NS, FACES, true, BDR, FB>(P, c, pr, wt * EPW, grp, gl, lane_used, flags, lam,
-                                                   en < P.ne ? en : -1);
-    }
+    for (int64_t wt = (int64_t)blockIdx.x * wpb + warp; wt < P.nwt; wt += wstride)
+        rhs_tile<DIM, N, NS, FACES, true, BDR, FB>(P, c, pr, wt * EPW, grp, gl, lane_used, flags, lam);
     lam = group_max<32>(lam);
     if (lane == 0) atomic_max_pos(P.lam_bits, lam);
     flags = __reduce_or_sync(0xffffffffu, flags);
