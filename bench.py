@@ -491,13 +491,14 @@ def run_adjoint(args, dev):
     fwd = timed(lambda: op.Mult(u, out), reps)
     vjp = timed(lambda: op.vjp(u, cot, out=bar), reps)
     op.profile(True)
-    for k in (pb.KERNEL_ADJ_RHS, pb.KERNEL_ADJ_LIFT, pb.KERNEL_LIFT_FACE) + pb.KERNEL_ADJ_FACE_NS:
+    for k in (pb.KERNEL_ADJ_RHS, pb.KERNEL_ADJ_LIFT, pb.KERNEL_LIFT_FACE, pb.KERNEL_ADJ_GATHER) + pb.KERNEL_ADJ_FACE_NS:
         op.profile_read(k)
     for _ in range(10):
         op.vjp(u, cot, out=bar)
     kernels = {}
     for name, kinds in (("lift_face_kernel", (pb.KERNEL_LIFT_FACE,)), ("adj_rhs_kernel", (pb.KERNEL_ADJ_RHS,)),
-                        ("adj_lift_kernel", (pb.KERNEL_ADJ_LIFT,)), ("adj_face_kernel", pb.KERNEL_ADJ_FACE_NS)):
+                        ("adj_lift_kernel", (pb.KERNEL_ADJ_LIFT,)), ("adj_faces_kernel", pb.KERNEL_ADJ_FACE_NS),
+                        ("adj_gather_kernel", (pb.KERNEL_ADJ_GATHER,))):
         t = sum(op.profile_read(k)[0] for k in kinds)
         kernels[name] = {"ms_per_vjp": t / 10}
     op.profile(False)

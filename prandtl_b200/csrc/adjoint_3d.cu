@@ -14,7 +14,11 @@ template <int N> static bool adj_info_n(int kind, KernelInfo *out)
         out->fn = (const void *)&adj_rhs_kernel<3, N>;
         out->el_doubles = AdjShape<3, N>::EL;
         break;
-    case KIND_ADJ_LIFT: out->fn = (const void *)&adj_lift_kernel<3, N>; out->el_doubles = S::EL_LIFT; break;
+    case KIND_ADJ_LIFT:
+        out->fn = (const void *)&adj_lift_kernel<3, N>;
+        out->el_doubles = S::EL_LIFT;
+        out->wpb = AdjLiftLaunch<3, N>::wpb;
+        break;
     case KIND_ADJ_FACE_E0: out->fn = (const void *)&adj_faces_kernel<3, N, false>; break;
     case KIND_ADJ_FACE_NS0: out->fn = (const void *)&adj_faces_kernel<3, N, true>; break;
     case KIND_ADJ_GATHER: out->fn = (const void *)&adj_gather_kernel<3, N>; break;

@@ -24,6 +24,29 @@
 
 namespace pdg {
 
+// Launch shapes of the adjoint element kernels for 3D N = 3 (the adjoint
+// benchmark's order): the lifting adjoint's 10 KB element slots pack an SM
+// better in blocks of ADJ_LIFT_WPB warps, with the register budget that
+// ADJ_LIFT_MIN_BLOCKS such blocks need.
+#ifndef PDG_ADJ_LIFT_WPB
+#define PDG_ADJ_LIFT_WPB 4
+#endif
+#ifndef PDG_ADJ_LIFT_MIN_BLOCKS
+#define PDG_ADJ_LIFT_MIN_BLOCKS 1
+#endif
+#ifndef PDG_ADJ_RHS_MIN_BLOCKS
+#define PDG_ADJ_RHS_MIN_BLOCKS 1
+#endif
+#ifndef PDG_ADJ_FACES_MIN_BLOCKS
+#define PDG_ADJ_FACES_MIN_BLOCKS 2
+#endif
+template <int DIM, int N> struct AdjLiftLaunch {
+    static constexpr bool tuned = DIM == 3 && N == 3;
+    static constexpr int wpb = tuned ? PDG_ADJ_LIFT_WPB : 4;
+    static constexpr int threads = 32 * wpb;
+    static constexpr int min_blocks = tuned ? PDG_ADJ_LIFT_MIN_BLOCKS : 1;
+};
+
 template <int DIM, int N> struct AdjShape {
     using S = Shape<DIM, N>;
     // slot: primitives (rho, v, beta), cotangent lam, primitive cotangents,
@@ -332,7 +355,7 @@ __device__ __forceinline__ void indicator_vjp(const double *pr, double *pb, doub
 // first kernel of a vector-Jacobian product: stores ubar = cotangent of u
 // through those terms.
 template <int DIM, int N>
-__global__ void __launch_bounds__(128, 3) adj_rhs_kernel(const KParams P, const double *__restrict__ cot,
+__global__ void __launch_bounds__(128, (DIM == 3 && N == 3) ? PDG_ADJ_RHS_MIN_BLOCKS : 1) adj_rhs_kernel(const KParams P, const double *__restrict__ cot,
                                                       double *__restrict__ ubar)
 {
     using S = Shape<DIM, N>;
@@ -438,7 +461,7 @@ __global__ void __launch_bounds__(128, 3) adj_rhs_kernel(const KParams P, const 
 // (lift_face_kernel of u); gcol receives, at every face node, the cotangent
 // of the face-normal entropy-variable gradient ([d][side][e][face node][v]).
 template <int DIM, int N>
-__global__ void __launch_bounds__(128) adj_lift_kernel(const KParams P, const double *__restrict__ cot,
+__global__ void __launch_bounds__(AdjLiftLaunch<DIM, N>::threads, AdjLiftLaunch<DIM, N>::min_blocks) adj_lift_kernel(const KParams P, const double *__restrict__ cot,
                                                        double *__restrict__ ubar, double *__restrict__ gcol)
 {
     using S = Shape<DIM, N>;
@@ -713,7 +736,7 @@ __device__ __forceinline__ void adj_face_node(const KParams &P, const double *c,
 // neighbour's index); adj_rhs_kernel adds them to ubar.  Threads run
 // direction-major inside chunks of 64 elements, as lift_face_kernel.
 template <int DIM, int N, bool NS>
-__global__ void __launch_bounds__(256, 2) adj_faces_kernel(const KParams P, const double *__restrict__ cot,
+__global__ void __launch_bounds__(256, PDG_ADJ_FACES_MIN_BLOCKS) adj_faces_kernel(const KParams P, const double *__restrict__ cot,
                                                         double *__restrict__ gbuf, const double *__restrict__ gcol)
 {
     using S = Shape<DIM, N>;

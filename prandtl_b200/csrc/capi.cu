@@ -294,7 +294,7 @@ int kernel_config(int dim, int N, int kind, int64_t ne, int device, LaunchCfg *c
     }
     const size_t per_warp = (size_t)ki.epw * ki.el_doubles * sizeof(double);
     const size_t base = (size_t)(kind == KIND_FILTER ? CONST_SLOTS : const_slots(Np)) * sizeof(double);
-    int wpb = 4;
+    int wpb = std::max(1, std::min(4, ki.wpb));
     while (wpb > 1 && base + wpb * per_warp > (size_t)max_smem) wpb--;
     if (base + wpb * per_warp > (size_t)max_smem) { *why = "element does not fit in shared memory"; return PDG_ERR_UNSUPPORTED; }
     const size_t smem = base + wpb * per_warp;

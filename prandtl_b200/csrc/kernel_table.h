@@ -45,6 +45,7 @@ struct KernelInfo {
     const void *fn;   // __global__ function, argument: const KParams
     int el_doubles;   // shared doubles per element slot (0: thread-per-face-node kernel)
     int epw;          // elements per warp
+    int wpb = 4;      // warps per block of an element kernel (fewer when shared memory is short)
 };
 
 bool kernel_info_2d(int N, int kind, KernelInfo *out);
