@@ -327,12 +327,13 @@ def run_ours(args):
     stage_bytes = V * (72 + 80 + 80) / 3.0
     achieved = stage_bytes / (stage_ms * 1e-3) / 1e9
     total_kernel_ms = sum(t for t, _ in kernel_ms.values())
-    traffic, traffic_src = None, None
+    traffic, traffic_src, fp64_inst = None, None, None
     tf = os.path.join(ROOT, "profiles", "traffic.json")
     if os.path.exists(tf):
         tj = json.load(open(tf))
-        if tj.get("workload") == config_dict(mesh, 1)["workload"]:
+        if tj.get("workload") == config_dict(mesh, 1)["workload"] and tj.get("compat") == COMPAT:
             traffic = tj.get("dram_bytes_per_stage")
+            fp64_inst = tj.get("fp64_thread_instructions_per_stage")
             traffic_src = tj.get("source")
     roofline = {"bound": "hbm", "kernel": "one NS RK stage: " + ", ".join(kernel_ms),
                 "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
@@ -343,6 +344,15 @@ def run_ours(args):
                                 "launches": c, "share": t / total_kernel_ms if total_kernel_ms else None}
                             for n, (t, c) in kernel_ms.items()},
                 "kernels_note": f"per-launch CUDA events over {prof_steps} plain-launched steps outside the timed region"}
+    if fp64_inst and clocks and clocks.get("sm_mhz"):
+        # the FP64 pipe: DADD, DMUL and DFMA each one issue; 64 per SM per cycle
+        sms = torch.cuda.get_device_properties(dev).multi_processor_count
+        fp64_peak = sms * 64 * clocks["sm_mhz"] * 1e6
+        fp64_rate = fp64_inst / (stage_ms * 1e-3)
+        roofline["fp64"] = {"bound": "fp64", "achieved": fp64_rate / 1e12, "peak": fp64_peak / 1e12,
+                            "unit": "1e12 FP64 thread instructions/s", "frac": fp64_rate / fp64_peak,
+                            "instructions_per_stage": fp64_inst,
+                            "peak_kind": f"{sms} SMs x 64 FP64 lanes x median SM clock of the timed region"}
     out = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
            "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
