@@ -68,7 +68,7 @@ typedef struct pdg_params {
     int32_t compat;           /* 1: reproduce the reference's value-changing quirks
                                  (stale viscous state, z-flux fill, 3D face
                                  dissipation term, running max wave speed) */
-    int32_t filter;           /* entropy/positivity filter after every RK stage */
+    int32_t filter;           /* after every RK stage: bit 1 the entropy filter, bit 2 the positivity limiter */
     double gamma;             /* ratio of specific heats */
     double Pr;                /* Prandtl number */
     double mu;                /* constant dynamic viscosity */
@@ -101,8 +101,11 @@ void pdg_default_params(pdg_params *p);
  * fields, error word) on the current device.  Two environment switches,
  * read here, exist for measurements: PDG_ELEMENT_FACES=0 makes the fixed
  * operator use the separate face kernels instead of face terms inside the
- * volume kernel (same results to rounding), PDG_PREFETCH=0 turns off the
- * lifting kernel's L2 prefetch of the next element. */
+ * volume kernel (same results to rounding), PDG_FACE_BUFFER=0 has each
+ * element evaluate its own faces' inviscid fluxes instead of reading the
+ * face buffer that the face-node kernel fills once per face (same results to
+ * rounding), PDG_PREFETCH=0 turns off the lifting kernel's L2 prefetch of
+ * the next element. */
 int pdg_create(const pdg_mesh *mesh, const pdg_params *params, pdg_ctx **out);
 int pdg_destroy(pdg_ctx *ctx);
 
@@ -189,7 +192,8 @@ int pdg_rhs_host(pdg_ctx *ctx, const double *u_host, double *dudt_host);
  *   stage 0: uout = us + dt*L(us)                       (us = un)
  *   stage 1: uout = 3/4 un + 1/4 (us + dt*L(us))
  *   stage 2: uout = 1/3 un + 2/3 (us + dt*L(us))
- * followed by the entropy filter when params.filter is set.  DEVICE pointers;
+ * followed by the entropy filter and/or the positivity limiter that
+ * params.filter selects.  DEVICE pointers;
  * uout may alias neither un nor us. */
 int pdg_rk_stage(pdg_ctx *ctx, int stage, double dt, const double *un,
                  const double *us, double *uout, void *stream);
@@ -258,13 +262,23 @@ int pdg_rhs_vjp(pdg_ctx *ctx, const double *u, const double *cot, double *ubar, 
 int pdg_rk_stage_vjp(pdg_ctx *ctx, int stage, double dt, const double *us, const double *lam, double *out,
                      double *bx, void *stream);
 
-/* Entropy filter (params.filter = 1): EntropyFilter::FilterSolution
+/* Entropy filter (params.filter & 1): EntropyFilter::FilterSolution
  * (src/Filters/EntropyFilter.cpp:171-242) after every RK stage, with the
  * element bounds of GetEntropyConstraints (:81-158) taken at the stage input.
  * Applies to pdg_rk_stage / pdg_rk3_step*; pdg_rhs is never filtered.
  * pdg_filter_count returns the number of element filterings since creation
  * (synchronises). */
 int pdg_filter_count(pdg_ctx *ctx, int64_t *filtered);
+
+/* Positivity limiter (params.filter & 2), after the entropy filter when both
+ * are set.  The reference's MinmodLimiter (src/Limiters/MinmodLimiter.cpp:
+ * 22-77) limits nothing and it has no positivity limiter; this is the
+ * conservative limiter of Zhang & Shu (2010) with the pressure step of Zhang,
+ * Xia & Shu (2012): each element's nodes are contracted towards its LGL mean
+ * until density and pressure are at least min(1e-13, mean density, mean
+ * pressure).  pdg_limiter_count returns the number of element limitings
+ * since creation (synchronises). */
+int pdg_limiter_count(pdg_ctx *ctx, int64_t *limited);
 
 /* Reads and clears the device error word (PDG_FLAG_*).  Synchronises. */
 int pdg_check(pdg_ctx *ctx, uint32_t *flags);
@@ -290,8 +304,9 @@ int64_t pdg_launch_count(const pdg_ctx *ctx);
 #define PDG_KERNEL_FILTER    11  /* entropy filter of a stage output */
 #define PDG_KERNEL_ADJ_RHS   12  /* adjoint: inviscid volume terms and blending */
 #define PDG_KERNEL_ADJ_LIFT  13  /* adjoint: viscous terms */
-#define PDG_KERNEL_ADJ_FACE_E0  14  /* adjoint Euler face kernels, x / y / z (14, 15, 16) */
-#define PDG_KERNEL_ADJ_FACE_NS0 17  /* adjoint Navier-Stokes face kernels (17, 18, 19) */
+#define PDG_KERNEL_ADJ_FACE_E0  14  /* adjoint Euler face terms, every direction */
+#define PDG_KERNEL_ADJ_GATHER   15  /* adjoint: face terms added to the output (+ the RK stage's adjoint) */
+#define PDG_KERNEL_ADJ_FACE_NS0 17  /* adjoint Navier-Stokes face terms, every direction */
 #define PDG_KERNEL_EULER_FACES 20   /* Euler volume + face terms (+ stage), fixed operator */
 #define PDG_KERNEL_NS_FACES  21     /* Navier-Stokes inviscid volume + all face terms (+ stage), fixed operator */
 #define PDG_KERNEL_BOUNDARY  22     /* boundary faces of the separate-face path (Euler) */
@@ -302,6 +317,11 @@ int64_t pdg_launch_count(const pdg_ctx *ctx);
 #define PDG_KERNEL_NS_FACES_BDR 27   /* volume kernel with element-side faces */
 #define PDG_KERNEL_BOUNDARY_NS 28    /* boundary faces of the separate-face path (Navier-Stokes) */
 #define PDG_KERNEL_LIFT_BDR_PTTT 29  /* lifting kernel of a 2D mesh with a total-pressure inflow */
+#define PDG_KERNEL_NS_FACES_FB 30    /* Navier-Stokes volume + face terms reading the face buffer (periodic, fixed) */
+#define PDG_KERNEL_EULER_FACES_FB 31 /* Euler volume + face terms reading the face buffer (periodic, fixed) */
+#define PDG_KERNEL_LIFT_FACE_FLUX 32 /* face-node kernel: BR1 jumps + inviscid face fluxes into the buffer */
+#define PDG_KERNEL_FACE_FLUX 33      /* face-node kernel: inviscid face fluxes into the buffer (Euler) */
+#define PDG_KERNEL_POSITIVITY 34     /* positivity limiter of a stage output */
 int pdg_profile_enable(pdg_ctx *ctx, int on);
 int pdg_profile_read(pdg_ctx *ctx, int kind, double *total_ms, int64_t *launches);
 

@@ -75,6 +75,9 @@ def lib(fma: bool = False):
         L.orc_get_gradients.argtypes = [C.c_void_p, _dp]
         L.orc_filtered_elements.restype = C.c_int64
         L.orc_filtered_elements.argtypes = [C.c_void_p]
+        L.orc_limited_elements.restype = C.c_int64
+        L.orc_limited_elements.argtypes = [C.c_void_p]
+        L.orc_positivity_apply.argtypes = [C.c_void_p, _dp]
         L.orc_gll.argtypes = [C.c_int, _dp, _dp]
         L.orc_derivative_matrices.argtypes = [C.c_int, _dp, _dp, _dp]
         L.orc_logmean.restype = C.c_double
@@ -155,6 +158,16 @@ class Oracle:
 
     def filtered_elements(self) -> int:
         return self._L.orc_filtered_elements(self.h)
+
+    def limited_elements(self) -> int:
+        """Positivity-limiter applications (params filter & 2) so far."""
+        return self._L.orc_limited_elements(self.h)
+
+    def positivity(self, u: np.ndarray) -> np.ndarray:
+        """The positivity limiter alone applied to a copy of u."""
+        x = np.array(u, dtype=np.float64, copy=True)
+        self._L.orc_positivity_apply(self.h, _ptr(x))
+        return x
 
 
 _ref_libs = {}

@@ -397,6 +397,7 @@ struct Ctx {
     double last_rhs_speed;              // max of the last RHS
     std::vector<double> k1, y1, z1;     // RK scratch
     int64_t filtered_elements;
+    int64_t limited_elements;           // positivity limiter applications
     double bc[16][8] = {};              // boundary conditions: type, prescribed state
 };
 
@@ -1419,30 +1420,88 @@ static void filter_apply(Ctx &c, double *x)
     c.filtered_elements += nf;
 }
 
+// ---------------------------------------------------------------------------
+// Positivity-preserving limiter (params.filter & 2).  The reference's
+// MinmodLimiter::LimitSolution limits nothing (src/Limiters/MinmodLimiter.cpp:
+// 22-77) and no positivity limiter exists there; this restates the published
+// one of Zhang & Shu (J. Comput. Phys. 229 (2010) 8918-8934): per element,
+// with the LGL means u_bar and eps = min(1e-13, rho_bar, p(u_bar)),
+//   (1) rho_i <- rho_bar + th1 (rho_i - rho_bar), th1 = (rho_bar - eps) /
+//       (rho_bar - min rho_i), when min rho_i < eps;
+//   (2) u_i <- u_bar + th2 (u_i - u_bar), th2 = min over nodes with
+//       p(u_i) < eps of (p_bar - eps) / (p_bar - p(u_i)): p is concave in u,
+//       so p(u_bar + th (u_i - u_bar)) >= (1 - th) p_bar + th p(u_i) = eps.
+// Element means are unchanged, so the limiter conserves.
+// ---------------------------------------------------------------------------
+static void positivity_apply(Ctx &c, double *x)
+{
+    const int nv = c.nv, nd = c.ndof, dim = c.dim, Np = c.Np;
+    int64_t nl = 0;
+#pragma omp parallel for schedule(static) reduction(+ : nl)
+    for (int64_t e = 0; e < c.ne; e++) {
+        double m[5] = {0, 0, 0, 0, 0}, W = 0.0, rmin = std::numeric_limits<double>::infinity();
+        for (int n = 0; n < nd; n++) {
+            double wn = c.w[n % Np] * c.w[(n / Np) % Np];
+            if (dim == 3) wn *= c.w[n / (Np * Np)];
+            W += wn;
+            for (int v = 0; v < nv; v++) m[v] += wn * x[idx(c, v, e, n)];
+            rmin = std::min(rmin, x[idx(c, 0, e, n)]);
+        }
+        for (int v = 0; v < nv; v++) m[v] /= W;
+        const double eps = std::min(1e-13, std::min(m[0], pressure(dim, c.p.gamma, m)));
+        bool limited = false;
+        if (rmin < eps) {
+            const double th = (m[0] - eps) / (m[0] - rmin);
+            for (int n = 0; n < nd; n++) x[idx(c, 0, e, n)] = m[0] + th * (x[idx(c, 0, e, n)] - m[0]);
+            limited = true;
+        }
+        const double pbar = pressure(dim, c.p.gamma, m);
+        double th2 = 1.0, s[5];
+        for (int n = 0; n < nd; n++) {
+            for (int v = 0; v < nv; v++) s[v] = x[idx(c, v, e, n)];
+            const double p = pressure(dim, c.p.gamma, s);
+            if (p < eps) th2 = std::min(th2, (pbar - eps) / (pbar - p));
+        }
+        if (th2 < 1.0) {
+            for (int n = 0; n < nd; n++)
+                for (int v = 0; v < nv; v++) x[idx(c, v, e, n)] = m[v] + th2 * (x[idx(c, v, e, n)] - m[v]);
+            limited = true;
+        }
+        nl += limited;
+    }
+    c.limited_elements += nl;
+}
+
 // RK3SSPSolver::Step (Shu-Osher SSP-RK3), optionally filtering each stage.
 static void rk3_step(Ctx &c, double dt, double *x)
 {
     const int64_t n = c.size;
     double *k = c.k1.data(), *y = c.y1.data(), *z = c.z1.data();
-    if (c.p.filter) filter_bounds(c, x);
+    const bool ef = c.p.filter & 1, pl = c.p.filter & 2;
+    if (ef) filter_bounds(c, x);
     rhs(c, x, k);
 #pragma omp parallel for schedule(static)
     for (int64_t i = 0; i < n; i++) y[i] = x[i] + dt * k[i];
-    if (c.p.filter) { filter_apply(c, y); filter_bounds(c, y); }
+    if (ef) filter_apply(c, y);
+    if (pl) positivity_apply(c, y);
+    if (ef) filter_bounds(c, y);
     rhs(c, y, k);
 #pragma omp parallel for schedule(static)
     for (int64_t i = 0; i < n; i++) {
         z[i] = y[i] + dt * k[i];
         y[i] = 3. / 4 * x[i] + 1. / 4 * z[i];
     }
-    if (c.p.filter) { filter_apply(c, y); filter_bounds(c, y); }
+    if (ef) filter_apply(c, y);
+    if (pl) positivity_apply(c, y);
+    if (ef) filter_bounds(c, y);
     rhs(c, y, k);
 #pragma omp parallel for schedule(static)
     for (int64_t i = 0; i < n; i++) {
         z[i] = y[i] + dt * k[i];
         x[i] = 1. / 3 * x[i] + 2. / 3 * z[i];
     }
-    if (c.p.filter) filter_apply(c, x);
+    if (ef) filter_apply(c, x);
+    if (pl) positivity_apply(c, x);
 }
 
 }  // namespace orc
@@ -1506,6 +1565,7 @@ void *orc_create(const pdg_mesh *m, const pdg_params *p)
     c->max_char_speed = -1.0;
     c->last_rhs_speed = -1.0;
     c->filtered_elements = 0;
+    c->limited_elements = 0;
     return c;
 }
 
@@ -1558,6 +1618,8 @@ void orc_get_gradients(void *h, double *g)
 }
 
 int64_t orc_filtered_elements(void *h) { return ((Ctx *)h)->filtered_elements; }
+int64_t orc_limited_elements(void *h) { return ((Ctx *)h)->limited_elements; }
+void orc_positivity_apply(void *h, double *u) { orc::positivity_apply(*(Ctx *)h, u); }
 
 void orc_filter_bounds(void *h, const double *u) { orc::filter_bounds(*(Ctx *)h, u); }
 void orc_filter_apply(void *h, double *u) { orc::filter_apply(*(Ctx *)h, u); }
@@ -1566,7 +1628,7 @@ void orc_filter_apply(void *h, double *u) { orc::filter_apply(*(Ctx *)h, u); }
 void orc_rk_stage(void *h, int stage, double dt, const double *un, const double *us, double *uout)
 {
     Ctx *c = (Ctx *)h;
-    if (c->p.filter) orc::filter_bounds(*c, us);
+    if (c->p.filter & 1) orc::filter_bounds(*c, us);
     orc::rhs(*c, us, c->k1.data());
     const double *k = c->k1.data();
 #pragma omp parallel for schedule(static)
@@ -1576,7 +1638,8 @@ void orc_rk_stage(void *h, int stage, double dt, const double *un, const double 
         else if (stage == 1) uout[i] = 3. / 4 * un[i] + 1. / 4 * z;
         else uout[i] = 1. / 3 * un[i] + 2. / 3 * z;
     }
-    if (c->p.filter) orc::filter_apply(*c, uout);
+    if (c->p.filter & 1) orc::filter_apply(*c, uout);
+    if (c->p.filter & 2) orc::positivity_apply(*c, uout);
 }
 
 void orc_gll(int Np, double *x, double *w)

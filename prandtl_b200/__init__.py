@@ -43,6 +43,9 @@ KERNEL_EULER_FACES, KERNEL_NS_FACES, KERNEL_BOUNDARY, KERNEL_ADJ_BOUNDARY, KERNE
 KERNEL_LIFT_FACE_BDR, KERNEL_LIFT_BDR, KERNEL_NS_FACES_BDR, KERNEL_BOUNDARY_NS = 25, 26, 27, 28
 KERNEL_LIFT_BDR_PTTT = 29
 KERNEL_NS_FACES_FB, KERNEL_EULER_FACES_FB, KERNEL_LIFT_FACE_FLUX, KERNEL_FACE_FLUX = 30, 31, 32, 33
+KERNEL_POSITIVITY = 34
+# params.filter bits
+FILTER_ENTROPY, FILTER_POSITIVITY = 1, 2
 # boundary condition types (pdg_set_boundary)
 BC_SUPERSONIC_INFLOW, BC_SUPERSONIC_OUTFLOW, BC_SPECIFIED_STATE, BC_SLIP_WALL, BC_SYMMETRY = 1, 2, 3, 4, 5
 BC_SUBSONIC_OUTFLOW_P, BC_SUBSONIC_INFLOW_RV, BC_SUBSONIC_INFLOW_PTTT, BC_RIEMANN_INVARIANT = 6, 7, 8, 9
@@ -126,6 +129,7 @@ def library():
     L.pdg_batch_last_error.restype = C.c_char_p
     L.pdg_batch_last_error.argtypes = [vp]
     L.pdg_filter_count.argtypes = [C.c_void_p, C.POINTER(C.c_int64)]
+    L.pdg_limiter_count.argtypes = [C.c_void_p, C.POINTER(C.c_int64)]
     L.pdg_rhs_vjp.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
     L.pdg_rk_stage_vjp.argtypes = [C.c_void_p, C.c_int, C.c_double, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                                    C.c_void_p]
@@ -158,8 +162,9 @@ class DGSEMOperator:
 
     Parameters mirror the reference's compile-time flags and runtime keys:
     ``parabolic`` (PARABOLIC), ``blending`` (SUBCELL_FV_BLENDING), ``compat``
-    (reproduce the reference's value-changing quirks), ``filter`` (entropy
-    filter after each RK stage), ``gamma``, ``Pr``, ``mu``, ``alpha_max``,
+    (reproduce the reference's value-changing quirks), ``filter`` (after
+    each RK stage: 1 the entropy filter, 2 the positivity limiter, 3 both),
+    ``gamma``, ``Pr``, ``mu``, ``alpha_max``,
     ``alpha_min``, ``face_dissipation``.
     """
 
@@ -332,6 +337,12 @@ class DGSEMOperator:
         """Element filterings by the entropy filter since creation (synchronises)."""
         n = C.c_int64()
         self._call(library().pdg_filter_count(self._ctx, C.byref(n)), "pdg_filter_count")
+        return n.value
+
+    def limiter_count(self) -> int:
+        """Element limitings by the positivity limiter since creation (synchronises)."""
+        n = C.c_int64()
+        self._call(library().pdg_limiter_count(self._ctx, C.byref(n)), "pdg_limiter_count")
         return n.value
 
     def launch_count(self) -> int:

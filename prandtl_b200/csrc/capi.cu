@@ -54,6 +54,7 @@ struct pdg_ctx {
     unsigned int *err = nullptr;
     double *ent_own = nullptr;                // filter: per-element entropy minimum at the stage input
     unsigned long long *filter_count = nullptr;
+    unsigned long long *limit_count = nullptr;  // positivity limiter applications
     double *gcol = nullptr;   // adjoint: cotangents of the face-normal entropy gradients
     double *gbuf = nullptr;   // adjoint: face-term cotangents of both sides of every face node
     // pdg_rk3_steps: one step captured in a CUDA graph for a (state, dt) pair
@@ -273,7 +274,7 @@ int kernel_config(int dim, int N, int kind, int64_t ne, int device, LaunchCfg *c
     }
     const int Np = N + 1, nfn = dim == 2 ? Np : Np * Np;
     if (ki.el_doubles == 0) {  // thread-per-face-node kernel
-        const int64_t threads = kind == KIND_FILTER_BOUNDS ? 32 * ne
+        const int64_t threads = (kind == KIND_FILTER_BOUNDS || kind == KIND_POSITIVITY) ? 32 * ne
                                 : (kind == KIND_BOUNDARY || kind == KIND_ADJ_BOUNDARY || kind == KIND_BOUNDARY_NS) ? ne
                                 : kind == KIND_ADJ_GATHER ? ne * nfn * (N + 1)  // thread per node
                                 : ((kind == KIND_LIFT_FACE || kind == KIND_LIFT_FACE_BDR || kind == KIND_LIFT_FACE_FLUX ||
@@ -316,9 +317,10 @@ int kernel_config(int dim, int N, int kind, int64_t ne, int device, LaunchCfg *c
     return PDG_OK;
 }
 
-bool kind_used(int kind, int dim, bool parabolic, bool filter)
+bool kind_used(int kind, int dim, bool parabolic, int filter)
 {
-    if (kind == KIND_FILTER_BOUNDS || kind == KIND_FILTER) return filter;
+    if (kind == KIND_FILTER_BOUNDS || kind == KIND_FILTER) return filter & 1;
+    if (kind == KIND_POSITIVITY) return (filter & 2) != 0;
     if ((kind >= KIND_ADJ_RHS && kind <= KIND_ADJ_FACE_NS2) || kind == KIND_ADJ_BOUNDARY)
         return false;  // configured by the first pdg_rhs_vjp
     const bool ns_kind = kind == KIND_NS || kind == KIND_NS_FACES || kind == KIND_LIFT || kind == KIND_LIFT_FACE ||
@@ -378,6 +380,7 @@ KParams base_params(pdg_ctx *c)
     P.err = c->err;
     P.ent_own = c->ent_own;
     P.filter_count = c->filter_count;
+    P.limit_count = c->limit_count;
     P.ne = c->ne;
     P.nnodes = c->nnodes;
     P.stage = -1;
@@ -506,7 +509,7 @@ int evaluate(pdg_ctx *c, int stage, double dt, const double *un, const double *u
     int r;
     const bool element_faces = c->element_faces && !c->p.compat;
     if (c->p.parabolic) {
-        if (c->p.filter && stage >= 0 && (r = launch(c, KIND_FILTER_BOUNDS, P, s))) return r;
+        if ((c->p.filter & 1) && stage >= 0 && (r = launch(c, KIND_FILTER_BOUNDS, P, s))) return r;
         if (c->bc_used) {
             // Navier-Stokes boundary faces: the conditions with a viscous boundary flux
             // slip wall and symmetry have no viscous flux in the reference
@@ -550,7 +553,7 @@ int evaluate(pdg_ctx *c, int stage, double dt, const double *un, const double *u
                 if ((r = launch(c, KIND_FACE_NS0 + d, P, s))) return r;
         }
     } else {
-        if (c->p.filter && stage >= 0 && (r = launch(c, KIND_FILTER_BOUNDS, P, s))) return r;
+        if ((c->p.filter & 1) && stage >= 0 && (r = launch(c, KIND_FILTER_BOUNDS, P, s))) return r;
         if (element_faces && c->fbuf) {
             if ((r = launch(c, KIND_FACE_FLUX, P, s))) return r;
             if ((r = launch(c, KIND_EULER_FACES_FB, P, s))) return r;
@@ -563,8 +566,10 @@ int evaluate(pdg_ctx *c, int stage, double dt, const double *un, const double *u
             if (c->bc_used && (r = launch(c, KIND_BOUNDARY, P, s))) return r;
         }
     }
-    // entropy filter of the stage output (EntropyFilter::FilterSolution)
-    if (c->p.filter && stage >= 0 && (r = launch(c, KIND_FILTER, P, s))) return r;
+    // entropy filter of the stage output (EntropyFilter::FilterSolution), then
+    // the positivity limiter
+    if ((c->p.filter & 1) && stage >= 0 && (r = launch(c, KIND_FILTER, P, s))) return r;
+    if ((c->p.filter & 2) && stage >= 0 && (r = launch(c, KIND_POSITIVITY, P, s))) return r;
     return PDG_OK;
 }
 
@@ -596,6 +601,7 @@ int pdg_create(const pdg_mesh *mesh, const pdg_params *params, pdg_ctx **out)
     if ((mesh->dim != 2 && mesh->dim != 3) || mesh->order < 1 || mesh->order > 5 || mesh->num_elements < 1)
         return PDG_ERR_ARG;
     if (!(params->gamma > 1.0) || (params->parabolic && !(params->Pr > 0.0))) return PDG_ERR_ARG;
+    if (params->filter < 0 || params->filter > 3) return PDG_ERR_ARG;
     pdg_ctx *c = new pdg_ctx();
     c->p = *params;
     c->dim = mesh->dim;
@@ -636,10 +642,15 @@ int pdg_create(const pdg_mesh *mesh, const pdg_params *params, pdg_ctx **out)
         cudaMalloc(&c->bc, sizeof(double) * PDG_MAX_BOUNDARIES * BC_SLOT))
         return cleanup(PDG_ERR_NOMEM);
     if (cudaMemset(c->bc, 0, sizeof(double) * PDG_MAX_BOUNDARIES * BC_SLOT) != cudaSuccess) return cleanup(PDG_ERR_CUDA);
-    if (c->p.filter) {
+    if (c->p.filter & 1) {
         if (cudaMalloc(&c->ent_own, sizeof(double) * c->ne) != cudaSuccess ||
             cudaMalloc(&c->filter_count, sizeof(unsigned long long)) != cudaSuccess ||
             cudaMemset(c->filter_count, 0, sizeof(unsigned long long)) != cudaSuccess)
+            return cleanup(PDG_ERR_NOMEM);
+    }
+    if (c->p.filter & 2) {
+        if (cudaMalloc(&c->limit_count, sizeof(unsigned long long)) != cudaSuccess ||
+            cudaMemset(c->limit_count, 0, sizeof(unsigned long long)) != cudaSuccess)
             return cleanup(PDG_ERR_NOMEM);
     }
     if (c->element_faces && c->face_buffer && !c->p.compat && !c->bc_used) {
@@ -661,7 +672,7 @@ int pdg_create(const pdg_mesh *mesh, const pdg_params *params, pdg_ctx **out)
         cudaMemset(c->lam_bits, 0, sizeof(unsigned long long)) || cudaMemset(c->err, 0, sizeof(unsigned int)))
         return cleanup(PDG_ERR_CUDA);
     for (int kind = 0; kind < KIND_COUNT; kind++) {
-        if (!kind_used(kind, c->dim, c->p.parabolic != 0, c->p.filter != 0)) continue;
+        if (!kind_used(kind, c->dim, c->p.parabolic != 0, c->p.filter)) continue;
         int r = configure_launch(c, kind);
         if (r) return cleanup(r);
     }
@@ -750,6 +761,7 @@ int pdg_destroy(pdg_ctx *c)
     if (c->graph) cudaGraphDestroy(c->graph);
     if (c->cap) cudaStreamDestroy(c->cap);
     cudaFree(c->filter_count);
+    cudaFree(c->limit_count);
     for (auto &t : c->timed) {
         cudaEventDestroy(t.a);
         cudaEventDestroy(t.b);
@@ -1044,10 +1056,24 @@ int pdg_rk_stage_vjp(pdg_ctx *c, int stage, double dt, const double *us, const d
     return vjp(c, stage, dt, us, lam, out, bx, (cudaStream_t)stream);
 }
 
+int pdg_limiter_count(pdg_ctx *c, int64_t *limited)
+{
+    if (!c || !limited) return PDG_ERR_ARG;
+    if (!(c->p.filter & 2)) {
+        *limited = 0;
+        return PDG_OK;
+    }
+    unsigned long long n = 0;
+    CK(cudaStreamSynchronize(c->last_stream), "synchronize");
+    CK(cudaMemcpy(&n, c->limit_count, sizeof(n), cudaMemcpyDeviceToHost), "read limiter count");
+    *limited = (int64_t)n;
+    return PDG_OK;
+}
+
 int pdg_filter_count(pdg_ctx *c, int64_t *filtered)
 {
     if (!c || !filtered) return PDG_ERR_ARG;
-    if (!c->p.filter) {
+    if (!(c->p.filter & 1)) {
         *filtered = 0;
         return PDG_OK;
     }

@@ -220,3 +220,87 @@ __global__ void __launch_bounds__(128) filter_kernel(const KParams P)
 }
 
 }  // namespace pdg
+
+namespace pdg {
+
+// ---------------------------------------------------------------------------
+// Positivity-preserving limiter after an RK stage (params.filter & 2).  The
+// reference's MinmodLimiter::LimitSolution limits nothing
+// (src/Limiters/MinmodLimiter.cpp:22-77) and it has no positivity limiter;
+// this is the published limiter of Zhang & Shu (J. Comput. Phys. 229 (2010)
+// 8918-8934).  Per element, with the LGL means u_bar and
+// eps = min(1e-13, rho_bar, p(u_bar)):
+//   (1) rho_i <- rho_bar + th1 (rho_i - rho_bar), th1 = (rho_bar - eps) /
+//       (rho_bar - min rho_i), when min rho_i < eps;
+//   (2) u_i <- u_bar + th2 (u_i - u_bar), th2 = min over nodes with
+//       p(u_i) < eps of (p_bar - eps) / (p_bar - p(u_i)), which the concavity
+//       of p in u makes a lower bound of p along the contraction (the exact
+//       root of p = eps is ill-conditioned where step (1) left a node almost
+//       empty, and its rounding can leave p below zero).
+// The means are unchanged, so the limiter conserves; nodes of an element it
+// leaves alone keep their bits.
+// ---------------------------------------------------------------------------
+constexpr double POSITIVITY_EPS = 1e-13;
+
+// One warp per element over the stage output P.out (in place); counts the
+// elements it changes in P.limit_count.
+template <int DIM, int N>
+__global__ void __launch_bounds__(256) positivity_kernel(const KParams P)
+{
+    using S = Shape<DIM, N>;
+    constexpr int Np = S::Np, NDOF = S::NDOF, NV = S::NV;
+    __shared__ double w[8];
+    if (threadIdx.x < Np) w[threadIdx.x] = P.K->w[threadIdx.x];
+    __syncthreads();
+    const int lane = threadIdx.x & 31;
+    const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
+    const int64_t nn = P.nnodes;
+    const double inf = __longlong_as_double(0x7ff0000000000000LL);
+    unsigned long long limited = 0;
+    for (int64_t e = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); e < P.ne; e += warps) {
+        double *x = P.out + e * NDOF;
+        double m[NV], W = 0.0, rmin = inf;
+#pragma unroll
+        for (int v = 0; v < NV; v++) m[v] = 0.0;
+        for (int n = lane; n < NDOF; n += 32) {
+            double wn = w[n % Np] * w[(n / Np) % Np];
+            if (DIM == 3) wn *= w[n / (Np * Np)];
+            W += wn;
+#pragma unroll
+            for (int v = 0; v < NV; v++) m[v] += wn * x[v * nn + n];
+            rmin = fmin(rmin, x[n]);
+        }
+        W = group_sum<32>(W);
+#pragma unroll
+        for (int v = 0; v < NV; v++) m[v] = group_sum<32>(m[v]) / W;
+        rmin = group_max<32>(-rmin) * -1.0;
+        const double pbar = filter_pressure<DIM>(m, P.gm1);
+        const double eps = fmin(POSITIVITY_EPS, fmin(m[0], pbar));
+        bool lim = false;
+        if (rmin < eps) {
+            const double th = (m[0] - eps) / (m[0] - rmin);
+            for (int n = lane; n < NDOF; n += 32) x[n] = m[0] + th * (x[n] - m[0]);
+            lim = true;
+        }
+        double th2 = 1.0;
+        for (int n = lane; n < NDOF; n += 32) {
+            double s[NV];
+#pragma unroll
+            for (int v = 0; v < NV; v++) s[v] = x[v * nn + n];
+            const double p = filter_pressure<DIM>(s, P.gm1);
+            if (p < eps) th2 = fmin(th2, (pbar - eps) / (pbar - p));
+        }
+        th2 = -group_max<32>(-th2);
+        if (th2 < 1.0) {
+            for (int n = lane; n < NDOF; n += 32)
+#pragma unroll
+                for (int v = 0; v < NV; v++) x[v * nn + n] = m[v] + th2 * (x[v * nn + n] - m[v]);
+            lim = true;
+        }
+        if (lane == 0 && lim) limited++;
+        __syncwarp();
+    }
+    if (lane == 0 && limited) atomicAdd(P.limit_count, limited);
+}
+
+}  // namespace pdg

@@ -30,7 +30,7 @@ void fill_constants(int dim, int N, const double *h, DevConst &K, double &modal_
 int kernel_config(int dim, int N, int kind, int64_t ne, int device, LaunchCfg *cfg, const char **why);
 
 // Whether a kernel kind takes part in the (dim, parabolic, filter) operator.
-bool kind_used(int kind, int dim, bool parabolic, bool filter);
+bool kind_used(int kind, int dim, bool parabolic, int filter);  // filter: params.filter bits
 
 int launch_kernel(const LaunchCfg &cfg, KParams P, int64_t ne, cudaStream_t s);
 

@@ -38,7 +38,8 @@ enum KernelKind {
     KIND_EULER_FACES_FB = 31,   // rhs_kernel<dim, N, false, true, false, true>: KIND_EULER_FACES reading it
     KIND_LIFT_FACE_FLUX = 32,   // lift_face_kernel<dim, N, false, FACE_JUMP | FACE_FLUX>: jumps + face fluxes (NS)
     KIND_FACE_FLUX = 33,        // lift_face_kernel<dim, N, false, FACE_FLUX>: face fluxes (Euler)
-    KIND_COUNT = 34
+    KIND_POSITIVITY = 34,       // positivity_kernel<dim, N>: positivity limiter of the stage output
+    KIND_COUNT = 35
 };
 
 struct KernelInfo {

@@ -48,6 +48,7 @@ template <int N> static bool info_n(int kind, KernelInfo *out)
     case KIND_FACE_NS1: out->fn = (const void *)&face_kernel<2, N, 1, true>; break;
     
     case KIND_FILTER_BOUNDS: out->fn = (const void *)&filter_bounds_kernel<2, N>; out->epw = 1; break;
+    case KIND_POSITIVITY: out->fn = (const void *)&positivity_kernel<2, N>; out->epw = 1; break;
     case KIND_FILTER:
         out->fn = (const void *)&filter_kernel<2, N>;
         out->el_doubles = FilterShape<2, N>::EL;

@@ -74,6 +74,7 @@ struct KParams {
     unsigned int *err;
     double *ent_own;                    // filter: per-element entropy minimum at the stage input
     unsigned long long *filter_count;   // filter: elements filtered so far
+    unsigned long long *limit_count;    // positivity limiter: elements limited so far
     int64_t ne, nnodes;
     int64_t nwt;          // number of warp tiles
     int stage;            // -1: plain RHS; 0, 1, 2: SSP-RK3 stage

@@ -1,0 +1,140 @@
+"""Positivity-preserving limiter (params.filter & 2) after RK stages.
+
+The reference's MinmodLimiter limits nothing (src/Limiters/MinmodLimiter.cpp:
+22-77) and it has no positivity limiter, so the oracle restates the published
+limiter of Zhang & Shu (2010) with the pressure step of Zhang, Xia & Shu
+(2012).  CPU tests check the oracle's limiter for what the method guarantees:
+element means unchanged (conservation), positive density and pressure at
+every node afterwards, and elements without a violation left bit for bit.
+GPU tests compare the CUDA limiter with the oracle after RK stages that
+produce negative densities and pressures (rough states at large CFL), at
+1e-12 relative in max norm with equal limiting counts, alone and after the
+entropy filter, and on the Kelvin-Helmholtz benchmark mesh (64 x 64, N = 4),
+whose configuration runs both.
+"""
+import numpy as np
+import pytest
+
+import oracle
+import prandtl_b200 as pb
+from prandtl_b200 import cases
+from prandtl_b200.mesh import gll_nodes, periodic_box
+
+from helpers import rel_maxnorm, rough
+
+TOL = 1e-12
+GAMMA = 1.4
+
+
+def _pressure(u, dim, nn):
+    U = u.reshape(dim + 2, nn)
+    return (GAMMA - 1.0) * (U[-1] - 0.5 * np.sum(U[1:1 + dim] ** 2, axis=0) / U[0])
+
+
+def _means(u, mesh):
+    _, w1 = gll_nodes(mesh.Np)
+    wq = w1
+    for _ in range(mesh.dim - 1):
+        wq = np.kron(w1, wq)
+    U = u.reshape(mesh.nv, mesh.num_elements, mesh.ndof)
+    return np.einsum("ven,n->ve", U, wq) / wq.sum()
+
+
+def _case(kind, order):
+    if kind == "kh2d":
+        m = periodic_box(2, order, (8, 9), -1.0, 1.0)
+        return m, rough(cases.kelvin_helmholtz(m), m, 3, 0.15, 0.03), dict(parabolic=0)
+    m = periodic_box(3, order, (4, 3, 5), 0.0, 2 * np.pi)
+    u = rough(cases.taylor_green(m), m, 5, 0.15, 0.05)
+    par = dict(parabolic=1, mu=0.01, Pr=0.71) if kind == "tgv3dns" else dict(parabolic=0)
+    return m, u, par
+
+
+def _dt(mesh, u, par, cfl):
+    o = oracle.Oracle(mesh, compat=0, **par)
+    o.rhs(u)
+    return cfl * min(mesh.h) / (o.max_char_speed() * (mesh.order + 1) ** 2)
+
+
+@pytest.mark.parametrize("kind,order,cfl", [("kh2d", 3, 10.0), ("kh2d", 4, 8.0), ("tgv3d", 3, 8.0)])
+def test_oracle_limiter_conserves_and_restores_positivity(kind, order, cfl):
+    mesh, u, par = _case(kind, order)
+    orc = oracle.Oracle(mesh, compat=0, **par)
+    y = orc.rk_stage(0, _dt(mesh, u, par, cfl), u, u)
+    nn = mesh.num_nodes
+    bad = (y[:nn] <= 0) | (_pressure(y, mesh.dim, nn) <= 0)
+    assert bad.any(), "the case must produce non-positive nodes"
+    z = oracle.Oracle(mesh, compat=0, filter=2, **par).positivity(y)
+    np.testing.assert_allclose(_means(z, mesh), _means(y, mesh), rtol=1e-13, atol=1e-13)
+    assert (z[:nn] > 0).all() and (_pressure(z, mesh.dim, nn) > 0).all()
+    # elements with no violation keep their bits
+    bad_el = bad.reshape(mesh.num_elements, mesh.ndof).any(axis=1)
+    Y = y.reshape(mesh.nv, mesh.num_elements, mesh.ndof)
+    Z = z.reshape(mesh.nv, mesh.num_elements, mesh.ndof)
+    assert np.array_equal(Y[:, ~bad_el], Z[:, ~bad_el])
+    assert not np.array_equal(Y[:, bad_el], Z[:, bad_el])
+
+
+def test_oracle_limiter_leaves_positive_states():
+    mesh = cases.vortex_mesh(8, 3)
+    u = cases.isentropic_vortex(mesh)
+    o = oracle.Oracle(mesh, compat=0, filter=2)
+    assert np.array_equal(o.positivity(u), u)
+    y = o.rk_stage(0, 1e-3, u, u)
+    assert o.limited_elements() == 0
+    assert np.array_equal(y, oracle.Oracle(mesh, compat=0).rk_stage(0, 1e-3, u, u))
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("filt", [2, 3])
+@pytest.mark.parametrize("compat", [0, 1])
+@pytest.mark.parametrize("kind,order,cfl", [("kh2d", 3, 10.0), ("kh2d", 4, 8.0), ("kh2d", 2, 10.0), ("tgv3d", 3, 8.0),
+                                            ("tgv3d", 2, 8.0), ("tgv3dns", 3, 6.0)])
+def test_gpu_limited_stages_match_oracle(kind, order, cfl, compat, filt, cuda_device):
+    import torch
+    mesh, u, par = _case(kind, order)
+    dt = _dt(mesh, u, par, cfl)
+    orc = oracle.Oracle(mesh, filter=filt, compat=compat, **par)
+    op = pb.DGSEMOperator(mesh, filter=filt, compat=compat, **par)
+    un = torch.from_numpy(u).to(cuda_device)
+    us = u
+    for stage in (0, 1, 2):
+        want = orc.rk_stage(stage, dt, u, us)
+        out = torch.full_like(un, float("nan"))
+        op.rk_stage(stage, dt, un, torch.from_numpy(us).to(cuda_device), out)
+        got = out.cpu().numpy()
+        assert rel_maxnorm(got, want) < TOL, f"stage {stage}"
+        assert op.limiter_count() == orc.limited_elements()
+        if filt & 1:
+            assert op.filter_count() == orc.filtered_elements()
+        us = want
+    if filt == 2:
+        assert orc.limited_elements() > 0, "the case must exercise the limiter"
+    nn = mesh.num_nodes
+    assert (us[:nn] > 0).all() and (_pressure(us, mesh.dim, nn) > 0).all()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("rough_state", [False, True])
+def test_gpu_kelvin_helmholtz_64_filter_and_limiter(rough_state, cuda_device):
+    """The Kelvin-Helmholtz benchmark mesh (64 x 64, N = 4) with the entropy
+    filter and the positivity limiter after every stage: one step's stages."""
+    import torch
+    mesh = cases.kh_mesh(64, 4)
+    u = cases.kelvin_helmholtz(mesh)
+    if rough_state:
+        u = rough(u, mesh, 13, 0.15, 0.05)
+    dt = _dt(mesh, u, dict(parabolic=0), 6.0 if rough_state else 0.5)
+    kw = dict(parabolic=0, filter=3, compat=0)
+    orc = oracle.Oracle(mesh, **kw)
+    op = pb.DGSEMOperator(mesh, **kw)
+    un = torch.from_numpy(u).to(cuda_device)
+    us = u
+    for stage in (0, 1, 2):
+        want = orc.rk_stage(stage, dt, u, us)
+        out = torch.empty_like(un)
+        op.rk_stage(stage, dt, un, torch.from_numpy(us).to(cuda_device), out)
+        assert rel_maxnorm(out.cpu().numpy(), want) < TOL, f"stage {stage}"
+        assert op.limiter_count() == orc.limited_elements()
+        assert op.filter_count() == orc.filtered_elements()
+        us = want
