@@ -2,8 +2,8 @@
 
 The reference's MinmodLimiter limits nothing (src/Limiters/MinmodLimiter.cpp:
 22-77) and it has no positivity limiter, so the oracle restates the published
-limiter of Zhang & Shu (2010) with the pressure step of Zhang, Xia & Shu
-(2012).  CPU tests check the oracle's limiter for what the method guarantees:
+limiter of Zhang & Shu (2010), with its pressure step taken from the
+concavity of the pressure.  CPU tests check the oracle's limiter for what the method guarantees:
 element means unchanged (conservation), positive density and pressure at
 every node afterwards, and elements without a violation left bit for bit.
 GPU tests compare the CUDA limiter with the oracle after RK stages that
@@ -85,12 +85,19 @@ def test_oracle_limiter_leaves_positive_states():
     assert np.array_equal(y, oracle.Oracle(mesh, compat=0).rk_stage(0, 1e-3, u, u))
 
 
+# (kind, order, CFL, stages): a CFL at which the unlimited stage output has
+# non-positive nodes while the limited stages stay finite; the Navier-Stokes
+# case is run for its first stage only (its later stages, from near-vacuum
+# nodes, are not finite at any CFL that limits)
+LIMITED = [("kh2d", 3, 3.0, 3), ("kh2d", 4, 5.0, 3), ("kh2d", 2, 3.0, 3), ("tgv3d", 3, 5.0, 3), ("tgv3d", 2, 3.0, 3),
+           ("tgv3d", 3, 10.0, 3), ("tgv3dns", 3, 4.0, 1)]
+
+
 @pytest.mark.gpu
 @pytest.mark.parametrize("filt", [2, 3])
 @pytest.mark.parametrize("compat", [0, 1])
-@pytest.mark.parametrize("kind,order,cfl", [("kh2d", 3, 10.0), ("kh2d", 4, 8.0), ("kh2d", 2, 10.0), ("tgv3d", 3, 8.0),
-                                            ("tgv3d", 2, 8.0), ("tgv3dns", 3, 6.0)])
-def test_gpu_limited_stages_match_oracle(kind, order, cfl, compat, filt, cuda_device):
+@pytest.mark.parametrize("kind,order,cfl,stages", LIMITED)
+def test_gpu_limited_stages_match_oracle(kind, order, cfl, stages, compat, filt, cuda_device):
     import torch
     mesh, u, par = _case(kind, order)
     dt = _dt(mesh, u, par, cfl)
@@ -98,8 +105,9 @@ def test_gpu_limited_stages_match_oracle(kind, order, cfl, compat, filt, cuda_de
     op = pb.DGSEMOperator(mesh, filter=filt, compat=compat, **par)
     un = torch.from_numpy(u).to(cuda_device)
     us = u
-    for stage in (0, 1, 2):
+    for stage in range(stages):
         want = orc.rk_stage(stage, dt, u, us)
+        assert np.isfinite(want).all()
         out = torch.full_like(un, float("nan"))
         op.rk_stage(stage, dt, un, torch.from_numpy(us).to(cuda_device), out)
         got = out.cpu().numpy()
@@ -124,7 +132,7 @@ def test_gpu_kelvin_helmholtz_64_filter_and_limiter(rough_state, cuda_device):
     u = cases.kelvin_helmholtz(mesh)
     if rough_state:
         u = rough(u, mesh, 13, 0.15, 0.05)
-    dt = _dt(mesh, u, dict(parabolic=0), 6.0 if rough_state else 0.5)
+    dt = _dt(mesh, u, dict(parabolic=0), 4.0 if rough_state else 0.5)
     kw = dict(parabolic=0, filter=3, compat=0)
     orc = oracle.Oracle(mesh, **kw)
     op = pb.DGSEMOperator(mesh, **kw)
@@ -138,3 +146,5 @@ def test_gpu_kelvin_helmholtz_64_filter_and_limiter(rough_state, cuda_device):
         assert op.limiter_count() == orc.limited_elements()
         assert op.filter_count() == orc.filtered_elements()
         us = want
+    if rough_state:
+        assert orc.limited_elements() > 0, "the roughened state must exercise the limiter"
