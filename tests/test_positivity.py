@@ -118,8 +118,14 @@ def test_gpu_limited_stages_match_oracle(kind, order, cfl, stages, compat, filt,
         us = want
     if filt == 2:
         assert orc.limited_elements() > 0, "the case must exercise the limiter"
+    # every element whose mean is admissible has positive nodes (at these
+    # CFLs, beyond the scheme's positivity condition, a mean can leave the
+    # admissible set, and then the limiter has nothing to contract towards)
     nn = mesh.num_nodes
-    assert (us[:nn] > 0).all() and (_pressure(us, mesh.dim, nn) > 0).all()
+    M = _means(us, mesh)
+    ok_el = (M[0] > 0) & ((GAMMA - 1.0) * (M[-1] - 0.5 * np.sum(M[1:1 + mesh.dim] ** 2, axis=0) / M[0]) > 0)
+    pos = ((us[:nn] > 0) & (_pressure(us, mesh.dim, nn) > 0)).reshape(mesh.num_elements, mesh.ndof).all(axis=1)
+    assert pos[ok_el].all()
 
 
 @pytest.mark.gpu
