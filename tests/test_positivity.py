@@ -8,7 +8,9 @@ element means unchanged (conservation), positive density and pressure at
 every node afterwards, and elements without a violation left bit for bit.
 GPU tests compare the CUDA limiter with the oracle after RK stages that
 produce negative densities and pressures (rough states at large CFL), at
-1e-12 relative in max norm with equal limiting counts, alone and after the
+1e-12 relative in max norm (or twice the rounding floor of the stage, the
+spread between the oracle's plain and fused-multiply-add builds, where that
+is larger) with equal limiting counts, alone and after the
 entropy filter, and on the Kelvin-Helmholtz benchmark mesh (64 x 64, N = 4),
 whose configuration runs both.
 """
@@ -48,6 +50,15 @@ def _case(kind, order):
     u = rough(cases.taylor_green(m), m, 5, 0.15, 0.05)
     par = dict(parabolic=1, mu=0.01, Pr=0.71) if kind == "tgv3dns" else dict(parabolic=0)
     return m, u, par
+
+
+def _stage_tol(mesh, kw, stage, dt, un, us, want):
+    """max(1e-12, twice the spread between the oracle's plain and
+    fused-multiply-add builds on the same stage): near-vacuum nodes that the
+    limiter leaves behind make a later stage's right-hand side very sensitive
+    to rounding."""
+    fma = oracle.Oracle(mesh, fma=True, **kw).rk_stage(stage, dt, un, us)
+    return max(TOL, 2.0 * rel_maxnorm(fma, want))
 
 
 def _dt(mesh, u, par, cfl):
@@ -111,7 +122,8 @@ def test_gpu_limited_stages_match_oracle(kind, order, cfl, stages, compat, filt,
         out = torch.full_like(un, float("nan"))
         op.rk_stage(stage, dt, un, torch.from_numpy(us).to(cuda_device), out)
         got = out.cpu().numpy()
-        assert rel_maxnorm(got, want) < TOL, f"stage {stage}"
+        tol = _stage_tol(mesh, dict(filter=filt, compat=compat, **par), stage, dt, u, us, want)
+        assert rel_maxnorm(got, want) < tol, f"stage {stage}"
         assert op.limiter_count() == orc.limited_elements()
         if filt & 1:
             assert op.filter_count() == orc.filtered_elements()
@@ -148,7 +160,8 @@ def test_gpu_kelvin_helmholtz_64_filter_and_limiter(rough_state, cuda_device):
         want = orc.rk_stage(stage, dt, u, us)
         out = torch.empty_like(un)
         op.rk_stage(stage, dt, un, torch.from_numpy(us).to(cuda_device), out)
-        assert rel_maxnorm(out.cpu().numpy(), want) < TOL, f"stage {stage}"
+        tol = _stage_tol(mesh, kw, stage, dt, u, us, want)
+        assert rel_maxnorm(out.cpu().numpy(), want) < tol, f"stage {stage}"
         assert op.limiter_count() == orc.limited_elements()
         assert op.filter_count() == orc.filtered_elements()
         us = want
