@@ -27,7 +27,13 @@
 
 namespace pdg {
 
-template <int N> constexpr int batch_slot_n() { return Shape<2, N>::EPW * Shape<2, N>::EL_RHS; }
+// Highest order the batched kernel is compiled for (its register budget is
+// that of its largest instantiation).
+#ifndef PDG_BATCH_MAX_N
+#define PDG_BATCH_MAX_N 5
+#endif
+
+template <int N> constexpr int batch_slot_n() { return N <= PDG_BATCH_MAX_N ? Shape<2, N>::EPW * Shape<2, N>::EL_RHS : 0; }
 constexpr int cmax(int a, int b) { return a > b ? a : b; }
 // per-warp shared memory: the case's constants and the largest tile slot
 constexpr int BATCH_SLOT = cmax(cmax(cmax(batch_slot_n<1>(), batch_slot_n<2>()), cmax(batch_slot_n<3>(), batch_slot_n<4>())),
@@ -85,10 +91,19 @@ __global__ void __launch_bounds__(MINB == 1 ? 256 : 128, MINB) batch_stage_kerne
             double lam = 0.0;
             switch (N) {
             case 1: batch_tile<1>(P, c, slot, tile.y, lane, flags, lam); break;
+#if PDG_BATCH_MAX_N >= 2
             case 2: batch_tile<2>(P, c, slot, tile.y, lane, flags, lam); break;
+#endif
+#if PDG_BATCH_MAX_N >= 3
             case 3: batch_tile<3>(P, c, slot, tile.y, lane, flags, lam); break;
+#endif
+#if PDG_BATCH_MAX_N >= 4
             case 4: batch_tile<4>(P, c, slot, tile.y, lane, flags, lam); break;
-            default: batch_tile<5>(P, c, slot, tile.y, lane, flags, lam); break;
+#endif
+#if PDG_BATCH_MAX_N >= 5
+            case 5: batch_tile<5>(P, c, slot, tile.y, lane, flags, lam); break;
+#endif
+            default: break;
             }
             lam = group_max<32>(lam);
             if (lane == 0) atomic_max_pos(P.lam_bits, lam);
@@ -306,7 +321,7 @@ int pdg_batch_create(int ncases, const pdg_mesh *meshes, const pdg_params *param
     std::vector<int32_t> hnbr;
     for (int c = 0; c < ncases; c++) {
         const pdg_mesh &m = meshes[c];
-        if (m.dim != 2 || m.order < 1 || m.order > 5 || m.num_elements < 1 || !m.nbr || !(m.h[0] > 0.0) ||
+        if (m.dim != 2 || m.order < 1 || m.order > PDG_BATCH_MAX_N || m.num_elements < 1 || !m.nbr || !(m.h[0] > 0.0) ||
             !(m.h[1] > 0.0))
             return cleanup(PDG_ERR_ARG);
         const int Np = m.order + 1;

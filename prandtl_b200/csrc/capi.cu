@@ -84,8 +84,19 @@ struct pdg_ctx {
     std::vector<TimedLaunch> timed;
     std::vector<cudaEvent_t> event_pool;
     cudaStream_t last_stream = 0;
+    // pdg_rk3_step_host's pipeline: element chunks, the chunks holding each
+    // chunk's face neighbours, copy and compute streams and their events
+    struct HostPipe {
+        bool ready = false, usable = false;
+        std::vector<int64_t> bounds;          // chunk k = elements [bounds[k], bounds[k + 1])
+        std::vector<std::vector<int>> near;   // chunks holding chunk k's elements and their face neighbours
+        cudaStream_t in = nullptr, comp = nullptr, out = nullptr;
+        std::vector<cudaEvent_t> ev_in, ev_done;
+        cudaEvent_t ev_start = nullptr;
+    } pipe;
     int device = 0;
     std::string last_error;
+    std::vector<int32_t> nbr_host;  // the neighbour table as given (the host step's pipeline reads it)
 };
 
 namespace {
@@ -419,7 +430,8 @@ int launch(pdg_ctx *c, int kind, KParams P, cudaStream_t s)
 {
     const KernelInfo &ki = c->kinfo[kind];
     if (!ki.fn || ki.epw < 1) return fail(c, PDG_ERR_UNSUPPORTED, "kernel %d is not configured", kind);
-    P.nwt = (c->ne + ki.epw - 1) / ki.epw;
+    const int64_t range = (P.e_end ? P.e_end : c->ne) - P.e_begin;  // element range (whole mesh by default)
+    P.nwt = (range + ki.epw - 1) / ki.epw;
     void *args[] = {&P};
     cudaEvent_t ea = nullptr, eb = nullptr;
     if (c->profile) {
@@ -625,6 +637,7 @@ int pdg_create(const pdg_mesh *mesh, const pdg_params *params, pdg_ctx **out)
         if (nb >= c->ne || nb < -PDG_MAX_BOUNDARIES) { delete c; return PDG_ERR_ARG; }
         if (nb < 0) c->bc_used |= 1u << (-1 - nb);
     }
+    c->nbr_host.assign(mesh->nbr, mesh->nbr + c->ne * 2 * c->dim);
     auto cleanup = [&](int code) {
         pdg_destroy(c);
         return code;
@@ -767,6 +780,12 @@ int pdg_destroy(pdg_ctx *c)
         cudaEventDestroy(t.b);
     }
     for (auto e : c->event_pool) cudaEventDestroy(e);
+    for (auto e : c->pipe.ev_in) cudaEventDestroy(e);
+    for (auto e : c->pipe.ev_done) cudaEventDestroy(e);
+    if (c->pipe.ev_start) cudaEventDestroy(c->pipe.ev_start);
+    if (c->pipe.in) cudaStreamDestroy(c->pipe.in);
+    if (c->pipe.comp) cudaStreamDestroy(c->pipe.comp);
+    if (c->pipe.out) cudaStreamDestroy(c->pipe.out);
     delete c;
     return PDG_OK;
 }
@@ -862,6 +881,163 @@ int pdg_rk3_steps(pdg_ctx *c, double dt, double *u, int nsteps, void *stream)
     return PDG_OK;
 }
 
+}  // extern "C"
+
+namespace {
+
+// pdg_rk3_step_host's pipeline (the fixed operator with the face buffer, no
+// filter, at least 8 x 512 elements): the state crosses PCIe in 8 chunks of
+// consecutive elements on a copy stream; stage 0's kernels run chunk by chunk
+// as soon as the chunks holding the chunk's face neighbours have landed;
+// stage 1 runs whole; stage 2 runs its face-node and lifting kernels whole
+// and its volume kernel chunk by chunk, each finished chunk copied back on a
+// second copy stream while the next is computed.  Per element the arithmetic
+// is that of the unchunked step, so the result is the same to the bit.
+constexpr int PIPE_CHUNKS = 8;
+constexpr int64_t PIPE_MIN_CHUNK = 512;
+
+int pipe_setup(pdg_ctx *c)
+{
+    auto &q = c->pipe;
+    if (q.ready) return PDG_OK;
+    q.ready = true;
+    q.usable = c->fbuf && !c->p.filter && c->ne >= PIPE_CHUNKS * PIPE_MIN_CHUNK;
+    if (const char *hp = std::getenv("PDG_HOST_PIPELINE")) q.usable = q.usable && std::atoi(hp) != 0;
+    if (!q.usable) return PDG_OK;
+    const int C = PIPE_CHUNKS, nf = 2 * c->dim;
+    q.bounds.resize(C + 1);
+    for (int k = 0; k <= C; k++) q.bounds[k] = c->ne * k / C;
+    auto chunk_of = [&](int64_t e) {
+        return (int)(std::upper_bound(q.bounds.begin(), q.bounds.end(), e) - q.bounds.begin()) - 1;
+    };
+    q.near.assign(C, {});
+    for (int k = 0; k < C; k++) {
+        std::vector<char> hit(C, 0);
+        hit[k] = 1;
+        for (int64_t e = q.bounds[k]; e < q.bounds[k + 1]; e++)
+            for (int f = 0; f < nf; f++) {
+                const int32_t nb = c->nbr_host[e * nf + f];
+                if (nb >= 0) hit[chunk_of(nb)] = 1;
+            }
+        for (int j = 0; j < C; j++)
+            if (hit[j]) q.near[k].push_back(j);
+    }
+    q.ev_in.assign(C, nullptr);
+    q.ev_done.assign(C, nullptr);
+    bool ok = cudaStreamCreateWithFlags(&q.in, cudaStreamNonBlocking) == cudaSuccess &&
+              cudaStreamCreateWithFlags(&q.comp, cudaStreamNonBlocking) == cudaSuccess &&
+              cudaStreamCreateWithFlags(&q.out, cudaStreamNonBlocking) == cudaSuccess &&
+              cudaEventCreateWithFlags(&q.ev_start, cudaEventDisableTiming) == cudaSuccess;
+    for (int k = 0; k < C && ok; k++)
+        ok = cudaEventCreateWithFlags(&q.ev_in[k], cudaEventDisableTiming) == cudaSuccess &&
+             cudaEventCreateWithFlags(&q.ev_done[k], cudaEventDisableTiming) == cudaSuccess;
+    if (!ok) return fail(c, PDG_ERR_CUDA, "pdg_rk3_step_host: stream or event creation failed");
+    return PDG_OK;
+}
+
+// Copies one chunk of every variable between the device state d and the host
+// state h (same byNODES offsets).
+int pipe_copy(pdg_ctx *c, int k, double *dst, const double *src, cudaMemcpyKind kind, cudaStream_t s)
+{
+    const auto &q = c->pipe;
+    const int64_t first = q.bounds[k] * c->ndof, count = (q.bounds[k + 1] - q.bounds[k]) * c->ndof;
+    for (int v = 0; v < c->nv; v++)
+        CK(cudaMemcpyAsync(dst + v * c->nnodes + first, src + v * c->nnodes + first, sizeof(double) * count, kind, s),
+           "chunk copy");
+    return PDG_OK;
+}
+
+int step_host_pipelined(pdg_ctx *c, double dt, double *u_host)
+{
+    auto &q = c->pipe;
+    const int C = PIPE_CHUNKS;
+    const bool ns = c->p.parabolic != 0;
+    const int k_face = ns ? KIND_LIFT_FACE_FLUX : KIND_FACE_FLUX;
+    const int k_vol = ns ? KIND_NS_FACES_FB : KIND_EULER_FACES_FB;
+    int r;
+    // after the caller's earlier work on the legacy default stream
+    CK(cudaEventRecord(q.ev_start, 0), "event record");
+    CK(cudaStreamWaitEvent(q.in, q.ev_start, 0), "stream wait");
+    CK(cudaStreamWaitEvent(q.comp, q.ev_start, 0), "stream wait");
+    for (int k = 0; k < C; k++) {
+        if ((r = pipe_copy(c, k, c->io_a, u_host, cudaMemcpyHostToDevice, q.in))) return r;
+        CK(cudaEventRecord(q.ev_in[k], q.in), "event record");
+    }
+    // stage 0: each kernel of each chunk once the chunks it reads have landed
+    // (t = the last chunk copy it waits for), in order of t, face-node before
+    // lifting before volume kernels
+    std::vector<int> t_face(C), t_lift(C), t_vol(C);
+    for (int k = 0; k < C; k++) t_face[k] = *std::max_element(q.near[k].begin(), q.near[k].end());
+    for (int k = 0; k < C; k++) {
+        t_lift[k] = t_vol[k] = 0;
+        for (int j : q.near[k]) {
+            t_lift[k] = std::max(t_lift[k], t_face[j]);
+            t_vol[k] = std::max(t_vol[k], t_face[j]);
+        }
+    }
+    if (ns)
+        for (int k = 0; k < C; k++)
+            for (int j : q.near[k]) t_vol[k] = std::max(t_vol[k], t_lift[j]);
+    struct Item { int t, type, k; };
+    std::vector<Item> items;
+    for (int k = 0; k < C; k++) {
+        items.push_back({t_face[k], 0, k});
+        if (ns) items.push_back({t_lift[k], 1, k});
+        items.push_back({t_vol[k], 2, k});
+    }
+    std::sort(items.begin(), items.end(), [](const Item &a, const Item &b) {
+        return a.t != b.t ? a.t < b.t : (a.type != b.type ? a.type < b.type : a.k < b.k);
+    });
+    CK(cudaMemsetAsync(c->lam_bits, 0, sizeof(unsigned long long), q.comp), "reset wave speed");
+    KParams P = base_params(c);
+    P.u = c->io_a;
+    P.un = c->io_a;
+    P.out = c->stage_a;
+    P.stage = 0;
+    P.dt = dt;
+    P.vbuf = c->vbuf;
+    int waited = -1;
+    for (const Item &it : items) {
+        if (it.t > waited) {
+            CK(cudaStreamWaitEvent(q.comp, q.ev_in[it.t], 0), "stream wait");
+            waited = it.t;
+        }
+        P.e_begin = q.bounds[it.k];
+        P.e_end = q.bounds[it.k + 1];
+        if ((r = launch(c, it.type == 0 ? k_face : it.type == 1 ? KIND_LIFT : k_vol, P, q.comp))) return r;
+    }
+    // stage 1 on the whole mesh
+    if ((r = evaluate(c, 1, dt, c->io_a, c->stage_a, c->stage_b, q.comp))) return r;
+    // stage 2: face nodes and lifting on the whole mesh, the volume kernel
+    // chunk by chunk, each chunk's result back to the host behind it
+    CK(cudaMemsetAsync(c->lam_bits, 0, sizeof(unsigned long long), q.comp), "reset wave speed");
+    P = base_params(c);
+    P.u = c->stage_b;
+    P.un = c->io_a;
+    P.out = c->io_a;  // stage 2 reads un and writes the same entries from the same thread
+    P.stage = 2;
+    P.dt = dt;
+    P.vbuf = c->vbuf;
+    if ((r = launch(c, k_face, P, q.comp))) return r;
+    if (ns && (r = launch(c, KIND_LIFT, P, q.comp))) return r;
+    for (int k = 0; k < C; k++) {
+        P.e_begin = q.bounds[k];
+        P.e_end = q.bounds[k + 1];
+        if ((r = launch(c, k_vol, P, q.comp))) return r;
+        CK(cudaEventRecord(q.ev_done[k], q.comp), "event record");
+        CK(cudaStreamWaitEvent(q.out, q.ev_done[k], 0), "stream wait");
+        if ((r = pipe_copy(c, k, u_host, c->io_a, cudaMemcpyDeviceToHost, q.out))) return r;
+    }
+    c->last_stream = q.comp;
+    CK(cudaStreamSynchronize(q.out), "synchronize");
+    CK(cudaStreamSynchronize(q.comp), "synchronize");
+    return PDG_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
 int pdg_rk3_step_host(pdg_ctx *c, double dt, double *u_host)
 {
     if (!c) return PDG_ERR_ARG;
@@ -871,9 +1047,12 @@ int pdg_rk3_step_host(pdg_ctx *c, double dt, double *u_host)
         if (cudaMalloc(&c->io_a, bytes) != cudaSuccess || cudaMalloc(&c->io_b, bytes) != cudaSuccess)
             return fail(c, PDG_ERR_NOMEM, "pdg_rk3_step_host: staging allocation failed");
     }
+    int r = pipe_setup(c);
+    if (r) return r;
+    if (c->pipe.usable && !c->profile) return step_host_pipelined(c, dt, u_host);
     cudaStream_t s = 0;
     CK(cudaMemcpyAsync(c->io_a, u_host, bytes, cudaMemcpyHostToDevice, s), "copy in");
-    int r = pdg_rk3_step(c, dt, c->io_a, s);
+    r = pdg_rk3_step(c, dt, c->io_a, s);
     if (r) return r;
     CK(cudaMemcpyAsync(u_host, c->io_a, bytes, cudaMemcpyDeviceToHost, s), "copy out");
     CK(cudaStreamSynchronize(s), "synchronize");

@@ -97,7 +97,12 @@ struct KParams {
     // adjoint stage
     const double *gbuf;
     double *bx;
+    // elements [e_begin, e_end) that the face-node, lifting and volume
+    // kernels process (e_end = 0: up to ne); nwt counts the range's tiles
+    int64_t e_begin, e_end;
 };
+
+__device__ __forceinline__ int64_t range_end(const KParams &P) { return P.e_end ? P.e_end : P.ne; }
 
 // Boundary conditions (src/Integrators/BoundaryConditions/): a neighbour
 // entry -1 - b marks a boundary face with condition b of the table P.bc.
@@ -721,7 +726,7 @@ __device__ __forceinline__ void rhs_tile(const KParams &P, const double *c, doub
     double *acc = pr + S::NPRIM * ST, *scratch = acc, *zf = acc + NV * ST;
     const bool compat = P.compat != 0;
     const int64_t e0 = e_base + grp;
-    const bool valid = lane_used && e0 < P.ne;
+    const bool valid = lane_used && e0 < range_end(P);
     const int64_t e = valid ? e0 : 0;
     // the RK base state is first read by the final combine: bring the
     // element's block of each variable into L2 now
@@ -885,7 +890,7 @@ __global__ void __launch_bounds__(128, RhsOccupancy<DIM, N>::min_blocks) rhs_ker
     unsigned int flags = 0;
     double lam = 0.0;
     for (int64_t wt = (int64_t)blockIdx.x * wpb + warp; wt < P.nwt; wt += wstride)
-        rhs_tile<DIM, N, NS, FACES, true, BDR, FB>(P, c, pr, wt * EPW, grp, gl, lane_used, flags, lam);
+        rhs_tile<DIM, N, NS, FACES, true, BDR, FB>(P, c, pr, P.e_begin + wt * EPW, grp, gl, lane_used, flags, lam);
     lam = group_max<32>(lam);
     if (lane == 0) atomic_max_pos(P.lam_bits, lam);
     flags = __reduce_or_sync(0xffffffffu, flags);
@@ -1499,16 +1504,17 @@ __global__ void __launch_bounds__(256, (MODE & FACE_FLUX) ? PDG_FACE_NODE_MIN_BL
     // in L2 for its later directions (direction-major order over the whole
     // mesh read the state from DRAM about twice per launch)
     constexpr int CH = 64, PER_CH = DIM * CH * NFN;
-    const int64_t nch = (P.ne + CH - 1) / CH;
+    const int64_t e_end = range_end(P);
+    const int64_t nch = (e_end - P.e_begin + CH - 1) / CH;
     for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < nch * PER_CH;
          t += (int64_t)gridDim.x * blockDim.x) {
         const int64_t ch = t / PER_CH;
         const int r = (int)(t - ch * PER_CH);
         const int d = r / (CH * NFN);
         const int r2 = r - d * (CH * NFN);
-        const int64_t a = ch * CH + r2 / NFN;
+        const int64_t a = P.e_begin + ch * CH + r2 / NFN;
         const int fn = r2 % NFN;
-        if (a >= P.ne) continue;
+        if (a >= e_end) continue;
         if (BDR) {
             const int32_t bp = __ldg(P.nbr + a * 2 * DIM + 2 * d + 1), bm = __ldg(P.nbr + a * 2 * DIM + 2 * d);
             double *dp = P.lbuf + ((d * P.ne + a) * NFN + fn) * (DIM + 2);
@@ -1653,13 +1659,14 @@ __global__ void __launch_bounds__(128, LiftOccupancy<DIM, N>::min_blocks) lift_k
     const bool compat = P.compat != 0;
     const int64_t wstride = (int64_t)gridDim.x * wpb;
     unsigned int flags = 0;
+    const int64_t e_end = range_end(P);
     for (int64_t wt = (int64_t)blockIdx.x * wpb + warp; wt < P.nwt; wt += wstride) {
-        const int64_t e0 = wt * EPW + grp;
-        const bool valid = lane_used && e0 < P.ne;
+        const int64_t e0 = P.e_begin + wt * EPW + grp;
+        const bool valid = lane_used && e0 < e_end;
         const int64_t e = valid ? e0 : 0;
         {
-            const int64_t en = (wt + wstride) * EPW + grp;
-            if (P.prefetch && lane_used && en < P.ne && gl < NV) prefetch_l2(P.u + (int64_t)gl * nn + en * NDOF, sizeof(double) * NDOF);
+            const int64_t en = P.e_begin + (wt + wstride) * EPW + grp;
+            if (P.prefetch && lane_used && en < e_end && gl < NV) prefetch_l2(P.u + (int64_t)gl * nn + en * NDOF, sizeof(double) * NDOF);
         }
         if (lane_used) {
 #pragma unroll

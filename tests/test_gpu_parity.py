@@ -243,3 +243,44 @@ def test_face_buffer_equals_element_faces(kind, dim, order, par, cuda_device, mo
         assert rel_maxnorm(a.cpu().numpy(), b.cpu().numpy()) < 1e-14, f"stage {stage}"
     assert op.GetMaxCharSpeed() == op_el.GetMaxCharSpeed()
     assert op.check() == 0 and op_el.check() == 0
+
+
+@pytest.mark.parametrize("kind", ["tgv16_ns", "tgv16_euler", "vortex64"])
+def test_host_step_pipeline_equals_device_step(kind, cuda_device, monkeypatch):
+    """pdg_rk3_step_host pipelines its copies with stages 0 and 2 on meshes of
+    4096 elements and more; two host steps equal two device steps bit for bit,
+    and the unpipelined host step (PDG_HOST_PIPELINE=0) as well."""
+    import torch
+    if kind == "vortex64":
+        mesh = cases.vortex_mesh(64, 3)
+        u = rough(cases.isentropic_vortex(mesh), mesh, 7, 0.05, 0.01)
+        kw = dict(parabolic=0, compat=0)
+    else:
+        mesh = cases.tgv_mesh(16, 3)
+        u = rough(cases.taylor_green(mesh), mesh, 7, 0.02, 0.002)
+        kw = dict(parabolic=1 if kind.endswith("ns") else 0, mu=1.0 / 1600.0, Pr=0.71, compat=0)
+    assert mesh.num_elements >= 4096
+    op = pb.DGSEMOperator(mesh, **kw)
+    x = dev(u, cuda_device)
+    op.Mult(x, torch.empty_like(x))
+    dt = op.cfl_dt(0.5)
+    ref = x.clone()
+    op.rk3_step(ref, dt, nsteps=2)
+    lam = op.GetMaxCharSpeed()
+    host = torch.from_numpy(u.copy()).pin_memory().numpy()
+    for _ in range(2):
+        op.rk3_step_host(host, dt)
+    assert np.array_equal(host, ref.cpu().numpy())
+    assert op.GetMaxCharSpeed() == lam
+    monkeypatch.setenv("PDG_HOST_PIPELINE", "0")
+    op2 = pb.DGSEMOperator(mesh, **kw)
+    monkeypatch.delenv("PDG_HOST_PIPELINE")
+    host2 = torch.from_numpy(u.copy()).pin_memory().numpy()
+    for _ in range(2):
+        op2.rk3_step_host(host2, dt)
+    assert np.array_equal(host2, host)
+    pageable = u.copy()  # the pipeline also serves pageable memory (without overlap)
+    op.rk3_step_host(pageable, dt)
+    op.rk3_step_host(pageable, dt)
+    assert np.array_equal(pageable, host)
+    assert op.check() == 0
