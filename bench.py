@@ -306,7 +306,7 @@ def run_ours(args):
             op.rk3_step_host(host, dt)
         io_bytes = 8 * V
         e2e_path = ("pdg_rk3_step_host (pinned host state in, 3 fused stages, state out; the copies pipelined "
-                    "with stages 0 and 2 in 8 element chunks)")
+                    "with stages 0 and 2 in element chunks)")
     e2e_step()
     barrier()
     t0 = time.perf_counter()

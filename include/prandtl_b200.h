@@ -214,12 +214,12 @@ int pdg_rk3_steps(pdg_ctx *ctx, double dt, double *u, int nsteps, void *stream);
  * copies the result back and synchronises.  u_host may be pinned or pageable
  * (pinned memory lets the copies overlap the kernels).  For the fixed
  * operator on a periodic mesh of at least 4096 elements without the filter
- * or limiter the step is pipelined: the state crosses PCIe in 8 element
- * chunks, stage 0 works on the chunks whose face neighbours have landed while
- * the rest are still copying, and stage 2's volume kernel runs chunk by chunk
- * with each finished chunk copied back behind it; the result equals
- * pdg_rk3_step's bit for bit.  Work already queued on the legacy default
- * stream comes first. */
+ * or limiter the step is pipelined: the state crosses PCIe in 32 element
+ * chunks, stage 0 works on the runs of chunks whose reads (radius three in
+ * face neighbours for Navier-Stokes) have landed while the rest are still
+ * copying, and stage 2's volume kernel runs in four runs with each finished
+ * run copied back behind it; the result equals pdg_rk3_step's bit for bit.
+ * Work already queued on the legacy default stream comes first. */
 int pdg_rk3_step_host(pdg_ctx *ctx, double dt, double *u_host);
 
 /* DGSEMOperator::GetMaxCharSpeed (DGSEMOperator.hpp:106-109).  With compat=1

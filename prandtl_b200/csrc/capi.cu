@@ -886,15 +886,20 @@ int pdg_rk3_steps(pdg_ctx *c, double dt, double *u, int nsteps, void *stream)
 namespace {
 
 // pdg_rk3_step_host's pipeline (the fixed operator with the face buffer, no
-// filter, at least 8 x 512 elements): the state crosses PCIe in 8 chunks of
-// consecutive elements on a copy stream; stage 0's kernels run chunk by chunk
-// as soon as the chunks holding the chunk's face neighbours have landed;
+// filter, at least PIPE_CHUNKS x PIPE_MIN_CHUNK elements): the state crosses
+// PCIe in chunks of consecutive elements on a copy stream.  At four
+// milestones of the copy, stage 0's kernels are launched over the runs of
+// consecutive chunks whose reads have landed (a face-node kernel reads its
+// chunk and the chunks of the face neighbours, a lifting kernel the
+// face-node results of its neighbours' chunks, a volume kernel the lifting
+// results of its neighbours' chunks; on a periodic mesh the last chunks to
+// land hold up their neighbours, so only part of stage 0 overlaps the copy);
 // stage 1 runs whole; stage 2 runs its face-node and lifting kernels whole
-// and its volume kernel chunk by chunk, each finished chunk copied back on a
-// second copy stream while the next is computed.  Per element the arithmetic
-// is that of the unchunked step, so the result is the same to the bit.
-constexpr int PIPE_CHUNKS = 8;
-constexpr int64_t PIPE_MIN_CHUNK = 512;
+// and its volume kernel in four runs, each copied back on a second copy
+// stream while the next is computed.  Per element the arithmetic is that of
+// the unchunked step, so the result is the same to the bit.
+constexpr int PIPE_CHUNKS = 32, PIPE_MILESTONES = 4;
+constexpr int64_t PIPE_MIN_CHUNK = 128;
 
 int pipe_setup(pdg_ctx *c)
 {
@@ -922,25 +927,25 @@ int pipe_setup(pdg_ctx *c)
         for (int j = 0; j < C; j++)
             if (hit[j]) q.near[k].push_back(j);
     }
-    q.ev_in.assign(C, nullptr);
-    q.ev_done.assign(C, nullptr);
+    q.ev_in.assign(PIPE_MILESTONES, nullptr);
+    q.ev_done.assign(PIPE_MILESTONES, nullptr);
     bool ok = cudaStreamCreateWithFlags(&q.in, cudaStreamNonBlocking) == cudaSuccess &&
               cudaStreamCreateWithFlags(&q.comp, cudaStreamNonBlocking) == cudaSuccess &&
               cudaStreamCreateWithFlags(&q.out, cudaStreamNonBlocking) == cudaSuccess &&
               cudaEventCreateWithFlags(&q.ev_start, cudaEventDisableTiming) == cudaSuccess;
-    for (int k = 0; k < C && ok; k++)
-        ok = cudaEventCreateWithFlags(&q.ev_in[k], cudaEventDisableTiming) == cudaSuccess &&
-             cudaEventCreateWithFlags(&q.ev_done[k], cudaEventDisableTiming) == cudaSuccess;
+    for (int m = 0; m < PIPE_MILESTONES && ok; m++)
+        ok = cudaEventCreateWithFlags(&q.ev_in[m], cudaEventDisableTiming) == cudaSuccess &&
+             cudaEventCreateWithFlags(&q.ev_done[m], cudaEventDisableTiming) == cudaSuccess;
     if (!ok) return fail(c, PDG_ERR_CUDA, "pdg_rk3_step_host: stream or event creation failed");
     return PDG_OK;
 }
 
-// Copies one chunk of every variable between the device state d and the host
-// state h (same byNODES offsets).
-int pipe_copy(pdg_ctx *c, int k, double *dst, const double *src, cudaMemcpyKind kind, cudaStream_t s)
+// Copies chunks [k0, k1) of every variable between the device state and the
+// host state (same byNODES offsets).
+int pipe_copy(pdg_ctx *c, int k0, int k1, double *dst, const double *src, cudaMemcpyKind kind, cudaStream_t s)
 {
     const auto &q = c->pipe;
-    const int64_t first = q.bounds[k] * c->ndof, count = (q.bounds[k + 1] - q.bounds[k]) * c->ndof;
+    const int64_t first = q.bounds[k0] * c->ndof, count = (q.bounds[k1] - q.bounds[k0]) * c->ndof;
     for (int v = 0; v < c->nv; v++)
         CK(cudaMemcpyAsync(dst + v * c->nnodes + first, src + v * c->nnodes + first, sizeof(double) * count, kind, s),
            "chunk copy");
@@ -950,44 +955,26 @@ int pipe_copy(pdg_ctx *c, int k, double *dst, const double *src, cudaMemcpyKind 
 int step_host_pipelined(pdg_ctx *c, double dt, double *u_host)
 {
     auto &q = c->pipe;
-    const int C = PIPE_CHUNKS;
+    const int C = PIPE_CHUNKS, M = PIPE_MILESTONES, per = C / M;
     const bool ns = c->p.parabolic != 0;
-    const int k_face = ns ? KIND_LIFT_FACE_FLUX : KIND_FACE_FLUX;
-    const int k_vol = ns ? KIND_NS_FACES_FB : KIND_EULER_FACES_FB;
+    const int kinds[3] = {ns ? KIND_LIFT_FACE_FLUX : KIND_FACE_FLUX, KIND_LIFT, ns ? KIND_NS_FACES_FB : KIND_EULER_FACES_FB};
     int r;
     // after the caller's earlier work on the legacy default stream
     CK(cudaEventRecord(q.ev_start, 0), "event record");
     CK(cudaStreamWaitEvent(q.in, q.ev_start, 0), "stream wait");
     CK(cudaStreamWaitEvent(q.comp, q.ev_start, 0), "stream wait");
-    for (int k = 0; k < C; k++) {
-        if ((r = pipe_copy(c, k, c->io_a, u_host, cudaMemcpyHostToDevice, q.in))) return r;
-        CK(cudaEventRecord(q.ev_in[k], q.in), "event record");
+    for (int m = 0; m < M; m++) {
+        if ((r = pipe_copy(c, m * per, (m + 1) * per, c->io_a, u_host, cudaMemcpyHostToDevice, q.in))) return r;
+        CK(cudaEventRecord(q.ev_in[m], q.in), "event record");
     }
-    // stage 0: each kernel of each chunk once the chunks it reads have landed
-    // (t = the last chunk copy it waits for), in order of t, face-node before
-    // lifting before volume kernels
-    std::vector<int> t_face(C), t_lift(C), t_vol(C);
-    for (int k = 0; k < C; k++) t_face[k] = *std::max_element(q.near[k].begin(), q.near[k].end());
-    for (int k = 0; k < C; k++) {
-        t_lift[k] = t_vol[k] = 0;
-        for (int j : q.near[k]) {
-            t_lift[k] = std::max(t_lift[k], t_face[j]);
-            t_vol[k] = std::max(t_vol[k], t_face[j]);
-        }
-    }
-    if (ns)
-        for (int k = 0; k < C; k++)
-            for (int j : q.near[k]) t_vol[k] = std::max(t_vol[k], t_lift[j]);
-    struct Item { int t, type, k; };
-    std::vector<Item> items;
-    for (int k = 0; k < C; k++) {
-        items.push_back({t_face[k], 0, k});
-        if (ns) items.push_back({t_lift[k], 1, k});
-        items.push_back({t_vol[k], 2, k});
-    }
-    std::sort(items.begin(), items.end(), [](const Item &a, const Item &b) {
-        return a.t != b.t ? a.t < b.t : (a.type != b.type ? a.type < b.type : a.k < b.k);
-    });
+    // readiness of stage 0's kernels: the last chunk (copy order) each reads
+    std::vector<int> t[3];
+    for (auto &v : t) v.assign(C, 0);
+    for (int k = 0; k < C; k++) t[0][k] = *std::max_element(q.near[k].begin(), q.near[k].end());
+    for (int k = 0; k < C; k++)
+        for (int j : q.near[k]) t[1][k] = std::max(t[1][k], t[0][j]);
+    for (int k = 0; k < C; k++)
+        for (int j : q.near[k]) t[2][k] = std::max(t[2][k], ns ? std::max(t[0][j], t[1][j]) : t[0][j]);
     CK(cudaMemsetAsync(c->lam_bits, 0, sizeof(unsigned long long), q.comp), "reset wave speed");
     KParams P = base_params(c);
     P.u = c->io_a;
@@ -996,20 +983,29 @@ int step_host_pipelined(pdg_ctx *c, double dt, double *u_host)
     P.stage = 0;
     P.dt = dt;
     P.vbuf = c->vbuf;
-    int waited = -1;
-    for (const Item &it : items) {
-        if (it.t > waited) {
-            CK(cudaStreamWaitEvent(q.comp, q.ev_in[it.t], 0), "stream wait");
-            waited = it.t;
+    std::vector<char> done[3];
+    for (auto &v : done) v.assign(C, 0);
+    for (int m = 0; m < M; m++) {
+        CK(cudaStreamWaitEvent(q.comp, q.ev_in[m], 0), "stream wait");
+        const int landed = (m + 1) * per - 1;
+        for (int type = 0; type < 3; type++) {
+            if (type == 1 && !ns) continue;
+            // runs of consecutive ready chunks, one launch each
+            for (int k = 0; k < C;) {
+                if (done[type][k] || t[type][k] > landed) { k++; continue; }
+                int k1 = k;
+                while (k1 < C && !done[type][k1] && t[type][k1] <= landed) done[type][k1++] = 1;
+                P.e_begin = q.bounds[k];
+                P.e_end = q.bounds[k1];
+                if ((r = launch(c, kinds[type], P, q.comp))) return r;
+                k = k1;
+            }
         }
-        P.e_begin = q.bounds[it.k];
-        P.e_end = q.bounds[it.k + 1];
-        if ((r = launch(c, it.type == 0 ? k_face : it.type == 1 ? KIND_LIFT : k_vol, P, q.comp))) return r;
     }
     // stage 1 on the whole mesh
     if ((r = evaluate(c, 1, dt, c->io_a, c->stage_a, c->stage_b, q.comp))) return r;
-    // stage 2: face nodes and lifting on the whole mesh, the volume kernel
-    // chunk by chunk, each chunk's result back to the host behind it
+    // stage 2: face nodes and lifting on the whole mesh, the volume kernel in
+    // M runs, each run's result back to the host behind it
     CK(cudaMemsetAsync(c->lam_bits, 0, sizeof(unsigned long long), q.comp), "reset wave speed");
     P = base_params(c);
     P.u = c->stage_b;
@@ -1018,15 +1014,15 @@ int step_host_pipelined(pdg_ctx *c, double dt, double *u_host)
     P.stage = 2;
     P.dt = dt;
     P.vbuf = c->vbuf;
-    if ((r = launch(c, k_face, P, q.comp))) return r;
+    if ((r = launch(c, kinds[0], P, q.comp))) return r;
     if (ns && (r = launch(c, KIND_LIFT, P, q.comp))) return r;
-    for (int k = 0; k < C; k++) {
-        P.e_begin = q.bounds[k];
-        P.e_end = q.bounds[k + 1];
-        if ((r = launch(c, k_vol, P, q.comp))) return r;
-        CK(cudaEventRecord(q.ev_done[k], q.comp), "event record");
-        CK(cudaStreamWaitEvent(q.out, q.ev_done[k], 0), "stream wait");
-        if ((r = pipe_copy(c, k, u_host, c->io_a, cudaMemcpyDeviceToHost, q.out))) return r;
+    for (int m = 0; m < M; m++) {
+        P.e_begin = q.bounds[m * per];
+        P.e_end = q.bounds[(m + 1) * per];
+        if ((r = launch(c, kinds[2], P, q.comp))) return r;
+        CK(cudaEventRecord(q.ev_done[m], q.comp), "event record");
+        CK(cudaStreamWaitEvent(q.out, q.ev_done[m], 0), "stream wait");
+        if ((r = pipe_copy(c, m * per, (m + 1) * per, u_host, c->io_a, cudaMemcpyDeviceToHost, q.out))) return r;
     }
     c->last_stream = q.comp;
     CK(cudaStreamSynchronize(q.out), "synchronize");
