@@ -289,6 +289,40 @@ int pdg_filter_count(pdg_ctx *ctx, int64_t *filtered);
  * since creation (synchronises). */
 int pdg_limiter_count(pdg_ctx *ctx, int64_t *limited);
 
+/* One kernel of a fused RK stage (pdg_rk_stage) over the elements
+ * [e_begin, e_end), for a caller that interleaves a stage with its own work:
+ * the multi-rank driver runs the elements that need no neighbour rank's data
+ * while face data is in flight, as the reference's shared-face exchange
+ * (ExchangeFaceNbrData, src/Operators/NonlinearForm/DGSEMNonlinearForm.cpp:
+ * 748; Navier-Stokes also :533, :1426-1429) separates its face loops.  A
+ * stage is PDG_PART_START (resets the wave-speed maximum), then over every
+ * element PDG_PART_FACES (face-node kernel: BR1 jumps and the inviscid flux
+ * of each element's +d faces, reading the state of the element and its +d
+ * neighbours), PDG_PART_LIFT (Navier-Stokes: lifting kernel, reading the
+ * face-node results of the element's faces and writing its viscous face
+ * columns) and PDG_PART_VOLUME (volume kernel: the element's stage output,
+ * reading the face-node results of its faces and its neighbours' viscous
+ * face columns), each part of an element after the parts it reads.  Fixed
+ * operator on a mesh without boundary faces, no filter or limiter
+ * (PDG_ERR_UNSUPPORTED otherwise).  DEVICE pointers as pdg_rk_stage; uout is
+ * only read by PDG_PART_VOLUME. */
+#define PDG_PART_START  0
+#define PDG_PART_FACES  1
+#define PDG_PART_LIFT   2
+#define PDG_PART_VOLUME 3
+int pdg_rk_stage_part(pdg_ctx *ctx, int part, int stage, double dt, const double *un, const double *us, double *uout,
+                      int64_t e_begin, int64_t e_end, void *stream);
+
+/* The context's viscous face columns (Navier-Stokes): *cols = device buffer
+ * of *count doubles, fcol[d][side][e][face node][i] (side 1: the element's +d
+ * face, i over the dim + 1 momentum and energy rows of the normal viscous
+ * flux), written by PDG_PART_LIFT.  A multi-rank driver copies the columns of
+ * its slab's boundary elements to the neighbour ranks, which write them into
+ * their ghost elements' slots before their PDG_PART_VOLUME.  No reference
+ * counterpart (the reference exchanges gradients, DGSEMNonlinearForm.cpp:
+ * 1426-1429). */
+int pdg_face_columns(pdg_ctx *ctx, double **cols, int64_t *count);
+
 /* Reads and clears the device error word (PDG_FLAG_*).  Synchronises. */
 int pdg_check(pdg_ctx *ctx, uint32_t *flags);
 

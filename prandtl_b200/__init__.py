@@ -51,6 +51,8 @@ BC_SUPERSONIC_INFLOW, BC_SUPERSONIC_OUTFLOW, BC_SPECIFIED_STATE, BC_SLIP_WALL, B
 BC_SUBSONIC_OUTFLOW_P, BC_SUBSONIC_INFLOW_RV, BC_SUBSONIC_INFLOW_PTTT, BC_RIEMANN_INVARIANT = 6, 7, 8, 9
 BC_NOSLIP_ADIABATIC, BC_NOSLIP_ISOTHERMAL = 10, 11
 MAX_BOUNDARIES = 16
+# pdg_rk_stage_part parts
+PART_START, PART_FACES, PART_LIFT, PART_VOLUME = 0, 1, 2, 3
 PDG_FLAG_NONFINITE = 1
 PDG_FLAG_NONPHYSICAL = 2
 _STATUS = {1: "bad argument", 2: "CUDA error", 3: "non-finite state", 4: "non-physical state",
@@ -135,6 +137,9 @@ def library():
                                    C.c_void_p]
     L.pdg_rhs_noalloc.argtypes = [C.POINTER(PdgMesh), C.POINTER(PdgParams), C.c_void_p, C.c_void_p, C.c_void_p]
     L.pdg_set_boundary.argtypes = [C.c_void_p, C.c_int, C.c_int, _dp]
+    L.pdg_rk_stage_part.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_double, C.c_void_p, C.c_void_p, C.c_void_p,
+                                    C.c_int64, C.c_int64, C.c_void_p]
+    L.pdg_face_columns.argtypes = [C.c_void_p, C.POINTER(C.c_void_p), C.POINTER(C.c_int64)]
     _lib = L
     return L
 
@@ -338,6 +343,34 @@ class DGSEMOperator:
         n = C.c_int64()
         self._call(library().pdg_filter_count(self._ctx, C.byref(n)), "pdg_filter_count")
         return n.value
+
+    def rk_stage_part(self, part: int, stage: int, dt: float, un, us, uout, e_begin: int, e_end: int, stream=None):
+        """One kernel of a fused stage over elements [e_begin, e_end)
+        (pdg_rk_stage_part): PART_START, then PART_FACES, PART_LIFT and
+        PART_VOLUME over every element, each after the parts it reads."""
+        for t in (un, us, uout):
+            if t is not None:
+                self._check_dev(t)
+        ptr = lambda t: C.c_void_p(t.data_ptr() if t is not None else 0)  # noqa: E731
+        self._call(library().pdg_rk_stage_part(self._ctx, int(part), int(stage), float(dt), ptr(un), ptr(us), ptr(uout),
+                                               int(e_begin), int(e_end), C.c_void_p(_stream_handle(stream))),
+                   "pdg_rk_stage_part")
+
+    def face_columns(self):
+        """The context's viscous face columns as a float64 CUDA tensor (a view,
+        shape [dim, 2, num_elements, face nodes, dim + 1]); Navier-Stokes only."""
+        import torch
+        ptr, n = C.c_void_p(), C.c_int64()
+        self._call(library().pdg_face_columns(self._ctx, C.byref(ptr), C.byref(n)), "pdg_face_columns")
+        m = self.mesh
+        shape = (m.dim, 2, m.num_elements, m.Np ** (m.dim - 1), m.dim + 1)
+        assert int(np.prod(shape)) == n.value
+
+        class _View:  # a CUDA array interface over the context's buffer
+            __cuda_array_interface__ = {"shape": shape, "typestr": "<f8", "data": (ptr.value, False), "version": 3,
+                                        "strides": None}
+        dev = torch.device("cuda", torch.cuda.current_device())
+        return torch.as_tensor(_View(), device=dev)
 
     def limiter_count(self) -> int:
         """Element limitings by the positivity limiter since creation (synchronises)."""

@@ -1055,6 +1055,51 @@ int pdg_rk3_step_host(pdg_ctx *c, double dt, double *u_host)
     return PDG_OK;
 }
 
+int pdg_rk_stage_part(pdg_ctx *c, int part, int stage, double dt, const double *un, const double *us, double *uout,
+                      int64_t e_begin, int64_t e_end, void *stream)
+{
+    if (!c) return PDG_ERR_ARG;
+    if (!c->fbuf || c->p.filter)
+        return fail(c, PDG_ERR_UNSUPPORTED, "pdg_rk_stage_part: needs the fixed operator on a periodic mesh, no filter");
+    if (part < PDG_PART_START || part > PDG_PART_VOLUME) return fail(c, PDG_ERR_ARG, "pdg_rk_stage_part: bad part");
+    if (stage < -1 || stage > 2) return fail(c, PDG_ERR_ARG, "pdg_rk_stage_part: stage must be -1, 0, 1 or 2");
+    if (e_begin < 0 || e_end > c->ne || e_begin > e_end) return fail(c, PDG_ERR_ARG, "pdg_rk_stage_part: bad range");
+    cudaStream_t s = (cudaStream_t)stream;
+    c->last_stream = s;
+    if (part == PDG_PART_START) {
+        CK(cudaMemsetAsync(c->lam_bits, 0, sizeof(unsigned long long), s), "reset wave speed");
+        return PDG_OK;
+    }
+    if (!us || (part == PDG_PART_VOLUME && (!uout || uout == us || (stage > 0 && !un))))
+        return fail(c, PDG_ERR_ARG, "pdg_rk_stage_part: null or aliased buffers");
+    if (e_begin == e_end) return PDG_OK;
+    const bool ns = c->p.parabolic != 0;
+    if (part == PDG_PART_LIFT && !ns) return PDG_OK;  // Euler has no lifting kernel
+    KParams P = base_params(c);
+    P.u = us;
+    P.un = stage > 0 ? un : us;
+    P.out = uout;
+    P.stage = stage;
+    P.dt = dt;
+    P.vbuf = c->vbuf;
+    P.e_begin = e_begin;
+    P.e_end = e_end;
+    const int kind = part == PDG_PART_FACES ? (ns ? KIND_LIFT_FACE_FLUX : KIND_FACE_FLUX)
+                     : part == PDG_PART_LIFT ? KIND_LIFT
+                                             : (ns ? KIND_NS_FACES_FB : KIND_EULER_FACES_FB);
+    return launch(c, kind, P, s);
+}
+
+int pdg_face_columns(pdg_ctx *c, double **cols, int64_t *count)
+{
+    if (!c || !cols || !count) return PDG_ERR_ARG;
+    if (!c->p.parabolic) return fail(c, PDG_ERR_ARG, "pdg_face_columns: operator is not parabolic");
+    const int64_t nfn = c->dim == 2 ? c->Np : c->Np * c->Np;
+    *cols = c->fcol;
+    *count = 2 * c->dim * c->ne * nfn * (c->nv - 1);
+    return PDG_OK;
+}
+
 int pdg_profile_enable(pdg_ctx *c, int on)
 {
     if (!c) return PDG_ERR_ARG;

@@ -178,3 +178,176 @@ class DistributedRK3:
         if self.dec.world > 1:
             dist.all_reduce(t, op=dist.ReduceOp.MAX, group=self.xchg.group)
         return float(t.item())
+
+
+class FaceTraceHalo:
+    """Face-trace exchange of a slab decomposition for the stage-part
+    driver (TraceHaloRK3).  Per stage a rank needs, of each ghost layer, only
+    the face shared with its own slab: the state at the ghost's face nodes
+    before the face-node kernel, and (Navier-Stokes) the ghost's viscous
+    columns at those nodes after the lifting kernel.  It sends the same of
+    its own first and last owned layers, the shared-face exchange of the
+    reference (``ExchangeFaceNbrData``, src/Operators/NonlinearForm/
+    DGSEMNonlinearForm.cpp:748; gradients :1426-1429) restricted to the face
+    nodes that are read.  Face traces are gathered into contiguous buffers
+    (per variable, per element, the Np^(d-1) nodes of the face are contiguous
+    in the byNODES layout); face columns of a layer are contiguous already.
+
+    Bytes per stage and rank: 2 faces x layer elements x Np^(d-1) x (nv
+    traces + (nv - 1) columns) doubles, against 2 x layer elements x Np^d x nv
+    for whole ghost layers (GhostExchange)."""
+
+    def __init__(self, dec: SlabDecomposition, group=None):
+        if dec.world < 2 or dec.ghost_lo_pos == dec.ghost_hi_pos or dec.owned_count < 2:
+            raise ValueError("face-trace halo needs two distinct ghost layers and two owned layers per rank")
+        self.dec = dec
+        self.group = group
+        g = dec.glob
+        self.nv, self.nd, self.ls = g.nv, g.ndof, dec.layer_size
+        self.fn = g.Np ** (g.dim - 1)  # nodes per face; the face of position 0 / N along the slab axis
+        self.bottom = dec.owned_first
+        self.top = dec.owned_first + dec.owned_count - 1
+        self.prev = (dec.rank - 1) % dec.world
+        self.next = (dec.rank + 1) % dec.world
+
+    def layer(self, pos):
+        """Element range of local layer position pos."""
+        return pos * self.ls, (pos + 1) * self.ls
+
+    def _face(self, u, pos, high):
+        """View [nv, layer elements, face nodes] of layer pos's face at
+        position N (high) or 0 along the slab axis."""
+        a, b = self.layer(pos)
+        v = u.view(self.nv, -1, self.nd)[:, a:b]
+        return v[:, :, self.nd - self.fn:] if high else v[:, :, :self.fn]
+
+    def trace_sends(self, us):
+        """(to prev, to next): the first owned layer's low face and the last
+        owned layer's high face, packed."""
+        return self._face(us, self.bottom, False).contiguous(), self._face(us, self.top, True).contiguous()
+
+    def trace_recv_buffers(self, us):
+        shape = (self.nv, self.ls, self.fn)
+        return us.new_empty(shape), us.new_empty(shape)  # (from next: ghost_hi's low face, from prev: ghost_lo's high face)
+
+    def trace_unpack(self, us, from_next, from_prev):
+        self._face(us, self.dec.ghost_hi_pos, False).copy_(from_next)
+        self._face(us, self.dec.ghost_lo_pos, True).copy_(from_prev)
+
+    def column_sends(self, cols):
+        """(to prev, to next): the first owned layer's low-face columns and the
+        last owned layer's high-face columns (cols = op.face_columns())."""
+        d = self.dec.dim - 1
+        a, b = self.layer(self.bottom)
+        c, e = self.layer(self.top)
+        return cols[d, 0, a:b], cols[d, 1, c:e]
+
+    def column_recvs(self, cols):
+        """(from next, from prev): the ghost layers' slots, received in place."""
+        d = self.dec.dim - 1
+        a, b = self.layer(self.dec.ghost_hi_pos)
+        c, e = self.layer(self.dec.ghost_lo_pos)
+        return cols[d, 0, a:b], cols[d, 1, c:e]
+
+    def post(self, to_prev, to_next, from_next, from_prev):
+        """Starts the four point-to-point messages, in the same order on every
+        rank (to prev, to next; from next, from prev); returns the requests."""
+        import torch.distributed as dist
+        ops = [dist.P2POp(dist.isend, to_prev, self.prev, self.group),
+               dist.P2POp(dist.isend, to_next, self.next, self.group),
+               dist.P2POp(dist.irecv, from_next, self.next, self.group),
+               dist.P2POp(dist.irecv, from_prev, self.prev, self.group)]
+        return dist.batch_isend_irecv(ops)
+
+
+class TraceHaloRK3:
+    """SSP-RK3 on a slab decomposition exchanging face traces only, with the
+    elements that need no neighbour rank's data computed while the messages
+    are in flight (pdg_rk_stage_part over element ranges of the local layers).
+
+    Per stage, with b and t the first and last owned layers and gl, gh the
+    ghost layers:
+      post the face traces;
+      face-node kernel over layers b..t-1, lifting kernel over b+1..t-1,
+      volume kernel over b+2..t-2 (none of them reads a ghost);
+      wait for the traces; face-node kernel over gl and t, lifting kernel over
+      b and t; post the face columns (Navier-Stokes);
+      volume kernel over b+1 and t-1;
+      wait for the columns; volume kernel over b and t.
+    The ghost layers hold state only at their shared face (their other nodes
+    are never read for an owned result), so owned results equal the
+    undivided mesh's bit for bit, as with whole ghost layers."""
+
+    def __init__(self, dec: SlabDecomposition, op, group=None):
+        self.dec, self.op = dec, op
+        self.halo = FaceTraceHalo(dec, group)
+        self.ns = bool(op.params.parabolic)
+        self._a = self._b = None
+
+    def stage_parts(self, stage: int, dt: float, un, us, out):
+        """One stage as a generator: it yields ("traces", sends, recvs) and
+        ("columns", sends, recvs) where the caller must deliver the messages
+        (sends are (to prev, to next), recvs (from next, from prev)), and
+        finishes the stage when resumed after the last one."""
+        import prandtl_b200 as pb
+        h, op = self.halo, self.op
+        b, t = h.bottom, h.top
+        ls = h.ls
+
+        def run(part, first, last):  # layers first..last inclusive
+            if last >= first:
+                op.rk_stage_part(part, stage, dt, un, us, out, first * ls, (last + 1) * ls)
+
+        op.rk_stage_part(pb.PART_START, stage, dt, un, us, out, 0, 0)
+        sends = h.trace_sends(us)
+        recvs = h.trace_recv_buffers(us)
+        yield ("traces", sends, recvs)
+        run(pb.PART_FACES, b, t - 1)
+        if self.ns:
+            run(pb.PART_LIFT, b + 1, t - 1)
+        run(pb.PART_VOLUME, b + 2, t - 2)
+        yield ("wait", None, None)
+        h.trace_unpack(us, *recvs)
+        run(pb.PART_FACES, self.dec.ghost_lo_pos, self.dec.ghost_lo_pos)
+        run(pb.PART_FACES, t, t)
+        if self.ns:
+            run(pb.PART_LIFT, b, b)
+            run(pb.PART_LIFT, t, t)
+            cols = op.face_columns()
+            yield ("columns", h.column_sends(cols), h.column_recvs(cols))
+        edge = sorted({b + 1, t - 1} - {b, t})
+        for layer in edge:
+            if not (b + 2 <= layer <= t - 2):
+                run(pb.PART_VOLUME, layer, layer)
+        if self.ns:
+            yield ("wait", None, None)
+        run(pb.PART_VOLUME, b, b)
+        if t != b:
+            run(pb.PART_VOLUME, t, t)
+
+    def _stage(self, stage, dt, un, us, out):
+        pending = None
+        for kind, sends, recvs in self.stage_parts(stage, dt, un, us, out):
+            if kind == "wait":
+                for r in pending:
+                    r.wait()
+                pending = None
+            else:
+                pending = self.halo.post(sends[0], sends[1], recvs[0], recvs[1])
+
+    def step(self, x, dt: float):
+        if self._a is None or self._a.shape != x.shape:
+            self._a, self._b = x.clone(), x.clone()
+        a, b = self._a, self._b
+        self._stage(0, dt, x, x, a)
+        self._stage(1, dt, x, a, b)
+        self._stage(2, dt, x, b, x)
+        return x
+
+    def max_char_speed(self, local_speed: float, device=None) -> float:
+        """Global running maximum wave speed (MPI_Allreduce MAX in the reference)."""
+        import torch
+        import torch.distributed as dist
+        t = torch.tensor([local_speed], dtype=torch.float64, device=device)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX, group=self.halo.group)
+        return float(t.item())

@@ -122,3 +122,84 @@ def test_decomposition_layout():
             assert np.all(np.diff(d.global_elements) > 0)
             assert d.mesh.nbr.min() >= 0 and d.mesh.nbr.max() < d.mesh.num_elements
         assert sorted(owned) == list(range(3 * 2 * 6))
+
+
+def _trace_worker(rank, world, port, dim, q):
+    """Face-trace halo plumbing on CPU tensors: ghost face nodes and ghost
+    face-column slots, zeroed first, must receive their owners' values."""
+    import torch.distributed as dist
+    os.environ["OMP_NUM_THREADS"] = "1"
+    import sys
+    sys.path.insert(0, ROOT)
+    from prandtl_b200.distributed import FaceTraceHalo
+    dist.init_process_group("gloo", init_method=f"tcp://127.0.0.1:{port}", rank=rank, world_size=world)
+    try:
+        n = (3, 2, 2 * world + 2) if dim == 3 else (4, 2 * world + 1)
+        dec = SlabDecomposition(dim, 2, n, 0.0, 1.0, world, rank)
+        g = dec.glob
+        u0 = np.arange(g.size, dtype=np.float64) * 1e-3 + 1.0
+        x = torch.from_numpy(dec.scatter(u0))
+        h = FaceTraceHalo(dec)
+        X = x.view(g.nv, -1, g.ndof)
+        for pos in (dec.ghost_lo_pos, dec.ghost_hi_pos):
+            a, b = h.layer(pos)
+            X[:, a:b] = 0.0
+        # face columns: owned slots hold a function of the global element
+        ne, fn = dec.mesh.num_elements, g.Np ** (dim - 1)
+        ge = torch.from_numpy(dec.global_elements.astype(np.float64))
+        cols = torch.zeros((dim, 2, ne, fn, dim + 1), dtype=torch.float64)
+        own = slice(*h.layer(h.bottom)[:1], h.layer(h.top)[1])
+        val = (ge[:, None, None] * 1000 + torch.arange(fn, dtype=torch.float64)[None, :, None] * 10 +
+               torch.arange(dim + 1, dtype=torch.float64)[None, None, :])
+        for d in range(dim):
+            for side in range(2):
+                cols[d, side, own] = val[own] + 0.5 * side + 0.25 * d
+        sends, recvs = h.trace_sends(x), h.trace_recv_buffers(x)
+        for r in h.post(sends[0], sends[1], recvs[0], recvs[1]):
+            r.wait()
+        h.trace_unpack(x, *recvs)
+        cs, cr = h.column_sends(cols), h.column_recvs(cols)
+        for r in h.post(cs[0], cs[1], cr[0], cr[1]):
+            r.wait()
+        U = u0.reshape(g.nv, g.num_elements, g.ndof)
+        err = 0.0
+        for pos, high in ((dec.ghost_lo_pos, True), (dec.ghost_hi_pos, False)):
+            a, b = h.layer(pos)
+            gl = dec.global_elements[a:b]
+            want = U[:, gl, g.ndof - fn:] if high else U[:, gl, :fn]
+            got = X[:, a:b, g.ndof - fn:] if high else X[:, a:b, :fn]
+            err = max(err, float(np.abs(got.numpy() - want).max()))
+            side = 1 if high else 0
+            wc = val[a:b] + 0.5 * side + 0.25 * (dim - 1)
+            err = max(err, float((cols[dim - 1, side, a:b] - wc).abs().max()))
+        q.put((rank, err))
+    finally:
+        dist.destroy_process_group()
+
+
+@pytest.mark.parametrize("world,dim", [(2, 3), (3, 3), (2, 2), (4, 2)])
+def test_face_trace_halo_delivers_owner_values(world, dim):
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_trace_worker, args=(r, world, port, dim, q)) for r in range(world)]
+    for p in procs:
+        p.start()
+    res = [q.get(timeout=300) for _ in range(world)]
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    for rank, err in res:
+        assert err == 0.0, f"rank {rank}: {err}"
+
+
+def test_face_trace_halo_bytes():
+    """Per stage and rank: face traces + face columns against whole ghost layers."""
+    from prandtl_b200.distributed import FaceTraceHalo
+    dec = SlabDecomposition(3, 3, (32, 32, 64), 0.0, 1.0, 2, 0)
+    h = FaceTraceHalo(dec)
+    g = dec.glob
+    trace = 2 * h.ls * h.fn * (g.nv + g.nv - 1) * 8
+    layers = 2 * h.ls * g.ndof * g.nv * 8
+    assert trace == 2 * 1024 * 16 * 9 * 8 and layers == 2 * 1024 * 64 * 5 * 8
+    assert layers / trace > 2.2
