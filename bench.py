@@ -374,10 +374,10 @@ def run_ours(args):
            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
            "config": config_dict(mesh, world), "e2e": e2e, "gpu_launches": launches,
            "roofline": roofline, "clocks": clocks}
-    if args.sweep_steps > 0 and world == 1:
-        out["sweep"] = run_sweep(args, dev)
     if not args.no_adjoint and world == 1:
         out["adjoint"] = run_adjoint(args, dev)
+    if args.sweep_steps > 0 and world == 1:
+        out["sweep"] = run_sweep(args, dev)
     if args.sweep_steps > 0 and world == 1 and COMPAT == 0:
         out["reference_operator"] = run_reference_operator(args, dev)
     if args.sweep_steps > 0 and world == 1:
