@@ -13,10 +13,8 @@
 //                    node to a buffer;
 //   adj_gather_kernel adds them to ubar, then (an RK stage's adjoint) the
 //                    stage algebra.
-// Order of a product: adj_rhs_kernel on the caller's stream while, on a
-// second stream, (NS: lift_face_kernel for the forward jumps,
-// adj_lift_kernel into a buffer of its own,) adj_faces_kernel run; then
-// adj_gather_kernel.
+// Order of a product: (NS: lift_face_kernel for the forward jumps,)
+// adj_rhs_kernel, (NS: adj_lift_kernel,) adj_faces_kernel, adj_gather_kernel.
 // The reference has no adjoint; each reversed step names the forward
 // function it reverses.
 #pragma once
@@ -458,8 +456,7 @@ __global__ void __launch_bounds__(128, (DIM == 3 && N == 3) ? PDG_ADJ_RHS_MIN_BL
     }
 }
 
-// Adjoint of the viscous terms (lift_kernel in reverse): stores them to ubar
-// (a buffer of its own: the gather kernel adds it to the volume terms).
+// Adjoint of the viscous terms (lift_kernel in reverse): adds them to ubar.
 // cot: cotangent of dudt; P.lbuf holds the forward BR1 face jumps
 // (lift_face_kernel of u); gcol receives, at every face node, the cotangent
 // of the face-normal entropy-variable gradient ([d][side][e][face node][v]).
@@ -663,7 +660,7 @@ __global__ void __launch_bounds__(AdjLiftLaunch<DIM, N>::threads, AdjLiftLaunch<
                     }
                     entropy_vars_vjp<DIM>(s, wb, P.gamma, P.gm1, P.gm1inv, sacc[k]);
 #pragma unroll
-                    for (int v = 0; v < NV; v++) ubar[v * nn + e * NDOF + n] = sacc[k][v];
+                    for (int v = 0; v < NV; v++) ubar[v * nn + e * NDOF + n] += sacc[k][v];
                 }
             }
         }
@@ -774,9 +771,8 @@ __global__ void __launch_bounds__(256, PDG_ADJ_FACES_MIN_BLOCKS) adj_faces_kerne
     }
 }
 
-// ubar += (Navier-Stokes) the viscous terms in P.vbar, then the face-term
-// cotangents of gbuf at every face node (in the order x, y [, z] faces), one
-// thread per node.  With P.stage >= 0 the RK stage's
+// ubar += the face-term cotangents of gbuf at every face node (in the order
+// x, y [, z] faces), one thread per node.  With P.stage >= 0 the RK stage's
 // adjoint follows: for stage s of out = a_s un + b_s (us + dt L(us)) and the
 // cotangent lam (cot) of out, with g = ubar = (dL/dus)^T lam,
 //   stage 2: ubar = 2/3 (lam + dt g), bx = 1/3 lam;
@@ -808,7 +804,6 @@ __global__ void __launch_bounds__(256) adj_gather_kernel(const KParams P, const 
         for (int v = 0; v < NV; v++) {
             const int64_t gi = v * nn + t;
             double x = ubar[gi];
-            if (P.vbar) x = x + __ldg(P.vbar + gi);  // the viscous terms (adj_lift_kernel)
 #pragma unroll
             for (int d = 0; d < DIM; d++)
                 if (src[d]) x += __ldg(src[d] + v * NFN);

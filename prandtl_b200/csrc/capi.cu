@@ -57,9 +57,6 @@ struct pdg_ctx {
     unsigned long long *limit_count = nullptr;  // positivity limiter applications
     double *gcol = nullptr;   // adjoint: cotangents of the face-normal entropy gradients
     double *gbuf = nullptr;   // adjoint: face-term cotangents of both sides of every face node
-    double *vbar = nullptr;   // adjoint (NS): the viscous terms' cotangent
-    cudaStream_t adj_side = nullptr;               // adjoint: second stream of the fork
-    cudaEvent_t adj_fork = nullptr, adj_join = nullptr;
     // pdg_rk3_steps: one step captured in a CUDA graph for a (state, dt) pair
     cudaStream_t cap = nullptr;
     cudaGraph_t graph = nullptr;
@@ -773,10 +770,6 @@ int pdg_destroy(pdg_ctx *c)
     cudaFree(c->ent_own);
     cudaFree(c->gcol);
     cudaFree(c->gbuf);
-    cudaFree(c->vbar);
-    if (c->adj_fork) cudaEventDestroy(c->adj_fork);
-    if (c->adj_join) cudaEventDestroy(c->adj_join);
-    if (c->adj_side) cudaStreamDestroy(c->adj_side);
     if (c->graph_exec) cudaGraphExecDestroy(c->graph_exec);
     if (c->graph) cudaGraphDestroy(c->graph);
     if (c->cap) cudaStreamDestroy(c->cap);
@@ -1215,23 +1208,16 @@ int vjp_setup(pdg_ctx *c)
     const size_t nfn = c->dim == 2 ? c->Np : c->Np * c->Np;
     if (c->p.parabolic && cudaMalloc(&c->gcol, sizeof(double) * 2 * c->dim * c->ne * nfn * c->nv) != cudaSuccess)
         return fail(c, PDG_ERR_NOMEM, "pdg_rhs_vjp: scratch allocation failed");
-    if (cudaMalloc(&c->gbuf, sizeof(double) * 2 * c->dim * c->ne * nfn * c->nv) != cudaSuccess ||
-        (c->p.parabolic && cudaMalloc(&c->vbar, sizeof(double) * c->size) != cudaSuccess))
+    if (cudaMalloc(&c->gbuf, sizeof(double) * 2 * c->dim * c->ne * nfn * c->nv) != cudaSuccess)
         return fail(c, PDG_ERR_NOMEM, "pdg_rhs_vjp: scratch allocation failed");
-    if (cudaStreamCreateWithFlags(&c->adj_side, cudaStreamNonBlocking) != cudaSuccess ||
-        cudaEventCreateWithFlags(&c->adj_fork, cudaEventDisableTiming) != cudaSuccess ||
-        cudaEventCreateWithFlags(&c->adj_join, cudaEventDisableTiming) != cudaSuccess)
-        return fail(c, PDG_ERR_CUDA, "pdg_rhs_vjp: stream or event creation failed");
     c->adj_ready = true;
     return PDG_OK;
 }
 
-// The volume terms to ubar on the caller's stream while a second stream
-// runs (NS: the forward BR1 jumps, the viscous terms to vbar,) every face's
-// adjoint terms to gbuf — the two chains read nothing of each other — then,
-// joined, their sum into ubar with, for stage >= 0, the RK stage's adjoint
-// (adj_gather_kernel).  Boundary faces (Euler, stage < 0 only) are added to
-// ubar last.
+// (NS: the forward BR1 jumps,) the volume terms to ubar, (NS: the viscous
+// terms added,) every face's adjoint terms to gbuf, then their sum into ubar
+// with, for stage >= 0, the RK stage's adjoint (adj_gather_kernel).  Boundary
+// faces (Euler, stage < 0 only) are added to ubar last.
 int vjp(pdg_ctx *c, int stage, double dt, const double *u, const double *cot, double *ubar, double *bx,
         cudaStream_t s)
 {
@@ -1244,19 +1230,11 @@ int vjp(pdg_ctx *c, int stage, double dt, const double *u, const double *cot, do
     P.dt = dt;
     P.bx = bx;
     c->last_stream = s;
-    P.vbar = c->vbar;  // null for Euler
     void *a_cot = (void *)&cot, *a_bar = (void *)&ubar, *a_g = (void *)&c->gcol, *a_gb = (void *)&c->gbuf;
-    void *a_vb = (void *)&c->vbar;
-    cudaStream_t side = c->adj_side;
-    CK(cudaEventRecord(c->adj_fork, s), "event record");
-    CK(cudaStreamWaitEvent(side, c->adj_fork, 0), "stream wait");
+    if (c->p.parabolic && (r = launch(c, KIND_LIFT_FACE, P, s))) return r;
     if ((r = launch_with(c, KIND_ADJ_RHS, P, a_cot, a_bar, nullptr, s))) return r;
-    if (c->p.parabolic && (r = launch(c, KIND_LIFT_FACE, P, side))) return r;
-    if (c->p.parabolic && (r = launch_with(c, KIND_ADJ_LIFT, P, a_cot, a_vb, a_g, side))) return r;
-    if ((r = launch_with(c, c->p.parabolic ? KIND_ADJ_FACE_NS0 : KIND_ADJ_FACE_E0, P, a_cot, a_gb, a_g, side)))
-        return r;
-    CK(cudaEventRecord(c->adj_join, side), "event record");
-    CK(cudaStreamWaitEvent(s, c->adj_join, 0), "stream wait");
+    if (c->p.parabolic && (r = launch_with(c, KIND_ADJ_LIFT, P, a_cot, a_bar, a_g, s))) return r;
+    if ((r = launch_with(c, c->p.parabolic ? KIND_ADJ_FACE_NS0 : KIND_ADJ_FACE_E0, P, a_cot, a_gb, a_g, s))) return r;
     if ((r = launch_with(c, KIND_ADJ_GATHER, P, a_cot, a_bar, nullptr, s))) return r;
     if (!c->p.parabolic && c->bc_used && (r = launch_with(c, KIND_ADJ_BOUNDARY, P, a_cot, a_bar, a_g, s))) return r;
     return PDG_OK;

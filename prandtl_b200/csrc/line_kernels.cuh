@@ -97,7 +97,6 @@ struct KParams {
     // adjoint stage
     const double *gbuf;
     double *bx;
-    const double *vbar;  // adjoint (Navier-Stokes): the viscous terms' cotangent (adj_lift_kernel)
     // elements [e_begin, e_end) that the face-node, lifting and volume
     // kernels process (e_end = 0: up to ne); nwt counts the range's tiles
     int64_t e_begin, e_end;
