@@ -110,6 +110,41 @@ void pdg_default_params(pdg_params *p);
 int pdg_create(const pdg_mesh *mesh, const pdg_params *params, pdg_ctx **out);
 int pdg_destroy(pdg_ctx *ctx);
 
+/* General geometry: skewed, graded, curved or unstructured quadrilaterals and
+ * hexahedra (the reference's meshes as MFEM reads them, src/Simulation/
+ * Simulation.cpp:271-336; DGSEMIntegrator evaluates MFEM's element
+ * transformation at every node, DGSEMIntegrator.cpp:252-266, forms the
+ * subcell metrics from it, :1199-1304, and the face normals with CalcOrtho,
+ * :186).  x: HOST pointer, dim * num_nodes physical coordinates of the DG
+ * nodes in the byNODES layout (x[k * num_nodes + e * Np^dim + lex]: the
+ * images of the LGL nodes under the element's map; the element's geometry
+ * is their degree-N interpolant).  Faces are taken in each element's own
+ * frame: nbr[e*2*dim + f] with f = 2 d + side along the element's local
+ * axis d.  face_orient: HOST pointer, num_elements * 2*dim codes, or NULL
+ * when every neighbour meets a face with its opposite face (f ^ 1) and
+ * aligned axes.  For an interior face the code is f2 + 8 o: the
+ * neighbour's face f2 that meets face f, and the map o of face-node indices:
+ * with (a, b) this element's node indices along the face's two tangential
+ * axes (ascending axis order; b = 0 in 2D) the neighbour's are (b, a) if
+ * o & 1 else (a, b), then a -> N - a if o & 2, b -> N - b if o & 4 (2D: o
+ * is 0 or 2).  The library forms J and the adjugate at every node, each face
+ * node's normal out of the face's element 1 (the lower-numbered element)
+ * and the CFL length, the smallest singular value of the Jacobian at an
+ * element centre (MFEM's GetElementSize(e, 1), Simulation.cpp:896-906),
+ * which replaces mesh->h.  Call once, before the first evaluation.  Euler
+ * (parabolic = 0) without filter; both operators (compat changes the 3D
+ * face dissipation term, the running maximum wave speed and the subsonic
+ * conditions' in-place divisions, as on box meshes); every boundary
+ * condition type.  One kernel per right-hand side or RK stage
+ * (PDG_KERNEL_GEO).  pdg_rhs_vjp, pdg_rk_stage_vjp and pdg_rk_stage_part
+ * return PDG_ERR_UNSUPPORTED on such a context; pdg_rk3_step_host copies
+ * the state whole.  PDG_ERR_ARG: a non-positive Jacobian at a node, a code
+ * whose neighbour face does not point back, or a neighbour whose normal at
+ * the matching node is not the opposite of this element's (a non-conforming
+ * face or a wrong code); PDG_ERR_UNSUPPORTED: a Navier-Stokes or filtered
+ * operator. */
+int pdg_set_geometry(pdg_ctx *ctx, const double *x, const int32_t *face_orient);
+
 /* Boundary conditions (the integrators of src/Integrators/BoundaryConditions/, attached to
  * boundary attributes by DGSEMOperator::AddBdrFaceIntegrator,
  * src/Operators/DGSEMOperator.cpp:593 and src/Simulation/Simulation.cpp:
@@ -365,6 +400,7 @@ int64_t pdg_launch_count(const pdg_ctx *ctx);
 #define PDG_KERNEL_LIFT_FACE_FLUX 32 /* face-node kernel: BR1 jumps + inviscid face fluxes into the buffer */
 #define PDG_KERNEL_FACE_FLUX 33      /* face-node kernel: inviscid face fluxes into the buffer (Euler) */
 #define PDG_KERNEL_POSITIVITY 34     /* positivity limiter of a stage output */
+#define PDG_KERNEL_GEO 35            /* Euler right-hand side on a general-geometry mesh (pdg_set_geometry) */
 int pdg_profile_enable(pdg_ctx *ctx, int on);
 int pdg_profile_read(pdg_ctx *ctx, int kind, double *total_ms, int64_t *launches);
 

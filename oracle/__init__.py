@@ -78,6 +78,8 @@ def lib(fma: bool = False):
         L.orc_limited_elements.restype = C.c_int64
         L.orc_limited_elements.argtypes = [C.c_void_p]
         L.orc_positivity_apply.argtypes = [C.c_void_p, _dp]
+        L.orc_set_geometry.restype = C.c_int
+        L.orc_set_geometry.argtypes = [C.c_void_p, _dp, _ip]
         L.orc_gll.argtypes = [C.c_int, _dp, _dp]
         L.orc_derivative_matrices.argtypes = [C.c_int, _dp, _dp, _dp]
         L.orc_logmean.restype = C.c_double
@@ -111,6 +113,12 @@ class Oracle:
             raise ValueError("orc_create rejected the mesh/params")
         for b, (typ, state) in (getattr(mesh, "boundaries", None) or {}).items():
             self.set_boundary(b, typ, state)
+        if getattr(mesh, "coords", None) is not None:
+            self._x = np.ascontiguousarray(mesh.coords, dtype=np.float64)
+            fo = getattr(mesh, "face_orient", None)
+            self._fo = None if fo is None else np.ascontiguousarray(fo, dtype=np.int32)
+            if self._L.orc_set_geometry(self.h, _ptr(self._x), None if self._fo is None else self._fo.ctypes.data_as(_ip)):
+                raise ValueError("orc_set_geometry rejected the geometry")
 
     def set_boundary(self, index: int, typ: int, state=None):
         st = None if state is None else np.ascontiguousarray(state, dtype=np.float64)
@@ -187,6 +195,9 @@ def ref_lib(parabolic: bool):
         L.ref_create.restype = C.c_void_p
         L.ref_create.argtypes = [C.c_int, C.c_int, C.c_int, _dp, _ip, C.c_double, C.c_double,
                                  C.c_double, C.c_double, C.c_double]
+        L.ref_create_geo.restype = C.c_void_p
+        L.ref_create_geo.argtypes = [C.c_int, C.c_int, C.c_int, _ip, _dp, _ip, C.c_double, C.c_double,
+                                     C.c_double, C.c_double, C.c_double]
         L.ref_destroy.argtypes = [C.c_void_p]
         L.ref_set_boundary.argtypes = [C.c_void_p, C.c_int, C.c_int, _dp]
         L.ref_rhs.restype = C.c_double
@@ -215,8 +226,16 @@ class Reference:
         self._nbr = np.ascontiguousarray(mesh.nbr, dtype=np.int32)
         h = np.array(list(mesh.h) + [1.0] * (3 - mesh.dim))
         self._h = h
-        self.h = self.L.ref_create(mesh.dim, mesh.order, mesh.num_elements, _ptr(h),
-                                   self._nbr.ctypes.data_as(_ip), gamma, Pr, mu, alpha_max, alpha_min)
+        if getattr(mesh, "coords", None) is not None:
+            self._x = np.ascontiguousarray(mesh.coords, dtype=np.float64)
+            fo = getattr(mesh, "face_orient", None)
+            self._fo = None if fo is None else np.ascontiguousarray(fo, dtype=np.int32)
+            self.h = self.L.ref_create_geo(mesh.dim, mesh.order, mesh.num_elements, self._nbr.ctypes.data_as(_ip),
+                                           _ptr(self._x), None if self._fo is None else self._fo.ctypes.data_as(_ip),
+                                           gamma, Pr, mu, alpha_max, alpha_min)
+        else:
+            self.h = self.L.ref_create(mesh.dim, mesh.order, mesh.num_elements, _ptr(h),
+                                       self._nbr.ctypes.data_as(_ip), gamma, Pr, mu, alpha_max, alpha_min)
         for b, (typ, state) in (getattr(mesh, "boundaries", None) or {}).items():
             st = None if state is None else np.ascontiguousarray(state, dtype=np.float64)
             if self.L.ref_set_boundary(self.h, int(b), int(typ), None if st is None else _ptr(st)):

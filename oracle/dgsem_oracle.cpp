@@ -399,6 +399,14 @@ struct Ctx {
     int64_t filtered_elements;
     int64_t limited_elements;           // positivity limiter applications
     double bc[16][8] = {};              // boundary conditions: type, prescribed state
+    // general geometry (orc_set_geometry): per node J and adjugate rows, the
+    // subcell normals per element, direction, line and interface, and per
+    // element face node the neighbour's face and matching node
+    bool geo = false;
+    std::vector<double> gJ, gadj;       // gJ[e*ndof + n], gadj[((e*ndof + n)*3 + r)*3 + k]
+    std::vector<double> gsnor;          // [e][d][line][i = 0..Np][k]
+    std::vector<int> gface;             // neighbour's face per element face
+    std::vector<int> gnode;             // [e][f][t]: neighbour's node matching face node t
 };
 
 static inline int64_t idx(const Ctx &c, int v, int64_t e, int n)
@@ -1254,8 +1262,230 @@ static void lifting(Ctx &c, const double *u)
 
 // DGSEMOperator::Mult (DGSEMOperator.cpp:537-591) with the loops of
 // DGSEMNonlinearForm::Mult (DGSEMNonlinearForm.cpp:647-849, 1302-1548).
+// ---------------------------------------------------------------------------
+// General geometry (Euler): the same steps with the metric terms of every
+// node (DGSEMIntegrator.cpp:252-266: Tr.SetIntPoint, Weight, AdjugateJacobian
+// at each integration point), the subcell metrics of ComputeSubcellMetrics
+// (:1199-1304) and the faces' CalcOrtho normals out of element 1 (:186).
+// ---------------------------------------------------------------------------
+static inline const double *gadj_row(const Ctx &c, int64_t e, int n, int r)
+{
+    return &c.gadj[(((size_t)e * c.ndof + n) * 3 + r) * 3];
+}
+static inline double gJ(const Ctx &c, int64_t e, int n) { return c.gJ[(size_t)e * c.ndof + n]; }
+
+// ComputeFVFluxes (DGSEMIntegrator.cpp:972-1196) on element e with its subcell
+// metrics; dU is divided by the node's own J times w.
+static double fv_fluxes_geo(const Ctx &c, int64_t e, const double *el_u, double alpha_value, double *el_dudt)
+{
+    const int Np = c.Np, nv = c.nv, dim = c.dim, nfn = c.ndof / Np;
+    const int Npy = dim > 1 ? Np : 1, Npz = dim > 2 ? Np : 1;
+    double lam = -1.0;
+    double dU[5], flux[5];
+    for (int dd = 0; dd < dim; dd++) {
+        int A = (dd == 2) ? Npy : Npz;
+        int B = (dd == 0) ? Npy : Np;
+        for (int a = 0; a < A; a++)
+            for (int b = 0; b < B; b++) {
+                int i = 0, j = 0, k = 0;
+                if (dd == 0) { k = a; j = b; }
+                else if (dd == 1) { k = a; i = b; }
+                else { j = a; i = b; }
+                const int line = dd == 0 ? j + Np * k : dd == 1 ? i + Np * k : i + Np * j;
+                const double *sn = &c.gsnor[((((size_t)e * dim + dd) * nfn + line) * (Np + 1)) * 3];
+                for (int v = 0; v < nv; v++) dU[v] = 0.0;
+                int id1 = line_node(c, dd, i, j, k, 0);
+                for (int l = 0; l < Np - 1; l++) {
+                    int id2 = line_node(c, dd, i, j, k, l + 1);
+                    const double *nor = sn + (size_t)(l + 1) * 3;
+                    const double *s1 = el_u + id1 * nv, *s2 = el_u + id2 * nv;
+                    lam = std::max(lam, face_flux(dim, c.p.gamma, c.p.compat, c.p.face_dissipation, s1, s2, nor, flux));
+                    for (int v = 0; v < nv; v++) {
+                        dU[v] -= flux[v];
+                        dU[v] /= gJ(c, e, id1) * c.w[l];
+                    }
+                    for (int v = 0; v < nv; v++) {
+                        if (dd == 0) el_dudt[id1 * nv + v] = dU[v];
+                        else el_dudt[id1 * nv + v] += dU[v];
+                    }
+                    for (int v = 0; v < nv; v++) dU[v] = flux[v];
+                    id1 = id2;
+                }
+                for (int v = 0; v < nv; v++) {
+                    dU[v] /= gJ(c, e, id1) * c.w[Np - 1];
+                    if (dd == 0) el_dudt[id1 * nv + v] = dU[v];
+                    else el_dudt[id1 * nv + v] += dU[v];
+                }
+            }
+    }
+    for (int i = 0; i < c.ndof * nv; i++) el_dudt[i] *= alpha_value;
+    return lam;
+}
+
+// AssembleElementVector, Euler (DGSEMIntegrator.cpp:224-433): two-point
+// fluxes with both nodes' metric rows, divided by the node's J.
+static double element_vector_geo(const Ctx &c, int64_t e, const double *el_u, double alpha, double *el_dudt)
+{
+    const int Np = c.Np, nv = c.nv, dim = c.dim, nd = c.ndof;
+    const int Npy = dim > 1 ? Np : 1, Npz = dim > 2 ? Np : 1;
+    double lam = -1.0;
+    for (int i = 0; i < nd * nv; i++) el_dudt[i] = 0.0;
+    if (c.p.blending) lam = std::max(lam, fv_fluxes_geo(c, e, el_u, alpha, el_dudt));
+    std::vector<double> Fs((size_t)dim * nd * Np * nv, 0.0);
+    auto FS = [&](int d, int n, int m) -> double * { return &Fs[(((size_t)d * nd + n) * Np + m) * nv]; };
+    double f[5];
+    for (int k = 0; k < Npz; k++)
+        for (int j = 0; j < Npy; j++)
+            for (int i = 0; i < Np; i++) {
+                const int id1 = (k * Npy + j) * Np + i;
+                const int pos[3] = {i, j, k};
+                for (int d = 0; d < dim; d++) {
+                    for (int v = 0; v < nv; v++) f[v] = 0.0;
+                    std::memcpy(FS(d, id1, pos[d]), f, sizeof(double) * nv);
+                    for (int m = pos[d] + 1; m < Np; m++) {
+                        const int id2 = line_node(c, d, i, j, k, m);
+                        lam = std::max(lam, volume_flux(dim, c.p.gamma, el_u + id1 * nv, el_u + id2 * nv,
+                                                        gadj_row(c, e, id1, d), gadj_row(c, e, id2, d), f));
+                        std::memcpy(FS(d, id1, m), f, sizeof(double) * nv);
+                        std::memcpy(FS(d, id2, pos[d]), f, sizeof(double) * nv);
+                    }
+                }
+            }
+    for (int k = 0; k < Npz; k++)
+        for (int j = 0; j < Npy; j++)
+            for (int i = 0; i < Np; i++) {
+                const int id1 = (k * Npy + j) * Np + i;
+                const int pos[3] = {i, j, k};
+                double dU[5];
+                for (int v = 0; v < nv; v++) dU[v] = 0.0;
+                for (int d = 0; d < dim; d++)
+                    for (int m = 0; m < Np; m++) {
+                        const double *col = FS(d, id1, m);
+                        const double a = c.Dhat2[pos[d] * Np + m];
+                        for (int v = 0; v < nv; v++) dU[v] += a * col[v];
+                    }
+                for (int v = 0; v < nv; v++) {
+                    double t = -dU[v];
+                    if (c.p.blending) t *= (1.0 - alpha);
+                    t /= gJ(c, e, id1);
+                    el_dudt[id1 * nv + v] += t;
+                }
+            }
+    return lam;
+}
+
+static inline bool is_element1(const Ctx &c, int64_t e, int f)
+{
+    const int64_t nb = c.nbr[e * 2 * c.dim + f];
+    return nb >= 0 && (e < nb || (e == nb && (f & 1)));
+}
+
+// AssembleFaceVector, Euler (DGSEMIntegrator.cpp:151-222) for face f of
+// element a, a being the face's element 1: buf[0][t][v] for a's face nodes,
+// buf[1][t][v] for the neighbour's matching nodes.
+static double face_vector_geo(const Ctx &c, const double *u, int64_t a, int f, double *buf)
+{
+    const int nv = c.nv, dim = c.dim, Np = c.Np, nfn = c.ndof / Np, nf = 2 * dim;
+    const int64_t b = c.nbr[a * nf + f];
+    const int d = f / 2, side = f % 2;
+    double lam = -1.0, s1[5], s2[5], flux[5], nor[3];
+    for (int t = 0; t < nfn; t++) {
+        const int n1 = face_node(c, d, side, t);
+        const int n2 = c.gnode[((size_t)a * nf + f) * nfn + t];
+        for (int v = 0; v < nv; v++) {
+            s1[v] = u[idx(c, v, a, n1)];
+            s2[v] = u[idx(c, v, b, n2)];
+        }
+        const double *row = gadj_row(c, a, n1, d);
+        for (int k = 0; k < dim; k++) nor[k] = side ? row[k] : -row[k];
+        lam = std::max(lam, face_flux(dim, c.p.gamma, c.p.compat, c.p.face_dissipation, s1, s2, nor, flux));
+        const double sc1 = 1.0 / (c.w[0] * gJ(c, a, n1)), sc2 = 1.0 / (c.w[0] * gJ(c, b, n2));
+        for (int v = 0; v < nv; v++) {
+            buf[t * nv + v] = sc1 * (-flux[v]);
+            buf[(size_t)nfn * nv + t * nv + v] = sc2 * flux[v];
+        }
+    }
+    return lam;
+}
+
+// Boundary face f of element e (BdrFaceIntegrator::AssembleFaceVector,
+// BdrFaceIntegrator.cpp:64-130) with the outward normal of the node.
+static double bdr_face_vector_geo(const Ctx &c, const double *u, int64_t e, int f, int b, double *out)
+{
+    const int nv = c.nv, dim = c.dim, nfn = c.ndof / c.Np;
+    const int d = f / 2, side = f % 2;
+    double lam = -1.0, s1[5], flux[5], nor[3];
+    for (int t = 0; t < nfn; t++) {
+        const int n = face_node(c, d, side, t);
+        for (int v = 0; v < nv; v++) s1[v] = u[idx(c, v, e, n)];
+        const double *row = gadj_row(c, e, n, d);
+        for (int k = 0; k < dim; k++) nor[k] = side ? row[k] : -row[k];
+        lam = std::max(lam, bdr_flux(c, b, s1, nor, flux));
+        const double scale = 1.0 / (c.w[0] * gJ(c, e, n));
+        for (int v = 0; v < nv; v++) out[t * nv + v] = scale * (-flux[v]);
+    }
+    return lam;
+}
+
+static void rhs_geo(Ctx &c, const double *u, double *dudt)
+{
+    const int nv = c.nv, dim = c.dim, nd = c.ndof, Np = c.Np, nfn = nd / Np, nf = 2 * dim;
+    if (c.p.blending) blending_coefficient(c, u);
+    else {
+        std::fill(c.alpha.begin(), c.alpha.end(), 0.0);
+        std::fill(c.eta.begin(), c.eta.end(), 0.0);
+    }
+    double lam = -1.0;
+    const size_t fstride = (size_t)2 * nfn * nv;
+#pragma omp parallel for schedule(static) reduction(max : lam)
+    for (int64_t e = 0; e < c.ne; e++)
+        for (int f = 0; f < nf; f++)
+            if (is_element1(c, e, f))
+                lam = std::max(lam, face_vector_geo(c, u, e, f, &c.facebuf[((size_t)e * nf + f) * fstride]));
+#pragma omp parallel for schedule(static) reduction(max : lam)
+    for (int64_t e = 0; e < c.ne; e++) {
+        std::vector<double> el_u(nd * nv), el_d(nd * nv), bface((size_t)nfn * nv);
+        for (int n = 0; n < nd; n++)
+            for (int v = 0; v < nv; v++) el_u[n * nv + v] = u[idx(c, v, e, n)];
+        lam = std::max(lam, element_vector_geo(c, e, el_u.data(), c.alpha[e], el_d.data()));
+        for (int n = 0; n < nd; n++)
+            for (int v = 0; v < nv; v++) dudt[idx(c, v, e, n)] = 0.0 + el_d[n * nv + v];
+        for (int f = 0; f < nf; f++) {
+            const int64_t nb = c.nbr[e * nf + f];
+            const double *mine;
+            if (nb < 0) {
+                lam = std::max(lam, bdr_face_vector_geo(c, u, e, f, (int)(-1 - nb), bface.data()));
+                mine = bface.data();
+            } else if (is_element1(c, e, f)) {
+                mine = &c.facebuf[((size_t)e * nf + f) * fstride];
+            } else {
+                const int f2 = c.gface[e * nf + f];
+                mine = &c.facebuf[((size_t)nb * nf + f2) * fstride] + (size_t)nfn * nv;
+                // the neighbour's face-node order: its node n2 of face node t2 is ours at t
+                std::vector<double> tmp((size_t)nfn * nv);
+                for (int t2 = 0; t2 < nfn; t2++) {
+                    const int n2 = c.gnode[((size_t)nb * nf + f2) * nfn + t2];  // our node
+                    int t = -1;
+                    for (int q = 0; q < nfn; q++)
+                        if (face_node(c, f / 2, f % 2, q) == n2) t = q;
+                    for (int v = 0; v < nv; v++) tmp[(size_t)t * nv + v] = mine[t2 * nv + v];
+                }
+                for (int n = 0; n < nfn * nv; n++) bface[n] = tmp[n];
+                mine = bface.data();
+            }
+            for (int t = 0; t < nfn; t++) {
+                const int n = face_node(c, f / 2, f % 2, t);
+                for (int v = 0; v < nv; v++) dudt[idx(c, v, e, n)] += mine[t * nv + v];
+            }
+        }
+    }
+    c.last_rhs_speed = lam;
+    c.max_char_speed = std::max(c.max_char_speed, lam);
+}
+
 static void rhs(Ctx &c, const double *u, double *dudt)
 {
+    if (c.geo) return rhs_geo(c, u, dudt);
     const int nv = c.nv, dim = c.dim, nd = c.ndof, Np = c.Np, nfn = nd / Np;
     if (c.p.blending) blending_coefficient(c, u);
     else {
@@ -1570,6 +1800,112 @@ void *orc_create(const pdg_mesh *m, const pdg_params *p)
 }
 
 void orc_destroy(void *h) { delete (Ctx *)h; }
+
+// General geometry (Euler): node coordinates x[k*nnodes + e*ndof + n] and
+// face orientation codes (NULL: opposite faces, aligned axes), as
+// pdg_set_geometry takes them.  J and the adjugate at every node from the
+// LGL derivative of the coordinates (MFEM's element transformation at the
+// integration points), the subcell metrics as ComputeSubcellMetrics forms
+// them (DGSEMIntegrator.cpp:1199-1304).  Returns 0, or 1 on a bad input.
+int orc_set_geometry(void *h, const double *x, const int32_t *face_orient)
+{
+    Ctx &c = *(Ctx *)h;
+    const int dim = c.dim, Np = c.Np, N = c.N, nd = c.ndof, nf = 2 * dim, nfn = nd / Np;
+    if (c.p.parabolic) return 1;
+    c.gJ.assign((size_t)c.ne * nd, 0.0);
+    c.gadj.assign((size_t)c.ne * nd * 9, 0.0);
+    for (int64_t e = 0; e < c.ne; e++)
+        for (int n = 0; n < nd; n++) {
+            const int pos[3] = {n % Np, (n / Np) % Np, n / (Np * Np)};
+            double A[3][3] = {};  // A[k][r] = dx_k / dxi_r
+            for (int k = 0; k < dim; k++)
+                for (int r = 0; r < dim; r++) {
+                    double t = 0.0;
+                    for (int l = 0; l < Np; l++) {
+                        const int m = line_node(c, r, pos[0], pos[1], pos[2], l);
+                        t += c.D[pos[r] * Np + l] * x[(size_t)k * c.nnodes + e * nd + m];
+                    }
+                    A[k][r] = t;
+                }
+            double adj[3][3] = {}, det;
+            if (dim == 2) {
+                adj[0][0] = A[1][1];
+                adj[0][1] = -A[0][1];
+                adj[1][0] = -A[1][0];
+                adj[1][1] = A[0][0];
+                det = A[0][0] * A[1][1] - A[0][1] * A[1][0];
+            } else {
+                // cofactor transpose: adj[r][k] = (-1)^(r+k) minor(k, r)
+                for (int r = 0; r < 3; r++)
+                    for (int k = 0; k < 3; k++) {
+                        const int r1 = (r + 1) % 3, r2 = (r + 2) % 3, k1 = (k + 1) % 3, k2 = (k + 2) % 3;
+                        adj[r][k] = A[k1][r1] * A[k2][r2] - A[k1][r2] * A[k2][r1];
+                    }
+                det = A[0][0] * adj[0][0] + A[0][1] * adj[1][0] + A[0][2] * adj[2][0];
+            }
+            if (!(det > 0.0)) return 1;
+            c.gJ[(size_t)e * nd + n] = det;
+            for (int r = 0; r < 3; r++)
+                for (int k = 0; k < 3; k++) c.gadj[(((size_t)e * nd + n) * 3 + r) * 3 + k] = adj[r][k];
+        }
+    // subcell metrics: n_i = row(x_0) + sum_{l<i} w_l sum_m D(l, m) row(x_m)
+    c.gsnor.assign((size_t)c.ne * dim * nfn * (Np + 1) * 3, 0.0);
+    for (int64_t e = 0; e < c.ne; e++)
+        for (int d = 0; d < dim; d++)
+            for (int line = 0; line < nfn; line++) {
+                int fi = 0, fj = 0, fk = 0;
+                if (d == 0) { fj = line % Np; fk = line / Np; }
+                else if (d == 1) { fi = line % Np; fk = line / Np; }
+                else { fi = line % Np; fj = line / Np; }
+                double *out = &c.gsnor[((((size_t)e * dim + d) * nfn + line) * (Np + 1)) * 3];
+                const double *m0 = gadj_row(c, e, line_node(c, d, fi, fj, fk, 0), d);
+                for (int i = 0; i < Np + 1; i++) {
+                    double nor[3] = {0, 0, 0};
+                    for (int k = 0; k < dim; k++) nor[k] = m0[k];
+                    for (int l = 0; l < i; l++) {
+                        double tmp[3] = {0, 0, 0};
+                        for (int m = 0; m < Np; m++) {
+                            const double *mr = gadj_row(c, e, line_node(c, d, fi, fj, fk, m), d);
+                            for (int k = 0; k < dim; k++) {
+                                double t = mr[k];
+                                t *= c.D[l * Np + m];
+                                tmp[k] += t;
+                            }
+                        }
+                        for (int k = 0; k < dim; k++) {
+                            tmp[k] *= c.w[l];
+                            nor[k] += tmp[k];
+                        }
+                    }
+                    for (int k = 0; k < dim; k++) out[(size_t)i * 3 + k] = nor[k];
+                }
+            }
+    // faces: the neighbour's face and the node matching each face node
+    c.gface.assign((size_t)c.ne * nf, 0);
+    c.gnode.assign((size_t)c.ne * nf * nfn, 0);
+    for (int64_t e = 0; e < c.ne; e++)
+        for (int f = 0; f < nf; f++) {
+            const int64_t nb = c.nbr[e * nf + f];
+            if (nb < 0) continue;
+            int f2 = f ^ 1, o = 0;
+            if (face_orient) {
+                f2 = face_orient[e * nf + f] & 7;
+                o = face_orient[e * nf + f] >> 3;
+            }
+            if (f2 >= nf || c.nbr[nb * nf + f2] != e) return 1;
+            c.gface[e * nf + f] = f2;
+            for (int t = 0; t < nfn; t++) {
+                int a = t % Np, b = dim == 3 ? t / Np : 0;
+                if (o & 1) std::swap(a, b);
+                if (o & 2) a = N - a;
+                if (o & 4) b = N - b;
+                c.gnode[((size_t)e * nf + f) * nfn + t] = face_node(c, f2 / 2, f2 % 2, a + Np * b);
+            }
+        }
+    c.facebuf.assign((size_t)c.ne * nf * 2 * nfn * c.nv, 0.0);
+    c.geo = true;
+    return 0;
+}
 
 // Boundary condition `index`: its type and parameters as pdg_set_boundary
 // takes them (types 1, 3: conserved state; 6: p; 7: rho, velocity; 8: cp,

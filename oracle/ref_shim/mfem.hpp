@@ -3,7 +3,8 @@
 // compiled unmodified (in place, from the reference tree) and run as a
 // parity check.  TEST INFRASTRUCTURE ONLY: nothing in the product uses it.
 //
-// Scope: affine, axis-aligned Cartesian quads/hexes; L2 Gauss-Lobatto nodal
+// Scope: affine, axis-aligned Cartesian quads/hexes, or nodal (curved,
+// skewed, unstructured) ones given by their DG nodes' coordinates; L2 Gauss-Lobatto nodal
 // elements; Gauss-Lobatto integration rules on [0,1]; dense linear algebra on
 // column-major matrices.  Semantics that change results are kept as MFEM
 // documents them:
@@ -614,14 +615,84 @@ public:
     const IntegrationRule &Get(int geom, int order);
 };
 
+// Lagrange basis through nodes x (n of them) at t: values L and derivatives dL.
+inline void StandInLagrange(const std::vector<real_t> &x, real_t t, real_t *L, real_t *dL)
+{
+    const int n = (int)x.size();
+    for (int j = 0; j < n; j++) {
+        real_t v = 1.0, dv = 0.0;
+        for (int m = 0; m < n; m++) {
+            if (m == j) continue;
+            real_t prod = 1.0 / (x[j] - x[m]);
+            for (int q = 0; q < n; q++)
+                if (q != j && q != m) prod *= (t - x[q]) / (x[j] - x[q]);
+            dv += prod;
+            v *= (t - x[m]) / (x[j] - x[m]);
+        }
+        L[j] = v;
+        dL[j] = dv;
+    }
+}
+
+// An element's map from [0,1]^dim: affine and axis-aligned (origin x0,
+// extents h), or nodal — the degree-N interpolant of its DG nodes' physical
+// coordinates X (X[k * dof + n], the LGL nodes x1d), whose Jacobian,
+// adjugate and determinant are evaluated at the integration point set last,
+// as MFEM's IsoparametricTransformation does for a curved mesh.
 class ElementTransformation {
 public:
     int ElementNo = 0;
     int dim = 2;
     real_t x0[3] = {0, 0, 0}, h[3] = {1, 1, 1};
+    bool nodal = false;
+    std::vector<real_t> X, x1d;
     DenseMatrix Jm, Adj;
     const IntegrationPoint *ip = nullptr;
     ElementTransformation() : Jm(3, 3), Adj(3, 3) {}
+    void SetupNodal(int d, int e, const std::vector<real_t> &nodes1d, const real_t *coords, int ndof)
+    {
+        dim = d;
+        ElementNo = e;
+        nodal = true;
+        x1d = nodes1d;
+        X.assign(coords, coords + (size_t)d * ndof);
+        Jm.SetSize(d, d);
+        Adj.SetSize(d, d);
+    }
+    void EvalNodal(const IntegrationPoint &p)
+    {
+        const int Np = (int)x1d.size();
+        std::vector<real_t> L[3], dL[3];
+        real_t r[3] = {p.x, p.y, p.z};
+        for (int q = 0; q < dim; q++) {
+            L[q].assign(Np, 0.0);
+            dL[q].assign(Np, 0.0);
+            StandInLagrange(x1d, r[q], L[q].data(), dL[q].data());
+        }
+        int dof = 1;
+        for (int q = 0; q < dim; q++) dof *= Np;
+        Jm = 0.0;
+        for (int n = 0; n < dof; n++) {
+            const int idx[3] = {n % Np, (n / Np) % Np, n / (Np * Np)};
+            for (int c = 0; c < dim; c++) {
+                real_t g = 1.0;
+                for (int q = 0; q < dim; q++) g *= q == c ? dL[q][idx[q]] : L[q][idx[q]];
+                for (int k = 0; k < dim; k++) Jm(k, c) += g * X[(size_t)k * dof + n];
+            }
+        }
+        if (dim == 2) {
+            Adj(0, 0) = Jm(1, 1);
+            Adj(0, 1) = -Jm(0, 1);
+            Adj(1, 0) = -Jm(1, 0);
+            Adj(1, 1) = Jm(0, 0);
+        } else {
+            for (int i = 0; i < 3; i++)
+                for (int j = 0; j < 3; j++) {
+                    const int i1 = (i + 1) % 3, i2 = (i + 2) % 3, j1 = (j + 1) % 3, j2 = (j + 2) % 3;
+                    Adj(i, j) = Jm(j1, i1) * Jm(j2, i2) - Jm(j1, i2) * Jm(j2, i1);
+                }
+        }
+    }
     void Setup(int d, int e, const real_t *origin, const real_t *hh)
     {
         dim = d;
@@ -644,7 +715,11 @@ public:
             Adj(2, 2) = Jm(0, 0) * Jm(1, 1);
         }
     }
-    void SetIntPoint(const IntegrationPoint *p) { ip = p; }
+    void SetIntPoint(const IntegrationPoint *p)
+    {
+        ip = p;
+        if (nodal) EvalNodal(*p);
+    }
     const IntegrationPoint &GetIntPoint() const { return *ip; }
     real_t Weight() { return Jm.Weight(); }
     const DenseMatrix &Jacobian() { return Jm; }
@@ -653,23 +728,85 @@ public:
     {
         phys.SetSize(dim);
         real_t r[3] = {p.x, p.y, p.z};
-        for (int i = 0; i < dim; i++) phys(i) = x0[i] + h[i] * r[i];
+        if (!nodal) {
+            for (int i = 0; i < dim; i++) phys(i) = x0[i] + h[i] * r[i];
+            return;
+        }
+        const int Np = (int)x1d.size();
+        std::vector<real_t> L[3], dL[3];
+        for (int q = 0; q < dim; q++) {
+            L[q].assign(Np, 0.0);
+            dL[q].assign(Np, 0.0);
+            StandInLagrange(x1d, r[q], L[q].data(), dL[q].data());
+        }
+        int dof = 1;
+        for (int q = 0; q < dim; q++) dof *= Np;
+        for (int i = 0; i < dim; i++) phys(i) = 0.0;
+        for (int n = 0; n < dof; n++) {
+            const int idx[3] = {n % Np, (n / Np) % Np, n / (Np * Np)};
+            real_t g = 1.0;
+            for (int q = 0; q < dim; q++) g *= L[q][idx[q]];
+            for (int i = 0; i < dim; i++) phys(i) += g * X[(size_t)i * dof + n];
+        }
     }
 };
 
 // Face between element 1 and element 2 of an axis-aligned Cartesian mesh.
 // Face point (s0[, s1]) sits at tangential coordinates (s0, s1) of both
 // elements; the face Jacobian is oriented so CalcOrtho points out of element 1.
+// General faces (nodal elements): element 1's face f1 = 2 d + side in its own
+// frame, element 2's face f2 and the orientation o of the neighbour's
+// tangential coordinates (swap if o & 1, then a -> 1 - a if o & 2, b -> 1 - b
+// if o & 4); the face Jacobian is element 1's tangent columns at the point,
+// ordered so that CalcOrtho points out of element 1, as MFEM orients it.
 class FaceElementTransformations {
 public:
     int Elem1No = 0, Elem2No = 0, ElementNo = 0;
     int dim = 2, dir = 0;
     int side1 = 1;  // 1: element 1's +dir face, 0: its -dir face
+    bool general = false;
+    int f2 = 0, orient = 0;
     ElementTransformation T1, T2;
     IntegrationPoint ip1, ip2;
     DenseMatrix FJ;
+    void SetAllIntPointsGeneral(const IntegrationPoint *fp)
+    {
+        const int d1 = dir, d2 = f2 / 2, s2 = f2 % 2;
+        real_t t[2] = {fp->x, dim == 3 ? fp->y : 0.0};
+        real_t p1[3] = {0, 0, 0}, p2[3] = {0, 0, 0};
+        int q = 0;
+        for (int d = 0; d < dim; d++) p1[d] = d == d1 ? (side1 ? 1.0 : 0.0) : t[q++];
+        real_t a = t[0], b = t[1];
+        if (orient & 1) std::swap(a, b);
+        if (orient & 2) a = 1.0 - a;
+        if (orient & 4) b = 1.0 - b;
+        real_t u[2] = {a, b};
+        q = 0;
+        for (int d = 0; d < dim; d++) p2[d] = d == d2 ? (s2 ? 1.0 : 0.0) : u[q++];
+        ip1.Set(p1, dim);
+        ip2.Set(p2, dim);
+        T1.SetIntPoint(&ip1);
+        if (Elem2No >= 0) T2.SetIntPoint(&ip2);
+        const DenseMatrix &J = T1.Jacobian();
+        if (dim == 2) {
+            FJ.SetSize(2, 1);
+            const int c = d1 == 0 ? 1 : 0;
+            const real_t sg = (d1 == 0) == (side1 == 1) ? 1.0 : -1.0;
+            FJ(0, 0) = sg * J(0, c);
+            FJ(1, 0) = sg * J(1, c);
+        } else {
+            FJ.SetSize(3, 2);
+            int c0 = (d1 + 1) % 3, c1 = (d1 + 2) % 3;
+            if (!side1) std::swap(c0, c1);
+            for (int k = 0; k < 3; k++) {
+                FJ(k, 0) = J(k, c0);
+                FJ(k, 1) = J(k, c1);
+            }
+        }
+    }
     void SetAllIntPoints(const IntegrationPoint *fp)
     {
+        if (general) return SetAllIntPointsGeneral(fp);
         real_t t[2] = {fp->x, fp->y};
         real_t p1[3], p2[3];
         int q = 0;

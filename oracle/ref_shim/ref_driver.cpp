@@ -153,8 +153,9 @@ struct RefCtx {
     std::unique_ptr<PerssonPeraireIndicator> indicator;
     double modalThreshold;
     double h[3];
-    struct Face { int e1, e2, dir, side1; };
+    struct Face { int e1, e2, dir, side1, f2 = 0, orient = 0; };
     std::vector<Face> faces;
+    bool general = false;  // nodal elements (ref_create_geo)
     // boundary faces (negative neighbour entries -1 - b) and the reference's
     // boundary integrator of each condition b
     struct BFace { int e, dir, side, b; };
@@ -183,6 +184,30 @@ void build_faces(RefCtx &c)
         }
 }
 
+// General meshes: every face once, from its element 1 (the lower-numbered
+// element), with the neighbour's face and orientation code.
+void build_faces_general(RefCtx &c, const int32_t *fo)
+{
+    const int nf = 2 * c.dim;
+    for (int e = 0; e < c.ne; e++)
+        for (int f = 0; f < nf; f++) {
+            const int nb = c.nbr[e * nf + f];
+            if (nb < 0) {
+                c.bfaces.push_back({e, f / 2, f % 2, -1 - nb});
+                continue;
+            }
+            if (!(e < nb || (e == nb && (f & 1)))) continue;
+            RefCtx::Face g;
+            g.e1 = e;
+            g.e2 = nb;
+            g.dir = f / 2;
+            g.side1 = f % 2;
+            g.f2 = fo ? (fo[e * nf + f] & 7) : (f ^ 1);
+            g.orient = fo ? (fo[e * nf + f] >> 3) : 0;
+            c.faces.push_back(g);
+        }
+}
+
 void setup_face(RefCtx &c, const RefCtx::Face &f, FaceElementTransformations &T)
 {
     T.Elem1No = f.e1;
@@ -192,6 +217,12 @@ void setup_face(RefCtx &c, const RefCtx::Face &f, FaceElementTransformations &T)
     T.side1 = f.side1;
     T.T1 = c.mesh->T[f.e1];
     T.T2 = c.mesh->T[f.e2];
+    if (c.general) {
+        T.general = true;
+        T.f2 = f.f2;
+        T.orient = f.orient;
+        return;
+    }
     const double *h = c.h;
     const bool out_plus = f.side1 == 1;  // outward normal of element 1 along +dir
     if (c.dim == 2) {
@@ -242,8 +273,28 @@ void blending(RefCtx &c, const Vector &u)
 
 extern "C" {
 
+static void *create_impl(int dim, int order, int ne, const double *h, const int32_t *nbr, const double *x,
+                         const int32_t *fo, double gamma, double Pr, double mu, double alpha_max, double alpha_min);
+
 void *ref_create(int dim, int order, int ne, const double *h, const int32_t *nbr, double gamma, double Pr,
                  double mu, double alpha_max, double alpha_min)
+{
+    return create_impl(dim, order, ne, h, nbr, nullptr, nullptr, gamma, Pr, mu, alpha_max, alpha_min);
+}
+
+// A mesh of nodal elements: x[k * num_nodes + e * ndof + n] the DG nodes'
+// coordinates, fo the face orientation codes (NULL: opposite faces, aligned).
+void *ref_create_geo(int dim, int order, int ne, const int32_t *nbr, const double *x, const int32_t *fo,
+                     double gamma, double Pr, double mu, double alpha_max, double alpha_min)
+{
+    const double h[3] = {1.0, 1.0, 1.0};
+    return create_impl(dim, order, ne, h, nbr, x, fo, gamma, Pr, mu, alpha_max, alpha_min);
+}
+
+}  // extern "C"
+
+static void *create_impl(int dim, int order, int ne, const double *h, const int32_t *nbr, const double *x,
+                         const int32_t *fo, double gamma, double Pr, double mu, double alpha_max, double alpha_min)
 {
     RefCtx *c = new RefCtx();
     c->dim = dim;
@@ -262,11 +313,23 @@ void *ref_create(int dim, int order, int ne, const double *h, const int32_t *nbr
     c->mesh->dim = dim;
     c->mesh->ne = ne;
     c->mesh->T.resize(ne);
-    for (int e = 0; e < ne; e++) {
-        double x0[3] = {0, 0, 0};
-        c->mesh->T[e].Setup(dim, e, x0, c->h);
-    }
     c->fec.reset(new DG_FECollection(order, dim, BasisType::GaussLobatto));
+    {
+        std::vector<double> x1d, w1d;
+        StandInGaussLobatto(order + 1, x1d, w1d);
+        const size_t nn = (size_t)ne * c->ndof;
+        std::vector<double> xe((size_t)dim * c->ndof);
+        for (int e = 0; e < ne; e++) {
+            if (!x) {
+                double x0[3] = {0, 0, 0};
+                c->mesh->T[e].Setup(dim, e, x0, c->h);
+                continue;
+            }
+            for (int k = 0; k < dim; k++)
+                for (int n = 0; n < c->ndof; n++) xe[(size_t)k * c->ndof + n] = x[k * nn + (size_t)e * c->ndof + n];
+            c->mesh->T[e].SetupNodal(dim, e, x1d, xe.data(), c->ndof);
+        }
+    }
     c->vfes = std::make_shared<ParFiniteElementSpace>();
     c->vfes->mesh = c->mesh.get();
     c->vfes->fe = c->fec->FiniteElementForGeometry(Geometry::SQUARE);
@@ -297,9 +360,13 @@ void *ref_create(int dim, int order, int ne, const double *h, const int32_t *nbr
     c->modal = std::make_shared<ModalBasis>(*c->fec, gtype, order, dim);
     c->indicator.reset(new PerssonPeraireIndicator(c->vfes, c->fes0, c->eta, c->modal, gamma));
     c->modalThreshold = 0.5 * std::pow(10.0, -1.8 * std::pow(order, 0.25));
-    build_faces(*c);
+    c->general = x != nullptr;
+    if (c->general) build_faces_general(*c, fo);
+    else build_faces(*c);
     return c;
 }
+
+extern "C" {
 
 void ref_destroy(void *h) { delete (RefCtx *)h; }
 

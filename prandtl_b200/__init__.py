@@ -44,6 +44,7 @@ KERNEL_LIFT_FACE_BDR, KERNEL_LIFT_BDR, KERNEL_NS_FACES_BDR, KERNEL_BOUNDARY_NS =
 KERNEL_LIFT_BDR_PTTT = 29
 KERNEL_NS_FACES_FB, KERNEL_EULER_FACES_FB, KERNEL_LIFT_FACE_FLUX, KERNEL_FACE_FLUX = 30, 31, 32, 33
 KERNEL_POSITIVITY = 34
+KERNEL_GEO = 35
 # params.filter bits
 FILTER_ENTROPY, FILTER_POSITIVITY = 1, 2
 # boundary condition types (pdg_set_boundary)
@@ -137,6 +138,7 @@ def library():
                                    C.c_void_p]
     L.pdg_rhs_noalloc.argtypes = [C.POINTER(PdgMesh), C.POINTER(PdgParams), C.c_void_p, C.c_void_p, C.c_void_p]
     L.pdg_set_boundary.argtypes = [C.c_void_p, C.c_int, C.c_int, _dp]
+    L.pdg_set_geometry.argtypes = [C.c_void_p, _dp, _ip]
     L.pdg_rk_stage_part.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_double, C.c_void_p, C.c_void_p, C.c_void_p,
                                     C.c_int64, C.c_int64, C.c_void_p]
     L.pdg_face_columns.argtypes = [C.c_void_p, C.POINTER(C.c_void_p), C.POINTER(C.c_int64)]
@@ -184,6 +186,19 @@ class DGSEMOperator:
         self._call(library().pdg_create(C.byref(self._m), C.byref(self.params), C.byref(self._ctx)), "pdg_create")
         for b, spec in (getattr(mesh, "boundaries", None) or {}).items():
             self.set_boundary(b, *spec)
+        if getattr(mesh, "coords", None) is not None:
+            self._set_geometry(mesh)
+
+    def _set_geometry(self, mesh):
+        """Node coordinates and face orientation codes of a general-geometry
+        mesh (pdg_set_geometry: skewed, graded, curved or unstructured elements)."""
+        self._coords = np.ascontiguousarray(mesh.coords, dtype=np.float64)
+        if self._coords.shape != (mesh.dim, mesh.num_nodes):
+            raise ValueError(f"mesh.coords has shape {self._coords.shape}, expected {(mesh.dim, mesh.num_nodes)}")
+        fo = getattr(mesh, "face_orient", None)
+        self._face_orient = None if fo is None else np.ascontiguousarray(fo, dtype=np.int32)
+        ptr = None if self._face_orient is None else self._face_orient.ctypes.data_as(_ip)
+        self._call(library().pdg_set_geometry(self._ctx, self._coords.ctypes.data_as(_dp), ptr), "pdg_set_geometry")
 
     def set_boundary(self, index: int, type: int, state=None):
         """Boundary condition ``index`` of the mesh's negative neighbour

@@ -97,6 +97,12 @@ struct pdg_ctx {
     int device = 0;
     std::string last_error;
     std::vector<int32_t> nbr_host;  // the neighbour table as given (the host step's pipeline reads it)
+    // general geometry (pdg_set_geometry): per node J and adjugate rows, per
+    // element face node the neighbour's matching node and element 1's normal
+    bool geo = false;
+    double *geo_d = nullptr;
+    int32_t *fnode_d = nullptr;
+    double *fnor_d = nullptr;
 };
 
 namespace {
@@ -332,6 +338,7 @@ bool kind_used(int kind, int dim, bool parabolic, int filter)
 {
     if (kind == KIND_FILTER_BOUNDS || kind == KIND_FILTER) return filter & 1;
     if (kind == KIND_POSITIVITY) return (filter & 2) != 0;
+    if (kind == KIND_GEO) return false;  // configured by pdg_set_geometry
     if ((kind >= KIND_ADJ_RHS && kind <= KIND_ADJ_FACE_NS2) || kind == KIND_ADJ_BOUNDARY)
         return false;  // configured by the first pdg_rhs_vjp
     const bool ns_kind = kind == KIND_NS || kind == KIND_NS_FACES || kind == KIND_LIFT || kind == KIND_LIFT_FACE ||
@@ -411,6 +418,9 @@ KParams base_params(pdg_ctx *c)
     P.has_bdr = c->bc_used != 0;
     P.lbuf_lo = c->lbuf_lo;
     P.fbuf = c->fbuf;
+    P.geo = c->geo_d;
+    P.fnode = c->fnode_d;
+    P.fnor = c->fnor_d;
     return P;
 }
 
@@ -519,6 +529,7 @@ int evaluate(pdg_ctx *c, int stage, double dt, const double *un, const double *u
     P.dt = dt;
     c->last_stream = s;
     int r;
+    if (c->geo) return launch(c, KIND_GEO, P, s);  // general geometry: one kernel
     const bool element_faces = c->element_faces && !c->p.compat;
     if (c->p.parabolic) {
         if ((c->p.filter & 1) && stage >= 0 && (r = launch(c, KIND_FILTER_BOUNDS, P, s))) return r;
@@ -748,6 +759,228 @@ int pdg_set_boundary(pdg_ctx *c, int index, int type, const double *state)
     return PDG_OK;
 }
 
+}  // extern "C"
+
+namespace {
+
+// Node index of position `pos` along direction d on line `line` (x fastest).
+inline int host_line_node(int dim, int Np, int d, int line, int pos)
+{
+    if (dim == 2) return d == 0 ? line * Np + pos : pos * Np + line;
+    if (d == 0) return line * Np + pos;
+    if (d == 1) return (line / Np) * Np * Np + pos * Np + (line % Np);
+    return pos * Np * Np + line;
+}
+
+// Smallest singular value of a dim x dim matrix A (row-major): the square
+// root of the smallest eigenvalue of A^T A, in closed form (2D) or by the
+// trigonometric solution of the symmetric 3 x 3 eigenproblem (Smith, 1961).
+double min_singular_value(int dim, const double *A)
+{
+    double B[9] = {};
+    for (int i = 0; i < dim; i++)
+        for (int j = 0; j < dim; j++)
+            for (int k = 0; k < dim; k++) B[i * 3 + j] += A[k * dim + i] * A[k * dim + j];
+    if (dim == 2) {
+        const double a = B[0], b = B[1], cc = B[4];
+        const double m = 0.5 * (a + cc), r = std::sqrt(0.25 * (a - cc) * (a - cc) + b * b);
+        return std::sqrt(std::max(m - r, 0.0));
+    }
+    const double p1 = B[1] * B[1] + B[2] * B[2] + B[5] * B[5];
+    if (p1 == 0.0) return std::sqrt(std::max(0.0, std::min(B[0], std::min(B[4], B[8]))));
+    const double q = (B[0] + B[4] + B[8]) / 3.0;
+    const double p2 = (B[0] - q) * (B[0] - q) + (B[4] - q) * (B[4] - q) + (B[8] - q) * (B[8] - q) + 2.0 * p1;
+    const double p = std::sqrt(p2 / 6.0);
+    double C[9];
+    for (int i = 0; i < 9; i++) C[i] = (B[i] - ((i % 4) == 0 ? q : 0.0)) / p;
+    const double det = C[0] * (C[4] * C[8] - C[5] * C[7]) - C[1] * (C[3] * C[8] - C[5] * C[6]) +
+                       C[2] * (C[3] * C[7] - C[4] * C[6]);
+    const double r = std::max(-1.0, std::min(1.0, 0.5 * det));
+    const double phi = std::acos(r) / 3.0;
+    const double lmin = q + 2.0 * p * std::cos(phi + 2.0 * 3.14159265358979323846 / 3.0);
+    return std::sqrt(std::max(lmin, 0.0));
+}
+
+}  // namespace
+
+extern "C" {
+
+int pdg_set_geometry(pdg_ctx *c, const double *x, const int32_t *face_orient)
+{
+    if (!c) return PDG_ERR_ARG;
+    if (!x) return fail(c, PDG_ERR_ARG, "pdg_set_geometry: null coordinates");
+    if (c->geo) return fail(c, PDG_ERR_ARG, "pdg_set_geometry: the geometry is already set");
+    if (c->p.parabolic || c->p.filter)
+        return fail(c, PDG_ERR_UNSUPPORTED, "pdg_set_geometry: general geometry takes Euler without filter");
+    const int dim = c->dim, Np = c->Np, N = c->N, nd = c->ndof, nf = 2 * dim;
+    const int nfn = dim == 2 ? Np : Np * Np;
+    const int64_t ne = c->ne, nn = c->nnodes;
+    const int nq = 1 + dim * dim;
+    const double *D = c->hK.D;  // D[i * Np + l] = l'_l(x_i)
+    std::vector<double> geo((size_t)nq * nn);
+    // Jacobian dx_k / dxi_r at every node from the node coordinates (the
+    // derivative of the element's degree-N interpolant of its geometry, what
+    // MFEM's element transformation evaluates at the LGL points), its
+    // adjugate (MFEM's AdjugateJacobian) and determinant (Weight)
+    for (int64_t e = 0; e < ne; e++)
+        for (int n = 0; n < nd; n++) {
+            const int pos[3] = {n % Np, (n / Np) % Np, n / (Np * Np)};
+            double Jm[9] = {};
+            for (int k = 0; k < dim; k++)
+                for (int r = 0; r < dim; r++) {
+                    const int line = r == 0 ? n / Np : r == 1 ? (dim == 2 ? pos[0] : pos[0] + Np * pos[2]) : pos[0] + Np * pos[1];
+                    double t = 0.0;
+                    for (int l = 0; l < Np; l++)
+                        t += D[pos[r] * Np + l] * x[(int64_t)k * nn + e * nd + host_line_node(dim, Np, r, line, l)];
+                    Jm[k * 3 + r] = t;
+                }
+            auto J_ = [&](int i, int j) { return Jm[i * 3 + j]; };
+            double adj[9] = {}, det;
+            if (dim == 2) {
+                adj[0] = J_(1, 1);
+                adj[1] = -J_(0, 1);
+                adj[3] = -J_(1, 0);
+                adj[4] = J_(0, 0);
+                det = J_(0, 0) * J_(1, 1) - J_(0, 1) * J_(1, 0);
+            } else {
+                // row r of the adjugate: the cross product of Jacobian columns r+1 and r+2
+                for (int r = 0; r < 3; r++) {
+                    const int a = (r + 1) % 3, b = (r + 2) % 3;
+                    adj[r * 3 + 0] = J_(1, a) * J_(2, b) - J_(2, a) * J_(1, b);
+                    adj[r * 3 + 1] = J_(2, a) * J_(0, b) - J_(0, a) * J_(2, b);
+                    adj[r * 3 + 2] = J_(0, a) * J_(1, b) - J_(1, a) * J_(0, b);
+                }
+                det = J_(0, 0) * (J_(1, 1) * J_(2, 2) - J_(1, 2) * J_(2, 1)) -
+                      J_(0, 1) * (J_(1, 0) * J_(2, 2) - J_(1, 2) * J_(2, 0)) +
+                      J_(0, 2) * (J_(1, 0) * J_(2, 1) - J_(1, 1) * J_(2, 0));
+            }
+            if (!(det > 0.0))
+                return fail(c, PDG_ERR_ARG, "pdg_set_geometry: element %lld node %d has Jacobian %g (not positive)",
+                            (long long)e, n, det);
+            const int64_t g = e * nd + n;
+            geo[g] = det;
+            for (int r = 0; r < dim; r++)
+                for (int k = 0; k < dim; k++) geo[(size_t)(1 + r * dim + k) * nn + g] = adj[r * 3 + k];
+        }
+    auto row = [&](int64_t e, int n, int r, int k) { return geo[(size_t)(1 + r * dim + k) * nn + e * nd + n]; };
+    // faces: the neighbour's matching node and the normal out of the face's
+    // element 1 (the lower-numbered element; its +d or -d adjugate row)
+    std::vector<int32_t> fnode((size_t)ne * nf * nfn, 0);
+    std::vector<double> fnor((size_t)ne * nf * nfn * dim, 0.0);
+    for (int64_t e = 0; e < ne; e++)
+        for (int f = 0; f < nf; f++) {
+            const int d = f / 2, side = f % 2;
+            const int64_t nb = c->nbr_host[e * nf + f];
+            int f2 = f ^ 1, o = 0;
+            if (nb >= 0 && face_orient) {
+                const int32_t code = face_orient[e * nf + f];
+                f2 = code & 7;
+                o = code >> 3;
+                if (f2 >= nf || o > 7 || (dim == 2 && (o & 5)))
+                    return fail(c, PDG_ERR_ARG, "pdg_set_geometry: element %lld face %d: bad orientation code %d",
+                                (long long)e, f, code);
+            }
+            if (nb >= 0 && c->nbr_host[nb * nf + f2] != e)
+                return fail(c, PDG_ERR_ARG, "pdg_set_geometry: element %lld face %d: the neighbour's face %d does not point back",
+                            (long long)e, f, f2);
+            for (int t = 0; t < nfn; t++) {
+                const int n = host_line_node(dim, Np, d, t, side ? N : 0);
+                const size_t fi = ((size_t)e * nf + f) * nfn + t;
+                double own[3];
+                for (int k = 0; k < dim; k++) own[k] = (side ? 1.0 : -1.0) * row(e, n, d, k);
+                if (nb < 0) {
+                    for (int k = 0; k < dim; k++) fnor[fi * dim + k] = own[k];
+                    continue;
+                }
+                int a = t % Np, b = dim == 3 ? t / Np : 0;
+                if (o & 1) std::swap(a, b);
+                if (o & 2) a = N - a;
+                if (o & 4) b = N - b;
+                const int t2 = a + Np * b, d2 = f2 / 2, side2 = f2 % 2;
+                const int n2 = host_line_node(dim, Np, d2, t2, side2 ? N : 0);
+                fnode[fi] = n2;
+                // matching nodes sit at the same point, up to one periodic
+                // shift per face
+                {
+                    const int nlast = host_line_node(dim, Np, d, nfn - 1, side ? N : 0);
+                    const int nfirst = host_line_node(dim, Np, d, 0, side ? N : 0);
+                    double ext = 0.0, dev = 0.0;
+                    for (int k = 0; k < dim; k++) {
+                        const double *xk = x + (int64_t)k * nn;
+                        const double shift0 = xk[e * nd + nfirst] - xk[nb * nd + fnode[((size_t)e * nf + f) * nfn]];
+                        const double dk = (xk[e * nd + n] - xk[nb * nd + n2]) - shift0;
+                        const double ek = xk[e * nd + nlast] - xk[e * nd + nfirst];
+                        dev += dk * dk;
+                        ext += ek * ek;
+                    }
+                    if (!(dev <= 1e-18 * ext))
+                        return fail(c, PDG_ERR_ARG,
+                                    "pdg_set_geometry: element %lld face %d node %d does not meet the neighbour's "
+                                    "matching node (a non-conforming face or a wrong orientation code)",
+                                    (long long)e, f, t);
+                }
+                double other[3], sq = 0.0, dsq = 0.0;
+                for (int k = 0; k < dim; k++) {
+                    other[k] = (side2 ? 1.0 : -1.0) * row(nb, n2, d2, k);
+                    sq += own[k] * own[k];
+                    dsq += (own[k] + other[k]) * (own[k] + other[k]);
+                }
+                if (!(dsq <= 1e-12 * sq))
+                    return fail(c, PDG_ERR_ARG,
+                                "pdg_set_geometry: element %lld face %d node %d: the neighbour's normal does not match "
+                                "(a non-conforming face or a wrong orientation code)",
+                                (long long)e, f, t);
+                const bool is1 = e < nb || (e == nb && side == 1);
+                // element 1's outward normal: this element's, or the neighbour's
+                for (int k = 0; k < dim; k++) fnor[fi * dim + k] = is1 ? own[k] : other[k];
+            }
+        }
+    // CFL length: the smallest singular value of the Jacobian at an element
+    // centre (MFEM's GetElementSize(e, 1), as Simulation.cpp:896-906 uses)
+    std::vector<double> xg(Np), wg(Np), Lc(Np), dLc(Np);
+    gauss_lobatto(Np, xg.data(), wg.data());
+    for (int j = 0; j < Np; j++) {
+        double v = 1.0, dv = 0.0;
+        for (int m = 0; m < Np; m++) {
+            if (m == j) continue;
+            double prod = 1.0 / (xg[j] - xg[m]);
+            for (int q = 0; q < Np; q++)
+                if (q != j && q != m) prod *= (0.5 - xg[q]) / (xg[j] - xg[q]);
+            dv += prod;
+            v *= (0.5 - xg[m]) / (xg[j] - xg[m]);
+        }
+        Lc[j] = v;
+        dLc[j] = dv;
+    }
+    double hmin = 1e300;
+    for (int64_t e = 0; e < ne; e++) {
+        double Jc[9] = {};
+        for (int n = 0; n < nd; n++) {
+            const int pos[3] = {n % Np, (n / Np) % Np, n / (Np * Np)};
+            for (int r = 0; r < dim; r++) {
+                double wgt = 1.0;
+                for (int q = 0; q < dim; q++) wgt *= q == r ? dLc[pos[q]] : Lc[pos[q]];
+                for (int k = 0; k < dim; k++) Jc[k * dim + r] += wgt * x[(int64_t)k * nn + e * nd + n];
+            }
+        }
+        hmin = std::min(hmin, min_singular_value(dim, Jc));
+    }
+    if (cudaMalloc(&c->geo_d, sizeof(double) * geo.size()) != cudaSuccess ||
+        cudaMalloc(&c->fnode_d, sizeof(int32_t) * fnode.size()) != cudaSuccess ||
+        cudaMalloc(&c->fnor_d, sizeof(double) * fnor.size()) != cudaSuccess)
+        return fail(c, PDG_ERR_NOMEM, "pdg_set_geometry: allocation failed");
+    CK(cudaMemcpy(c->geo_d, geo.data(), sizeof(double) * geo.size(), cudaMemcpyHostToDevice), "geometry upload");
+    CK(cudaMemcpy(c->fnode_d, fnode.data(), sizeof(int32_t) * fnode.size(), cudaMemcpyHostToDevice), "geometry upload");
+    CK(cudaMemcpy(c->fnor_d, fnor.data(), sizeof(double) * fnor.size(), cudaMemcpyHostToDevice), "geometry upload");
+    int r = configure_launch(c, KIND_GEO);
+    if (r) return r;
+    cudaFree(c->fbuf);  // the box path's face buffer is not used
+    c->fbuf = nullptr;
+    c->hmin = hmin;
+    c->geo = true;
+    return PDG_OK;
+}
+
 int pdg_destroy(pdg_ctx *c)
 {
     if (!c) return PDG_OK;
@@ -770,6 +1003,9 @@ int pdg_destroy(pdg_ctx *c)
     cudaFree(c->ent_own);
     cudaFree(c->gcol);
     cudaFree(c->gbuf);
+    cudaFree(c->geo_d);
+    cudaFree(c->fnode_d);
+    cudaFree(c->fnor_d);
     if (c->graph_exec) cudaGraphExecDestroy(c->graph_exec);
     if (c->graph) cudaGraphDestroy(c->graph);
     if (c->cap) cudaStreamDestroy(c->cap);
@@ -906,7 +1142,7 @@ int pipe_setup(pdg_ctx *c)
     auto &q = c->pipe;
     if (q.ready) return PDG_OK;
     q.ready = true;
-    q.usable = c->fbuf && !c->p.filter && c->ne >= PIPE_CHUNKS * PIPE_MIN_CHUNK;
+    q.usable = c->fbuf && !c->geo && !c->p.filter && c->ne >= PIPE_CHUNKS * PIPE_MIN_CHUNK;
     if (const char *hp = std::getenv("PDG_HOST_PIPELINE")) q.usable = q.usable && std::atoi(hp) != 0;
     if (!q.usable) return PDG_OK;
     const int C = PIPE_CHUNKS, nf = 2 * c->dim;
@@ -1059,8 +1295,8 @@ int pdg_rk_stage_part(pdg_ctx *c, int part, int stage, double dt, const double *
                       int64_t e_begin, int64_t e_end, void *stream)
 {
     if (!c) return PDG_ERR_ARG;
-    if (!c->fbuf || c->p.filter)
-        return fail(c, PDG_ERR_UNSUPPORTED, "pdg_rk_stage_part: needs the fixed operator on a periodic mesh, no filter");
+    if (!c->fbuf || c->geo || c->p.filter)
+        return fail(c, PDG_ERR_UNSUPPORTED, "pdg_rk_stage_part: needs the fixed operator on a periodic box mesh, no filter");
     if (part < PDG_PART_START || part > PDG_PART_VOLUME) return fail(c, PDG_ERR_ARG, "pdg_rk_stage_part: bad part");
     if (stage < -1 || stage > 2) return fail(c, PDG_ERR_ARG, "pdg_rk_stage_part: stage must be -1, 0, 1 or 2");
     if (e_begin < 0 || e_end > c->ne || e_begin > e_end) return fail(c, PDG_ERR_ARG, "pdg_rk_stage_part: bad range");
@@ -1242,6 +1478,7 @@ int vjp(pdg_ctx *c, int stage, double dt, const double *u, const double *cot, do
 
 int vjp_check(pdg_ctx *c, const char *what)
 {
+    if (c->geo) return fail(c, PDG_ERR_UNSUPPORTED, "%s: the adjoint takes box meshes only", what);
     if (c->p.compat) return fail(c, PDG_ERR_UNSUPPORTED, "%s: the adjoint is of the fixed operator (compat = 0)", what);
     if (c->p.parabolic && c->bc_used)
         return fail(c, PDG_ERR_UNSUPPORTED, "%s: Navier-Stokes boundary faces are not differentiated", what);

@@ -1,0 +1,514 @@
+// geo_kernels.cuh — the Euler right-hand side on meshes of general geometry
+// (skewed, graded, curved or unstructured quadrilaterals and hexahedra).
+//
+// The reference evaluates every metric term from MFEM's element
+// transformation at the integration points: the two-point volume fluxes use
+// the mean of both nodes' contravariant metric rows (adj rows of the
+// Jacobian, DGSEMIntegrator.cpp:252-266, ChandrashekarFlux.cpp:11-83), the
+// volume term is divided by the node's own J (:427-431), the faces use the
+// normal CalcOrtho gives out of the face's element 1 and each side's own
+// J (:151-222), and the subcell finite-volume fluxes use the subcell normals
+// n_i = adj(x_0) + sum_{l<i} w_l (D adj)_l along each line
+// (ComputeSubcellMetrics, :1199-1304; ComputeFVFluxes, :972-1196) and
+// divide by J w at the node.  Here the metric terms sit in HBM per node
+// (P.geo: J and the adjugate rows), the face normals and the neighbour's
+// matching node per element face node (P.fnor, P.fnode: conforming faces in
+// any orientation), and the subcell normals are formed per line in the
+// kernel from the metric rows, in the reference's order of operations.
+//
+// Work decomposition: as rhs_kernel — a lane group per element, line tasks
+// per direction (each two-point flux evaluated once per line pair and added
+// to both nodes), then each element evaluates its own face nodes with the
+// element-1 rule (both elements of a face evaluate it from the same inputs
+// in the same order and receive bit-identical fluxes) and stores the
+// finished stage.  One launch per right-hand side or RK stage.
+#pragma once
+
+#include "line_kernels.cuh"
+
+namespace pdg {
+
+// Metric row r of node n of element e (dim components).
+template <int DIM>
+__device__ __forceinline__ void geo_row(const KParams &P, int64_t gnode, int r, double *m)
+{
+#pragma unroll
+    for (int k = 0; k < DIM; k++) m[k] = __ldg(P.geo + (int64_t)(1 + r * DIM + k) * P.nnodes + gnode);
+}
+__device__ __forceinline__ double geo_J(const KParams &P, int64_t gnode) { return __ldg(P.geo + gnode); }
+
+// Flux-differencing line tasks along direction d with per-node metrics: the
+// pair (a < b) of a line takes the metric mean (m_a + m_b) / 2 of both nodes'
+// row d, its flux contributes Dhat2(a,b) F to node a and Dhat2(b,a) F to
+// node b, in ascending partner order.  The unscaled line sums are stored
+// (d == 0) or added to acc.
+template <int DIM, int N>
+__device__ __forceinline__ void ec_lines_geo(const KParams &P, int d, const double *pr, double *acc,
+                                             const double *c, int gl, int64_t e, bool valid)
+{
+    using S = Shape<DIM, N>;
+    constexpr int Np = S::Np, NV = S::NV, NDOF = S::NDOF;
+    const double *D2 = C_DHAT2(c);
+#pragma unroll 1
+    for (int r = 0; r < S::LPL; r++) {
+        const int line = gl + r * S::L;
+        if (line < S::NFN) {
+            Prim<DIM> q[Np];
+            double m[Np][DIM];
+#pragma unroll
+            for (int l = 0; l < Np; l++) {
+                const int n = line_node_rt<DIM, Np>(d, line, l);
+                q[l] = slot_prim<DIM>(pr, sp<DIM, Np>(n), S::NS_);
+                if (valid) geo_row<DIM>(P, e * NDOF + n, d, m[l]);
+                else
+#pragma unroll
+                    for (int k = 0; k < DIM; k++) m[l][k] = k == d ? 1.0 : 0.0;
+            }
+            double la[Np][NV];
+#pragma unroll
+            for (int l = 0; l < Np; l++)
+#pragma unroll
+                for (int v = 0; v < NV; v++) la[l][v] = 0.0;
+#pragma unroll
+            for (int a = 0; a < Np; a++)
+#pragma unroll
+                for (int b = a + 1; b < Np; b++) {
+                    double mt[DIM], F[NV];
+#pragma unroll
+                    for (int k = 0; k < DIM; k++) mt[k] = (m[a][k] + m[b][k]) * 0.5;
+                    volume_flux_n<DIM>(q[a], q[b], mt, P.gm1inv, F);
+                    const double cab = D2[a * Np + b], cba = D2[b * Np + a];
+#pragma unroll
+                    for (int v = 0; v < NV; v++) {
+                        la[a][v] += cab * F[v];
+                        la[b][v] += cba * F[v];
+                    }
+                }
+#pragma unroll
+            for (int l = 0; l < Np; l++) {
+                const int n = sp<DIM, Np>(line_node_rt<DIM, Np>(d, line, l));
+#pragma unroll
+                for (int v = 0; v < NV; v++) {
+                    if (d == 0) acc[v * S::NS_ + n] = la[l][v];
+                    else acc[v * S::NS_ + n] += la[l][v];
+                }
+            }
+        }
+    }
+    __syncwarp();
+}
+
+// Subcell finite-volume line tasks along d: the interface normals of the
+// line from its metric rows (n_0 = m_0, n_{i+1} = n_i + w_i sum_m D(i,m) m_m),
+// the Chandrashekar face flux across each interior interface, and node l
+// receiving alpha (f_{l-1/2} - f_{l+1/2}) / (J_l w_l).
+template <int DIM, int N>
+__device__ __forceinline__ void fv_lines_geo(const KParams &P, int d, const double *pr, double *acc,
+                                             const double *c, int gl, int64_t e, bool valid, double alpha)
+{
+    using S = Shape<DIM, N>;
+    constexpr int Np = S::Np, NV = S::NV, NDOF = S::NDOF;
+    const double *Dm = C_D(c), *w = C_W(c);
+#pragma unroll 1
+    for (int r = 0; r < S::LPL; r++) {
+        const int line = gl + r * S::L;
+        if (line < S::NFN) {
+            double m[Np][DIM], sc[Np];
+#pragma unroll
+            for (int l = 0; l < Np; l++) {
+                const int n = line_node_rt<DIM, Np>(d, line, l);
+                if (valid) {
+                    geo_row<DIM>(P, e * NDOF + n, d, m[l]);
+                    sc[l] = 1.0 / (geo_J(P, e * NDOF + n) * w[l]);
+                } else {
+#pragma unroll
+                    for (int k = 0; k < DIM; k++) m[l][k] = k == d ? 1.0 : 0.0;
+                    sc[l] = 1.0;
+                }
+            }
+            double nor[DIM], prev[NV];
+#pragma unroll
+            for (int k = 0; k < DIM; k++) nor[k] = m[0][k];
+#pragma unroll
+            for (int v = 0; v < NV; v++) prev[v] = 0.0;
+            Prim<DIM> qa = slot_prim<DIM>(pr, sp<DIM, Np>(line_node_rt<DIM, Np>(d, line, 0)), S::NS_);
+            complete_prim<DIM>(qa, P.gamma);
+#pragma unroll
+            for (int l = 0; l < Np; l++) {
+                const int n = sp<DIM, Np>(line_node_rt<DIM, Np>(d, line, l));
+                double F[NV];
+                Prim<DIM> qb;
+                if (l < N) {
+                    // interface l + 1/2: n_{l+1} = n_l + w_l (D m)_l
+#pragma unroll
+                    for (int k = 0; k < DIM; k++) {
+                        double t = 0.0;
+#pragma unroll
+                        for (int j = 0; j < Np; j++) t += m[j][k] * Dm[l * Np + j];
+                        nor[k] += t * w[l];
+                    }
+                    qb = slot_prim<DIM>(pr, sp<DIM, Np>(line_node_rt<DIM, Np>(d, line, l + 1)), S::NS_);
+                    complete_prim<DIM>(qb, P.gamma);
+                    double ma[DIM], mb[DIM];
+#pragma unroll
+                    for (int k = 0; k < DIM; k++) {
+                        ma[k] = qa.rho * qa.v[k];
+                        mb[k] = qb.rho * qb.v[k];
+                    }
+                    face_flux_n<DIM>(qa, qb, ma, mb, nor, P.gm1inv, P.compat != 0, P.diss_scale, F);
+                } else {
+#pragma unroll
+                    for (int v = 0; v < NV; v++) F[v] = 0.0;
+                }
+#pragma unroll
+                for (int v = 0; v < NV; v++) {
+                    acc[v * S::NS_ + n] += alpha * ((prev[v] - F[v]) * sc[l]);
+                    prev[v] = F[v];
+                }
+                if (l < N) qa = qb;
+            }
+        }
+    }
+    __syncwarp();
+}
+
+// The normal and tangents of a boundary face (RotateState,
+// src/BasicOperations/BasicOperations.cpp:238-258): the momentum of `s`
+// expressed in the frame (n, t1[, t2]) of the unit normal n.
+template <int DIM> __device__ __forceinline__ void rotate_momentum(double *s, const double *n)
+{
+    double t1[3] = {0, 0, 0}, t2[3] = {0, 0, 0};
+    if (DIM == 2) {
+        t1[0] = -n[1];
+        t1[1] = n[0];
+    } else {
+        const bool gen = fabs(n[0]) > 1e-10;
+        const double q = gen ? n[1] / n[0] : 0.0;
+        t1[0] = gen ? -q / sqrt(1.0 + q * q) : -1.0;
+        t1[1] = gen ? 1.0 / sqrt(1.0 + q * q) : 0.0;
+        t1[2] = 0.0;
+        t2[0] = n[1] * t1[2] - n[2] * t1[1];
+        t2[1] = n[2] * t1[0] - n[0] * t1[2];
+        t2[2] = n[0] * t1[1] - n[1] * t1[0];
+    }
+    double ru = 0.0, rv = 0.0, rw = 0.0;
+#pragma unroll
+    for (int d = 0; d < DIM; d++) {
+        ru += s[1 + d] * n[d];
+        rv += s[1 + d] * t1[d];
+    }
+    if (DIM == 3) {
+#pragma unroll
+        for (int d = 0; d < 3; d++) rw += s[1 + d] * t2[d];
+        s[3] = rw;
+    }
+    s[1] = ru;
+    s[2] = rv;
+}
+
+// Boundary face node with interior state s1 and outward normal nor (not
+// normalised; |nor| is the face's area element): the normal flux F of
+// condition b and the wave speed it reports (BdrFaceIntegrator::
+// AssembleFaceVector and each condition's ComputeBdrFaceInviscidFlux /
+// ComputeOuterInviscidState, src/Integrators/BoundaryConditions/).  Slip
+// wall (and, without viscosity, both no-slip walls): the state rotated to the
+// face frame, p* from the wall Riemann problem (SlipWallBdrFaceIntegrator.cpp:
+// 15-58), flux p* nor in the momentum rows.  Other conditions: the outer
+// state and the Chandrashekar face flux; the subsonic and Riemann-invariant
+// conditions of the reference-value operator divide the interior momenta in
+// place first, as the reference's Vector views do (ComputePressure,
+// BasicOperations.cpp:31-37).
+template <int DIM>
+__device__ __noinline__ double geo_bdr_flux(const KParams &P, int b, const double *s_in, const double *nor, double *F)
+{
+    constexpr int NV = DIM + 2;
+    const double *bc = P.bc + b * BC_SLOT;
+    const int type = (int)bc[0];
+    const double gamma = P.gamma, gm1 = P.gm1, gm1inv = P.gm1inv;
+    const bool compat = P.compat != 0;
+    double nn = 0.0, un[DIM];
+#pragma unroll
+    for (int d = 0; d < DIM; d++) nn += nor[d] * nor[d];
+    const double inv = 1.0 / sqrt(nn);
+#pragma unroll
+    for (int d = 0; d < DIM; d++) un[d] = nor[d] * inv;
+    double s1[NV], s2[NV];
+#pragma unroll
+    for (int v = 0; v < NV; v++) s1[v] = s2[v] = s_in[v];
+    if (type == BC_SLIP_WALL || type == BC_NOSLIP_ADIABATIC || type == BC_NOSLIP_ISOTHERMAL) {
+        rotate_momentum<DIM>(s2, un);
+        const double rho = s2[0];
+        double vv = 0.0;
+#pragma unroll
+        for (int d = 0; d < DIM; d++) {
+            const double V = s2[1 + d] / rho;
+            vv += V * V;
+        }
+        const double p = gm1 * (s2[NV - 1] - 0.5 * rho * vv);
+        const double an = sqrt(gamma * p / rho);
+        const double u = s2[1] / rho;
+        const double gp1 = 1.0 + gamma, gp1inv = 1.0 / gp1;
+        double ps;
+        if (u > 0.0) ps = p + 0.25 * u * gp1 * rho * (u + sqrt(u * u + 8.0 * gp1inv / rho * p * (gm1 * gp1inv + 1.0)));
+        else ps = p * pow(fmax(1.0 + 0.5 * gm1 * u / an, 0.0001), 2.0 * gamma * gm1inv);
+        F[0] = 0.0;
+#pragma unroll
+        for (int d = 0; d < DIM; d++) F[1 + d] = ps * nor[d];
+        F[NV - 1] = 0.0;
+        return sqrt(vv) + an;
+    }
+    const double *prm = bc + 1;
+    if (type == BC_SUPERSONIC_INFLOW || type == BC_SPECIFIED_STATE) {
+#pragma unroll
+        for (int v = 0; v < NV; v++) s2[v] = prm[v];
+    } else if (type == BC_SYMMETRY) {
+        double mn = 0.0;
+#pragma unroll
+        for (int d = 0; d < DIM; d++) mn += s2[1 + d] * un[d];
+#pragma unroll
+        for (int d = 0; d < DIM; d++) s2[1 + d] += -2.0 * mn * un[d];
+    } else if (type == BC_SUBSONIC_OUTFLOW_P || type == BC_SUBSONIC_INFLOW_PTTT) {
+        const double rho = s_in[0], r1 = 1.0 / rho;
+        double V[DIM], vv = 0.0;
+#pragma unroll
+        for (int d = 0; d < DIM; d++) V[d] = compat ? s_in[1 + d] * r1 : s_in[1 + d] / rho;
+#pragma unroll
+        for (int d = 0; d < DIM; d++) vv += V[d] * V[d];
+        if (compat)
+#pragma unroll
+            for (int d = 0; d < DIM; d++) s1[1 + d] = V[d];
+        if (type == BC_SUBSONIC_OUTFLOW_P) {
+#pragma unroll
+            for (int v = 0; v < NV; v++) s2[v] = s1[v];
+            s2[NV - 1] = prm[0] * gm1inv + 0.5 * rho * vv;
+        } else {
+            const double cp = prm[0], p0 = prm[1], T0 = prm[2];
+            const double p = gm1 * (s_in[NV - 1] - 0.5 * rho * vv);
+            double V_sq = 2.0 * cp * T0 * (1.0 - pow(p / p0, gm1 / gamma));
+            V_sq = fmax(0.0, V_sq);
+            s2[0] = gamma * gm1inv * p / (cp * T0 - 0.5 * V_sq);
+#pragma unroll
+            for (int d = 0; d < DIM; d++) s2[1 + d] = s2[0] * sqrt(V_sq) * prm[3 + d];
+            s2[NV - 1] = p * gm1inv + 0.5 * s2[0] * V_sq;
+        }
+    } else if (type == BC_SUBSONIC_INFLOW_RV) {
+        const double r = prm[0];
+        s2[0] = r;
+        double dke = -s_in[1] * s_in[1], uu = 0.0;
+#pragma unroll
+        for (int d = 0; d < DIM; d++) {
+            s2[1 + d] = r * prm[1 + d];
+            if (d > 0) dke -= s_in[1 + d] * s_in[1 + d];
+            uu += prm[1 + d] * prm[1 + d];
+        }
+        dke *= 0.5 / s_in[0];
+        dke += 0.5 * uu * r;
+        s2[NV - 1] = s_in[NV - 1] + dke;
+    } else if (type == BC_RIEMANN_INVARIANT) {
+        const double ginv = 1.0 / gamma;
+        const double rho = s_in[0], r1 = 1.0 / rho;
+        const double rho_o = prm[0], p_o = prm[NV - 1];
+        double V[DIM], Vn_i = 0.0, Vn_o = 0.0;
+#pragma unroll
+        for (int d = 0; d < DIM; d++) V[d] = compat ? s_in[1 + d] * r1 : s_in[1 + d] / rho;
+#pragma unroll
+        for (int d = 0; d < DIM; d++) {
+            Vn_i += V[d] * un[d];
+            Vn_o += prm[1 + d] * un[d];
+        }
+        double W[DIM], ww = 0.0;
+#pragma unroll
+        for (int d = 0; d < DIM; d++) W[d] = compat ? V[d] * r1 : V[d];
+#pragma unroll
+        for (int d = 0; d < DIM; d++) ww += W[d] * W[d];
+        const double p_i = gm1 * (s_in[NV - 1] - 0.5 * rho * ww);
+        if (compat)
+#pragma unroll
+            for (int d = 0; d < DIM; d++) V[d] = s1[1 + d] = W[d];
+        const double a_o = sqrt(gamma * p_o / rho_o), a_i = sqrt(gamma * p_i / rho);
+        const double R_minus = (fabs(Vn_o) >= a_o && Vn_i >= 0.0) ? Vn_i - 2.0 * a_i * gm1inv : Vn_o - 2.0 * a_o * gm1inv;
+        const double R_plus = (fabs(Vn_o) >= a_o && Vn_i < 0.0) ? Vn_o + 2.0 * a_o * gm1inv : Vn_i + 2.0 * a_i * gm1inv;
+        const double Vn_b = 0.5 * (R_plus + R_minus), a_b = 0.25 * gm1 * (R_plus - R_minus);
+        const double dVn_i = Vn_b - Vn_i, dVn_o = Vn_b - Vn_o;
+        s2[0] = (Vn_i < 0.0) ? pow(a_b * a_b * ginv * rho_o / p_o, gm1inv) * rho_o
+                             : pow(a_b * a_b * ginv * rho / p_i, gm1inv) * rho;
+        double e2 = 0.0;
+#pragma unroll
+        for (int d = 0; d < DIM; d++) {
+            s2[1 + d] = (Vn_i >= 0.0) ? s2[0] * (V[d] + dVn_i * un[d]) : s2[0] * (prm[1 + d] + dVn_o * un[d]);
+            e2 = d == 0 ? s2[1] * s2[1] : e2 + s2[1 + d] * s2[1 + d];
+        }
+        const double p_b = a_b * a_b * s2[0] * ginv;
+        e2 *= (0.5 / s2[0]);
+        e2 += p_b * gm1inv;
+        s2[NV - 1] = e2;
+    }  // BC_SUPERSONIC_OUTFLOW: the interior state
+    const Prim<DIM> qa = make_prim<DIM>(s1, gamma, gm1), qb = make_prim<DIM>(s2, gamma, gm1);
+    double ma[DIM], mb[DIM];
+#pragma unroll
+    for (int d = 0; d < DIM; d++) {
+        ma[d] = s1[1 + d];
+        mb[d] = s2[1 + d];
+    }
+    face_flux_n<DIM>(qa, qb, ma, mb, nor, gm1inv, compat, P.diss_scale, F);
+    return fmax(qa.lam, qb.lam);
+}
+
+// One warp tile of geo_rhs_kernel: EPW elements from e_base, one lane group
+// each.  Volume terms into acc (flux differencing scaled by -(1 - alpha) / J
+// per node, then the subcell FV terms), the stage combine, the face terms of
+// every face node of the element (times the stage factor), the store.
+template <int DIM, int N>
+__device__ __forceinline__ void geo_tile(const KParams &P, const double *c, double *pr, int64_t e_base, int grp, int gl,
+                                         bool lane_used, unsigned int &flags, double &lam)
+{
+    using S = Shape<DIM, N>;
+    constexpr int Np = S::Np, NDOF = S::NDOF, NV = S::NV, NFN = S::NFN, L = S::L;
+    constexpr int ST = S::NS_;
+    double *acc = pr + S::NPRIM * ST, *scratch = acc;
+    const int64_t e0 = e_base + grp;
+    const bool valid = lane_used && e0 < range_end(P);
+    const int64_t e = valid ? e0 : 0;
+    const int64_t nn = P.nnodes;
+    if (lane_used) {
+        const double ls = stage_nodes<DIM, N>(P, e, valid, gl, pr, scratch, flags);
+        if (valid) lam = fmax(lam, ls);
+    }
+    __syncwarp();
+    double alpha = 0.0;
+    if (P.blending) {
+        const double eta = indicator_eta<DIM, N>(scratch, gl, C_VINV(c));
+        alpha = blending_alpha(eta, P);
+        if (valid && gl == 0) {
+            P.eta_out[e] = eta;
+            P.alpha_out[e] = alpha;
+        }
+    }
+    if (lane_used) {
+#pragma unroll 1
+        for (int d = 0; d < DIM; d++) ec_lines_geo<DIM, N>(P, d, pr, acc, c, gl, e, valid);
+    }
+    // -(1 - alpha) dU / J at every node (DGSEMIntegrator.cpp:423-431)
+    if (lane_used) {
+#pragma unroll
+        for (int k = 0; k < S::NPL; k++) {
+            const int n = gl + k * L;
+            if (n < NDOF) {
+                const double J = valid ? geo_J(P, e * NDOF + n) : 1.0;
+#pragma unroll
+                for (int v = 0; v < NV; v++) {
+                    double t = -acc[v * ST + sp<DIM, Np>(n)];
+                    t *= (1.0 - alpha);
+                    acc[v * ST + sp<DIM, Np>(n)] = t / J;
+                }
+            }
+        }
+    }
+    __syncwarp();
+    if (P.blending && __any_sync(0xffffffffu, alpha > 0.0)) {
+        if (lane_used) {
+#pragma unroll 1
+            for (int d = 0; d < DIM; d++) fv_lines_geo<DIM, N>(P, d, pr, acc, c, gl, e, valid, alpha);
+        }
+    }
+    const double coef = stage_coef(P);
+    if (valid) {
+#pragma unroll
+        for (int k = 0; k < S::NPL; k++) {
+            const int n = gl + k * L;
+            if (n < NDOF) {
+#pragma unroll
+                for (int v = 0; v < NV; v++) {
+                    const int64_t gi = (int64_t)v * nn + e * NDOF + n;
+                    acc[v * ST + sp<DIM, Np>(n)] = stage_combine(P, gi, acc[v * ST + sp<DIM, Np>(n)]);
+                }
+            }
+        }
+    }
+    __syncwarp();
+    // faces: direction by direction, so that no two lanes update one node at once
+    const double iw0 = 1.0 / C_W(c)[0];
+#pragma unroll 1
+    for (int d = 0; d < DIM; d++) {
+        if (valid) {
+            for (int t = gl; t < 2 * NFN; t += L) {
+                const int side = t >= NFN, fn = side ? t - NFN : t;
+                const int f = 2 * d + side;
+                const int n = line_node_rt<DIM, Np>(d, fn, side ? N : 0);
+                const int64_t other = __ldg(P.nbr + e * 2 * DIM + f);
+                const int64_t fi = (e * 2 * DIM + f) * NFN + fn;
+                double nor[DIM], s[NV], F[NV];
+#pragma unroll
+                for (int k = 0; k < DIM; k++) nor[k] = __ldg(P.fnor + fi * DIM + k);
+#pragma unroll
+                for (int v = 0; v < NV; v++) s[v] = __ldg(P.u + (int64_t)v * nn + e * NDOF + n);
+                const double J = geo_J(P, e * NDOF + n);
+                double sgn;
+                if (other >= 0) {
+                    const int n2 = __ldg(P.fnode + fi);
+                    double o[NV];
+#pragma unroll
+                    for (int v = 0; v < NV; v++) o[v] = __ldg(P.u + (int64_t)v * nn + other * NDOF + n2);
+                    const bool is1 = e < other || (e == other && side == 1);
+                    double s1[NV], s2[NV];
+#pragma unroll
+                    for (int v = 0; v < NV; v++) {
+                        s1[v] = is1 ? s[v] : o[v];
+                        s2[v] = is1 ? o[v] : s[v];
+                    }
+                    const Prim<DIM> qa = make_prim<DIM>(s1, P.gamma, P.gm1), qb = make_prim<DIM>(s2, P.gamma, P.gm1);
+                    face_flux_n<DIM>(qa, qb, s1 + 1, s2 + 1, nor, P.gm1inv, P.compat != 0, P.diss_scale, F);
+                    lam = fmax(lam, fmax(qa.lam, qb.lam));
+                    sgn = is1 ? -1.0 : 1.0;
+                } else {
+                    lam = fmax(lam, geo_bdr_flux<DIM>(P, (int)(-1 - other), s, nor, F));
+                    sgn = -1.0;
+                }
+                // AddMult_a_VWt(1 / (w0 J), shape, +-F)
+                const double scale = iw0 / J;
+                const int m = sp<DIM, Np>(n);
+#pragma unroll
+                for (int v = 0; v < NV; v++) acc[v * ST + m] += coef * (scale * (sgn * F[v]));
+            }
+        }
+        __syncwarp();
+    }
+    if (valid) {
+#pragma unroll
+        for (int k = 0; k < S::NPL; k++) {
+            const int n = gl + k * L;
+            if (n < NDOF) {
+#pragma unroll
+                for (int v = 0; v < NV; v++) P.out[(int64_t)v * nn + e * NDOF + n] = acc[v * ST + sp<DIM, Np>(n)];
+            }
+        }
+    }
+    __syncwarp();
+}
+
+template <int DIM, int N>
+__global__ void __launch_bounds__(128) geo_rhs_kernel(const KParams P)
+{
+    using S = Shape<DIM, N>;
+    constexpr int Np = S::Np, L = S::L, EPW = S::EPW;
+    extern __shared__ double smem[];
+    double *c = smem;
+    load_consts(P.K, c, Np);
+    __syncthreads();
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int grp = lane / L, gl = lane % L;
+    const int wpb = blockDim.x >> 5;
+    const bool lane_used = grp < EPW;
+    double *pr = smem + const_slots(Np) + (size_t)(warp * EPW + (lane_used ? grp : 0)) * S::EL_RHS_FB;
+    const int64_t wstride = (int64_t)gridDim.x * wpb;
+    unsigned int flags = 0;
+    double lam = 0.0;
+    for (int64_t wt = (int64_t)blockIdx.x * wpb + warp; wt < P.nwt; wt += wstride)
+        geo_tile<DIM, N>(P, c, pr, P.e_begin + wt * EPW, grp, gl, lane_used, flags, lam);
+    lam = group_max<32>(lam);
+    if (lane == 0) atomic_max_pos(P.lam_bits, lam);
+    flags = __reduce_or_sync(0xffffffffu, flags);
+    if (lane == 0 && flags) atomicOr(P.err, flags);
+}
+
+}  // namespace pdg

@@ -39,7 +39,8 @@ enum KernelKind {
     KIND_LIFT_FACE_FLUX = 32,   // lift_face_kernel<dim, N, false, FACE_JUMP | FACE_FLUX>: jumps + face fluxes (NS)
     KIND_FACE_FLUX = 33,        // lift_face_kernel<dim, N, false, FACE_FLUX>: face fluxes (Euler)
     KIND_POSITIVITY = 34,       // positivity_kernel<dim, N>: positivity limiter of the stage output
-    KIND_COUNT = 35
+    KIND_GEO = 35,              // geo_rhs_kernel<dim, N>: Euler right-hand side (+ stage) on a general-geometry mesh
+    KIND_COUNT = 36
 };
 
 struct KernelInfo {

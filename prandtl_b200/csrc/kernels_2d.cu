@@ -3,6 +3,7 @@
 #include "kernel_table.h"
 #include "line_kernels.cuh"
 #include "filter_kernels.cuh"
+#include "geo_kernels.cuh"
 
 namespace pdg {
 
@@ -49,6 +50,7 @@ template <int N> static bool info_n(int kind, KernelInfo *out)
     
     case KIND_FILTER_BOUNDS: out->fn = (const void *)&filter_bounds_kernel<2, N>; out->epw = 1; break;
     case KIND_POSITIVITY: out->fn = (const void *)&positivity_kernel<2, N>; out->epw = 1; break;
+    case KIND_GEO: out->fn = (const void *)&geo_rhs_kernel<2, N>; out->el_doubles = S::EL_RHS_FB; break;
     case KIND_FILTER:
         out->fn = (const void *)&filter_kernel<2, N>;
         out->el_doubles = FilterShape<2, N>::EL;

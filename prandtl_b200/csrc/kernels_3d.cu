@@ -3,6 +3,7 @@
 #include "kernel_table.h"
 #include "line_kernels.cuh"
 #include "filter_kernels.cuh"
+#include "geo_kernels.cuh"
 
 namespace pdg {
 
@@ -48,6 +49,7 @@ template <int N> static bool info_n(int kind, KernelInfo *out)
     case KIND_FACE_NS2: out->fn = (const void *)&face_kernel<3, N, 2, true>; break;
     case KIND_FILTER_BOUNDS: out->fn = (const void *)&filter_bounds_kernel<3, N>; out->epw = 1; break;
     case KIND_POSITIVITY: out->fn = (const void *)&positivity_kernel<3, N>; out->epw = 1; break;
+    case KIND_GEO: out->fn = (const void *)&geo_rhs_kernel<3, N>; out->el_doubles = S::EL_RHS_FB; break;
     case KIND_FILTER:
         out->fn = (const void *)&filter_kernel<3, N>;
         out->el_doubles = FilterShape<3, N>::EL;

@@ -100,6 +100,13 @@ struct KParams {
     // elements [e_begin, e_end) that the face-node, lifting and volume
     // kernels process (e_end = 0: up to ne); nwt counts the range's tiles
     int64_t e_begin, e_end;
+    // general geometry (geo_rhs_kernel): per node J and the adjugate rows,
+    // geo[q * nnodes + node], q = 0: J, 1 + r * dim + k: adj(r, k); per
+    // element face node the neighbour's matching node (local index) and the
+    // face normal as the face's element 1 sees it, [e][face][face node](, k)
+    const double *geo;
+    const int32_t *fnode;
+    const double *fnor;
 };
 
 __device__ __forceinline__ int64_t range_end(const KParams &P) { return P.e_end ? P.e_end : P.ne; }

@@ -190,6 +190,63 @@ PDG_FN void face_flux(const Prim<DIM> &a, const Prim<DIM> &b, const double *ma, 
     F[1 + DIM] = fm * h_hat - lam * diss;
 }
 
+// volume_flux for a general contravariant metric vector n (the mean of the
+// two nodes' metric rows on a curved element, ChandrashekarFlux.cpp:11-83):
+// Vn = v_mean . n and the pressure term p_hat n.
+template <int DIM>
+PDG_FN void volume_flux_n(const Prim<DIM> &a, const Prim<DIM> &b, const double *n, double gm1inv, double *F)
+{
+    double rho_ln, irho_ln, ibeta_ln, isb, p_hat;
+    two_point_means(a.rho, b.rho, a.beta, b.beta, rho_ln, irho_ln, ibeta_ln, isb, p_hat);
+    double vm[DIM];
+    double h_hat = 0.0, Vn = 0.0;
+#pragma unroll
+    for (int d = 0; d < DIM; d++) {
+        vm[d] = 0.5 * (a.v[d] + b.v[d]);
+        h_hat += -0.25 * (a.v[d] * a.v[d] + b.v[d] * b.v[d]) + vm[d] * vm[d];
+        Vn += vm[d] * n[d];
+    }
+    h_hat += 0.5 * ibeta_ln * gm1inv + p_hat * irho_ln;
+    const double fm = rho_ln * Vn;
+    F[0] = fm;
+#pragma unroll
+    for (int d = 0; d < DIM; d++) F[1 + d] = fm * vm[d] + p_hat * n[d];
+    F[1 + DIM] = fm * h_hat;
+}
+
+// face_flux for a general normal vector n (ChandrashekarFlux.cpp:85-161): the
+// Lax-Friedrichs term scales with |n|.
+template <int DIM>
+PDG_FN void face_flux_n(const Prim<DIM> &a, const Prim<DIM> &b, const double *ma, const double *mb,
+                        const double *n, double gm1inv, bool compat, double diss_scale, double *F)
+{
+    double rho_ln, irho_ln, ibeta_ln, isb, p_hat;
+    two_point_means(a.rho, b.rho, a.beta, b.beta, rho_ln, irho_ln, ibeta_ln, isb, p_hat);
+    const double rho_mean = 0.5 * (a.rho + b.rho), drho = b.rho - a.rho;
+    double vm[DIM];
+    double h_hat = 0.0, diss = 0.0, Vn = 0.0, nn = 0.0;
+#pragma unroll
+    for (int d = 0; d < DIM; d++) {
+        vm[d] = 0.5 * (a.v[d] + b.v[d]);
+        const double dv = b.v[d] - a.v[d];
+        h_hat += -0.25 * (a.v[d] * a.v[d] + b.v[d] * b.v[d]) + vm[d] * vm[d];
+        if (DIM == 3 && d == 2 && compat)
+            diss += 0.5 * drho * a.v[d] * b.v[d] + rho_mean * dv + vm[d];
+        else
+            diss += 0.5 * drho * a.v[d] * b.v[d] + rho_mean * dv * vm[d];
+        Vn += vm[d] * n[d];
+        nn += n[d] * n[d];
+    }
+    h_hat += 0.5 * ibeta_ln * gm1inv + p_hat * irho_ln;
+    diss += 0.5 * drho * gm1inv * ibeta_ln + 0.5 * rho_mean * gm1inv * (b.ib - a.ib);
+    const double lam = 0.5 * fmax(a.lam, b.lam) * diss_scale * sqrt(nn);
+    const double fm = rho_ln * Vn;
+    F[0] = fm - lam * drho;
+#pragma unroll
+    for (int d = 0; d < DIM; d++) F[1 + d] = fm * vm[d] + p_hat * n[d] - lam * (mb[d] - ma[d]);
+    F[1 + DIM] = fm * h_hat - lam * diss;
+}
+
 // NavierStokesFlux::ComputeViscousFlux (src/Fluxes/NavierStokesFlux.cpp:12-90),
 // constant mu, mu_bulk = 2/3, column `dir` only (flux along x_dir): momentum
 // rows out[0..DIM-1] and the energy row out[DIM].  g(d, v) returns the

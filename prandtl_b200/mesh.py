@@ -76,6 +76,18 @@ class CartesianMesh:
     attributes: np.ndarray | None = None
     reoriented: np.ndarray | None = None   # elements whose corner order the reader relabelled
     frames: np.ndarray | None = None       # (ne, dim) file frame of each element, +-(axis + 1)
+    # general geometry (skewed, graded, curved or unstructured elements): the
+    # physical coordinates of every DG node, (dim, num_nodes) byNODES, and the
+    # face orientation codes of the C ABI's pdg_set_geometry, (ne, 2*dim)
+    # (None: every neighbour meets a face with its opposite face, axes aligned)
+    coords: np.ndarray | None = None
+    face_orient: np.ndarray | None = None
+    corners: np.ndarray | None = None      # (ne, 2^dim) corner vertex ids, lexicographic corner order
+
+    @property
+    def general(self) -> bool:
+        """True when the mesh carries its own node coordinates (the general-geometry path)."""
+        return self.coords is not None
 
     @property
     def Np(self) -> int:
@@ -110,6 +122,12 @@ class CartesianMesh:
     def node_coords(self, elements=None) -> np.ndarray:
         """Physical coordinates, shape (dim, num_nodes), in the byNODES order
         (of the listed elements only, when `elements` is given)."""
+        if self.coords is not None:
+            if elements is None:
+                return np.array(self.coords, dtype=np.float64)
+            e = np.asarray(elements, dtype=np.int64)
+            X = np.asarray(self.coords).reshape(self.dim, self.num_elements, self.ndof)
+            return X[:, e, :].reshape(self.dim, -1)
         x1, _ = gll_nodes(self.Np)
         Np, dim = self.Np, self.dim
         e = np.arange(self.num_elements) if elements is None else np.asarray(elements, dtype=np.int64)

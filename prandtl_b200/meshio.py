@@ -45,9 +45,15 @@ from __future__ import annotations
 
 import numpy as np
 
+from .geometry import connect, multilinear_nodes
 from .mesh import CartesianMesh
 
 MAX_CONDITIONS = 16          # PDG_MAX_BOUNDARIES
+
+
+class NotBoxError(ValueError):
+    """The elements are not equal axis-aligned boxes on one grid (the box
+    kernels' form); the mesh may still be read as a general-geometry mesh."""
 
 # corner k of an MFEM/Gmsh quadrilateral or hexahedron -> its (x, y, z) bits
 _CORNER_BITS = {
@@ -56,10 +62,14 @@ _CORNER_BITS = {
 }
 
 
-def read_mesh(path: str, order: int, refine: int = 0, tol: float = 1e-8) -> CartesianMesh:
+def read_mesh(path: str, order: int, refine: int = 0, tol: float = 1e-8, general=None) -> CartesianMesh:
     """The mesh in ``path`` (MFEM v1.0 or Gmsh 2.2 ASCII) with polynomial
     order ``order``, refined ``refine`` times.  ``tol`` is the relative
-    tolerance of the box-shape and uniform-size checks."""
+    tolerance of the box-shape and uniform-size checks.  ``general``: False
+    reads equal axis-aligned boxes only (the box kernels), True every mesh
+    as a general-geometry mesh (``build_general_mesh``: node coordinates
+    and face orientation codes for the general-geometry kernel), None the
+    box form when the elements allow it, else the general form."""
     with open(path) as f:
         text = f.read()
     head = text.lstrip()[:40]
@@ -69,9 +79,17 @@ def read_mesh(path: str, order: int, refine: int = 0, tol: float = 1e-8) -> Cart
         parsed = _parse_gmsh(text)
     else:
         raise ValueError(f"{path}: neither an MFEM v1.0 nor a Gmsh 2.2 mesh")
-    mesh = build_mesh(order=order, tol=tol, **parsed)
+    if general:
+        mesh = build_general_mesh(order=order, **parsed)
+    else:
+        try:
+            mesh = build_mesh(order=order, tol=tol, **parsed)
+        except NotBoxError:
+            if general is False:
+                raise
+            mesh = build_general_mesh(order=order, **parsed)
     for _ in range(int(refine)):
-        mesh = refine_mesh(mesh)
+        mesh = refine_general(mesh) if mesh.coords is not None else refine_mesh(mesh)
     return mesh
 
 
@@ -225,7 +243,7 @@ def _canonical_corners(dim, verts, coords):
     inv[rows, key.reshape(-1)] = np.tile(np.arange(nc), ne)
     if np.any(inv < 0):
         bad = int(np.nonzero(np.any(inv < 0, axis=1))[0][0])
-        raise ValueError(f"element {bad} is not a box (degenerate or non-convex corners)")
+        raise NotBoxError(f"element {bad} is not a box (degenerate or non-convex corners)")
     pos = inv[:, want]
     moved = np.nonzero(np.any(pos != np.arange(nc), axis=1))[0]
     cbits = np.array(_CORNER_BITS[dim], dtype=np.int64)
@@ -255,20 +273,20 @@ def build_mesh(dim, order, verts, coords, bdr, names, attrs=None, tol=1e-8) -> C
     ext = np.stack([coords[:, (1, 3, 4)[d], d] - origin[:, d] for d in range(dim)], axis=1)
     if np.any(ext <= 0):
         bad = int(np.nonzero(np.any(ext <= 0, axis=1))[0][0])
-        raise ValueError(f"element {bad} is degenerate (an extent of zero)")
+        raise NotBoxError(f"element {bad} is degenerate (an extent of zero)")
     h = ext.mean(axis=0)
     expect = origin[:, None, :] + bits[None, :, :] * ext[:, None, :]
     if np.any(np.abs(coords - expect) > tol * h):
         bad = int(np.nonzero(np.any(np.abs(coords - expect) > tol * h, axis=(1, 2)))[0][0])
-        raise ValueError(f"element {bad} is not an axis-aligned box (curved or skewed geometry is not supported)")
+        raise NotBoxError(f"element {bad} is not an axis-aligned box (curved or skewed geometry is not supported)")
     if np.any(np.abs(ext - h) > tol * h):
-        raise ValueError("elements of different sizes (graded meshes are not supported)")
+        raise NotBoxError("elements of different sizes (graded meshes are not supported)")
     lo = origin.min(axis=0)
     hi = (origin + ext).max(axis=0)
     g = (origin - lo) / h
     gi = np.rint(g).astype(np.int64)
     if np.any(np.abs(g - gi) > 1e-6):
-        raise ValueError("element corners off the grid of the element size")
+        raise NotBoxError("element corners off the grid of the element size")
     n = tuple(int(v) for v in np.rint((hi - lo) / h))
     cells = np.zeros(ne, dtype=np.int64)
     stride = 1
@@ -276,7 +294,7 @@ def build_mesh(dim, order, verts, coords, bdr, names, attrs=None, tol=1e-8) -> C
         cells += gi[:, d] * stride
         stride *= n[d]
     if len(np.unique(cells)) != ne:
-        raise ValueError("overlapping elements")
+        raise NotBoxError("overlapping elements")
 
     nbr = np.full((ne, 2 * dim), np.iinfo(np.int32).min, dtype=np.int64)
     faces: dict = {}
@@ -291,7 +309,7 @@ def build_mesh(dim, order, verts, coords, bdr, names, attrs=None, tol=1e-8) -> C
         if len(owners) == 2:
             (e1, d1, s1), (e2, d2, s2) = owners
             if d1 != d2 or s1 == s2:
-                raise ValueError(f"elements {e1} and {e2} meet with differently oriented axes")
+                raise NotBoxError(f"elements {e1} and {e2} meet with differently oriented axes")
             nbr[e1, 2 * d1 + s1] = e2
             nbr[e2, 2 * d2 + s2] = e1
         elif len(owners) == 1:
@@ -391,3 +409,129 @@ def to_reference_order(mesh: CartesianMesh, u: np.ndarray) -> np.ndarray:
     x = np.asarray(u).reshape(-1, mesh.num_elements, mesh.ndof)
     rows = np.arange(mesh.num_elements)[:, None]
     return x[:, rows, perm].reshape(np.shape(u))
+
+
+def _lex_positions(dim):
+    """Lexicographic corner index (x fastest) of each MFEM/Gmsh corner k."""
+    return [sum(b << d for d, b in enumerate(bits)) for bits in _CORNER_BITS[dim]]
+
+
+def _corner_jacobians(dim, xyz):
+    """Determinant of the multilinear map's Jacobian at every corner of
+    every element (corners in lexicographic order), (ne, 2^dim)."""
+    ne, nc = xyz.shape[0], xyz.shape[1]
+    out = np.empty((ne, nc))
+    for c in range(nc):
+        cols = []
+        for a in range(dim):
+            lo_c, hi_c = c & ~(1 << a), c | (1 << a)
+            cols.append(xyz[:, hi_c, :] - xyz[:, lo_c, :])
+        out[:, c] = np.linalg.det(np.stack(cols, axis=2))
+    return out
+
+
+def _general_mesh(dim, order, corners, xyz, boundary, names, attrs, frames, reoriented):
+    nbr, orient = connect(dim, corners, boundary)
+    ne = corners.shape[0]
+    lo = xyz.reshape(-1, dim).min(axis=0)
+    hi = xyz.reshape(-1, dim).max(axis=0)
+    size = np.sqrt(np.abs(_corner_jacobians(dim, xyz)).min()) if dim == 2 else np.cbrt(
+        np.abs(_corner_jacobians(dim, xyz)).min())
+    used = {int(-1 - b) + 1 for b in nbr[nbr < 0]}
+    m = CartesianMesh(dim, int(order), (ne,) + (1,) * (dim - 1), tuple(float(v) for v in lo),
+                      tuple(float(v) for v in hi), nbr, spacing=(float(size),) * dim, boundaries={},
+                      boundary_names={k: int(v) - 1 for k, v in names.items() if int(v) in used},
+                      attributes=None if attrs is None else np.asarray(attrs), reoriented=reoriented, frames=frames)
+    m.coords = multilinear_nodes(dim, order, xyz)
+    m.face_orient = orient
+    m.corners = corners
+    m.corner_xyz = xyz
+    return m
+
+
+def build_general_mesh(dim, order, verts, coords, bdr, names, attrs=None) -> CartesianMesh:
+    """A general-geometry mesh (skewed, graded or unstructured quadrilaterals
+    or hexahedra with straight edges): each element keeps the file's frame
+    (its corners in MFEM/Gmsh order map to the reference element's corners),
+    its DG nodes sit at the images of the LGL nodes under the element's
+    bilinear / trilinear map, and ``connect`` pairs faces by their vertices
+    and derives the orientation codes.  An element whose corners the file
+    lists clockwise (a negative Jacobian) is mirrored by exchanging its first
+    two local axes, as MFEM's mesh finalisation does for quadrilaterals
+    (swapping corners 1 and 3); ``mesh.reoriented`` lists it and
+    ``mesh.frames`` holds its file frame for ``to_reference_order``."""
+    ne, nc = verts.shape
+    if nc != 2 ** dim:
+        raise ValueError(f"elements with {nc} corners in {dim}D")
+    lex = _lex_positions(dim)
+    corners = np.empty((ne, nc), dtype=np.int64)
+    xyz = np.empty((ne, nc, dim))
+    corners[:, lex] = verts
+    xyz[:, lex, :] = coords
+    det = _corner_jacobians(dim, xyz)
+    neg = np.all(det < 0, axis=1)
+    bad = ~(np.all(det > 0, axis=1) | neg)
+    if bad.any():
+        raise ValueError(f"element {int(np.nonzero(bad)[0][0])} is degenerate or not convex")
+    frames = np.tile(np.arange(1, dim + 1, dtype=np.int8), (ne, 1))
+    reoriented = np.nonzero(neg)[0]
+    if reoriented.size:
+        swap = np.array([(c & ~3) | ((c & 1) << 1) | ((c >> 1) & 1) for c in range(nc)])
+        corners[reoriented] = corners[reoriented][:, swap]
+        xyz[reoriented] = xyz[reoriented][:, swap, :]
+        frames[reoriented, 0], frames[reoriented, 1] = 2, 1
+    boundary = {}
+    for key, a in bdr.items():
+        if not 1 <= int(a) <= MAX_CONDITIONS:
+            raise ValueError(f"boundary attribute {a}: attributes 1..{MAX_CONDITIONS} are supported")
+        boundary[frozenset(int(v) for v in key)] = int(a) - 1
+    return _general_mesh(dim, order, corners, xyz, boundary, names, attrs, frames, reoriented)
+
+
+def refine_general(mesh: CartesianMesh) -> CartesianMesh:
+    """Every element of a general mesh split into 2^dim children (``2^dim e
+    + c``, c lexicographic in the element's frame) at the midpoints of its
+    multilinear map; new vertices are shared through the parent vertices
+    they lie between, boundary faces keep their conditions."""
+    if getattr(mesh, "corner_xyz", None) is None:
+        raise ValueError("refine_general() takes a mesh from build_general_mesh")
+    dim, nc = mesh.dim, 2 ** mesh.dim
+    ne = mesh.num_elements
+    P, X = np.asarray(mesh.corners), np.asarray(mesh.corner_xyz)
+    keys: dict = {}
+    corners = np.empty((ne * nc, nc), dtype=np.int64)
+    xyz = np.empty((ne * nc, nc, dim))
+    for e in range(ne):
+        for c in range(nc):
+            for k in range(nc):
+                half = [((c >> q) & 1) + ((k >> q) & 1) for q in range(dim)]   # 0, 1, 2 in half steps
+                touched = [pc for pc in range(nc)
+                           if all((half[q] == 1) or (((pc >> q) & 1) == half[q] // 2) for q in range(dim))]
+                key = frozenset(int(P[e, pc]) for pc in touched)
+                if len(touched) == nc:
+                    key = ("cell", e)
+                if key not in keys:
+                    keys[key] = len(keys)
+                corners[e * nc + c, k] = keys[key]
+                w = np.ones(nc)
+                for pc in range(nc):
+                    for q in range(dim):
+                        t = half[q] / 2.0
+                        w[pc] *= t if (pc >> q) & 1 else 1.0 - t
+                xyz[e * nc + c, k] = w @ X[e]
+    # boundary faces: a child face on a parent boundary face keeps its condition
+    boundary = {}
+    from .geometry import face_corner_slots
+    for e, f in zip(*np.nonzero(mesh.nbr < 0)):
+        b = int(-1 - mesh.nbr[e, f])
+        d, side = divmod(int(f), 2)
+        for c in range(nc):
+            if ((c >> d) & 1) != side:
+                continue
+            vs = corners[e * nc + c, face_corner_slots(dim, int(f))]
+            boundary[frozenset(int(v) for v in vs)] = b
+    names = {k: v + 1 for k, v in (mesh.boundary_names or {}).items()}
+    attrs = None if mesh.attributes is None else np.repeat(mesh.attributes, nc)
+    m = _general_mesh(dim, mesh.order, corners, xyz, boundary, names, attrs, None, None)
+    m.boundaries = dict(mesh.boundaries or {})
+    return m

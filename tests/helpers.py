@@ -12,7 +12,9 @@ GOLDEN = os.path.join(os.path.dirname(__file__), "golden")
 
 
 def golden_cases():
-    return sorted(os.path.splitext(os.path.basename(p))[0] for p in glob.glob(os.path.join(GOLDEN, "*.npz")))
+    # (mesh_*.npz are mesh fixtures, not right-hand-side cases)
+    return sorted(os.path.splitext(os.path.basename(p))[0] for p in glob.glob(os.path.join(GOLDEN, "*.npz"))
+                  if not os.path.basename(p).startswith("mesh_"))
 
 
 def load_golden(name):
@@ -39,3 +41,58 @@ def rough(u, mesh, seed, amp_rho=0.15, amp_e=0.03):
     u[:nn] *= 1 + amp_rho * rng.standard_normal(nn)
     u[(mesh.nv - 1) * nn:] *= 1 + amp_e * rng.standard_normal(nn)
     return u
+
+
+def smooth_state(mesh, seed=0):
+    """A positive state with random smooth-free node values (every element
+    rough enough that the blending switches on)."""
+    rng = np.random.default_rng(seed)
+    nn, dim = mesh.num_nodes, mesh.dim
+    u = np.empty(mesh.size)
+    u[:nn] = 1 + 0.1 * rng.random(nn)
+    for d in range(dim):
+        u[(1 + d) * nn:(2 + d) * nn] = 0.2 * rng.standard_normal(nn)
+    u[(dim + 1) * nn:] = 2.5 + 0.1 * rng.random(nn)
+    return u
+
+
+# Boundary conditions of the general-geometry layouts with boundary faces:
+# Mach-3-like inflow, outflow, slip wall, symmetry (2D); plus Riemann
+# invariants and a subsonic pressure outflow (3D).
+GEO_BCS_2D = {0: (1, [1.4, 4.2, 0.3, 8.8]), 1: (2, None), 2: (4, None), 3: (5, None)}
+GEO_BCS_3D = {0: (1, [1.4, 4.2, 0.3, 0.1, 8.8]), 1: (2, None), 2: (4, None), 3: (5, None),
+              4: (9, [1.0, 0.5, 0.1, 0.0, 1.0]), 5: (6, [0.9])}
+
+
+def geometry_case(name):
+    """General-geometry meshes: curved (a warped box, degree-N elements),
+    skewed (an affine shear), perturbed (bilinear / trilinear elements with
+    randomly moved vertices), rotated (element frames rotated, so that faces
+    meet in other orientations, as in an unstructured mesh), and boundary
+    layouts of perturbed boxes."""
+    from prandtl_b200 import geometry as G
+    from prandtl_b200.mesh import periodic_box
+    if name == "warped2d":
+        return G.warped(periodic_box(2, 3, (4, 5), 0.0, 1.0), 0.04)
+    if name == "skewed2d":
+        return G.skewed(periodic_box(2, 4, (5, 4), 0.0, 1.0), 0.4)
+    if name == "perturbed2d":
+        return G.perturbed_box(2, 3, (4, 5), 0.0, 1.0, 0.3, seed=1)
+    if name == "rotated2d":
+        return G.rotate_frames(G.perturbed_box(2, 3, (4, 5), 0.0, 1.0, 0.3, seed=1), [0, 3, 5, 7, 8, 12], seed=2)
+    if name == "boundary2d":
+        return G.perturbed_box(2, 3, (5, 4), 0.0, 1.0, 0.3, seed=5, bdr=[(0, 1), (2, 3)], boundaries=GEO_BCS_2D)
+    if name == "warped3d":
+        return G.warped(periodic_box(3, 2, (3, 4, 3), 0.0, 1.0), 0.03)
+    if name == "perturbed3d":
+        return G.perturbed_box(3, 3, (3, 3, 3), 0.0, 1.0, 0.25, seed=3)
+    if name == "rotated3d":
+        return G.rotate_frames(G.perturbed_box(3, 2, (3, 3, 3), 0.0, 1.0, 0.25, seed=3), [0, 4, 9, 13, 20], seed=4)
+    if name == "boundary3d":
+        return G.perturbed_box(3, 2, (3, 3, 4), 0.0, 1.0, 0.25, seed=6, bdr=[(0, 1), (2, 3), (4, 5)],
+                               boundaries=GEO_BCS_3D)
+    raise KeyError(name)
+
+
+GEO_CASES = ["warped2d", "skewed2d", "perturbed2d", "rotated2d", "boundary2d", "warped3d", "perturbed3d",
+             "rotated3d", "boundary3d"]

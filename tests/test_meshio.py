@@ -12,7 +12,7 @@ import pytest
 
 import prandtl_b200 as pb
 from prandtl_b200 import meshio
-from prandtl_b200.mesh import box, periodic_box
+from prandtl_b200.mesh import box, gll_nodes, periodic_box
 
 CORNERS = meshio._CORNER_BITS
 
@@ -260,7 +260,8 @@ def test_rejections(tmp_path):
     lines[i] = " ".join([r[0], str(float(r[1]) + 0.01)] + r[2:])      # skew one vertex
     open(path, "w").write("\n".join(lines))
     with pytest.raises(ValueError, match="box|sizes|grid"):
-        meshio.read_mesh(path, 1)
+        meshio.read_mesh(path, 1, general=False)
+    assert meshio.read_mesh(path, 1).coords is not None  # read as a general-geometry mesh
     open(path, "w").write(text.replace("$MeshFormat\n2.2 0 8", "$MeshFormat\n2.2 1 8"))
     with pytest.raises(ValueError, match="ASCII"):
         meshio.read_mesh(path, 1)
@@ -320,7 +321,7 @@ def test_reference_gmsh_meshes():
                      ("Euler/2D/Ramp/Ramp15deg_v2.msh", "axis-aligned"),
                      ("Euler/2D/Nagashima_Ramjet/TR0/Nagashima_TR0_11kQuad_v2.msh", "box")):
         with pytest.raises(ValueError, match=why):
-            meshio.read_mesh(ref_file(rel), 2)
+            meshio.read_mesh(ref_file(rel), 2, general=False)
 
 
 def test_read_mesh_runs_in_the_oracle(tmp_path):
@@ -436,4 +437,255 @@ def test_gpu_read_mesh_matches_oracle(tmp_path, compat, parabolic, dim, cuda_dev
     op.rk3_step(x, dt, nsteps=1, graph=True)
     torch.cuda.synchronize()
     assert rel_maxnorm(x.cpu().numpy(), y) < 1e-11
+    assert op.check() == 0
+
+
+# ---- general-geometry meshes (graded, skewed, unstructured) ----
+
+def face_tables_consistent(m, period=None):
+    """Every interior face node meets its neighbour's matching node (up to one
+    periodic shift per face) and every neighbour points back."""
+    from prandtl_b200.geometry import map_face_index
+    dim, Np, N = m.dim, m.Np, m.order
+    X = np.asarray(m.coords).reshape(dim, m.num_elements, m.ndof)
+    fo = m.face_orient
+    nfn = Np ** (dim - 1)
+    for e in range(m.num_elements):
+        for f in range(2 * dim):
+            nb = int(m.nbr[e, f])
+            if nb < 0:
+                continue
+            f2, o = int(fo[e, f]) & 7, int(fo[e, f]) >> 3
+            assert int(m.nbr[nb, f2]) == e
+            shift = None
+            for t in range(nfn):
+                a, b = t % Np, t // Np
+                a2, b2 = map_face_index(dim, N, a, b, o)
+                d = X[:, e, _fnode(dim, Np, f, a + Np * b)] - X[:, nb, _fnode(dim, Np, f2, a2 + Np * b2)]
+                shift = d if shift is None else shift
+                assert np.abs(d - shift).max() < 1e-9
+
+
+def _fnode(dim, Np, f, t):
+    d, side = divmod(f, 2)
+    pos = Np - 1 if side else 0
+    if dim == 2:
+        return t * Np + pos if d == 0 else pos * Np + t
+    if d == 0:
+        return t * Np + pos
+    if d == 1:
+        return (t // Np) * Np * Np + pos * Np + (t % Np)
+    return pos * Np * Np + t
+
+
+def write_gmsh_general(path, m, rng):
+    """A Gmsh file of a general mesh with straight edges: vertices from its
+    corner nodes, elements listed with rotated or mirrored corners in a
+    shuffled order, boundary lines with attribute b + 1."""
+    dim, Np = m.dim, m.Np
+    X = np.asarray(m.coords).reshape(dim, m.num_elements, m.ndof)
+    lexc = [sum(((c >> q) & 1) * (Np - 1) * Np ** q for q in range(dim)) for c in range(2 ** dim)]
+    nv = int(m.corners.max()) + 1
+    vxyz = np.zeros((nv, 3))
+    for e in range(m.num_elements):
+        for c in range(2 ** dim):
+            vxyz[m.corners[e, c], :dim] = X[:, e, lexc[c]]
+    gorder = [sum(b << d for d, b in enumerate(bits)) for bits in meshio._CORNER_BITS[dim]]
+    file_corners = m.corners[:, gorder]                # MFEM/Gmsh order
+    perm = rng.permutation(m.num_elements)
+    listed = rotate(file_corners[perm], dim, rng)
+    from prandtl_b200.geometry import face_corner_slots
+    bl = []
+    for e, f in zip(*np.nonzero(m.nbr < 0)):
+        bl.append((int(-m.nbr[e, f]), m.corners[e, face_corner_slots(dim, int(f))]))
+    lines = ["$MeshFormat", "2.2 0 8", "$EndMeshFormat", "$Nodes", str(nv)]
+    lines += [f"{k + 1} " + " ".join(f"{v:.17g}" for v in vxyz[k]) for k in range(nv)]
+    lines += ["$EndNodes", "$Elements", str(len(bl) + len(listed))]
+    eid = 0
+    for a, vs in bl:
+        eid += 1
+        lines.append(f"{eid} 1 2 {a} {a} " + " ".join(str(v + 1) for v in vs))
+    for c in listed:
+        eid += 1
+        lines.append(f"{eid} 3 2 99 1 " + " ".join(str(v + 1) for v in c))
+    lines.append("$EndElements")
+    open(path, "w").write("\n".join(lines) + "\n")
+    return perm
+
+
+def test_general_gmsh_round_trip(tmp_path):
+    """A perturbed (skewed, non-affine) channel written with shuffled elements
+    and rotated or mirrored corner listings reads back as the same mesh: the
+    oracle's right-hand side agrees node by node (matched by position)."""
+    import oracle
+    from prandtl_b200 import geometry as G
+    bcs = {0: (1, [1.4, 4.2, 0.3, 8.8]), 1: (2, None), 2: (4, None), 3: (4, None)}
+    orig = G.perturbed_box(2, 3, (6, 4), 0.0, 1.0, 0.3, seed=3, bdr=[(0, 1), (2, 3)], boundaries=bcs)
+    rng = np.random.default_rng(5)
+    path = str(tmp_path / "g.msh")
+    perm = write_gmsh_general(path, orig, rng)
+    m = meshio.read_mesh(path, 3)
+    assert m.coords is not None and m.num_elements == orig.num_elements and len(m.reoriented) > 0
+    face_tables_consistent(m)
+    m.boundaries = {b: bcs[b] for b in bcs}
+    x = m.node_coords()
+    u = np.concatenate([1 + 0.2 * np.sin(3 * x[0]) * np.cos(2 * x[1]), 0.3 + 0.1 * x[1], 0.1 * x[0] - 0.05,
+                        2.5 + 0.1 * np.cos(x[0] + x[1])])
+    xo = orig.node_coords()
+    uo = np.concatenate([1 + 0.2 * np.sin(3 * xo[0]) * np.cos(2 * xo[1]), 0.3 + 0.1 * xo[1], 0.1 * xo[0] - 0.05,
+                         2.5 + 0.1 * np.cos(xo[0] + xo[1])])
+    r = oracle.Oracle(m, compat=0, parabolic=0).rhs(u).reshape(4, m.num_elements, m.ndof)
+    ro = oracle.Oracle(orig, compat=0, parabolic=0).rhs(uo).reshape(4, orig.num_elements, orig.ndof)
+    X = x.reshape(2, m.num_elements, m.ndof)
+    XO = xo.reshape(2, orig.num_elements, orig.ndof)
+    for i in range(m.num_elements):
+        eo = perm[i]
+        for n in range(m.ndof):
+            k = int(np.argmin(np.abs(XO[0, eo] - X[0, i, n]) + np.abs(XO[1, eo] - X[1, i, n])))
+            assert abs(XO[0, eo, k] - X[0, i, n]) + abs(XO[1, eo, k] - X[1, i, n]) < 1e-12
+            np.testing.assert_allclose(r[:, i, n], ro[:, eo, k], rtol=1e-11, atol=1e-11 * np.abs(ro).max())
+
+
+def test_general_refinement():
+    """Two refinements of a general mesh: 16x the elements, conforming faces,
+    the same area, and the oracle runs on it."""
+    import oracle
+    from prandtl_b200 import geometry as G
+    orig = G.perturbed_box(2, 2, (3, 4), 0.0, 1.0, 0.3, seed=2, bdr=[(0, 0), (0, 0)], boundaries={0: (2, None)})
+    gm = meshio.build_general_mesh(2, 2, _file_corners(orig), _corner_xyz(orig), _bdr(orig), {"wall": 1})
+    fine = meshio.refine_general(meshio.refine_general(gm))
+    assert fine.num_elements == 16 * orig.num_elements
+    face_tables_consistent(fine)
+    _, w = gll_nodes(3)
+    area = lambda mm: float(np.sum(oracle_J(mm) * np.tile(np.outer(w, w).reshape(-1), mm.num_elements)))
+    assert abs(area(fine) - area(gm)) < 1e-12
+    oracle.Oracle(fine, compat=0, parabolic=0)
+
+
+def _file_corners(m):
+    gorder = [sum(b << d for d, b in enumerate(bits)) for bits in meshio._CORNER_BITS[m.dim]]
+    return np.asarray(m.corners)[:, gorder]
+
+
+def _corner_xyz(m):
+    dim, Np = m.dim, m.Np
+    X = np.asarray(m.coords).reshape(dim, m.num_elements, m.ndof)
+    gorder = [sum(b << d for d, b in enumerate(bits)) for bits in meshio._CORNER_BITS[dim]]
+    lexc = [sum(((c >> q) & 1) * (Np - 1) * Np ** q for q in range(dim)) for c in gorder]
+    return np.transpose(X[:, :, lexc], (1, 2, 0))
+
+
+def _bdr(m):
+    from prandtl_b200.geometry import face_corner_slots
+    return {frozenset(int(v) for v in m.corners[e, face_corner_slots(m.dim, int(f))]): int(-m.nbr[e, f])
+            for e, f in zip(*np.nonzero(m.nbr < 0))}
+
+
+def oracle_J(m):
+    """det of the Jacobian at every node (order-2 LGL derivative of the coordinates)."""
+    from prandtl_b200.mesh import gll_nodes as g
+    Np = m.Np
+    x1, _ = g(Np)
+    D = np.array([[_lagrange_deriv(x1, l, x1[i]) for l in range(Np)] for i in range(Np)])
+    X = np.asarray(m.coords).reshape(2, m.num_elements, Np, Np)      # [k, e, j, i]
+    dxi = np.einsum("il,kejl->keji", D, X)
+    deta = np.einsum("jl,keli->keji", D, X)
+    return (dxi[0] * deta[1] - dxi[1] * deta[0]).reshape(-1)
+
+
+def _lagrange_deriv(x, l, t):
+    s = 0.0
+    for m_ in range(len(x)):
+        if m_ == l:
+            continue
+        p = 1.0 / (x[l] - x[m_])
+        for q in range(len(x)):
+            if q != l and q != m_:
+                p *= (t - x[q]) / (x[l] - x[q])
+        s += p
+    return s
+
+
+def test_reference_general_meshes():
+    """The graded forward-facing step (ser_ref_levels = 1), the 15-degree ramp
+    and the unstructured ramjet read as general-geometry meshes: conforming
+    face tables and, with every boundary given the free stream, a uniform
+    state has a right-hand side of rounding size (free-stream preservation)."""
+    import oracle
+    for rel, refine, ne, names in (
+            ("Euler/2D/ForwardFacingStep/ForwardFacingStep.msh", 1, 13600, {"left", "right", "top", "bottom"}),
+            ("Euler/2D/Ramp/Ramp15deg_v2.msh", 0, 4802, {"inlet", "outlet", "axis", "ramp", "top"}),
+            ("Euler/2D/Nagashima_Ramjet/TR0/Nagashima_TR0_11kQuad_v2.msh", 0, 10856,
+             {"inlet", "outlet", "axis", "center-body", "cowl-inner", "cowl-outer", "valve"})):
+        m = meshio.read_mesh(ref_file(rel), 1, refine=refine)
+        assert m.coords is not None and m.num_elements == ne and set(m.boundary_names) == names
+        face_tables_consistent(m)
+        state = [1.4, 4.2, 0.3, 8.8]
+        m.boundaries = {b: (3, state) for b in m.boundary_names.values()}
+        nn = m.num_nodes
+        u = np.repeat(np.array(state), nn)
+        r = oracle.Oracle(m, compat=0, parabolic=0).rhs(u)
+        assert np.abs(r).max() < 1e-9 * np.abs(u).max() / min(m.h)
+
+
+def fixture_mesh(case, order):
+    """A reference mesh from its fixture (tests/golden/make_mesh_fixtures.py),
+    refined as its configuration says (the step: ser_ref_levels = 1)."""
+    z = np.load(os.path.join(os.path.dirname(__file__), "golden", f"mesh_{case}.npz"))
+    bdr = {frozenset(int(v) for v in row): int(a) for row, a in zip(z["bverts"], z["battr"])}
+    names = {str(k): int(v) for k, v in zip(z["name_keys"], z["name_vals"])}
+    m = meshio.build_general_mesh(int(z["dim"]), order, z["verts"].astype(np.int64), z["coords"], bdr, names,
+                                  z["attrs"])
+    return meshio.refine_general(m) if case == "ffs" else m
+
+
+def test_mesh_fixtures_match_files():
+    """The fixtures hold what the reader parses from the reference's files."""
+    for case, rel, refine in (("ffs", "Euler/2D/ForwardFacingStep/ForwardFacingStep.msh", 1),
+                              ("ramp", "Euler/2D/Ramp/Ramp15deg_v2.msh", 0),
+                              ("ramjet", "Euler/2D/Nagashima_Ramjet/TR0/Nagashima_TR0_11kQuad_v2.msh", 0)):
+        a = meshio.read_mesh(ref_file(rel), 2, refine=refine)
+        b = fixture_mesh(case, 2)
+        assert np.array_equal(a.coords, b.coords) and np.array_equal(a.nbr, b.nbr)
+        assert np.array_equal(a.face_orient, b.face_orient) and a.boundary_names == b.boundary_names
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("compat", [0, 1])
+@pytest.mark.parametrize("case", ["ffs", "ramp", "ramjet"])
+def test_gpu_reference_general_meshes_match_oracle(case, compat, cuda_device):
+    """The graded forward-facing step, the ramp and the unstructured ramjet at
+    N = 3 with Mach-3 inflow, outflow, slip walls (and the ramp's and
+    ramjet's axis as a symmetry plane): right-hand side and the three stages
+    of an SSP-RK3 step, GPU against the oracle."""
+    import oracle
+    import torch
+    m = fixture_mesh(case, 3)
+    free = [1.4, 4.2, 0.0, 1.0 / 0.4 + 0.5 * 1.4 * 9.0]
+    kinds = {"left": 1, "inlet": 1, "right": 2, "outlet": 2, "axis": 5}
+    m.boundaries = {b: ((kinds[nm], free) if kinds.get(nm) == 1 else (kinds.get(nm, 4), None))
+                    for nm, b in m.boundary_names.items()}
+    x = m.node_coords()
+    L = max(m.hi[0] - m.lo[0], m.hi[1] - m.lo[1])
+    s = np.sin(7 * x[0] / L) * np.cos(5 * x[1] / L)
+    u = np.concatenate([1.4 * (1 + 0.1 * s), 4.2 * (1 + 0.05 * s), 0.3 * s, free[3] * (1 + 0.02 * s)])
+    kw = dict(compat=compat, parabolic=0)
+    orc = oracle.Oracle(m, **kw)
+    want = orc.rhs(u)
+    op = pb.DGSEMOperator(m, **kw)
+    xd = torch.from_numpy(u).to(cuda_device)
+    out = torch.empty_like(xd)
+    op.Mult(xd, out)
+    fma = oracle.Oracle(m, fma=True, **kw).rhs(u)
+    rel_err = np.abs(out.cpu().numpy() - want).max() / np.abs(want).max()
+    floor = np.abs(fma - want).max() / np.abs(want).max()
+    assert rel_err < max(1e-12, 4 * floor)
+    dt = op.cfl_dt(0.3)
+    us = u
+    for stage in range(3):
+        w = orc.rk_stage(stage, dt, u, us)
+        o = torch.empty_like(xd)
+        op.rk_stage(stage, dt, xd, torch.from_numpy(us).to(cuda_device), o)
+        assert np.abs(o.cpu().numpy() - w).max() / np.abs(w).max() < 1e-12
+        us = w
     assert op.check() == 0
