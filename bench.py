@@ -53,6 +53,8 @@ def parse():
     ap.add_argument("--e2e-steps", type=int, default=10)
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--case", default="all", choices=["all", "geometry"],
+                    help="geometry: only the general-geometry measurements (one JSON object, for profiling)")
     ap.add_argument("--no-adjoint", action="store_true", help="skip the adjoint cost measurement")
     ap.add_argument("--compat", type=int, default=0, choices=[0, 1],
                     help="1: the reference-value operator (diverges on Taylor-Green after a few dozen steps)")
@@ -386,6 +388,7 @@ def run_ours(args):
     if args.sweep_steps > 0 and world == 1:
         out["filter_case"] = run_filter_case(args, dev)
         out["boundary_case"] = run_boundary_case(args, dev)
+        out["geometry_case"] = run_geometry_case(args, dev)
     if rank == 0 and world == 1 and not args.no_cpu:
         out["cpu_baseline"] = cpu_baseline(mesh, u0, params, args.cpu_seconds)
     if rank == 0:
@@ -646,6 +649,72 @@ def run_boundary_case(args, dev):
             "path": "pdg_rk3_steps (graph-replayed steps)"}
 
 
+def _timed_steps(op, x, dt, warmup, steps):
+    import torch
+    op.rk3_step(x, dt, nsteps=warmup, graph=True)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    op.rk3_step(x, dt, nsteps=steps, graph=True)
+    e1.record()
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1) / steps
+
+
+def run_geometry_case(args, dev):
+    """General geometry (geo_rhs_kernel, Euler, fixed operator, blending on):
+    a curved 3D mesh (the Taylor-Green box 32^3, N = 3, its nodes moved by a
+    smooth periodic field) and an unstructured-orientation 2D mesh (128^2
+    bilinear elements with randomly moved vertices, every other element's
+    frame rotated, N = 4, Kelvin-Helmholtz state): graph-replayed SSP-RK3
+    steps, each beside the box kernels on the same element count.  Roofline
+    of geo_rhs_kernel: per element and stage it must read the stage input
+    and (stages 1 and 2) the RK base state, write the output, and read its
+    metric terms (J and dim^2 adjugate entries per node) and face tables
+    (dim normal components and one node index per face node); one launch per
+    stage, so the launch time is taken as a third of the step."""
+    import torch
+
+    import prandtl_b200 as pb
+    from prandtl_b200 import geometry as G
+    hbm, kind = measured_peaks()
+    out = {}
+    for name, dim, order, n in (("curved_tgv_32^3_N3", 3, 3, 32), ("unstructured_kh_128^2_N4", 2, 4, 128)):
+        if dim == 3:
+            box = periodic_box(3, order, n, 0.0, 2 * np.pi)
+            g = G.warped(box, 0.02)
+            u = cases.taylor_green(g)
+            ub = cases.taylor_green(box)
+        else:
+            box = periodic_box(2, order, n, -1.0, 1.0)
+            g = G.rotate_frames(G.perturbed_box(2, order, n, -1.0, 1.0, 0.2, seed=1),
+                                range(0, n * n, 2), seed=2)
+            u = cases.kelvin_helmholtz(g)
+            ub = cases.kelvin_helmholtz(box)
+        op = pb.DGSEMOperator(g, parabolic=0, compat=0)
+        x = torch.from_numpy(u).to(dev)
+        op.Mult(x, torch.empty_like(x))
+        dt = op.cfl_dt(0.3)
+        ms = _timed_steps(op, x, dt, args.warmup, 20)
+        opb = pb.DGSEMOperator(box, parabolic=0, compat=0)
+        xb = torch.from_numpy(ub).to(dev)
+        opb.Mult(xb, torch.empty_like(xb))
+        ms_box = _timed_steps(opb, xb, opb.cfl_dt(0.3), args.warmup, 20)
+        op.check()
+        nv, nd = dim + 2, (order + 1) ** dim
+        nfn = (order + 1) ** (dim - 1)
+        per_el = 8 * (nv * nd * (2 + 2 / 3) + (1 + dim * dim) * nd + 2 * dim * nfn * dim) + 4 * 2 * dim * nfn
+        bytes_stage = per_el * g.num_elements
+        stage_s = ms / 3 * 1e-3
+        out[name] = {"vdofs": g.size, "steps": 20, "ms_per_step": ms, "value": g.size * 3 / (ms * 1e-3),
+                     "unit": UNIT, "box_mesh_ms_per_step": ms_box,
+                     "roofline": {"bound": "hbm", "achieved": bytes_stage / stage_s / 1e9, "peak": hbm,
+                                  "unit": "GB/s", "frac": bytes_stage / stage_s / 1e9 / hbm,
+                                  "bytes_per_stage": bytes_stage, "peak_kind": kind},
+                     "path": "pdg_set_geometry + pdg_rk3_steps (graph-replayed steps)"}
+    return out
+
+
 def _ref_worker(payload):
     """One reference process: SSP-RK3 steps of its own TGV block, timed."""
     n_el, order, steps, seconds = payload
@@ -729,6 +798,9 @@ def main():
     COMPAT = args.compat
     if args.impl == "reference":
         run_reference(args)
+    elif args.case == "geometry":
+        import torch
+        print(json.dumps({"geometry_case": run_geometry_case(args, torch.device("cuda", 0))}), flush=True)
     else:
         run_ours(args)
 

@@ -486,8 +486,16 @@ __device__ __forceinline__ void geo_tile(const KParams &P, const double *c, doub
     __syncwarp();
 }
 
+// Resident 4-warp blocks the register budget must allow (3D N = 3).
+#ifndef PDG_GEO3_MIN_BLOCKS
+#define PDG_GEO3_MIN_BLOCKS 4
+#endif
+template <int DIM, int N> struct GeoOccupancy {
+    static constexpr int min_blocks = (DIM == 3 && N == 3) ? PDG_GEO3_MIN_BLOCKS : 1;
+};
+
 template <int DIM, int N>
-__global__ void __launch_bounds__(128) geo_rhs_kernel(const KParams P)
+__global__ void __launch_bounds__(128, GeoOccupancy<DIM, N>::min_blocks) geo_rhs_kernel(const KParams P)
 {
     using S = Shape<DIM, N>;
     constexpr int Np = S::Np, L = S::L, EPW = S::EPW;
