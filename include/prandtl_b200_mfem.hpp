@@ -67,6 +67,16 @@ public:
         check_status(pdg_set_boundary(ctx_, index, type, data.Size() ? data.GetData() : nullptr), ctx_,
                      "pdg_set_boundary");
     }
+    // The mesh's general geometry (skewed, graded, curved or unstructured
+    // elements): `nodes` holds the DG nodes' coordinates in the state's
+    // byNODES layout (dim components; e.g. an L2 Gauss-Lobatto vector space
+    // of the operator's order with the identity projected onto it),
+    // `face_orient` one code per element face as pdg_set_geometry takes them
+    // (null: opposite faces, aligned axes).  Euler only; before the first Mult.
+    void SetGeometry(const mfem::Vector &nodes, const int32_t *face_orient)
+    {
+        check_status(pdg_set_geometry(ctx_, nodes.GetData(), face_orient), ctx_, "pdg_set_geometry");
+    }
     pdg_ctx *context() const { return ctx_; }
 
 private:
