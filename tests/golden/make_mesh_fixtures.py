@@ -3,8 +3,9 @@ coordinates and boundary elements parsed from three of the reference's Gmsh
 files (TestCases/Euler/2D/ForwardFacingStep/ForwardFacingStep.msh,
 Ramp/Ramp15deg_v2.msh, Nagashima_Ramjet/TR0/Nagashima_TR0_11kQuad_v2.msh),
 so that the GPU tests can build those meshes where the reference tree is
-absent.  Run here, where the tree is:  python tests/golden/make_mesh_fixtures.py
-[reference tree, default /root/reference].
+absent.  Run where the tree is:  python tests/golden/make_mesh_fixtures.py
+[reference tree] (else PRANDTL_REFERENCE, else where oracle/build_ref.sh found
+the tree, recorded in oracle/_ref/REFERENCE_TREE).
 """
 import os
 import sys
@@ -24,7 +25,11 @@ FILES = {
 
 
 def main():
-    ref = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    rec = os.path.join(HERE, "..", "..", "oracle", "_ref", "REFERENCE_TREE")
+    ref = (sys.argv[1] if len(sys.argv) > 1 else os.environ.get("PRANDTL_REFERENCE")
+           or (open(rec).read().strip() if os.path.exists(rec) else ""))
+    if not ref or not os.path.isdir(ref):
+        sys.exit("reference tree not found (pass it, or set PRANDTL_REFERENCE)")
     for name, rel in FILES.items():
         with open(os.path.join(ref, rel)) as f:
             p = meshio._parse_gmsh(f.read())
