@@ -712,7 +712,33 @@ def run_geometry_case(args, dev):
                                   "unit": "GB/s", "frac": bytes_stage / stage_s / 1e9 / hbm,
                                   "bytes_per_stage": bytes_stage, "peak_kind": kind},
                      "path": "pdg_set_geometry + pdg_rk3_steps (graph-replayed steps)"}
+        out[name]["cpu_baseline"] = _geometry_reference_sample(dim, order)
     return out
+
+
+def _geometry_reference_sample(dim, order):
+    """The reference's own integrators (oracle/_ref, compiled against the
+    stand-in MFEM header with a nodal element transformation) on one host
+    core: one right-hand side of a smaller mesh of the same kind (3D: the
+    curved box at 8^3; 2D: the perturbed, frame-rotated box at 32^2), as
+    DOF-stage updates per second."""
+    import oracle
+    from prandtl_b200 import geometry as G
+    if not oracle.ref_available(False):
+        return {"unavailable": "oracle/_ref/libref_euler.so not built (needs the reference tree)"}
+    if dim == 3:
+        g = G.warped(periodic_box(3, order, 8, 0.0, 2 * np.pi), 0.02)
+        u = cases.taylor_green(g)
+        sample = "one RHS of the curved Taylor-Green box 8^3, N=3"
+    else:
+        g = G.rotate_frames(G.perturbed_box(2, order, 32, -1.0, 1.0, 0.2, seed=1), range(0, 32 * 32, 2), seed=2)
+        u = cases.kelvin_helmholtz(g)
+        sample = "one RHS of the perturbed, frame-rotated box 32^2, N=4"
+    r = oracle.Reference(g)
+    t0 = time.perf_counter()
+    r.rhs(u)
+    t = time.perf_counter() - t0
+    return {"value": g.size / t, "unit": UNIT, "cores": 1, "kind": "reference", "sample": sample}
 
 
 def _ref_worker(payload):
