@@ -1324,21 +1324,45 @@ static double fv_fluxes_geo(const Ctx &c, int64_t e, const double *el_u, double 
 
 // AssembleElementVector, Euler (DGSEMIntegrator.cpp:224-433): two-point
 // fluxes with both nodes' metric rows, divided by the node's J.
-static double element_vector_geo(const Ctx &c, int64_t e, const double *el_u, double alpha, double *el_dudt)
+static double element_vector_geo(const Ctx &c, int64_t e, const double *el_u, const double *el_g, double alpha,
+                                 double *el_dudt)
 {
     const int Np = c.Np, nv = c.nv, dim = c.dim, nd = c.ndof;
     const int Npy = dim > 1 ? Np : 1, Npz = dim > 2 ? Np : 1;
     double lam = -1.0;
     for (int i = 0; i < nd * nv; i++) el_dudt[i] = 0.0;
     if (c.p.blending) lam = std::max(lam, fv_fluxes_geo(c, e, el_u, alpha, el_dudt));
+    // Navier-Stokes: contravariant viscous fluxes MultABt(adj, flux) per node
+    // (DGSEMIntegrator.cpp:616-640, 764-786), with the state of the member
+    // id1 in compat (the element's last node, Q1)
+    std::vector<double> Fv;  // [d][node][v]
+    if (c.p.parabolic) {
+        Fv.assign((size_t)dim * nd * nv, 0.0);
+        double flux[15], dq[15];
+        for (int n = 0; n < nd; n++) {
+            const int sn = c.p.compat ? nd - 1 : n;
+            for (int d = 0; d < dim; d++)
+                for (int v = 0; v < nv; v++) dq[d * nv + v] = el_g[((size_t)d * nd + n) * nv + v];
+            viscous_flux(dim, c.p.gamma, c.p.Pr, c.p.mu, el_u + sn * nv, dq, flux);
+            for (int a = 0; a < dim; a++) {
+                const double *adj = gadj_row(c, e, n, a);
+                for (int v = 0; v < nv; v++) {
+                    double acc = 0.0;
+                    for (int b = 0; b < dim; b++) acc += adj[b] * flux[v * dim + b];
+                    Fv[((size_t)a * nd + n) * nv + v] = acc;
+                }
+            }
+        }
+    }
     std::vector<double> Fs((size_t)dim * nd * Np * nv, 0.0);
     auto FS = [&](int d, int n, int m) -> double * { return &Fs[(((size_t)d * nd + n) * Np + m) * nv]; };
-    double f[5];
+    double f[5], g[5];
     for (int k = 0; k < Npz; k++)
         for (int j = 0; j < Npy; j++)
             for (int i = 0; i < Np; i++) {
                 const int id1 = (k * Npy + j) * Np + i;
                 const int pos[3] = {i, j, k};
+                for (int v = 0; v < nv; v++) g[v] = 0.0;
                 for (int d = 0; d < dim; d++) {
                     for (int v = 0; v < nv; v++) f[v] = 0.0;
                     std::memcpy(FS(d, id1, pos[d]), f, sizeof(double) * nv);
@@ -1347,7 +1371,11 @@ static double element_vector_geo(const Ctx &c, int64_t e, const double *el_u, do
                         lam = std::max(lam, volume_flux(dim, c.p.gamma, el_u + id1 * nv, el_u + id2 * nv,
                                                         gadj_row(c, e, id1, d), gadj_row(c, e, id2, d), f));
                         std::memcpy(FS(d, id1, m), f, sizeof(double) * nv);
-                        std::memcpy(FS(d, id2, pos[d]), f, sizeof(double) * nv);
+                        // the NS 3D path fills the z partner column with the
+                        // last y-direction flux g (DGSEMIntegrator.cpp:702, Q2)
+                        const double *fill = (d == 2 && c.p.parabolic && c.p.compat) ? g : f;
+                        std::memcpy(FS(d, id2, pos[d]), fill, sizeof(double) * nv);
+                        if (d == 1) std::memcpy(g, f, sizeof(double) * nv);
                     }
                 }
             }
@@ -1356,17 +1384,29 @@ static double element_vector_geo(const Ctx &c, int64_t e, const double *el_u, do
             for (int i = 0; i < Np; i++) {
                 const int id1 = (k * Npy + j) * Np + i;
                 const int pos[3] = {i, j, k};
-                double dU[5];
-                for (int v = 0; v < nv; v++) dU[v] = 0.0;
+                double dU[5], dUv[5];
+                for (int v = 0; v < nv; v++) dU[v] = dUv[v] = 0.0;
                 for (int d = 0; d < dim; d++)
                     for (int m = 0; m < Np; m++) {
                         const double *col = FS(d, id1, m);
                         const double a = c.Dhat2[pos[d] * Np + m];
                         for (int v = 0; v < nv; v++) dU[v] += a * col[v];
                     }
+                if (c.p.parabolic)
+                    for (int d = 0; d < dim; d++)
+                        for (int l = 0; l < Np; l++) {
+                            const int nl = line_node(c, d, i, j, k, l);
+                            const double a = c.Dhat[pos[d] * Np + l];
+                            for (int v = 0; v < nv; v++) {
+                                double t = Fv[((size_t)d * nd + nl) * nv + v];
+                                t *= a;
+                                dUv[v] += t;
+                            }
+                        }
                 for (int v = 0; v < nv; v++) {
                     double t = -dU[v];
                     if (c.p.blending) t *= (1.0 - alpha);
+                    if (c.p.parabolic) t = t + dUv[v];
                     t /= gJ(c, e, id1);
                     el_dudt[id1 * nv + v] += t;
                 }
@@ -1398,11 +1438,53 @@ static double face_vector_geo(const Ctx &c, const double *u, int64_t a, int f, d
         }
         const double *row = gadj_row(c, a, n1, d);
         for (int k = 0; k < dim; k++) nor[k] = side ? row[k] : -row[k];
-        lam = std::max(lam, face_flux(dim, c.p.gamma, c.p.compat, c.p.face_dissipation, s1, s2, nor, flux));
+        if (c.p.parabolic && c.p.compat) {
+            // velocities in the momentum slots, as the NS face integrator
+            // leaves them (DGSEMIntegrator.cpp:467-481)
+            double t1[5], t2[5];
+            for (int v = 0; v < nv; v++) { t1[v] = s1[v]; t2[v] = s2[v]; }
+            for (int q = 0; q < dim; q++) { t1[1 + q] = s1[1 + q] / s1[0]; t2[1 + q] = s2[1 + q] / s2[0]; }
+            lam = std::max(lam, face_flux(dim, c.p.gamma, c.p.compat, c.p.face_dissipation, t1, t2, nor, flux));
+        } else {
+            lam = std::max(lam, face_flux(dim, c.p.gamma, c.p.compat, c.p.face_dissipation, s1, s2, nor, flux));
+        }
+        double dU1[5], dU2[5];
+        for (int v = 0; v < nv; v++) {
+            dU2[v] = flux[v];
+            dU1[v] = -flux[v];
+        }
+        if (c.p.parabolic) {
+            // central viscous flux of both sides' states and gradients
+            // (DGSEMIntegrator.cpp:435-549)
+            double dq1[15], dq2[15], fm1[15], fm2[15];
+            for (int q = 0; q < dim; q++)
+                for (int v = 0; v < nv; v++) {
+                    dq1[q * nv + v] = c.grads[(size_t)q * c.size + idx(c, v, a, n1)];
+                    dq2[q * nv + v] = c.grads[(size_t)q * c.size + idx(c, v, b, n2)];
+                }
+            double u1[5], u2[5];
+            for (int v = 0; v < nv; v++) {
+                u1[v] = u[idx(c, v, a, n1)];
+                u2[v] = u[idx(c, v, b, n2)];
+            }
+            viscous_flux(dim, c.p.gamma, c.p.Pr, c.p.mu, u1, dq1, fm1);
+            viscous_flux(dim, c.p.gamma, c.p.Pr, c.p.mu, u2, dq2, fm2);
+            for (int v = 0; v < nv; v++) {
+                double fn = 0.0;
+                for (int q = 0; q < dim; q++) {
+                    double avg = fm1[v * dim + q];
+                    avg += fm2[v * dim + q];
+                    avg *= 0.5;
+                    fn += avg * nor[q];
+                }
+                dU1[v] += fn;
+                dU2[v] -= fn;
+            }
+        }
         const double sc1 = 1.0 / (c.w[0] * gJ(c, a, n1)), sc2 = 1.0 / (c.w[0] * gJ(c, b, n2));
         for (int v = 0; v < nv; v++) {
-            buf[t * nv + v] = sc1 * (-flux[v]);
-            buf[(size_t)nfn * nv + t * nv + v] = sc2 * flux[v];
+            buf[t * nv + v] = sc1 * dU1[v];
+            buf[(size_t)nfn * nv + t * nv + v] = sc2 * dU2[v];
         }
     }
     return lam;
@@ -1422,10 +1504,38 @@ static double bdr_face_vector_geo(const Ctx &c, const double *u, int64_t e, int 
         for (int k = 0; k < dim; k++) nor[k] = side ? row[k] : -row[k];
         lam = std::max(lam, bdr_flux(c, b, s1, nor, flux));
         const double scale = 1.0 / (c.w[0] * gJ(c, e, n));
-        for (int v = 0; v < nv; v++) out[t * nv + v] = scale * (-flux[v]);
+        double dU[5];
+        for (int v = 0; v < nv; v++) dU[v] = -flux[v];
+        const int type = (int)c.bc[b][0];
+        if (c.p.parabolic && (type == 2 || type == 10 || type == 11 || type == 8)) {
+            // ComputeBdrFaceViscousFlux with the node's own normal, as on box meshes
+            double dq[15], fm[15], fn[5];
+            for (int q = 0; q < dim; q++)
+                for (int v = 0; v < nv; v++) dq[q * nv + v] = c.grads[(size_t)q * c.size + idx(c, v, e, n)];
+            if (type == 8) {
+                double so[5], fl[5];
+                bdr_flux(c, b, s1, nor, fl, so);
+                viscous_flux(dim, c.p.gamma, c.p.Pr, c.p.mu, so, dq, fm);
+            } else {
+                viscous_flux(dim, c.p.gamma, c.p.Pr, c.p.mu, s1, dq, fm);
+            }
+            for (int v = 0; v < nv; v++) {
+                fn[v] = 0.0;
+                for (int q = 0; q < dim; q++) fn[v] += fm[v * dim + q] * nor[q];
+            }
+            if (type == 10) {
+                double en = 0.0;
+                for (int q = 0; q < dim; q++) en += c.bc[b][1 + q] * fn[1 + q];
+                fn[nv - 1] = en + 0.0;
+            }
+            for (int v = 0; v < nv; v++) dU[v] += fn[v];
+        }
+        for (int v = 0; v < nv; v++) out[t * nv + v] = scale * dU[v];
     }
     return lam;
 }
+
+static void lifting_geo(Ctx &c, const double *u);
 
 static void rhs_geo(Ctx &c, const double *u, double *dudt)
 {
@@ -1435,6 +1545,8 @@ static void rhs_geo(Ctx &c, const double *u, double *dudt)
         std::fill(c.alpha.begin(), c.alpha.end(), 0.0);
         std::fill(c.eta.begin(), c.eta.end(), 0.0);
     }
+    if (c.p.parabolic) lifting_geo(c, u);
+    const double *G = c.grads.data();
     double lam = -1.0;
     const size_t fstride = (size_t)2 * nfn * nv;
 #pragma omp parallel for schedule(static) reduction(max : lam)
@@ -1444,10 +1556,17 @@ static void rhs_geo(Ctx &c, const double *u, double *dudt)
                 lam = std::max(lam, face_vector_geo(c, u, e, f, &c.facebuf[((size_t)e * nf + f) * fstride]));
 #pragma omp parallel for schedule(static) reduction(max : lam)
     for (int64_t e = 0; e < c.ne; e++) {
-        std::vector<double> el_u(nd * nv), el_d(nd * nv), bface((size_t)nfn * nv);
+        std::vector<double> el_u(nd * nv), el_d(nd * nv), bface((size_t)nfn * nv), el_g;
         for (int n = 0; n < nd; n++)
             for (int v = 0; v < nv; v++) el_u[n * nv + v] = u[idx(c, v, e, n)];
-        lam = std::max(lam, element_vector_geo(c, e, el_u.data(), c.alpha[e], el_d.data()));
+        if (c.p.parabolic) {
+            el_g.resize((size_t)dim * nd * nv);
+            for (int d = 0; d < dim; d++)
+                for (int n = 0; n < nd; n++)
+                    for (int v = 0; v < nv; v++)
+                        el_g[((size_t)d * nd + n) * nv + v] = G[(size_t)d * c.size + idx(c, v, e, n)];
+        }
+        lam = std::max(lam, element_vector_geo(c, e, el_u.data(), el_g.data(), c.alpha[e], el_d.data()));
         for (int n = 0; n < nd; n++)
             for (int v = 0; v < nv; v++) dudt[idx(c, v, e, n)] = 0.0 + el_d[n * nv + v];
         for (int f = 0; f < nf; f++) {
@@ -1481,6 +1600,98 @@ static void rhs_geo(Ctx &c, const double *u, double *dudt)
     }
     c.last_rhs_speed = lam;
     c.max_char_speed = std::max(c.max_char_speed, lam);
+}
+
+// BR1 lifting on a general mesh (LiftingBR1.cpp:10-115 faces, :156-272
+// elements, :311-407 boundary faces): per node the reference-direction
+// derivatives of the entropy variables times the adjugate (mfem::Mult) times
+// 1/J, each face adding 0.5 (w2 - w1) n_k / (w0 J) to both sides' gradient k
+// with element 1's normal, then EntropyGrad2PrimGrad per direction.
+static void lifting_geo(Ctx &c, const double *u)
+{
+    const int nv = c.nv, dim = c.dim, nd = c.ndof, Np = c.Np, nfn = nd / Np, nf = 2 * dim;
+#pragma omp parallel for schedule(static)
+    for (int64_t e = 0; e < c.ne; e++) {
+        double s[5], w[5];
+        for (int n = 0; n < nd; n++) {
+            for (int v = 0; v < nv; v++) s[v] = u[idx(c, v, e, n)];
+            conserv2entropy(dim, c.p.gamma, s, w);
+            for (int v = 0; v < nv; v++) c.went[idx(c, v, e, n)] = w[v];
+        }
+    }
+    const double *W = c.went.data();
+    double *G = c.grads.data();
+#pragma omp parallel for schedule(static)
+    for (int64_t e = 0; e < c.ne; e++) {
+        for (int n = 0; n < nd; n++) {
+            const int pos[3] = {n % Np, (n / Np) % Np, n / (Np * Np)};
+            double gr[5][3] = {};
+            for (int r = 0; r < dim; r++)
+                for (int v = 0; v < nv; v++) {
+                    double acc = 0.0;
+                    for (int l = 0; l < Np; l++) {
+                        double t = W[idx(c, v, e, line_node(c, r, pos[0], pos[1], pos[2], l))];
+                        t *= c.D[pos[r] * Np + l];
+                        acc += t;
+                    }
+                    gr[v][r] = acc;
+                }
+            const double ij = 1.0 / gJ(c, e, n);
+            for (int k = 0; k < dim; k++)
+                for (int v = 0; v < nv; v++) {
+                    double g = 0.0;
+                    for (int r = 0; r < dim; r++) g += gr[v][r] * gadj_row(c, e, n, r)[k];
+                    g *= ij;
+                    G[(size_t)k * c.size + idx(c, v, e, n)] = g;
+                }
+        }
+        for (int f = 0; f < nf; f++) {
+            const int d = f / 2, side = f % 2;
+            const int64_t nb = c.nbr[e * nf + f];
+            for (int t = 0; t < nfn; t++) {
+                const int n = face_node(c, d, side, t);
+                const double scale = 1.0 / (c.w[0] * gJ(c, e, n));
+                double fl[5], nor[3];
+                if (nb < 0) {
+                    double s1[5], w1[5];
+                    const double *row = gadj_row(c, e, n, d);
+                    for (int k = 0; k < dim; k++) nor[k] = side ? row[k] : -row[k];
+                    for (int v = 0; v < nv; v++) {
+                        s1[v] = u[idx(c, v, e, n)];
+                        w1[v] = W[idx(c, v, e, n)];
+                    }
+                    bdr_lifting_flux(c, (int)(-1 - nb), s1, w1, nor, fl);
+                } else {
+                    const int n2 = c.gnode[((size_t)e * nf + f) * nfn + t];
+                    const bool is1 = is_element1(c, e, f);
+                    const int f2 = c.gface[e * nf + f];
+                    const double *row = is1 ? gadj_row(c, e, n, d) : gadj_row(c, nb, n2, f2 / 2);
+                    const int sd = is1 ? side : f2 % 2;
+                    for (int k = 0; k < dim; k++) nor[k] = sd ? row[k] : -row[k];
+                    for (int v = 0; v < nv; v++) {
+                        const double w1 = is1 ? W[idx(c, v, e, n)] : W[idx(c, v, nb, n2)];
+                        const double w2 = is1 ? W[idx(c, v, nb, n2)] : W[idx(c, v, e, n)];
+                        fl[v] = 0.5 * (w2 - w1);
+                    }
+                }
+                for (int k = 0; k < dim; k++)
+                    for (int v = 0; v < nv; v++) {
+                        double fv = fl[v];
+                        fv *= nor[k];
+                        G[(size_t)k * c.size + idx(c, v, e, n)] += scale * fv;
+                    }
+            }
+        }
+        double s[5], g[5];
+        for (int n = 0; n < nd; n++) {
+            for (int v = 0; v < nv; v++) s[v] = u[idx(c, v, e, n)];
+            for (int d = 0; d < dim; d++) {
+                for (int v = 0; v < nv; v++) g[v] = G[(size_t)d * c.size + idx(c, v, e, n)];
+                entgrad2primgrad(dim, c.p.gamma, c.p.compat, s, g);
+                for (int v = 0; v < nv; v++) G[(size_t)d * c.size + idx(c, v, e, n)] = g[v];
+            }
+        }
+    }
 }
 
 static void rhs(Ctx &c, const double *u, double *dudt)
@@ -1811,7 +2022,6 @@ int orc_set_geometry(void *h, const double *x, const int32_t *face_orient)
 {
     Ctx &c = *(Ctx *)h;
     const int dim = c.dim, Np = c.Np, N = c.N, nd = c.ndof, nf = 2 * dim, nfn = nd / Np;
-    if (c.p.parabolic) return 1;
     c.gJ.assign((size_t)c.ne * nd, 0.0);
     c.gadj.assign((size_t)c.ne * nd * 9, 0.0);
     for (int64_t e = 0; e < c.ne; e++)

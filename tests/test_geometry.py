@@ -143,3 +143,45 @@ def test_oracle_rejects_inverted_elements():
     g.coords = X.reshape(2, -1)
     with pytest.raises(ValueError):
         oracle.Oracle(g, compat=0, parabolic=0)
+
+
+NS = dict(mu=0.01, Pr=0.71)
+GEO_BCS_NS_2D = {0: (1, [1.4, 0.42, 0.03, 2.6]), 1: (2, None), 2: (3, [1.3, 0.2, 0.0, 2.4]), 3: (2, None)}
+
+
+def ns_geometry_case(name):
+    """Navier-Stokes layouts: the periodic general meshes and a perturbed
+    channel with inflow, outflow and a prescribed state."""
+    if name == "boundary2d_ns":
+        return G.perturbed_box(2, 3, (5, 4), 0.0, 1.0, 0.3, seed=5, bdr=[(0, 1), (2, 3)], boundaries=GEO_BCS_NS_2D)
+    return geometry_case(name)
+
+
+NS_GEO_CASES = ["warped2d", "perturbed2d", "rotated2d", "warped3d", "perturbed3d", "rotated3d", "boundary2d_ns"]
+
+
+@pytest.mark.skipif(not oracle.ref_available(True), reason="oracle/_ref not built (reference tree absent)")
+@pytest.mark.parametrize("name", NS_GEO_CASES)
+def test_oracle_navier_stokes_matches_reference_on_general_geometry(name):
+    """The BR1 lifting with the adjugate at every node (LiftingBR1.cpp), the
+    contravariant viscous fluxes and the central viscous face fluxes, against
+    the reference's own NS build (reference-value operator: stale viscous
+    state, z-direction fill)."""
+    g = ns_geometry_case(name)
+    u = smooth_state(g, 11)
+    ref = oracle.Reference(g, parabolic=True, **NS)
+    want = ref.rhs(u)
+    orc = oracle.Oracle(g, compat=1, parabolic=1, **NS)
+    assert rel_maxnorm(orc.rhs(u), want) < REF_TOL
+    assert rel_maxnorm(orc.gradients(), ref.gradients()) < REF_TOL
+
+
+@pytest.mark.parametrize("dim,order,n", [(2, 3, (4, 5)), (3, 2, (3, 4, 3))])
+@pytest.mark.parametrize("compat", [0, 1])
+def test_oracle_navier_stokes_geometry_path_equals_box_path(dim, order, n, compat):
+    m = periodic_box(dim, order, n, 0.0, 1.0)
+    u = smooth_state(m, 3)
+    a = oracle.Oracle(m, compat=compat, parabolic=1, **NS)
+    b = oracle.Oracle(G.warped(m, 0.0), compat=compat, parabolic=1, **NS)
+    assert rel_maxnorm(b.rhs(u), a.rhs(u)) < 1e-13
+    assert rel_maxnorm(b.gradients(), a.gradients()) < 1e-13
