@@ -103,6 +103,7 @@ struct pdg_ctx {
     double *geo_d = nullptr;
     int32_t *fnode_d = nullptr;
     double *fnor_d = nullptr;
+    double *geo_grads = nullptr;  // Navier-Stokes: primitive gradients [d][v][node]
 };
 
 namespace {
@@ -338,7 +339,7 @@ bool kind_used(int kind, int dim, bool parabolic, int filter)
 {
     if (kind == KIND_FILTER_BOUNDS || kind == KIND_FILTER) return filter & 1;
     if (kind == KIND_POSITIVITY) return (filter & 2) != 0;
-    if (kind == KIND_GEO) return false;  // configured by pdg_set_geometry
+    if (kind == KIND_GEO || kind == KIND_GEO_LIFT || kind == KIND_GEO_NS) return false;  // configured by pdg_set_geometry
     if ((kind >= KIND_ADJ_RHS && kind <= KIND_ADJ_FACE_NS2) || kind == KIND_ADJ_BOUNDARY)
         return false;  // configured by the first pdg_rhs_vjp
     const bool ns_kind = kind == KIND_NS || kind == KIND_NS_FACES || kind == KIND_LIFT || kind == KIND_LIFT_FACE ||
@@ -421,6 +422,7 @@ KParams base_params(pdg_ctx *c)
     P.geo = c->geo_d;
     P.fnode = c->fnode_d;
     P.fnor = c->fnor_d;
+    P.geo_grads = c->geo_grads;
     return P;
 }
 
@@ -529,7 +531,20 @@ int evaluate(pdg_ctx *c, int stage, double dt, const double *un, const double *u
     P.dt = dt;
     c->last_stream = s;
     int r;
-    if (c->geo) return launch(c, KIND_GEO, P, s);  // general geometry: one kernel
+    if (c->geo) {
+        // general geometry: one kernel (Navier-Stokes: the lifting kernel first)
+        if (!c->p.parabolic) return launch(c, KIND_GEO, P, s);
+        for (int b = 0; b < PDG_MAX_BOUNDARIES; b++) {
+            const int t = (int)c->bc_host[b * BC_SLOT];
+            if ((c->bc_used >> b & 1u) && t != PDG_BC_SUPERSONIC_INFLOW && t != PDG_BC_SUPERSONIC_OUTFLOW &&
+                t != PDG_BC_SPECIFIED_STATE)
+                return fail(c, PDG_ERR_UNSUPPORTED,
+                            "boundary condition %d: Navier-Stokes on general geometry takes supersonic inflow, outflow "
+                            "and specified states", b);
+        }
+        if ((r = launch(c, KIND_GEO_LIFT, P, s))) return r;
+        return launch(c, KIND_GEO_NS, P, s);
+    }
     const bool element_faces = c->element_faces && !c->p.compat;
     if (c->p.parabolic) {
         if ((c->p.filter & 1) && stage >= 0 && (r = launch(c, KIND_FILTER_BOUNDS, P, s))) return r;
@@ -810,8 +825,9 @@ int pdg_set_geometry(pdg_ctx *c, const double *x, const int32_t *face_orient)
     if (!c) return PDG_ERR_ARG;
     if (!x) return fail(c, PDG_ERR_ARG, "pdg_set_geometry: null coordinates");
     if (c->geo) return fail(c, PDG_ERR_ARG, "pdg_set_geometry: the geometry is already set");
-    if (c->p.parabolic || c->p.filter)
-        return fail(c, PDG_ERR_UNSUPPORTED, "pdg_set_geometry: general geometry takes Euler without filter");
+    if (c->p.filter || (c->p.parabolic && c->p.compat))
+        return fail(c, PDG_ERR_UNSUPPORTED,
+                    "pdg_set_geometry: general geometry takes no filter, and Navier-Stokes with compat = 0");
     const int dim = c->dim, Np = c->Np, N = c->N, nd = c->ndof, nf = 2 * dim;
     const int nfn = dim == 2 ? Np : Np * Np;
     const int64_t ne = c->ne, nn = c->nnodes;
@@ -972,8 +988,13 @@ int pdg_set_geometry(pdg_ctx *c, const double *x, const int32_t *face_orient)
     CK(cudaMemcpy(c->geo_d, geo.data(), sizeof(double) * geo.size(), cudaMemcpyHostToDevice), "geometry upload");
     CK(cudaMemcpy(c->fnode_d, fnode.data(), sizeof(int32_t) * fnode.size(), cudaMemcpyHostToDevice), "geometry upload");
     CK(cudaMemcpy(c->fnor_d, fnor.data(), sizeof(double) * fnor.size(), cudaMemcpyHostToDevice), "geometry upload");
-    int r = configure_launch(c, KIND_GEO);
+    int r = configure_launch(c, c->p.parabolic ? KIND_GEO_NS : KIND_GEO);
     if (r) return r;
+    if (c->p.parabolic) {
+        if ((r = configure_launch(c, KIND_GEO_LIFT))) return r;
+        if (cudaMalloc(&c->geo_grads, sizeof(double) * dim * c->nv * nn) != cudaSuccess)
+            return fail(c, PDG_ERR_NOMEM, "pdg_set_geometry: allocation failed");
+    }
     cudaFree(c->fbuf);  // the box path's face buffer is not used
     c->fbuf = nullptr;
     c->hmin = hmin;
@@ -1006,6 +1027,7 @@ int pdg_destroy(pdg_ctx *c)
     cudaFree(c->geo_d);
     cudaFree(c->fnode_d);
     cudaFree(c->fnor_d);
+    cudaFree(c->geo_grads);
     if (c->graph_exec) cudaGraphExecDestroy(c->graph_exec);
     if (c->graph) cudaGraphDestroy(c->graph);
     if (c->cap) cudaStreamDestroy(c->cap);
@@ -1405,6 +1427,11 @@ int pdg_gradients(pdg_ctx *c, const double *u, double *grads, void *stream)
     c->last_stream = (cudaStream_t)stream;
     KParams P = base_params(c);
     P.out = nullptr;
+    if (c->geo) {  // general geometry: the lifting kernel writes the caller's buffer
+        P.u = u;
+        P.geo_grads = grads;
+        return launch(c, KIND_GEO_LIFT, P, (cudaStream_t)stream);
+    }
     return lift(c, P, u, grads, (cudaStream_t)stream);
 }
 

@@ -36,6 +36,12 @@ __device__ __forceinline__ void geo_row(const KParams &P, int64_t gnode, int r, 
     for (int k = 0; k < DIM; k++) m[k] = __ldg(P.geo + (int64_t)(1 + r * DIM + k) * P.nnodes + gnode);
 }
 __device__ __forceinline__ double geo_J(const KParams &P, int64_t gnode) { return __ldg(P.geo + gnode); }
+// Component c of metric row r of global node gnode.
+template <int DIM>
+__device__ __forceinline__ double geo_row1(const KParams &P, int64_t gnode, int r, int c)
+{
+    return __ldg(P.geo + (int64_t)(1 + r * DIM + c) * P.nnodes + gnode);
+}
 
 // Flux-differencing line tasks along direction d with per-node metrics: the
 // pair (a < b) of a line takes the metric mean (m_a + m_b) / 2 of both nodes'
@@ -354,11 +360,115 @@ __device__ __noinline__ double geo_bdr_flux(const KParams &P, int b, const doubl
     return fmax(qa.lam, qb.lam);
 }
 
+// Element slot of geo_rhs_kernel: primitives and accumulator; Navier-Stokes
+// adds the contravariant viscous fluxes [d][row][node] and their divergence
+// [row][node] (rows: momenta and energy).
+template <int DIM, int N, bool NS> struct GeoShape {
+    using S = Shape<DIM, N>;
+    static constexpr int FV = S::EL_RHS_FB;                         // offset of the viscous fluxes
+    static constexpr int DV = FV + DIM * (S::NV - 1) * S::NS_;      // offset of their divergence
+    static constexpr int EL = NS ? DV + (S::NV - 1) * S::NS_ : S::EL_RHS_FB;
+};
+
+// The viscous flux (NavierStokesFlux::ComputeViscousFlux, constant mu) of a
+// state and its primitive gradients gr[k][v] (k: physical direction):
+// fm[q][r], column q, rows r = momenta and energy.
+template <int DIM>
+__device__ __forceinline__ void viscous_flux_cols(const KParams &P, const double *s, const double (*gr)[DIM + 2],
+                                                  double (*fm)[DIM + 1])
+{
+    Prim<DIM> q = make_prim<DIM>(s, P.gamma, P.gm1);
+    auto G = [&](int d, int v) { return gr[d][v]; };
+#pragma unroll
+    for (int c = 0; c < DIM; c++) viscous_col<DIM>(q, G, c, P.gm1inv, P.mu, P.lambda_k, fm[c]);
+}
+
+// Primitive gradients of global node g (geo_lift_kernel's output).
+template <int DIM>
+__device__ __forceinline__ void load_grads(const KParams &P, int64_t g, double (*gr)[DIM + 2])
+{
+#pragma unroll
+    for (int k = 0; k < DIM; k++)
+#pragma unroll
+        for (int v = 0; v < DIM + 2; v++) gr[k][v] = __ldg(P.geo_grads + ((int64_t)k * (DIM + 2) + v) * P.nnodes + g);
+}
+
+// Contravariant viscous fluxes of the element's nodes (MultABt(adj, flux),
+// DGSEMIntegrator.cpp:616-640, 764-786) into the slot, then their
+// divergence along each direction's lines, dUv(l) = sum_m Dhat(l, m) F_d(m).
+template <int DIM, int N>
+__device__ __forceinline__ void viscous_volume_geo(const KParams &P, double *fv, double *dv, const double *c, int gl,
+                                                   int64_t e, bool valid)
+{
+    using S = Shape<DIM, N>;
+    constexpr int Np = S::Np, NDOF = S::NDOF, NV = S::NV, NR = NV - 1, ST = S::NS_;
+#pragma unroll 1
+    for (int k = 0; k < S::NPL; k++) {
+        const int n = gl + k * S::L;
+        if (n < NDOF) {
+            double sv[NV], gr[DIM][DIM + 2], fm[DIM][DIM + 1];
+            const int64_t g = e * NDOF + n;
+#pragma unroll
+            for (int v = 0; v < NV; v++)
+                sv[v] = valid ? __ldg(P.u + (int64_t)v * P.nnodes + g) : (v == 0 ? 1.0 : (v == NV - 1 ? P.gm1inv : 0.0));
+            if (valid) load_grads<DIM>(P, g, gr);
+            else
+#pragma unroll
+                for (int a = 0; a < DIM; a++)
+#pragma unroll
+                    for (int v = 0; v < NV; v++) gr[a][v] = 0.0;
+            viscous_flux_cols<DIM>(P, sv, gr, fm);
+            const int m = sp<DIM, Np>(n);
+#pragma unroll
+            for (int a = 0; a < DIM; a++) {
+                double adj[DIM];
+#pragma unroll
+                for (int b = 0; b < DIM; b++) adj[b] = valid ? geo_row1<DIM>(P, g, a, b) : (a == b ? 1.0 : 0.0);
+#pragma unroll
+                for (int r = 0; r < NR; r++) {
+                    double acc = 0.0;
+#pragma unroll
+                    for (int b = 0; b < DIM; b++) acc += adj[b] * fm[b][r];
+                    fv[(a * NR + r) * ST + m] = acc;
+                }
+            }
+        }
+    }
+    __syncwarp();
+    const double *Dh = C_DHAT(c);
+#pragma unroll 1
+    for (int d = 0; d < DIM; d++) {
+#pragma unroll 1
+        for (int rr = 0; rr < S::LPL; rr++) {
+            const int line = gl + rr * S::L;
+            if (line < S::NFN) {
+                double x[Np][NR];
+#pragma unroll
+                for (int l = 0; l < Np; l++)
+#pragma unroll
+                    for (int r = 0; r < NR; r++) x[l][r] = fv[(d * NR + r) * ST + sp<DIM, Np>(line_node_rt<DIM, Np>(d, line, l))];
+#pragma unroll
+                for (int l = 0; l < Np; l++) {
+                    const int m = sp<DIM, Np>(line_node_rt<DIM, Np>(d, line, l));
+#pragma unroll
+                    for (int r = 0; r < NR; r++) {
+                        double t = d == 0 ? 0.0 : dv[r * ST + m];
+#pragma unroll
+                        for (int j = 0; j < Np; j++) t += x[j][r] * Dh[l * Np + j];
+                        dv[r * ST + m] = t;
+                    }
+                }
+            }
+        }
+        __syncwarp();
+    }
+}
+
 // One warp tile of geo_rhs_kernel: EPW elements from e_base, one lane group
 // each.  Volume terms into acc (flux differencing scaled by -(1 - alpha) / J
 // per node, then the subcell FV terms), the stage combine, the face terms of
 // every face node of the element (times the stage factor), the store.
-template <int DIM, int N>
+template <int DIM, int N, bool NS>
 __device__ __forceinline__ void geo_tile(const KParams &P, const double *c, double *pr, int64_t e_base, int grp, int gl,
                                          bool lane_used, unsigned int &flags, double &lam)
 {
@@ -388,7 +498,9 @@ __device__ __forceinline__ void geo_tile(const KParams &P, const double *c, doub
 #pragma unroll 1
         for (int d = 0; d < DIM; d++) ec_lines_geo<DIM, N>(P, d, pr, acc, c, gl, e, valid);
     }
-    // -(1 - alpha) dU / J at every node (DGSEMIntegrator.cpp:423-431)
+    double *dv = pr + GeoShape<DIM, N, NS>::DV;
+    if (NS && lane_used) viscous_volume_geo<DIM, N>(P, pr + GeoShape<DIM, N, NS>::FV, dv, c, gl, e, valid);
+    // (-(1 - alpha) dU [+ dUv]) / J at every node (DGSEMIntegrator.cpp:423-431, 840-860)
     if (lane_used) {
 #pragma unroll
         for (int k = 0; k < S::NPL; k++) {
@@ -399,6 +511,7 @@ __device__ __forceinline__ void geo_tile(const KParams &P, const double *c, doub
                 for (int v = 0; v < NV; v++) {
                     double t = -acc[v * ST + sp<DIM, Np>(n)];
                     t *= (1.0 - alpha);
+                    if (NS && v > 0) t = t + dv[(v - 1) * ST + sp<DIM, Np>(n)];
                     acc[v * ST + sp<DIM, Np>(n)] = t / J;
                 }
             }
@@ -443,7 +556,9 @@ __device__ __forceinline__ void geo_tile(const KParams &P, const double *c, doub
 #pragma unroll
                 for (int v = 0; v < NV; v++) s[v] = __ldg(P.u + (int64_t)v * nn + e * NDOF + n);
                 const double J = geo_J(P, e * NDOF + n);
-                double sgn;
+                double sgn, fnv[NV];  // fnv: the central viscous flux . n (Navier-Stokes)
+#pragma unroll
+                for (int v = 0; v < NV; v++) fnv[v] = 0.0;
                 if (other >= 0) {
                     const int n2 = __ldg(P.fnode + fi);
                     double o[NV];
@@ -460,15 +575,52 @@ __device__ __forceinline__ void geo_tile(const KParams &P, const double *c, doub
                     face_flux_n<DIM>(qa, qb, s1 + 1, s2 + 1, nor, P.gm1inv, P.compat != 0, P.diss_scale, F);
                     lam = fmax(lam, fmax(qa.lam, qb.lam));
                     sgn = is1 ? -1.0 : 1.0;
+                    if (NS) {
+                        // 0.5 (F_v(1) + F_v(2)) . n with element 1's normal (DGSEMIntegrator.cpp:435-549)
+                        double g1[DIM][DIM + 2], g2[DIM][DIM + 2], f1[DIM][DIM + 1], f2[DIM][DIM + 1];
+                        load_grads<DIM>(P, (is1 ? e : other) * NDOF + (is1 ? n : n2), g1);
+                        load_grads<DIM>(P, (is1 ? other : e) * NDOF + (is1 ? n2 : n), g2);
+                        viscous_flux_cols<DIM>(P, s1, g1, f1);
+                        viscous_flux_cols<DIM>(P, s2, g2, f2);
+#pragma unroll
+                        for (int r = 0; r < NV - 1; r++) {
+                            double t = 0.0;
+#pragma unroll
+                            for (int q = 0; q < DIM; q++) {
+                                double avg = f1[q][r];
+                                avg += f2[q][r];
+                                avg *= 0.5;
+                                t += avg * nor[q];
+                            }
+                            fnv[1 + r] = t;
+                        }
+                    }
                 } else {
                     lam = fmax(lam, geo_bdr_flux<DIM>(P, (int)(-1 - other), s, nor, F));
                     sgn = -1.0;
+                    if (NS && (int)P.bc[(-1 - other) * BC_SLOT] == BC_SUPERSONIC_OUTFLOW) {
+                        // the interior state's own viscous flux (SupersonicOutflowBdrFaceIntegrator.cpp:15-20)
+                        double g1[DIM][DIM + 2], f1[DIM][DIM + 1];
+                        load_grads<DIM>(P, e * NDOF + n, g1);
+                        viscous_flux_cols<DIM>(P, s, g1, f1);
+#pragma unroll
+                        for (int r = 0; r < NV - 1; r++) {
+                            double t = 0.0;
+#pragma unroll
+                            for (int q = 0; q < DIM; q++) t += f1[q][r] * nor[q];
+                            fnv[1 + r] = t;
+                        }
+                    }
                 }
-                // AddMult_a_VWt(1 / (w0 J), shape, +-F)
-                const double scale = iw0 / J;
+                // AddMult_a_VWt(1 / (w0 J), shape, dU): dU = -+ (F - Fv.n) for element 1 / 2
+                const double scale = NS ? 1.0 / (C_W(c)[0] * J) : iw0 / J;
                 const int m = sp<DIM, Np>(n);
 #pragma unroll
-                for (int v = 0; v < NV; v++) acc[v * ST + m] += coef * (scale * (sgn * F[v]));
+                for (int v = 0; v < NV; v++) {
+                    double dU = sgn * F[v];
+                    if (NS) dU = sgn < 0.0 ? dU + fnv[v] : dU - fnv[v];
+                    acc[v * ST + m] += coef * (scale * dU);
+                }
             }
         }
         __syncwarp();
@@ -486,6 +638,166 @@ __device__ __forceinline__ void geo_tile(const KParams &P, const double *c, doub
     __syncwarp();
 }
 
+// BR1 lifting on a general mesh (LiftingBR1.cpp:10-115 faces, :156-272
+// elements; ComputeGlobalPrimitiveGradVector, DGSEMOperator.cpp:96-159): per
+// node the entropy variables' derivatives along the reference directions,
+// times the adjugate, times 1/J; every face node adds 0.5 (w2 - w1) n_k /
+// (w0 J) with element 1's states and normal (a boundary face: the condition's
+// outer state, supersonic inflow / outflow / specified state); then the
+// primitive gradients per direction, stored to P.geo_grads [d][v][node].
+// Slot: entropy variables [v][node], gradients [d][v][node].
+template <int DIM, int N> struct GeoLiftShape {
+    using S = Shape<DIM, N>;
+    static constexpr int EL = (1 + DIM) * S::NV * S::NS_;
+};
+
+template <int DIM, int N>
+__global__ void __launch_bounds__(128) geo_lift_kernel(const KParams P)
+{
+    using S = Shape<DIM, N>;
+    constexpr int Np = S::Np, NDOF = S::NDOF, NV = S::NV, NFN = S::NFN, L = S::L, EPW = S::EPW, ST = S::NS_;
+    extern __shared__ double smem[];
+    double *c = smem;
+    load_consts(P.K, c, Np);
+    __syncthreads();
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int grp = lane / L, gl = lane % L;
+    const int wpb = blockDim.x >> 5;
+    double *W = smem + const_slots(Np) + (size_t)(warp * EPW + grp) * GeoLiftShape<DIM, N>::EL;
+    double *Gs = W + NV * ST;
+    const double *Dm = C_D(c);
+    const int64_t nn = P.nnodes;
+    const int64_t wstride = (int64_t)gridDim.x * wpb;
+    for (int64_t wt = (int64_t)blockIdx.x * wpb + warp; wt < P.nwt; wt += wstride) {
+        const int64_t e0 = P.e_begin + wt * EPW + grp;
+        const bool valid = e0 < range_end(P);
+        const int64_t e = valid ? e0 : 0;
+#pragma unroll
+        for (int k = 0; k < S::NPL; k++) {
+            const int n = gl + k * L;
+            if (n < NDOF) {
+                double sv[NV], w[NV];
+#pragma unroll
+                for (int v = 0; v < NV; v++)
+                    sv[v] = valid ? __ldg(P.u + (int64_t)v * nn + e * NDOF + n) : (v == 0 ? 1.0 : (v == NV - 1 ? P.gm1inv : 0.0));
+                entropy_vars<DIM>(sv, P.gamma, P.gm1, P.gm1inv, w);
+#pragma unroll
+                for (int v = 0; v < NV; v++) W[v * ST + sp<DIM, Np>(n)] = w[v];
+            }
+        }
+        __syncwarp();
+        // element part
+#pragma unroll 1
+        for (int k = 0; k < S::NPL; k++) {
+            const int n = gl + k * L;
+            if (n < NDOF) {
+                const int pos[3] = {n % Np, (n / Np) % Np, n / (Np * Np)};
+                const int line[3] = {n / Np, DIM == 2 ? pos[0] : pos[0] + Np * pos[2], pos[0] + Np * pos[1]};
+                double gr[NV][DIM];
+#pragma unroll
+                for (int r = 0; r < DIM; r++)
+#pragma unroll
+                    for (int v = 0; v < NV; v++) {
+                        double acc = 0.0;
+#pragma unroll
+                        for (int l = 0; l < Np; l++)
+                            acc += W[v * ST + sp<DIM, Np>(line_node_rt<DIM, Np>(r, line[r], l))] * Dm[pos[r] * Np + l];
+                        gr[v][r] = acc;
+                    }
+                const int64_t g = e * NDOF + n;
+                const double ij = 1.0 / (valid ? geo_J(P, g) : 1.0);
+                double adj[DIM][DIM];
+#pragma unroll
+                for (int r = 0; r < DIM; r++)
+#pragma unroll
+                    for (int q = 0; q < DIM; q++) adj[r][q] = valid ? geo_row1<DIM>(P, g, r, q) : (r == q ? 1.0 : 0.0);
+#pragma unroll
+                for (int q = 0; q < DIM; q++)
+#pragma unroll
+                    for (int v = 0; v < NV; v++) {
+                        double t = 0.0;
+#pragma unroll
+                        for (int r = 0; r < DIM; r++) t += gr[v][r] * adj[r][q];
+                        Gs[(q * NV + v) * ST + sp<DIM, Np>(n)] = t * ij;
+                    }
+            }
+        }
+        __syncwarp();
+        // faces, direction by direction (a node lies on one face per direction)
+#pragma unroll 1
+        for (int d = 0; d < DIM; d++) {
+            if (valid) {
+                for (int t = gl; t < 2 * NFN; t += L) {
+                    const int side = t >= NFN, fn = side ? t - NFN : t;
+                    const int f = 2 * d + side;
+                    const int n = line_node_rt<DIM, Np>(d, fn, side ? N : 0);
+                    const int m = sp<DIM, Np>(n);
+                    const int64_t other = __ldg(P.nbr + e * 2 * DIM + f);
+                    const int64_t fi = (e * 2 * DIM + f) * NFN + fn;
+                    double nor[DIM], w1[NV], w2[NV];
+#pragma unroll
+                    for (int k = 0; k < DIM; k++) nor[k] = __ldg(P.fnor + fi * DIM + k);
+                    if (other >= 0) {
+                        const int n2 = __ldg(P.fnode + fi);
+                        double o[NV], wo[NV];
+#pragma unroll
+                        for (int v = 0; v < NV; v++) o[v] = __ldg(P.u + (int64_t)v * nn + other * NDOF + n2);
+                        entropy_vars<DIM>(o, P.gamma, P.gm1, P.gm1inv, wo);
+                        const bool is1 = e < other || (e == other && side == 1);
+#pragma unroll
+                        for (int v = 0; v < NV; v++) {
+                            w1[v] = is1 ? W[v * ST + m] : wo[v];
+                            w2[v] = is1 ? wo[v] : W[v * ST + m];
+                        }
+                    } else {
+                        // outer state: prescribed (inflow, specified state) or the interior (outflow)
+                        const double *bc = P.bc + (-1 - other) * BC_SLOT;
+                        const int type = (int)bc[0];
+                        double so[NV];
+#pragma unroll
+                        for (int v = 0; v < NV; v++)
+                            so[v] = (type == BC_SUPERSONIC_INFLOW || type == BC_SPECIFIED_STATE)
+                                        ? bc[1 + v] : __ldg(P.u + (int64_t)v * nn + e * NDOF + n);
+                        entropy_vars<DIM>(so, P.gamma, P.gm1, P.gm1inv, w2);
+#pragma unroll
+                        for (int v = 0; v < NV; v++) w1[v] = W[v * ST + m];
+                    }
+                    const double scale = 1.0 / (C_W(c)[0] * geo_J(P, e * NDOF + n));
+#pragma unroll
+                    for (int v = 0; v < NV; v++) {
+                        const double fl = 0.5 * (w2[v] - w1[v]);
+#pragma unroll
+                        for (int q = 0; q < DIM; q++) Gs[(q * NV + v) * ST + m] += scale * (fl * nor[q]);
+                    }
+                }
+            }
+            __syncwarp();
+        }
+        // primitive gradients
+        if (valid) {
+#pragma unroll 1
+            for (int k = 0; k < S::NPL; k++) {
+                const int n = gl + k * L;
+                if (n < NDOF) {
+                    double sv[NV];
+#pragma unroll
+                    for (int v = 0; v < NV; v++) sv[v] = __ldg(P.u + (int64_t)v * nn + e * NDOF + n);
+#pragma unroll
+                    for (int q = 0; q < DIM; q++) {
+                        double g[NV];
+#pragma unroll
+                        for (int v = 0; v < NV; v++) g[v] = Gs[(q * NV + v) * ST + sp<DIM, Np>(n)];
+                        entgrad_to_primgrad<DIM>(sv, P.gm1, P.gm1inv, false, g);
+#pragma unroll
+                        for (int v = 0; v < NV; v++) P.geo_grads[((int64_t)q * NV + v) * nn + e * NDOF + n] = g[v];
+                    }
+                }
+            }
+        }
+        __syncwarp();
+    }
+}
+
 // Resident 4-warp blocks the register budget must allow (3D N = 3).
 #ifndef PDG_GEO3_MIN_BLOCKS
 #define PDG_GEO3_MIN_BLOCKS 4
@@ -494,8 +806,8 @@ template <int DIM, int N> struct GeoOccupancy {
     static constexpr int min_blocks = (DIM == 3 && N == 3) ? PDG_GEO3_MIN_BLOCKS : 1;
 };
 
-template <int DIM, int N>
-__global__ void __launch_bounds__(128, GeoOccupancy<DIM, N>::min_blocks) geo_rhs_kernel(const KParams P)
+template <int DIM, int N, bool NS = false>
+__global__ void __launch_bounds__(128, NS ? 1 : GeoOccupancy<DIM, N>::min_blocks) geo_rhs_kernel(const KParams P)
 {
     using S = Shape<DIM, N>;
     constexpr int Np = S::Np, L = S::L, EPW = S::EPW;
@@ -507,12 +819,12 @@ __global__ void __launch_bounds__(128, GeoOccupancy<DIM, N>::min_blocks) geo_rhs
     const int grp = lane / L, gl = lane % L;
     const int wpb = blockDim.x >> 5;
     const bool lane_used = grp < EPW;
-    double *pr = smem + const_slots(Np) + (size_t)(warp * EPW + (lane_used ? grp : 0)) * S::EL_RHS_FB;
+    double *pr = smem + const_slots(Np) + (size_t)(warp * EPW + (lane_used ? grp : 0)) * GeoShape<DIM, N, NS>::EL;
     const int64_t wstride = (int64_t)gridDim.x * wpb;
     unsigned int flags = 0;
     double lam = 0.0;
     for (int64_t wt = (int64_t)blockIdx.x * wpb + warp; wt < P.nwt; wt += wstride)
-        geo_tile<DIM, N>(P, c, pr, P.e_begin + wt * EPW, grp, gl, lane_used, flags, lam);
+        geo_tile<DIM, N, NS>(P, c, pr, P.e_begin + wt * EPW, grp, gl, lane_used, flags, lam);
     lam = group_max<32>(lam);
     if (lane == 0) atomic_max_pos(P.lam_bits, lam);
     flags = __reduce_or_sync(0xffffffffu, flags);

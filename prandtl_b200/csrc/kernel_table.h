@@ -40,7 +40,9 @@ enum KernelKind {
     KIND_FACE_FLUX = 33,        // lift_face_kernel<dim, N, false, FACE_FLUX>: face fluxes (Euler)
     KIND_POSITIVITY = 34,       // positivity_kernel<dim, N>: positivity limiter of the stage output
     KIND_GEO = 35,              // geo_rhs_kernel<dim, N>: Euler right-hand side (+ stage) on a general-geometry mesh
-    KIND_COUNT = 36
+    KIND_GEO_LIFT = 36,         // geo_lift_kernel<dim, N>: BR1 primitive gradients on a general-geometry mesh
+    KIND_GEO_NS = 37,           // geo_rhs_kernel<dim, N, true>: Navier-Stokes right-hand side (+ stage), general geometry
+    KIND_COUNT = 38
 };
 
 struct KernelInfo {

@@ -49,7 +49,9 @@ template <int N> static bool info_n(int kind, KernelInfo *out)
     case KIND_FACE_NS2: out->fn = (const void *)&face_kernel<3, N, 2, true>; break;
     case KIND_FILTER_BOUNDS: out->fn = (const void *)&filter_bounds_kernel<3, N>; out->epw = 1; break;
     case KIND_POSITIVITY: out->fn = (const void *)&positivity_kernel<3, N>; out->epw = 1; break;
-    case KIND_GEO: out->fn = (const void *)&geo_rhs_kernel<3, N>; out->el_doubles = S::EL_RHS_FB; break;
+    case KIND_GEO: out->fn = (const void *)&geo_rhs_kernel<3, N>; out->el_doubles = GeoShape<3, N, false>::EL; break;
+    case KIND_GEO_NS: out->fn = (const void *)&geo_rhs_kernel<3, N, true>; out->el_doubles = GeoShape<3, N, true>::EL; break;
+    case KIND_GEO_LIFT: out->fn = (const void *)&geo_lift_kernel<3, N>; out->el_doubles = GeoLiftShape<3, N>::EL; break;
     case KIND_FILTER:
         out->fn = (const void *)&filter_kernel<3, N>;
         out->el_doubles = FilterShape<3, N>::EL;

@@ -107,6 +107,9 @@ struct KParams {
     const double *geo;
     const int32_t *fnode;
     const double *fnor;
+    // general geometry, Navier-Stokes: primitive gradients [d][v][node]
+    // (geo_lift_kernel writes them, geo_rhs_kernel<NS> reads them)
+    double *geo_grads;
 };
 
 __device__ __forceinline__ int64_t range_end(const KParams &P) { return P.e_end ? P.e_end : P.ne; }

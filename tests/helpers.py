@@ -96,3 +96,18 @@ def geometry_case(name):
 
 GEO_CASES = ["warped2d", "skewed2d", "perturbed2d", "rotated2d", "boundary2d", "warped3d", "perturbed3d",
              "rotated3d", "boundary3d"]
+
+
+GEO_BCS_NS_2D = {0: (1, [1.4, 0.42, 0.03, 2.6]), 1: (2, None), 2: (3, [1.3, 0.2, 0.0, 2.4]), 3: (2, None)}
+
+
+def ns_geometry_case(name):
+    """Navier-Stokes layouts: the periodic general meshes and a perturbed
+    channel with inflow, outflow and a prescribed state."""
+    if name == "boundary2d_ns":
+        from prandtl_b200 import geometry as G
+        return G.perturbed_box(2, 3, (5, 4), 0.0, 1.0, 0.3, seed=5, bdr=[(0, 1), (2, 3)], boundaries=GEO_BCS_NS_2D)
+    return geometry_case(name)
+
+
+NS_GEO_CASES = ["warped2d", "perturbed2d", "rotated2d", "warped3d", "perturbed3d", "rotated3d", "boundary2d_ns"]

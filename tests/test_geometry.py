@@ -25,7 +25,7 @@ import oracle
 from prandtl_b200 import geometry as G
 from prandtl_b200.mesh import box, periodic_box
 
-from helpers import GEO_CASES, geometry_case, rel_maxnorm, smooth_state
+from helpers import GEO_CASES, NS_GEO_CASES, geometry_case, ns_geometry_case, rel_maxnorm, smooth_state
 
 REF_TOL = 1e-12
 
@@ -146,18 +146,6 @@ def test_oracle_rejects_inverted_elements():
 
 
 NS = dict(mu=0.01, Pr=0.71)
-GEO_BCS_NS_2D = {0: (1, [1.4, 0.42, 0.03, 2.6]), 1: (2, None), 2: (3, [1.3, 0.2, 0.0, 2.4]), 3: (2, None)}
-
-
-def ns_geometry_case(name):
-    """Navier-Stokes layouts: the periodic general meshes and a perturbed
-    channel with inflow, outflow and a prescribed state."""
-    if name == "boundary2d_ns":
-        return G.perturbed_box(2, 3, (5, 4), 0.0, 1.0, 0.3, seed=5, bdr=[(0, 1), (2, 3)], boundaries=GEO_BCS_NS_2D)
-    return geometry_case(name)
-
-
-NS_GEO_CASES = ["warped2d", "perturbed2d", "rotated2d", "warped3d", "perturbed3d", "rotated3d", "boundary2d_ns"]
 
 
 @pytest.mark.skipif(not oracle.ref_available(True), reason="oracle/_ref not built (reference tree absent)")

@@ -17,7 +17,7 @@ import oracle
 import prandtl_b200 as pb
 from prandtl_b200 import geometry as G
 
-from helpers import GEO_CASES, geometry_case, rel_maxnorm, smooth_state
+from helpers import GEO_CASES, NS_GEO_CASES, geometry_case, ns_geometry_case, rel_maxnorm, smooth_state
 
 pytestmark = pytest.mark.gpu
 
@@ -144,11 +144,69 @@ def test_gpu_geometry_errors(cuda_device):
     with pytest.raises(pb.PdgError) as ei:
         pb.DGSEMOperator(inv, compat=0, parabolic=0)
     assert ei.value.code == 1  # PDG_ERR_ARG
-    # Navier-Stokes and the adjoint are box-mesh only
+    # the reference-value Navier-Stokes operator and the adjoint are box-mesh only
     with pytest.raises(pb.PdgError) as ei:
-        pb.DGSEMOperator(g, compat=0, parabolic=1, mu=0.01)
+        pb.DGSEMOperator(g, compat=1, parabolic=1, mu=0.01)
     assert ei.value.code == 5  # PDG_ERR_UNSUPPORTED
     op = pb.DGSEMOperator(g, compat=0, parabolic=0)
     x = torch.from_numpy(smooth_state(g, 1)).to(cuda_device)
     with pytest.raises(pb.PdgError):
         op.vjp(x, torch.ones_like(x))
+
+
+NS = dict(mu=0.01, Pr=0.71)
+
+
+@pytest.mark.parametrize("name", NS_GEO_CASES)
+def test_gpu_navier_stokes_matches_oracle(name, cuda_device):
+    """Navier-Stokes on general geometry (fixed operator): the lifting
+    kernel's primitive gradients, the right-hand side, the three RK stages
+    and graph-replayed steps against the oracle (whose general NS path
+    matches the reference's own NS build, tests/test_geometry.py)."""
+    import torch
+    g = ns_geometry_case(name)
+    u = smooth_state(g, 31)
+    kw = dict(compat=0, parabolic=1, **NS)
+    op = pb.DGSEMOperator(g, **kw)
+    x = torch.from_numpy(u).to(cuda_device)
+    out = torch.empty_like(x)
+    n0 = op.launch_count()
+    op.Mult(x, out)
+    assert op.launch_count() - n0 == 2
+    tol, want = _tol(g, kw, lambda o: o.rhs(u))
+    assert rel_maxnorm(out.cpu().numpy(), want) < tol
+    orc = oracle.Oracle(g, **kw)
+    orc.rhs(u)
+    fma = oracle.Oracle(g, fma=True, **kw)
+    fma.rhs(u)
+    gw = orc.gradients()
+    gtol = max(TOL, FLOOR_FACTOR * rel_maxnorm(fma.gradients(), gw))
+    assert rel_maxnorm(op.gradients(x).cpu().numpy().reshape(-1), gw) < gtol
+    dt = op.cfl_dt(0.3)
+    us = u
+    for stage in range(3):
+        tol, want = _tol(g, kw, lambda o: o.rk_stage(stage, dt, u, us))
+        o = torch.empty_like(x)
+        op.rk_stage(stage, dt, x, torch.from_numpy(us).to(cuda_device), o)
+        assert rel_maxnorm(o.cpu().numpy(), want) < tol, f"stage {stage}"
+        us = want
+    want, fw = u, u
+    of = oracle.Oracle(g, fma=True, **kw)
+    for _ in range(2):
+        want = orc.rk3_step(want, dt)
+        fw = of.rk3_step(fw, dt)
+    y = x.clone()
+    op.rk3_step(y, dt, nsteps=2, graph=True)
+    assert rel_maxnorm(y.cpu().numpy(), want) < max(TOL, FLOOR_FACTOR * rel_maxnorm(fw, want))
+    assert op.check() == 0
+
+
+def test_gpu_navier_stokes_geometry_rejects_other_conditions(cuda_device):
+    import torch
+    from helpers import GEO_BCS_2D
+    g = G.perturbed_box(2, 3, (5, 4), 0.0, 1.0, 0.3, seed=5, bdr=[(0, 1), (2, 3)], boundaries=GEO_BCS_2D)
+    op = pb.DGSEMOperator(g, compat=0, parabolic=1, **NS)   # a slip wall and a symmetry plane
+    x = torch.from_numpy(smooth_state(g, 2)).to(cuda_device)
+    with pytest.raises(pb.PdgError) as ei:
+        op.Mult(x, torch.empty_like(x))
+    assert ei.value.code == 5  # PDG_ERR_UNSUPPORTED
