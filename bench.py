@@ -679,7 +679,10 @@ def run_geometry_case(args, dev):
     from prandtl_b200 import geometry as G
     hbm, kind = measured_peaks()
     out = {}
-    for name, dim, order, n in (("curved_tgv_32^3_N3", 3, 3, 32), ("unstructured_kh_128^2_N4", 2, 4, 128)):
+    for name, dim, order, n in (("curved_tgv_32^3_N3", 3, 3, 32), ("curved_tgv_ns_32^3_N3", 3, 3, 32),
+                                ("unstructured_kh_128^2_N4", 2, 4, 128)):
+        ns = "_ns_" in name
+        par = dict(parabolic=1, compat=0, mu=1.0 / 1600.0, Pr=0.71) if ns else dict(parabolic=0, compat=0)
         if dim == 3:
             box = periodic_box(3, order, n, 0.0, 2 * np.pi)
             g = G.warped(box, 0.02)
@@ -691,12 +694,12 @@ def run_geometry_case(args, dev):
                                 range(0, n * n, 2), seed=2)
             u = cases.kelvin_helmholtz(g)
             ub = cases.kelvin_helmholtz(box)
-        op = pb.DGSEMOperator(g, parabolic=0, compat=0)
+        op = pb.DGSEMOperator(g, **par)
         x = torch.from_numpy(u).to(dev)
         op.Mult(x, torch.empty_like(x))
         dt = op.cfl_dt(0.3)
         ms = _timed_steps(op, x, dt, args.warmup, 20)
-        opb = pb.DGSEMOperator(box, parabolic=0, compat=0)
+        opb = pb.DGSEMOperator(box, **par)
         xb = torch.from_numpy(ub).to(dev)
         opb.Mult(xb, torch.empty_like(xb))
         ms_box = _timed_steps(opb, xb, opb.cfl_dt(0.3), args.warmup, 20)
@@ -704,6 +707,8 @@ def run_geometry_case(args, dev):
         nv, nd = dim + 2, (order + 1) ** dim
         nfn = (order + 1) ** (dim - 1)
         per_el = 8 * (nv * nd * (2 + 2 / 3) + (1 + dim * dim) * nd + 2 * dim * nfn * dim) + 4 * 2 * dim * nfn
+        if ns:  # the lifting kernel: state and metric terms in, gradients out; the volume kernel reads them
+            per_el += 8 * (nv * nd + (1 + dim * dim) * nd + 2 * dim * nfn * dim + 2 * dim * nv * nd) + 4 * 2 * dim * nfn
         bytes_stage = per_el * g.num_elements
         stage_s = ms / 3 * 1e-3
         out[name] = {"vdofs": g.size, "steps": 20, "ms_per_step": ms, "value": g.size * 3 / (ms * 1e-3),
@@ -712,7 +717,10 @@ def run_geometry_case(args, dev):
                                   "unit": "GB/s", "frac": bytes_stage / stage_s / 1e9 / hbm,
                                   "bytes_per_stage": bytes_stage, "peak_kind": kind},
                      "path": "pdg_set_geometry + pdg_rk3_steps (graph-replayed steps)"}
-        out[name]["cpu_baseline"] = _geometry_reference_sample(dim, order)
+        if ns:
+            out[name]["roofline"]["kernels"] = "geo_lift_kernel + geo_rhs_kernel<NS> per stage"
+        else:
+            out[name]["cpu_baseline"] = _geometry_reference_sample(dim, order)
     return out
 
 

@@ -131,18 +131,22 @@ int pdg_destroy(pdg_ctx *ctx);
  * node's normal out of the face's element 1 (the lower-numbered element)
  * and the CFL length, the smallest singular value of the Jacobian at an
  * element centre (MFEM's GetElementSize(e, 1), Simulation.cpp:896-906),
- * which replaces mesh->h.  Call once, before the first evaluation.  Euler
- * (parabolic = 0) without filter; both operators (compat changes the 3D
- * face dissipation term, the running maximum wave speed and the subsonic
- * conditions' in-place divisions, as on box meshes); every boundary
- * condition type.  One kernel per right-hand side or RK stage
- * (PDG_KERNEL_GEO).  pdg_rhs_vjp, pdg_rk_stage_vjp and pdg_rk_stage_part
+ * which replaces mesh->h.  Call once, before the first evaluation.  No
+ * filter.  Euler: both operators (compat changes the 3D face dissipation
+ * term, the running maximum wave speed and the subsonic conditions' in-place
+ * divisions, as on box meshes), every boundary condition type, one kernel
+ * per right-hand side or RK stage (PDG_KERNEL_GEO).  Navier-Stokes: the
+ * fixed operator (compat = 0) with supersonic inflow, supersonic outflow and
+ * specified-state boundaries (others: PDG_ERR_UNSUPPORTED at the first
+ * evaluation); the BR1 lifting kernel (PDG_KERNEL_GEO_LIFT, the adjugate at
+ * every node; pdg_gradients runs it alone) and the right-hand-side kernel
+ * with the contravariant viscous fluxes (PDG_KERNEL_GEO_NS).  pdg_rhs_vjp, pdg_rk_stage_vjp and pdg_rk_stage_part
  * return PDG_ERR_UNSUPPORTED on such a context; pdg_rk3_step_host copies
  * the state whole.  PDG_ERR_ARG: a non-positive Jacobian at a node, a code
  * whose neighbour face does not point back, or a neighbour whose normal at
  * the matching node is not the opposite of this element's (a non-conforming
- * face or a wrong code); PDG_ERR_UNSUPPORTED: a Navier-Stokes or filtered
- * operator. */
+ * face or a wrong code); PDG_ERR_UNSUPPORTED: a filtered operator, or the
+ * reference-value Navier-Stokes operator. */
 int pdg_set_geometry(pdg_ctx *ctx, const double *x, const int32_t *face_orient);
 
 /* Boundary conditions (the integrators of src/Integrators/BoundaryConditions/, attached to
@@ -401,6 +405,8 @@ int64_t pdg_launch_count(const pdg_ctx *ctx);
 #define PDG_KERNEL_FACE_FLUX 33      /* face-node kernel: inviscid face fluxes into the buffer (Euler) */
 #define PDG_KERNEL_POSITIVITY 34     /* positivity limiter of a stage output */
 #define PDG_KERNEL_GEO 35            /* Euler right-hand side on a general-geometry mesh (pdg_set_geometry) */
+#define PDG_KERNEL_GEO_LIFT 36       /* BR1 lifting on a general-geometry mesh */
+#define PDG_KERNEL_GEO_NS 37         /* Navier-Stokes right-hand side on a general-geometry mesh */
 int pdg_profile_enable(pdg_ctx *ctx, int on);
 int pdg_profile_read(pdg_ctx *ctx, int kind, double *total_ms, int64_t *launches);
 

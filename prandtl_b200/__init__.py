@@ -45,6 +45,8 @@ KERNEL_LIFT_BDR_PTTT = 29
 KERNEL_NS_FACES_FB, KERNEL_EULER_FACES_FB, KERNEL_LIFT_FACE_FLUX, KERNEL_FACE_FLUX = 30, 31, 32, 33
 KERNEL_POSITIVITY = 34
 KERNEL_GEO = 35
+KERNEL_GEO_LIFT = 36
+KERNEL_GEO_NS = 37
 # params.filter bits
 FILTER_ENTROPY, FILTER_POSITIVITY = 1, 2
 # boundary condition types (pdg_set_boundary)
