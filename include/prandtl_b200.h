@@ -136,9 +136,9 @@ int pdg_destroy(pdg_ctx *ctx);
  * term, the running maximum wave speed and the subsonic conditions' in-place
  * divisions, as on box meshes), every boundary condition type, one kernel
  * per right-hand side or RK stage (PDG_KERNEL_GEO).  Navier-Stokes: the
- * fixed operator (compat = 0) with supersonic inflow, supersonic outflow and
- * specified-state boundaries (others: PDG_ERR_UNSUPPORTED at the first
- * evaluation); the BR1 lifting kernel (PDG_KERNEL_GEO_LIFT, the adjugate at
+ * fixed operator (compat = 0) with every condition the box path takes with
+ * Navier-Stokes (slip wall and symmetry: PDG_ERR_UNSUPPORTED at the first
+ * evaluation, as there); the BR1 lifting kernel (PDG_KERNEL_GEO_LIFT, the adjugate at
  * every node; pdg_gradients runs it alone) and the right-hand-side kernel
  * with the contravariant viscous fluxes (PDG_KERNEL_GEO_NS).  pdg_rhs_vjp, pdg_rk_stage_vjp and pdg_rk_stage_part
  * return PDG_ERR_UNSUPPORTED on such a context; pdg_rk3_step_host copies

@@ -536,11 +536,10 @@ int evaluate(pdg_ctx *c, int stage, double dt, const double *un, const double *u
         if (!c->p.parabolic) return launch(c, KIND_GEO, P, s);
         for (int b = 0; b < PDG_MAX_BOUNDARIES; b++) {
             const int t = (int)c->bc_host[b * BC_SLOT];
-            if ((c->bc_used >> b & 1u) && t != PDG_BC_SUPERSONIC_INFLOW && t != PDG_BC_SUPERSONIC_OUTFLOW &&
-                t != PDG_BC_SPECIFIED_STATE)
+            // as on box meshes: the reference has no viscous flux for the slip wall and the symmetry plane
+            if ((c->bc_used >> b & 1u) && (t == PDG_BC_SLIP_WALL || t == PDG_BC_SYMMETRY))
                 return fail(c, PDG_ERR_UNSUPPORTED,
-                            "boundary condition %d: Navier-Stokes on general geometry takes supersonic inflow, outflow "
-                            "and specified states", b);
+                            "boundary condition %d: type %d has no viscous boundary flux here", b, t);
         }
         if ((r = launch(c, KIND_GEO_LIFT, P, s))) return r;
         return launch(c, KIND_GEO_NS, P, s);

@@ -225,7 +225,8 @@ template <int DIM> __device__ __forceinline__ void rotate_momentum(double *s, co
 // place first, as the reference's Vector views do (ComputePressure,
 // BasicOperations.cpp:31-37).
 template <int DIM>
-__device__ __noinline__ double geo_bdr_flux(const KParams &P, int b, const double *s_in, const double *nor, double *F)
+__device__ __noinline__ double geo_bdr_flux(const KParams &P, int b, const double *s_in, const double *nor, double *F,
+                                            double *outer = nullptr)
 {
     constexpr int NV = DIM + 2;
     const double *bc = P.bc + b * BC_SLOT;
@@ -349,6 +350,9 @@ __device__ __noinline__ double geo_bdr_flux(const KParams &P, int b, const doubl
         e2 += p_b * gm1inv;
         s2[NV - 1] = e2;
     }  // BC_SUPERSONIC_OUTFLOW: the interior state
+    if (outer)
+#pragma unroll
+        for (int v = 0; v < NV; v++) outer[v] = s2[v];
     const Prim<DIM> qa = make_prim<DIM>(s1, gamma, gm1), qb = make_prim<DIM>(s2, gamma, gm1);
     double ma[DIM], mb[DIM];
 #pragma unroll
@@ -598,17 +602,37 @@ __device__ __forceinline__ void geo_tile(const KParams &P, const double *c, doub
                 } else {
                     lam = fmax(lam, geo_bdr_flux<DIM>(P, (int)(-1 - other), s, nor, F));
                     sgn = -1.0;
-                    if (NS && (int)P.bc[(-1 - other) * BC_SLOT] == BC_SUPERSONIC_OUTFLOW) {
-                        // the interior state's own viscous flux (SupersonicOutflowBdrFaceIntegrator.cpp:15-20)
-                        double g1[DIM][DIM + 2], f1[DIM][DIM + 1];
+                    const double *bcv = P.bc + (-1 - other) * BC_SLOT;
+                    const int bt = (int)bcv[0];
+                    if (NS && (bt == BC_SUPERSONIC_OUTFLOW || bt == BC_NOSLIP_ADIABATIC || bt == BC_NOSLIP_ISOTHERMAL ||
+                               bt == BC_SUBSONIC_INFLOW_PTTT)) {
+                        // ComputeBdrFaceViscousFlux: the interior state's own viscous flux
+                        // (SupersonicOutflowBdrFaceIntegrator.cpp:15-20; the walls', whose
+                        // adiabatic energy row is the wall velocity's work,
+                        // NoSlipAdiabWallBdrFaceIntegrator.cpp:21-36), or the outer
+                        // state's with the interior gradients (SubsonicInflowPtTtAngBdrFaceIntegrator.cpp:88-92)
+                        double g1[DIM][DIM + 2], f1[DIM][DIM + 1], sv[NV];
                         load_grads<DIM>(P, e * NDOF + n, g1);
-                        viscous_flux_cols<DIM>(P, s, g1, f1);
+                        if (bt == BC_SUBSONIC_INFLOW_PTTT) {
+                            double Fd[NV];
+                            geo_bdr_flux<DIM>(P, (int)(-1 - other), s, nor, Fd, sv);
+                        } else {
+#pragma unroll
+                            for (int v = 0; v < NV; v++) sv[v] = s[v];
+                        }
+                        viscous_flux_cols<DIM>(P, sv, g1, f1);
 #pragma unroll
                         for (int r = 0; r < NV - 1; r++) {
                             double t = 0.0;
 #pragma unroll
                             for (int q = 0; q < DIM; q++) t += f1[q][r] * nor[q];
                             fnv[1 + r] = t;
+                        }
+                        if (bt == BC_NOSLIP_ADIABATIC) {
+                            double en = 0.0;
+#pragma unroll
+                            for (int q = 0; q < DIM; q++) en += bcv[1 + q] * fnv[1 + q];
+                            fnv[NV - 1] = en + 0.0;
                         }
                     }
                 }
@@ -734,7 +758,7 @@ __global__ void __launch_bounds__(128) geo_lift_kernel(const KParams P)
                     const int m = sp<DIM, Np>(n);
                     const int64_t other = __ldg(P.nbr + e * 2 * DIM + f);
                     const int64_t fi = (e * 2 * DIM + f) * NFN + fn;
-                    double nor[DIM], w1[NV], w2[NV];
+                    double nor[DIM], w1[NV], w2[NV], fl[NV];
 #pragma unroll
                     for (int k = 0; k < DIM; k++) nor[k] = __ldg(P.fnor + fi * DIM + k);
                     if (other >= 0) {
@@ -748,26 +772,47 @@ __global__ void __launch_bounds__(128) geo_lift_kernel(const KParams P)
                         for (int v = 0; v < NV; v++) {
                             w1[v] = is1 ? W[v * ST + m] : wo[v];
                             w2[v] = is1 ? wo[v] : W[v * ST + m];
+                            fl[v] = 0.5 * (w2[v] - w1[v]);
                         }
                     } else {
-                        // outer state: prescribed (inflow, specified state) or the interior (outflow)
+                        // ComputeBdrFaceLiftingFlux (BdrFaceIntegrator.cpp:275-282): half the jump
+                        // to the condition's outer state; the no-slip walls
+                        // (NoSlipAdiabWallBdrFaceIntegrator.cpp:74-95, NoSlipIsothWallBdrFaceIntegrator.cpp:41-65):
+                        // (w1_0, beta V_wall, -beta) - w1
                         const double *bc = P.bc + (-1 - other) * BC_SLOT;
                         const int type = (int)bc[0];
-                        double so[NV];
-#pragma unroll
-                        for (int v = 0; v < NV; v++)
-                            so[v] = (type == BC_SUPERSONIC_INFLOW || type == BC_SPECIFIED_STATE)
-                                        ? bc[1 + v] : __ldg(P.u + (int64_t)v * nn + e * NDOF + n);
-                        entropy_vars<DIM>(so, P.gamma, P.gm1, P.gm1inv, w2);
 #pragma unroll
                         for (int v = 0; v < NV; v++) w1[v] = W[v * ST + m];
+                        if (type == BC_NOSLIP_ADIABATIC || type == BC_NOSLIP_ISOTHERMAL) {
+                            const double beta = type == BC_NOSLIP_ADIABATIC ? -w1[NV - 1] : bc[1 + DIM];
+                            fl[0] = w1[0] - w1[0];
+#pragma unroll
+                            for (int q = 0; q < DIM; q++) fl[1 + q] = bc[1 + q] * beta - w1[1 + q];
+                            fl[NV - 1] = -beta - w1[NV - 1];
+                        } else {
+                            double si[NV], so[NV];
+#pragma unroll
+                            for (int v = 0; v < NV; v++) si[v] = __ldg(P.u + (int64_t)v * nn + e * NDOF + n);
+                            if (type == BC_SUPERSONIC_INFLOW || type == BC_SPECIFIED_STATE) {
+#pragma unroll
+                                for (int v = 0; v < NV; v++) so[v] = bc[1 + v];
+                            } else if (type == BC_SUPERSONIC_OUTFLOW) {
+#pragma unroll
+                                for (int v = 0; v < NV; v++) so[v] = si[v];
+                            } else {
+                                double Fd[NV];
+                                geo_bdr_flux<DIM>(P, (int)(-1 - other), si, nor, Fd, so);
+                            }
+                            entropy_vars<DIM>(so, P.gamma, P.gm1, P.gm1inv, w2);
+#pragma unroll
+                            for (int v = 0; v < NV; v++) fl[v] = 0.5 * (w2[v] - w1[v]);
+                        }
                     }
                     const double scale = 1.0 / (C_W(c)[0] * geo_J(P, e * NDOF + n));
 #pragma unroll
                     for (int v = 0; v < NV; v++) {
-                        const double fl = 0.5 * (w2[v] - w1[v]);
 #pragma unroll
-                        for (int q = 0; q < DIM; q++) Gs[(q * NV + v) * ST + m] += scale * (fl * nor[q]);
+                        for (int q = 0; q < DIM; q++) Gs[(q * NV + v) * ST + m] += scale * (fl[v] * nor[q]);
                     }
                 }
             }

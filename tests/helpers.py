@@ -107,7 +107,36 @@ def ns_geometry_case(name):
     if name == "boundary2d_ns":
         from prandtl_b200 import geometry as G
         return G.perturbed_box(2, 3, (5, 4), 0.0, 1.0, 0.3, seed=5, bdr=[(0, 1), (2, 3)], boundaries=GEO_BCS_NS_2D)
+    if name in ("walls2d_ns", "subsonic2d_ns", "riemann2d_ns", "walls3d_ns"):
+        return _ns_channel(name)
     return geometry_case(name)
 
 
-NS_GEO_CASES = ["warped2d", "perturbed2d", "rotated2d", "warped3d", "perturbed3d", "rotated3d", "boundary2d_ns"]
+GEO_BCS_NS_WALLS_2D = {0: (1, [1.4, 0.42, 0.03, 2.6]), 1: (2, None), 2: (10, [0.0, 0.0]),
+                       3: (11, [0.0035, 0.1, 0.0])}
+GEO_BCS_NS_SUBSONIC_2D = {0: (8, [3.5, 1.3, 2.0, 10.0, 0.0]), 1: (6, [0.95]), 2: (7, [1.2, 0.3, 0.0]),
+                          3: (10, [0.0, 0.0])}
+# the Riemann invariants (fixed operator only: the reference's NS lifting
+# flux for them reads a normal left by an earlier face)
+GEO_BCS_NS_RIEMANN_2D = {0: (9, [1.0, 0.3, 0.0, 1.0]), 1: (9, [1.0, 0.3, 0.0, 1.0]), 2: (10, [0.0, 0.0]),
+                         3: (10, [0.0, 0.0])}
+GEO_BCS_NS_WALLS_3D = {0: (1, [1.4, 0.42, 0.03, 0.0, 2.6]), 1: (2, None), 2: (10, [0.0, 0.0, 0.0]),
+                       3: (11, [0.0035, 0.1, 0.0, 0.0]), 4: (6, [0.95]), 5: (7, [1.2, 0.3, 0.0, 0.0])}
+
+
+def _ns_channel(name):
+    from prandtl_b200 import geometry as G
+    if name == "walls2d_ns":
+        return G.perturbed_box(2, 3, (5, 4), 0.0, 1.0, 0.3, seed=7, bdr=[(0, 1), (2, 3)], boundaries=GEO_BCS_NS_WALLS_2D)
+    if name == "subsonic2d_ns":
+        return G.perturbed_box(2, 3, (5, 4), 0.0, 1.0, 0.3, seed=8, bdr=[(0, 1), (2, 3)],
+                               boundaries=GEO_BCS_NS_SUBSONIC_2D)
+    if name == "riemann2d_ns":
+        return G.perturbed_box(2, 3, (5, 4), 0.0, 1.0, 0.3, seed=10, bdr=[(0, 1), (2, 3)],
+                               boundaries=GEO_BCS_NS_RIEMANN_2D)
+    return G.perturbed_box(3, 2, (3, 3, 4), 0.0, 1.0, 0.25, seed=9, bdr=[(0, 1), (2, 3), (4, 5)],
+                           boundaries=GEO_BCS_NS_WALLS_3D)
+
+
+NS_GEO_CASES = ["warped2d", "perturbed2d", "rotated2d", "warped3d", "perturbed3d", "rotated3d", "boundary2d_ns",
+                "walls2d_ns", "subsonic2d_ns", "walls3d_ns"]

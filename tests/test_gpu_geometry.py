@@ -157,7 +157,7 @@ def test_gpu_geometry_errors(cuda_device):
 NS = dict(mu=0.01, Pr=0.71)
 
 
-@pytest.mark.parametrize("name", NS_GEO_CASES)
+@pytest.mark.parametrize("name", NS_GEO_CASES + ["riemann2d_ns"])
 def test_gpu_navier_stokes_matches_oracle(name, cuda_device):
     """Navier-Stokes on general geometry (fixed operator): the lifting
     kernel's primitive gradients, the right-hand side, the three RK stages
@@ -202,6 +202,7 @@ def test_gpu_navier_stokes_matches_oracle(name, cuda_device):
 
 
 def test_gpu_navier_stokes_geometry_rejects_other_conditions(cuda_device):
+    """Slip walls and symmetry planes have no viscous flux (as on box meshes)."""
     import torch
     from helpers import GEO_BCS_2D
     g = G.perturbed_box(2, 3, (5, 4), 0.0, 1.0, 0.3, seed=5, bdr=[(0, 1), (2, 3)], boundaries=GEO_BCS_2D)
