@@ -1,4 +1,6 @@
-"""Periodic Cartesian meshes in the layout the C ABI expects.
+"""Cartesian meshes in the layout the C ABI expects (general geometry —
+node coordinates and face orientation codes — is carried by the same class;
+see ``prandtl_b200.geometry``).
 
 The reference builds its meshes with MFEM (src/Simulation/Simulation.cpp:271-336)
 and numbers DG nodes element by element, lexicographically inside an element

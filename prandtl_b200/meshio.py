@@ -21,17 +21,20 @@ attribute is the physical tag).  Two formats are read here:
 Both number a quadrilateral's corners counter-clockwise from its first
 corner, and a hexahedron's bottom face that way and then its top face.
 
-The kernels take one element size per direction and element axes along the
-coordinate axes, so a mesh is accepted only when every element is an
-axis-aligned box of the same size.  An element whose corners the file lists
+A mesh whose elements are all axis-aligned boxes of one size is read for
+the box kernels (one element size per direction, element axes along the
+coordinate axes); any other mesh — graded, skewed or unstructured, like the
+forward-facing step, the ramp and the ramjet — is read as a general-geometry
+mesh (``build_general_mesh``: each element in the file's frame, node
+coordinates from its bilinear or trilinear map, face orientation codes from
+its corner vertices) for the general-geometry kernel.  For the box form, an
+element whose corners the file lists
 in a rotated or mirrored order (Gmsh does this in the step meshes) is
 relabelled so that its first corner is its lowest one and its second lies
 along +x (fourth along +y, fifth along +z); its DG nodes are then numbered in
 that frame, not the reference's, ``mesh.reoriented`` lists it and
 ``to_reference_order`` / ``from_reference_order`` move fields between the two
-node orders.  Curved,
-skewed or graded meshes (the ramp, the ramjet) raise ``ValueError``.  Elements keep the
-file's order; faces are paired by their corner vertices, so periodic
+node orders.  Elements keep the file's order; faces are paired by their corner vertices, so periodic
 identifications of an MFEM mesh carry over (a periodic direction needs three
 elements or more, else two faces share their vertices).  A boundary face takes condition
 ``attribute - 1`` (neighbour entry ``-attribute``).
