@@ -1,5 +1,7 @@
-// geo_kernels.cuh — the Euler right-hand side on meshes of general geometry
-// (skewed, graded, curved or unstructured quadrilaterals and hexahedra).
+// geo_kernels.cuh — the Euler and Navier-Stokes right-hand sides on meshes of
+// general geometry (skewed, graded, curved or unstructured quadrilaterals and
+// hexahedra): geo_rhs_kernel (Euler, or with NS the viscous terms as well)
+// and geo_lift_kernel (BR1 gradients, Navier-Stokes).
 //
 // The reference evaluates every metric term from MFEM's element
 // transformation at the integration points: the two-point volume fluxes use
@@ -21,7 +23,8 @@
 // to both nodes), then each element evaluates its own face nodes with the
 // element-1 rule (both elements of a face evaluate it from the same inputs
 // in the same order and receive bit-identical fluxes) and stores the
-// finished stage.  One launch per right-hand side or RK stage.
+// finished stage.  One launch per right-hand side or RK stage (Navier-Stokes:
+// the lifting kernel first).
 #pragma once
 
 #include "line_kernels.cuh"
