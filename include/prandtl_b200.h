@@ -131,8 +131,9 @@ int pdg_destroy(pdg_ctx *ctx);
  * node's normal out of the face's element 1 (the lower-numbered element)
  * and the CFL length, the smallest singular value of the Jacobian at an
  * element centre (MFEM's GetElementSize(e, 1), Simulation.cpp:896-906),
- * which replaces mesh->h.  Call once, before the first evaluation.  No
- * filter.  Euler: both operators (compat changes the 3D face dissipation
+ * which replaces mesh->h.  Call once, before the first evaluation.  The
+ * entropy filter and the positivity limiter run as on box meshes (the
+ * limiter contracts towards J-weighted element means).  Euler: both operators (compat changes the 3D face dissipation
  * term, the running maximum wave speed and the subsonic conditions' in-place
  * divisions, as on box meshes), every boundary condition type, one kernel
  * per right-hand side or RK stage (PDG_KERNEL_GEO).  Navier-Stokes: the
@@ -145,8 +146,8 @@ int pdg_destroy(pdg_ctx *ctx);
  * the state whole.  PDG_ERR_ARG: a non-positive Jacobian at a node, a code
  * whose neighbour face does not point back, or a neighbour whose normal at
  * the matching node is not the opposite of this element's (a non-conforming
- * face or a wrong code); PDG_ERR_UNSUPPORTED: a filtered operator, or the
- * reference-value Navier-Stokes operator. */
+ * face or a wrong code); PDG_ERR_UNSUPPORTED: the reference-value
+ * Navier-Stokes operator. */
 int pdg_set_geometry(pdg_ctx *ctx, const double *x, const int32_t *face_orient);
 
 /* Boundary conditions (the integrators of src/Integrators/BoundaryConditions/, attached to

@@ -1884,6 +1884,7 @@ static void positivity_apply(Ctx &c, double *x)
         for (int n = 0; n < nd; n++) {
             double wn = c.w[n % Np] * c.w[(n / Np) % Np];
             if (dim == 3) wn *= c.w[n / (Np * Np)];
+            if (c.geo) wn *= c.gJ[(size_t)e * nd + n];  // general geometry: the J-weighted mean
             W += wn;
             for (int v = 0; v < nv; v++) m[v] += wn * x[idx(c, v, e, n)];
             rmin = std::min(rmin, x[idx(c, 0, e, n)]);

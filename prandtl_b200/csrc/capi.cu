@@ -532,17 +532,27 @@ int evaluate(pdg_ctx *c, int stage, double dt, const double *un, const double *u
     c->last_stream = s;
     int r;
     if (c->geo) {
-        // general geometry: one kernel (Navier-Stokes: the lifting kernel first)
-        if (!c->p.parabolic) return launch(c, KIND_GEO, P, s);
-        for (int b = 0; b < PDG_MAX_BOUNDARIES; b++) {
-            const int t = (int)c->bc_host[b * BC_SLOT];
-            // as on box meshes: the reference has no viscous flux for the slip wall and the symmetry plane
-            if ((c->bc_used >> b & 1u) && (t == PDG_BC_SLIP_WALL || t == PDG_BC_SYMMETRY))
-                return fail(c, PDG_ERR_UNSUPPORTED,
-                            "boundary condition %d: type %d has no viscous boundary flux here", b, t);
+        // general geometry: one kernel (Navier-Stokes: the lifting kernel
+        // first), with the filter's bounds before and the filter and the
+        // positivity limiter after it, as on box meshes
+        if (c->p.parabolic)
+            for (int b = 0; b < PDG_MAX_BOUNDARIES; b++) {
+                const int t = (int)c->bc_host[b * BC_SLOT];
+                // as on box meshes: the reference has no viscous flux for the slip wall and the symmetry plane
+                if ((c->bc_used >> b & 1u) && (t == PDG_BC_SLIP_WALL || t == PDG_BC_SYMMETRY))
+                    return fail(c, PDG_ERR_UNSUPPORTED,
+                                "boundary condition %d: type %d has no viscous boundary flux here", b, t);
+            }
+        if ((c->p.filter & 1) && stage >= 0 && (r = launch(c, KIND_FILTER_BOUNDS, P, s))) return r;
+        if (!c->p.parabolic) {
+            if ((r = launch(c, KIND_GEO, P, s))) return r;
+        } else {
+            if ((r = launch(c, KIND_GEO_LIFT, P, s))) return r;
+            if ((r = launch(c, KIND_GEO_NS, P, s))) return r;
         }
-        if ((r = launch(c, KIND_GEO_LIFT, P, s))) return r;
-        return launch(c, KIND_GEO_NS, P, s);
+        if ((c->p.filter & 1) && stage >= 0 && (r = launch(c, KIND_FILTER, P, s))) return r;
+        if ((c->p.filter & 2) && stage >= 0 && (r = launch(c, KIND_POSITIVITY, P, s))) return r;
+        return PDG_OK;
     }
     const bool element_faces = c->element_faces && !c->p.compat;
     if (c->p.parabolic) {
@@ -824,9 +834,8 @@ int pdg_set_geometry(pdg_ctx *c, const double *x, const int32_t *face_orient)
     if (!c) return PDG_ERR_ARG;
     if (!x) return fail(c, PDG_ERR_ARG, "pdg_set_geometry: null coordinates");
     if (c->geo) return fail(c, PDG_ERR_ARG, "pdg_set_geometry: the geometry is already set");
-    if (c->p.filter || (c->p.parabolic && c->p.compat))
-        return fail(c, PDG_ERR_UNSUPPORTED,
-                    "pdg_set_geometry: general geometry takes no filter, and Navier-Stokes with compat = 0");
+    if (c->p.parabolic && c->p.compat)
+        return fail(c, PDG_ERR_UNSUPPORTED, "pdg_set_geometry: Navier-Stokes on general geometry takes compat = 0");
     const int dim = c->dim, Np = c->Np, N = c->N, nd = c->ndof, nf = 2 * dim;
     const int nfn = dim == 2 ? Np : Np * Np;
     const int64_t ne = c->ne, nn = c->nnodes;

@@ -265,6 +265,7 @@ __global__ void __launch_bounds__(256) positivity_kernel(const KParams P)
         for (int n = lane; n < NDOF; n += 32) {
             double wn = w[n % Np] * w[(n / Np) % Np];
             if (DIM == 3) wn *= w[n / (Np * Np)];
+            if (P.geo) wn *= __ldg(P.geo + e * NDOF + n);  // general geometry: the J-weighted mean
             W += wn;
 #pragma unroll
             for (int v = 0; v < NV; v++) m[v] += wn * x[v * nn + n];

@@ -174,3 +174,101 @@ def test_gpu_kelvin_helmholtz_64_filter_and_limiter(rough_state, cuda_device):
         us = want
     if rough_state:
         assert orc.limited_elements() > 0, "the roughened state must exercise the limiter"
+
+
+# ---- general geometry: the limiter contracts towards J-weighted means ----
+
+def _geo_case(kind):
+    from prandtl_b200 import geometry as G
+    if kind == "kh2d_curved":
+        m = G.warped(periodic_box(2, 3, (8, 9), -1.0, 1.0), 0.03)
+        return m, rough(cases.kelvin_helmholtz(m), m, 3, 0.15, 0.03)
+    m = G.perturbed_box(3, 3, (4, 3, 5), 0.0, 2 * np.pi, 0.2, seed=2)
+    return m, rough(cases.taylor_green(m), m, 5, 0.15, 0.05)
+
+
+def _geo_means(u, mesh):
+    """J-weighted element means (J from the LGL derivative of the node coordinates)."""
+    _, w1 = gll_nodes(mesh.Np)
+    wq = w1
+    for _ in range(mesh.dim - 1):
+        wq = np.kron(w1, wq)
+    J = _node_jacobians(mesh)
+    U = u.reshape(mesh.nv, mesh.num_elements, mesh.ndof)
+    wt = J * wq[None, :]
+    return np.einsum("ven,en->ve", U, wt) / wt.sum(axis=1)
+
+
+def _node_jacobians(mesh):
+    """det of dx/dxi at every node: the LGL derivative of the node coordinates."""
+    x1, _ = gll_nodes(mesh.Np)
+    Np, dim = mesh.Np, mesh.dim
+    bw = np.array([1.0 / np.prod([x1[l] - x1[q] for q in range(Np) if q != l]) for l in range(Np)])
+    D = np.zeros((Np, Np))
+    for i in range(Np):
+        for l in range(Np):
+            if l != i:
+                D[i, l] = bw[l] / bw[i] / (x1[i] - x1[l])
+        D[i, i] = -D[i].sum()
+    X = np.asarray(mesh.coords).reshape((dim, mesh.num_elements) + (Np,) * dim)
+    cols = []
+    for r in range(dim):
+        ax = X.ndim - 1 - r  # reference axis r (x fastest) is array axis -1 - r
+        cols.append(np.moveaxis(np.tensordot(D, X, axes=([1], [ax])), 0, ax))
+    Jm = np.stack(cols, axis=-1)            # (dim_k, ne, ..., r)
+    Jm = np.moveaxis(Jm, 0, -2)             # (ne, ..., k, r)
+    return np.linalg.det(Jm).reshape(mesh.num_elements, -1)
+
+
+@pytest.mark.parametrize("kind,cfl", [("kh2d_curved", 8.0), ("tgv3d_perturbed", 5.0)])
+def test_oracle_limiter_on_general_geometry(kind, cfl):
+    mesh, u = _geo_case(kind)
+    par = dict(parabolic=0)
+    o = oracle.Oracle(mesh, compat=0, **par)
+    o.rhs(u)
+    dt = cfl * min(mesh.h) / (o.max_char_speed() * (mesh.order + 1) ** 2)
+    y = o.rk_stage(0, dt, u, u)
+    nn = mesh.num_nodes
+    bad = (y[:nn] <= 0) | (_pressure(y, mesh.dim, nn) <= 0)
+    assert bad.any()
+    z = oracle.Oracle(mesh, compat=0, filter=2, **par).positivity(y)
+    np.testing.assert_allclose(_geo_means(z, mesh), _geo_means(y, mesh), rtol=1e-12, atol=1e-12)
+    M = _geo_means(y, mesh)
+    ok_el = (M[0] > 0) & ((GAMMA - 1.0) * (M[-1] - 0.5 * np.sum(M[1:1 + mesh.dim] ** 2, axis=0) / M[0]) > 0)
+    pos = ((z[:nn] > 0) & (_pressure(z, mesh.dim, nn) > 0)).reshape(mesh.num_elements, mesh.ndof).all(axis=1)
+    assert pos[ok_el].all()
+    bad_el = bad.reshape(mesh.num_elements, mesh.ndof).any(axis=1)
+    Y = y.reshape(mesh.nv, mesh.num_elements, mesh.ndof)
+    Z = z.reshape(mesh.nv, mesh.num_elements, mesh.ndof)
+    assert np.array_equal(Y[:, ~bad_el], Z[:, ~bad_el])
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("filt", [2, 3])
+@pytest.mark.parametrize("kind,cfl", [("kh2d_curved", 3.0), ("tgv3d_perturbed", 3.0)])
+def test_gpu_limited_stages_on_general_geometry(kind, cfl, filt, cuda_device):
+    """The entropy filter and the positivity limiter after each stage on a
+    curved 2D and a perturbed 3D mesh, GPU against the oracle."""
+    import torch
+    mesh, u = _geo_case(kind)
+    par = dict(parabolic=0)
+    o = oracle.Oracle(mesh, compat=0, **par)
+    o.rhs(u)
+    dt = cfl * min(mesh.h) / (o.max_char_speed() * (mesh.order + 1) ** 2)
+    kw = dict(filter=filt, compat=0, **par)
+    orc = oracle.Oracle(mesh, **kw)
+    op = pb.DGSEMOperator(mesh, **kw)
+    un = torch.from_numpy(u).to(cuda_device)
+    us = u
+    for stage in range(3):
+        want = orc.rk_stage(stage, dt, u, us)
+        out = torch.empty_like(un)
+        op.rk_stage(stage, dt, un, torch.from_numpy(us).to(cuda_device), out)
+        tol = _stage_tol(mesh, kw, stage, dt, u, us, want)
+        assert rel_maxnorm(out.cpu().numpy(), want) < tol, f"stage {stage}"
+        assert op.limiter_count() == orc.limited_elements()
+        if filt & 1:
+            assert op.filter_count() == orc.filtered_elements()
+        us = want
+    if filt == 2:
+        assert orc.limited_elements() > 0
