@@ -1,6 +1,7 @@
 """Slab decomposition of a Cartesian mesh (periodic along its last axis,
 optionally with boundary faces on the others) over ranks, with a ghost layer
-exchange per RK stage.
+exchange per RK stage; element partitions of meshes of general geometry
+(``ElementPartition``, whole ghost elements exchanged per stage).
 
 The reference partitions elements over MPI ranks and exchanges face-neighbour
 data once per right-hand-side pass (``ExchangeFaceNbrData``,
@@ -149,13 +150,152 @@ class GhostExchange:
             r.wait()
 
 
-class DistributedRK3:
-    """SSP-RK3 on a slab decomposition: exchange, then one fused stage of the
-    rank's operator (``op.rk_stage(stage, dt, un, us, uout)``) per stage."""
+class ElementPartition:
+    """Rank `rank`'s share of a mesh of general geometry (or any mesh): the
+    elements with part[e] == rank (default: `world` contiguous index ranges)
+    plus `layers` layers of ghost elements, the owned elements' face
+    neighbours (one layer for Euler; Navier-Stokes needs two, so that the
+    first layer's BR1 gradients at the shared faces are exact, its own face
+    neighbours being held).  The local mesh keeps the elements in global
+    order (so element 1 of every face, the lower-numbered element, is the
+    same as on the whole mesh), their node coordinates and face orientation
+    codes; a ghost's face towards an element that is not held becomes a
+    boundary face of a spare condition (supersonic outflow), whose values
+    reach no owned element.  The reference partitions with METIS and
+    exchanges face-neighbour data (DGSEMNonlinearForm.cpp:748); here the
+    partition is given and whole ghost elements are exchanged."""
 
-    def __init__(self, dec: SlabDecomposition, op, group=None):
+    SPARE = 15  # boundary condition index of the cut faces
+
+    def __init__(self, mesh: CartesianMesh, world: int, rank: int, layers: int = 1, part=None):
+        ne = mesh.num_elements
+        if world < 1 or not (0 <= rank < world):
+            raise ValueError("need 0 <= rank < world")
+        self.glob, self.world, self.rank, self.layers = mesh, world, rank, int(layers)
+        self.part = (np.arange(ne) * world) // ne if part is None else np.asarray(part, dtype=np.int64)
+        if self.part.shape != (ne,) or self.part.min() < 0 or self.part.max() >= world:
+            raise ValueError("part must give every element a rank in [0, world)")
+        self.local_sets = [self._local(q) for q in range(world)]
+        local = self.local_sets[rank]
+        self.local = local
+        g2l = np.full(ne, -1, dtype=np.int64)
+        g2l[local] = np.arange(local.size)
+        nbr = mesh.nbr[local].astype(np.int64)
+        inner = nbr >= 0
+        tgt = np.where(inner, g2l[np.where(inner, nbr, 0)], 0)
+        cut = inner & (tgt < 0)
+        new = np.where(inner, tgt, nbr)
+        boundaries = dict(mesh.boundaries or {})
+        if cut.any():
+            if self.SPARE in boundaries or (mesh.nbr == -1 - self.SPARE).any():
+                raise ValueError(f"boundary condition {self.SPARE} is in use; the partition needs it for cut faces")
+            new[cut] = -1 - self.SPARE
+            boundaries[self.SPARE] = (2, None)
+        dim = mesh.dim
+        fo = None
+        if mesh.face_orient is not None:
+            fo = np.where(cut, 0, np.asarray(mesh.face_orient)[local]).astype(np.int32)
+        nl = int(local.size)
+        m = CartesianMesh(dim, mesh.order, (nl,) + (1,) * (dim - 1), tuple(mesh.lo), tuple(mesh.hi),
+                          new.astype(np.int32), spacing=tuple(mesh.h), boundaries=boundaries)
+        if mesh.coords is not None:
+            X = np.asarray(mesh.coords).reshape(dim, ne, mesh.ndof)
+            m.coords = np.ascontiguousarray(X[:, local, :].reshape(dim, -1))
+            m.face_orient = fo
+        elif (local != np.arange(ne)).any():
+            raise ValueError("a partition of a box mesh needs its node coordinates (use geometry.warped(mesh, 0.0))")
+        self.mesh = m
+        self.owned_local = np.nonzero(self.part[local] == rank)[0]
+        # exchange lists: per peer, the local positions to send (my owned
+        # elements it holds) and to receive (its owned elements I hold), both
+        # in ascending global order
+        self.send_idx, self.recv_idx = {}, {}
+        mine = set(np.nonzero(self.part == rank)[0].tolist())
+        for q in range(world):
+            if q == rank:
+                continue
+            theirs = self.local_sets[q]
+            s_glob = np.array([g for g in theirs.tolist() if g in mine], dtype=np.int64)
+            r_pos = np.nonzero(self.part[local] == q)[0]
+            if s_glob.size:
+                self.send_idx[q] = g2l[s_glob]
+            if r_pos.size:
+                self.recv_idx[q] = r_pos
+
+    def _local(self, q):
+        owned = np.nonzero(self.part == q)[0]
+        have = set(owned.tolist())
+        frontier = owned.tolist()
+        for _ in range(self.layers):
+            nxt = []
+            for e in frontier:
+                for nb in self.glob.nbr[e]:
+                    nb = int(nb)
+                    if nb >= 0 and nb not in have:
+                        have.add(nb)
+                        nxt.append(nb)
+            frontier = nxt
+        return np.array(sorted(have), dtype=np.int64)
+
+    def scatter(self, u_global: np.ndarray) -> np.ndarray:
+        g = self.glob
+        U = np.asarray(u_global).reshape(g.nv, g.num_elements, g.ndof)
+        return np.ascontiguousarray(U[:, self.local, :].reshape(-1))
+
+    def owned(self, u_local):
+        g = self.glob
+        U = np.asarray(u_local).reshape(g.nv, self.local.size, g.ndof)
+        return U[:, self.owned_local, :]
+
+    def owned_global_elements(self) -> np.ndarray:
+        return self.local[self.owned_local]
+
+
+class PartitionExchange:
+    """Point-to-point exchange of whole ghost elements of an ElementPartition:
+    per peer, the owned elements it holds are gathered into one buffer per
+    message and its owned elements held here scattered from one (every rank
+    posts its messages in ascending peer order)."""
+
+    def __init__(self, part: ElementPartition, group=None):
+        self.dec = part
+        self.group = group
+
+    def exchange(self, u):
+        import torch.distributed as dist
+        p = self.dec
+        if p.world == 1:
+            return
+        g = p.glob
+        U = u.view(g.nv, p.local.size, g.ndof)
+        ops, recvs = [], []
+        for q in sorted(set(p.send_idx) | set(p.recv_idx)):
+            if q in p.send_idx:
+                idx = _index(u, p.send_idx[q])
+                ops.append(dist.P2POp(dist.isend, U[:, idx, :].contiguous(), q, self.group))
+            if q in p.recv_idx:
+                buf = u.new_empty((g.nv, p.recv_idx[q].size, g.ndof))
+                recvs.append((q, buf))
+                ops.append(dist.P2POp(dist.irecv, buf, q, self.group))
+        for r in dist.batch_isend_irecv(ops):
+            r.wait()
+        for q, buf in recvs:
+            U[:, _index(u, p.recv_idx[q]), :] = buf
+
+
+def _index(t, idx):
+    import torch
+    return torch.as_tensor(idx, dtype=torch.long, device=t.device)
+
+
+class DistributedRK3:
+    """SSP-RK3 on a slab decomposition (or an ElementPartition): exchange,
+    then one fused stage of the rank's operator (``op.rk_stage(stage, dt, un,
+    us, uout)``) per stage."""
+
+    def __init__(self, dec, op, group=None):
         self.dec, self.op = dec, op
-        self.xchg = GhostExchange(dec, group)
+        self.xchg = PartitionExchange(dec, group) if isinstance(dec, ElementPartition) else GhostExchange(dec, group)
         self._a = self._b = None
 
     def step(self, x, dt: float):

@@ -203,3 +203,71 @@ def test_face_trace_halo_bytes():
     layers = 2 * h.ls * g.ndof * g.nv * 8
     assert trace == 2 * 1024 * 16 * 9 * 8 and layers == 2 * 1024 * 64 * 5 * 8
     assert layers / trace > 2.2
+
+
+# ---- element partitions of general meshes (ElementPartition) ----
+
+def general_case(case):
+    import sys
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    from helpers import geometry_case, ns_geometry_case, smooth_state
+    name, par = {"perturbed2d": ("perturbed2d", dict(parabolic=0)),
+                 "rotated2d": ("rotated2d", dict(parabolic=0, filter=3)),
+                 "boundary3d": ("boundary3d", dict(parabolic=0)),
+                 "warped3d_ns": ("warped3d", dict(parabolic=1, mu=0.02, Pr=0.71)),
+                 "walls2d_ns": ("walls2d_ns", dict(parabolic=1, mu=0.02, Pr=0.71))}[case]
+    m = ns_geometry_case(name) if name.endswith("_ns") else geometry_case(name)
+    return m, smooth_state(m, 13), par
+
+
+def _pworker(rank, world, port, case, compat, q):
+    import torch.distributed as dist
+    os.environ["OMP_NUM_THREADS"] = "1"
+    import sys
+    sys.path.insert(0, ROOT)
+    dist.init_process_group("gloo", init_method=f"tcp://127.0.0.1:{port}", rank=rank, world_size=world)
+    try:
+        from prandtl_b200.distributed import ElementPartition
+        gm, u0, par = general_case(case)
+        rng = np.random.default_rng(3)
+        part = rng.integers(0, world, gm.num_elements)   # scattered, not contiguous
+        dec = ElementPartition(gm, world, rank, layers=2 if par.get("parabolic") else 1, part=part)
+        op = OracleStages(dec.mesh, compat=compat, **par)
+        drv = DistributedRK3(dec, op)
+        x = torch.from_numpy(dec.scatter(u0))
+        dt = 2e-3
+        for _ in range(2):
+            drv.step(x, dt)
+        import oracle
+        ref = oracle.Oracle(gm, compat=compat, **par)
+        y = u0.copy()
+        for _ in range(2):
+            y = ref.rk3_step(y, dt)
+        want = y.reshape(gm.nv, gm.num_elements, gm.ndof)[:, dec.owned_global_elements(), :]
+        got = dec.owned(x.numpy())
+        err = float(np.abs(got - want).max() / np.abs(want).max())
+        q.put((rank, err, dec.owned_local.size))
+    finally:
+        dist.destroy_process_group()
+
+
+@pytest.mark.parametrize("world,case,compat", [(2, "perturbed2d", 1), (3, "perturbed2d", 0), (3, "rotated2d", 0),
+                                               (2, "boundary3d", 1), (2, "warped3d_ns", 0), (3, "walls2d_ns", 1)])
+def test_element_partition_matches_undivided(world, case, compat):
+    """A general mesh split over 2-3 gloo ranks by a scattered element
+    partition (one ghost layer for Euler, two for Navier-Stokes), the oracle
+    as each rank's stage: owned elements equal the undivided mesh's SSP-RK3
+    steps bit for bit (filter and limiter included in one case)."""
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_pworker, args=(r, world, port, case, compat, q)) for r in range(world)]
+    for p in procs:
+        p.start()
+    res = [q.get(timeout=300) for _ in range(world)]
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    assert sum(n for _, _, n in res) == general_case(case)[0].num_elements
+    for rank, err, _ in res:
+        assert err == 0.0, f"rank {rank}: {err}"
