@@ -460,9 +460,12 @@ def build_general_mesh(dim, order, verts, coords, bdr, names, attrs=None) -> Car
     bilinear / trilinear map, and ``connect`` pairs faces by their vertices
     and derives the orientation codes.  An element whose corners the file
     lists clockwise (a negative Jacobian) is mirrored by exchanging its first
-    two local axes, as MFEM's mesh finalisation does for quadrilaterals
-    (swapping corners 1 and 3); ``mesh.reoriented`` lists it and
-    ``mesh.frames`` holds its file frame for ``to_reference_order``."""
+    two local axes (corners 1 and 3 of the listing exchanged); MFEM fixes
+    inverted elements when it reads a mesh, and for a quadrilateral that fix
+    is taken here to be the same exchange, so the element's DG nodes keep
+    the reference's order (``mesh.frames`` is the identity) while
+    ``mesh.reoriented`` lists it.  None of the reference's meshes has such an
+    element, so this choice has not been compared with the reference."""
     ne, nc = verts.shape
     if nc != 2 ** dim:
         raise ValueError(f"elements with {nc} corners in {dim}D")
@@ -482,7 +485,6 @@ def build_general_mesh(dim, order, verts, coords, bdr, names, attrs=None) -> Car
         swap = np.array([(c & ~3) | ((c & 1) << 1) | ((c >> 1) & 1) for c in range(nc)])
         corners[reoriented] = corners[reoriented][:, swap]
         xyz[reoriented] = xyz[reoriented][:, swap, :]
-        frames[reoriented, 0], frames[reoriented, 1] = 2, 1
     boundary = {}
     for key, a in bdr.items():
         if not 1 <= int(a) <= MAX_CONDITIONS:
