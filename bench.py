@@ -719,12 +719,11 @@ def run_geometry_case(args, dev):
                      "path": "pdg_set_geometry + pdg_rk3_steps (graph-replayed steps)"}
         if ns:
             out[name]["roofline"]["kernels"] = "geo_lift_kernel + geo_rhs_kernel<NS> per stage"
-        else:
-            out[name]["cpu_baseline"] = _geometry_reference_sample(dim, order)
+        out[name]["cpu_baseline"] = _geometry_reference_sample(dim, order, ns)
     return out
 
 
-def _geometry_reference_sample(dim, order):
+def _geometry_reference_sample(dim, order, ns=False):
     """The reference's own integrators (oracle/_ref, compiled against the
     stand-in MFEM header with a nodal element transformation) on one host
     core: one right-hand side of a smaller mesh of the same kind (3D: the
@@ -732,17 +731,17 @@ def _geometry_reference_sample(dim, order):
     DOF-stage updates per second."""
     import oracle
     from prandtl_b200 import geometry as G
-    if not oracle.ref_available(False):
-        return {"unavailable": "oracle/_ref/libref_euler.so not built (needs the reference tree)"}
+    if not oracle.ref_available(ns):
+        return {"unavailable": "oracle/_ref/libref_%s.so not built (needs the reference tree)" % ("ns" if ns else "euler")}
     if dim == 3:
         g = G.warped(periodic_box(3, order, 8, 0.0, 2 * np.pi), 0.02)
         u = cases.taylor_green(g)
-        sample = "one RHS of the curved Taylor-Green box 8^3, N=3"
+        sample = "one RHS of the curved Taylor-Green box 8^3, N=3" + (", Navier-Stokes" if ns else "")
     else:
         g = G.rotate_frames(G.perturbed_box(2, order, 32, -1.0, 1.0, 0.2, seed=1), range(0, 32 * 32, 2), seed=2)
         u = cases.kelvin_helmholtz(g)
         sample = "one RHS of the perturbed, frame-rotated box 32^2, N=4"
-    r = oracle.Reference(g)
+    r = oracle.Reference(g, parabolic=True, mu=1.0 / 1600.0, Pr=0.71) if ns else oracle.Reference(g)
     t0 = time.perf_counter()
     r.rhs(u)
     t = time.perf_counter() - t0
