@@ -131,3 +131,29 @@ def test_gpu_restart_continues_bit_for_bit(case, tmp_path, cuda_device):
     op2.rk3_step(y, dt, nsteps=3)
     assert torch.equal(y, ref)
     assert op2.check() == 0
+
+
+def test_restart_on_a_general_mesh_in_reference_order(tmp_path):
+    """The 15-degree ramp as read from the reference's file (general
+    geometry; its fixture), saved in the reference's per-element node order
+    and restarted: two steps equal one step, save, load, one step."""
+    import sys
+    sys.path.insert(0, os.path.dirname(__file__))
+    from test_meshio import fixture_mesh
+    from prandtl_b200 import meshio
+    m = fixture_mesh("ramp", 2)
+    free = [1.4, 4.2, 0.0, 1.0 / 0.4 + 0.5 * 1.4 * 9.0]
+    kinds = {"inlet": 1, "outlet": 2}
+    m.boundaries = {b: ((1, free) if kinds.get(nm) == 1 else (kinds.get(nm, 4), None))
+                    for nm, b in m.boundary_names.items()}
+    u0 = np.repeat(np.array(free), m.num_nodes)
+    x = m.node_coords()
+    u0[:m.num_nodes] *= 1 + 0.05 * np.sin(3 * x[0]) * np.cos(2 * x[1])
+    orc = oracle.Oracle(m, compat=0, parabolic=0)
+    orc.rhs(u0)
+    dt = 0.3 * min(m.h) / (orc.max_char_speed() * 9)
+    u1 = orc.rk3_step(u0, dt)
+    u2 = orc.rk3_step(u1, dt)
+    checkpoint.save(str(tmp_path), 1, dt, meshio.to_reference_order(m, u1), m.dim, m.order)
+    ck = checkpoint.load(str(tmp_path), 1)
+    assert np.array_equal(orc.rk3_step(meshio.from_reference_order(m, ck.u), dt), u2)
