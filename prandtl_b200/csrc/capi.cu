@@ -834,6 +834,8 @@ int pdg_set_geometry(pdg_ctx *c, const double *x, const int32_t *face_orient)
     if (!c) return PDG_ERR_ARG;
     if (!x) return fail(c, PDG_ERR_ARG, "pdg_set_geometry: null coordinates");
     if (c->geo) return fail(c, PDG_ERR_ARG, "pdg_set_geometry: the geometry is already set");
+    if (c->launches > 0 || c->graph_exec)
+        return fail(c, PDG_ERR_ARG, "pdg_set_geometry: must precede the first evaluation");
     if (c->p.parabolic && c->p.compat)
         return fail(c, PDG_ERR_UNSUPPORTED, "pdg_set_geometry: Navier-Stokes on general geometry takes compat = 0");
     const int dim = c->dim, Np = c->Np, N = c->N, nd = c->ndof, nf = 2 * dim;

@@ -152,6 +152,16 @@ def test_gpu_geometry_errors(cuda_device):
     x = torch.from_numpy(smooth_state(g, 1)).to(cuda_device)
     with pytest.raises(pb.PdgError):
         op.vjp(x, torch.ones_like(x))
+    # the geometry must be set before the first evaluation (a captured step
+    # would otherwise replay the box kernels)
+    from prandtl_b200.mesh import periodic_box
+    bm = periodic_box(2, 3, (4, 5), 0.0, 1.0)
+    opb = pb.DGSEMOperator(bm, compat=0, parabolic=0)
+    xb = torch.from_numpy(smooth_state(bm, 1)).to(cuda_device)
+    opb.Mult(xb, torch.empty_like(xb))
+    with pytest.raises(pb.PdgError) as ei:
+        opb._set_geometry(G.warped(bm, 0.01))
+    assert ei.value.code == 1  # PDG_ERR_ARG
 
 
 NS = dict(mu=0.01, Pr=0.71)
