@@ -143,7 +143,8 @@ int pdg_destroy(pdg_ctx *ctx);
  * every node; pdg_gradients runs it alone) and the right-hand-side kernel
  * with the contravariant viscous fluxes (PDG_KERNEL_GEO_NS).  pdg_rhs_vjp, pdg_rk_stage_vjp and pdg_rk_stage_part
  * return PDG_ERR_UNSUPPORTED on such a context; pdg_rk3_step_host copies
- * the state whole.  PDG_ERR_ARG: a non-positive Jacobian at a node, a code
+ * the state whole.  PDG_ERR_ARG: a call after the first evaluation, a
+ * non-positive Jacobian at a node, a code
  * whose neighbour face does not point back, or a neighbour whose normal at
  * the matching node is not the opposite of this element's (a non-conforming
  * face or a wrong code); PDG_ERR_UNSUPPORTED: the reference-value
