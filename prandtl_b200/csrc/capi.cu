@@ -103,7 +103,10 @@ struct pdg_ctx {
     double *geo_d = nullptr;
     int32_t *fnode_d = nullptr;
     double *fnor_d = nullptr;
-    double *geo_grads = nullptr;  // Navier-Stokes: primitive gradients [d][v][node]
+    double *geo_grads = nullptr;  // (unused: the primitive gradients go only to pdg_gradients' buffer)
+    double *geo_fv = nullptr;     // Navier-Stokes: contravariant viscous fluxes [d][row][node]
+    double *geo_cf = nullptr;     // Navier-Stokes: viscous flux . face normal [e][face][face node][row]
+    int32_t *fpart_d = nullptr;   // the neighbour's face-node slot of every face node (-1: boundary)
 };
 
 namespace {
@@ -423,6 +426,9 @@ KParams base_params(pdg_ctx *c)
     P.fnode = c->fnode_d;
     P.fnor = c->fnor_d;
     P.geo_grads = c->geo_grads;
+    P.geo_fv = c->geo_fv;
+    P.geo_cf = c->geo_cf;
+    P.fpart = c->fpart_d;
     return P;
 }
 
@@ -892,6 +898,9 @@ int pdg_set_geometry(pdg_ctx *c, const double *x, const int32_t *face_orient)
     // faces: the neighbour's matching node and the normal out of the face's
     // element 1 (the lower-numbered element; its +d or -d adjugate row)
     std::vector<int32_t> fnode((size_t)ne * nf * nfn, 0);
+    std::vector<int32_t> fpart((size_t)ne * nf * nfn, -1);
+    if ((int64_t)ne * nf * nfn >= (int64_t)INT32_MAX)
+        return fail(c, PDG_ERR_ARG, "pdg_set_geometry: too many face nodes for the face tables");
     std::vector<double> fnor((size_t)ne * nf * nfn * dim, 0.0);
     for (int64_t e = 0; e < ne; e++)
         for (int f = 0; f < nf; f++) {
@@ -925,6 +934,7 @@ int pdg_set_geometry(pdg_ctx *c, const double *x, const int32_t *face_orient)
                 const int t2 = a + Np * b, d2 = f2 / 2, side2 = f2 % 2;
                 const int n2 = host_line_node(dim, Np, d2, t2, side2 ? N : 0);
                 fnode[fi] = n2;
+                fpart[fi] = (int32_t)(((int64_t)nb * nf + f2) * nfn + t2);
                 // matching nodes sit at the same point, up to one periodic
                 // shift per face
                 {
@@ -1002,8 +1012,12 @@ int pdg_set_geometry(pdg_ctx *c, const double *x, const int32_t *face_orient)
     if (r) return r;
     if (c->p.parabolic) {
         if ((r = configure_launch(c, KIND_GEO_LIFT))) return r;
-        if (cudaMalloc(&c->geo_grads, sizeof(double) * dim * c->nv * nn) != cudaSuccess)
+        if (cudaMalloc(&c->geo_fv, sizeof(double) * dim * (c->nv - 1) * nn) != cudaSuccess ||
+            cudaMalloc(&c->geo_cf, sizeof(double) * fpart.size() * (c->nv - 1)) != cudaSuccess ||
+            cudaMalloc(&c->fpart_d, sizeof(int32_t) * fpart.size()) != cudaSuccess)
             return fail(c, PDG_ERR_NOMEM, "pdg_set_geometry: allocation failed");
+        CK(cudaMemcpy(c->fpart_d, fpart.data(), sizeof(int32_t) * fpart.size(), cudaMemcpyHostToDevice),
+           "geometry upload");
     }
     cudaFree(c->fbuf);  // the box path's face buffer is not used
     c->fbuf = nullptr;
@@ -1038,6 +1052,9 @@ int pdg_destroy(pdg_ctx *c)
     cudaFree(c->fnode_d);
     cudaFree(c->fnor_d);
     cudaFree(c->geo_grads);
+    cudaFree(c->geo_fv);
+    cudaFree(c->geo_cf);
+    cudaFree(c->fpart_d);
     if (c->graph_exec) cudaGraphExecDestroy(c->graph_exec);
     if (c->graph) cudaGraphDestroy(c->graph);
     if (c->cap) cudaStreamDestroy(c->cap);

@@ -368,12 +368,11 @@ __device__ __noinline__ double geo_bdr_flux(const KParams &P, int b, const doubl
 }
 
 // Element slot of geo_rhs_kernel: primitives and accumulator; Navier-Stokes
-// adds the contravariant viscous fluxes [d][row][node] and their divergence
-// [row][node] (rows: momenta and energy).
+// adds the divergence of the contravariant viscous fluxes [row][node] (rows:
+// momenta and energy).
 template <int DIM, int N, bool NS> struct GeoShape {
     using S = Shape<DIM, N>;
-    static constexpr int FV = S::EL_RHS_FB;                         // offset of the viscous fluxes
-    static constexpr int DV = FV + DIM * (S::NV - 1) * S::NS_;      // offset of their divergence
+    static constexpr int DV = S::EL_RHS_FB;  // offset of the viscous divergence
     static constexpr int EL = NS ? DV + (S::NV - 1) * S::NS_ : S::EL_RHS_FB;
 };
 
@@ -390,58 +389,16 @@ __device__ __forceinline__ void viscous_flux_cols(const KParams &P, const double
     for (int c = 0; c < DIM; c++) viscous_col<DIM>(q, G, c, P.gm1inv, P.mu, P.lambda_k, fm[c]);
 }
 
-// Primitive gradients of global node g (geo_lift_kernel's output).
-template <int DIM>
-__device__ __forceinline__ void load_grads(const KParams &P, int64_t g, double (*gr)[DIM + 2])
-{
-#pragma unroll
-    for (int k = 0; k < DIM; k++)
-#pragma unroll
-        for (int v = 0; v < DIM + 2; v++) gr[k][v] = __ldg(P.geo_grads + ((int64_t)k * (DIM + 2) + v) * P.nnodes + g);
-}
-
-// Contravariant viscous fluxes of the element's nodes (MultABt(adj, flux),
-// DGSEMIntegrator.cpp:616-640, 764-786) into the slot, then their
-// divergence along each direction's lines, dUv(l) = sum_m Dhat(l, m) F_d(m).
+// Divergence of the contravariant viscous fluxes geo_lift_kernel stored
+// (MultABt(adj, flux) per node, DGSEMIntegrator.cpp:616-640, 764-786) along
+// each direction's lines, dUv(l) = sum_m Dhat(l, m) F_d(m), accumulated over
+// the directions into dv.
 template <int DIM, int N>
-__device__ __forceinline__ void viscous_volume_geo(const KParams &P, double *fv, double *dv, const double *c, int gl,
-                                                   int64_t e, bool valid)
+__device__ __forceinline__ void viscous_volume_geo(const KParams &P, double *dv, const double *c, int gl, int64_t e,
+                                                   bool valid)
 {
     using S = Shape<DIM, N>;
     constexpr int Np = S::Np, NDOF = S::NDOF, NV = S::NV, NR = NV - 1, ST = S::NS_;
-#pragma unroll 1
-    for (int k = 0; k < S::NPL; k++) {
-        const int n = gl + k * S::L;
-        if (n < NDOF) {
-            double sv[NV], gr[DIM][DIM + 2], fm[DIM][DIM + 1];
-            const int64_t g = e * NDOF + n;
-#pragma unroll
-            for (int v = 0; v < NV; v++)
-                sv[v] = valid ? __ldg(P.u + (int64_t)v * P.nnodes + g) : (v == 0 ? 1.0 : (v == NV - 1 ? P.gm1inv : 0.0));
-            if (valid) load_grads<DIM>(P, g, gr);
-            else
-#pragma unroll
-                for (int a = 0; a < DIM; a++)
-#pragma unroll
-                    for (int v = 0; v < NV; v++) gr[a][v] = 0.0;
-            viscous_flux_cols<DIM>(P, sv, gr, fm);
-            const int m = sp<DIM, Np>(n);
-#pragma unroll
-            for (int a = 0; a < DIM; a++) {
-                double adj[DIM];
-#pragma unroll
-                for (int b = 0; b < DIM; b++) adj[b] = valid ? geo_row1<DIM>(P, g, a, b) : (a == b ? 1.0 : 0.0);
-#pragma unroll
-                for (int r = 0; r < NR; r++) {
-                    double acc = 0.0;
-#pragma unroll
-                    for (int b = 0; b < DIM; b++) acc += adj[b] * fm[b][r];
-                    fv[(a * NR + r) * ST + m] = acc;
-                }
-            }
-        }
-    }
-    __syncwarp();
     const double *Dh = C_DHAT(c);
 #pragma unroll 1
     for (int d = 0; d < DIM; d++) {
@@ -453,7 +410,10 @@ __device__ __forceinline__ void viscous_volume_geo(const KParams &P, double *fv,
 #pragma unroll
                 for (int l = 0; l < Np; l++)
 #pragma unroll
-                    for (int r = 0; r < NR; r++) x[l][r] = fv[(d * NR + r) * ST + sp<DIM, Np>(line_node_rt<DIM, Np>(d, line, l))];
+                    for (int r = 0; r < NR; r++)
+                        x[l][r] = valid ? __ldg(P.geo_fv + (int64_t)(d * NR + r) * P.nnodes + e * NDOF +
+                                                line_node_rt<DIM, Np>(d, line, l))
+                                        : 0.0;
 #pragma unroll
                 for (int l = 0; l < Np; l++) {
                     const int m = sp<DIM, Np>(line_node_rt<DIM, Np>(d, line, l));
@@ -506,7 +466,7 @@ __device__ __forceinline__ void geo_tile(const KParams &P, const double *c, doub
         for (int d = 0; d < DIM; d++) ec_lines_geo<DIM, N>(P, d, pr, acc, c, gl, e, valid);
     }
     double *dv = pr + GeoShape<DIM, N, NS>::DV;
-    if (NS && lane_used) viscous_volume_geo<DIM, N>(P, pr + GeoShape<DIM, N, NS>::FV, dv, c, gl, e, valid);
+    if (NS && lane_used) viscous_volume_geo<DIM, N>(P, dv, c, gl, e, valid);
     // (-(1 - alpha) dU [+ dUv]) / J at every node (DGSEMIntegrator.cpp:423-431, 840-860)
     if (lane_used) {
 #pragma unroll
@@ -583,23 +543,15 @@ __device__ __forceinline__ void geo_tile(const KParams &P, const double *c, doub
                     lam = fmax(lam, fmax(qa.lam, qb.lam));
                     sgn = is1 ? -1.0 : 1.0;
                     if (NS) {
-                        // 0.5 (F_v(1) + F_v(2)) . n with element 1's normal (DGSEMIntegrator.cpp:435-549)
-                        double g1[DIM][DIM + 2], g2[DIM][DIM + 2], f1[DIM][DIM + 1], f2[DIM][DIM + 1];
-                        load_grads<DIM>(P, (is1 ? e : other) * NDOF + (is1 ? n : n2), g1);
-                        load_grads<DIM>(P, (is1 ? other : e) * NDOF + (is1 ? n2 : n), g2);
-                        viscous_flux_cols<DIM>(P, s1, g1, f1);
-                        viscous_flux_cols<DIM>(P, s2, g2, f2);
+                        // 0.5 (F_v(1) . n + F_v(2) . n) with element 1's normal
+                        // (DGSEMIntegrator.cpp:435-549); both sides' F_v . n
+                        // come from the lifting kernel
+                        const int64_t pi = __ldg(P.fpart + fi);
 #pragma unroll
                         for (int r = 0; r < NV - 1; r++) {
-                            double t = 0.0;
-#pragma unroll
-                            for (int q = 0; q < DIM; q++) {
-                                double avg = f1[q][r];
-                                avg += f2[q][r];
-                                avg *= 0.5;
-                                t += avg * nor[q];
-                            }
-                            fnv[1 + r] = t;
+                            const double co = __ldg(P.geo_cf + fi * (NV - 1) + r);
+                            const double cn = __ldg(P.geo_cf + pi * (NV - 1) + r);
+                            fnv[1 + r] = 0.5 * (is1 ? co + cn : cn + co);
                         }
                     }
                 } else {
@@ -609,28 +561,13 @@ __device__ __forceinline__ void geo_tile(const KParams &P, const double *c, doub
                     const int bt = (int)bcv[0];
                     if (NS && (bt == BC_SUPERSONIC_OUTFLOW || bt == BC_NOSLIP_ADIABATIC || bt == BC_NOSLIP_ISOTHERMAL ||
                                bt == BC_SUBSONIC_INFLOW_PTTT)) {
-                        // ComputeBdrFaceViscousFlux: the interior state's own viscous flux
-                        // (SupersonicOutflowBdrFaceIntegrator.cpp:15-20; the walls', whose
-                        // adiabatic energy row is the wall velocity's work,
-                        // NoSlipAdiabWallBdrFaceIntegrator.cpp:21-36), or the outer
-                        // state's with the interior gradients (SubsonicInflowPtTtAngBdrFaceIntegrator.cpp:88-92)
-                        double g1[DIM][DIM + 2], f1[DIM][DIM + 1], sv[NV];
-                        load_grads<DIM>(P, e * NDOF + n, g1);
-                        if (bt == BC_SUBSONIC_INFLOW_PTTT) {
-                            double Fd[NV];
-                            geo_bdr_flux<DIM>(P, (int)(-1 - other), s, nor, Fd, sv);
-                        } else {
+                        // ComputeBdrFaceViscousFlux . n, formed by the lifting kernel: the
+                        // interior state's own viscous flux (SupersonicOutflowBdrFaceIntegrator.cpp:15-20;
+                        // the walls', whose adiabatic energy row is the wall velocity's work,
+                        // NoSlipAdiabWallBdrFaceIntegrator.cpp:21-36), or the outer state's
+                        // with the interior gradients (SubsonicInflowPtTtAngBdrFaceIntegrator.cpp:88-92)
 #pragma unroll
-                            for (int v = 0; v < NV; v++) sv[v] = s[v];
-                        }
-                        viscous_flux_cols<DIM>(P, sv, g1, f1);
-#pragma unroll
-                        for (int r = 0; r < NV - 1; r++) {
-                            double t = 0.0;
-#pragma unroll
-                            for (int q = 0; q < DIM; q++) t += f1[q][r] * nor[q];
-                            fnv[1 + r] = t;
-                        }
+                        for (int r = 0; r < NV - 1; r++) fnv[1 + r] = __ldg(P.geo_cf + fi * (NV - 1) + r);
                         if (bt == BC_NOSLIP_ADIABATIC) {
                             double en = 0.0;
 #pragma unroll
@@ -830,14 +767,61 @@ __global__ void __launch_bounds__(128) geo_lift_kernel(const KParams P)
                     double sv[NV];
 #pragma unroll
                     for (int v = 0; v < NV; v++) sv[v] = __ldg(P.u + (int64_t)v * nn + e * NDOF + n);
+                    const int64_t gn = e * NDOF + n;
+                    double g[DIM][NV];
 #pragma unroll
                     for (int q = 0; q < DIM; q++) {
-                        double g[NV];
 #pragma unroll
-                        for (int v = 0; v < NV; v++) g[v] = Gs[(q * NV + v) * ST + sp<DIM, Np>(n)];
-                        entgrad_to_primgrad<DIM>(sv, P.gm1, P.gm1inv, false, g);
+                        for (int v = 0; v < NV; v++) g[q][v] = Gs[(q * NV + v) * ST + sp<DIM, Np>(n)];
+                        entgrad_to_primgrad<DIM>(sv, P.gm1, P.gm1inv, false, g[q]);
+                        if (P.geo_grads)
 #pragma unroll
-                        for (int v = 0; v < NV; v++) P.geo_grads[((int64_t)q * NV + v) * nn + e * NDOF + n] = g[v];
+                            for (int v = 0; v < NV; v++) P.geo_grads[((int64_t)q * NV + v) * nn + gn] = g[q][v];
+                    }
+                    if (!P.geo_fv) continue;
+                    // the viscous flux (NavierStokesFlux::ComputeViscousFlux), its
+                    // contravariant rows MultABt(adj, flux) (DGSEMIntegrator.cpp:616-640,
+                    // 764-786) and, at every face the node lies on, its product with
+                    // the face normal (element 1's; a boundary face's outward one)
+                    double fm[DIM][DIM + 1];
+                    viscous_flux_cols<DIM>(P, sv, g, fm);
+#pragma unroll
+                    for (int a = 0; a < DIM; a++)
+#pragma unroll
+                        for (int r = 0; r < NV - 1; r++) {
+                            double acc = 0.0;
+#pragma unroll
+                            for (int b = 0; b < DIM; b++) acc += geo_row1<DIM>(P, gn, a, b) * fm[b][r];
+                            P.geo_fv[(int64_t)(a * (NV - 1) + r) * nn + gn] = acc;
+                        }
+                    const int pos[3] = {n % Np, (n / Np) % Np, n / (Np * Np)};
+                    const int line[3] = {n / Np, DIM == 2 ? pos[0] : pos[0] + Np * pos[2], pos[0] + Np * pos[1]};
+#pragma unroll
+                    for (int d = 0; d < DIM; d++) {
+                        if (pos[d] != 0 && pos[d] != N) continue;
+                        const int f = 2 * d + (pos[d] == N ? 1 : 0);
+                        const int64_t fi = (e * 2 * DIM + f) * NFN + line[d];
+                        double nor[DIM];
+#pragma unroll
+                        for (int k2 = 0; k2 < DIM; k2++) nor[k2] = __ldg(P.fnor + fi * DIM + k2);
+                        const int64_t other = __ldg(P.nbr + e * 2 * DIM + f);
+                        double fo[DIM][DIM + 1];
+                        const double(*fx)[DIM + 1] = fm;
+                        if (other < 0 && (int)P.bc[(-1 - other) * BC_SLOT] == BC_SUBSONIC_INFLOW_PTTT) {
+                            // the outer state's viscous flux with the interior gradients
+                            // (SubsonicInflowPtTtAngBdrFaceIntegrator.cpp:88-92)
+                            double so[NV], Fd[NV];
+                            geo_bdr_flux<DIM>(P, (int)(-1 - other), sv, nor, Fd, so);
+                            viscous_flux_cols<DIM>(P, so, g, fo);
+                            fx = fo;
+                        }
+#pragma unroll
+                        for (int r = 0; r < NV - 1; r++) {
+                            double t = 0.0;
+#pragma unroll
+                            for (int q = 0; q < DIM; q++) t += fx[q][r] * nor[q];
+                            P.geo_cf[fi * (NV - 1) + r] = t;
+                        }
                     }
                 }
             }
@@ -845,6 +829,12 @@ __global__ void __launch_bounds__(128) geo_lift_kernel(const KParams P)
         __syncwarp();
     }
 }
+
+// Resident 4-warp blocks of the Navier-Stokes variant (its 7 KB element
+// slots fit three per SM).
+#ifndef PDG_GEONS_MIN_BLOCKS
+#define PDG_GEONS_MIN_BLOCKS 3
+#endif
 
 // Resident 4-warp blocks the register budget must allow (3D N = 3).
 #ifndef PDG_GEO3_MIN_BLOCKS
@@ -860,7 +850,8 @@ template <int DIM, int N> struct GeoOccupancy {
 };
 
 template <int DIM, int N, bool NS = false>
-__global__ void __launch_bounds__(128, NS ? 1 : GeoOccupancy<DIM, N>::min_blocks) geo_rhs_kernel(const KParams P)
+__global__ void __launch_bounds__(128, NS ? PDG_GEONS_MIN_BLOCKS : GeoOccupancy<DIM, N>::min_blocks)
+    geo_rhs_kernel(const KParams P)
 {
     using S = Shape<DIM, N>;
     constexpr int Np = S::Np, L = S::L, EPW = S::EPW;

@@ -107,9 +107,16 @@ struct KParams {
     const double *geo;
     const int32_t *fnode;
     const double *fnor;
-    // general geometry, Navier-Stokes: primitive gradients [d][v][node]
-    // (geo_lift_kernel writes them, geo_rhs_kernel<NS> reads them)
+    // general geometry, Navier-Stokes (written by geo_lift_kernel): the
+    // primitive gradients [d][v][node] (when requested), the contravariant
+    // viscous fluxes [d][row][node] and, per element face node, the viscous
+    // flux dotted with the face normal [e][face][face node][row] (rows:
+    // momenta and energy); fpart: the neighbour's slot of each face node in
+    // that last array (-1 on boundary faces)
     double *geo_grads;
+    double *geo_fv;
+    double *geo_cf;
+    const int32_t *fpart;
 };
 
 __device__ __forceinline__ int64_t range_end(const KParams &P) { return P.e_end ? P.e_end : P.ne; }
