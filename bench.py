@@ -707,8 +707,14 @@ def run_geometry_case(args, dev):
         nv, nd = dim + 2, (order + 1) ** dim
         nfn = (order + 1) ** (dim - 1)
         per_el = 8 * (nv * nd * (2 + 2 / 3) + (1 + dim * dim) * nd + 2 * dim * nfn * dim) + 4 * 2 * dim * nfn
-        if ns:  # the lifting kernel: state and metric terms in, gradients out; the volume kernel reads them
-            per_el += 8 * (nv * nd + (1 + dim * dim) * nd + 2 * dim * nfn * dim + 2 * dim * nv * nd) + 4 * 2 * dim * nfn
+        if ns:
+            # the lifting kernel: state, metric terms and face normals in; the
+            # contravariant viscous fluxes and the face nodes' viscous normal
+            # fluxes out, which the volume kernel reads back (the face values
+            # of both sides) with the neighbour-slot table
+            nr = nv - 1
+            per_el += 8 * (nv * nd + (1 + dim * dim) * nd + 2 * dim * nfn * dim + 2 * dim * nr * nd
+                           + 3 * 2 * dim * nfn * nr) + 4 * 2 * dim * nfn * 2
         bytes_stage = per_el * g.num_elements
         stage_s = ms / 3 * 1e-3
         out[name] = {"vdofs": g.size, "steps": 20, "ms_per_step": ms, "value": g.size * 3 / (ms * 1e-3),
