@@ -107,7 +107,6 @@ struct pdg_ctx {
     double *geo_fv = nullptr;     // Navier-Stokes: contravariant viscous fluxes [d][row][node]
     double *geo_cf = nullptr;     // Navier-Stokes: viscous flux . face normal [e][face][face node][row]
     int32_t *fpart_d = nullptr;   // the neighbour's face-node slot of every face node (-1: boundary)
-    double *geo_fb = nullptr;     // inviscid face fluxes at element-1 slots [e][face][face node][v]
 };
 
 namespace {
@@ -299,7 +298,6 @@ int kernel_config(int dim, int N, int kind, int64_t ne, int device, LaunchCfg *c
         const int64_t threads = (kind == KIND_FILTER_BOUNDS || kind == KIND_POSITIVITY) ? 32 * ne
                                 : (kind == KIND_BOUNDARY || kind == KIND_ADJ_BOUNDARY || kind == KIND_BOUNDARY_NS) ? ne
                                 : kind == KIND_ADJ_GATHER ? ne * nfn * (N + 1)  // thread per node
-                                : kind == KIND_GEO_FACE ? 2LL * dim * ne * nfn  // thread per element face node
                                 : ((kind == KIND_LIFT_FACE || kind == KIND_LIFT_FACE_BDR || kind == KIND_LIFT_FACE_FLUX ||
                                     kind == KIND_FACE_FLUX || kind == KIND_ADJ_FACE_E0 || kind == KIND_ADJ_FACE_NS0)
                                        ? (int64_t)dim : 1) * ne * nfn;
@@ -344,8 +342,7 @@ bool kind_used(int kind, int dim, bool parabolic, int filter)
 {
     if (kind == KIND_FILTER_BOUNDS || kind == KIND_FILTER) return filter & 1;
     if (kind == KIND_POSITIVITY) return (filter & 2) != 0;
-    if (kind == KIND_GEO || kind == KIND_GEO_LIFT || kind == KIND_GEO_NS || kind == KIND_GEO_FACE)
-        return false;  // configured by pdg_set_geometry
+    if (kind == KIND_GEO || kind == KIND_GEO_LIFT || kind == KIND_GEO_NS) return false;  // configured by pdg_set_geometry
     if ((kind >= KIND_ADJ_RHS && kind <= KIND_ADJ_FACE_NS2) || kind == KIND_ADJ_BOUNDARY)
         return false;  // configured by the first pdg_rhs_vjp
     const bool ns_kind = kind == KIND_NS || kind == KIND_NS_FACES || kind == KIND_LIFT || kind == KIND_LIFT_FACE ||
@@ -432,7 +429,6 @@ KParams base_params(pdg_ctx *c)
     P.geo_fv = c->geo_fv;
     P.geo_cf = c->geo_cf;
     P.fpart = c->fpart_d;
-    P.geo_fb = c->geo_fb;
     return P;
 }
 
@@ -554,7 +550,6 @@ int evaluate(pdg_ctx *c, int stage, double dt, const double *un, const double *u
                                 "boundary condition %d: type %d has no viscous boundary flux here", b, t);
             }
         if ((c->p.filter & 1) && stage >= 0 && (r = launch(c, KIND_FILTER_BOUNDS, P, s))) return r;
-        if ((r = launch(c, KIND_GEO_FACE, P, s))) return r;
         if (!c->p.parabolic) {
             if ((r = launch(c, KIND_GEO, P, s))) return r;
         } else {
@@ -1015,16 +1010,14 @@ int pdg_set_geometry(pdg_ctx *c, const double *x, const int32_t *face_orient)
     CK(cudaMemcpy(c->fnor_d, fnor.data(), sizeof(double) * fnor.size(), cudaMemcpyHostToDevice), "geometry upload");
     int r = configure_launch(c, c->p.parabolic ? KIND_GEO_NS : KIND_GEO);
     if (r) return r;
-    if ((r = configure_launch(c, KIND_GEO_FACE))) return r;
-    if (cudaMalloc(&c->fpart_d, sizeof(int32_t) * fpart.size()) != cudaSuccess ||
-        cudaMalloc(&c->geo_fb, sizeof(double) * fpart.size() * c->nv) != cudaSuccess)
-        return fail(c, PDG_ERR_NOMEM, "pdg_set_geometry: allocation failed");
-    CK(cudaMemcpy(c->fpart_d, fpart.data(), sizeof(int32_t) * fpart.size(), cudaMemcpyHostToDevice), "geometry upload");
     if (c->p.parabolic) {
         if ((r = configure_launch(c, KIND_GEO_LIFT))) return r;
         if (cudaMalloc(&c->geo_fv, sizeof(double) * dim * (c->nv - 1) * nn) != cudaSuccess ||
-            cudaMalloc(&c->geo_cf, sizeof(double) * fpart.size() * (c->nv - 1)) != cudaSuccess)
+            cudaMalloc(&c->geo_cf, sizeof(double) * fpart.size() * (c->nv - 1)) != cudaSuccess ||
+            cudaMalloc(&c->fpart_d, sizeof(int32_t) * fpart.size()) != cudaSuccess)
             return fail(c, PDG_ERR_NOMEM, "pdg_set_geometry: allocation failed");
+        CK(cudaMemcpy(c->fpart_d, fpart.data(), sizeof(int32_t) * fpart.size(), cudaMemcpyHostToDevice),
+           "geometry upload");
     }
     cudaFree(c->fbuf);  // the box path's face buffer is not used
     c->fbuf = nullptr;
@@ -1062,7 +1055,6 @@ int pdg_destroy(pdg_ctx *c)
     cudaFree(c->geo_fv);
     cudaFree(c->geo_cf);
     cudaFree(c->fpart_d);
-    cudaFree(c->geo_fb);
     if (c->graph_exec) cudaGraphExecDestroy(c->graph_exec);
     if (c->graph) cudaGraphDestroy(c->graph);
     if (c->cap) cudaStreamDestroy(c->cap);

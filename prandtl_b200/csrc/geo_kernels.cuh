@@ -527,13 +527,20 @@ __device__ __forceinline__ void geo_tile(const KParams &P, const double *c, doub
 #pragma unroll
                 for (int v = 0; v < NV; v++) fnv[v] = 0.0;
                 if (other >= 0) {
-                    const bool is1 = e < other || (e == other && side == 1);
-                    // the face's flux, evaluated once at its element 1's slot by
-                    // geo_face_kernel (both elements' volume nodes already
-                    // bound the wave speed it would report)
-                    const int64_t slot = is1 ? fi : (int64_t)__ldg(P.fpart + fi);
+                    const int n2 = __ldg(P.fnode + fi);
+                    double o[NV];
 #pragma unroll
-                    for (int v = 0; v < NV; v++) F[v] = __ldg(P.geo_fb + slot * NV + v);
+                    for (int v = 0; v < NV; v++) o[v] = __ldg(P.u + (int64_t)v * nn + other * NDOF + n2);
+                    const bool is1 = e < other || (e == other && side == 1);
+                    double s1[NV], s2[NV];
+#pragma unroll
+                    for (int v = 0; v < NV; v++) {
+                        s1[v] = is1 ? s[v] : o[v];
+                        s2[v] = is1 ? o[v] : s[v];
+                    }
+                    const Prim<DIM> qa = make_prim<DIM>(s1, P.gamma, P.gm1), qb = make_prim<DIM>(s2, P.gamma, P.gm1);
+                    face_flux_n<DIM>(qa, qb, s1 + 1, s2 + 1, nor, P.gm1inv, P.compat != 0, P.diss_scale, F);
+                    lam = fmax(lam, fmax(qa.lam, qb.lam));
                     sgn = is1 ? -1.0 : 1.0;
                     if (NS) {
                         // 0.5 (F_v(1) . n + F_v(2) . n) with element 1's normal
@@ -820,42 +827,6 @@ __global__ void __launch_bounds__(128) geo_lift_kernel(const KParams P)
             }
         }
         __syncwarp();
-    }
-}
-
-// The inviscid face flux of every interior face node, once per face: a
-// thread per element face node whose element is the face's element 1 (the
-// lower-numbered one) evaluates the Chandrashekar + LLF flux of element 1's
-// and the neighbour's states with element 1's normal (DGSEMIntegrator.cpp:
-// 151-222) and stores it at that slot; geo_rhs_kernel reads it for both
-// elements, so both receive the same flux.
-template <int DIM, int N>
-__global__ void __launch_bounds__(256) geo_face_kernel(const KParams P)
-{
-    using S = Shape<DIM, N>;
-    constexpr int Np = S::Np, NDOF = S::NDOF, NV = S::NV, NFN = S::NFN;
-    const int64_t nn = P.nnodes;
-    const int64_t slots = P.ne * 2 * DIM * NFN;
-    for (int64_t fi = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; fi < slots; fi += (int64_t)gridDim.x * blockDim.x) {
-        const int64_t e = fi / (2 * DIM * NFN);
-        const int f = (int)((fi / NFN) % (2 * DIM)), t = (int)(fi % NFN);
-        const int d = f / 2, side = f % 2;
-        const int64_t other = __ldg(P.nbr + e * 2 * DIM + f);
-        if (other < 0 || !(e < other || (e == other && side == 1))) continue;
-        const int n = line_node_rt<DIM, Np>(d, t, side ? N : 0);
-        const int n2 = __ldg(P.fnode + fi);
-        double s1[NV], s2[NV], nor[DIM], F[NV];
-#pragma unroll
-        for (int v = 0; v < NV; v++) {
-            s1[v] = __ldg(P.u + (int64_t)v * nn + e * NDOF + n);
-            s2[v] = __ldg(P.u + (int64_t)v * nn + other * NDOF + n2);
-        }
-#pragma unroll
-        for (int k = 0; k < DIM; k++) nor[k] = __ldg(P.fnor + fi * DIM + k);
-        const Prim<DIM> qa = make_prim<DIM>(s1, P.gamma, P.gm1), qb = make_prim<DIM>(s2, P.gamma, P.gm1);
-        face_flux_n<DIM>(qa, qb, s1 + 1, s2 + 1, nor, P.gm1inv, P.compat != 0, P.diss_scale, F);
-#pragma unroll
-        for (int v = 0; v < NV; v++) P.geo_fb[fi * NV + v] = F[v];
     }
 }
 

@@ -42,8 +42,7 @@ enum KernelKind {
     KIND_GEO = 35,              // geo_rhs_kernel<dim, N>: Euler right-hand side (+ stage) on a general-geometry mesh
     KIND_GEO_LIFT = 36,         // geo_lift_kernel<dim, N>: BR1 primitive gradients on a general-geometry mesh
     KIND_GEO_NS = 37,           // geo_rhs_kernel<dim, N, true>: Navier-Stokes right-hand side (+ stage), general geometry
-    KIND_GEO_FACE = 38,         // geo_face_kernel<dim, N>: the inviscid flux of every interior face node, once per face
-    KIND_COUNT = 39
+    KIND_COUNT = 38
 };
 
 struct KernelInfo {

@@ -52,7 +52,6 @@ template <int N> static bool info_n(int kind, KernelInfo *out)
     case KIND_POSITIVITY: out->fn = (const void *)&positivity_kernel<2, N>; out->epw = 1; break;
     case KIND_GEO: out->fn = (const void *)&geo_rhs_kernel<2, N>; out->el_doubles = GeoShape<2, N, false>::EL; break;
     case KIND_GEO_NS: out->fn = (const void *)&geo_rhs_kernel<2, N, true>; out->el_doubles = GeoShape<2, N, true>::EL; break;
-    case KIND_GEO_FACE: out->fn = (const void *)&geo_face_kernel<2, N>; break;
     case KIND_GEO_LIFT: out->fn = (const void *)&geo_lift_kernel<2, N>; out->el_doubles = GeoLiftShape<2, N>::EL; break;
     case KIND_FILTER:
         out->fn = (const void *)&filter_kernel<2, N>;

@@ -51,7 +51,6 @@ template <int N> static bool info_n(int kind, KernelInfo *out)
     case KIND_POSITIVITY: out->fn = (const void *)&positivity_kernel<3, N>; out->epw = 1; break;
     case KIND_GEO: out->fn = (const void *)&geo_rhs_kernel<3, N>; out->el_doubles = GeoShape<3, N, false>::EL; break;
     case KIND_GEO_NS: out->fn = (const void *)&geo_rhs_kernel<3, N, true>; out->el_doubles = GeoShape<3, N, true>::EL; break;
-    case KIND_GEO_FACE: out->fn = (const void *)&geo_face_kernel<3, N>; break;
     case KIND_GEO_LIFT:  // 2-warp blocks: its 20 KB per warp then fits five blocks per SM instead of two of 4 warps
         out->fn = (const void *)&geo_lift_kernel<3, N>;
         out->el_doubles = GeoLiftShape<3, N>::EL;

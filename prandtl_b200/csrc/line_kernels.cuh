@@ -117,9 +117,6 @@ struct KParams {
     double *geo_fv;
     double *geo_cf;
     const int32_t *fpart;
-    // general geometry: the inviscid face flux of every interior face node,
-    // at its element 1's slot [e][face][face node][v] (geo_face_kernel)
-    double *geo_fb;
 };
 
 __device__ __forceinline__ int64_t range_end(const KParams &P) { return P.e_end ? P.e_end : P.ne; }
