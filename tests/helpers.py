@@ -140,3 +140,56 @@ def _ns_channel(name):
 
 NS_GEO_CASES = ["warped2d", "perturbed2d", "rotated2d", "warped3d", "perturbed3d", "rotated3d", "boundary2d_ns",
                 "walls2d_ns", "subsonic2d_ns", "walls3d_ns"]
+
+
+def node_jacobian(mesh):
+    """det of the Jacobian at every node of a general mesh: the LGL derivative
+    matrix applied to each element's node coordinates (the element map is the
+    degree-N interpolant of its nodes)."""
+    from prandtl_b200.mesh import gll_nodes
+    dim, Np, ne = mesh.dim, mesh.Np, mesh.num_elements
+    x, _ = gll_nodes(Np)
+    bw = np.array([1.0 / np.prod([x[l] - x[m] for m in range(Np) if m != l]) for l in range(Np)])
+    D = np.zeros((Np, Np))
+    for i in range(Np):
+        for l in range(Np):
+            if l != i:
+                D[i, l] = bw[l] / bw[i] / (x[i] - x[l])
+        D[i, i] = -D[i].sum()
+    X = np.asarray(mesh.coords).reshape((dim, ne) + (Np,) * dim)   # [k, e, (z,) y, x]
+    # A[k][d] = dX_k / dxi_d; xi_0 runs along the last axis
+    A = [[np.moveaxis(np.tensordot(D, X[k], axes=([1], [dim - d])), 0, dim - d) for d in range(dim)]
+         for k in range(dim)]
+    if dim == 2:
+        J = A[0][0] * A[1][1] - A[0][1] * A[1][0]
+    else:
+        J = (A[0][0] * (A[1][1] * A[2][2] - A[1][2] * A[2][1])
+             - A[0][1] * (A[1][0] * A[2][2] - A[1][2] * A[2][0])
+             + A[0][2] * (A[1][0] * A[2][1] - A[1][1] * A[2][0]))
+    return J.reshape(-1)
+
+
+def entropy_vars(u, dim, nn, gamma=1.4):
+    """Entropy variables (rows: nv) of conservative node values u (byNODES)."""
+    U = u.reshape(dim + 2, nn)
+    rho = U[0]
+    vel = U[1:1 + dim] / rho
+    vsq = np.sum(vel * vel, axis=0)
+    p = (gamma - 1.0) * (U[-1] - 0.5 * rho * vsq)
+    beta = rho / p
+    s = np.log(p * rho ** (-gamma))
+    return np.vstack([(gamma - s) / (gamma - 1.0) - 0.5 * beta * vsq, beta * vel, -beta])
+
+
+def entropy_production(mesh, u, dudt):
+    """(sum_i J_i w_i w(u_i) . du_i/dt, sum_i J_i w_i |w(u_i) . du_i/dt|) over
+    every node, J_i the node's Jacobian determinant and w_i its LGL weight."""
+    from prandtl_b200.mesh import gll_nodes
+    dim, nn = mesh.dim, mesh.num_nodes
+    _, w1 = gll_nodes(mesh.Np)
+    wq = w1
+    for _ in range(dim - 1):
+        wq = np.kron(w1, wq)
+    W = np.tile(wq, mesh.num_elements) * node_jacobian(mesh)
+    local = np.sum(entropy_vars(u, dim, nn) * np.asarray(dudt).reshape(dim + 2, nn), axis=0)
+    return float(np.sum(W * local)), float(np.sum(W * np.abs(local)))
