@@ -200,11 +200,16 @@ def perturbed_box(dim: int, order: int, n, lo, hi, amp: float, seed: int = 0, bd
     return m
 
 
-def warped(mesh: CartesianMesh, amp: float, waves: int = 1) -> CartesianMesh:
+def warped(mesh: CartesianMesh, amp: float, waves: int = 1, twist: float = 0.0) -> CartesianMesh:
     """A box mesh (periodic or not, all cells present) with its DG nodes
-    moved by the smooth field dx_d = amp L_d prod_q sin(2 pi k (x_q - lo_q) / L_q),
-    k = waves, which vanishes on the box's sides and is periodic: curved
-    elements whose geometry is the degree-N interpolant of the field."""
+    moved by the smooth field dx_d = amp L_d prod_q sin(2 pi k (x_q - lo_q) / L_q)
+    (1 + twist cos(2 pi k (x_{d+1} - lo_{d+1}) / L_{d+1})), k = waves, which
+    vanishes on the box's sides and is periodic: curved elements whose
+    geometry is the degree-N interpolant of the field.  With twist = 0 every
+    component moves by the same scalar field, so in 3D the quadratic terms of
+    the Jacobian's column cross products cancel and the pointwise metric
+    terms meet the discrete metric identities; a twist turns the
+    displacement's direction from node to node, and they do not."""
     if mesh.cells is not None or mesh.coords is not None:
         raise ValueError("warped() takes a full box mesh")
     X = mesh.node_coords()
@@ -213,7 +218,12 @@ def warped(mesh: CartesianMesh, amp: float, waves: int = 1) -> CartesianMesh:
     for q in range(mesh.dim):
         s = s * np.sin(2 * np.pi * waves * (X[q] - mesh.lo[q]) / L[q])
     out = _copy(mesh)
-    out.coords = X + amp * L[:, None] * s[None, :]
+    disp = amp * L[:, None] * s[None, :]
+    if twist:
+        for d in range(mesh.dim):
+            q = (d + 1) % mesh.dim
+            disp[d] *= 1.0 + twist * np.cos(2 * np.pi * waves * (X[q] - mesh.lo[q]) / L[q])
+    out.coords = X + disp
     periodic = [bool(np.all(mesh.nbr[:, 2 * d:2 * d + 2] >= 0)) for d in range(mesh.dim)]
     corners, _, _, _ = _lattice(mesh.dim, mesh.n, mesh.lo, mesh.hi, periodic)
     out.corners = corners

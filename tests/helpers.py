@@ -65,7 +65,8 @@ GEO_BCS_3D = {0: (1, [1.4, 4.2, 0.3, 0.1, 8.8]), 1: (2, None), 2: (4, None), 3: 
 
 
 def geometry_case(name):
-    """General-geometry meshes: curved (a warped box, degree-N elements),
+    """General-geometry meshes: curved (a warped box, degree-N elements;
+    twisted: the displacement's direction varies),
     skewed (an affine shear), perturbed (bilinear / trilinear elements with
     randomly moved vertices), rotated (element frames rotated, so that faces
     meet in other orientations, as in an unstructured mesh), and boundary
@@ -84,6 +85,10 @@ def geometry_case(name):
         return G.perturbed_box(2, 3, (5, 4), 0.0, 1.0, 0.3, seed=5, bdr=[(0, 1), (2, 3)], boundaries=GEO_BCS_2D)
     if name == "warped3d":
         return G.warped(periodic_box(3, 2, (3, 4, 3), 0.0, 1.0), 0.03)
+    if name == "twisted3d":
+        # the displacement turns from node to node: the pointwise metric terms
+        # miss the discrete metric identities (no free-stream preservation)
+        return G.warped(periodic_box(3, 3, (3, 4, 3), 0.0, 1.0), 0.03, twist=0.8)
     if name == "perturbed3d":
         return G.perturbed_box(3, 3, (3, 3, 3), 0.0, 1.0, 0.25, seed=3)
     if name == "rotated3d":
@@ -94,8 +99,8 @@ def geometry_case(name):
     raise KeyError(name)
 
 
-GEO_CASES = ["warped2d", "skewed2d", "perturbed2d", "rotated2d", "boundary2d", "warped3d", "perturbed3d",
-             "rotated3d", "boundary3d"]
+GEO_CASES = ["warped2d", "skewed2d", "perturbed2d", "rotated2d", "boundary2d", "warped3d", "twisted3d",
+             "perturbed3d", "rotated3d", "boundary3d"]
 
 
 GEO_BCS_NS_2D = {0: (1, [1.4, 0.42, 0.03, 2.6]), 1: (2, None), 2: (3, [1.3, 0.2, 0.0, 2.4]), 3: (2, None)}
@@ -138,8 +143,8 @@ def _ns_channel(name):
                            boundaries=GEO_BCS_NS_WALLS_3D)
 
 
-NS_GEO_CASES = ["warped2d", "perturbed2d", "rotated2d", "warped3d", "perturbed3d", "rotated3d", "boundary2d_ns",
-                "walls2d_ns", "subsonic2d_ns", "walls3d_ns"]
+NS_GEO_CASES = ["warped2d", "perturbed2d", "rotated2d", "warped3d", "twisted3d", "perturbed3d", "rotated3d",
+                "boundary2d_ns", "walls2d_ns", "subsonic2d_ns", "walls3d_ns"]
 
 
 def node_jacobian(mesh):

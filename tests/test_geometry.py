@@ -196,3 +196,20 @@ def test_oracle_entropy_conservation_on_general_geometry(name):
     assert abs(prod) < 1e-13 * scale
     prod_d, _ = entropy_production(g, u, oracle.Oracle(g, parabolic=0, blending=0, compat=0).rhs(u))
     assert prod_d < -1e-3 * scale
+
+
+def test_oracle_twisted_mesh_misses_the_metric_identities():
+    """On a 3D mesh whose displacement turns from node to node the pointwise
+    metric terms miss the discrete metric identities, as in the reference
+    (the right-hand side still matches the reference's, GEO_CASES): a free
+    stream is not kept and entropy is not conserved without dissipation."""
+    from helpers import entropy_production
+    g = geometry_case("twisted3d")
+    nn = g.num_nodes
+    u = np.empty(g.size)
+    u[:nn], u[nn:2 * nn], u[2 * nn:3 * nn], u[3 * nn:4 * nn], u[4 * nn:] = 1.2, 0.6, 0.3, 0.0, 3.0
+    assert np.abs(oracle.Oracle(g, compat=0, parabolic=0, blending=0).rhs(u)).max() > 1e-3
+    v = smooth_state(g, 4)
+    prod, scale = entropy_production(g, v, oracle.Oracle(g, parabolic=0, blending=0, compat=0,
+                                                         face_dissipation=0.0).rhs(v))
+    assert abs(prod) > 1e-6 * scale
